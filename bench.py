@@ -1,0 +1,332 @@
+"""Benchmark of the P1 matrix-free multigrid path on B200.
+
+Workload (one "step"): one application of the P1 constant-stencil Laplacian (flag Inner) on the
+unit cube split into six macro-tetrahedra, refinement level 8 (16,974,593 DoFs, 16,581,375
+inner), FP64 storage — the operator apply of the level-8 cube configuration.  The metric is MDoF/s
+(inner DoFs x applies / s, ApplyBenchmark.cpp:104 of the reference).  Extra fields report one
+FP64 V(3,3) Chebyshev(3) cycle on the same mesh and level.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: the path shards by macro-primitive but the multi-GPU exchange is not built yet, so N>1
+runs N independent replicas (weak scaling), timed with CUDA events, max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+LEVEL = 8
+METRIC = "MDoF/s apply (P1 constant-stencil Laplace, FP64)"
+UNIT = "MDoF/s"
+WORKLOAD = "P1 constant-stencil Laplace apply, unit cube 6 macro-tets, level 8, FP64, flag Inner"
+
+
+def inner_dofs(L):
+    n = 1 << L
+    return (n - 1) ** 3
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--level", type=int, default=LEVEL)
+    p.add_argument("--no-vcycle", action="store_true")
+    return p.parse_args()
+
+
+def dist_setup(n):
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=2)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the cell apply kernel from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "p1_cell_apply_cube_L8.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get("traffic_bytes_per_launch")
+    except Exception:
+        return None
+
+
+def cpu_reference_apply(L, seconds=10.0, max_steps=None, threads=None):
+    """The reference's own generated cell-apply kernel (oracle/_ref) on the six macro-cells, one
+    macro-cell per OpenMP thread.  Returns (MDoF/s, applies, threads, seconds)."""
+    import ctypes as C
+
+    from oracle import hyteg_oracle as O
+    from oracle import ref as R
+
+    if not R.available():
+        return None
+    n = 1 << L
+    size = O.tet_size(n + 1)
+    rng = np.random.default_rng(0)
+    ncell = 6
+    src = [rng.uniform(-1, 1, size) for _ in range(ncell)]
+    dst = [np.zeros(size) for _ in range(ncell)]
+    st = np.tile(np.array([5.0] + [-0.5] * 8 + [0.25] * 6), ncell)
+    dp = C.POINTER(C.c_double)
+    sp = (dp * ncell)(*[a.ctypes.data_as(dp) for a in src])
+    dpp = (dp * ncell)(*[a.ctypes.data_as(dp) for a in dst])
+    threads = threads or min(ncell, os.cpu_count() or 1)
+    lib = R.lib()
+    lib.ref_cell_apply_many(ncell, dpp, sp, L, st.ctypes.data_as(dp), threads)  # warm-up
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        lib.ref_cell_apply_many(ncell, dpp, sp, L, st.ctypes.data_as(dp), threads)
+        k += 1
+        el = time.perf_counter() - t0
+        if (max_steps and k >= max_steps) or (not max_steps and el >= seconds):
+            break
+    cell_inner = ncell * O.tet_size(n - 3) if n >= 4 else 0
+    return cell_inner * k / el / 1e6, k, threads, el
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    L = args.level
+    n = 1 << L
+    from oracle import hyteg_oracle as O
+    from oracle import ref as R
+
+    if not R.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhyteg_ref.so was not built"}))
+        return
+    for _ in range(args.warmup):
+        cpu_reference_apply(L, max_steps=1)
+    rate, k, threads, el = cpu_reference_apply(L, max_steps=args.steps)
+    cell_inner = 6 * O.tet_size(n - 3)
+    ms = el / k * 1e3
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world, "steps": k,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded uniform [-1,1] input)",
+        "config": {"workload": WORKLOAD + " (macro-cell interiors, the reference's generated kernel)", "level": L,
+                   "inner_dofs_cells": cell_inner},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{k} full applies of the 6 macro-cell interiors at level {L}"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    import hyteg_b200 as H
+
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    L = args.level
+    ctx = H.Context(local, stream.cuda_stream)
+    pm = H.PrimitiveStorage.cuboid(ctx=ctx)
+    A = H.P1ConstantLaplaceOperator(pm, 0, L, ctx)
+    x = H.P1Function("x", pm, L, L, ctx)
+    y = H.P1Function("y", pm, L, L, ctx)
+    packed = pm.packed_size(L)
+    rng = np.random.default_rng(1234 + rank)
+    host_x = rng.uniform(-1.0, 1.0, packed)
+    x.upload(L, host_x)
+    ndof = inner_dofs(L)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # device-resident timing (inputs in HBM; each 136 MB vector exceeds the 126 MB L2)
+    for _ in range(max(3, args.warmup)):
+        A.apply(x, y, L, H.Inner)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    l0 = ctx.launches
+    with torch.cuda.stream(stream):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            e0.record(stream)
+            for _ in range(args.steps):
+                A.apply(x, y, L, H.Inner)
+            e1.record(stream)
+            e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = ctx.launches - l0
+    barrier()
+    torch.cuda.synchronize()
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * ndof / (ms_max * 1e-3) / 1e6
+
+    # end to end through the public API: host vector in, apply, host vector out
+    e2e_steps = max(3, min(args.steps, 10))
+    x.upload(L, host_x)
+    y.download(L)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        x.upload(L, host_x)
+        A.apply(x, y, L, H.Inner)
+        out = y.download(L)
+    t_e2e = (time.perf_counter() - t0) / e2e_steps
+    te = torch.tensor([t_e2e], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = world * ndof / float(te.item()) / 1e6
+
+    # one FP64 V(3,3) Chebyshev(3) multigrid cycle on the same level (graph-captured)
+    vcycle = None
+    if not args.no_vcycle:
+        b = H.P1Function("b", pm, 0, L, ctx)
+        xv = H.P1Function("xv", pm, 0, L, ctx)
+        b.upload(L, np.where(np.abs(host_x) > 0, rng.uniform(-1, 1, packed), 0.0))
+        gmg = H.GeometricMultigridSolver(ctx, A, 0, L, preSmoothSteps=3, postSmoothSteps=3, smoother="chebyshev",
+                                         chebyshev_order=3, power_iterations=20)
+        gmg.solve(A, xv, b, L)  # setup + capture
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            v0 = torch.cuda.Event(enable_timing=True)
+            v1 = torch.cuda.Event(enable_timing=True)
+            v0.record(stream)
+            nv = 5
+            for _ in range(nv):
+                gmg.solve(A, xv, b, L)
+            v1.record(stream)
+            v1.synchronize()
+        vcycle = {"ms_per_cycle": v0.elapsed_time(v1) / nv, "cycle": "V(3,3) Chebyshev(3), CG coarse level 0",
+                  "dtype": "f64", "graph": True}
+
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peak()
+    alg_bytes = 2 * 8 * ndof  # read x, write y per inner DoF
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    cpu = cpu_reference_apply(L, seconds=10.0)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded uniform [-1,1] input vector)",
+        "config": {"workload": WORKLOAD, "level": L, "inner_dofs": ndof, "dofs": (2 ** L + 1) ** 3,
+                   "l2": "inputs larger than L2 (136 MB per vector)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "traffic": profile_traffic(),
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "kernel": "k_cell_stencil<double,OP_APPLY> + k_bnd_stencil (one apply)"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": packed * 8, "d2h_bytes_per_step": packed * 8},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if vcycle:
+        line["vcycle"] = vcycle
+    if cpu:
+        rate, k, threads, el = cpu
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                                "sample": f"{k} applies of the 6 macro-cell interiors at level {L} in {el:.1f} s "
+                                          f"(reference's generated kernel, one macro-cell per thread)"}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

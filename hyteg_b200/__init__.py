@@ -1,0 +1,480 @@
+"""hyteg_b200: B200-native matrix-free multigrid for HyTeG-style hybrid tetrahedral grids.
+
+Python mirror of the reference's C++ interface for this path (class and method names follow
+HyTeG: ``P1Function``, ``P1ConstantLaplaceOperator.apply(src, dst, level, flag, updateType)``,
+``smooth_jac``, ``P1toP1LinearRestriction``, ``P1toP1LinearProlongation``,
+``GeometricMultigridSolver``, ``CGSolver``, ``ChebyshevSmoother``).  Every call goes through the
+C ABI declared in ``include/hyteg_b200.h`` and runs CUDA kernels built for sm_100a; there is no
+CPU fallback: without the compiled library or a GPU the calls raise.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(_HERE, "libhyteg_b200.so")
+
+# DoFType (types/types.hpp:29-43) and UpdateType
+Inner = 1
+DirichletBoundary = 2
+NeumannBoundary = 4
+FreeslipBoundary = 8
+All = 15
+Replace = 0
+Add = 1
+
+F64, F32, F16 = 0, 1, 2
+_DTYPES = {"float64": F64, "double": F64, "f64": F64, "float32": F32, "float": F32, "f32": F32,
+           "float16": F16, "half": F16, "f16": F16}
+
+P1_CONST_LAPLACE = 1
+P1_CONST_MASS = 2
+SMOOTHER_JACOBI = 0
+SMOOTHER_CHEBYSHEV = 1
+VCYCLE = 0
+WCYCLE = 1
+
+_lib = None
+
+
+class HybError(RuntimeError):
+    pass
+
+
+class _GmgParams(C.Structure):
+    _fields_ = [
+        ("min_level", C.c_int), ("max_level", C.c_int),
+        ("pre_smooth", C.c_int), ("post_smooth", C.c_int), ("smooth_increment", C.c_int),
+        ("cycle", C.c_int), ("smoother", C.c_int), ("jacobi_relax", C.c_double),
+        ("cheb_order", C.c_int), ("cheb_upper_factor", C.c_double), ("cheb_lower_factor", C.c_double),
+        ("cheb_power_iterations", C.c_int), ("coarse_max_iter", C.c_int),
+        ("coarse_rtol", C.c_double), ("coarse_atol", C.c_double), ("use_graph", C.c_int),
+    ]
+
+
+_SIGS = {
+    "hyb_version": (C.c_char_p, []),
+    "hyb_last_error": (C.c_char_p, []),
+    "hyb_ctx_create": (C.c_int, [C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "hyb_ctx_destroy": (C.c_int, [C.c_void_p]),
+    "hyb_ctx_synchronize": (C.c_int, [C.c_void_p]),
+    "hyb_ctx_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "hyb_ctx_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "hyb_mesh_create": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "hyb_mesh_create_cuboid": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                         C.POINTER(C.c_void_p)]),
+    "hyb_mesh_create_gmsh": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p)]),
+    "hyb_mesh_destroy": (C.c_int, [C.c_void_p]),
+    "hyb_mesh_set_boundary_flags_on_boundary": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "hyb_mesh_set_bc_type": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32]),
+    "hyb_mesh_counts": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "hyb_mesh_primitive_vertices": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "hyb_mesh_primitive_flag": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "hyb_layout_packed_size": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
+    "hyb_layout_primitive_offsets": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "hyb_layout_cell_index": (C.c_int64, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    "hyb_layout_face_index": (C.c_int64, [C.c_int, C.c_int, C.c_int]),
+    "hyb_fn_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "hyb_fn_destroy": (C.c_int, [C.c_void_p]),
+    "hyb_fn_upload": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "hyb_fn_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "hyb_fn_interpolate_const": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_uint32]),
+    "hyb_fn_interpolate_callback": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32]),
+    "hyb_fn_assign": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32]),
+    "hyb_fn_add": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32]),
+    "hyb_fn_mult_elementwise": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32]),
+    "hyb_fn_invert_elementwise": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32]),
+    "hyb_fn_dot": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.POINTER(C.c_double)]),
+    "hyb_fn_copy_from": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "hyb_fn_swap": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "hyb_fn_device_ptr": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
+    "hyb_op_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "hyb_op_destroy": (C.c_int, [C.c_void_p]),
+    "hyb_op_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_int]),
+    "hyb_op_smooth_jac": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_uint32]),
+    "hyb_op_inverse_diagonal": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32]),
+    "hyb_op_stencil": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "hyb_restrict": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32]),
+    "hyb_prolongate": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_int]),
+    "hyb_gmg_params_default": (C.c_int, [C.POINTER(_GmgParams)]),
+    "hyb_gmg_create": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(_GmgParams), C.POINTER(C.c_void_p)]),
+    "hyb_gmg_destroy": (C.c_int, [C.c_void_p]),
+    "hyb_gmg_set_radii": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "hyb_gmg_get_radii": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "hyb_gmg_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "hyb_gmg_solve_cycles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_void_p,
+                                       C.POINTER(C.c_int)]),
+    "hyb_estimate_radius": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "hyb_chebyshev_coefficients": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_void_p]),
+    "hyb_cg_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
+                               C.POINTER(C.c_int)]),
+    "hyb_residual_norm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32,
+                                    C.POINTER(C.c_double)]),
+}
+
+
+def lib():
+    """Load the compiled C-ABI library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBRARY_PATH):
+            raise HybError(f"{LIBRARY_PATH} is missing: build it with `python -m hyteg_b200.build`")
+        L = C.CDLL(LIBRARY_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise HybError(f"hyteg_b200 error {rc}: {lib().hyb_last_error().decode()}")
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Context:
+    """Device + stream.  ``stream``: an integer cudaStream_t handle (e.g. torch's) or None."""
+
+    def __init__(self, device=0, stream=None):
+        h = C.c_void_p()
+        _check(lib().hyb_ctx_create(device, C.c_void_p(stream) if stream else None, C.byref(h)))
+        self.h = h
+
+    def synchronize(self):
+        _check(lib().hyb_ctx_synchronize(self.h))
+
+    @property
+    def launches(self):
+        v = C.c_int64()
+        _check(lib().hyb_ctx_launch_count(self.h, C.byref(v)))
+        return v.value
+
+    @property
+    def stream(self):
+        v = C.c_void_p()
+        _check(lib().hyb_ctx_stream(self.h, C.byref(v)))
+        return v.value or 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hyb_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PrimitiveStorage:
+    """Macro mesh with HyTeG's primitive ids, orientations and boundary flags."""
+
+    def __init__(self, handle, ctx=None):
+        self.h = handle
+        self.ctx = ctx
+
+    @classmethod
+    def from_tets(cls, coords, tets, ctx=None):
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        tets = np.ascontiguousarray(tets, dtype=np.int32)
+        h = C.c_void_p()
+        _check(lib().hyb_mesh_create(ctx.h if ctx else None, coords.shape[0], _ptr(coords), tets.shape[0], _ptr(tets),
+                                     C.byref(h)))
+        return cls(h, ctx)
+
+    @classmethod
+    def cuboid(cls, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), nx=1, ny=1, nz=1, ctx=None):
+        """MeshInfo::meshCuboid; nx=ny=nz=1 gives the six-tetrahedra unit cube."""
+        lo = np.asarray(lo, dtype=np.float64)
+        hi = np.asarray(hi, dtype=np.float64)
+        h = C.c_void_p()
+        _check(lib().hyb_mesh_create_cuboid(ctx.h if ctx else None, _ptr(lo), _ptr(hi), nx, ny, nz, C.byref(h)))
+        return cls(h, ctx)
+
+    @classmethod
+    def from_gmsh(cls, path, ctx=None):
+        h = C.c_void_p()
+        _check(lib().hyb_mesh_create_gmsh(ctx.h if ctx else None, str(path).encode(), C.byref(h)))
+        return cls(h, ctx)
+
+    def set_boundary_flags_on_boundary(self, on_boundary=1, inner=0):
+        _check(lib().hyb_mesh_set_boundary_flags_on_boundary(self.h, on_boundary, inner))
+
+    def set_bc_type(self, flag, dof_type):
+        _check(lib().hyb_mesh_set_bc_type(self.h, flag, dof_type))
+
+    def counts(self):
+        a = np.zeros(4, dtype=np.int32)
+        _check(lib().hyb_mesh_counts(self.h, _ptr(a)))
+        return tuple(int(v) for v in a)
+
+    def primitive_vertices(self, kind, idx):
+        a = np.zeros(4, dtype=np.int32)
+        _check(lib().hyb_mesh_primitive_vertices(self.h, kind, idx, _ptr(a)))
+        return [int(v) for v in a if v >= 0]
+
+    def primitive_flag(self, kind, idx):
+        v = C.c_int()
+        _check(lib().hyb_mesh_primitive_flag(self.h, kind, idx, C.byref(v)))
+        return v.value
+
+    def packed_size(self, level):
+        v = C.c_int64()
+        _check(lib().hyb_layout_packed_size(self.h, level, C.byref(v)))
+        return v.value
+
+    def primitive_offsets(self, level):
+        n = sum(self.counts())
+        off = np.zeros(n, dtype=np.int64)
+        sz = np.zeros(n, dtype=np.int64)
+        _check(lib().hyb_layout_primitive_offsets(self.h, level, _ptr(off), _ptr(sz)))
+        return off, sz
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hyb_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_CALLBACK = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_void_p)
+
+
+class P1Function:
+    """P1Function<ValueType> on levels min_level..max_level (device storage, HyTeG layout)."""
+
+    def __init__(self, name, storage, min_level, max_level, ctx, dtype="float64"):
+        self.name = name
+        self.storage = storage
+        self.ctx = ctx
+        self.min_level, self.max_level = min_level, max_level
+        self.dtype = _DTYPES[dtype] if isinstance(dtype, str) else int(dtype)
+        h = C.c_void_p()
+        _check(lib().hyb_fn_create(ctx.h, storage.h, self.dtype, min_level, max_level, C.byref(h)))
+        self.h = h
+
+    # data movement -----------------------------------------------------------------------
+    def upload(self, level, packed):
+        a = np.ascontiguousarray(packed, dtype=np.float64)
+        if a.size != self.storage.packed_size(level):
+            raise ValueError("packed vector has the wrong size for this level")
+        _check(lib().hyb_fn_upload(self.h, level, _ptr(a)))
+
+    def download(self, level):
+        a = np.zeros(self.storage.packed_size(level), dtype=np.float64)
+        _check(lib().hyb_fn_download(self.h, level, _ptr(a)))
+        return a
+
+    # HyTeG function API ---------------------------------------------------------------------
+    def interpolate(self, value, level, flag=All):
+        if callable(value):
+            def cb(xyz, _user):
+                return float(value(xyz[0], xyz[1], xyz[2]))
+            fn = _CALLBACK(cb)
+            _check(lib().hyb_fn_interpolate_callback(self.h, fn, None, level, flag))
+        else:
+            _check(lib().hyb_fn_interpolate_const(self.h, float(value), level, flag))
+
+    def setToZero(self, level):
+        self.interpolate(0.0, level, All)
+
+    def assign(self, scalars, functions, level, flag=All):
+        s = np.ascontiguousarray(scalars, dtype=np.float64)
+        arr = (C.c_void_p * len(functions))(*[f.h.value for f in functions])
+        _check(lib().hyb_fn_assign(self.h, len(functions), _ptr(s), arr, level, flag))
+
+    def add(self, scalars, functions, level, flag=All):
+        s = np.ascontiguousarray(scalars, dtype=np.float64)
+        arr = (C.c_void_p * len(functions))(*[f.h.value for f in functions])
+        _check(lib().hyb_fn_add(self.h, len(functions), _ptr(s), arr, level, flag))
+
+    def multElementwise(self, functions, level, flag=All):
+        a, b = functions
+        _check(lib().hyb_fn_mult_elementwise(self.h, a.h, b.h, level, flag))
+
+    def invertElementwise(self, level, flag=All):
+        _check(lib().hyb_fn_invert_elementwise(self.h, level, flag))
+
+    def dotGlobal(self, other, level, flag=All):
+        v = C.c_double()
+        _check(lib().hyb_fn_dot(self.h, other.h, level, flag, C.byref(v)))
+        return v.value
+
+    def copyFrom(self, other, level):
+        _check(lib().hyb_fn_copy_from(self.h, other.h, level))
+
+    def swap(self, other, level):
+        _check(lib().hyb_fn_swap(self.h, other.h, level))
+
+    def device_ptr(self, level):
+        p, n = C.c_void_p(), C.c_int64()
+        _check(lib().hyb_fn_device_ptr(self.h, level, C.byref(p), C.byref(n)))
+        return p.value, n.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hyb_fn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _ConstantOperator:
+    kind = None
+
+    def __init__(self, storage, min_level, max_level, ctx):
+        self.storage, self.ctx = storage, ctx
+        self.min_level, self.max_level = min_level, max_level
+        h = C.c_void_p()
+        _check(lib().hyb_op_create(ctx.h, storage.h, self.kind, min_level, max_level, C.byref(h)))
+        self.h = h
+
+    def apply(self, src, dst, level, flag, updateType=Replace):
+        _check(lib().hyb_op_apply(self.h, src.h, dst.h, level, flag, updateType))
+
+    def smooth_jac(self, dst, rhs, src, relax, level, flag):
+        _check(lib().hyb_op_smooth_jac(self.h, dst.h, rhs.h, src.h, float(relax), level, flag))
+
+    def getInverseDiagonalValues(self, out, level, flag=All):
+        _check(lib().hyb_op_inverse_diagonal(self.h, out.h, level, flag))
+        return out
+
+    def stencil(self, level, cell, cls=0):
+        a = np.zeros(15)
+        _check(lib().hyb_op_stencil(self.h, level, cell, cls, _ptr(a)))
+        return a
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hyb_op_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class P1ConstantLaplaceOperator(_ConstantOperator):
+    kind = P1_CONST_LAPLACE
+
+
+class P1ConstantMassOperator(_ConstantOperator):
+    kind = P1_CONST_MASS
+
+
+class P1toP1LinearRestriction:
+    def restrict(self, function, sourceLevel, flag):
+        _check(lib().hyb_restrict(function.h, sourceLevel, flag))
+
+
+class P1toP1LinearProlongation:
+    def prolongate(self, function, sourceLevel, flag):
+        _check(lib().hyb_prolongate(function.h, sourceLevel, flag, Replace))
+
+    def prolongateAndAdd(self, function, sourceLevel, flag):
+        _check(lib().hyb_prolongate(function.h, sourceLevel, flag, Add))
+
+
+def chebyshev_coefficients(order, lower, upper):
+    out = np.zeros(order)
+    _check(lib().hyb_chebyshev_coefficients(order, lower, upper, _ptr(out)))
+    return out
+
+
+def estimate_radius(op, x, tmp, level, iterations):
+    """chebyshev::estimateRadius: power iteration on D^-1 A (x is the start vector, overwritten)."""
+    v = C.c_double()
+    _check(lib().hyb_estimate_radius(op.h, x.h, tmp.h, level, iterations, C.byref(v)))
+    return v.value
+
+
+class CGSolver:
+    def __init__(self, storage, minLevel, maxLevel, maxIter=10**6, relativeTolerance=1e-16, absoluteTolerance=1e-16):
+        self.maxIter, self.rtol, self.atol = maxIter, relativeTolerance, absoluteTolerance
+        self.iterations = 0
+
+    def solve(self, A, x, b, level):
+        it = C.c_int()
+        _check(lib().hyb_cg_solve(A.h, x.h, b.h, level, self.maxIter, self.rtol, self.atol, C.byref(it)))
+        self.iterations = it.value
+
+
+def residual_norm(A, x, b, tmp, level, flag=Inner | NeumannBoundary | FreeslipBoundary):
+    v = C.c_double()
+    _check(lib().hyb_residual_norm(A.h, x.h, b.h, tmp.h, level, flag, C.byref(v)))
+    return v.value
+
+
+class GeometricMultigridSolver:
+    """GeometricMultigridSolver with weighted-Jacobi or Chebyshev smoothing and a device CG coarse solver."""
+
+    def __init__(self, ctx, A, minLevel, maxLevel, preSmoothSteps=3, postSmoothSteps=3, smoothIncrementOnCoarserGrids=0,
+                 cycleType=VCYCLE, smoother="jacobi", relax=2.0 / 3.0, chebyshev_order=3, chebyshev_upper=1.2,
+                 chebyshev_lower=0.3, power_iterations=50, coarse_max_iter=1000, coarse_rtol=1e-14, coarse_atol=1e-16,
+                 use_graph=True):
+        p = _GmgParams()
+        _check(lib().hyb_gmg_params_default(C.byref(p)))
+        p.min_level, p.max_level = minLevel, maxLevel
+        p.pre_smooth, p.post_smooth, p.smooth_increment = preSmoothSteps, postSmoothSteps, smoothIncrementOnCoarserGrids
+        p.cycle = cycleType
+        p.smoother = SMOOTHER_CHEBYSHEV if smoother == "chebyshev" else SMOOTHER_JACOBI
+        p.jacobi_relax = relax
+        p.cheb_order, p.cheb_upper_factor, p.cheb_lower_factor = chebyshev_order, chebyshev_upper, chebyshev_lower
+        p.cheb_power_iterations = power_iterations
+        p.coarse_max_iter, p.coarse_rtol, p.coarse_atol = coarse_max_iter, coarse_rtol, coarse_atol
+        p.use_graph = 1 if use_graph else 0
+        self.params = p
+        self.A, self.ctx = A, ctx
+        h = C.c_void_p()
+        _check(lib().hyb_gmg_create(ctx.h, A.h, C.byref(p), C.byref(h)))
+        self.h = h
+
+    def set_radii(self, radii):
+        r = np.ascontiguousarray(radii, dtype=np.float64)
+        _check(lib().hyb_gmg_set_radii(self.h, _ptr(r)))
+
+    def radii(self):
+        r = np.zeros(self.params.max_level - self.params.min_level + 1)
+        _check(lib().hyb_gmg_get_radii(self.h, _ptr(r)))
+        return r
+
+    def solve(self, A, x, b, level):
+        _check(lib().hyb_gmg_solve(self.h, x.h, b.h, level))
+
+    def solve_cycles(self, x, b, level, max_cycles, rtol=0.0):
+        hist = np.zeros(max_cycles + 1)
+        done = C.c_int()
+        _check(lib().hyb_gmg_solve_cycles(self.h, x.h, b.h, level, max_cycles, rtol, _ptr(hist), C.byref(done)))
+        return hist[: done.value + 1]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hyb_gmg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

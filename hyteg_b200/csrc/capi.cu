@@ -1,0 +1,1314 @@
+// extern "C" entry points of hyteg_b200 and the host-side solver drivers.
+#include "hyb_internal.hpp"
+#include "../../include/hyteg_b200.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <random>
+#include <sstream>
+#include <stdexcept>
+
+struct hyb_ctx
+{
+   hyb::Context c;
+};
+struct hyb_mesh
+{
+   hyb::Mesh m;
+};
+struct hyb_fn
+{
+   hyb::Function f;
+   hyb_ctx*      ctx = nullptr;
+};
+struct hyb_op
+{
+   hyb::Operator o;
+   hyb_ctx*      ctx = nullptr;
+};
+
+namespace hyb {
+std::vector< std::array< double, 3 > > g_unused;
+int  read_gmsh( const std::string& path, std::vector< std::array< double, 3 > >& coords, std::vector< std::array< int, 4 > >& tets );
+void cuboid( const double* lo, const double* hi, int nx, int ny, int nz, std::vector< std::array< double, 3 > >& coords,
+             std::vector< std::array< int, 4 > >& tets );
+std::vector< double > chebyshev_coefficients( int order, double lower, double upper );
+}  // namespace hyb
+
+using namespace hyb;
+
+static thread_local std::string g_err;
+
+#define HYB_TRY try {
+#define HYB_CATCH                                                                                                              \
+   }                                                                                                                           \
+   catch ( const std::invalid_argument& e )                                                                                    \
+   {                                                                                                                           \
+      g_err = e.what();                                                                                                        \
+      return HYB_EINVAL;                                                                                                       \
+   }                                                                                                                           \
+   catch ( const std::bad_alloc& e )                                                                                           \
+   {                                                                                                                           \
+      g_err = "out of host memory";                                                                                            \
+      return HYB_ENOMEM;                                                                                                       \
+   }                                                                                                                           \
+   catch ( const std::runtime_error& e )                                                                                       \
+   {                                                                                                                           \
+      g_err = e.what();                                                                                                        \
+      return ( g_err.find( "out of memory" ) != std::string::npos ) ? HYB_ENOMEM : HYB_EDEVICE;                                \
+   }                                                                                                                           \
+   catch ( const std::exception& e )                                                                                           \
+   {                                                                                                                           \
+      g_err = e.what();                                                                                                        \
+      return HYB_EINTERNAL;                                                                                                    \
+   }                                                                                                                           \
+   return HYB_OK;
+
+static void require( bool cond, const char* msg )
+{
+   if ( !cond ) throw std::invalid_argument( msg );
+}
+
+static void require_level( const Function& f, int L )
+{
+   if ( L < f.minL || L > f.maxL ) throw std::invalid_argument( "level outside the function's level range" );
+}
+
+static void set_device( Context& c ) { check_cuda( cudaSetDevice( c.device ), "cudaSetDevice" ); }
+
+extern "C" {
+
+const char* hyb_version( void ) { return "hyteg_b200 0.1 (sm_100a)"; }
+const char* hyb_last_error( void ) { return g_err.c_str(); }
+
+int hyb_ctx_create( int device, void* stream, hyb_ctx** out )
+{
+   HYB_TRY
+   require( out != nullptr, "out is NULL" );
+   int count = 0;
+   check_cuda( cudaGetDeviceCount( &count ), "cudaGetDeviceCount" );
+   require( device >= 0 && device < count, "device ordinal out of range" );
+   auto* h     = new hyb_ctx();
+   h->c.device = device;
+   set_device( h->c );
+   if ( stream ) h->c.stream = (cudaStream_t) stream;
+   else
+   {
+      check_cuda( cudaStreamCreateWithFlags( &h->c.stream, cudaStreamNonBlocking ), "cudaStreamCreate" );
+      h->c.own_stream = true;
+   }
+   check_cuda( cudaMalloc( &h->c.d_scalars, 64 * sizeof( double ) ), "cudaMalloc(scalars)" );
+   *out = h;
+   HYB_CATCH
+}
+
+int hyb_ctx_destroy( hyb_ctx* ctx )
+{
+   HYB_TRY
+   if ( !ctx ) return HYB_OK;
+   cudaStreamSynchronize( ctx->c.stream );
+   cudaFree( ctx->c.d_partials );
+   cudaFree( ctx->c.d_scalars );
+   if ( ctx->c.own_stream ) cudaStreamDestroy( ctx->c.stream );
+   delete ctx;
+   HYB_CATCH
+}
+
+int hyb_ctx_synchronize( hyb_ctx* ctx )
+{
+   HYB_TRY
+   require( ctx, "ctx is NULL" );
+   check_cuda( cudaStreamSynchronize( ctx->c.stream ), "cudaStreamSynchronize" );
+   HYB_CATCH
+}
+
+int hyb_ctx_launch_count( const hyb_ctx* ctx, int64_t* out )
+{
+   HYB_TRY
+   require( ctx && out, "NULL argument" );
+   *out = ctx->c.launches;
+   HYB_CATCH
+}
+
+int hyb_ctx_stream( const hyb_ctx* ctx, void** stream )
+{
+   HYB_TRY
+   require( ctx && stream, "NULL argument" );
+   *stream = (void*) ctx->c.stream;
+   HYB_CATCH
+}
+
+// ------------------------------------------------------------------------------------------- mesh
+static int make_mesh( hyb_ctx* ctx, const std::vector< std::array< double, 3 > >& coords,
+                      const std::vector< std::array< int, 4 > >& tets, hyb_mesh** out )
+{
+   require( out != nullptr, "out is NULL" );
+   require( !tets.empty(), "mesh without tetrahedra" );
+   auto* h  = new hyb_mesh();
+   h->m.ctx = ctx ? &ctx->c : nullptr;
+   try
+   {
+      h->m.topo.build( coords, tets );
+   } catch ( ... )
+   {
+      delete h;
+      throw;
+   }
+   *out = h;
+   return HYB_OK;
+}
+
+int hyb_mesh_create( hyb_ctx* ctx, int nverts, const double* coords, int ntets, const int* tets, hyb_mesh** out )
+{
+   HYB_TRY
+   require( nverts > 0 && ntets > 0 && coords && tets, "empty mesh" );
+   std::vector< std::array< double, 3 > > c( nverts );
+   std::vector< std::array< int, 4 > >    t( ntets );
+   for ( int i = 0; i < nverts; ++i ) c[i] = { coords[3 * i], coords[3 * i + 1], coords[3 * i + 2] };
+   for ( int i = 0; i < ntets; ++i ) t[i] = { tets[4 * i], tets[4 * i + 1], tets[4 * i + 2], tets[4 * i + 3] };
+   return make_mesh( ctx, c, t, out );
+   HYB_CATCH
+}
+
+int hyb_mesh_create_cuboid( hyb_ctx* ctx, const double* lo, const double* hi, int nx, int ny, int nz, hyb_mesh** out )
+{
+   HYB_TRY
+   require( lo && hi && nx > 0 && ny > 0 && nz > 0, "invalid cuboid" );
+   for ( int d = 0; d < 3; ++d ) require( lo[d] < hi[d], "cuboid lower corner must be below upper corner" );
+   std::vector< std::array< double, 3 > > c;
+   std::vector< std::array< int, 4 > >    t;
+   cuboid( lo, hi, nx, ny, nz, c, t );
+   return make_mesh( ctx, c, t, out );
+   HYB_CATCH
+}
+
+int hyb_mesh_create_gmsh( hyb_ctx* ctx, const char* path, hyb_mesh** out )
+{
+   HYB_TRY
+   require( path, "path is NULL" );
+   std::vector< std::array< double, 3 > > c;
+   std::vector< std::array< int, 4 > >    t;
+   read_gmsh( path, c, t );
+   return make_mesh( ctx, c, t, out );
+   HYB_CATCH
+}
+
+int hyb_mesh_destroy( hyb_mesh* mesh )
+{
+   HYB_TRY
+   delete mesh;
+   HYB_CATCH
+}
+
+int hyb_mesh_set_boundary_flags_on_boundary( hyb_mesh* mesh, int on_boundary, int inner )
+{
+   HYB_TRY
+   require( mesh, "mesh is NULL" );
+   require( mesh->m.levels.empty(), "boundary flags must be set before functions or operators use the mesh" );
+   mesh->m.topo.set_boundary_flags_on_boundary( on_boundary, inner );
+   HYB_CATCH
+}
+
+int hyb_mesh_set_bc_type( hyb_mesh* mesh, int flag, uint32_t dof_type )
+{
+   HYB_TRY
+   require( mesh, "mesh is NULL" );
+   require( mesh->m.levels.empty(), "boundary types must be set before functions or operators use the mesh" );
+   require( dof_type == kInner || dof_type == kDirichlet || dof_type == kNeumann || dof_type == kFreeslip,
+            "dof_type must be a single DoFType bit" );
+   mesh->m.topo.bc_of_flag[flag] = dof_type;
+   HYB_CATCH
+}
+
+int hyb_mesh_counts( const hyb_mesh* mesh, int* counts )
+{
+   HYB_TRY
+   require( mesh && counts, "NULL argument" );
+   counts[0] = mesh->m.topo.nV;
+   counts[1] = mesh->m.topo.nE;
+   counts[2] = mesh->m.topo.nF;
+   counts[3] = mesh->m.topo.nC;
+   HYB_CATCH
+}
+
+int hyb_mesh_primitive_vertices( const hyb_mesh* mesh, int kind, int id, int* out4 )
+{
+   HYB_TRY
+   require( mesh && out4, "NULL argument" );
+   const Topology& t = mesh->m.topo;
+   for ( int k = 0; k < 4; ++k ) out4[k] = -1;
+   switch ( kind )
+   {
+   case 0: require( id >= 0 && id < t.nV, "id out of range" ), out4[0] = id; break;
+   case 1:
+      require( id >= 0 && id < t.nE, "id out of range" );
+      for ( int k = 0; k < 2; ++k ) out4[k] = t.ev[id][k];
+      break;
+   case 2:
+      require( id >= 0 && id < t.nF, "id out of range" );
+      for ( int k = 0; k < 3; ++k ) out4[k] = t.fv[id][k];
+      break;
+   case 3:
+      require( id >= 0 && id < t.nC, "id out of range" );
+      for ( int k = 0; k < 4; ++k ) out4[k] = t.cv[id][k];
+      break;
+   default: throw std::invalid_argument( "kind must be 0..3" );
+   }
+   HYB_CATCH
+}
+
+int hyb_mesh_primitive_flag( const hyb_mesh* mesh, int kind, int id, int* flag )
+{
+   HYB_TRY
+   require( mesh && flag, "NULL argument" );
+   const Topology& t = mesh->m.topo;
+   const std::vector< int >* v = kind == 0 ? &t.flag_v : kind == 1 ? &t.flag_e : kind == 2 ? &t.flag_f : kind == 3 ? &t.flag_c : nullptr;
+   require( v != nullptr, "kind must be 0..3" );
+   require( id >= 0 && id < int( v->size() ), "id out of range" );
+   *flag = ( *v )[id];
+   HYB_CATCH
+}
+
+int hyb_layout_packed_size( hyb_mesh* mesh, int level, int64_t* size )
+{
+   HYB_TRY
+   require( mesh && size, "NULL argument" );
+   require( level >= 0 && level <= 14, "level must be in 0..14" );
+   *size = mesh->m.level( level ).packed_size;
+   HYB_CATCH
+}
+
+int hyb_layout_primitive_offsets( hyb_mesh* mesh, int level, int64_t* offsets, int64_t* sizes )
+{
+   HYB_TRY
+   require( mesh, "mesh is NULL" );
+   require( level >= 0 && level <= 14, "level must be in 0..14" );
+   const P1Level& P = mesh->m.level( level );
+   if ( offsets ) std::copy( P.packed_off.begin(), P.packed_off.end(), offsets );
+   if ( sizes ) std::copy( P.psize.begin(), P.psize.end(), sizes );
+   HYB_CATCH
+}
+
+int64_t hyb_layout_cell_index( int level, int x, int y, int z ) { return cidx( 1 << level, x, y, z ); }
+int64_t hyb_layout_face_index( int level, int i, int j ) { return fidx( 1 << level, i, j ); }
+
+// ------------------------------------------------------------------------------------------- functions
+int hyb_fn_create( hyb_ctx* ctx, hyb_mesh* mesh, int dtype, int min_level, int max_level, hyb_fn** out )
+{
+   HYB_TRY
+   require( ctx && mesh && out, "NULL argument" );
+   require( dtype == F64 || dtype == F32 || dtype == F16, "unknown dtype" );
+   require( min_level >= 0 && min_level <= max_level && max_level <= 14, "invalid level range" );
+   set_device( ctx->c );
+   auto* h    = new hyb_fn();
+   h->ctx     = ctx;
+   h->f.mesh  = &mesh->m;
+   h->f.dtype = dtype;
+   h->f.minL  = min_level;
+   h->f.maxL  = max_level;
+   try
+   {
+      for ( int L = min_level; L <= max_level; ++L )
+      {
+         void*        p  = nullptr;
+         const size_t by = h->f.bytes( L );
+         check_cuda( cudaMalloc( &p, by ), "cudaMalloc(function)" );
+         h->f.data.push_back( p );
+         check_cuda( cudaMemsetAsync( p, 0, by, ctx->c.stream ), "cudaMemset(function)" );
+      }
+   } catch ( ... )
+   {
+      delete h;
+      throw;
+   }
+   *out = h;
+   HYB_CATCH
+}
+
+int hyb_fn_destroy( hyb_fn* fn )
+{
+   HYB_TRY
+   if ( fn ) cudaStreamSynchronize( fn->ctx->c.stream );
+   delete fn;
+   HYB_CATCH
+}
+
+static void sync_copies( hyb_fn* fn, int L )
+{
+   PointArgs a{};
+   a.op   = PT_SYNC;
+   a.flag = kAll;
+   a.dst  = fn->f.ptr( L );
+   launch_point( &fn->ctx->c, fn->f.mesh, L, fn->f.dtype, a );
+}
+
+static void to_device( hyb_fn* fn, int L, const std::vector< double >& padded )
+{
+   const int64_t count = int64_t( padded.size() );
+   if ( fn->f.dtype == F64 )
+   {
+      check_cuda( cudaMemcpyAsync( fn->f.ptr( L ), padded.data(), count * 8, cudaMemcpyHostToDevice, fn->ctx->c.stream ), "upload" );
+      check_cuda( cudaStreamSynchronize( fn->ctx->c.stream ), "upload sync" );
+   }
+   else
+   {
+      double* tmp = nullptr;
+      check_cuda( cudaMalloc( &tmp, count * 8 ), "cudaMalloc(upload staging)" );
+      check_cuda( cudaMemcpyAsync( tmp, padded.data(), count * 8, cudaMemcpyHostToDevice, fn->ctx->c.stream ), "upload" );
+      launch_convert( &fn->ctx->c, count, fn->f.dtype, fn->f.ptr( L ), F64, tmp );
+      check_cuda( cudaStreamSynchronize( fn->ctx->c.stream ), "upload sync" );
+      cudaFree( tmp );
+   }
+}
+
+static std::vector< double > from_device( hyb_fn* fn, int L )
+{
+   const int64_t         count = fn->f.mesh->level( L ).size;
+   std::vector< double > padded( count );
+   if ( fn->f.dtype == F64 )
+   {
+      check_cuda( cudaMemcpyAsync( padded.data(), fn->f.ptr( L ), count * 8, cudaMemcpyDeviceToHost, fn->ctx->c.stream ), "download" );
+      check_cuda( cudaStreamSynchronize( fn->ctx->c.stream ), "download sync" );
+   }
+   else
+   {
+      double* tmp = nullptr;
+      check_cuda( cudaMalloc( &tmp, count * 8 ), "cudaMalloc(download staging)" );
+      launch_convert( &fn->ctx->c, count, F64, tmp, fn->f.dtype, fn->f.ptr( L ) );
+      check_cuda( cudaMemcpyAsync( padded.data(), tmp, count * 8, cudaMemcpyDeviceToHost, fn->ctx->c.stream ), "download" );
+      check_cuda( cudaStreamSynchronize( fn->ctx->c.stream ), "download sync" );
+      cudaFree( tmp );
+   }
+   return padded;
+}
+
+int hyb_fn_upload( hyb_fn* fn, int level, const double* host_packed )
+{
+   HYB_TRY
+   require( fn && host_packed, "NULL argument" );
+   require_level( fn->f, level );
+   const P1Level&        P = fn->f.mesh->level( level );
+   std::vector< double > padded( P.size, 0.0 );
+   for ( size_t p = 0; p < P.off.size(); ++p )
+      std::copy( host_packed + P.packed_off[p], host_packed + P.packed_off[p] + P.psize[p], padded.begin() + P.off[p] );
+   to_device( fn, level, padded );
+   sync_copies( fn, level );
+   HYB_CATCH
+}
+
+int hyb_fn_download( hyb_fn* fn, int level, double* host_packed )
+{
+   HYB_TRY
+   require( fn && host_packed, "NULL argument" );
+   require_level( fn->f, level );
+   const P1Level& P      = fn->f.mesh->level( level );
+   auto           padded = from_device( fn, level );
+   for ( size_t p = 0; p < P.off.size(); ++p )
+      std::copy( padded.begin() + P.off[p], padded.begin() + P.off[p] + P.psize[p], host_packed + P.packed_off[p] );
+   HYB_CATCH
+}
+
+static void pointwise( hyb_fn* dst, int L, uint32_t flag, int op, int n, const double* sc, hyb_fn* const* srcs )
+{
+   require_level( dst->f, L );
+   require( n >= 0 && n <= 3, "at most three source functions" );
+   for ( int k = 0; k < n; ++k )
+   {
+      require( srcs[k] != nullptr, "source function is NULL" );
+      require( srcs[k]->f.mesh == dst->f.mesh, "functions live on different meshes" );
+      require( srcs[k]->f.dtype == dst->f.dtype, "functions of different value types (use hyb_fn_copy_from)" );
+      require_level( srcs[k]->f, L );
+   }
+   if ( flag == kAll && op == PT_LINCOMB )
+   {
+      const void* s[3] = { nullptr, nullptr, nullptr };
+      double      a[3] = { 0, 0, 0 };
+      for ( int k = 0; k < n; ++k ) s[k] = srcs[k]->f.ptr( L ), a[k] = sc[k];
+      if ( n == 0 ) a[0] = sc ? sc[0] : 0.0;
+      launch_flat_lincomb( &dst->ctx->c, dst->f.mesh->level( L ).size, dst->f.dtype, dst->f.ptr( L ), n, s, a );
+      return;
+   }
+   PointArgs a{};
+   a.op   = op;
+   a.flag = flag;
+   a.nsrc = n;
+   a.s0   = n > 0 ? srcs[0]->f.ptr( L ) : nullptr;
+   a.s1   = n > 1 ? srcs[1]->f.ptr( L ) : nullptr;
+   a.s2   = n > 2 ? srcs[2]->f.ptr( L ) : nullptr;
+   a.dst  = dst->f.ptr( L );
+   a.a0   = n > 0 || op == PT_SET ? sc[0] : 0.0;
+   a.a1   = n > 1 ? sc[1] : 0.0;
+   a.a2   = n > 2 ? sc[2] : 0.0;
+   launch_point( &dst->ctx->c, dst->f.mesh, L, dst->f.dtype, a );
+}
+
+int hyb_fn_interpolate_const( hyb_fn* fn, double value, int level, uint32_t flag )
+{
+   HYB_TRY
+   require( fn, "fn is NULL" );
+   require_level( fn->f, level );
+   if ( flag == kAll )
+   {
+      const double a[3] = { value, 0, 0 };
+      launch_flat_lincomb( &fn->ctx->c, fn->f.mesh->level( level ).size, fn->f.dtype, fn->f.ptr( level ), 0, nullptr, a );
+   }
+   else
+      pointwise( fn, level, flag, PT_SET, 0, &value, nullptr );
+   HYB_CATCH
+}
+
+int hyb_fn_interpolate_callback( hyb_fn* fn, double ( *f )( const double*, void* ), void* user, int level, uint32_t flag )
+{
+   HYB_TRY
+   require( fn && f, "NULL argument" );
+   require_level( fn->f, level );
+   const Topology& t      = fn->f.mesh->topo;
+   const P1Level&  P      = fn->f.mesh->level( level );
+   const int       n      = P.n;
+   auto            padded = from_device( fn, level );
+   double          X[3];
+   // owned DoFs per primitive, coordinates from the primitive's own map (coordinateFromIndex of
+   // VertexDoFMacroVertex/Edge/Face/Cell)
+   for ( int v = 0; v < t.nV; ++v )
+      if ( t.bc( t.flag_v[v] ) & flag ) padded[P.off[v]] = f( t.vx[v].data(), user );
+   for ( int e = 0; e < t.nE; ++e )
+   {
+      if ( !( t.bc( t.flag_e[e] ) & flag ) ) continue;
+      const auto &a = t.vx[t.ev[e][0]], &b = t.vx[t.ev[e][1]];
+      for ( int i = 1; i < n; ++i )
+      {
+         for ( int d = 0; d < 3; ++d ) X[d] = a[d] + ( ( b[d] - a[d] ) * ( 1.0 / n ) ) * i;
+         padded[P.off[t.nV + e] + i] = f( X, user );
+      }
+   }
+   for ( int fc = 0; fc < t.nF; ++fc )
+   {
+      if ( !( t.bc( t.flag_f[fc] ) & flag ) ) continue;
+      const auto &a = t.vx[t.fv[fc][0]], &b = t.vx[t.fv[fc][1]], &c = t.vx[t.fv[fc][2]];
+      for ( int j = 1; j < n; ++j )
+         for ( int i = 1; i + j < n; ++i )
+         {
+            for ( int d = 0; d < 3; ++d ) X[d] = a[d] + ( ( b[d] - a[d] ) * ( 1.0 / n ) ) * i + ( ( c[d] - a[d] ) * ( 1.0 / n ) ) * j;
+            padded[P.off[t.nV + t.nE + fc] + fidx( n, i, j )] = f( X, user );
+         }
+   }
+   for ( int c = 0; c < t.nC; ++c )
+   {
+      if ( !( t.bc( t.flag_c[c] ) & flag ) ) continue;
+      const auto &p0 = t.vx[t.cv[c][0]], &p1 = t.vx[t.cv[c][1]], &p2 = t.vx[t.cv[c][2]], &p3 = t.vx[t.cv[c][3]];
+      const int64_t base = P.off[t.nV + t.nE + t.nF + c];
+      for ( int z = 1; z < n; ++z )
+         for ( int y = 1; y + z < n; ++y )
+            for ( int x = 1; x + y + z < n; ++x )
+            {
+               for ( int d = 0; d < 3; ++d )
+                  X[d] = p0[d] + ( ( p1[d] - p0[d] ) * ( 1.0 / n ) ) * x + ( ( p2[d] - p0[d] ) * ( 1.0 / n ) ) * y +
+                         ( ( p3[d] - p0[d] ) * ( 1.0 / n ) ) * z;
+               padded[base + cidx( n, x, y, z )] = f( X, user );
+            }
+   }
+   to_device( fn, level, padded );
+   sync_copies( fn, level );
+   HYB_CATCH
+}
+
+int hyb_fn_assign( hyb_fn* dst, int n, const double* scalars, hyb_fn* const* srcs, int level, uint32_t flag )
+{
+   HYB_TRY
+   require( dst && ( n == 0 || ( scalars && srcs ) ), "NULL argument" );
+   require( n >= 1, "assign needs at least one source" );
+   pointwise( dst, level, flag, PT_LINCOMB, n, scalars, srcs );
+   HYB_CATCH
+}
+
+int hyb_fn_add( hyb_fn* dst, int n, const double* scalars, hyb_fn* const* srcs, int level, uint32_t flag )
+{
+   HYB_TRY
+   require( dst && scalars && srcs && n >= 1, "NULL argument" );
+   pointwise( dst, level, flag, PT_ADD, n, scalars, srcs );
+   HYB_CATCH
+}
+
+int hyb_fn_mult_elementwise( hyb_fn* dst, hyb_fn* a, hyb_fn* b, int level, uint32_t flag )
+{
+   HYB_TRY
+   require( dst && a && b, "NULL argument" );
+   hyb_fn* s[2]  = { a, b };
+   double  sc[2] = { 1, 1 };
+   pointwise( dst, level, flag, PT_MULT, 2, sc, s );
+   HYB_CATCH
+}
+
+int hyb_fn_invert_elementwise( hyb_fn* fn, int level, uint32_t flag )
+{
+   HYB_TRY
+   require( fn, "fn is NULL" );
+   hyb_fn* s[1]  = { fn };
+   double  sc[1] = { 1 };
+   pointwise( fn, level, flag, PT_INVERT, 1, sc, s );
+   HYB_CATCH
+}
+
+int hyb_fn_dot( hyb_fn* a, hyb_fn* b, int level, uint32_t flag, double* out )
+{
+   HYB_TRY
+   require( a && b && out, "NULL argument" );
+   require( a->f.mesh == b->f.mesh && a->f.dtype == b->f.dtype, "incompatible functions" );
+   require_level( a->f, level );
+   require_level( b->f, level );
+   Context& c = a->ctx->c;
+   launch_dot( &c, a->f.mesh, level, a->f.dtype, flag, a->f.ptr( level ), b->f.ptr( level ), c.d_scalars + 32 );
+   check_cuda( cudaMemcpyAsync( out, c.d_scalars + 32, sizeof( double ), cudaMemcpyDeviceToHost, c.stream ), "dot readback" );
+   check_cuda( cudaStreamSynchronize( c.stream ), "dot sync" );
+   HYB_CATCH
+}
+
+int hyb_fn_copy_from( hyb_fn* dst, hyb_fn* src, int level )
+{
+   HYB_TRY
+   require( dst && src, "NULL argument" );
+   require( dst->f.mesh == src->f.mesh, "functions live on different meshes" );
+   require_level( dst->f, level );
+   require_level( src->f, level );
+   launch_convert( &dst->ctx->c, dst->f.mesh->level( level ).size, dst->f.dtype, dst->f.ptr( level ), src->f.dtype,
+                   src->f.ptr( level ) );
+   HYB_CATCH
+}
+
+int hyb_fn_swap( hyb_fn* a, hyb_fn* b, int level )
+{
+   HYB_TRY
+   require( a && b, "NULL argument" );
+   require( a->f.mesh == b->f.mesh && a->f.dtype == b->f.dtype, "incompatible functions" );
+   require_level( a->f, level );
+   require_level( b->f, level );
+   std::swap( a->f.data[level - a->f.minL], b->f.data[level - b->f.minL] );
+   HYB_CATCH
+}
+
+int hyb_fn_device_ptr( hyb_fn* fn, int level, void** ptr, int64_t* nslots )
+{
+   HYB_TRY
+   require( fn, "fn is NULL" );
+   require_level( fn->f, level );
+   if ( ptr ) *ptr = fn->f.ptr( level );
+   if ( nslots ) *nslots = fn->f.mesh->level( level ).size;
+   HYB_CATCH
+}
+
+// ------------------------------------------------------------------------------------------- operators
+int hyb_op_create( hyb_ctx* ctx, hyb_mesh* mesh, int kind, int min_level, int max_level, hyb_op** out )
+{
+   HYB_TRY
+   require( ctx && mesh && out, "NULL argument" );
+   require( kind == HYB_P1_CONST_LAPLACE || kind == HYB_P1_CONST_MASS, "unknown operator kind" );
+   require( min_level >= 0 && min_level <= max_level && max_level <= 14, "invalid level range" );
+   set_device( ctx->c );
+   auto* h   = new hyb_op();
+   h->ctx    = ctx;
+   h->o.mesh = &mesh->m;
+   h->o.kind = kind;
+   h->o.minL = min_level;
+   h->o.maxL = max_level;
+   try
+   {
+      for ( int L = min_level; L <= max_level; ++L ) build_operator_level( &h->o, L );
+   } catch ( ... )
+   {
+      delete h;
+      throw;
+   }
+   *out = h;
+   HYB_CATCH
+}
+
+int hyb_op_destroy( hyb_op* op )
+{
+   HYB_TRY
+   if ( op ) cudaStreamSynchronize( op->ctx->c.stream );
+   delete op;
+   HYB_CATCH
+}
+
+static void check_op_fn( hyb_op* op, hyb_fn* f, int L )
+{
+   require( f != nullptr, "function is NULL" );
+   require( f->f.mesh == op->o.mesh, "function and operator live on different meshes" );
+   require_level( f->f, L );
+   require( L >= op->o.minL && L <= op->o.maxL, "level outside the operator's level range" );
+}
+
+static void stencil( hyb_op* op, int L, int dtype, int code, uint32_t flag, int copy_unflagged, const void* src, const void* v1,
+                     void* v2, void* dst, double a0 = 0, double a1 = 0 )
+{
+   StencilArgs a{};
+   a.op             = code;
+   a.flag           = flag;
+   a.copy_unflagged = copy_unflagged;
+   a.src            = src;
+   a.v1             = v1;
+   a.v2             = v2;
+   a.dst            = dst;
+   a.a0             = a0;
+   a.a1             = a1;
+   launch_stencil( &op->ctx->c, op->o.mesh, &op->o, L, dtype, a );
+}
+
+int hyb_op_apply( hyb_op* op, hyb_fn* src, hyb_fn* dst, int level, uint32_t flag, int update )
+{
+   HYB_TRY
+   require( op, "op is NULL" );
+   check_op_fn( op, src, level );
+   check_op_fn( op, dst, level );
+   require( src != dst, "src and dst must differ" );
+   require( src->f.dtype == dst->f.dtype, "src and dst value types differ" );
+   require( update == HYB_REPLACE || update == HYB_ADD, "update must be HYB_REPLACE or HYB_ADD" );
+   stencil( op, level, src->f.dtype, update == HYB_ADD ? OP_APPLY_ADD : OP_APPLY, flag, 0, src->f.ptr( level ), nullptr, nullptr,
+            dst->f.ptr( level ) );
+   HYB_CATCH
+}
+
+int hyb_op_smooth_jac( hyb_op* op, hyb_fn* dst, hyb_fn* rhs, hyb_fn* src, double relax, int level, uint32_t flag )
+{
+   HYB_TRY
+   require( op, "op is NULL" );
+   check_op_fn( op, dst, level );
+   check_op_fn( op, rhs, level );
+   check_op_fn( op, src, level );
+   require( src != dst, "src and dst must differ" );
+   require( src->f.dtype == dst->f.dtype && rhs->f.dtype == dst->f.dtype, "value types differ" );
+   stencil( op, level, dst->f.dtype, OP_JAC, flag, 0, src->f.ptr( level ), rhs->f.ptr( level ), nullptr, dst->f.ptr( level ),
+            relax );
+   HYB_CATCH
+}
+
+int hyb_op_inverse_diagonal( hyb_op* op, hyb_fn* out, int level, uint32_t flag )
+{
+   HYB_TRY
+   require( op, "op is NULL" );
+   check_op_fn( op, out, level );
+   const OpLevel&  ol = op->o.lv.at( level );
+   const P1Level&  P  = op->o.mesh->level( level );
+   const Topology& t  = op->o.mesh->topo;
+   auto            padded = from_device( out, level );
+   const int       n      = P.n;
+   for ( const auto& tk : P.tasks )
+   {
+      const int b = tk[0];
+      uint32_t  bc = b < t.nV ? t.bc( t.flag_v[b] ) : b < t.nV + t.nE ? t.bc( t.flag_e[b - t.nV] ) : t.bc( t.flag_f[b - t.nV - t.nE] );
+      if ( !( bc & flag ) ) continue;
+      const int64_t o = P.off[b] + ( b < t.nV ? 0 : b < t.nV + t.nE ? tk[1] : fidx( n, tk[1], tk[2] ) );
+      padded[o]       = ol.invd_b[b];
+   }
+   for ( int c = 0; c < t.nC; ++c )
+   {
+      if ( !( t.bc( t.flag_c[c] ) & flag ) ) continue;
+      const int64_t base = P.off[P.nB + c];
+      for ( int z = 1; z < n; ++z )
+         for ( int y = 1; y + z < n; ++y )
+            for ( int x = 1; x + y + z < n; ++x ) padded[base + cidx( n, x, y, z )] = ol.invd_c[c];
+   }
+   to_device( out, level, padded );
+   sync_copies( out, level );
+   HYB_CATCH
+}
+
+int hyb_op_stencil( hyb_op* op, int level, int cell, int cls, double* out15 )
+{
+   HYB_TRY
+   require( op && out15, "NULL argument" );
+   require( level >= op->o.minL && level <= op->o.maxL, "level outside the operator's level range" );
+   require( cell >= 0 && cell < op->o.mesh->topo.nC && cls >= 0 && cls < kNumClasses, "cell or class out of range" );
+   const OpLevel& ol = op->o.lv.at( level );
+   std::copy( ol.W.begin() + ( size_t( cell ) * kNumClasses + cls ) * kNumDirs,
+              ol.W.begin() + ( size_t( cell ) * kNumClasses + cls + 1 ) * kNumDirs, out15 );
+   HYB_CATCH
+}
+
+// ------------------------------------------------------------------------------------------- transfer
+int hyb_restrict( hyb_fn* fn, int source_level, uint32_t flag )
+{
+   HYB_TRY
+   require( fn, "fn is NULL" );
+   require_level( fn->f, source_level );
+   require_level( fn->f, source_level - 1 );
+   launch_restrict( &fn->ctx->c, fn->f.mesh, source_level, fn->f.dtype, flag, fn->f.ptr( source_level ),
+                    fn->f.ptr( source_level - 1 ) );
+   HYB_CATCH
+}
+
+int hyb_prolongate( hyb_fn* fn, int source_level, uint32_t flag, int update )
+{
+   HYB_TRY
+   require( fn, "fn is NULL" );
+   require_level( fn->f, source_level );
+   require_level( fn->f, source_level + 1 );
+   require( update == HYB_REPLACE || update == HYB_ADD, "update must be HYB_REPLACE or HYB_ADD" );
+   launch_prolongate( &fn->ctx->c, fn->f.mesh, source_level, fn->f.dtype, flag, fn->f.ptr( source_level ),
+                      fn->f.ptr( source_level + 1 ), update == HYB_ADD );
+   HYB_CATCH
+}
+
+}  // extern "C"
+
+// =============================================================================================
+// solvers
+// =============================================================================================
+namespace hyb {
+
+struct FnHolder
+{
+   hyb_fn* h = nullptr;
+   ~FnHolder() { hyb_fn_destroy( h ); }
+};
+
+static hyb_fn* new_fn( hyb_ctx* ctx, Mesh* m, int dtype, int minL, int maxL )
+{
+   hyb_fn* h  = new hyb_fn();
+   h->ctx     = ctx;
+   h->f.mesh  = m;
+   h->f.dtype = dtype;
+   h->f.minL  = minL;
+   h->f.maxL  = maxL;
+   for ( int L = minL; L <= maxL; ++L )
+   {
+      void* p = nullptr;
+      check_cuda( cudaMalloc( &p, h->f.bytes( L ) ), "cudaMalloc(solver temporary)" );
+      check_cuda( cudaMemsetAsync( p, 0, h->f.bytes( L ), ctx->c.stream ), "cudaMemset" );
+      h->f.data.push_back( p );
+   }
+   return h;
+}
+
+constexpr uint32_t kSolveFlag = kInner | kNeumann | kFreeslip;
+
+// CG on the device; all control scalars stay on the device so the loop can be graph-captured.
+struct CGState
+{
+   hyb_fn* p  = nullptr;
+   hyb_fn* ap = nullptr;
+   hyb_fn* r  = nullptr;
+   double* st = nullptr;  // 16 doubles
+};
+
+static void cg_run( hyb_op* op, CGState& s, hyb_fn* x, hyb_fn* b, int L, int maxit, double rtol, double atol, bool host_checks )
+{
+   Context& c  = op->ctx->c;
+   const int dt = x->f.dtype;
+   for ( hyb_fn* f : { s.p, s.ap, s.r } )
+      check_cuda( cudaMemsetAsync( f->f.ptr( L ), 0, f->f.bytes( L ), c.stream ), "cudaMemset(cg)" );
+   // init (CGSolver::init): r = b - A x ; p = r ; prsold = r.r
+   stencil( op, L, dt, OP_RESID, kSolveFlag, 0, x->f.ptr( L ), b->f.ptr( L ), nullptr, s.r->f.ptr( L ) );
+   {
+      PointArgs a{};
+      a.op   = PT_LINCOMB;
+      a.flag = kSolveFlag;
+      a.nsrc = 1;
+      a.s0   = s.r->f.ptr( L );
+      a.dst  = s.p->f.ptr( L );
+      a.a0   = 1.0;
+      launch_point( &c, op->o.mesh, L, dt, a );
+   }
+   launch_dot( &c, op->o.mesh, L, dt, kSolveFlag, s.r->f.ptr( L ), s.r->f.ptr( L ), s.st + 3 );
+   launch_cg_scalar( &c, s.st, 0, rtol, atol );
+   for ( int it = 0; it < maxit; ++it )
+   {
+      if ( host_checks && ( it % 8 ) == 0 )
+      {
+         double done = 0;
+         check_cuda( cudaMemcpyAsync( &done, s.st + 6, sizeof( double ), cudaMemcpyDeviceToHost, c.stream ), "cg readback" );
+         check_cuda( cudaStreamSynchronize( c.stream ), "cg sync" );
+         if ( done != 0.0 ) break;
+      }
+      stencil( op, L, dt, OP_APPLY, kSolveFlag, 0, s.p->f.ptr( L ), nullptr, nullptr, s.ap->f.ptr( L ) );
+      launch_dot( &c, op->o.mesh, L, dt, kSolveFlag, s.p->f.ptr( L ), s.ap->f.ptr( L ), s.st + 2 );
+      launch_cg_scalar( &c, s.st, 1, rtol, atol );
+      PointArgs a{};
+      a.op          = PT_CG_XR;
+      a.flag        = kSolveFlag;
+      a.s0          = x->f.ptr( L );
+      a.s1          = s.p->f.ptr( L );
+      a.s2          = s.ap->f.ptr( L );
+      a.dst         = s.r->f.ptr( L );
+      a.dev_scalars = s.st;
+      launch_point( &c, op->o.mesh, L, dt, a );
+      launch_dot( &c, op->o.mesh, L, dt, kSolveFlag, s.r->f.ptr( L ), s.r->f.ptr( L ), s.st + 3 );
+      launch_cg_scalar( &c, s.st, 2, rtol, atol );
+      PointArgs q{};
+      q.op          = PT_CG_P;
+      q.flag        = kSolveFlag;
+      q.s0          = s.r->f.ptr( L );
+      q.dst         = s.p->f.ptr( L );
+      q.dev_scalars = s.st;
+      launch_point( &c, op->o.mesh, L, dt, q );
+   }
+}
+
+std::vector< double > chebyshev_coefficients( int order, double lower, double upper )
+{
+   // error polynomial e(t) = T_k((theta - t)/delta) / T_k(theta/delta); x += p(D^-1 A) D^-1 r with
+   // 1 - t p(t) = e(t), i.e. p_i = -e_{i+1} (same coefficients as
+   // ChebyshevSmoother::setupCoefficientsInternal, ChebyshevSmoother.hpp:329-555)
+   if ( order < 1 || order > 16 ) throw std::invalid_argument( "Chebyshev order must be 1..16" );
+   if ( !( upper > lower ) || !( lower > 0 ) ) throw std::invalid_argument( "Chebyshev bounds must satisfy 0 < lower < upper" );
+   const double theta = 0.5 * ( upper + lower ), delta = 0.5 * ( upper - lower );
+   std::vector< std::vector< double > > T = { { 1.0 }, { 0.0, 1.0 } };
+   for ( int k = 2; k <= order; ++k )
+   {
+      std::vector< double > t( k + 1, 0.0 );
+      for ( size_t i = 0; i < T[k - 1].size(); ++i ) t[i + 1] += 2 * T[k - 1][i];
+      for ( size_t i = 0; i < T[k - 2].size(); ++i ) t[i] -= T[k - 2][i];
+      T.push_back( t );
+   }
+   const auto&           Tk = T[order];
+   std::vector< double > poly( order + 1, 0.0 ), pw = { 1.0 };
+   for ( int k = 0; k <= order; ++k )
+   {
+      for ( size_t i = 0; i < pw.size(); ++i ) poly[i] += Tk[k] * pw[i];
+      std::vector< double > nx( pw.size() + 1, 0.0 );
+      for ( size_t i = 0; i < pw.size(); ++i )
+      {
+         nx[i] += pw[i] * ( theta / delta );
+         nx[i + 1] += pw[i] * ( -1.0 / delta );
+      }
+      pw = nx;
+   }
+   double norm = 0, s = theta / delta, sp = 1;
+   for ( int k = 0; k <= order; ++k ) norm += Tk[k] * sp, sp *= s;
+   std::vector< double > out( order );
+   for ( int i = 0; i < order; ++i ) out[i] = -poly[i + 1] / norm;
+   return out;
+}
+
+}  // namespace hyb
+
+struct hyb_gmg
+{
+   hyb_ctx*                             ctx = nullptr;
+   hyb_op*                              op  = nullptr;
+   hyb_gmg_params                       p{};
+   int                                  dtype = -1;
+   hyb_fn*                              tmp   = nullptr;  // residual per level
+   hyb_fn*                              jt    = nullptr;  // Jacobi ping-pong partner of x
+   hyb_fn*                              z0    = nullptr;  // Chebyshev temporaries
+   hyb_fn*                              z1    = nullptr;
+   hyb::CGState                         cg;
+   std::vector< double >                radii;
+   std::vector< std::vector< double > > coeff;
+   std::vector< int >                   swaps;  // Jacobi swaps per level in the current cycle
+   // graph cache
+   cudaGraphExec_t gexec   = nullptr;
+   void*           g_x     = nullptr;
+   void*           g_b     = nullptr;
+   int             g_level = -1;
+   ~hyb_gmg()
+   {
+      if ( gexec ) cudaGraphExecDestroy( gexec );
+      hyb_fn_destroy( tmp );
+      hyb_fn_destroy( jt );
+      hyb_fn_destroy( z0 );
+      hyb_fn_destroy( z1 );
+      hyb_fn_destroy( cg.p );
+      hyb_fn_destroy( cg.ap );
+      hyb_fn_destroy( cg.r );
+      cudaFree( cg.st );
+   }
+};
+
+namespace hyb {
+
+static void gmg_alloc( hyb_gmg* g, int dtype )
+{
+   if ( g->dtype == dtype ) return;
+   if ( g->dtype >= 0 ) throw std::invalid_argument( "a multigrid solver instance serves one value type" );
+   Mesh*     m = g->op->o.mesh;
+   const int a = g->p.min_level, b = g->p.max_level;
+   g->tmp      = new_fn( g->ctx, m, dtype, a, b );
+   if ( g->p.smoother == HYB_SMOOTHER_JACOBI ) g->jt = new_fn( g->ctx, m, dtype, a, b );
+   else
+   {
+      g->z0 = new_fn( g->ctx, m, dtype, a, b );
+      g->z1 = new_fn( g->ctx, m, dtype, a, b );
+   }
+   g->cg.p  = new_fn( g->ctx, m, dtype, a, a );
+   g->cg.ap = new_fn( g->ctx, m, dtype, a, a );
+   g->cg.r  = new_fn( g->ctx, m, dtype, a, a );
+   check_cuda( cudaMalloc( &g->cg.st, 16 * sizeof( double ) ), "cudaMalloc(cg state)" );
+   check_cuda( cudaMemsetAsync( g->cg.st, 0, 16 * sizeof( double ), g->ctx->c.stream ), "cudaMemset" );
+   g->dtype = dtype;
+}
+
+static void smooth( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int L )
+{
+   hyb_op* op = g->op;
+   const int dt = x->f.dtype;
+   if ( g->p.smoother == HYB_SMOOTHER_JACOBI )
+   {
+      // WeightedJacobiSmoother::solve: tmp <- x (All); x <- tmp + w D^-1 (b - A tmp).  The copy is
+      // replaced by exchanging the storage of x and its partner; unflagged DoFs are carried over by
+      // the sweep itself.
+      std::swap( x->f.data[L - x->f.minL], g->jt->f.data[L - g->jt->f.minL] );
+      g->swaps[L - g->p.min_level] ^= 1;
+      stencil( op, L, dt, OP_JAC, kSolveFlag, 1, g->jt->f.ptr( L ), b->f.ptr( L ), nullptr, x->f.ptr( L ), g->p.jacobi_relax );
+      return;
+   }
+   // ChebyshevSmoother::solve (ChebyshevSmoother.hpp:112-240), fused: step 0 z0 = D^-1 (b - A x),
+   // step m z_m = D^-1 A z_{m-1} with x += c_{m-1} z_{m-1}, last step adds c_{k-1} z_{k-1} too.
+   const auto& c     = g->coeff.at( L - g->p.min_level );
+   const int   order = int( c.size() );
+   hyb_fn*     za = g->z0, *zb = g->z1;
+   stencil( op, L, dt, OP_CHEB0, kSolveFlag, 1, x->f.ptr( L ), b->f.ptr( L ), nullptr, za->f.ptr( L ) );
+   if ( order == 1 )
+   {
+      PointArgs a{};
+      a.op   = PT_ADD;
+      a.flag = kSolveFlag;
+      a.nsrc = 1;
+      a.s0   = za->f.ptr( L );
+      a.dst  = x->f.ptr( L );
+      a.a0   = c[0];
+      launch_point( &g->ctx->c, op->o.mesh, L, dt, a );
+      return;
+   }
+   for ( int m = 1; m < order; ++m )
+   {
+      if ( m < order - 1 )
+      {
+         stencil( op, L, dt, OP_CHEBI, kSolveFlag, 1, za->f.ptr( L ), nullptr, x->f.ptr( L ), zb->f.ptr( L ), c[m - 1] );
+         std::swap( za, zb );
+      }
+      else
+         stencil( op, L, dt, OP_CHEBL, kSolveFlag, 0, za->f.ptr( L ), nullptr, x->f.ptr( L ), nullptr, c[m - 1], c[m] );
+   }
+}
+
+static void cycle_rec( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int L, int invoked, bool host_checks )
+{
+   hyb_op*   op = g->op;
+   Context&  cx = g->ctx->c;
+   const int dt = x->f.dtype;
+   if ( L == g->p.min_level )
+   {
+      cg_run( op, g->cg, x, b, L, g->p.coarse_max_iter, g->p.coarse_rtol, g->p.coarse_atol, host_checks );
+      return;
+   }
+   const int pre = g->p.pre_smooth + g->p.smooth_increment * ( invoked - L );
+   for ( int i = 0; i < pre; ++i ) smooth( g, x, b, L );
+   // residual, restricted straight into b on level L-1 (b.assign({1},{tmp},L-1,flag) of the reference)
+   stencil( op, L, dt, OP_RESID, kSolveFlag, 0, x->f.ptr( L ), b->f.ptr( L ), nullptr, g->tmp->f.ptr( L ) );
+   launch_restrict( &cx, op->o.mesh, L, dt, kSolveFlag, g->tmp->f.ptr( L ), b->f.ptr( L - 1 ) );
+   check_cuda( cudaMemsetAsync( x->f.ptr( L - 1 ), 0, x->f.bytes( L - 1 ), cx.stream ), "x.interpolate(0)" );
+   cycle_rec( g, x, b, L - 1, invoked, host_checks );
+   if ( g->p.cycle == HYB_WCYCLE ) cycle_rec( g, x, b, L - 1, invoked, host_checks );
+   launch_prolongate( &cx, op->o.mesh, L - 1, dt, kSolveFlag, x->f.ptr( L - 1 ), x->f.ptr( L ), 1 );
+   const int post = g->p.post_smooth + g->p.smooth_increment * ( invoked - L );
+   for ( int i = 0; i < post; ++i ) smooth( g, x, b, L );
+}
+
+static void one_cycle( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int L, bool host_checks )
+{
+   std::fill( g->swaps.begin(), g->swaps.end(), 0 );
+   cycle_rec( g, x, b, L, L, host_checks );
+   // restore the storage assignment of x so that every cycle (and a captured graph) starts alike
+   for ( int l = g->p.min_level; l <= L; ++l )
+      if ( g->swaps[l - g->p.min_level] )
+      {
+         const int64_t count = x->f.mesh->level( l ).size;
+         const void*   s[1]  = { x->f.ptr( l ) };
+         const double  a[3]  = { 1, 0, 0 };
+         launch_flat_lincomb( &g->ctx->c, count, x->f.dtype, g->jt->f.ptr( l ), 1, s, a );
+         std::swap( x->f.data[l - x->f.minL], g->jt->f.data[l - g->jt->f.minL] );
+      }
+}
+
+static void run_cycle( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int L )
+{
+   Context& cx = g->ctx->c;
+   if ( !g->p.use_graph )
+   {
+      one_cycle( g, x, b, L, true );
+      return;
+   }
+   if ( !( g->gexec && g->g_x == x->f.ptr( L ) && g->g_b == b->f.ptr( L ) && g->g_level == L ) )
+   {
+      if ( g->gexec ) cudaGraphExecDestroy( g->gexec ), g->gexec = nullptr;
+      cudaGraph_t graph;
+      check_cuda( cudaStreamBeginCapture( cx.stream, cudaStreamCaptureModeThreadLocal ), "begin capture" );
+      try
+      {
+         one_cycle( g, x, b, L, false );
+      } catch ( ... )
+      {
+         cudaStreamEndCapture( cx.stream, &graph );
+         throw;
+      }
+      check_cuda( cudaStreamEndCapture( cx.stream, &graph ), "end capture" );
+      check_cuda( cudaGraphInstantiate( &g->gexec, graph, 0 ), "graph instantiate" );
+      cudaGraphDestroy( graph );
+      g->g_x     = x->f.ptr( L );
+      g->g_b     = b->f.ptr( L );
+      g->g_level = L;
+   }
+   check_cuda( cudaGraphLaunch( g->gexec, cx.stream ), "graph launch" );
+   cx.launches += 1;
+}
+
+static double residual_norm( hyb_op* op, hyb_fn* x, hyb_fn* b, hyb_fn* tmp, int L, uint32_t flag )
+{
+   Context& c = op->ctx->c;
+   stencil( op, L, x->f.dtype, OP_RESID, flag, 0, x->f.ptr( L ), b->f.ptr( L ), nullptr, tmp->f.ptr( L ) );
+   launch_dot( &c, op->o.mesh, L, x->f.dtype, flag, tmp->f.ptr( L ), tmp->f.ptr( L ), c.d_scalars + 40 );
+   double r = 0;
+   check_cuda( cudaMemcpyAsync( &r, c.d_scalars + 40, sizeof( double ), cudaMemcpyDeviceToHost, c.stream ), "readback" );
+   check_cuda( cudaStreamSynchronize( c.stream ), "sync" );
+   return std::sqrt( r );
+}
+
+static double power_iteration( hyb_op* op, hyb_fn* x, hyb_fn* aux, int L, int iters )
+{
+   // estimateSpectralRadiusWithPowerIteration on D^-1 A with flag All (SpectrumEstimation.hpp:56-84)
+   Context& c  = op->ctx->c;
+   const int dt = x->f.dtype;
+   const int64_t count = op->o.mesh->level( L ).size;
+   auto dot = [&]( hyb_fn* a, hyb_fn* b ) {
+      launch_dot( &c, op->o.mesh, L, dt, kAll, a->f.ptr( L ), b->f.ptr( L ), c.d_scalars + 48 );
+      double r = 0;
+      check_cuda( cudaMemcpyAsync( &r, c.d_scalars + 48, sizeof( double ), cudaMemcpyDeviceToHost, c.stream ), "readback" );
+      check_cuda( cudaStreamSynchronize( c.stream ), "sync" );
+      return r;
+   };
+   auto scale = [&]( hyb_fn* dst, hyb_fn* src, double s ) {
+      const void*  p[1] = { src->f.ptr( L ) };
+      const double a[3] = { s, 0, 0 };
+      launch_flat_lincomb( &c, count, dt, dst->f.ptr( L ), 1, p, a );
+   };
+   double norm = std::sqrt( dot( x, x ) );
+   scale( x, x, 1.0 / norm );
+   stencil( op, L, dt, OP_DINV_APPLY, kAll, 0, x->f.ptr( L ), nullptr, nullptr, aux->f.ptr( L ) );
+   double radius = 0;
+   for ( int it = 1; it <= iters; ++it )
+   {
+      norm = std::sqrt( dot( aux, aux ) );
+      scale( x, aux, 1.0 / norm );
+      stencil( op, L, dt, OP_DINV_APPLY, kAll, 0, x->f.ptr( L ), nullptr, nullptr, aux->f.ptr( L ) );
+      radius = dot( x, aux );
+   }
+   return radius;
+}
+
+static void set_coefficients( hyb_gmg* g )
+{
+   g->coeff.clear();
+   for ( size_t i = 0; i < g->radii.size(); ++i )
+      g->coeff.push_back( chebyshev_coefficients( g->p.cheb_order, g->p.cheb_lower_factor * g->radii[i],
+                                                  g->p.cheb_upper_factor * g->radii[i] ) );
+   if ( g->gexec ) cudaGraphExecDestroy( g->gexec ), g->gexec = nullptr;
+}
+
+// seeded start vector for the power iteration: uniform in [-1, 1] on every owned DoF
+static void seeded_vector( hyb_fn* x, int L, uint64_t seed )
+{
+   const P1Level&                           P = x->f.mesh->level( L );
+   std::vector< double >                    packed( P.packed_size, 0.0 );
+   std::mt19937_64                          rng( seed );
+   std::uniform_real_distribution< double > U( -1.0, 1.0 );
+   for ( auto& v : packed ) v = U( rng );
+   hyb_fn_upload( x, L, packed.data() );
+}
+
+}  // namespace hyb
+
+extern "C" {
+
+int hyb_gmg_params_default( hyb_gmg_params* p )
+{
+   HYB_TRY
+   require( p, "NULL argument" );
+   *p                       = hyb_gmg_params{};
+   p->min_level             = 0;
+   p->max_level             = 0;
+   p->pre_smooth            = 3;
+   p->post_smooth           = 3;
+   p->smooth_increment      = 0;
+   p->cycle                 = HYB_VCYCLE;
+   p->smoother              = HYB_SMOOTHER_JACOBI;
+   p->jacobi_relax          = 2.0 / 3.0;
+   p->cheb_order            = 3;
+   p->cheb_upper_factor     = 1.2;
+   p->cheb_lower_factor     = 0.3;
+   p->cheb_power_iterations = 50;
+   p->coarse_max_iter       = 1000;
+   p->coarse_rtol           = 1e-14;
+   p->coarse_atol           = 1e-16;
+   p->use_graph             = 1;
+   HYB_CATCH
+}
+
+int hyb_gmg_create( hyb_ctx* ctx, hyb_op* op, const hyb_gmg_params* params, hyb_gmg** out )
+{
+   HYB_TRY
+   require( ctx && op && params && out, "NULL argument" );
+   const hyb_gmg_params& p = *params;
+   require( p.min_level >= op->o.minL && p.max_level <= op->o.maxL && p.min_level <= p.max_level,
+            "multigrid levels outside the operator's level range" );
+   require( p.smoother == HYB_SMOOTHER_JACOBI || p.smoother == HYB_SMOOTHER_CHEBYSHEV, "unknown smoother" );
+   require( p.cycle == HYB_VCYCLE || p.cycle == HYB_WCYCLE, "unknown cycle type" );
+   require( p.pre_smooth >= 0 && p.post_smooth >= 0 && p.smooth_increment >= 0, "negative smoothing steps" );
+   require( p.coarse_max_iter >= 0, "negative coarse iteration count" );
+   auto* g = new hyb_gmg();
+   g->ctx  = ctx;
+   g->op   = op;
+   g->p    = p;
+   g->swaps.assign( p.max_level - p.min_level + 1, 0 );
+   *out = g;
+   HYB_CATCH
+}
+
+int hyb_gmg_destroy( hyb_gmg* gmg )
+{
+   HYB_TRY
+   if ( gmg ) cudaStreamSynchronize( gmg->ctx->c.stream );
+   delete gmg;
+   HYB_CATCH
+}
+
+int hyb_gmg_set_radii( hyb_gmg* g, const double* radii )
+{
+   HYB_TRY
+   require( g && radii, "NULL argument" );
+   g->radii.assign( radii, radii + ( g->p.max_level - g->p.min_level + 1 ) );
+   set_coefficients( g );
+   HYB_CATCH
+}
+
+int hyb_gmg_get_radii( hyb_gmg* g, double* radii )
+{
+   HYB_TRY
+   require( g && radii, "NULL argument" );
+   require( !g->radii.empty(), "radii not set yet" );
+   std::copy( g->radii.begin(), g->radii.end(), radii );
+   HYB_CATCH
+}
+
+static void gmg_prepare( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int level )
+{
+   require( g && x && b, "NULL argument" );
+   require( x != b, "x and b must differ" );
+   require( x->f.mesh == g->op->o.mesh && b->f.mesh == g->op->o.mesh, "functions live on another mesh" );
+   require( x->f.dtype == b->f.dtype, "x and b value types differ" );
+   require( level >= g->p.min_level && level <= g->p.max_level, "level outside the multigrid range" );
+   require( x->f.minL <= g->p.min_level && x->f.maxL >= level && b->f.minL <= g->p.min_level && b->f.maxL >= level,
+            "x and b must hold every level from the coarse level up to `level`" );
+   gmg_alloc( g, x->f.dtype );
+   if ( g->p.smoother == HYB_SMOOTHER_CHEBYSHEV && g->radii.empty() )
+   {
+      hyb_fn* v   = new_fn( g->ctx, g->op->o.mesh, x->f.dtype, g->p.min_level, g->p.max_level );
+      hyb_fn* aux = new_fn( g->ctx, g->op->o.mesh, x->f.dtype, g->p.min_level, g->p.max_level );
+      for ( int L = g->p.min_level; L <= g->p.max_level; ++L )
+      {
+         seeded_vector( v, L, 1234567u + L );
+         g->radii.push_back( power_iteration( g->op, v, aux, L, g->p.cheb_power_iterations ) );
+      }
+      hyb_fn_destroy( v );
+      hyb_fn_destroy( aux );
+      set_coefficients( g );
+   }
+}
+
+int hyb_gmg_solve( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int level )
+{
+   HYB_TRY
+   gmg_prepare( g, x, b, level );
+   run_cycle( g, x, b, level );
+   HYB_CATCH
+}
+
+int hyb_gmg_solve_cycles( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int level, int max_cycles, double rtol, double* res_history,
+                          int* cycles_done )
+{
+   HYB_TRY
+   gmg_prepare( g, x, b, level );
+   require( max_cycles >= 0, "negative cycle count" );
+   double r0   = residual_norm( g->op, x, b, g->tmp, level, kSolveFlag );
+   if ( res_history ) res_history[0] = r0;
+   int k = 0;
+   for ( ; k < max_cycles; ++k )
+   {
+      run_cycle( g, x, b, level );
+      const double r = residual_norm( g->op, x, b, g->tmp, level, kSolveFlag );
+      if ( res_history ) res_history[k + 1] = r;
+      if ( !std::isfinite( r ) ) throw std::runtime_error( "multigrid diverged: residual is not finite" );
+      if ( r0 > 0 && r / r0 < rtol )
+      {
+         ++k;
+         break;
+      }
+   }
+   if ( cycles_done ) *cycles_done = k;
+   HYB_CATCH
+}
+
+int hyb_estimate_radius( hyb_op* op, hyb_fn* x, hyb_fn* tmp, int level, int iterations, double* radius )
+{
+   HYB_TRY
+   require( op && x && tmp && radius, "NULL argument" );
+   check_op_fn( op, x, level );
+   check_op_fn( op, tmp, level );
+   require( iterations >= 1, "iterations must be >= 1" );
+   *radius = power_iteration( op, x, tmp, level, iterations );
+   HYB_CATCH
+}
+
+int hyb_chebyshev_coefficients( int order, double lower, double upper, double* out )
+{
+   HYB_TRY
+   require( out, "NULL argument" );
+   auto c = chebyshev_coefficients( order, lower, upper );
+   std::copy( c.begin(), c.end(), out );
+   HYB_CATCH
+}
+
+int hyb_cg_solve( hyb_op* op, hyb_fn* x, hyb_fn* b, int level, int max_iter, double rtol, double atol, int* iterations )
+{
+   HYB_TRY
+   require( op && x && b, "NULL argument" );
+   check_op_fn( op, x, level );
+   check_op_fn( op, b, level );
+   require( x->f.dtype == b->f.dtype, "value types differ" );
+   CGState s;
+   FnHolder hp, ha, hr;
+   hp.h = s.p  = new_fn( op->ctx, op->o.mesh, x->f.dtype, level, level );
+   ha.h = s.ap = new_fn( op->ctx, op->o.mesh, x->f.dtype, level, level );
+   hr.h = s.r  = new_fn( op->ctx, op->o.mesh, x->f.dtype, level, level );
+   check_cuda( cudaMalloc( &s.st, 16 * sizeof( double ) ), "cudaMalloc(cg state)" );
+   try
+   {
+      cg_run( op, s, x, b, level, max_iter, rtol, atol, true );
+      double st[16];
+      check_cuda( cudaMemcpyAsync( st, s.st, sizeof( st ), cudaMemcpyDeviceToHost, op->ctx->c.stream ), "readback" );
+      check_cuda( cudaStreamSynchronize( op->ctx->c.stream ), "sync" );
+      if ( iterations ) *iterations = int( st[7] );
+   } catch ( ... )
+   {
+      cudaFree( s.st );
+      throw;
+   }
+   cudaFree( s.st );
+   HYB_CATCH
+}
+
+int hyb_residual_norm( hyb_op* op, hyb_fn* x, hyb_fn* b, hyb_fn* tmp, int level, uint32_t flag, double* out )
+{
+   HYB_TRY
+   require( op && x && b && tmp && out, "NULL argument" );
+   check_op_fn( op, x, level );
+   check_op_fn( op, b, level );
+   check_op_fn( op, tmp, level );
+   *out = residual_norm( op, x, b, tmp, level, flag );
+   HYB_CATCH
+}
+
+}  // extern "C"

@@ -1,0 +1,247 @@
+// Internal declarations of the hyteg_b200 runtime (host C++ and CUDA).
+//
+// Data model (per function, per level): one device buffer holding every macro-primitive's
+// vertex-DoF array in HyTeG's own per-primitive layout (VertexDoFMemory.hpp:39-60 of the
+// reference), packed in the order vertices, edges, faces, cells, each primitive array starting
+// on a 32-element boundary.  Owned DoFs are the cell interiors, face interiors, edge interiors
+// and the macro-vertices.  Cell arrays also hold copies of the face/edge/vertex DoFs on their
+// boundary; every kernel that writes a lower-dimensional owner also writes those copies
+// ("write-through"), so cell arrays are always consistent and no separate ghost exchange is
+// needed before a stencil sweep.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+
+#include <array>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace hyb {
+
+// DoFType bits (types/types.hpp:29-43 of the reference)
+enum : uint32_t { kInner = 1, kDirichlet = 2, kNeumann = 4, kFreeslip = 8, kAll = 15 };
+
+enum DType : int { F64 = 0, F32 = 1, F16 = 2 };
+
+inline size_t dtype_size(int dt) { return dt == F64 ? 8 : dt == F32 ? 4 : 2; }
+
+// --------------------------------------------------------------------------------------------
+// index math (MacroCellIndexing.hpp:39-52, MacroFaceIndexing.hpp:39-50)
+// --------------------------------------------------------------------------------------------
+__host__ __device__ inline int64_t tet_size(int64_t w) { return ((w + 2) * (w + 1) * w) / 6; }
+__host__ __device__ inline int64_t tri_size(int64_t w) { return ((w + 1) * w) / 2; }
+
+// cell-local (x, y, z) with x+y+z <= n  ->  offset inside the cell array (width n+1)
+__host__ __device__ inline int64_t cidx(int n, int x, int y, int z)
+{
+   const int64_t w  = n + 1;
+   const int64_t wz = w - z;
+   return tet_size(w) - tet_size(wz) + (int64_t) y * (wz + 1) - ((int64_t) y * (y + 1)) / 2 + x;
+}
+
+// face-local (i, j) with i+j <= n  ->  offset inside the face array (width n+1)
+__host__ __device__ inline int64_t fidx(int n, int i, int j)
+{
+   const int64_t w = n + 1;
+   return (int64_t) j * (w + 1) - ((int64_t) j * (j + 1)) / 2 + i;
+}
+
+// The 15 stencil directions: centre first, then the 14 neighbours of the 3D P1 stencil
+// (VertexDoFIndexing.hpp:289-323).
+constexpr int kNumDirs = 15;
+extern const int kDirs[kNumDirs][3];
+
+// Position classes of a micro-vertex inside a macro-cell: 0 interior, 1..4 cell faces 0..3,
+// 5..10 cell edges 0..5, 11..14 cell vertices 0..3.  Cell-local numbering follows
+// SetupPrimitiveStorage.cpp:305-315 (faces 012, 013, 023, 123; edges 01, 02, 12, 03, 13, 23).
+constexpr int kNumClasses = 15;
+// bit mask of directions that stay inside the cell for a point of each class
+extern const uint16_t kClassDirMask[kNumClasses];
+int class_of_point(int n, int x, int y, int z);  // host version
+
+struct Incidence {
+   int   cell;
+   int   cls;
+   int8_t o[3];   // origin = n * o (cell-local corner of the primitive's vertex 0)
+   int8_t e1[3];  // cell-local step per primitive-local i
+   int8_t e2[3];  // cell-local step per primitive-local j
+   int8_t pad[3];
+};
+
+// --------------------------------------------------------------------------------------------
+// macro mesh / primitive storage (host)
+// --------------------------------------------------------------------------------------------
+struct Topology {
+   int nV = 0, nE = 0, nF = 0, nC = 0;
+   std::vector< std::array< double, 3 > > vx;  // coordinates per vertex (id order)
+   std::vector< std::array< int, 2 > >    ev;  // edge vertices (sorted)
+   std::vector< std::array< int, 3 > >    fv;  // face vertices (sorted)
+   std::vector< std::array< int, 4 > >    cv;  // cell vertices (mesh order)
+   std::vector< std::array< int, 6 > >    ce;  // cell local edges
+   std::vector< std::array< int, 4 > >    cf;  // cell local faces
+   std::vector< std::vector< int > >      v_edges, v_faces, v_cells, e_faces, e_cells, f_cells;
+   std::vector< int >                     flag_v, flag_e, flag_f, flag_c;  // mesh boundary flags
+   std::map< int, uint32_t >              bc_of_flag{ { 0, kInner }, { 1, kDirichlet }, { 2, kNeumann }, { 3, kFreeslip } };
+   // optional blending (0 = affine, 1 = icosahedral shell)
+   int    blending = 0;
+   double shell_rmin = 0, shell_rmax = 0;
+
+   uint32_t bc(int flag) const
+   {
+      auto it = bc_of_flag.find( flag );
+      return it == bc_of_flag.end() ? kInner : it->second;
+   }
+   void build( const std::vector< std::array< double, 3 > >& coords, const std::vector< std::array< int, 4 > >& tets );
+   void set_boundary_flags_on_boundary( int onBoundary, int inner );
+};
+
+// per-level host + device tables of the P1 layout
+struct P1Level {
+   int     L = 0, n = 0;
+   int64_t size = 0;         // slots incl. padding
+   int64_t packed_size = 0;  // slots without padding (HyTeG export)
+   std::vector< int64_t > off;         // slot offset of each primitive (v, e, f, c order)
+   std::vector< int64_t > packed_off;  // same without padding
+   std::vector< int64_t > psize;       // HyTeG array size of each primitive
+   // boundary primitives (vertices, edges, faces) in one index space: b = v | nV+e | nV+nE+f
+   int                          nB = 0;
+   std::vector< int >           inc_begin;  // nB+1
+   std::vector< Incidence >     inc;
+   std::vector< std::array< int, 4 > > tasks;  // {b, i, j, 0}: owned DoFs of boundary primitives
+   std::vector< std::array< int, 2 > > rows;   // (y, z) of cell interior rows
+   int64_t n_owned_cell = 0;
+   // device copies
+   int64_t*   d_off       = nullptr;  // all primitives
+   int*       d_inc_begin = nullptr;
+   Incidence* d_inc       = nullptr;
+   int4*      d_tasks     = nullptr;
+   int2*      d_rows      = nullptr;
+   uint8_t*   d_bc        = nullptr;  // bc type per primitive (v, e, f, c order)
+   int8_t*    d_bkind     = nullptr;  // 0 vertex, 1 edge, 2 face per boundary primitive
+   float*     d_ncell_cls = nullptr;  // per cell, per class: number of macro-cells around the sub-primitive
+};
+
+struct Context;
+
+struct Mesh {
+   Context*                                  ctx = nullptr;
+   Topology                                  topo;
+   std::map< int, std::unique_ptr< P1Level > > levels;
+   P1Level&                                  level( int L );
+   ~Mesh();
+};
+
+struct Function {
+   Mesh*                mesh  = nullptr;
+   int                  dtype = F64;
+   int                  minL = 0, maxL = 0;
+   std::vector< void* > data;  // device buffer per level (index L - minL)
+   void*                ptr( int L ) const { return data.at( L - minL ); }
+   size_t               bytes( int L ) const;
+   ~Function();
+};
+
+// constant-stencil operator (P1ConstantLaplaceOperator and friends)
+struct OpLevel {
+   std::vector< double > W;      // [nC][15 classes][15 dirs]
+   std::vector< double > invd_b; // per boundary primitive
+   std::vector< double > invd_c; // per cell
+   double* d_W = nullptr;
+   float*  d_Wf = nullptr;
+   double* d_invd_b = nullptr;
+   double* d_invd_c = nullptr;
+   float*  d_invd_bf = nullptr;
+   float*  d_invd_cf = nullptr;
+};
+
+struct Operator {
+   Mesh*                     mesh = nullptr;
+   int                       kind = 0;
+   int                       minL = 0, maxL = 0;
+   std::map< int, OpLevel >  lv;
+   ~Operator();
+};
+
+struct Context {
+   int          device = 0;
+   cudaStream_t stream = nullptr;
+   bool         own_stream = false;
+   std::string  last_error;
+   // scratch for reductions
+   double* d_partials = nullptr;
+   int     partial_cap = 0;
+   double* d_scalars = nullptr;  // small pool of device scalars
+   int64_t launches = 0;         // kernel launches issued through this context
+};
+
+// --------------------------------------------------------------------------------------------
+// kernel launchers (p1_kernels.cu)
+// --------------------------------------------------------------------------------------------
+enum StencilOp : int {
+   OP_APPLY = 0,     // dst = A src
+   OP_APPLY_ADD,     // dst += A src
+   OP_RESID,         // dst = v1 - A src
+   OP_JAC,           // dst = src + a0 * (invd * (v1 - A src)); unflagged: dst = src
+   OP_CHEB0,         // dst = invd * (v1 - A src); unflagged: dst = src
+   OP_CHEBI,         // dst = invd * (A src); v2 += a0 * src; unflagged: dst = v2
+   OP_CHEBL,         // v2 = (v2 + a0 * src) + a1 * (invd * (A src))
+   OP_DINV_APPLY,    // dst = invd * (A src)
+};
+
+struct StencilArgs {
+   int         op;
+   uint32_t    flag;
+   int         copy_unflagged;
+   const void* src;
+   const void* v1;
+   void*       v2;
+   void*       dst;
+   double      a0, a1;
+};
+
+void launch_stencil( Context* ctx, Mesh* m, Operator* A, int L, int dtype, const StencilArgs& a );
+
+enum PointOp : int {
+   PT_LINCOMB = 0,  // dst = a0*s0 + a1*s1 + a2*s2 (nsrc terms)
+   PT_ADD,          // dst += a0*s0 + a1*s1 + a2*s2
+   PT_MULT,         // dst = s0 * s1
+   PT_INVERT,       // dst = 1 / s0
+   PT_SET,          // dst = a0
+   PT_CG_XR,        // s0 += alpha*s1 (x += alpha p);  dst -= alpha*s2 (r -= alpha ap)
+   PT_CG_P,         // dst = s0 + beta*dst (p = r + beta p)
+   PT_SYNC,         // write-through of owners only
+};
+
+struct PointArgs {
+   int         op;
+   uint32_t    flag;
+   int         nsrc;
+   const void* s0;
+   const void* s1;
+   const void* s2;
+   void*       dst;
+   double      a0, a1, a2;
+   const double* dev_scalars;  // CG state (alpha at [4], beta at [5], done at [6])
+};
+
+void launch_point( Context* ctx, Mesh* m, int L, int dtype, const PointArgs& a );
+void launch_flat_lincomb( Context* ctx, int64_t count, int dtype, void* dst, int nsrc, const void* const* srcs, const double* scal );
+void launch_convert( Context* ctx, int64_t count, int dst_dtype, void* dst, int src_dtype, const void* src );
+// deterministic dot over owned flagged DoFs -> *out (device)
+void launch_dot( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const void* a, const void* b, double* out );
+void launch_restrict( Context* ctx, Mesh* m, int Lfine, int dtype, uint32_t flag, const void* fine, void* coarse );
+void launch_prolongate( Context* ctx, Mesh* m, int Lcoarse, int dtype, uint32_t flag, const void* coarse, void* fine, int add );
+void launch_cg_scalar( Context* ctx, double* state, int stage, double rtol, double atol );
+
+// host helpers
+void check_cuda( cudaError_t e, const char* what );
+void build_level( Mesh* m, int L );
+void ensure_device( Mesh* m, P1Level& P );
+void build_operator_level( Operator* A, int L );
+void ensure_device_op( OpLevel& ol );
+
+}  // namespace hyb

@@ -1,0 +1,831 @@
+// CUDA kernels of the P1 vertex-DoF multigrid path (sm_100a).
+//
+// Two kernel families cover every operation:
+//  * cell kernels: one warp per interior row (y, z) of a macro-cell, lanes over x.  The 15-point
+//    stencil reads only the cell's own array, whose boundary slabs hold up-to-date copies of the
+//    face/edge/vertex owners (write-through invariant).
+//  * boundary kernels: one thread per owned DoF of a macro-face/edge/vertex.  The stencil is the
+//    sum over the neighbouring macro-cells of the cell-restricted stencil of the point's position
+//    class, read from each cell's array (the same decomposition as
+//    P1ConstantOperator::apply_face3D_generated, P1ConstantOperator.cpp:239-357, which sums the
+//    one-sided stencil of every neighbour cell).  The result is written to the owner and to every
+//    copy in the neighbouring cell arrays.
+// The path is bandwidth bound: no tensor cores, fp64 accumulation for fp64 storage and fp32
+// accumulation for fp32/fp16 storage.
+#include "hyb_internal.hpp"
+
+#include <cstdio>
+#include <stdexcept>
+
+namespace hyb {
+
+__constant__ int      c_dirs[kNumDirs][3];
+__constant__ uint16_t c_cls_mask[kNumClasses];
+__constant__ int8_t   c_mask_to_cls[16];
+
+static bool g_const_ready = false;
+static void ensure_constants()
+{
+   if ( g_const_ready ) return;
+   check_cuda( cudaMemcpyToSymbol( c_dirs, kDirs, sizeof( kDirs ) ), "constants(dirs)" );
+   check_cuda( cudaMemcpyToSymbol( c_cls_mask, kClassDirMask, sizeof( kClassDirMask ) ), "constants(mask)" );
+   int8_t m2c[16];
+   for ( int m = 0; m < 16; ++m ) m2c[m] = -1;
+   // z==0 -> bit0, y==0 -> bit1, x==0 -> bit2, x+y+z==n -> bit3
+   const int faces[kNumClasses] = { 0, 1, 2, 4, 8, 3, 5, 9, 6, 10, 12, 7, 11, 13, 14 };
+   for ( int c = 0; c < kNumClasses; ++c ) m2c[faces[c]] = int8_t( c );
+   check_cuda( cudaMemcpyToSymbol( c_mask_to_cls, m2c, sizeof( m2c ) ), "constants(classes)" );
+   g_const_ready = true;
+}
+
+template < typename T >
+struct AccT
+{
+   using type = float;
+};
+template <>
+struct AccT< double >
+{
+   using type = double;
+};
+
+__device__ __forceinline__ double ldv( const double* p ) { return __ldg( p ); }
+__device__ __forceinline__ float  ldv( const float* p ) { return __ldg( p ); }
+__device__ __forceinline__ float  ldv( const __half* p ) { return __half2float( __ldg( p ) ); }
+// plain (coherent) loads for vectors that are also written by the same kernel
+__device__ __forceinline__ double ldc( const double* p ) { return *p; }
+__device__ __forceinline__ float  ldc( const float* p ) { return *p; }
+__device__ __forceinline__ float  ldc( const __half* p ) { return __half2float( *p ); }
+__device__ __forceinline__ void   stv( double* p, double v ) { *p = v; }
+__device__ __forceinline__ void   stv( float* p, float v ) { *p = v; }
+__device__ __forceinline__ void   stv( __half* p, float v ) { *p = __float2half_rn( v ); }
+
+__device__ __forceinline__ int point_class( int n, int x, int y, int z )
+{
+   const int m = ( z == 0 ) | ( ( y == 0 ) << 1 ) | ( ( x == 0 ) << 2 ) | ( ( x + y + z == n ) << 3 );
+   return c_mask_to_cls[m];
+}
+
+// ---------------------------------------------------------------------------------------------
+// argument blocks
+// ---------------------------------------------------------------------------------------------
+struct LevelView
+{
+   int              n;
+   int              nrows;
+   const int2*      rows;
+   int              ntasks;
+   const int4*      tasks;
+   const int64_t*   off;       // all primitives
+   const int64_t*   cell_off;  // off + nB
+   const int*       inc_begin;
+   const Incidence* inc;
+   const uint8_t*   bc;       // all primitives
+   const uint8_t*   cell_bc;  // bc + nB
+   const int8_t*    bkind;
+   const float*     ncell_cls;
+};
+
+template < typename A >
+struct OpView
+{
+   const A* W;       // [nC][15][15]
+   const A* invd_b;  // per boundary primitive
+   const A* invd_c;  // per cell
+};
+
+static LevelView make_view( Mesh* m, int L )
+{
+   P1Level& P = m->level( L );
+   ensure_device( m, P );
+   LevelView v;
+   v.n         = P.n;
+   v.nrows     = int( P.rows.size() );
+   v.rows      = P.d_rows;
+   v.ntasks    = int( P.tasks.size() );
+   v.tasks     = P.d_tasks;
+   v.off       = P.d_off;
+   v.cell_off  = P.d_off + P.nB;
+   v.inc_begin = P.d_inc_begin;
+   v.inc       = P.d_inc;
+   v.bc        = P.d_bc;
+   v.cell_bc   = P.d_bc + P.nB;
+   v.bkind     = P.d_bkind;
+   v.ncell_cls = P.d_ncell_cls;
+   return v;
+}
+
+__device__ __forceinline__ int64_t owner_slot( const LevelView& v, int b, int i, int j )
+{
+   const int k = v.bkind[b];
+   return v.off[b] + ( k == 0 ? 0 : ( k == 1 ? int64_t( i ) : fidx( v.n, i, j ) ) );
+}
+
+__device__ __forceinline__ void inc_point( const Incidence& I, int n, int i, int j, int& x, int& y, int& z )
+{
+   x = n * I.o[0] + i * I.e1[0] + j * I.e2[0];
+   y = n * I.o[1] + i * I.e1[1] + j * I.e2[1];
+   z = n * I.o[2] + i * I.e1[2] + j * I.e2[2];
+}
+
+// store val to the owner slot and every copy in the neighbouring cell arrays
+template < typename T, typename A >
+__device__ __forceinline__ void write_through( const LevelView& v, T* vec, int b, int i, int j, int64_t owner, A val )
+{
+   stv( vec + owner, val );
+   for ( int q = v.inc_begin[b]; q < v.inc_begin[b + 1]; ++q )
+   {
+      const Incidence I = v.inc[q];
+      int             x, y, z;
+      inc_point( I, v.n, i, j, x, y, z );
+      stv( vec + v.cell_off[I.cell] + cidx( v.n, x, y, z ), val );
+   }
+}
+
+// ---------------------------------------------------------------------------------------------
+// stencil sweeps
+// ---------------------------------------------------------------------------------------------
+template < typename T, typename A, int OP >
+__device__ __forceinline__ void stencil_epilogue( int64_t i, A s, A invd, const T* src, const T* v1, T* v2, T* dst, A a0, A a1 )
+{
+   if constexpr ( OP == OP_APPLY ) stv( dst + i, s );
+   else if constexpr ( OP == OP_APPLY_ADD ) stv( dst + i, A( ldc( dst + i ) ) + s );
+   else if constexpr ( OP == OP_RESID ) stv( dst + i, A( ldv( v1 + i ) ) - s );
+   else if constexpr ( OP == OP_JAC ) stv( dst + i, A( ldv( src + i ) ) + a0 * ( invd * ( A( ldv( v1 + i ) ) - s ) ) );
+   else if constexpr ( OP == OP_CHEB0 ) stv( dst + i, invd * ( A( ldv( v1 + i ) ) - s ) );
+   else if constexpr ( OP == OP_CHEBI )
+   {
+      stv( dst + i, invd * s );
+      stv( v2 + i, A( ldc( v2 + i ) ) + a0 * A( ldv( src + i ) ) );
+   }
+   else if constexpr ( OP == OP_CHEBL ) stv( v2 + i, ( A( ldc( v2 + i ) ) + a0 * A( ldv( src + i ) ) ) + a1 * ( invd * s ) );
+   else if constexpr ( OP == OP_DINV_APPLY ) stv( dst + i, invd * s );
+}
+
+template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( 256 ) k_cell_stencil( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
+                                                          const T* __restrict__ v1, T* v2, T* dst, A a0, A a1 )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int r    = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   if ( r >= v.nrows ) return;
+   if ( !( v.cell_bc[c] & flag ) ) return;
+   const int2    yz   = v.rows[r];
+   const int     y = yz.x, z = yz.y, n = v.n;
+   const int64_t base = v.cell_off[c];
+   const T*      s    = src + base;
+   const int64_t r00 = cidx( n, 0, y, z ), rm0 = cidx( n, 0, y - 1, z ), rp0 = cidx( n, 0, y + 1, z );
+   const int64_t r0m = cidx( n, 0, y, z - 1 ), r0p = cidx( n, 0, y, z + 1 );
+   const int64_t rmp = cidx( n, 0, y - 1, z + 1 ), rpm = cidx( n, 0, y + 1, z - 1 );
+   const A*      W   = o.W + size_t( c ) * kNumClasses * kNumDirs;  // interior class 0
+   const A w0 = W[0], wW = W[1], wE = W[2], wS = W[3], wN = W[4], wB = W[5], wT = W[6], wNW = W[7], wSE = W[8], wTW = W[9],
+           wBE = W[10], wTS = W[11], wBN = W[12], wTSE = W[13], wBNW = W[14];
+   const A   invd = o.invd_c[c];
+   const int xmax = n - 1 - y - z;
+   for ( int x = 1 + lane; x <= xmax; x += 32 )
+   {
+      A acc = w0 * A( ldv( s + r00 + x ) );
+      acc += wW * A( ldv( s + r00 + x - 1 ) );
+      acc += wE * A( ldv( s + r00 + x + 1 ) );
+      acc += wS * A( ldv( s + rm0 + x ) );
+      acc += wN * A( ldv( s + rp0 + x ) );
+      acc += wB * A( ldv( s + r0m + x ) );
+      acc += wT * A( ldv( s + r0p + x ) );
+      acc += wNW * A( ldv( s + rp0 + x - 1 ) );
+      acc += wSE * A( ldv( s + rm0 + x + 1 ) );
+      acc += wTW * A( ldv( s + r0p + x - 1 ) );
+      acc += wBE * A( ldv( s + r0m + x + 1 ) );
+      acc += wTS * A( ldv( s + rmp + x ) );
+      acc += wBN * A( ldv( s + rpm + x ) );
+      acc += wTSE * A( ldv( s + rmp + x + 1 ) );
+      acc += wBNW * A( ldv( s + rpm + x - 1 ) );
+      stencil_epilogue< T, A, OP >( base + r00 + x, acc, invd, src, v1, v2, dst, a0, a1 );
+   }
+}
+
+template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( 256 ) k_bnd_stencil( LevelView v, OpView< A > o, uint32_t flag, int copy_unflagged,
+                                                         const T* __restrict__ src, const T* __restrict__ v1, T* v2, T* dst,
+                                                         A a0, A a1 )
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( t >= v.ntasks ) return;
+   const int4    tk    = v.tasks[t];
+   const int     b     = tk.x, i = tk.y, j = tk.z, n = v.n;
+   const int64_t owner = owner_slot( v, b, i, j );
+   if ( !( v.bc[b] & flag ) )
+   {
+      if ( !copy_unflagged ) return;
+      if constexpr ( OP == OP_JAC || OP == OP_CHEB0 ) write_through( v, dst, b, i, j, owner, A( ldv( src + owner ) ) );
+      else if constexpr ( OP == OP_CHEBI ) write_through( v, dst, b, i, j, owner, A( ldc( v2 + owner ) ) );
+      return;
+   }
+   A acc = A( 0 );
+   for ( int q = v.inc_begin[b]; q < v.inc_begin[b + 1]; ++q )
+   {
+      const Incidence I = v.inc[q];
+      int             x, y, z;
+      inc_point( I, n, i, j, x, y, z );
+      const T*       s    = src + v.cell_off[I.cell];
+      const A*       W    = o.W + ( size_t( I.cell ) * kNumClasses + I.cls ) * kNumDirs;
+      const uint16_t mask = c_cls_mask[I.cls];
+      A              part = A( 0 );
+      for ( int d = 0; d < kNumDirs; ++d )
+         if ( mask & ( 1u << d ) )
+            part += W[d] * A( ldv( s + cidx( n, x + c_dirs[d][0], y + c_dirs[d][1], z + c_dirs[d][2] ) ) );
+      acc += part;
+   }
+   const A invd = o.invd_b[b];
+   if constexpr ( OP == OP_APPLY ) write_through( v, dst, b, i, j, owner, acc );
+   else if constexpr ( OP == OP_APPLY_ADD ) write_through( v, dst, b, i, j, owner, A( ldc( dst + owner ) ) + acc );
+   else if constexpr ( OP == OP_RESID ) write_through( v, dst, b, i, j, owner, A( ldv( v1 + owner ) ) - acc );
+   else if constexpr ( OP == OP_JAC )
+      write_through( v, dst, b, i, j, owner, A( ldv( src + owner ) ) + a0 * ( invd * ( A( ldv( v1 + owner ) ) - acc ) ) );
+   else if constexpr ( OP == OP_CHEB0 ) write_through( v, dst, b, i, j, owner, invd * ( A( ldv( v1 + owner ) ) - acc ) );
+   else if constexpr ( OP == OP_CHEBI )
+   {
+      write_through( v, dst, b, i, j, owner, invd * acc );
+      write_through( v, v2, b, i, j, owner, A( ldc( v2 + owner ) ) + a0 * A( ldv( src + owner ) ) );
+   }
+   else if constexpr ( OP == OP_CHEBL )
+      write_through( v, v2, b, i, j, owner, ( A( ldc( v2 + owner ) ) + a0 * A( ldv( src + owner ) ) ) + a1 * ( invd * acc ) );
+   else if constexpr ( OP == OP_DINV_APPLY ) write_through( v, dst, b, i, j, owner, invd * acc );
+}
+
+template < typename T, typename A, int OP >
+static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o, int nC, const StencilArgs& a )
+{
+   const T* src = (const T*) a.src;
+   const T* v1  = (const T*) a.v1;
+   T*       v2  = (T*) a.v2;
+   T*       dst = (T*) a.dst;
+   if ( v.nrows > 0 && nC > 0 )
+   {
+      dim3 grid( ( v.nrows + 7 ) / 8, nC );
+      k_cell_stencil< T, A, OP ><<< grid, 256, 0, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ) );
+      ++ctx->launches;
+   }
+   if ( v.ntasks > 0 )
+   {
+      k_bnd_stencil< T, A, OP ><<< ( v.ntasks + 255 ) / 256, 256, 0, ctx->stream >>>( v, o, a.flag, a.copy_unflagged, src, v1, v2,
+                                                                                       dst, A( a.a0 ), A( a.a1 ) );
+      ++ctx->launches;
+   }
+   check_cuda( cudaGetLastError(), "stencil launch" );
+}
+
+template < typename T, typename A >
+static void dispatch_stencil( Context* ctx, const LevelView& v, const OpView< A >& o, int nC, const StencilArgs& a )
+{
+   switch ( a.op )
+   {
+   case OP_APPLY: run_stencil< T, A, OP_APPLY >( ctx, v, o, nC, a ); break;
+   case OP_APPLY_ADD: run_stencil< T, A, OP_APPLY_ADD >( ctx, v, o, nC, a ); break;
+   case OP_RESID: run_stencil< T, A, OP_RESID >( ctx, v, o, nC, a ); break;
+   case OP_JAC: run_stencil< T, A, OP_JAC >( ctx, v, o, nC, a ); break;
+   case OP_CHEB0: run_stencil< T, A, OP_CHEB0 >( ctx, v, o, nC, a ); break;
+   case OP_CHEBI: run_stencil< T, A, OP_CHEBI >( ctx, v, o, nC, a ); break;
+   case OP_CHEBL: run_stencil< T, A, OP_CHEBL >( ctx, v, o, nC, a ); break;
+   case OP_DINV_APPLY: run_stencil< T, A, OP_DINV_APPLY >( ctx, v, o, nC, a ); break;
+   default: throw std::invalid_argument( "unknown stencil op" );
+   }
+}
+
+void launch_stencil( Context* ctx, Mesh* m, Operator* Op, int L, int dtype, const StencilArgs& a )
+{
+   ensure_constants();
+   LevelView v  = make_view( m, L );
+   OpLevel&  ol = Op->lv.at( L );
+   ensure_device_op( ol );
+   const int nC = m->topo.nC;
+   if ( dtype == F64 )
+      dispatch_stencil< double, double >( ctx, v, OpView< double >{ ol.d_W, ol.d_invd_b, ol.d_invd_c }, nC, a );
+   else if ( dtype == F32 )
+      dispatch_stencil< float, float >( ctx, v, OpView< float >{ ol.d_Wf, ol.d_invd_bf, ol.d_invd_cf }, nC, a );
+   else
+      dispatch_stencil< __half, float >( ctx, v, OpView< float >{ ol.d_Wf, ol.d_invd_bf, ol.d_invd_cf }, nC, a );
+}
+
+// ---------------------------------------------------------------------------------------------
+// pointwise operations on owned DoFs
+// ---------------------------------------------------------------------------------------------
+template < typename T, typename A, int OP >
+__device__ __forceinline__ A point_value( int64_t i, int nsrc, const T* s0, const T* s1, const T* s2, const T* dst, A a0, A a1, A a2 )
+{
+   if constexpr ( OP == PT_LINCOMB || OP == PT_ADD )
+   {
+      A r = a0 * A( ldc( s0 + i ) );
+      if ( nsrc > 1 ) r += a1 * A( ldc( s1 + i ) );
+      if ( nsrc > 2 ) r += a2 * A( ldc( s2 + i ) );
+      if constexpr ( OP == PT_ADD ) r = A( ldc( dst + i ) ) + r;
+      return r;
+   }
+   else if constexpr ( OP == PT_MULT ) return A( ldc( s0 + i ) ) * A( ldc( s1 + i ) );
+   else if constexpr ( OP == PT_INVERT ) return A( 1 ) / A( ldc( s0 + i ) );
+   else if constexpr ( OP == PT_SET ) return a0;
+   else if constexpr ( OP == PT_SYNC ) return A( ldc( dst + i ) );
+   return A( 0 );
+}
+
+template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( 256 ) k_cell_point( LevelView v, uint32_t flag, int nsrc, const T* s0, const T* s1, const T* s2,
+                                                        T* dst, A a0, A a1, A a2, const double* sc )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int r    = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   if ( r >= v.nrows ) return;
+   if ( !( v.cell_bc[c] & flag ) ) return;
+   if constexpr ( OP == PT_CG_XR || OP == PT_CG_P )
+      if ( sc[6] != 0.0 ) return;
+   const int2    yz   = v.rows[r];
+   const int64_t base = v.cell_off[c] + cidx( v.n, 0, yz.x, yz.y );
+   const int     xmax = v.n - 1 - yz.x - yz.y;
+   for ( int x = 1 + lane; x <= xmax; x += 32 )
+   {
+      const int64_t i = base + x;
+      if constexpr ( OP == PT_CG_XR )
+      {
+         const double alpha = sc[4];
+         stv( (T*) s0 + i, A( ldc( s0 + i ) ) + A( alpha ) * A( ldc( s1 + i ) ) );
+         stv( dst + i, A( ldc( dst + i ) ) - A( alpha ) * A( ldc( s2 + i ) ) );
+      }
+      else if constexpr ( OP == PT_CG_P )
+      {
+         const double beta = sc[5];
+         stv( dst + i, A( ldc( s0 + i ) ) + A( beta ) * A( ldc( dst + i ) ) );
+      }
+      else
+         stv( dst + i, point_value< T, A, OP >( i, nsrc, s0, s1, s2, dst, a0, a1, a2 ) );
+   }
+}
+
+template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( 256 ) k_bnd_point( LevelView v, uint32_t flag, int nsrc, const T* s0, const T* s1, const T* s2,
+                                                       T* dst, A a0, A a1, A a2, const double* sc )
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( t >= v.ntasks ) return;
+   const int4 tk = v.tasks[t];
+   const int  b = tk.x, i = tk.y, j = tk.z;
+   if ( !( v.bc[b] & flag ) ) return;
+   if constexpr ( OP == PT_CG_XR || OP == PT_CG_P )
+      if ( sc[6] != 0.0 ) return;
+   const int64_t owner = owner_slot( v, b, i, j );
+   if constexpr ( OP == PT_CG_XR )
+   {
+      const double alpha = sc[4];
+      write_through( v, (T*) s0, b, i, j, owner, A( ldc( s0 + owner ) ) + A( alpha ) * A( ldc( s1 + owner ) ) );
+      write_through( v, dst, b, i, j, owner, A( ldc( dst + owner ) ) - A( alpha ) * A( ldc( s2 + owner ) ) );
+   }
+   else if constexpr ( OP == PT_CG_P )
+   {
+      const double beta = sc[5];
+      write_through( v, dst, b, i, j, owner, A( ldc( s0 + owner ) ) + A( beta ) * A( ldc( dst + owner ) ) );
+   }
+   else
+      write_through( v, dst, b, i, j, owner, point_value< T, A, OP >( owner, nsrc, s0, s1, s2, dst, a0, a1, a2 ) );
+}
+
+template < typename T, typename A, int OP >
+static void run_point( Context* ctx, const LevelView& v, int nC, const PointArgs& a )
+{
+   if ( v.nrows > 0 && nC > 0 && OP != PT_SYNC )
+   {
+      dim3 grid( ( v.nrows + 7 ) / 8, nC );
+      k_cell_point< T, A, OP ><<< grid, 256, 0, ctx->stream >>>( v, a.flag, a.nsrc, (const T*) a.s0, (const T*) a.s1,
+                                                                 (const T*) a.s2, (T*) a.dst, A( a.a0 ), A( a.a1 ), A( a.a2 ),
+                                                                 a.dev_scalars );
+      ++ctx->launches;
+   }
+   if ( v.ntasks > 0 )
+   {
+      k_bnd_point< T, A, OP ><<< ( v.ntasks + 255 ) / 256, 256, 0, ctx->stream >>>(
+          v, a.flag, a.nsrc, (const T*) a.s0, (const T*) a.s1, (const T*) a.s2, (T*) a.dst, A( a.a0 ), A( a.a1 ), A( a.a2 ),
+          a.dev_scalars );
+      ++ctx->launches;
+   }
+   check_cuda( cudaGetLastError(), "pointwise launch" );
+}
+
+template < typename T, typename A >
+static void dispatch_point( Context* ctx, const LevelView& v, int nC, const PointArgs& a )
+{
+   switch ( a.op )
+   {
+   case PT_LINCOMB: run_point< T, A, PT_LINCOMB >( ctx, v, nC, a ); break;
+   case PT_ADD: run_point< T, A, PT_ADD >( ctx, v, nC, a ); break;
+   case PT_MULT: run_point< T, A, PT_MULT >( ctx, v, nC, a ); break;
+   case PT_INVERT: run_point< T, A, PT_INVERT >( ctx, v, nC, a ); break;
+   case PT_SET: run_point< T, A, PT_SET >( ctx, v, nC, a ); break;
+   case PT_CG_XR: run_point< T, A, PT_CG_XR >( ctx, v, nC, a ); break;
+   case PT_CG_P: run_point< T, A, PT_CG_P >( ctx, v, nC, a ); break;
+   case PT_SYNC: run_point< T, A, PT_SYNC >( ctx, v, nC, a ); break;
+   default: throw std::invalid_argument( "unknown pointwise op" );
+   }
+}
+
+void launch_point( Context* ctx, Mesh* m, int L, int dtype, const PointArgs& a )
+{
+   ensure_constants();
+   LevelView v  = make_view( m, L );
+   const int nC = m->topo.nC;
+   if ( dtype == F64 ) dispatch_point< double, double >( ctx, v, nC, a );
+   else if ( dtype == F32 ) dispatch_point< float, float >( ctx, v, nC, a );
+   else dispatch_point< __half, float >( ctx, v, nC, a );
+}
+
+// whole-buffer linear combination (flag All): every slot, copies included, stays consistent
+template < typename T, typename A >
+__global__ void k_flat_lincomb( int64_t count, T* dst, int nsrc, const T* s0, const T* s1, const T* s2, A a0, A a1, A a2 )
+{
+   for ( int64_t i = blockIdx.x * int64_t( blockDim.x ) + threadIdx.x; i < count; i += int64_t( gridDim.x ) * blockDim.x )
+   {
+      A r = nsrc > 0 ? a0 * A( ldc( s0 + i ) ) : a0;
+      if ( nsrc > 1 ) r += a1 * A( ldc( s1 + i ) );
+      if ( nsrc > 2 ) r += a2 * A( ldc( s2 + i ) );
+      stv( dst + i, r );
+   }
+}
+
+void launch_flat_lincomb( Context* ctx, int64_t count, int dtype, void* dst, int nsrc, const void* const* srcs, const double* scal )
+{
+   if ( count <= 0 ) return;
+   const int blocks = int( std::min< int64_t >( ( count + 255 ) / 256, 148 * 16 ) );
+   const void* s0 = nsrc > 0 ? srcs[0] : nullptr;
+   const void* s1 = nsrc > 1 ? srcs[1] : nullptr;
+   const void* s2 = nsrc > 2 ? srcs[2] : nullptr;
+   if ( dtype == F64 )
+      k_flat_lincomb< double, double ><<< blocks, 256, 0, ctx->stream >>>( count, (double*) dst, nsrc, (const double*) s0,
+                                                                          (const double*) s1, (const double*) s2, scal[0],
+                                                                          scal[1], scal[2] );
+   else if ( dtype == F32 )
+      k_flat_lincomb< float, float ><<< blocks, 256, 0, ctx->stream >>>( count, (float*) dst, nsrc, (const float*) s0,
+                                                                        (const float*) s1, (const float*) s2, float( scal[0] ),
+                                                                        float( scal[1] ), float( scal[2] ) );
+   else
+      k_flat_lincomb< __half, float ><<< blocks, 256, 0, ctx->stream >>>( count, (__half*) dst, nsrc, (const __half*) s0,
+                                                                         (const __half*) s1, (const __half*) s2, float( scal[0] ),
+                                                                         float( scal[1] ), float( scal[2] ) );
+   ++ctx->launches;
+   check_cuda( cudaGetLastError(), "flat lincomb launch" );
+}
+
+template < typename TD, typename TS >
+__global__ void k_convert( int64_t count, TD* dst, const TS* src )
+{
+   for ( int64_t i = blockIdx.x * int64_t( blockDim.x ) + threadIdx.x; i < count; i += int64_t( gridDim.x ) * blockDim.x )
+   {
+      if constexpr ( std::is_same< TD, __half >::value ) dst[i] = __float2half_rn( float( ldc( src + i ) ) );
+      else dst[i] = TD( ldc( src + i ) );
+   }
+}
+
+void launch_convert( Context* ctx, int64_t count, int dd, void* dst, int sd, const void* src )
+{
+   if ( count <= 0 ) return;
+   const int blocks = int( std::min< int64_t >( ( count + 255 ) / 256, 148 * 16 ) );
+#define HYB_CONV( TD, TS ) k_convert< TD, TS ><<< blocks, 256, 0, ctx->stream >>>( count, (TD*) dst, (const TS*) src )
+   if ( dd == F64 && sd == F64 ) HYB_CONV( double, double );
+   else if ( dd == F64 && sd == F32 ) HYB_CONV( double, float );
+   else if ( dd == F64 && sd == F16 ) HYB_CONV( double, __half );
+   else if ( dd == F32 && sd == F64 ) HYB_CONV( float, double );
+   else if ( dd == F32 && sd == F32 ) HYB_CONV( float, float );
+   else if ( dd == F32 && sd == F16 ) HYB_CONV( float, __half );
+   else if ( dd == F16 && sd == F64 ) HYB_CONV( __half, double );
+   else if ( dd == F16 && sd == F32 ) HYB_CONV( __half, float );
+   else HYB_CONV( __half, __half );
+#undef HYB_CONV
+   ++ctx->launches;
+   check_cuda( cudaGetLastError(), "convert launch" );
+}
+
+// ---------------------------------------------------------------------------------------------
+// deterministic dot product over owned flagged DoFs
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ double block_sum( double v )
+{
+   __shared__ double sh[32];
+   for ( int o = 16; o > 0; o >>= 1 ) v += __shfl_down_sync( 0xffffffffu, v, o );
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   if ( lane == 0 ) sh[warp] = v;
+   __syncthreads();
+   const int nw = ( blockDim.x + 31 ) >> 5;
+   v            = ( threadIdx.x < nw ) ? sh[threadIdx.x] : 0.0;
+   if ( warp == 0 )
+      for ( int o = 16; o > 0; o >>= 1 ) v += __shfl_down_sync( 0xffffffffu, v, o );
+   return v;
+}
+
+template < typename T >
+__global__ void __launch_bounds__( 256 ) k_dot_cells( LevelView v, uint32_t flag, const T* a, const T* b, double* partials )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int r    = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   double    acc  = 0.0;
+   if ( r < v.nrows && ( v.cell_bc[c] & flag ) )
+   {
+      const int2    yz   = v.rows[r];
+      const int64_t base = v.cell_off[c] + cidx( v.n, 0, yz.x, yz.y );
+      const int     xmax = v.n - 1 - yz.x - yz.y;
+      for ( int x = 1 + lane; x <= xmax; x += 32 ) acc += double( ldv( a + base + x ) ) * double( ldv( b + base + x ) );
+   }
+   acc = block_sum( acc );
+   if ( threadIdx.x == 0 ) partials[size_t( blockIdx.y ) * gridDim.x + blockIdx.x] = acc;
+}
+
+template < typename T >
+__global__ void __launch_bounds__( 256 ) k_dot_bnd( LevelView v, uint32_t flag, const T* a, const T* b, double* partials )
+{
+   const int t   = blockIdx.x * blockDim.x + threadIdx.x;
+   double    acc = 0.0;
+   if ( t < v.ntasks )
+   {
+      const int4 tk = v.tasks[t];
+      if ( v.bc[tk.x] & flag )
+      {
+         const int64_t o = owner_slot( v, tk.x, tk.y, tk.z );
+         acc             = double( ldv( a + o ) ) * double( ldv( b + o ) );
+      }
+   }
+   acc = block_sum( acc );
+   if ( threadIdx.x == 0 ) partials[blockIdx.x] = acc;
+}
+
+__global__ void __launch_bounds__( 1024 ) k_sum_partials( const double* partials, int count, double* out )
+{
+   double acc = 0.0;
+   for ( int i = threadIdx.x; i < count; i += blockDim.x ) acc += partials[i];
+   acc = block_sum( acc );
+   if ( threadIdx.x == 0 ) *out = acc;
+}
+
+static double* partials( Context* ctx, int count )
+{
+   if ( count > ctx->partial_cap )
+   {
+      if ( ctx->d_partials ) check_cuda( cudaFree( ctx->d_partials ), "cudaFree(partials)" );
+      ctx->partial_cap = std::max( count, 1 << 16 );
+      check_cuda( cudaMalloc( &ctx->d_partials, sizeof( double ) * ctx->partial_cap ), "cudaMalloc(partials)" );
+   }
+   return ctx->d_partials;
+}
+
+template < typename T >
+static void run_dot( Context* ctx, const LevelView& v, int nC, uint32_t flag, const void* a, const void* b, double* out )
+{
+   const int nb_cells = ( v.nrows > 0 && nC > 0 ) ? ( ( v.nrows + 7 ) / 8 ) * nC : 0;
+   const int nb_bnd   = v.ntasks > 0 ? ( v.ntasks + 255 ) / 256 : 0;
+   double*   p        = partials( ctx, nb_cells + nb_bnd + 1 );
+   if ( nb_cells )
+   {
+      dim3 grid( ( v.nrows + 7 ) / 8, nC );
+      k_dot_cells< T ><<< grid, 256, 0, ctx->stream >>>( v, flag, (const T*) a, (const T*) b, p );
+      ++ctx->launches;
+   }
+   if ( nb_bnd )
+   {
+      k_dot_bnd< T ><<< nb_bnd, 256, 0, ctx->stream >>>( v, flag, (const T*) a, (const T*) b, p + nb_cells );
+      ++ctx->launches;
+   }
+   k_sum_partials<<< 1, 1024, 0, ctx->stream >>>( p, nb_cells + nb_bnd, out );
+   ++ctx->launches;
+   check_cuda( cudaGetLastError(), "dot launch" );
+}
+
+void launch_dot( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const void* a, const void* b, double* out )
+{
+   ensure_constants();
+   LevelView v  = make_view( m, L );
+   const int nC = m->topo.nC;
+   if ( dtype == F64 ) run_dot< double >( ctx, v, nC, flag, a, b, out );
+   else if ( dtype == F32 ) run_dot< float >( ctx, v, nC, flag, a, b, out );
+   else run_dot< __half >( ctx, v, nC, flag, a, b, out );
+}
+
+// ---------------------------------------------------------------------------------------------
+// restriction (generated pull kernel semantics, R = P^T) and prolongation
+// ---------------------------------------------------------------------------------------------
+template < typename T, typename A >
+__global__ void __launch_bounds__( 256 ) k_restrict_cells( LevelView cv, LevelView fv, uint32_t flag, const T* __restrict__ fine,
+                                                            T* coarse )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int r    = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   if ( r >= cv.nrows ) return;
+   if ( !( cv.cell_bc[c] & flag ) ) return;
+   const int2    yz   = cv.rows[r];
+   const int     y = yz.x, z = yz.y, nf = fv.n;
+   const T*      f    = fine + fv.cell_off[c];
+   const int64_t cb   = cv.cell_off[c] + cidx( cv.n, 0, y, z );
+   const int     xmax = cv.n - 1 - y - z;
+   for ( int x = 1 + lane; x <= xmax; x += 32 )
+   {
+      const int X = 2 * x, Y = 2 * y, Z = 2 * z;
+      A         leaves = A( 0 );
+#pragma unroll
+      for ( int d = 1; d < kNumDirs; ++d )
+         leaves += A( ldv( f + cidx( nf, X + c_dirs[d][0], Y + c_dirs[d][1], Z + c_dirs[d][2] ) ) );
+      stv( coarse + cb + x, A( ldv( f + cidx( nf, X, Y, Z ) ) ) + A( 0.5 ) * leaves );
+   }
+}
+
+template < typename T, typename A >
+__global__ void __launch_bounds__( 256 ) k_restrict_bnd( LevelView cv, LevelView fv, uint32_t flag, const T* __restrict__ fine,
+                                                          T* coarse )
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( t >= cv.ntasks ) return;
+   const int4 tk = cv.tasks[t];
+   const int  b = tk.x, i = tk.y, j = tk.z;
+   if ( !( cv.bc[b] & flag ) ) return;
+   const int nf  = fv.n;
+   A         acc = A( 0 );
+   for ( int q = cv.inc_begin[b]; q < cv.inc_begin[b + 1]; ++q )
+   {
+      const Incidence I = cv.inc[q];
+      int             x, y, z;
+      inc_point( I, cv.n, i, j, x, y, z );
+      const int      X = 2 * x, Y = 2 * y, Z = 2 * z;
+      const T*       f    = fine + fv.cell_off[I.cell];
+      const float*   ncc  = fv.ncell_cls + size_t( I.cell ) * kNumClasses;
+      const uint16_t mask = c_cls_mask[I.cls];
+      A              part = A( ldv( f + cidx( nf, X, Y, Z ) ) ) / A( ncc[I.cls] );
+      for ( int d = 1; d < kNumDirs; ++d )
+         if ( mask & ( 1u << d ) )
+         {
+            const int px = X + c_dirs[d][0], py = Y + c_dirs[d][1], pz = Z + c_dirs[d][2];
+            part += A( 0.5 ) / A( ncc[point_class( nf, px, py, pz )] ) * A( ldv( f + cidx( nf, px, py, pz ) ) );
+         }
+      acc += part;
+   }
+   write_through( cv, coarse, b, i, j, owner_slot( cv, b, i, j ), acc );
+}
+
+// coarse micro-edge through an odd fine point: direction per odd-coordinate pattern
+__device__ __forceinline__ void parity_dir( int x, int y, int z, int& dx, int& dy, int& dz )
+{
+   const int p = ( x & 1 ) | ( ( y & 1 ) << 1 ) | ( ( z & 1 ) << 2 );
+   dx = dy = dz = 0;
+   switch ( p )
+   {
+   case 1: dx = 1; break;
+   case 2: dy = 1; break;
+   case 4: dz = 1; break;
+   case 3: dx = 1, dy = -1; break;
+   case 5: dx = 1, dz = -1; break;
+   case 6: dy = 1, dz = -1; break;
+   case 7: dx = 1, dy = -1, dz = 1; break;
+   default: break;
+   }
+}
+
+template < typename T, typename A >
+__device__ __forceinline__ A interp( const T* c, int nc, int x, int y, int z )
+{
+   int dx, dy, dz;
+   parity_dir( x, y, z, dx, dy, dz );
+   if ( ( dx | dy | dz ) == 0 ) return A( ldv( c + cidx( nc, x >> 1, y >> 1, z >> 1 ) ) );
+   const A a = A( ldv( c + cidx( nc, ( x - dx ) >> 1, ( y - dy ) >> 1, ( z - dz ) >> 1 ) ) );
+   const A b = A( ldv( c + cidx( nc, ( x + dx ) >> 1, ( y + dy ) >> 1, ( z + dz ) >> 1 ) ) );
+   return A( 0.5 ) * a + A( 0.5 ) * b;
+}
+
+template < typename T, typename A >
+__global__ void __launch_bounds__( 256 ) k_prolong_cells( LevelView cv, LevelView fv, uint32_t flag, const T* __restrict__ coarse,
+                                                           T* fine, int add )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int r    = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   if ( r >= fv.nrows ) return;
+   if ( !( fv.cell_bc[c] & flag ) ) return;
+   const int2    yz   = fv.rows[r];
+   const int     y = yz.x, z = yz.y;
+   const T*      cc   = coarse + cv.cell_off[c];
+   const int64_t fb   = fv.cell_off[c] + cidx( fv.n, 0, y, z );
+   const int     xmax = fv.n - 1 - y - z;
+   for ( int x = 1 + lane; x <= xmax; x += 32 )
+   {
+      const A val = interp< T, A >( cc, cv.n, x, y, z );
+      stv( fine + fb + x, add ? A( ldc( fine + fb + x ) ) + val : val );
+   }
+}
+
+template < typename T, typename A >
+__global__ void __launch_bounds__( 256 ) k_prolong_bnd( LevelView cv, LevelView fv, uint32_t flag, const T* __restrict__ coarse,
+                                                         T* fine, int add )
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( t >= fv.ntasks ) return;
+   const int4 tk = fv.tasks[t];
+   const int  b = tk.x, i = tk.y, j = tk.z;
+   if ( !( fv.bc[b] & flag ) ) return;
+   const Incidence I = fv.inc[fv.inc_begin[b]];
+   int             x, y, z;
+   inc_point( I, fv.n, i, j, x, y, z );
+   const A       val   = interp< T, A >( coarse + cv.cell_off[I.cell], cv.n, x, y, z );
+   const int64_t owner = owner_slot( fv, b, i, j );
+   write_through( fv, fine, b, i, j, owner, add ? A( ldc( fine + owner ) ) + val : val );
+}
+
+template < typename T, typename A >
+static void run_restrict( Context* ctx, const LevelView& cv, const LevelView& fv, int nC, uint32_t flag, const void* fine,
+                          void* coarse )
+{
+   if ( cv.nrows > 0 && nC > 0 )
+   {
+      dim3 grid( ( cv.nrows + 7 ) / 8, nC );
+      k_restrict_cells< T, A ><<< grid, 256, 0, ctx->stream >>>( cv, fv, flag, (const T*) fine, (T*) coarse );
+      ++ctx->launches;
+   }
+   if ( cv.ntasks > 0 )
+   {
+      k_restrict_bnd< T, A ><<< ( cv.ntasks + 255 ) / 256, 256, 0, ctx->stream >>>( cv, fv, flag, (const T*) fine, (T*) coarse );
+      ++ctx->launches;
+   }
+   check_cuda( cudaGetLastError(), "restrict launch" );
+}
+
+void launch_restrict( Context* ctx, Mesh* m, int Lf, int dtype, uint32_t flag, const void* fine, void* coarse )
+{
+   ensure_constants();
+   LevelView fv = make_view( m, Lf );
+   LevelView cv = make_view( m, Lf - 1 );
+   const int nC = m->topo.nC;
+   if ( dtype == F64 ) run_restrict< double, double >( ctx, cv, fv, nC, flag, fine, coarse );
+   else if ( dtype == F32 ) run_restrict< float, float >( ctx, cv, fv, nC, flag, fine, coarse );
+   else run_restrict< __half, float >( ctx, cv, fv, nC, flag, fine, coarse );
+}
+
+template < typename T, typename A >
+static void run_prolong( Context* ctx, const LevelView& cv, const LevelView& fv, int nC, uint32_t flag, const void* coarse,
+                         void* fine, int add )
+{
+   if ( fv.nrows > 0 && nC > 0 )
+   {
+      dim3 grid( ( fv.nrows + 7 ) / 8, nC );
+      k_prolong_cells< T, A ><<< grid, 256, 0, ctx->stream >>>( cv, fv, flag, (const T*) coarse, (T*) fine, add );
+      ++ctx->launches;
+   }
+   if ( fv.ntasks > 0 )
+   {
+      k_prolong_bnd< T, A ><<< ( fv.ntasks + 255 ) / 256, 256, 0, ctx->stream >>>( cv, fv, flag, (const T*) coarse, (T*) fine,
+                                                                                     add );
+      ++ctx->launches;
+   }
+   check_cuda( cudaGetLastError(), "prolongate launch" );
+}
+
+void launch_prolongate( Context* ctx, Mesh* m, int Lc, int dtype, uint32_t flag, const void* coarse, void* fine, int add )
+{
+   ensure_constants();
+   LevelView cv = make_view( m, Lc );
+   LevelView fv = make_view( m, Lc + 1 );
+   const int nC = m->topo.nC;
+   if ( dtype == F64 ) run_prolong< double, double >( ctx, cv, fv, nC, flag, coarse, fine, add );
+   else if ( dtype == F32 ) run_prolong< float, float >( ctx, cv, fv, nC, flag, coarse, fine, add );
+   else run_prolong< __half, float >( ctx, cv, fv, nC, flag, coarse, fine, add );
+}
+
+// ---------------------------------------------------------------------------------------------
+// CG scalars on the device (CGSolver.hpp:94-206 control flow without host round trips)
+// state: [0] prsold [1] res_start [2] pAp [3] rsnew [4] alpha [5] beta [6] done [7] iterations
+// ---------------------------------------------------------------------------------------------
+__global__ void k_cg_scalar( double* s, int stage, double rtol, double atol )
+{
+   if ( stage == 0 )
+   {
+      s[0] = s[3];
+      s[1] = sqrt( s[3] );
+      s[6] = ( s[1] < atol ) ? 1.0 : 0.0;
+      s[7] = 0.0;
+      s[4] = s[5] = 0.0;
+      return;
+   }
+   if ( s[6] != 0.0 ) return;
+   if ( stage == 1 ) { s[4] = s[0] / s[2]; }
+   else
+   {
+      const double sq = sqrt( s[3] );
+      s[7] += 1.0;
+      if ( sq / s[1] < rtol || sq < atol ) { s[6] = 1.0; }
+      else
+      {
+         s[5] = s[3] / s[0];
+         s[0] = s[3];
+      }
+   }
+}
+
+void launch_cg_scalar( Context* ctx, double* state, int stage, double rtol, double atol )
+{
+   k_cg_scalar<<< 1, 1, 0, ctx->stream >>>( state, stage, rtol, atol );
+   ++ctx->launches;
+   check_cuda( cudaGetLastError(), "cg scalar launch" );
+}
+
+}  // namespace hyb

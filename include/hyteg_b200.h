@@ -1,0 +1,209 @@
+/*
+ * hyteg_b200 — C ABI of the B200 matrix-free multigrid path for HyTeG-style hybrid
+ * tetrahedral grids.
+ *
+ * Every entry point returns an int status (HYB_OK on success) and never throws.  On failure
+ * hyb_last_error() returns a message for the calling thread.  All handles are opaque; every
+ * create has a matching destroy.  Device work is issued on the context's CUDA stream; entry
+ * points that return host values (dot products, residual histories, downloads) synchronise that
+ * stream, the others are asynchronous.
+ *
+ * The reference interface each group replaces is cited per declaration (paths relative to the
+ * hyteg source tree).
+ */
+#ifndef HYTEG_B200_H
+#define HYTEG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (reference: WALBERLA_ABORT / WALBERLA_CHECK abort the process, e.g.
+ * src/hyteg/operators/Operator.hpp:80; here they become return codes) */
+#define HYB_OK 0
+#define HYB_EINVAL 1
+#define HYB_ENOMEM 2
+#define HYB_EDEVICE 3
+#define HYB_ETIMEOUT 4
+#define HYB_EINTERNAL 5
+
+/* value types of function storage (FunctionMemory<ValueType>, src/hyteg/memory/FunctionMemory.hpp:47-130) */
+#define HYB_F64 0
+#define HYB_F32 1
+#define HYB_F16 2
+
+/* DoFType bits (src/hyteg/types/types.hpp:29-43) */
+#define HYB_INNER 1u
+#define HYB_DIRICHLET 2u
+#define HYB_NEUMANN 4u
+#define HYB_FREESLIP 8u
+#define HYB_ALL 15u
+
+/* UpdateType (src/hyteg/types/types.hpp:88-92) */
+#define HYB_REPLACE 0
+#define HYB_ADD 1
+
+/* operator kinds */
+#define HYB_P1_CONST_LAPLACE 1 /* P1ConstantLaplaceOperator, constant_stencil_operator/P1ConstantOperator.hpp:167 */
+#define HYB_P1_CONST_MASS 2    /* P1ConstantMassOperator, same file */
+
+/* smoother kinds */
+#define HYB_SMOOTHER_JACOBI 0    /* solvers/WeightedJacobiSmoother.hpp:46-66 */
+#define HYB_SMOOTHER_CHEBYSHEV 1 /* solvers/ChebyshevSmoother.hpp:112-240 */
+
+#define HYB_VCYCLE 0 /* CycleType::VCYCLE, solvers/GeometricMultigridSolver.hpp */
+#define HYB_WCYCLE 1
+
+typedef struct hyb_ctx  hyb_ctx;
+typedef struct hyb_mesh hyb_mesh;
+typedef struct hyb_fn   hyb_fn;
+typedef struct hyb_op   hyb_op;
+typedef struct hyb_gmg  hyb_gmg;
+
+/* ---------------------------------------------------------------- context and errors */
+const char* hyb_version( void );
+/* message of the last failed call on this thread */
+const char* hyb_last_error( void );
+/* device: CUDA ordinal; stream: a cudaStream_t to issue work on, or NULL for a private stream */
+int hyb_ctx_create( int device, void* stream, hyb_ctx** out );
+int hyb_ctx_destroy( hyb_ctx* ctx );
+int hyb_ctx_synchronize( hyb_ctx* ctx );
+/* number of kernels this library launched through ctx so far */
+int hyb_ctx_launch_count( const hyb_ctx* ctx, int64_t* out );
+/* the context's stream (cudaStream_t) */
+int hyb_ctx_stream( const hyb_ctx* ctx, void** stream );
+
+/* ---------------------------------------------------------------- macro mesh and primitive storage
+ * Replaces MeshInfo (src/hyteg/mesh/MeshInfo.hpp:221,512,562) + SetupPrimitiveStorage
+ * (src/hyteg/primitivestorage/SetupPrimitiveStorage.hpp:45) + PrimitiveStorage
+ * (src/hyteg/primitivestorage/PrimitiveStorage.hpp:116).  Primitive ids and local orientations
+ * follow the reference; boundary flags default to setMeshBoundaryFlagsOnBoundary(1, 0, true) and
+ * flag -> DoFType to BoundaryCondition::create0123BC (0 Inner, 1 Dirichlet, 2 Neumann, 3 Freeslip). */
+int hyb_mesh_create( hyb_ctx* ctx, int nverts, const double* coords /* 3*nverts */, int ntets, const int* tets /* 4*ntets */,
+                     hyb_mesh** out );
+/* MeshInfo::meshCuboid (src/hyteg/mesh/MeshGenCuboid.cpp:35-172) */
+int hyb_mesh_create_cuboid( hyb_ctx* ctx, const double* lo, const double* hi, int nx, int ny, int nz, hyb_mesh** out );
+/* MeshInfo::fromGmshFile, MSH 2.2 and 4.1 tetrahedral meshes (src/hyteg/mesh/GmshReaderForMSH22.hpp) */
+int hyb_mesh_create_gmsh( hyb_ctx* ctx, const char* path, hyb_mesh** out );
+int hyb_mesh_destroy( hyb_mesh* mesh );
+/* SetupPrimitiveStorage::setMeshBoundaryFlagsOnBoundary (SetupPrimitiveStorage.cpp:977-988) */
+int hyb_mesh_set_boundary_flags_on_boundary( hyb_mesh* mesh, int on_boundary, int inner );
+/* BoundaryCondition: DoFType of primitives carrying mesh boundary flag `flag` */
+int hyb_mesh_set_bc_type( hyb_mesh* mesh, int flag, uint32_t dof_type );
+/* counts[4] = macro vertices, edges, faces, cells */
+int hyb_mesh_counts( const hyb_mesh* mesh, int* counts );
+/* kind 0 vertex, 1 edge, 2 face, 3 cell: vertex ids of primitive `id` in its local order (-1 padded) */
+int hyb_mesh_primitive_vertices( const hyb_mesh* mesh, int kind, int id, int* out4 );
+/* mesh boundary flag of a primitive */
+int hyb_mesh_primitive_flag( const hyb_mesh* mesh, int kind, int id, int* flag );
+
+/* ---------------------------------------------------------------- vertex-DoF layout
+ * Packed HyTeG layout of one level: every primitive's FunctionMemory array
+ * (p1functionspace/VertexDoFMemory.hpp:39-60: vertex 1+nEdges, edge (n+1)+nFaces*n+nCells*(n-1),
+ * face tri(n+1)+nCells*tri(n), cell tet(n+1)) concatenated in id order vertices, edges, faces, cells. */
+int hyb_layout_packed_size( hyb_mesh* mesh, int level, int64_t* size );
+/* packed offsets and sizes of all primitives (nV+nE+nF+nC entries each; either may be NULL) */
+int hyb_layout_primitive_offsets( hyb_mesh* mesh, int level, int64_t* offsets, int64_t* sizes );
+/* linearMacroCellIndex / linearMacroFaceIndex (indexing/MacroCellIndexing.hpp:45-52, MacroFaceIndexing.hpp:45-50) */
+int64_t hyb_layout_cell_index( int level, int x, int y, int z );
+int64_t hyb_layout_face_index( int level, int i, int j );
+
+/* ---------------------------------------------------------------- functions
+ * P1Function<ValueType> (p1functionspace/P1Function.hpp, VertexDoFFunction.hpp). */
+int hyb_fn_create( hyb_ctx* ctx, hyb_mesh* mesh, int dtype, int min_level, int max_level, hyb_fn** out );
+int hyb_fn_destroy( hyb_fn* fn );
+/* host <-> device in the packed layout; host values are doubles.  Upload refreshes every copy of
+ * an owned DoF from its owner (communicate). */
+int hyb_fn_upload( hyb_fn* fn, int level, const double* host_packed );
+int hyb_fn_download( hyb_fn* fn, int level, double* host_packed );
+/* interpolate(constant, level, flag) (VertexDoFFunction.cpp:384) */
+int hyb_fn_interpolate_const( hyb_fn* fn, double value, int level, uint32_t flag );
+/* interpolate(std::function<real_t(const Point3D&)>, level, flag) (VertexDoFFunction.cpp:384-470) */
+int hyb_fn_interpolate_callback( hyb_fn* fn, double ( *f )( const double* xyz, void* user ), void* user, int level,
+                                 uint32_t flag );
+/* assign(scalars, functions, level, flag): dst = sum_k scalars[k] * srcs[k], n <= 3 (VertexDoFFunction.cpp:1131) */
+int hyb_fn_assign( hyb_fn* dst, int n, const double* scalars, hyb_fn* const* srcs, int level, uint32_t flag );
+/* add(scalars, functions, level, flag): dst += sum_k scalars[k] * srcs[k] (VertexDoFFunction.cpp:1224) */
+int hyb_fn_add( hyb_fn* dst, int n, const double* scalars, hyb_fn* const* srcs, int level, uint32_t flag );
+/* multElementwise({a, b}, level, flag) (VertexDoFFunction.cpp:1487) */
+int hyb_fn_mult_elementwise( hyb_fn* dst, hyb_fn* a, hyb_fn* b, int level, uint32_t flag );
+/* invertElementwise(level, flag) (VertexDoFFunction.cpp:1566) */
+int hyb_fn_invert_elementwise( hyb_fn* fn, int level, uint32_t flag );
+/* dotGlobal(other, level, flag) (VertexDoFFunction.cpp:1710-1790); deterministic */
+int hyb_fn_dot( hyb_fn* a, hyb_fn* b, int level, uint32_t flag, double* out );
+/* copyFrom between value types (VertexDoFFunction.hpp:150-151) */
+int hyb_fn_copy_from( hyb_fn* dst, hyb_fn* src, int level );
+/* swap(other, level) */
+int hyb_fn_swap( hyb_fn* a, hyb_fn* b, int level );
+/* device pointer and slot count of one level (padded device layout) */
+int hyb_fn_device_ptr( hyb_fn* fn, int level, void** ptr, int64_t* nslots );
+
+/* ---------------------------------------------------------------- operators
+ * Operator<Src,Dst>::apply(src, dst, level, flag, updateType) (operators/Operator.hpp:74-81),
+ * P1Operator::apply (p1functionspace/P1Operator.hpp:192-320). */
+int hyb_op_create( hyb_ctx* ctx, hyb_mesh* mesh, int kind, int min_level, int max_level, hyb_op** out );
+int hyb_op_destroy( hyb_op* op );
+int hyb_op_apply( hyb_op* op, hyb_fn* src, hyb_fn* dst, int level, uint32_t flag, int update );
+/* WeightedJacobiSmoothable::smooth_jac(dst, rhs, src, relax, level, flag) (solvers/Smoothables.hpp:33-40,
+ * P1Operator.hpp:429-447): dst = src + relax * D^-1 (rhs - A src) on flagged DoFs */
+int hyb_op_smooth_jac( hyb_op* op, hyb_fn* dst, hyb_fn* rhs, hyb_fn* src, double relax, int level, uint32_t flag );
+/* OperatorWithInverseDiagonal::getInverseDiagonalValues (solvers/Smoothables.hpp:109-119) written into out */
+int hyb_op_inverse_diagonal( hyb_op* op, hyb_fn* out, int level, uint32_t flag );
+/* stencil of cell `cell`, position class cls (0 interior, 1-4 faces, 5-10 edges, 11-14 vertices), 15 weights:
+ * centre, then directions W E S N B T NW SE TW BE TS BN TSE BNW (P1Elements.hpp:466-529) */
+int hyb_op_stencil( hyb_op* op, int level, int cell, int cls, double* out15 );
+
+/* ---------------------------------------------------------------- grid transfer
+ * P1toP1LinearRestriction::restrict (gridtransferoperators/P1toP1LinearRestriction.cpp:169-346) and
+ * P1toP1LinearProlongation::prolongate / prolongateAndAdd (P1toP1LinearProlongation.hpp:35-55). */
+int hyb_restrict( hyb_fn* fn, int source_level, uint32_t flag );
+int hyb_prolongate( hyb_fn* fn, int source_level, uint32_t flag, int update );
+
+/* ---------------------------------------------------------------- solvers */
+typedef struct hyb_gmg_params
+{
+   int    min_level, max_level;
+   int    pre_smooth, post_smooth, smooth_increment; /* GeometricMultigridSolver.hpp:61-75 */
+   int    cycle;                                     /* HYB_VCYCLE | HYB_WCYCLE */
+   int    smoother;                                  /* HYB_SMOOTHER_* */
+   double jacobi_relax;                              /* WeightedJacobiSmoother relax */
+   int    cheb_order;                                /* ChebyshevSmoother::setupCoefficients order */
+   double cheb_upper_factor, cheb_lower_factor;      /* 1.2, 0.3 */
+   int    cheb_power_iterations;                     /* chebyshev::estimateRadius iterations per level */
+   int    coarse_max_iter;                           /* CGSolver(maxIter, relTol, absTol), CGSolver.hpp:44-75 */
+   double coarse_rtol, coarse_atol;
+   int    use_graph;                                 /* capture each cycle in a CUDA graph */
+} hyb_gmg_params;
+
+int hyb_gmg_params_default( hyb_gmg_params* p );
+/* GeometricMultigridSolver (solvers/GeometricMultigridSolver.hpp:61-162) with its smoother and a CG
+ * coarse solver on the device.  For Chebyshev smoothing the spectral radius of D^-1 A is estimated per
+ * level by power iteration (chebyshev::estimateRadius, ChebyshevSmoother.hpp:656) from a seeded
+ * start vector unless set explicitly. */
+int hyb_gmg_create( hyb_ctx* ctx, hyb_op* op, const hyb_gmg_params* params, hyb_gmg** out );
+int hyb_gmg_destroy( hyb_gmg* gmg );
+/* per-level spectral radii (max_level-min_level+1 values); recomputes Chebyshev coefficients */
+int hyb_gmg_set_radii( hyb_gmg* gmg, const double* radii );
+int hyb_gmg_get_radii( hyb_gmg* gmg, double* radii );
+/* Solver::solve(A, x, b, level) (solvers/Solver.hpp:31-35): one multigrid cycle */
+int hyb_gmg_solve( hyb_gmg* gmg, hyb_fn* x, hyb_fn* b, int level );
+/* up to max_cycles cycles until ||r||/||r0|| < rtol (discrete L2 over non-Dirichlet DoFs);
+ * res_history receives ||r_0|| .. ||r_k|| (max_cycles+1 entries) */
+int hyb_gmg_solve_cycles( hyb_gmg* gmg, hyb_fn* x, hyb_fn* b, int level, int max_cycles, double rtol, double* res_history,
+                          int* cycles_done );
+/* chebyshev::estimateRadius (ChebyshevSmoother.hpp:656-676): power iteration on D^-1 A, flag All */
+int hyb_estimate_radius( hyb_op* op, hyb_fn* x, hyb_fn* tmp, int level, int iterations, double* radius );
+/* ChebyshevSmoother::setupCoefficientsInternal (ChebyshevSmoother.hpp:329-555) */
+int hyb_chebyshev_coefficients( int order, double lower, double upper, double* out );
+/* CGSolver::solve (solvers/CGSolver.hpp:94-206), identity preconditioner, flag Inner|Neumann|Freeslip */
+int hyb_cg_solve( hyb_op* op, hyb_fn* x, hyb_fn* b, int level, int max_iter, double rtol, double atol, int* iterations );
+/* discrete L2 norm of b - A x over the flagged DoFs */
+int hyb_residual_norm( hyb_op* op, hyb_fn* x, hyb_fn* b, hyb_fn* tmp, int level, uint32_t flag, double* out );
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HYTEG_B200_H */

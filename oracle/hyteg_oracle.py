@@ -1,0 +1,784 @@
+"""CPU oracle for HyTeG's matrix-free P1 multigrid path.
+
+TEST INFRASTRUCTURE ONLY.  Nothing in the ``hyteg_b200`` product imports this
+module; it is used by ``tests/``, ``__graft_entry__.smoke()`` and the CPU leg
+of ``bench.py`` as the checker.
+
+What it restates (reference paths are relative to the hyteg source tree):
+
+* Primitive ordering and local orientation of a macro mesh:
+  ``src/hyteg/mesh/MeshInfo.cpp`` (``addEdge``/``addFace`` sort the vertex ids,
+  cells keep the mesh order) and
+  ``src/hyteg/primitivestorage/SetupPrimitiveStorage.cpp:130-412`` (ids are
+  generated vertex -> edge -> face -> cell in map order; face vertex order is
+  the sorted order; cell local edges/faces at :305-315).
+* Boundary flags: ``SetupPrimitiveStorage.cpp:977-988,1092-1150``
+  (``setMeshBoundaryFlagsOnBoundary``/``onBoundary``).
+* Vertex-DoF memory layout per primitive and level:
+  ``src/hyteg/p1functionspace/VertexDoFMemory.hpp:39-60``,
+  ``src/hyteg/indexing/MacroCellIndexing.hpp:39-52``,
+  ``src/hyteg/indexing/MacroFaceIndexing.hpp:39-50``.
+* Micro-cells of a refined macro-cell:
+  ``src/hyteg/volumedofspace/CellDoFIndexing.hpp:64-198``;
+  micro-vertex coordinates ``src/hyteg/p1functionspace/VertexDoFMacroCell.hpp:70-77``.
+* P1 Laplace element matrix (FEniCS form ``p1_tet_diffusion``,
+  ``src/hyteg/forms/form_fenics_generated/p1_tet_diffusion.h``):
+  K = |det J| / 6 * G G^T.
+* ``P1Operator::apply`` (``src/hyteg/p1functionspace/P1Operator.hpp:192-320``):
+  y = A x on owned DoFs whose boundary type matches ``flag``.  The oracle
+  assembles A from micro-cell element matrices over HyTeG's own layout
+  instead of going through stencils and ghost layers: every P1 stencil entry
+  of HyTeG is a sum of element-matrix entries over the micro-cells around a
+  micro-vertex (``src/hyteg/p1functionspace/P1Elements.hpp:466-529``), so the
+  two agree up to rounding of the summation order.
+* ``P1toP1LinearRestriction::restrict3D`` (``P1toP1LinearRestriction.cpp:169-346``)
+  through the generated pull kernel ``restrict_3D_macrocell_P1_pull_additive``:
+  per macro-cell pull with weights 1 and 1/2, each fine value scaled by
+  1/(number of macro-cells around the primitive owning that fine point), then
+  additive communication into flagged owners.
+* ``P1toP1LinearProlongation::prolongate3DAdditively``
+  (``P1toP1LinearProlongation.cpp:194-410``): linear interpolation added to
+  (or replacing) flagged owned fine DoFs.
+* ``WeightedJacobiSmoother::solve`` (``solvers/WeightedJacobiSmoother.hpp:46-66``)
+  with ``P1Operator::smooth_jac`` (``P1Operator.hpp:429-447``).
+* ``ChebyshevSmoother::solve`` (``solvers/ChebyshevSmoother.hpp:112-240``),
+  coefficients (``:329-555``), ``chebyshev::estimateRadius`` (``:656-676``)
+  and ``estimateSpectralRadiusWithPowerIteration``
+  (``numerictools/SpectrumEstimation.hpp:56-84``).
+* ``CGSolver::solve`` (``solvers/CGSolver.hpp:94-206``).
+* ``GeometricMultigridSolver::solveRecursively``
+  (``solvers/GeometricMultigridSolver.hpp:207-305``).
+
+Vectors are HyTeG layout buffers of one level (all primitives packed in the
+order vertices, edges, faces, cells, each with its full HyTeG array including
+ghost layers).  Only owned slots carry meaning; copy slots can be filled with
+``Level.sync``.
+"""
+
+from __future__ import annotations
+
+import itertools
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.sparse as sp
+
+INNER = 1
+DIRICHLET = 2
+NEUMANN = 4
+FREESLIP = 8
+ALL = INNER | DIRICHLET | NEUMANN | FREESLIP
+
+# 14 neighbour directions of the 3D P1 stencil
+# (src/hyteg/p1functionspace/VertexDoFIndexing.hpp:289-323).
+STENCIL_DIRS = np.array(
+    [
+        (-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1),
+        (-1, 1, 0), (1, -1, 0), (-1, 0, 1), (1, 0, -1), (0, -1, 1), (0, 1, -1),
+        (1, -1, 1), (-1, 1, -1),
+    ],
+    dtype=np.int64,
+)
+
+# Micro-cell types: vertex offsets and row width (number of micro-edges per
+# edge minus the shift), CellDoFIndexing.hpp:64-198.
+MICRO_CELL_TYPES = [
+    ("WHITE_UP", [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1)], 0),
+    ("BLUE_UP", [(1, 0, 0), (1, 1, 0), (0, 1, 0), (1, 0, 1)], 1),
+    ("GREEN_UP", [(1, 0, 0), (0, 1, 0), (1, 0, 1), (0, 0, 1)], 1),
+    ("WHITE_DOWN", [(1, 1, 0), (1, 1, 1), (0, 1, 1), (1, 0, 1)], 2),
+    ("BLUE_DOWN", [(1, 0, 1), (0, 1, 1), (0, 0, 1), (0, 1, 0)], 1),
+    ("GREEN_DOWN", [(0, 1, 0), (1, 1, 0), (1, 0, 1), (0, 1, 1)], 1),
+]
+
+
+def tet_size(w):
+    """linearMacroCellSize (MacroCellIndexing.hpp:39-42)."""
+    return ((w + 2) * (w + 1) * w) // 6
+
+
+def tri_size(w):
+    """linearMacroFaceSize (MacroFaceIndexing.hpp:39-42)."""
+    return ((w + 1) * w) // 2
+
+
+def cell_index(n, x, y, z):
+    """linearMacroCellIndex with width n+1 (MacroCellIndexing.hpp:45-52)."""
+    w = n + 1
+    wz = w - z
+    slice_off = tet_size(w) - ((wz + 2) * (wz + 1) * wz) // 6
+    row_off = y * (wz + 1) - ((y + 1) * y) // 2
+    return slice_off + row_off + x
+
+
+def face_index(n, i, j):
+    """linearMacroFaceIndex with width n+1 (MacroFaceIndexing.hpp:45-50)."""
+    w = n + 1
+    return j * (w + 1) - ((j + 1) * j) // 2 + i
+
+
+def tet_points(w):
+    """All (x, y, z) with x+y+z <= w-1, in HyTeG memory order (z-major, then y, then x)."""
+    pts = []
+    for z in range(w):
+        for y in range(w - z):
+            for x in range(w - z - y):
+                pts.append((x, y, z))
+    return np.array(pts, dtype=np.int64).reshape(-1, 3)
+
+
+class MacroMesh:
+    """Macro-primitive topology with HyTeG's id order and local orientations."""
+
+    def __init__(self, coords, tets, boundary_flag=1, inner_flag=0, bc_types=None):
+        coords = np.asarray(coords, dtype=np.float64)
+        self.vcoords = coords
+        nv = coords.shape[0]
+        cells = sorted(tuple(int(v) for v in t) for t in tets)  # std::map keyed by vertex list
+        edge_set, face_set = set(), set()
+        for c in cells:
+            for a, b in itertools.combinations(c, 2):
+                edge_set.add(tuple(sorted((a, b))))
+            for tri in itertools.combinations(c, 3):
+                face_set.add(tuple(sorted(tri)))
+        self.edges = sorted(edge_set)
+        self.faces = sorted(face_set)
+        self.cells = cells
+        self.edge_id = {e: i for i, e in enumerate(self.edges)}
+        self.face_id = {f: i for i, f in enumerate(self.faces)}
+        nE, nF, nC = len(self.edges), len(self.faces), len(self.cells)
+        self.nV, self.nE, self.nF, self.nC = nv, nE, nF, nC
+        # neighbour lists in insertion order
+        self.v_edges = [[] for _ in range(nv)]
+        self.v_faces = [[] for _ in range(nv)]
+        self.v_cells = [[] for _ in range(nv)]
+        self.e_faces = [[] for _ in range(nE)]
+        self.e_cells = [[] for _ in range(nE)]
+        self.f_cells = [[] for _ in range(nF)]
+        for i, (a, b) in enumerate(self.edges):
+            self.v_edges[a].append(i)
+            self.v_edges[b].append(i)
+        for i, f in enumerate(self.faces):
+            for v in f:
+                self.v_faces[v].append(i)
+            for e in itertools.combinations(f, 2):
+                self.e_faces[self.edge_id[e]].append(i)
+        # cell local edges / faces (SetupPrimitiveStorage.cpp:305-315)
+        self.cell_edges, self.cell_faces = [], []
+        for ci, c in enumerate(cells):
+            v0, v1, v2, v3 = c
+            ce = [self.edge_id[tuple(sorted(p))] for p in ((v0, v1), (v0, v2), (v1, v2), (v0, v3), (v1, v3), (v2, v3))]
+            cf = [self.face_id[tuple(sorted(t))] for t in ((v0, v1, v2), (v0, v1, v3), (v0, v2, v3), (v1, v2, v3))]
+            self.cell_edges.append(ce)
+            self.cell_faces.append(cf)
+            for v in c:
+                self.v_cells[v].append(ci)
+            for e in ce:
+                self.e_cells[e].append(ci)
+            for f in cf:
+                self.f_cells[f].append(ci)
+        # boundary flags (setMeshBoundaryFlagsOnBoundary(boundary_flag, inner_flag, true))
+        f_bnd = [len(self.f_cells[f]) == 1 for f in range(nF)]
+        e_bnd = [any(f_bnd[f] for f in self.e_faces[e]) for e in range(nE)]
+        v_bnd = [any(f_bnd[f] for f in self.v_faces[v]) for v in range(nv)]
+        self.flag_v = [boundary_flag if b else inner_flag for b in v_bnd]
+        self.flag_e = [boundary_flag if b else inner_flag for b in e_bnd]
+        self.flag_f = [boundary_flag if b else inner_flag for b in f_bnd]
+        self.flag_c = [inner_flag] * nC
+        # BoundaryCondition::create0123BC: flag 0 Inner, 1 Dirichlet, 2 Neumann, 3 Freeslip
+        self.bc_types = bc_types or {0: INNER, 1: DIRICHLET, 2: NEUMANN, 3: FREESLIP}
+
+    def bc(self, kind, idx):
+        flag = {"v": self.flag_v, "e": self.flag_e, "f": self.flag_f, "c": self.flag_c}[kind][idx]
+        return self.bc_types.get(flag, INNER)
+
+
+# ---------------------------------------------------------------------------------------------
+# meshes used by the tests and the configs
+# ---------------------------------------------------------------------------------------------
+
+def mesh_cuboid(lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), nx=1, ny=1, nz=1):
+    """MeshInfo::meshCuboid (src/hyteg/mesh/MeshGenCuboid.cpp:35-172): six tets per sub-cube."""
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    hx, hy, hz = (x1 - x0) / nx, (y1 - y0) / ny, (z1 - z0) / nz
+    coords = []
+    for iz in range(nz + 1):
+        for iy in range(ny + 1):
+            for ix in range(nx + 1):
+                coords.append((x0 + ix * hx, y0 + iy * hy, z0 + iz * hz))
+    corner = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)]
+    split = [(4, 5, 7, 3), (0, 3, 1, 4), (4, 1, 5, 3), (5, 6, 7, 2), (1, 3, 2, 5), (7, 2, 3, 5)]
+    tets = []
+    for iz in range(nz):
+        for iy in range(ny):
+            for ix in range(nx):
+                for t in split:
+                    ids = []
+                    for m in t:
+                        ox, oy, oz = corner[m]
+                        ids.append((iz + oz) * (nx + 1) * (ny + 1) + (iy + oy) * (nx + 1) + (ix + ox))
+                    tets.append(ids)
+    return np.array(coords), tets
+
+
+# ---------------------------------------------------------------------------------------------
+# layout of one level
+# ---------------------------------------------------------------------------------------------
+
+class Level:
+    """HyTeG vertex-DoF layout of all primitives at one level, plus owner maps."""
+
+    def __init__(self, mesh: MacroMesh, L: int):
+        self.mesh, self.L = mesh, L
+        n = 1 << L
+        self.n = n
+        m = mesh
+        sizes_v = [1 + len(m.v_edges[v]) for v in range(m.nV)]
+        sizes_e = [(n + 1) + len(m.e_faces[e]) * n + len(m.e_cells[e]) * (n - 1) for e in range(m.nE)]
+        sizes_f = [tri_size(n + 1) + len(m.f_cells[f]) * tri_size(n) for f in range(m.nF)]
+        sizes_c = [tet_size(n + 1)] * m.nC
+        allsizes = sizes_v + sizes_e + sizes_f + sizes_c
+        offs = np.concatenate([[0], np.cumsum(allsizes)]).astype(np.int64)
+        self.size = int(offs[-1])
+        self.off_v = offs[: m.nV]
+        self.off_e = offs[m.nV: m.nV + m.nE]
+        self.off_f = offs[m.nV + m.nE: m.nV + m.nE + m.nF]
+        self.off_c = offs[m.nV + m.nE + m.nF: m.nV + m.nE + m.nF + m.nC]
+        self.sizes = dict(v=sizes_v, e=sizes_e, f=sizes_f, c=sizes_c)
+        self._build_owned()
+        self._cell_pts = tet_points(n + 1)  # all points of a cell array in memory order
+
+    # owned slots -----------------------------------------------------------------------------
+    def _build_owned(self):
+        m, n = self.mesh, self.n
+        owned, bc = [], []
+        for v in range(m.nV):
+            owned.append(np.array([self.off_v[v]]))
+            bc.append(np.full(1, m.bc("v", v)))
+        for e in range(m.nE):
+            idx = self.off_e[e] + np.arange(1, n)
+            owned.append(idx)
+            bc.append(np.full(idx.size, m.bc("e", e)))
+        for f in range(m.nF):
+            ij = [(i, j) for j in range(1, n) for i in range(1, n - j)]
+            idx = np.array([self.off_f[f] + face_index(n, i, j) for i, j in ij], dtype=np.int64)
+            owned.append(idx)
+            bc.append(np.full(idx.size, m.bc("f", f)))
+        for c in range(m.nC):
+            pts = tet_points(n + 1)
+            inner = (pts.min(axis=1) >= 1) & (pts.sum(axis=1) <= n - 1)
+            idx = self.off_c[c] + cell_index(n, pts[inner, 0], pts[inner, 1], pts[inner, 2])
+            owned.append(idx)
+            bc.append(np.full(idx.size, m.bc("c", c)))
+        self.owned = np.concatenate(owned).astype(np.int64)
+        self.owned_bc = np.concatenate(bc).astype(np.int64)
+        self.bc_of_slot = np.zeros(self.size, dtype=np.int64)
+        self.bc_of_slot[self.owned] = self.owned_bc
+
+    def owned_mask(self, flag=ALL):
+        mask = np.zeros(self.size, dtype=bool)
+        sel = (self.owned_bc & flag) != 0
+        mask[self.owned[sel]] = True
+        return mask
+
+    # owner of cell-local points --------------------------------------------------------------
+    def owner(self, c, x, y, z):
+        """Owner slot of the cell-local micro-vertex (x, y, z) of macro-cell c (vectorised).
+
+        The owner follows from the barycentric integer weights (n-x-y-z, x, y, z) on the
+        cell's vertices: one non-zero weight -> macro-vertex, two -> macro-edge (local index =
+        weight of the edge's second vertex), three -> macro-face (local (i, j) = weights of the
+        face's second and third vertex), four -> cell interior.
+        """
+        m, n = self.mesh, self.n
+        x, y, z = (np.asarray(a, dtype=np.int64) for a in (x, y, z))
+        w = np.stack([n - x - y - z, x, y, z], axis=-1)
+        cv = m.cells[c]
+        nz = w != 0
+        out = np.full(x.shape, -1, dtype=np.int64)
+        patterns = {}
+        key = nz[..., 0] * 1 + nz[..., 1] * 2 + nz[..., 2] * 4 + nz[..., 3] * 8
+        for k in np.unique(key):
+            sel = key == k
+            locs = [i for i in range(4) if (k >> i) & 1]
+            gv = [cv[i] for i in locs]
+            if len(locs) == 1:
+                out[sel] = self.off_v[gv[0]]
+            elif len(locs) == 2:
+                e = m.edge_id[tuple(sorted(gv))]
+                ev1 = m.edges[e][1]
+                wi = w[sel][:, locs[gv.index(ev1)]]
+                out[sel] = self.off_e[e] + wi
+            elif len(locs) == 3:
+                f = m.face_id[tuple(sorted(gv))]
+                fv = m.faces[f]
+                wi = w[sel][:, locs[gv.index(fv[1])]]
+                wj = w[sel][:, locs[gv.index(fv[2])]]
+                out[sel] = self.off_f[f] + face_index(n, wi, wj)
+            else:
+                out[sel] = self.off_c[c] + cell_index(n, x[sel], y[sel], z[sel])
+        return out
+
+    def coords(self, c, x, y, z):
+        """vertexdof::macrocell::coordinateFromIndex (VertexDoFMacroCell.hpp:70-77)."""
+        cv = self.mesh.cells[c]
+        P = self.mesh.vcoords[list(cv)]
+        step = 1.0 / self.n
+        xs, ys, zs = (P[1] - P[0]) * step, (P[2] - P[0]) * step, (P[3] - P[0]) * step
+        x, y, z = (np.asarray(a, dtype=np.float64)[..., None] for a in (x, y, z))
+        return P[0] + xs * x + ys * y + zs * z
+
+    def copy_map(self):
+        """(dst, src) pairs: every cell-array slot that is a copy of a lower-dimensional owner."""
+        dsts, srcs = [], []
+        pts = self._cell_pts
+        for c in range(self.mesh.nC):
+            own = self.owner(c, pts[:, 0], pts[:, 1], pts[:, 2])
+            slot = self.off_c[c] + cell_index(self.n, pts[:, 0], pts[:, 1], pts[:, 2])
+            sel = own != slot
+            dsts.append(slot[sel])
+            srcs.append(own[sel])
+        return np.concatenate(dsts), np.concatenate(srcs)
+
+    def sync(self, vec):
+        """Fill cell-array copy slots from their owners (communicate<Vertex..Face, Cell>)."""
+        if not hasattr(self, "_cmap"):
+            self._cmap = self.copy_map()
+        d, s = self._cmap
+        vec[d] = vec[s]
+        return vec
+
+    def micro_cells(self, c):
+        """Owner slots (k, 4) and coordinates (k, 4, 3) of all micro-cells of macro-cell c."""
+        n = self.n
+        slots, xyz = [], []
+        for _, offs, shift in MICRO_CELL_TYPES:
+            w = n - shift
+            if w <= 0:
+                continue
+            base = tet_points(w)
+            vs = [base + np.array(o, dtype=np.int64) for o in offs]
+            slots.append(np.stack([self.owner(c, v[:, 0], v[:, 1], v[:, 2]) for v in vs], axis=1))
+            xyz.append(np.stack([self.coords(c, v[:, 0], v[:, 1], v[:, 2]) for v in vs], axis=1))
+        return np.concatenate(slots), np.concatenate(xyz)
+
+
+# ---------------------------------------------------------------------------------------------
+# element matrices and operators
+# ---------------------------------------------------------------------------------------------
+
+def p1_laplace_element(X):
+    """P1 stiffness matrices for tets X (k, 4, 3): K = |det J|/6 * G G^T (p1_tet_diffusion form)."""
+    J = np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], axis=2)  # columns
+    det = np.linalg.det(J)
+    Jinv = np.linalg.inv(J)  # rows of Jinv are grad of lambda_1..3
+    G = np.concatenate([-Jinv.sum(axis=1, keepdims=True), Jinv], axis=1)  # (k, 4, 3)
+    return (np.abs(det) / 6.0)[:, None, None] * np.einsum("kid,kjd->kij", G, G)
+
+
+def p1_mass_element(X):
+    """P1 mass matrices: |det J|/120 * (1 + delta_ij)."""
+    J = np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], axis=2)
+    det = np.abs(np.linalg.det(J))
+    M = (np.ones((4, 4)) + np.eye(4)) / 120.0
+    return det[:, None, None] * M[None]
+
+
+def assemble(level: Level, element=p1_laplace_element):
+    """Global matrix over HyTeG layout slots from micro-cell element matrices."""
+    rows, cols, vals = [], [], []
+    for c in range(level.mesh.nC):
+        slots, X = level.micro_cells(c)
+        K = element(X)
+        rows.append(np.repeat(slots, 4, axis=1).ravel())
+        cols.append(np.tile(slots, (1, 4)).ravel())
+        vals.append(K.reshape(K.shape[0], 16).ravel())
+    A = sp.coo_matrix(
+        (np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(level.size, level.size)
+    ).tocsr()
+    A.sum_duplicates()
+    return A
+
+
+class P1ConstantLaplace:
+    """P1 Laplace operator over levels minL..maxL (apply / smooth_jac / inverse diagonal)."""
+
+    def __init__(self, mesh, minL, maxL, element=p1_laplace_element):
+        self.mesh, self.minL, self.maxL = mesh, minL, maxL
+        self.levels = {L: Level(mesh, L) for L in range(minL, maxL + 1)}
+        self.A = {L: assemble(self.levels[L], element) for L in range(minL, maxL + 1)}
+        self.invdiag = {}
+        for L, A in self.A.items():
+            d = A.diagonal()
+            inv = np.zeros_like(d)
+            own = self.levels[L].owned
+            inv[own] = 1.0 / d[own]
+            self.invdiag[L] = inv
+
+    def apply(self, src, dst, L, flag, add=False):
+        """P1Operator::apply: dst = A src (or dst += A src) on owned DoFs matching flag."""
+        y = self.A[L] @ src
+        mask = self.levels[L].owned_mask(flag)
+        if add:
+            dst[mask] += y[mask]
+        else:
+            dst[mask] = y[mask]
+        return dst
+
+    def smooth_jac(self, dst, rhs, src, relax, L, flag):
+        """P1Operator::smooth_jac (P1Operator.hpp:429-447): dst = src + relax * D^-1 (rhs - A src)."""
+        mask = self.levels[L].owned_mask(flag)
+        y = self.A[L] @ src
+        t = rhs - y
+        t = self.invdiag[L] * t
+        dst[mask] = src[mask] + relax * t[mask]
+        return dst
+
+
+# ---------------------------------------------------------------------------------------------
+# grid transfer
+# ---------------------------------------------------------------------------------------------
+
+def _num_neighbor_cells_of_owner(level: Level):
+    """For every slot: number of macro-cells around the owning primitive (1 for cell interior)."""
+    m = level.mesh
+    cnt = np.ones(level.size)
+    for v in range(m.nV):
+        cnt[level.off_v[v]: level.off_v[v] + level.sizes["v"][v]] = len(m.v_cells[v])
+    for e in range(m.nE):
+        cnt[level.off_e[e]: level.off_e[e] + level.sizes["e"][e]] = len(m.e_cells[e])
+    for f in range(m.nF):
+        cnt[level.off_f[f]: level.off_f[f] + level.sizes["f"][f]] = len(m.f_cells[f])
+    return cnt
+
+
+def restriction_matrix(fine: Level, coarse: Level):
+    """restrict3D with the generated pull kernel as a matrix over owner slots.
+
+    ``restrict_3D_macrocell_P1_pull_additive`` (gridtransferoperators/generatedKernels,
+    :53-120 for the vertex-0 case) pulls, per macro-cell, the fine centre with weight 1 and the
+    fine stencil neighbours with weight 1/2, each scaled by 1/(number of macro-cells around the
+    primitive that owns the *fine* point); ``communicateAdditively<Cell, *>``
+    (P1toP1LinearRestriction.cpp:342-344) then sums the cell shares into flagged owners.
+    """
+    assert fine.L == coarse.L + 1
+    nc = coarse.n
+    pts = tet_points(nc + 1)
+    ncells = _num_neighbor_cells_of_owner(fine)
+    rows, cols, vals = [], [], []
+    for c in range(fine.mesh.nC):
+        dst = coarse.owner(c, pts[:, 0], pts[:, 1], pts[:, 2])
+        src = fine.owner(c, 2 * pts[:, 0], 2 * pts[:, 1], 2 * pts[:, 2])
+        rows.append(dst), cols.append(src), vals.append(1.0 / ncells[src])
+        for d in STENCIL_DIRS:
+            q = 2 * pts + d
+            inside = (q.min(axis=1) >= 0) & (q.sum(axis=1) <= fine.n)
+            s = fine.owner(c, q[inside, 0], q[inside, 1], q[inside, 2])
+            rows.append(dst[inside]), cols.append(s), vals.append(0.5 / ncells[s])
+    R = sp.coo_matrix(
+        (np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(coarse.size, fine.size)
+    ).tocsr()
+    R.sum_duplicates()
+    return R
+
+
+def prolongation_matrix(coarse: Level, fine: Level):
+    """Linear interpolation (prolongate3DAdditively, P1toP1LinearProlongation.cpp:194-410)."""
+    assert fine.L == coarse.L + 1
+    pts = tet_points(fine.n + 1)
+    seen = np.zeros(fine.size, dtype=bool)
+    rows, cols, vals = [], [], []
+    for c in range(fine.mesh.nC):
+        dst = fine.owner(c, pts[:, 0], pts[:, 1], pts[:, 2])
+        odd = pts % 2
+        even = odd.sum(axis=1) == 0
+        # the coarse micro-edge through an odd fine point has direction d in the stencil
+        # set with |d_k| = odd_k; choose the representative with d_x >= 0 and d = sign pattern
+        d = np.zeros_like(pts)
+        for dirv in STENCIL_DIRS:
+            match = np.all(np.abs(dirv)[None, :] == odd, axis=1)
+            d[match] = dirv
+        a = (pts - d) // 2
+        b = (pts + d) // 2
+        new = ~seen[dst]
+        # mark first occurrence only (all cells give the same interpolation)
+        uniq_dst, first = np.unique(dst[new], return_index=True)
+        sel = np.flatnonzero(new)[first]
+        seen[uniq_dst] = True
+        ev = even[sel]
+        ca = coarse.owner(c, a[sel, 0], a[sel, 1], a[sel, 2])
+        cb = coarse.owner(c, b[sel, 0], b[sel, 1], b[sel, 2])
+        rows.append(dst[sel][ev]), cols.append(ca[ev]), vals.append(np.ones(ev.sum()))
+        ne = ~ev
+        rows.append(dst[sel][ne]), cols.append(ca[ne]), vals.append(np.full(ne.sum(), 0.5))
+        rows.append(dst[sel][ne]), cols.append(cb[ne]), vals.append(np.full(ne.sum(), 0.5))
+    P = sp.coo_matrix(
+        (np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(fine.size, coarse.size)
+    ).tocsr()
+    P.sum_duplicates()
+    return P
+
+
+class Transfer:
+    def __init__(self, op: P1ConstantLaplace):
+        self.op = op
+        self.R, self.P = {}, {}
+        for L in range(op.minL + 1, op.maxL + 1):
+            self.R[L] = restriction_matrix(op.levels[L], op.levels[L - 1])
+            self.P[L] = prolongation_matrix(op.levels[L - 1], op.levels[L])
+
+    def restrict(self, fine_vec, coarse_vec, L, flag):
+        """coarse (level L-1) <- R fine (level L) on flagged owned coarse DoFs."""
+        y = self.R[L] @ fine_vec
+        mask = self.op.levels[L - 1].owned_mask(flag)
+        coarse_vec[mask] = y[mask]
+        return coarse_vec
+
+    def prolongate(self, coarse_vec, fine_vec, L, flag, add=True):
+        """fine (level L) (+)= P coarse (level L-1) on flagged owned fine DoFs."""
+        y = self.P[L] @ coarse_vec
+        mask = self.op.levels[L].owned_mask(flag)
+        if add:
+            fine_vec[mask] += y[mask]
+        else:
+            fine_vec[mask] = y[mask]
+        return fine_vec
+
+
+# ---------------------------------------------------------------------------------------------
+# solvers
+# ---------------------------------------------------------------------------------------------
+
+def dot(level: Level, a, b, flag):
+    """dotGlobal over owned DoFs of the flagged types (VertexDoFFunction.cpp:1710-1790)."""
+    mask = level.owned_mask(flag)
+    return float(np.dot(a[mask], b[mask]))
+
+
+def chebyshev_coefficients(order, lower, upper):
+    """Coefficients c_0..c_{k-1} with x += sum_i c_i (D^-1 A)^i D^-1 r.
+
+    Equivalent to ChebyshevSmoother::setupCoefficientsInternal (ChebyshevSmoother.hpp:329-555):
+    the error polynomial 1 - t p(t) equals T_k((theta - t)/delta) / T_k(theta/delta),
+    theta = (upper+lower)/2, delta = (upper-lower)/2.  Derived here by polynomial algebra.
+    """
+    theta = 0.5 * (upper + lower)
+    delta = 0.5 * (upper - lower)
+    # Chebyshev T_k as coefficient lists in s
+    T = [np.array([1.0]), np.array([0.0, 1.0])]
+    for k in range(2, order + 1):
+        T.append(np.concatenate([[0.0], 2 * T[-1]]) - np.concatenate([T[-2], [0.0, 0.0]]))
+    Tk = T[order]
+    # substitute s = (theta - t)/delta  -> polynomial in t
+    poly_t = np.zeros(order + 1)
+    base = np.array([theta / delta, -1.0 / delta])
+    powk = np.array([1.0])
+    for k in range(order + 1):
+        poly_t[: powk.size] += Tk[k] * powk
+        powk = np.convolve(powk, base)
+    norm = np.polyval(Tk[::-1], theta / delta)
+    e = poly_t / norm  # e(0) = 1
+    # 1 - t p(t) = e(t)  =>  p_i = -e_{i+1}
+    return [-e[i + 1] for i in range(order)]
+
+
+class GMG:
+    """GeometricMultigridSolver (V/W cycle) with weighted Jacobi or Chebyshev smoothing."""
+
+    def __init__(self, op, transfer, minL, maxL, pre=2, post=2, increment=0, cycle="V",
+                 smoother="jacobi", omega=2.0 / 3.0, cheb_order=3, cheb_radii=None,
+                 cg_tol=1e-14, cg_abs=1e-16, cg_maxit=10**6):
+        self.op, self.tr = op, transfer
+        self.minL, self.maxL = minL, maxL
+        self.pre, self.post, self.inc, self.cycle = pre, post, increment, cycle
+        self.smoother, self.omega = smoother, omega
+        self.flag = INNER | NEUMANN | FREESLIP
+        self.cg_tol, self.cg_abs, self.cg_maxit = cg_tol, cg_abs, cg_maxit
+        if smoother == "chebyshev":
+            self.cheb = {L: chebyshev_coefficients(cheb_order, 0.3 * cheb_radii[L], 1.2 * cheb_radii[L])
+                         for L in range(minL, maxL + 1)}
+
+    # smoothers -----------------------------------------------------------------------------
+    def smooth(self, x, b, L):
+        op = self.op
+        if self.smoother == "jacobi":
+            tmp = x.copy()  # tmp.assign({1}, {x}, level, All)
+            op.smooth_jac(x, b, tmp, self.omega, L, self.flag)
+        else:
+            self.chebyshev_step(x, b, L)
+
+    def chebyshev_step(self, x, b, L):
+        """ChebyshevSmoother::solve (ChebyshevSmoother.hpp:112-240)."""
+        op, lev = self.op, self.op.levels[L]
+        mask = lev.owned_mask(self.flag)
+        coeff = self.cheb[L]
+        # copyBCs(x, tmp1/tmp2): boundary entries of the temporaries carry x's boundary values
+        tmp1 = x.copy()
+        tmp2 = x.copy()
+        op.apply(x, tmp2, L, self.flag)
+        tmp2[mask] = b[mask] - tmp2[mask]
+        tmp1[mask] = op.invdiag[L][mask] * tmp2[mask]
+        x[mask] = x[mask] + coeff[0] * tmp1[mask]
+        for k in range(1, len(coeff)):
+            op.apply(tmp1, tmp2, L, self.flag)
+            tmp1[mask] = op.invdiag[L][mask] * tmp2[mask]
+            x[mask] = x[mask] + coeff[k] * tmp1[mask]
+
+    # coarse solver -------------------------------------------------------------------------
+    def cg(self, x, b, L):
+        """CGSolver::solve (CGSolver.hpp:94-206) with identity preconditioner."""
+        op, lev, flag = self.op, self.op.levels[L], self.flag
+        mask = lev.owned_mask(flag)
+        r = np.zeros_like(x)
+        ap = np.zeros_like(x)
+        # init: r = b - A x ; p = z = r
+        op.apply(x, ap, L, flag)
+        r[mask] = b[mask] - ap[mask]
+        p = np.where(mask, r, 0.0)
+        prsold = dot(lev, r, r, flag)
+        res_start = math.sqrt(prsold)
+        if res_start < self.cg_abs:
+            return 0
+        for it in range(self.cg_maxit):
+            op.apply(p, ap, L, flag)
+            pAp = dot(lev, p, ap, flag)
+            alpha = prsold / pAp
+            x[mask] += alpha * p[mask]
+            r[mask] -= alpha * ap[mask]
+            rsnew = dot(lev, r, r, flag)
+            sq = math.sqrt(rsnew)
+            if sq / res_start < self.cg_tol or sq < self.cg_abs:
+                return it
+            beta = rsnew / prsold
+            p[mask] = r[mask] + beta * p[mask]
+            prsold = rsnew
+        return self.cg_maxit
+
+    # cycle -----------------------------------------------------------------------------------
+    def solve(self, x, b, L):
+        """x, b: dicts level -> layout vector.  One multigrid cycle on level L."""
+        self.invoked = L
+        self._rec(x, b, L)
+
+    def _rec(self, x, b, L):
+        op = self.op
+        if L == self.minL:
+            self.cg(x[L], b[L], L)
+            return
+        for _ in range(self.pre + self.inc * (self.invoked - L)):
+            self.smooth(x[L], b[L], L)
+        tmp = np.zeros(op.levels[L].size)
+        op.apply(x[L], tmp, L, self.flag)
+        mask = op.levels[L].owned_mask(self.flag)
+        tmp[mask] = b[L][mask] - tmp[mask]
+        coarse_tmp = np.zeros(op.levels[L - 1].size)
+        self.tr.restrict(tmp, coarse_tmp, L, self.flag)
+        cm = op.levels[L - 1].owned_mask(self.flag)
+        b[L - 1][cm] = coarse_tmp[cm]
+        x[L - 1][:] = 0.0
+        self._rec(x, b, L - 1)
+        if self.cycle == "W":
+            self._rec(x, b, L - 1)
+        self.tr.prolongate(x[L - 1], x[L], L, self.flag, add=True)
+        for _ in range(self.post + self.inc * (self.invoked - L)):
+            self.smooth(x[L], b[L], L)
+
+
+def power_iteration_radius(op: P1ConstantLaplace, L, x0, iters):
+    """estimateSpectralRadiusWithPowerIteration on D^-1 A (SpectrumEstimation.hpp:56-84), flag All."""
+    lev = op.levels[L]
+    x = x0.copy()
+    aux = np.zeros_like(x)
+
+    def dinv_a(src, dst):
+        op.apply(src, dst, L, ALL)
+        m = lev.owned_mask(ALL)
+        dst[m] = op.invdiag[L][m] * dst[m]
+
+    norm = math.sqrt(dot(lev, x, x, ALL))
+    x = x * (1.0 / norm)
+    dinv_a(x, aux)
+    radius = 0.0
+    for _ in range(iters):
+        norm = math.sqrt(dot(lev, aux, aux, ALL))
+        x = aux * (1.0 / norm)
+        dinv_a(x, aux)
+        radius = dot(lev, x, aux, ALL)
+    return radius
+
+
+def residual_norm(op, x, b, L, flag=INNER | NEUMANN | FREESLIP):
+    lev = op.levels[L]
+    r = np.zeros(lev.size)
+    op.apply(x, r, L, flag)
+    mask = lev.owned_mask(flag)
+    r[mask] = b[mask] - r[mask]
+    return math.sqrt(dot(lev, r, r, flag))
+
+
+# ---------------------------------------------------------------------------------------------
+# single macro-cell kernels (the per-cell steps of apply / restrict / prolongate)
+# ---------------------------------------------------------------------------------------------
+STENCIL15 = np.concatenate([np.zeros((1, 3), dtype=np.int64), STENCIL_DIRS])
+
+
+def _cell_class_weight(pts, n, nc14):
+    """1/(number of macro-cells around the cell sub-primitive holding each point); nc14 = edges 0-5,
+    faces 0-3, vertices 0-3 of the cell."""
+    x, y, z = pts[:, 0], pts[:, 1], pts[:, 2]
+    on = np.stack([z == 0, y == 0, x == 0, x + y + z == n], axis=1)  # cell faces 012, 013, 023, 123
+    key = on[:, 0] * 1 + on[:, 1] * 2 + on[:, 2] * 4 + on[:, 3] * 8
+    table = {0: None, 1: 6, 2: 7, 4: 8, 8: 9, 3: 0, 5: 1, 9: 2, 6: 3, 10: 4, 12: 5, 7: 10, 11: 11, 13: 12, 14: 13}
+    w = np.ones(len(pts))
+    for k, idx in table.items():
+        if idx is not None:
+            w[key == k] = 1.0 / nc14[idx]
+    return w
+
+
+def cell_stencil_apply(src, L, stencil15):
+    """apply_3D_macrocell_vertexdof_to_vertexdof_replace: interior points get sum_d s_d src[p+d]."""
+    n = 1 << L
+    pts = tet_points(n + 1)
+    inner = (pts.min(axis=1) >= 1) & (pts.sum(axis=1) <= n - 1)
+    p = pts[inner]
+    out = np.zeros_like(src)
+    acc = np.zeros(len(p))
+    for d, s in zip(STENCIL15, stencil15):
+        q = p + d
+        acc += s * src[cell_index(n, q[:, 0], q[:, 1], q[:, 2])]
+    out[cell_index(n, p[:, 0], p[:, 1], p[:, 2])] = acc
+    return out
+
+
+def cell_restrict(fine, Lc, nc14):
+    """restrict_3D_macrocell_P1_pull_additive on one cell (all coarse points)."""
+    nc, nf = 1 << Lc, 2 << Lc
+    cp = tet_points(nc + 1)
+    fc = 2 * cp
+    out = _cell_class_weight(fc, nf, nc14) * fine[cell_index(nf, fc[:, 0], fc[:, 1], fc[:, 2])]
+    for d in STENCIL_DIRS:
+        q = fc + d
+        inside = (q.min(axis=1) >= 0) & (q.sum(axis=1) <= nf)
+        qi = q[inside]
+        out[inside] += 0.5 * _cell_class_weight(qi, nf, nc14) * fine[cell_index(nf, qi[:, 0], qi[:, 1], qi[:, 2])]
+    return out
+
+
+def cell_prolongate(coarse, Lc, nc14, fine=None):
+    """prolongate_3D_macrocell_P1_push_additive on one cell: fine += w * linear interpolation."""
+    nc, nf = 1 << Lc, 2 << Lc
+    fp = tet_points(nf + 1)
+    out = np.zeros(tet_size(nf + 1)) if fine is None else fine.copy()
+    odd = fp % 2
+    d = np.zeros_like(fp)
+    for dirv in STENCIL_DIRS:
+        d[np.all(np.abs(dirv)[None, :] == odd, axis=1)] = dirv
+    a, b = (fp - d) // 2, (fp + d) // 2
+    ev = odd.sum(axis=1) == 0
+    val = np.where(ev, coarse[cell_index(nc, a[:, 0], a[:, 1], a[:, 2])],
+                   0.5 * coarse[cell_index(nc, a[:, 0], a[:, 1], a[:, 2])] + 0.5 * coarse[cell_index(nc, b[:, 0], b[:, 1], b[:, 2])])
+    out[cell_index(nf, fp[:, 0], fp[:, 1], fp[:, 2])] += _cell_class_weight(fp, nf, nc14) * val
+    return out

@@ -1,0 +1,65 @@
+"""ctypes access to oracle/_ref/libhyteg_ref.so: the reference's own generated P1 kernels and
+FEniCS P1 diffusion form, compiled from the reference sources by oracle/Makefile.
+
+TEST INFRASTRUCTURE ONLY (pins the oracle; CPU baseline of bench.py).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PATH = os.path.join(HERE, "_ref", "libhyteg_ref.so")
+_lib = None
+
+
+def available():
+    return os.path.exists(PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(PATH)
+        dp = C.POINTER(C.c_double)
+        L.ref_cell_apply.argtypes = [dp, dp, C.c_int, dp]
+        L.ref_cell_apply_many.argtypes = [C.c_int, C.POINTER(dp), C.POINTER(dp), C.c_int, dp, C.c_int]
+        L.ref_restrict.argtypes = [dp, dp, C.c_int, dp]
+        L.ref_prolongate.argtypes = [dp, dp, C.c_int, dp]
+        L.ref_p1_diffusion_element.argtypes = [dp, dp]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def cell_apply(src_cell, level, stencil15):
+    dst = np.zeros_like(src_cell)
+    lib().ref_cell_apply(_p(dst), _p(np.ascontiguousarray(src_cell)), level, _p(np.ascontiguousarray(stencil15, dtype=np.float64)))
+    return dst
+
+
+def restrict(fine_cell, coarse_level, nc14):
+    n = 1 << coarse_level
+    coarse = np.zeros(((n + 3) * (n + 2) * (n + 1)) // 6)
+    lib().ref_restrict(_p(coarse), _p(np.ascontiguousarray(fine_cell)), coarse_level, _p(np.asarray(nc14, dtype=np.float64)))
+    return coarse
+
+
+def prolongate(coarse_cell, coarse_level, nc14, fine_init=None):
+    n = 2 << coarse_level
+    fine = np.zeros(((n + 3) * (n + 2) * (n + 1)) // 6) if fine_init is None else np.array(fine_init, dtype=np.float64)
+    lib().ref_prolongate(_p(np.ascontiguousarray(coarse_cell)), _p(fine), coarse_level, _p(np.asarray(nc14, dtype=np.float64)))
+    return fine
+
+
+def p1_diffusion_element(X):
+    """X: (4, 3) vertex coordinates -> 4x4 element matrix from the FEniCS form."""
+    A = np.zeros(16)
+    lib().ref_p1_diffusion_element(_p(np.ascontiguousarray(X, dtype=np.float64).ravel()), _p(A))
+    return A.reshape(4, 4)

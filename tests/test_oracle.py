@@ -1,0 +1,186 @@
+"""CPU tests: the oracle against the reference's own kernels (golden vectors and, where built, the
+compiled reference library) and against the reference tests' known answers."""
+
+import os
+
+import numpy as np
+import pytest
+
+from oracle import hyteg_oracle as O
+from oracle import ref as R
+from tests import meshes as M
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "ref_p1_kernels.npz")
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return np.load(GOLDEN)
+
+
+def test_golden_element_matrix(golden):
+    K = O.p1_laplace_element(golden["elem_X"])
+    np.testing.assert_allclose(K, golden["elem_A"], rtol=0, atol=1e-14)
+
+
+def test_golden_cell_apply(golden):
+    L = int(golden["apply_level"])
+    out = O.cell_stencil_apply(golden["apply_src"], L, golden["apply_stencil"])
+    np.testing.assert_allclose(out, golden["apply_dst"], rtol=0, atol=1e-14)
+
+
+def test_golden_restrict(golden):
+    L = int(golden["apply_level"])
+    out = O.cell_restrict(golden["restrict_fine"], L - 1, golden["nc14"])
+    np.testing.assert_allclose(out, golden["restrict_coarse"], rtol=0, atol=1e-14)
+
+
+def test_golden_prolongate(golden):
+    L = int(golden["apply_level"])
+    out = O.cell_prolongate(golden["prolong_coarse"], L - 1, golden["nc14"])
+    np.testing.assert_allclose(out, golden["prolong_fine"], rtol=0, atol=1e-14)
+
+
+def _nc14(m, c):
+    return ([len(m.e_cells[e]) for e in m.cell_edges[c]] + [len(m.f_cells[f]) for f in m.cell_faces[c]]
+            + [len(m.v_cells[v]) for v in m.cells[c]])
+
+
+@pytest.mark.parametrize("name", ["cube_6", "octahedron_8", "pyramid_4"])
+def test_global_operators_match_per_cell_kernels(name):
+    """Global A, R, P of the oracle equal the per-cell kernel steps plus additive communication."""
+    coords, tets = M.ALL[name]()
+    m = O.MacroMesh(coords, tets)
+    L = 3
+    op = O.P1ConstantLaplace(m, L - 1, L)
+    tr = O.Transfer(op)
+    fine, coarse = op.levels[L], op.levels[L - 1]
+    rng = np.random.default_rng(7)
+    x = np.zeros(fine.size)
+    x[fine.owned] = rng.uniform(-1, 1, fine.owned.size)
+    fine.sync(x)
+    fpts, cpts = O.tet_points(fine.n + 1), O.tet_points(coarse.n + 1)
+    tot = np.zeros(coarse.size)
+    for c in range(m.nC):
+        cell = x[fine.off_c[c] + O.cell_index(fine.n, fpts[:, 0], fpts[:, 1], fpts[:, 2])]
+        np.add.at(tot, coarse.owner(c, cpts[:, 0], cpts[:, 1], cpts[:, 2]), O.cell_restrict(cell, L - 1, _nc14(m, c)))
+    ro = tr.R[L] @ x
+    mask = coarse.owned_mask(O.ALL)
+    np.testing.assert_allclose(tot[mask], ro[mask], rtol=1e-13, atol=1e-13)
+    xc = np.zeros(coarse.size)
+    xc[coarse.owned] = rng.uniform(-1, 1, coarse.owned.size)
+    coarse.sync(xc)
+    tot = np.zeros(fine.size)
+    for c in range(m.nC):
+        cc = xc[coarse.off_c[c] + O.cell_index(coarse.n, cpts[:, 0], cpts[:, 1], cpts[:, 2])]
+        np.add.at(tot, fine.owner(c, fpts[:, 0], fpts[:, 1], fpts[:, 2]), O.cell_prolongate(cc, L - 1, _nc14(m, c)))
+    po = tr.P[L] @ xc
+    mask = fine.owned_mask(O.ALL)
+    np.testing.assert_allclose(tot[mask], po[mask], rtol=1e-13, atol=1e-13)
+
+
+@pytest.mark.skipif(not R.available(), reason="oracle/_ref not built")
+def test_assembled_apply_matches_reference_cell_kernel():
+    coords, tets = M.cube_6()
+    m = O.MacroMesh(coords, tets)
+    L = 4
+    op = O.P1ConstantLaplace(m, L, L)
+    lev = op.levels[L]
+    rng = np.random.default_rng(3)
+    x = np.zeros(lev.size)
+    x[lev.owned] = rng.uniform(-1, 1, lev.owned.size)
+    lev.sync(x)
+    y = op.A[L] @ x
+    pts = O.tet_points(lev.n + 1)
+    inner = (pts.min(axis=1) >= 1) & (pts.sum(axis=1) <= lev.n - 1)
+    for c in range(m.nC):
+        cell = x[lev.off_c[c] + O.cell_index(lev.n, pts[:, 0], pts[:, 1], pts[:, 2])]
+        p = lev.owner(c, np.array([2]), np.array([2]), np.array([2]))[0]
+        st = [op.A[L][p, lev.owner(c, np.array([2 + d[0]]), np.array([2 + d[1]]), np.array([2 + d[2]]))[0]]
+              for d in O.STENCIL15]
+        out = R.cell_apply(cell, L, st)
+        slots = lev.off_c[c] + O.cell_index(lev.n, pts[inner, 0], pts[inner, 1], pts[inner, 2])
+        np.testing.assert_allclose(out[inner], y[slots], rtol=1e-12, atol=1e-13)
+
+
+@pytest.mark.parametrize("name", sorted(M.ALL))
+@pytest.mark.parametrize("L", [2, 3])
+def test_laplace_annihilates_linear_functions(name, L):
+    """P1LaplaceOperator3DTest.cpp:41-127: A u = 0 for constant and linear u at inner DoFs (L2 < 2.8e-13)."""
+    coords, tets = M.ALL[name]()
+    m = O.MacroMesh(coords, tets)
+    op = O.P1ConstantLaplace(m, L, L)
+    lev = op.levels[L]
+    pts = O.tet_points(lev.n + 1)
+    for f in (lambda X: np.ones(len(X)), lambda X: 1.0 + 2 * X[:, 0] - 3 * X[:, 1] + 0.5 * X[:, 2]):
+        x = np.zeros(lev.size)
+        for c in range(m.nC):
+            x[lev.owner(c, pts[:, 0], pts[:, 1], pts[:, 2])] = f(lev.coords(c, pts[:, 0], pts[:, 1], pts[:, 2]))
+        y = np.zeros(lev.size)
+        op.apply(x, y, L, O.INNER)
+        mask = lev.owned_mask(O.INNER)
+        if mask.sum() == 0:
+            continue
+        assert np.sqrt(np.mean(y[mask] ** 2)) < 2.8e-13
+
+
+def test_restriction_is_prolongation_transpose():
+    coords, tets = M.octahedron_8()
+    m = O.MacroMesh(coords, tets)
+    op = O.P1ConstantLaplace(m, 2, 3)
+    tr = O.Transfer(op)
+    fi = np.flatnonzero(op.levels[3].owned_mask(O.ALL))
+    ci = np.flatnonzero(op.levels[2].owned_mask(O.ALL))
+    D = (tr.R[3] - tr.P[3].T).tocsr()[ci][:, fi]
+    assert abs(D).max() < 1e-15
+
+
+def test_chebyshev_polynomial_property():
+    """setupCoefficientsInternal: 1 - t p(t) = T_k((theta - t)/delta) / T_k(theta/delta)."""
+    for order in range(1, 6):
+        lo, hi = 0.3 * 2.2, 1.2 * 2.2
+        c = O.chebyshev_coefficients(order, lo, hi)
+        theta, delta = (hi + lo) / 2, (hi - lo) / 2
+        for t in np.linspace(0.1, 3.0, 7):
+            p = sum(ci * t ** i for i, ci in enumerate(c))
+            ref = np.polynomial.chebyshev.chebval((theta - t) / delta, [0] * order + [1]) / \
+                np.polynomial.chebyshev.chebval(theta / delta, [0] * order + [1])
+            assert abs((1 - t * p) - ref) < 1e-12
+
+
+def test_gmg_convergence_octahedron():
+    """P1GMG3DConvergenceTest shape check (there with Gauss-Seidel, bound 3.2e-2 per cycle): weighted-Jacobi
+    V(3,3) cycles converge at a rate below 0.2 per cycle on the octahedron."""
+    coords, tets = M.octahedron_8()
+    m = O.MacroMesh(coords, tets)
+    L = 3
+    op = O.P1ConstantLaplace(m, 0, L)
+    tr = O.Transfer(op)
+    rng = np.random.default_rng(0)
+    b = {l: np.zeros(op.levels[l].size) for l in range(L + 1)}
+    x = {l: np.zeros(op.levels[l].size) for l in range(L + 1)}
+    mask = op.levels[L].owned_mask(O.INNER)
+    b[L][mask] = rng.uniform(-1, 1, mask.sum())
+    g = O.GMG(op, tr, 0, L, pre=3, post=3)
+    r0 = O.residual_norm(op, x[L], b[L], L)
+    for _ in range(5):
+        g.solve(x, b, L)
+    r = O.residual_norm(op, x[L], b[L], L)
+    assert r / r0 < 0.2 ** 5
+
+
+def test_cg_solves_small_system():
+    coords, tets = M.pyramid_4()
+    m = O.MacroMesh(coords, tets)
+    L = 2
+    op = O.P1ConstantLaplace(m, L, L)
+    tr = O.Transfer(op) if False else None
+    lev = op.levels[L]
+    rng = np.random.default_rng(5)
+    b = np.zeros(lev.size)
+    mask = lev.owned_mask(O.INNER)
+    b[mask] = rng.uniform(-1, 1, mask.sum())
+    x = np.zeros(lev.size)
+    g = O.GMG(op, tr, L, L, cg_tol=1e-12)
+    g.cg(x, b, L)
+    assert O.residual_norm(op, x, b, L) / np.linalg.norm(b[mask]) < 1e-11
