@@ -53,6 +53,7 @@ class _GmgParams(C.Structure):
         ("cheb_order", C.c_int), ("cheb_upper_factor", C.c_double), ("cheb_lower_factor", C.c_double),
         ("cheb_power_iterations", C.c_int), ("coarse_max_iter", C.c_int),
         ("coarse_rtol", C.c_double), ("coarse_atol", C.c_double), ("use_graph", C.c_int),
+        ("coarse_fp64", C.c_int),
     ]
 
 
@@ -112,6 +113,8 @@ _SIGS = {
     "hyb_chebyshev_coefficients": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_void_p]),
     "hyb_cg_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
                                C.POINTER(C.c_int)]),
+    "hyb_mixed_solve": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                  C.c_double, C.c_void_p, C.POINTER(C.c_int)]),
     "hyb_residual_norm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32,
                                     C.POINTER(C.c_double)]),
 }
@@ -466,6 +469,15 @@ class GeometricMultigridSolver:
         hist = np.zeros(max_cycles + 1)
         done = C.c_int()
         _check(lib().hyb_gmg_solve_cycles(self.h, x.h, b.h, level, max_cycles, rtol, _ptr(hist), C.byref(done)))
+        return hist[: done.value + 1]
+
+    def mixed_solve(self, A, x, b, level, inner_dtype="float32", inner_cycles=1, max_outer=50, rtol=1e-8):
+        """Mixed-precision defect correction: FP64 x, b; inner cycles of this solver in `inner_dtype`."""
+        dt = _DTYPES[inner_dtype] if isinstance(inner_dtype, str) else int(inner_dtype)
+        hist = np.zeros(max_outer + 1)
+        done = C.c_int()
+        _check(lib().hyb_mixed_solve(self.h, dt, A.h, x.h, b.h, level, inner_cycles, max_outer, rtol, _ptr(hist),
+                                     C.byref(done)))
         return hist[: done.value + 1]
 
     def close(self):

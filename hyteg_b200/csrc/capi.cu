@@ -11,24 +11,81 @@
 #include <sstream>
 #include <stdexcept>
 
+// Handles are reference counted: functions, operators and solvers keep their context, mesh and
+// operator alive, so the caller may destroy handles in any order.
 struct hyb_ctx
 {
    hyb::Context c;
+   int          refs = 1;
+   ~hyb_ctx()
+   {
+      cudaStreamSynchronize( c.stream );
+      cudaFree( c.d_partials );
+      cudaFree( c.d_scalars );
+      cudaFree( c.d_error );
+      if ( c.aux ) cudaStreamSynchronize( c.aux ), cudaStreamDestroy( c.aux );
+      if ( c.ev_fork ) cudaEventDestroy( c.ev_fork );
+      if ( c.ev_join ) cudaEventDestroy( c.ev_join );
+      if ( c.own_stream ) cudaStreamDestroy( c.stream );
+   }
 };
 struct hyb_mesh
 {
    hyb::Mesh m;
+   int       refs = 1;
 };
+static void ctx_ref( hyb_ctx* c )
+{
+   if ( c ) ++c->refs;
+}
+static void ctx_unref( hyb_ctx* c )
+{
+   if ( c && --c->refs == 0 ) delete c;
+}
+static void mesh_ref( hyb::Mesh* m )
+{
+   if ( m ) ++static_cast< hyb_mesh* >( m->handle )->refs;
+}
+static void mesh_unref( hyb::Mesh* m )
+{
+   if ( !m ) return;
+   auto* h = static_cast< hyb_mesh* >( m->handle );
+   if ( --h->refs == 0 )
+   {
+      hyb_ctx* c = static_cast< hyb_ctx* >( m->owner_ctx );
+      delete h;
+      ctx_unref( c );
+   }
+}
 struct hyb_fn
 {
    hyb::Function f;
    hyb_ctx*      ctx = nullptr;
+   ~hyb_fn()
+   {
+      if ( ctx ) cudaStreamSynchronize( ctx->c.stream );
+      for ( void* p : f.data ) cudaFree( p );
+      f.data.clear();
+      mesh_unref( f.mesh );
+      ctx_unref( ctx );
+   }
 };
 struct hyb_op
 {
    hyb::Operator o;
    hyb_ctx*      ctx = nullptr;
+   int           refs = 1;
 };
+static void op_unref( hyb_op* o )
+{
+   if ( !o || --o->refs > 0 ) return;
+   hyb_ctx*   c = o->ctx;
+   hyb::Mesh* m = o->o.mesh;
+   cudaStreamSynchronize( c->c.stream );
+   delete o;
+   mesh_unref( m );
+   ctx_unref( c );
+}
 
 namespace hyb {
 std::vector< std::array< double, 3 > > g_unused;
@@ -101,6 +158,11 @@ int hyb_ctx_create( int device, void* stream, hyb_ctx** out )
       h->c.own_stream = true;
    }
    check_cuda( cudaMalloc( &h->c.d_scalars, 64 * sizeof( double ) ), "cudaMalloc(scalars)" );
+   check_cuda( cudaStreamCreateWithFlags( &h->c.aux, cudaStreamNonBlocking ), "cudaStreamCreate(aux)" );
+   check_cuda( cudaMalloc( &h->c.d_error, sizeof( int ) ), "cudaMalloc(error word)" );
+   check_cuda( cudaMemset( h->c.d_error, 0, sizeof( int ) ), "cudaMemset(error word)" );
+   check_cuda( cudaEventCreateWithFlags( &h->c.ev_fork, cudaEventDisableTiming ), "cudaEventCreate" );
+   check_cuda( cudaEventCreateWithFlags( &h->c.ev_join, cudaEventDisableTiming ), "cudaEventCreate" );
    *out = h;
    HYB_CATCH
 }
@@ -108,12 +170,7 @@ int hyb_ctx_create( int device, void* stream, hyb_ctx** out )
 int hyb_ctx_destroy( hyb_ctx* ctx )
 {
    HYB_TRY
-   if ( !ctx ) return HYB_OK;
-   cudaStreamSynchronize( ctx->c.stream );
-   cudaFree( ctx->c.d_partials );
-   cudaFree( ctx->c.d_scalars );
-   if ( ctx->c.own_stream ) cudaStreamDestroy( ctx->c.stream );
-   delete ctx;
+   ctx_unref( ctx );
    HYB_CATCH
 }
 
@@ -122,6 +179,14 @@ int hyb_ctx_synchronize( hyb_ctx* ctx )
    HYB_TRY
    require( ctx, "ctx is NULL" );
    check_cuda( cudaStreamSynchronize( ctx->c.stream ), "cudaStreamSynchronize" );
+   int e = 0;
+   check_cuda( cudaMemcpy( &e, ctx->c.d_error, sizeof( int ), cudaMemcpyDeviceToHost ), "error word readback" );
+   if ( e )
+   {
+      cudaMemset( ctx->c.d_error, 0, sizeof( int ) );
+      g_err = "a device-side bounded wait ran out (shared-memory staging did not complete)";
+      return HYB_ETIMEOUT;
+   }
    HYB_CATCH
 }
 
@@ -147,8 +212,10 @@ static int make_mesh( hyb_ctx* ctx, const std::vector< std::array< double, 3 > >
 {
    require( out != nullptr, "out is NULL" );
    require( !tets.empty(), "mesh without tetrahedra" );
-   auto* h  = new hyb_mesh();
-   h->m.ctx = ctx ? &ctx->c : nullptr;
+   auto* h        = new hyb_mesh();
+   h->m.ctx       = ctx ? &ctx->c : nullptr;
+   h->m.handle    = h;
+   h->m.owner_ctx = ctx;
    try
    {
       h->m.topo.build( coords, tets );
@@ -157,6 +224,7 @@ static int make_mesh( hyb_ctx* ctx, const std::vector< std::array< double, 3 > >
       delete h;
       throw;
    }
+   ctx_ref( ctx );
    *out = h;
    return HYB_OK;
 }
@@ -199,7 +267,7 @@ int hyb_mesh_create_gmsh( hyb_ctx* ctx, const char* path, hyb_mesh** out )
 int hyb_mesh_destroy( hyb_mesh* mesh )
 {
    HYB_TRY
-   delete mesh;
+   if ( mesh ) mesh_unref( &mesh->m );
    HYB_CATCH
 }
 
@@ -309,6 +377,8 @@ int hyb_fn_create( hyb_ctx* ctx, hyb_mesh* mesh, int dtype, int min_level, int m
    h->f.dtype = dtype;
    h->f.minL  = min_level;
    h->f.maxL  = max_level;
+   ctx_ref( ctx );
+   mesh_ref( &mesh->m );
    try
    {
       for ( int L = min_level; L <= max_level; ++L )
@@ -331,7 +401,6 @@ int hyb_fn_create( hyb_ctx* ctx, hyb_mesh* mesh, int dtype, int min_level, int m
 int hyb_fn_destroy( hyb_fn* fn )
 {
    HYB_TRY
-   if ( fn ) cudaStreamSynchronize( fn->ctx->c.stream );
    delete fn;
    HYB_CATCH
 }
@@ -613,12 +682,14 @@ int hyb_op_create( hyb_ctx* ctx, hyb_mesh* mesh, int kind, int min_level, int ma
    h->o.kind = kind;
    h->o.minL = min_level;
    h->o.maxL = max_level;
+   ctx_ref( ctx );
+   mesh_ref( &mesh->m );
    try
    {
       for ( int L = min_level; L <= max_level; ++L ) build_operator_level( &h->o, L );
    } catch ( ... )
    {
-      delete h;
+      op_unref( h );
       throw;
    }
    *out = h;
@@ -628,8 +699,7 @@ int hyb_op_create( hyb_ctx* ctx, hyb_mesh* mesh, int kind, int min_level, int ma
 int hyb_op_destroy( hyb_op* op )
 {
    HYB_TRY
-   if ( op ) cudaStreamSynchronize( op->ctx->c.stream );
-   delete op;
+   op_unref( op );
    HYB_CATCH
 }
 
@@ -773,6 +843,8 @@ static hyb_fn* new_fn( hyb_ctx* ctx, Mesh* m, int dtype, int minL, int maxL )
    h->f.dtype = dtype;
    h->f.minL  = minL;
    h->f.maxL  = maxL;
+   ctx_ref( ctx );
+   mesh_ref( m );
    for ( int L = minL; L <= maxL; ++L )
    {
       void* p = nullptr;
@@ -896,6 +968,13 @@ struct hyb_gmg
    hyb_fn*                              z0    = nullptr;  // Chebyshev temporaries
    hyb_fn*                              z1    = nullptr;
    hyb::CGState                         cg;
+   hyb::CGState                         cg64;   // FP64 coarse solve for low-precision hierarchies
+   hyb_fn*                              cgx64 = nullptr;
+   hyb_fn*                              cgb64 = nullptr;
+   // mixed-precision refinement temporaries (inner dtype r and c, fp64 residual)
+   hyb_fn*                              mx_r = nullptr;
+   hyb_fn*                              mx_c = nullptr;
+   hyb_fn*                              mx_t = nullptr;
    std::vector< double >                radii;
    std::vector< std::vector< double > > coeff;
    std::vector< int >                   swaps;  // Jacobi swaps per level in the current cycle
@@ -915,6 +994,19 @@ struct hyb_gmg
       hyb_fn_destroy( cg.ap );
       hyb_fn_destroy( cg.r );
       cudaFree( cg.st );
+      hyb_fn_destroy( cg64.p );
+      hyb_fn_destroy( cg64.ap );
+      hyb_fn_destroy( cg64.r );
+      cudaFree( cg64.st );
+      hyb_fn_destroy( cgx64 );
+      hyb_fn_destroy( cgb64 );
+      hyb_fn_destroy( mx_r );
+      hyb_fn_destroy( mx_c );
+      hyb_fn_destroy( mx_t );
+      hyb_op*  o = op;
+      hyb_ctx* c = ctx;
+      op_unref( o );
+      ctx_unref( c );
    }
 };
 
@@ -938,6 +1030,16 @@ static void gmg_alloc( hyb_gmg* g, int dtype )
    g->cg.r  = new_fn( g->ctx, m, dtype, a, a );
    check_cuda( cudaMalloc( &g->cg.st, 16 * sizeof( double ) ), "cudaMalloc(cg state)" );
    check_cuda( cudaMemsetAsync( g->cg.st, 0, 16 * sizeof( double ), g->ctx->c.stream ), "cudaMemset" );
+   if ( dtype != F64 && g->p.coarse_fp64 )
+   {
+      g->cg64.p  = new_fn( g->ctx, m, F64, a, a );
+      g->cg64.ap = new_fn( g->ctx, m, F64, a, a );
+      g->cg64.r  = new_fn( g->ctx, m, F64, a, a );
+      g->cgx64   = new_fn( g->ctx, m, F64, a, a );
+      g->cgb64   = new_fn( g->ctx, m, F64, a, a );
+      check_cuda( cudaMalloc( &g->cg64.st, 16 * sizeof( double ) ), "cudaMalloc(cg state)" );
+      check_cuda( cudaMemsetAsync( g->cg64.st, 0, 16 * sizeof( double ), g->ctx->c.stream ), "cudaMemset" );
+   }
    g->dtype = dtype;
 }
 
@@ -992,7 +1094,17 @@ static void cycle_rec( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int L, int invoked, boo
    const int dt = x->f.dtype;
    if ( L == g->p.min_level )
    {
-      cg_run( op, g->cg, x, b, L, g->p.coarse_max_iter, g->p.coarse_rtol, g->p.coarse_atol, host_checks );
+      if ( g->cgx64 )
+      {
+         // coarse-grid solve in FP64 for a low-precision hierarchy
+         const int64_t cnt = x->f.mesh->level( L ).size;
+         launch_convert( &cx, cnt, F64, g->cgb64->f.ptr( L ), dt, b->f.ptr( L ) );
+         check_cuda( cudaMemsetAsync( g->cgx64->f.ptr( L ), 0, g->cgx64->f.bytes( L ), cx.stream ), "cudaMemset" );
+         cg_run( op, g->cg64, g->cgx64, g->cgb64, L, g->p.coarse_max_iter, g->p.coarse_rtol, g->p.coarse_atol, host_checks );
+         launch_convert( &cx, cnt, dt, x->f.ptr( L ), F64, g->cgx64->f.ptr( L ) );
+      }
+      else
+         cg_run( op, g->cg, x, b, L, g->p.coarse_max_iter, g->p.coarse_rtol, g->p.coarse_atol, host_checks );
       return;
    }
    const int pre = g->p.pre_smooth + g->p.smooth_increment * ( invoked - L );
@@ -1034,6 +1146,8 @@ static void run_cycle( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int L )
    }
    if ( !( g->gexec && g->g_x == x->f.ptr( L ) && g->g_b == b->f.ptr( L ) && g->g_level == L ) )
    {
+      // every lazily created device table must exist before the capture starts
+      prepare_device( &cx, g->op->o.mesh, &g->op->o, g->p.min_level, L );
       if ( g->gexec ) cudaGraphExecDestroy( g->gexec ), g->gexec = nullptr;
       cudaGraph_t graph;
       check_cuda( cudaStreamBeginCapture( cx.stream, cudaStreamCaptureModeThreadLocal ), "begin capture" );
@@ -1144,6 +1258,7 @@ int hyb_gmg_params_default( hyb_gmg_params* p )
    p->coarse_rtol           = 1e-14;
    p->coarse_atol           = 1e-16;
    p->use_graph             = 1;
+   p->coarse_fp64           = 1;
    HYB_CATCH
 }
 
@@ -1161,6 +1276,8 @@ int hyb_gmg_create( hyb_ctx* ctx, hyb_op* op, const hyb_gmg_params* params, hyb_
    auto* g = new hyb_gmg();
    g->ctx  = ctx;
    g->op   = op;
+   ctx_ref( ctx );
+   ++op->refs;
    g->p    = p;
    g->swaps.assign( p.max_level - p.min_level + 1, 0 );
    *out = g;
@@ -1312,3 +1429,73 @@ int hyb_residual_norm( hyb_op* op, hyb_fn* x, hyb_fn* b, hyb_fn* tmp, int level,
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// mixed-precision iterative refinement
+// =============================================================================================
+namespace hyb {
+
+static double count_owned( Mesh* m, int L, uint32_t flag )
+{
+   const P1Level&  P = m->level( L );
+   const Topology& t = m->topo;
+   double          n = 0;
+   for ( const auto& tk : P.tasks )
+   {
+      const int b  = tk[0];
+      uint32_t  bc = b < t.nV ? t.bc( t.flag_v[b] ) : b < t.nV + t.nE ? t.bc( t.flag_e[b - t.nV] ) : t.bc( t.flag_f[b - t.nV - t.nE] );
+      if ( bc & flag ) n += 1;
+   }
+   for ( int c = 0; c < t.nC; ++c )
+      if ( t.bc( t.flag_c[c] ) & flag ) n += double( P.n_owned_cell );
+   return n;
+}
+
+}  // namespace hyb
+
+extern "C" int hyb_mixed_solve( hyb_gmg* g, int inner_dtype, hyb_op* op, hyb_fn* x, hyb_fn* b, int level, int inner_cycles,
+                                int max_outer, double rtol, double* res_history, int* outer_iters )
+{
+   HYB_TRY
+   require( g && op && x && b, "NULL argument" );
+   require( inner_dtype == F32 || inner_dtype == F16 || inner_dtype == F64, "unknown inner dtype" );
+   require( x->f.dtype == F64 && b->f.dtype == F64, "x and b must hold FP64 values" );
+   require( g->op == op || g->op->o.mesh == op->o.mesh, "inner solver lives on another mesh" );
+   require( inner_cycles >= 1 && max_outer >= 0, "invalid iteration counts" );
+   check_op_fn( op, x, level );
+   check_op_fn( op, b, level );
+   require( level >= g->p.min_level && level <= g->p.max_level, "level outside the inner multigrid range" );
+   Mesh* m = op->o.mesh;
+   if ( !g->mx_r || g->mx_r->f.maxL < level || g->mx_r->f.dtype != inner_dtype )
+   {
+      hyb_fn_destroy( g->mx_r );
+      hyb_fn_destroy( g->mx_c );
+      hyb_fn_destroy( g->mx_t );
+      g->mx_r = new_fn( g->ctx, m, inner_dtype, g->p.min_level, level );
+      g->mx_c = new_fn( g->ctx, m, inner_dtype, g->p.min_level, level );
+      g->mx_t = new_fn( g->ctx, m, F64, level, level );
+   }
+   gmg_prepare( g, g->mx_c, g->mx_r, level );
+   Context&      cx    = g->ctx->c;
+   const int64_t cnt   = m->level( level ).size;
+   const double  nown  = std::max( 1.0, count_owned( m, level, kSolveFlag ) );
+   double        r0    = residual_norm( op, x, b, g->mx_t, level, kSolveFlag );
+   double        rn    = r0;
+   if ( res_history ) res_history[0] = r0;
+   int k = 0;
+   for ( ; k < max_outer; ++k )
+   {
+      if ( r0 == 0.0 || rn / r0 < rtol ) break;
+      // r (fp64, written by residual_norm into mx_t) -> inner precision, scaled to unit RMS
+      const double s = std::sqrt( nown ) / rn;
+      launch_convert( &cx, cnt, inner_dtype, g->mx_r->f.ptr( level ), F64, g->mx_t->f.ptr( level ), s );
+      check_cuda( cudaMemsetAsync( g->mx_c->f.ptr( level ), 0, g->mx_c->f.bytes( level ), cx.stream ), "cudaMemset" );
+      for ( int c = 0; c < inner_cycles; ++c ) run_cycle( g, g->mx_c, g->mx_r, level );
+      launch_axpy_to_f64( &cx, cnt, (double*) x->f.ptr( level ), inner_dtype, g->mx_c->f.ptr( level ), 1.0 / s );
+      rn = residual_norm( op, x, b, g->mx_t, level, kSolveFlag );
+      if ( res_history ) res_history[k + 1] = rn;
+      if ( !std::isfinite( rn ) ) throw std::runtime_error( "mixed-precision refinement diverged: residual is not finite" );
+   }
+   if ( outer_iters ) *outer_iters = k;
+   HYB_CATCH
+}

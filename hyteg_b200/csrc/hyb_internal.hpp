@@ -113,6 +113,13 @@ struct P1Level {
    std::vector< Incidence >     inc;
    std::vector< std::array< int, 4 > > tasks;  // {b, i, j, 0}: owned DoFs of boundary primitives
    std::vector< std::array< int, 2 > > rows;   // (y, z) of cell interior rows
+   // y-marching work items of the cell stencil sweep: (z, x0, y_first, y_last); a warp covers
+   // x0..x0+31 of slice z and marches over rows y_first..y_last
+   std::vector< std::array< int, 4 > > march;
+   // shared-memory staged sweep: tiles (z, y_first, y_last) covering the interior rows of a slice,
+   // and the largest shared-memory stage (bytes, FP64) any tile needs
+   std::vector< std::array< int, 4 > > tiles;
+   int                                 tile_rows = 0;
    int64_t n_owned_cell = 0;
    // device copies
    int64_t*   d_off       = nullptr;  // all primitives
@@ -120,6 +127,8 @@ struct P1Level {
    Incidence* d_inc       = nullptr;
    int4*      d_tasks     = nullptr;
    int2*      d_rows      = nullptr;
+   int4*      d_march     = nullptr;
+   int4*      d_tiles     = nullptr;
    uint8_t*   d_bc        = nullptr;  // bc type per primitive (v, e, f, c order)
    int8_t*    d_bkind     = nullptr;  // 0 vertex, 1 edge, 2 face per boundary primitive
    float*     d_ncell_cls = nullptr;  // per cell, per class: number of macro-cells around the sub-primitive
@@ -129,6 +138,8 @@ struct Context;
 
 struct Mesh {
    Context*                                  ctx = nullptr;
+   void*                                     handle    = nullptr;  // owning C-ABI handle (reference count)
+   void*                                     owner_ctx = nullptr;  // C-ABI context handle the mesh holds
    Topology                                  topo;
    std::map< int, std::unique_ptr< P1Level > > levels;
    P1Level&                                  level( int L );
@@ -142,7 +153,6 @@ struct Function {
    std::vector< void* > data;  // device buffer per level (index L - minL)
    void*                ptr( int L ) const { return data.at( L - minL ); }
    size_t               bytes( int L ) const;
-   ~Function();
 };
 
 // constant-stencil operator (P1ConstantLaplaceOperator and friends)
@@ -170,11 +180,15 @@ struct Context {
    int          device = 0;
    cudaStream_t stream = nullptr;
    bool         own_stream = false;
+   cudaStream_t aux     = nullptr;  // second stream for the boundary half of each operation
+   cudaEvent_t  ev_fork = nullptr;
+   cudaEvent_t  ev_join = nullptr;
    std::string  last_error;
    // scratch for reductions
    double* d_partials = nullptr;
    int     partial_cap = 0;
    double* d_scalars = nullptr;  // small pool of device scalars
+   int*    d_error   = nullptr;  // device error word (bounded waits that gave up)
    int64_t launches = 0;         // kernel launches issued through this context
 };
 
@@ -230,11 +244,13 @@ struct PointArgs {
 
 void launch_point( Context* ctx, Mesh* m, int L, int dtype, const PointArgs& a );
 void launch_flat_lincomb( Context* ctx, int64_t count, int dtype, void* dst, int nsrc, const void* const* srcs, const double* scal );
-void launch_convert( Context* ctx, int64_t count, int dst_dtype, void* dst, int src_dtype, const void* src );
+void launch_convert( Context* ctx, int64_t count, int dst_dtype, void* dst, int src_dtype, const void* src, double scale = 1.0 );
 // deterministic dot over owned flagged DoFs -> *out (device)
 void launch_dot( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const void* a, const void* b, double* out );
 void launch_restrict( Context* ctx, Mesh* m, int Lfine, int dtype, uint32_t flag, const void* fine, void* coarse );
 void launch_prolongate( Context* ctx, Mesh* m, int Lcoarse, int dtype, uint32_t flag, const void* coarse, void* fine, int add );
+void launch_axpy_to_f64( Context* ctx, int64_t count, double* x, int src_dtype, const void* c, double a );
+void prepare_device( Context* ctx, Mesh* m, Operator* op, int minL, int maxL );
 void launch_cg_scalar( Context* ctx, double* state, int stage, double rtol, double atol );
 
 // host helpers

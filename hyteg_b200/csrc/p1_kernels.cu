@@ -15,7 +15,9 @@
 #include "hyb_internal.hpp"
 
 #include <cstdio>
+#include <cstdlib>
 #include <stdexcept>
+#include <string>
 
 namespace hyb {
 
@@ -37,6 +39,25 @@ static void ensure_constants()
    check_cuda( cudaMemcpyToSymbol( c_mask_to_cls, m2c, sizeof( m2c ) ), "constants(classes)" );
    g_const_ready = true;
 }
+
+// Cell-interior and boundary-primitive kernels of one operation write disjoint slots, so the
+// boundary kernel runs on an auxiliary stream forked from (and joined back into) the context stream.
+struct Fork
+{
+   Context* c;
+   explicit Fork( Context* ctx )
+   : c( ctx )
+   {
+      check_cuda( cudaEventRecord( c->ev_fork, c->stream ), "fork record" );
+      check_cuda( cudaStreamWaitEvent( c->aux, c->ev_fork, 0 ), "fork wait" );
+   }
+   cudaStream_t aux() const { return c->aux; }
+   ~Fork()
+   {
+      cudaEventRecord( c->ev_join, c->aux );
+      cudaStreamWaitEvent( c->stream, c->ev_join, 0 );
+   }
+};
 
 template < typename T >
 struct AccT
@@ -84,6 +105,11 @@ struct LevelView
    const uint8_t*   cell_bc;  // bc + nB
    const int8_t*    bkind;
    const float*     ncell_cls;
+   int              nmarch;
+   const int4*      march;
+   int              ntiles;
+   const int4*      tiles;
+   const std::vector< std::array< int, 4 > >* host_tiles;
 };
 
 template < typename A >
@@ -112,6 +138,11 @@ static LevelView make_view( Mesh* m, int L )
    v.cell_bc   = P.d_bc + P.nB;
    v.bkind     = P.d_bkind;
    v.ncell_cls = P.d_ncell_cls;
+   v.nmarch     = int( P.march.size() );
+   v.march      = P.d_march;
+   v.ntiles     = int( P.tiles.size() );
+   v.tiles      = P.d_tiles;
+   v.host_tiles = &P.tiles;
    return v;
 }
 
@@ -204,6 +235,307 @@ __global__ void __launch_bounds__( 256 ) k_cell_stencil( LevelView v, OpView< A 
    }
 }
 
+
+// y-marching cell sweep: a warp owns x0..x0+31 of slice z and walks the rows y_first..y_last.  The
+// rows (y-1, y, y+1) of slice z, (y-1, y) of slice z+1 and (y, y+1) of slice z-1 roll through
+// registers, so each step loads three new rows (x-1, x, x+1 per lane; neighbours hit L1) instead
+// of fifteen values per point.
+template < typename T, typename A >
+struct Row3
+{
+   A m, o, p;
+};
+
+template < typename T, typename A >
+__device__ __forceinline__ Row3< T, A > load_row( const T* s, int n, int yy, int zz, int x )
+{
+   const int64_t rb  = cidx( n, 0, yy, zz );
+   const int     len = n - yy - zz;  // last valid x of the row
+   Row3< T, A >  r;
+   r.m = ( x - 1 <= len ) ? A( ldv( s + rb + x - 1 ) ) : A( 0 );
+   r.o = ( x <= len ) ? A( ldv( s + rb + x ) ) : A( 0 );
+   r.p = ( x + 1 <= len ) ? A( ldv( s + rb + x + 1 ) ) : A( 0 );
+   return r;
+}
+
+template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( 256 ) k_cell_march( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
+                                                        const T* __restrict__ v1, T* v2, T* dst, A a0, A a1 )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int item = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   if ( item >= v.nmarch ) return;
+   if ( !( v.cell_bc[c] & flag ) ) return;
+   const int4    it   = v.march[item];
+   const int     z = it.x, x = it.y + lane, ya = it.z, yb = it.w, n = v.n;
+   const int64_t base = v.cell_off[c];
+   const T*      s    = src + base;
+   const A*      W    = o.W + size_t( c ) * kNumClasses * kNumDirs;
+   const A w0 = W[0], wW = W[1], wE = W[2], wS = W[3], wN = W[4], wB = W[5], wT = W[6], wNW = W[7], wSE = W[8], wTW = W[9],
+           wBE = W[10], wTS = W[11], wBN = W[12], wTSE = W[13], wBNW = W[14];
+   const A invd = o.invd_c[c];
+   Row3< T, A > cm = load_row< T, A >( s, n, ya - 1, z, x );
+   Row3< T, A > c0 = load_row< T, A >( s, n, ya, z, x );
+   Row3< T, A > tm = load_row< T, A >( s, n, ya - 1, z + 1, x );
+   Row3< T, A > b0 = load_row< T, A >( s, n, ya, z - 1, x );
+#pragma unroll 2
+   for ( int y = ya; y <= yb; ++y )
+   {
+      const Row3< T, A > cp = load_row< T, A >( s, n, y + 1, z, x );
+      const Row3< T, A > t0 = load_row< T, A >( s, n, y, z + 1, x );
+      const Row3< T, A > bp = load_row< T, A >( s, n, y + 1, z - 1, x );
+      if ( x + y + z <= n - 1 )
+      {
+         A acc = w0 * c0.o;
+         acc += wW * c0.m;
+         acc += wE * c0.p;
+         acc += wS * cm.o;
+         acc += wN * cp.o;
+         acc += wB * b0.o;
+         acc += wT * t0.o;
+         acc += wNW * cp.m;
+         acc += wSE * cm.p;
+         acc += wTW * t0.m;
+         acc += wBE * b0.p;
+         acc += wTS * tm.o;
+         acc += wBN * bp.o;
+         acc += wTSE * tm.p;
+         acc += wBNW * bp.m;
+         stencil_epilogue< T, A, OP >( base + cidx( n, x, y, z ), acc, invd, src, v1, v2, dst, a0, a1 );
+      }
+      cm = c0;
+      c0 = cp;
+      tm = t0;
+      b0 = bp;
+   }
+}
+
+
+// ---------------------------------------------------------------------------------------------
+// Shared-memory staged cell sweep (cp.async.bulk + mbarrier, two stages).
+//
+// A tile is TY interior rows y_first..y_last of slice z of one macro-cell.  Its input lives in three
+// contiguous ranges of the cell array: rows y_first-1..y_last+1 of slice z, rows y_first-1..y_last of
+// slice z+1 and rows y_first..y_last+1 of slice z-1.  One thread issues the three bulk copies of the
+// next tile into the other stage while the block computes the current one; every thread owns one
+// x (or a few) and marches over the tile's rows, rolling the rows through registers and reading
+// three new rows per step from shared memory.  Bytes in flight no longer depend on registers.
+// Each wait on an mbarrier is bounded; if it runs out the block records an error and returns.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr( const void* p ) { return uint32_t( __cvta_generic_to_shared( p ) ); }
+
+__device__ __forceinline__ void mbar_init( uint64_t* bar, uint32_t count )
+{
+   asm volatile( "mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"( smem_addr( bar ) ), "r"( count ) : "memory" );
+}
+
+__device__ __forceinline__ void mbar_expect_tx( uint64_t* bar, uint32_t bytes )
+{
+   asm volatile( "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"( smem_addr( bar ) ), "r"( bytes ) : "memory" );
+}
+
+__device__ __forceinline__ bool mbar_try_wait( uint64_t* bar, uint32_t parity )
+{
+   uint32_t ok;
+   asm volatile( "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"( ok )
+                 : "r"( smem_addr( bar ) ), "r"( parity )
+                 : "memory" );
+   return ok != 0;
+}
+
+__device__ __forceinline__ void bulk_copy_g2s( void* dst, const void* src, uint32_t bytes, uint64_t* bar )
+{
+   asm volatile( "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"( smem_addr( dst ) ),
+                 "l"( src ), "r"( bytes ), "r"( smem_addr( bar ) )
+                 : "memory" );
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile( "fence.proxy.async.shared::cta;" ::: "memory" ); }
+
+// element range [first, end) of rows r0..r1 of slice zz, widened to 16-byte boundaries
+struct TileRange
+{
+   int64_t first, end;
+};
+
+template < typename T >
+__host__ __device__ __forceinline__ TileRange tile_range( int n, int r0, int r1, int zz )
+{
+   constexpr int64_t al = 16 / sizeof( T );
+   const int64_t     a  = cidx( n, 0, r0, zz );
+   const int64_t     b  = cidx( n, 0, r1 + 1, zz );
+   return TileRange{ a / al * al, ( b + al - 1 ) / al * al };
+}
+
+constexpr int kTmaThreads = 256;
+constexpr int kSpinLimit  = 1 << 22;
+
+template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( kTmaThreads ) k_cell_tma( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
+                                                             const T* __restrict__ v1, T* v2, T* dst, A a0, A a1, int ntiles,
+                                                             int nC, int64_t stage_elems, const int4* __restrict__ tiles, int* err )
+{
+   extern __shared__ __align__( 128 ) unsigned char smem_raw[];
+   __shared__ uint64_t bars[2];
+   T*                  stage[2] = { reinterpret_cast< T* >( smem_raw ), reinterpret_cast< T* >( smem_raw ) + stage_elems };
+   const int           tid = threadIdx.x, n = v.n;
+   const int           total = ntiles * nC;
+   if ( tid == 0 )
+   {
+      mbar_init( &bars[0], 1 );
+      mbar_init( &bars[1], 1 );
+      asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
+   }
+   __syncthreads();
+
+   // issue the three bulk copies of work item t into stage st (thread 0 only)
+   auto issue = [&]( int t, int st ) {
+      const int     c  = t / ntiles;
+      const int4    tl = tiles[t % ntiles];
+      const int     z = tl.x, ya = tl.y, yb = tl.z;
+      const T*      g  = src + v.cell_off[c];
+      TileRange     rs = tile_range< T >( n, ya - 1, yb + 1, z );
+      TileRange     rt = tile_range< T >( n, ya - 1, yb, z + 1 );
+      TileRange     rb = tile_range< T >( n, ya, yb + 1, z - 1 );
+      const int64_t ns = rs.end - rs.first, nt = rt.end - rt.first, nb = rb.end - rb.first;
+      mbar_expect_tx( &bars[st], uint32_t( ( ns + nt + nb ) * sizeof( T ) ) );
+      bulk_copy_g2s( stage[st], g + rs.first, uint32_t( ns * sizeof( T ) ), &bars[st] );
+      bulk_copy_g2s( stage[st] + ns, g + rt.first, uint32_t( nt * sizeof( T ) ), &bars[st] );
+      bulk_copy_g2s( stage[st] + ns + nt, g + rb.first, uint32_t( nb * sizeof( T ) ), &bars[st] );
+   };
+   auto active = [&]( int t ) { return ( v.cell_bc[t / ntiles] & flag ) != 0; };
+
+   int t = blockIdx.x;
+   while ( t < total && !active( t ) ) t += gridDim.x;
+   if ( tid == 0 && t < total ) issue( t, 0 );
+   uint32_t phase[2] = { 0, 0 };
+   int      st       = 0;
+   while ( t < total )
+   {
+      int tn = t + gridDim.x;
+      while ( tn < total && !active( tn ) ) tn += gridDim.x;
+      if ( tid == 0 && tn < total )
+      {
+         fence_proxy_async();
+         issue( tn, st ^ 1 );
+      }
+      // bounded wait for the current stage
+      int  spins    = 0;
+      bool timedout = false;
+      while ( !mbar_try_wait( &bars[st], phase[st] ) )
+         if ( ++spins > kSpinLimit )
+         {
+            timedout = true;
+            break;
+         }
+      if ( __syncthreads_or( timedout ) )
+      {
+         if ( tid == 0 ) atomicExch( err, 1 );
+         // give copies still in flight a bounded chance to land before the block exits
+         for ( int k = 0; k < kSpinLimit && !mbar_try_wait( &bars[st ^ 1], phase[st ^ 1] ); ++k ) {}
+         return;
+      }
+      phase[st] ^= 1u;
+
+      // compute the tile from shared memory
+      {
+         const int     c    = t / ntiles;
+         const int4    tl   = tiles[t % ntiles];
+         const int     z = tl.x, ya = tl.y, yb = tl.z;
+         const int64_t base = v.cell_off[c];
+         TileRange     rs   = tile_range< T >( n, ya - 1, yb + 1, z );
+         TileRange     rt   = tile_range< T >( n, ya - 1, yb, z + 1 );
+         TileRange     rb   = tile_range< T >( n, ya, yb + 1, z - 1 );
+         const T*      S    = stage[st] - rs.first;
+         const T*      Tt   = stage[st] + ( rs.end - rs.first ) - rt.first;
+         const T*      B    = stage[st] + ( rs.end - rs.first ) + ( rt.end - rt.first ) - rb.first;
+         const A*      W    = o.W + size_t( c ) * kNumClasses * kNumDirs;
+         const A w0 = W[0], wW = W[1], wE = W[2], wS = W[3], wN = W[4], wB = W[5], wT = W[6], wNW = W[7], wSE = W[8],
+                 wTW = W[9], wBE = W[10], wTS = W[11], wBN = W[12], wTSE = W[13], wBNW = W[14];
+         const A invd = o.invd_c[c];
+         for ( int x = 1 + tid; x <= n - 1 - z - ya; x += kTmaThreads )
+         {
+            auto rd = [&]( const T* R, int yy, int zz, Row3< T, A >& r ) {
+               const T* p = R + cidx( n, x, yy, zz );
+               r.m        = A( p[-1] );
+               r.o        = A( p[0] );
+               r.p        = A( p[1] );
+            };
+            Row3< T, A > cm, c0, tm, b0, cp, t0, bp;
+            rd( S, ya - 1, z, cm );
+            rd( S, ya, z, c0 );
+            rd( Tt, ya - 1, z + 1, tm );
+            rd( B, ya, z - 1, b0 );
+            for ( int y = ya; y <= yb && x + y + z <= n - 1; ++y )
+            {
+               rd( S, y + 1, z, cp );
+               rd( Tt, y, z + 1, t0 );
+               rd( B, y + 1, z - 1, bp );
+               A acc = w0 * c0.o;
+               acc += wW * c0.m;
+               acc += wE * c0.p;
+               acc += wS * cm.o;
+               acc += wN * cp.o;
+               acc += wB * b0.o;
+               acc += wT * t0.o;
+               acc += wNW * cp.m;
+               acc += wSE * cm.p;
+               acc += wTW * t0.m;
+               acc += wBE * b0.p;
+               acc += wTS * tm.o;
+               acc += wBN * bp.o;
+               acc += wTSE * tm.p;
+               acc += wBNW * bp.m;
+               stencil_epilogue< T, A, OP >( base + cidx( n, x, y, z ), acc, invd, src, v1, v2, dst, a0, a1 );
+               cm = c0;
+               c0 = cp;
+               tm = t0;
+               b0 = bp;
+            }
+         }
+      }
+      __syncthreads();  // every thread is done with stage st before it is refilled
+      st ^= 1;
+      t = tn;
+   }
+}
+
+static int cell_kernel_variant()
+{
+   static int v = -1;
+   if ( v < 0 )
+   {
+      const char* e = getenv( "HYB_CELL_KERNEL" );
+      v             = ( e && std::string( e ) == "rows" ) ? 0 : ( e && std::string( e ) == "march" ) ? 1 : 2;
+   }
+   return v;
+}
+
+
+// Stencil of one position class at cell-local (x, y, z): the 15 directions are unrolled with the
+// seven row bases computed once, so all loads of a point are independent and in flight together.
+template < typename T, typename A >
+__device__ __forceinline__ A class_stencil( const T* s, const A* W, uint16_t mask, int n, int x, int y, int z )
+{
+   const int64_t r00 = cidx( n, 0, y, z );
+   const int64_t rm0 = y > 0 ? cidx( n, 0, y - 1, z ) : 0;
+   const int64_t rp0 = y + z < n ? cidx( n, 0, y + 1, z ) : 0;
+   const int64_t r0m = z > 0 ? cidx( n, 0, y, z - 1 ) : 0;
+   const int64_t r0p = y + z < n ? cidx( n, 0, y, z + 1 ) : 0;
+   const int64_t rmp = ( y > 0 && y + z <= n ) ? cidx( n, 0, y - 1, z + 1 ) : 0;
+   const int64_t rpm = ( z > 0 && y + z <= n ) ? cidx( n, 0, y + 1, z - 1 ) : 0;
+   const int64_t idx[kNumDirs] = { r00 + x,     r00 + x - 1, r00 + x + 1, rm0 + x,     rp0 + x,
+                                   r0m + x,     r0p + x,     rp0 + x - 1, rm0 + x + 1, r0p + x - 1,
+                                   r0m + x + 1, rmp + x,     rpm + x,     rmp + x + 1, rpm + x - 1 };
+   A acc = A( 0 );
+#pragma unroll
+   for ( int d = 0; d < kNumDirs; ++d )
+      if ( mask & ( 1u << d ) ) acc += W[d] * A( ldv( s + idx[d] ) );
+   return acc;
+}
+
 template < typename T, typename A, int OP >
 __global__ void __launch_bounds__( 256 ) k_bnd_stencil( LevelView v, OpView< A > o, uint32_t flag, int copy_unflagged,
                                                          const T* __restrict__ src, const T* __restrict__ v1, T* v2, T* dst,
@@ -227,14 +559,8 @@ __global__ void __launch_bounds__( 256 ) k_bnd_stencil( LevelView v, OpView< A >
       const Incidence I = v.inc[q];
       int             x, y, z;
       inc_point( I, n, i, j, x, y, z );
-      const T*       s    = src + v.cell_off[I.cell];
-      const A*       W    = o.W + ( size_t( I.cell ) * kNumClasses + I.cls ) * kNumDirs;
-      const uint16_t mask = c_cls_mask[I.cls];
-      A              part = A( 0 );
-      for ( int d = 0; d < kNumDirs; ++d )
-         if ( mask & ( 1u << d ) )
-            part += W[d] * A( ldv( s + cidx( n, x + c_dirs[d][0], y + c_dirs[d][1], z + c_dirs[d][2] ) ) );
-      acc += part;
+      acc += class_stencil< T, A >( src + v.cell_off[I.cell], o.W + ( size_t( I.cell ) * kNumClasses + I.cls ) * kNumDirs,
+                                    c_cls_mask[I.cls], n, x, y, z );
    }
    const A invd = o.invd_b[b];
    if constexpr ( OP == OP_APPLY ) write_through( v, dst, b, i, j, owner, acc );
@@ -260,7 +586,44 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
    const T* v1  = (const T*) a.v1;
    T*       v2  = (T*) a.v2;
    T*       dst = (T*) a.dst;
-   if ( v.nrows > 0 && nC > 0 )
+   Fork     fk( ctx );
+   if ( cell_kernel_variant() == 2 && v.n >= 32 && v.ntiles > 0 && nC > 0 )
+   {
+      // stage size: largest tile of this level (elements of T)
+      int64_t stage = 0;
+      for ( const auto& tl : *v.host_tiles )
+      {
+         const auto rs = tile_range< T >( v.n, tl[1] - 1, tl[2] + 1, tl[0] );
+         const auto rt = tile_range< T >( v.n, tl[1] - 1, tl[2], tl[0] + 1 );
+         const auto rb = tile_range< T >( v.n, tl[1], tl[2] + 1, tl[0] - 1 );
+         stage         = std::max( stage, ( rs.end - rs.first ) + ( rt.end - rt.first ) + ( rb.end - rb.first ) );
+      }
+      const size_t smem = size_t( 2 * stage ) * sizeof( T );
+      static int   s_sms = 0, s_set = 0;
+      static size_t s_smem_set = 0;
+      if ( !s_sms ) check_cuda( cudaDeviceGetAttribute( &s_sms, cudaDevAttrMultiProcessorCount, 0 ), "device attribute" );
+      if ( smem > s_smem_set )
+      {
+         check_cuda( cudaFuncSetAttribute( k_cell_tma< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize, int( smem ) ),
+                     "cudaFuncSetAttribute(smem)" );
+         s_smem_set = smem;
+      }
+      (void) s_set;
+      int per_sm = 0;
+      check_cuda( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, k_cell_tma< T, A, OP >, kTmaThreads, smem ), "occupancy" );
+      const int total = v.ntiles * nC;
+      const int grid  = std::max( 1, std::min( total, std::max( 1, per_sm ) * s_sms ) );
+      k_cell_tma< T, A, OP ><<< grid, kTmaThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ),
+                                                                          v.ntiles, nC, stage, v.tiles, ctx->d_error );
+      ++ctx->launches;
+   }
+   else if ( cell_kernel_variant() >= 1 && v.nmarch > 0 && nC > 0 )
+   {
+      dim3 grid( ( v.nmarch + 7 ) / 8, nC );
+      k_cell_march< T, A, OP ><<< grid, 256, 0, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ) );
+      ++ctx->launches;
+   }
+   else if ( v.nrows > 0 && nC > 0 )
    {
       dim3 grid( ( v.nrows + 7 ) / 8, nC );
       k_cell_stencil< T, A, OP ><<< grid, 256, 0, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ) );
@@ -268,7 +631,7 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
    }
    if ( v.ntasks > 0 )
    {
-      k_bnd_stencil< T, A, OP ><<< ( v.ntasks + 255 ) / 256, 256, 0, ctx->stream >>>( v, o, a.flag, a.copy_unflagged, src, v1, v2,
+      k_bnd_stencil< T, A, OP ><<< ( v.ntasks + 255 ) / 256, 256, 0, fk.aux() >>>( v, o, a.flag, a.copy_unflagged, src, v1, v2,
                                                                                        dst, A( a.a0 ), A( a.a1 ) );
       ++ctx->launches;
    }
@@ -391,6 +754,7 @@ __global__ void __launch_bounds__( 256 ) k_bnd_point( LevelView v, uint32_t flag
 template < typename T, typename A, int OP >
 static void run_point( Context* ctx, const LevelView& v, int nC, const PointArgs& a )
 {
+   Fork fk( ctx );
    if ( v.nrows > 0 && nC > 0 && OP != PT_SYNC )
    {
       dim3 grid( ( v.nrows + 7 ) / 8, nC );
@@ -401,7 +765,7 @@ static void run_point( Context* ctx, const LevelView& v, int nC, const PointArgs
    }
    if ( v.ntasks > 0 )
    {
-      k_bnd_point< T, A, OP ><<< ( v.ntasks + 255 ) / 256, 256, 0, ctx->stream >>>(
+      k_bnd_point< T, A, OP ><<< ( v.ntasks + 255 ) / 256, 256, 0, fk.aux() >>>(
           v, a.flag, a.nsrc, (const T*) a.s0, (const T*) a.s1, (const T*) a.s2, (T*) a.dst, A( a.a0 ), A( a.a1 ), A( a.a2 ),
           a.dev_scalars );
       ++ctx->launches;
@@ -473,20 +837,21 @@ void launch_flat_lincomb( Context* ctx, int64_t count, int dtype, void* dst, int
 }
 
 template < typename TD, typename TS >
-__global__ void k_convert( int64_t count, TD* dst, const TS* src )
+__global__ void k_convert( int64_t count, TD* dst, const TS* src, double scale )
 {
    for ( int64_t i = blockIdx.x * int64_t( blockDim.x ) + threadIdx.x; i < count; i += int64_t( gridDim.x ) * blockDim.x )
    {
-      if constexpr ( std::is_same< TD, __half >::value ) dst[i] = __float2half_rn( float( ldc( src + i ) ) );
-      else dst[i] = TD( ldc( src + i ) );
+      if constexpr ( std::is_same< TD, __half >::value ) dst[i] = __float2half_rn( float( double( ldc( src + i ) ) * scale ) );
+      else if constexpr ( std::is_same< TD, float >::value ) dst[i] = float( double( ldc( src + i ) ) * scale );
+      else dst[i] = TD( double( ldc( src + i ) ) * scale );
    }
 }
 
-void launch_convert( Context* ctx, int64_t count, int dd, void* dst, int sd, const void* src )
+void launch_convert( Context* ctx, int64_t count, int dd, void* dst, int sd, const void* src, double scale )
 {
    if ( count <= 0 ) return;
    const int blocks = int( std::min< int64_t >( ( count + 255 ) / 256, 148 * 16 ) );
-#define HYB_CONV( TD, TS ) k_convert< TD, TS ><<< blocks, 256, 0, ctx->stream >>>( count, (TD*) dst, (const TS*) src )
+#define HYB_CONV( TD, TS ) k_convert< TD, TS ><<< blocks, 256, 0, ctx->stream >>>( count, (TD*) dst, (const TS*) src, scale )
    if ( dd == F64 && sd == F64 ) HYB_CONV( double, double );
    else if ( dd == F64 && sd == F32 ) HYB_CONV( double, float );
    else if ( dd == F64 && sd == F16 ) HYB_CONV( double, __half );
@@ -499,6 +864,26 @@ void launch_convert( Context* ctx, int64_t count, int dd, void* dst, int sd, con
 #undef HYB_CONV
    ++ctx->launches;
    check_cuda( cudaGetLastError(), "convert launch" );
+}
+
+
+// x (fp64) += a * convert(c) over every slot
+template < typename TS >
+__global__ void k_axpy_to_f64( int64_t count, double* x, const TS* c, double a )
+{
+   for ( int64_t i = blockIdx.x * int64_t( blockDim.x ) + threadIdx.x; i < count; i += int64_t( gridDim.x ) * blockDim.x )
+      x[i] += a * double( ldc( c + i ) );
+}
+
+void launch_axpy_to_f64( Context* ctx, int64_t count, double* x, int src_dtype, const void* c, double a )
+{
+   if ( count <= 0 ) return;
+   const int blocks = int( std::min< int64_t >( ( count + 255 ) / 256, 148 * 16 ) );
+   if ( src_dtype == F64 ) k_axpy_to_f64< double ><<< blocks, 256, 0, ctx->stream >>>( count, x, (const double*) c, a );
+   else if ( src_dtype == F32 ) k_axpy_to_f64< float ><<< blocks, 256, 0, ctx->stream >>>( count, x, (const float*) c, a );
+   else k_axpy_to_f64< __half ><<< blocks, 256, 0, ctx->stream >>>( count, x, (const __half*) c, a );
+   ++ctx->launches;
+   check_cuda( cudaGetLastError(), "axpy launch" );
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -579,16 +964,19 @@ static void run_dot( Context* ctx, const LevelView& v, int nC, uint32_t flag, co
    const int nb_cells = ( v.nrows > 0 && nC > 0 ) ? ( ( v.nrows + 7 ) / 8 ) * nC : 0;
    const int nb_bnd   = v.ntasks > 0 ? ( v.ntasks + 255 ) / 256 : 0;
    double*   p        = partials( ctx, nb_cells + nb_bnd + 1 );
-   if ( nb_cells )
    {
+      Fork fk( ctx );
+      if ( nb_cells )
+      {
       dim3 grid( ( v.nrows + 7 ) / 8, nC );
       k_dot_cells< T ><<< grid, 256, 0, ctx->stream >>>( v, flag, (const T*) a, (const T*) b, p );
       ++ctx->launches;
-   }
-   if ( nb_bnd )
-   {
-      k_dot_bnd< T ><<< nb_bnd, 256, 0, ctx->stream >>>( v, flag, (const T*) a, (const T*) b, p + nb_cells );
-      ++ctx->launches;
+      }
+      if ( nb_bnd )
+      {
+         k_dot_bnd< T ><<< nb_bnd, 256, 0, fk.aux() >>>( v, flag, (const T*) a, (const T*) b, p + nb_cells );
+         ++ctx->launches;
+      }
    }
    k_sum_partials<<< 1, 1024, 0, ctx->stream >>>( p, nb_cells + nb_bnd, out );
    ++ctx->launches;
@@ -736,6 +1124,7 @@ template < typename T, typename A >
 static void run_restrict( Context* ctx, const LevelView& cv, const LevelView& fv, int nC, uint32_t flag, const void* fine,
                           void* coarse )
 {
+   Fork fk( ctx );
    if ( cv.nrows > 0 && nC > 0 )
    {
       dim3 grid( ( cv.nrows + 7 ) / 8, nC );
@@ -744,7 +1133,7 @@ static void run_restrict( Context* ctx, const LevelView& cv, const LevelView& fv
    }
    if ( cv.ntasks > 0 )
    {
-      k_restrict_bnd< T, A ><<< ( cv.ntasks + 255 ) / 256, 256, 0, ctx->stream >>>( cv, fv, flag, (const T*) fine, (T*) coarse );
+      k_restrict_bnd< T, A ><<< ( cv.ntasks + 255 ) / 256, 256, 0, fk.aux() >>>( cv, fv, flag, (const T*) fine, (T*) coarse );
       ++ctx->launches;
    }
    check_cuda( cudaGetLastError(), "restrict launch" );
@@ -765,6 +1154,7 @@ template < typename T, typename A >
 static void run_prolong( Context* ctx, const LevelView& cv, const LevelView& fv, int nC, uint32_t flag, const void* coarse,
                          void* fine, int add )
 {
+   Fork fk( ctx );
    if ( fv.nrows > 0 && nC > 0 )
    {
       dim3 grid( ( fv.nrows + 7 ) / 8, nC );
@@ -773,7 +1163,7 @@ static void run_prolong( Context* ctx, const LevelView& cv, const LevelView& fv,
    }
    if ( fv.ntasks > 0 )
    {
-      k_prolong_bnd< T, A ><<< ( fv.ntasks + 255 ) / 256, 256, 0, ctx->stream >>>( cv, fv, flag, (const T*) coarse, (T*) fine,
+      k_prolong_bnd< T, A ><<< ( fv.ntasks + 255 ) / 256, 256, 0, fk.aux() >>>( cv, fv, flag, (const T*) coarse, (T*) fine,
                                                                                      add );
       ++ctx->launches;
    }
@@ -789,6 +1179,21 @@ void launch_prolongate( Context* ctx, Mesh* m, int Lc, int dtype, uint32_t flag,
    if ( dtype == F64 ) run_prolong< double, double >( ctx, cv, fv, nC, flag, coarse, fine, add );
    else if ( dtype == F32 ) run_prolong< float, float >( ctx, cv, fv, nC, flag, coarse, fine, add );
    else run_prolong< __half, float >( ctx, cv, fv, nC, flag, coarse, fine, add );
+}
+
+// allocate every lazily created device table for levels minL..maxL (needed before graph capture)
+void prepare_device( Context* ctx, Mesh* m, Operator* op, int minL, int maxL )
+{
+   ensure_constants();
+   int most = 1;
+   for ( int L = minL; L <= maxL; ++L )
+   {
+      LevelView v = make_view( m, L );
+      if ( op ) ensure_device_op( op->lv.at( L ) );
+      const int nb = ( ( v.nrows + 7 ) / 8 ) * m->topo.nC + ( v.ntasks + 255 ) / 256 + 1;
+      most         = std::max( most, nb );
+   }
+   partials( ctx, most );
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -277,6 +277,23 @@ void build_level( Mesh* m, int L )
    for ( int f = 0; f < t.nF; ++f )
       for ( int j = 1; j < n; ++j )
          for ( int i = 1; i + j < n; ++i ) P.tasks.push_back( { t.nV + t.nE + f, i, j, 0 } );
+   // y-marching work items (interior points: x, y, z >= 1, x+y+z <= n-1)
+   {
+      const int YC = 16;
+      for ( int z = 1; z <= n - 3; ++z )
+         for ( int x0 = 1; x0 <= n - 2 - z; x0 += 32 )
+         {
+            const int ylast = n - 1 - z - x0;
+            for ( int y0 = 1; y0 <= ylast; y0 += YC ) P.march.push_back( { z, x0, y0, std::min( ylast, y0 + YC - 1 ) } );
+         }
+   }
+   // shared-memory staged tiles: TY interior rows of one slice per tile
+   {
+      const int TY = n >= 512 ? 4 : 8;
+      P.tile_rows  = TY;
+      for ( int z = 1; z <= n - 3; ++z )
+         for ( int y0 = 1; y0 <= n - 2 - z; y0 += TY ) P.tiles.push_back( { z, y0, std::min( n - 2 - z, y0 + TY - 1 ), 0 } );
+   }
    // cell interior rows (y, z), memory order
    for ( int z = 1; z <= n - 2; ++z )
       for ( int y = 1; y + z <= n - 2; ++y )
@@ -308,6 +325,12 @@ void ensure_device( Mesh* m, P1Level& P )
    std::vector< int2 > rw( P.rows.size() );
    for ( size_t i = 0; i < rw.size(); ++i ) rw[i] = make_int2( P.rows[i][0], P.rows[i][1] );
    up( &P.d_rows, rw.data(), rw.size() );
+   std::vector< int4 > mi( P.march.size() );
+   for ( size_t i = 0; i < mi.size(); ++i ) mi[i] = make_int4( P.march[i][0], P.march[i][1], P.march[i][2], P.march[i][3] );
+   up( &P.d_march, mi.data(), mi.size() );
+   std::vector< int4 > ti( P.tiles.size() );
+   for ( size_t i = 0; i < ti.size(); ++i ) ti[i] = make_int4( P.tiles[i][0], P.tiles[i][1], P.tiles[i][2], 0 );
+   up( &P.d_tiles, ti.data(), ti.size() );
    std::vector< uint8_t > bc( nP );
    std::vector< int8_t >  bk( P.nB );
    for ( int v = 0; v < t.nV; ++v ) bc[v] = uint8_t( t.bc( t.flag_v[v] ) ), bk[v] = 0;
@@ -349,6 +372,8 @@ Mesh::~Mesh()
       cudaFree( P.d_inc );
       cudaFree( P.d_tasks );
       cudaFree( P.d_rows );
+      cudaFree( P.d_march );
+      cudaFree( P.d_tiles );
       cudaFree( P.d_bc );
       cudaFree( P.d_bkind );
       cudaFree( P.d_ncell_cls );
@@ -508,10 +533,6 @@ Operator::~Operator()
 
 size_t Function::bytes( int L ) const { return size_t( mesh->level( L ).size ) * dtype_size( dtype ); }
 
-Function::~Function()
-{
-   for ( void* p : data ) cudaFree( p );
-}
 
 void check_cuda( cudaError_t e, const char* what )
 {

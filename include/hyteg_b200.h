@@ -175,6 +175,7 @@ typedef struct hyb_gmg_params
    int    coarse_max_iter;                           /* CGSolver(maxIter, relTol, absTol), CGSolver.hpp:44-75 */
    double coarse_rtol, coarse_atol;
    int    use_graph;                                 /* capture each cycle in a CUDA graph */
+   int    coarse_fp64;                               /* FP32/FP16 hierarchies: coarse-grid CG in FP64 */
 } hyb_gmg_params;
 
 int hyb_gmg_params_default( hyb_gmg_params* p );
@@ -199,6 +200,14 @@ int hyb_estimate_radius( hyb_op* op, hyb_fn* x, hyb_fn* tmp, int level, int iter
 int hyb_chebyshev_coefficients( int order, double lower, double upper, double* out );
 /* CGSolver::solve (solvers/CGSolver.hpp:94-206), identity preconditioner, flag Inner|Neumann|Freeslip */
 int hyb_cg_solve( hyb_op* op, hyb_fn* x, hyb_fn* b, int level, int max_iter, double rtol, double atol, int* iterations );
+/* Mixed-precision iterative refinement (defect correction) after
+ * tests/hyteg/mixedPrecision/mixedPrecisionIterativeRefinement.cpp:163-173: x and b are FP64; each outer
+ * step forms r = b - A x in FP64, scales r to unit RMS and stores it in the value type of `inner` (FP32 or
+ * FP16, fixed by `inner_dtype`), runs `inner_cycles` multigrid cycles of `inner` from a zero guess (coarse
+ * solve in FP64) and adds the rescaled correction to x in FP64.  Stops when ||r||/||r_0|| < rtol or after
+ * max_outer steps; res_history receives ||r_0|| .. ||r_k|| (max_outer+1 entries). */
+int hyb_mixed_solve( hyb_gmg* inner, int inner_dtype, hyb_op* op, hyb_fn* x, hyb_fn* b, int level, int inner_cycles,
+                     int max_outer, double rtol, double* res_history, int* outer_iters );
 /* discrete L2 norm of b - A x over the flagged DoFs */
 int hyb_residual_norm( hyb_op* op, hyb_fn* x, hyb_fn* b, hyb_fn* tmp, int level, uint32_t flag, double* out );
 
