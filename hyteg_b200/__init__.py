@@ -69,11 +69,14 @@ _SIGS = {
     "hyb_mesh_create_cuboid": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                          C.POINTER(C.c_void_p)]),
     "hyb_mesh_create_gmsh": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p)]),
+    "hyb_mesh_create_spherical_shell": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
+                                                  C.POINTER(C.c_void_p)]),
     "hyb_mesh_destroy": (C.c_int, [C.c_void_p]),
     "hyb_mesh_set_boundary_flags_on_boundary": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "hyb_mesh_set_bc_type": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32]),
     "hyb_mesh_counts": (C.c_int, [C.c_void_p, C.c_void_p]),
     "hyb_mesh_primitive_vertices": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "hyb_mesh_vertex_coords": (C.c_int, [C.c_void_p, C.c_void_p]),
     "hyb_mesh_primitive_flag": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]),
     "hyb_layout_packed_size": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
     "hyb_layout_primitive_offsets": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
@@ -95,6 +98,8 @@ _SIGS = {
     "hyb_fn_device_ptr": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
     "hyb_op_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "hyb_op_destroy": (C.c_int, [C.c_void_p]),
+    "hyb_op_create_divkgrad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                         C.POINTER(C.c_void_p)]),
     "hyb_op_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_int]),
     "hyb_op_smooth_jac": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_uint32]),
     "hyb_op_inverse_diagonal": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32]),
@@ -117,6 +122,17 @@ _SIGS = {
                                   C.c_double, C.c_void_p, C.POINTER(C.c_int)]),
     "hyb_residual_norm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32,
                                     C.POINTER(C.c_double)]),
+    "hyb_fn_fill_random": (C.c_int, [C.c_void_p, C.c_int, C.c_uint64]),
+    "hyb_serve_params_default": (C.c_int, [C.c_void_p]),
+    "hyb_serve_create": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "hyb_serve_destroy": (C.c_int, [C.c_void_p]),
+    "hyb_serve_now": (C.c_double, [C.c_void_p]),
+    "hyb_serve_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int64)]),
+    "hyb_serve_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "hyb_serve_status": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_double)]),
+    "hyb_serve_last_error": (C.c_char_p, []),
 }
 
 
@@ -205,6 +221,13 @@ class PrimitiveStorage:
         return cls(h, ctx)
 
     @classmethod
+    def spherical_shell(cls, ntan, nrad, rmin, rmax, ctx=None):
+        """MeshInfo::meshSphericalShell (SHELLMESH_CLASSIC)."""
+        h = C.c_void_p()
+        _check(lib().hyb_mesh_create_spherical_shell(ctx.h if ctx else None, ntan, nrad, rmin, rmax, C.byref(h)))
+        return cls(h, ctx)
+
+    @classmethod
     def from_gmsh(cls, path, ctx=None):
         h = C.c_void_p()
         _check(lib().hyb_mesh_create_gmsh(ctx.h if ctx else None, str(path).encode(), C.byref(h)))
@@ -225,6 +248,11 @@ class PrimitiveStorage:
         a = np.zeros(4, dtype=np.int32)
         _check(lib().hyb_mesh_primitive_vertices(self.h, kind, idx, _ptr(a)))
         return [int(v) for v in a if v >= 0]
+
+    def vertex_coords(self):
+        a = np.zeros((self.counts()[0], 3))
+        _check(lib().hyb_mesh_vertex_coords(self.h, _ptr(a)))
+        return a
 
     def primitive_flag(self, kind, idx):
         v = C.c_int()
@@ -277,6 +305,10 @@ class P1Function:
         if a.size != self.storage.packed_size(level):
             raise ValueError("packed vector has the wrong size for this level")
         _check(lib().hyb_fn_upload(self.h, level, _ptr(a)))
+
+    def fill_random(self, level, seed):
+        """Seeded uniform values in [-1, 1] on every DoF of `level` (generated on the device)."""
+        _check(lib().hyb_fn_fill_random(self.h, level, seed))
 
     def download(self, level):
         a = np.zeros(self.storage.packed_size(level), dtype=np.float64)
@@ -386,6 +418,38 @@ class P1ConstantMassOperator(_ConstantOperator):
     kind = P1_CONST_MASS
 
 
+class _Coeff(C.Structure):
+    _fields_ = [("kind", C.c_int), ("value", C.c_double), ("amp", C.c_double), ("freq", C.c_double),
+                ("phase", C.c_double * 3)]
+
+
+class P1ElementwiseBlendingDivKGradOperator(_ConstantOperator):
+    """-div(k grad u), elementwise P1 with the form p1_div_k_grad_blending_q3.
+
+    k: None (k = 1), a constant, or ("expsin", amp, (p0, p1, p2)[, freq]) for
+    k = exp(amp sin(2 pi f (x+p0)) cos(2 pi f (y+p1)) sin(2 pi f (z+p2))).  blending: None or "shell".
+    """
+
+    def __init__(self, storage, min_level, max_level, ctx, k=None, blending=None):
+        self.storage, self.ctx = storage, ctx
+        self.min_level, self.max_level = min_level, max_level
+        c = _Coeff()
+        c.kind, c.value, c.amp, c.freq = 0, 1.0, 0.5, 1.0
+        if isinstance(k, (int, float)):
+            c.value = float(k)
+        elif k is not None:
+            c.kind = 1
+            c.amp = float(k[1])
+            for d in range(3):
+                c.phase[d] = float(k[2][d])
+            if len(k) > 3:
+                c.freq = float(k[3])
+        h = C.c_void_p()
+        _check(lib().hyb_op_create_divkgrad(ctx.h, storage.h, min_level, max_level, C.byref(c),
+                                            1 if blending == "shell" else 0, C.byref(h)))
+        self.h = h
+
+
 class P1toP1LinearRestriction:
     def restrict(self, function, sourceLevel, flag):
         _check(lib().hyb_restrict(function.h, sourceLevel, flag))
@@ -483,6 +547,120 @@ class GeometricMultigridSolver:
     def close(self):
         if getattr(self, "h", None):
             lib().hyb_gmg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------------------------------- serving
+class _ServeParams(C.Structure):
+    _fields_ = [("max_slots", C.c_int), ("hbm_budget_bytes", C.c_double), ("inner_dtype", C.c_int),
+                ("pre_smooth", C.c_int), ("post_smooth", C.c_int), ("power_iterations", C.c_int)]
+
+
+class _Request(C.Structure):
+    _fields_ = [("mesh", C.c_void_p), ("op_kind", C.c_int), ("coeff", _Coeff), ("blending", C.c_int),
+                ("level", C.c_int), ("rhs", C.c_void_p), ("seed", C.c_uint64), ("rtol", C.c_double),
+                ("max_cycles", C.c_int), ("mixed", C.c_int), ("arrival_time", C.c_double),
+                ("x_out", C.c_void_p)]
+
+
+QUEUED, RUNNING, CONVERGED, STOPPED = 0, 1, 2, 3
+
+
+class SolveServer:
+    """Continuous-batching solve server over resident multigrid hierarchies (no reference counterpart).
+
+    ``submit`` queues a Poisson / div-k-grad solve; ``step`` runs one scheduler pass (retire finished
+    solves, launch the next V-cycle of every running solve, admit queued requests into free slots);
+    ``status`` reports (state, t_arrival, t_admit, t_done, cycles, relative residual).
+    """
+
+    def __init__(self, ctx, max_slots=32, hbm_budget_bytes=0.0, inner_dtype="float32", pre_smooth=3, post_smooth=3,
+                 power_iterations=20):
+        p = _ServeParams()
+        _check(lib().hyb_serve_params_default(C.byref(p)))
+        p.max_slots, p.hbm_budget_bytes = max_slots, float(hbm_budget_bytes)
+        p.inner_dtype = _DTYPES[inner_dtype] if isinstance(inner_dtype, str) else int(inner_dtype)
+        p.pre_smooth, p.post_smooth, p.power_iterations = pre_smooth, post_smooth, power_iterations
+        self.ctx = ctx
+        self._keep = {}
+        h = C.c_void_p()
+        rc = lib().hyb_serve_create(ctx.h, C.byref(p), C.byref(h))
+        if rc != 0:
+            raise HybError(f"hyb_serve_create: {lib().hyb_serve_last_error().decode()}")
+        self.h = h
+
+    def now(self):
+        return lib().hyb_serve_now(self.h)
+
+    def submit(self, storage, level, kind="laplace", k=None, blending=None, rhs=None, seed=0, rtol=1e-8,
+               max_cycles=50, mixed=False, arrival_time=-1.0, want_solution=False):
+        r = _Request()
+        r.mesh = storage.h
+        r.op_kind = P1_CONST_LAPLACE if kind == "laplace" else 3
+        r.coeff.kind, r.coeff.value, r.coeff.amp, r.coeff.freq = 0, 1.0, 0.5, 1.0
+        if isinstance(k, (int, float)):
+            r.coeff.value = float(k)
+        elif k is not None:
+            r.coeff.kind, r.coeff.amp = 1, float(k[1])
+            for d in range(3):
+                r.coeff.phase[d] = float(k[2][d])
+            if len(k) > 3:
+                r.coeff.freq = float(k[3])
+        r.blending = 1 if blending == "shell" else 0
+        r.level, r.seed, r.rtol, r.max_cycles = level, seed, rtol, max_cycles
+        r.mixed, r.arrival_time = 1 if mixed else 0, float(arrival_time)
+        keep = []
+        if rhs is not None:
+            a = np.ascontiguousarray(rhs, dtype=np.float64)
+            keep.append(a)
+            r.rhs = a.ctypes.data
+        out = None
+        if want_solution:
+            out = np.zeros(storage.packed_size(level))
+            keep.append(out)
+            r.x_out = out.ctypes.data
+        rid = C.c_int64()
+        rc = lib().hyb_serve_submit(self.h, C.byref(r), C.byref(rid))
+        if rc != 0:
+            raise HybError(f"hyb_serve_submit failed with status {rc}")
+        self._keep[rid.value] = (keep, out)
+        return rid.value
+
+    def step(self):
+        run, q = C.c_int(), C.c_int()
+        rc = lib().hyb_serve_step(self.h, C.byref(run), C.byref(q))
+        if rc != 0:
+            raise HybError(f"hyb_serve_step: {lib().hyb_serve_last_error().decode()}")
+        return run.value, q.value
+
+    def status(self, rid):
+        st, ta, tb, tc, cy, rr = C.c_int(), C.c_double(), C.c_double(), C.c_double(), C.c_int(), C.c_double()
+        _check(lib().hyb_serve_status(self.h, rid, C.byref(st), C.byref(ta), C.byref(tb), C.byref(tc), C.byref(cy),
+                                      C.byref(rr)))
+        return {"state": st.value, "t_arrival": ta.value, "t_admit": tb.value, "t_done": tc.value, "cycles": cy.value,
+                "rel_res": rr.value}
+
+    def solution(self, rid):
+        return self._keep[rid][1]
+
+    def drain(self, poll=None):
+        """Run scheduler passes until no request is queued or running."""
+        while True:
+            run, q = self.step()
+            if run == 0 and q == 0:
+                return
+            if poll:
+                poll()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hyb_serve_destroy(self.h)
             self.h = None
 
     def __del__(self):

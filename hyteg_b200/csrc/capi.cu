@@ -92,6 +92,8 @@ std::vector< std::array< double, 3 > > g_unused;
 int  read_gmsh( const std::string& path, std::vector< std::array< double, 3 > >& coords, std::vector< std::array< int, 4 > >& tets );
 void cuboid( const double* lo, const double* hi, int nx, int ny, int nz, std::vector< std::array< double, 3 > >& coords,
              std::vector< std::array< int, 4 > >& tets );
+void spherical_shell( int ntan, const std::vector< double >& layers, std::vector< std::array< double, 3 > >& coords,
+                      std::vector< std::array< int, 4 > >& tets );
 std::vector< double > chebyshev_coefficients( int order, double lower, double upper );
 }  // namespace hyb
 
@@ -253,6 +255,23 @@ int hyb_mesh_create_cuboid( hyb_ctx* ctx, const double* lo, const double* hi, in
    HYB_CATCH
 }
 
+int hyb_mesh_create_spherical_shell( hyb_ctx* ctx, int ntan, int nrad, double rmin, double rmax, hyb_mesh** out )
+{
+   HYB_TRY
+   require( nrad >= 2, "nrad must be >= 2" );
+   require( rmin > 0 && rmin < rmax, "need 0 < rmin < rmax" );
+   std::vector< double > layers( nrad );
+   for ( int k = 0; k < nrad; ++k ) layers[k] = rmin + ( ( rmax - rmin ) / double( nrad - 1 ) ) * double( k );
+   std::vector< std::array< double, 3 > > c;
+   std::vector< std::array< int, 4 > >    t;
+   spherical_shell( ntan, layers, c, t );
+   int rc = make_mesh( ctx, c, t, out );
+   ( *out )->m.topo.shell_rmin = rmin;
+   ( *out )->m.topo.shell_rmax = rmax;
+   return rc;
+   HYB_CATCH
+}
+
 int hyb_mesh_create_gmsh( hyb_ctx* ctx, const char* path, hyb_mesh** out )
 {
    HYB_TRY
@@ -325,6 +344,15 @@ int hyb_mesh_primitive_vertices( const hyb_mesh* mesh, int kind, int id, int* ou
       break;
    default: throw std::invalid_argument( "kind must be 0..3" );
    }
+   HYB_CATCH
+}
+
+int hyb_mesh_vertex_coords( const hyb_mesh* mesh, double* out )
+{
+   HYB_TRY
+   require( mesh && out, "NULL argument" );
+   for ( int v = 0; v < mesh->m.topo.nV; ++v )
+      for ( int d = 0; d < 3; ++d ) out[3 * v + d] = mesh->m.topo.vx[v][d];
    HYB_CATCH
 }
 
@@ -696,6 +724,45 @@ int hyb_op_create( hyb_ctx* ctx, hyb_mesh* mesh, int kind, int min_level, int ma
    HYB_CATCH
 }
 
+int hyb_op_create_divkgrad( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, const hyb_coeff* k, int blending,
+                            hyb_op** out )
+{
+   HYB_TRY
+   require( ctx && mesh && out, "NULL argument" );
+   require( min_level >= 0 && min_level <= max_level && max_level <= 14, "invalid level range" );
+   require( blending == HYB_BLEND_NONE || blending == HYB_BLEND_SHELL, "unknown blending" );
+   require( !k || k->kind == HYB_COEFF_CONSTANT || k->kind == HYB_COEFF_EXPSIN, "unknown coefficient kind" );
+   set_device( ctx->c );
+   auto* h          = new hyb_op();
+   h->ctx           = ctx;
+   h->o.mesh        = &mesh->m;
+   h->o.kind        = HYB_P1_ELEM_DIVKGRAD;
+   h->o.minL        = min_level;
+   h->o.maxL        = max_level;
+   h->o.elementwise = true;
+   h->o.blending    = blending;
+   if ( k )
+   {
+      h->o.coeff.kind  = k->kind;
+      h->o.coeff.value = k->value;
+      h->o.coeff.amp   = k->amp;
+      h->o.coeff.freq  = k->freq;
+      for ( int d = 0; d < 3; ++d ) h->o.coeff.phase[d] = k->phase[d];
+   }
+   ctx_ref( ctx );
+   mesh_ref( &mesh->m );
+   try
+   {
+      build_elementwise_operator( &h->o );
+   } catch ( ... )
+   {
+      op_unref( h );
+      throw;
+   }
+   *out = h;
+   HYB_CATCH
+}
+
 int hyb_op_destroy( hyb_op* op )
 {
    HYB_TRY
@@ -760,6 +827,14 @@ int hyb_op_inverse_diagonal( hyb_op* op, hyb_fn* out, int level, uint32_t flag )
    HYB_TRY
    require( op, "op is NULL" );
    check_op_fn( op, out, level );
+   if ( op->o.elementwise )
+   {
+      ensure_elementwise_level( &op->ctx->c, &op->o, level, F64 );
+      const int64_t cnt = op->o.mesh->level( level ).size;
+      launch_convert( &op->ctx->c, cnt, out->f.dtype, out->f.ptr( level ), F64, op->o.el[level].d_invd[F64] );
+      sync_copies( out, level );
+      return HYB_OK;
+   }
    const OpLevel&  ol = op->o.lv.at( level );
    const P1Level&  P  = op->o.mesh->level( level );
    const Topology& t  = op->o.mesh->topo;
@@ -790,6 +865,7 @@ int hyb_op_stencil( hyb_op* op, int level, int cell, int cls, double* out15 )
 {
    HYB_TRY
    require( op && out15, "NULL argument" );
+   require( !op->o.elementwise, "elementwise operators have no constant stencil" );
    require( level >= op->o.minL && level <= op->o.maxL, "level outside the operator's level range" );
    require( cell >= 0 && cell < op->o.mesh->topo.nC && cls >= 0 && cls < kNumClasses, "cell or class out of range" );
    const OpLevel& ol = op->o.lv.at( level );
@@ -1147,7 +1223,7 @@ static void run_cycle( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int L )
    if ( !( g->gexec && g->g_x == x->f.ptr( L ) && g->g_b == b->f.ptr( L ) && g->g_level == L ) )
    {
       // every lazily created device table must exist before the capture starts
-      prepare_device( &cx, g->op->o.mesh, &g->op->o, g->p.min_level, L );
+      prepare_device( &cx, g->op->o.mesh, &g->op->o, g->p.min_level, L, x->f.dtype );
       if ( g->gexec ) cudaGraphExecDestroy( g->gexec ), g->gexec = nullptr;
       cudaGraph_t graph;
       check_cuda( cudaStreamBeginCapture( cx.stream, cudaStreamCaptureModeThreadLocal ), "begin capture" );
@@ -1497,5 +1573,62 @@ extern "C" int hyb_mixed_solve( hyb_gmg* g, int inner_dtype, hyb_op* op, hyb_fn*
       if ( !std::isfinite( rn ) ) throw std::runtime_error( "mixed-precision refinement diverged: residual is not finite" );
    }
    if ( outer_iters ) *outer_iters = k;
+   HYB_CATCH
+}
+
+// =============================================================================================
+// asynchronous pieces used by the serving loop (not part of the public header)
+// =============================================================================================
+// r = b - A x over the solve flag into tmp, ||r||^2 into d_out (device); no host synchronisation
+extern "C" int hyb_internal_residual_async( hyb_op* op, hyb_fn* x, hyb_fn* b, hyb_fn* tmp, int level, double* d_out )
+{
+   HYB_TRY
+   Context& c = op->ctx->c;
+   stencil( op, level, x->f.dtype, OP_RESID, kSolveFlag, 0, x->f.ptr( level ), b->f.ptr( level ), nullptr, tmp->f.ptr( level ) );
+   launch_dot( &c, op->o.mesh, level, x->f.dtype, kSolveFlag, tmp->f.ptr( level ), tmp->f.ptr( level ), d_out );
+   HYB_CATCH
+}
+
+// one defect-correction step with the residual already in g->mx_t (FP64) and its norm rn on the
+// host: scale and convert, one inner cycle, FP64 update, new residual into g->mx_t and ||r||^2
+// into d_out
+extern "C" int hyb_internal_mixed_step_async( hyb_gmg* g, int inner_dtype, hyb_op* op, hyb_fn* x, hyb_fn* b, int level, double rn,
+                                              double* d_out )
+{
+   HYB_TRY
+   Mesh* m = op->o.mesh;
+   if ( !g->mx_r || g->mx_r->f.maxL < level || g->mx_r->f.dtype != inner_dtype )
+   {
+      hyb_fn_destroy( g->mx_r );
+      hyb_fn_destroy( g->mx_c );
+      hyb_fn_destroy( g->mx_t );
+      g->mx_r = new_fn( g->ctx, m, inner_dtype, g->p.min_level, level );
+      g->mx_c = new_fn( g->ctx, m, inner_dtype, g->p.min_level, level );
+      g->mx_t = new_fn( g->ctx, m, F64, level, level );
+   }
+   gmg_prepare( g, g->mx_c, g->mx_r, level );
+   Context&      cx  = g->ctx->c;
+   const int64_t cnt = m->level( level ).size;
+   if ( rn > 0 )
+   {
+      const double s = std::sqrt( std::max( 1.0, count_owned( m, level, kSolveFlag ) ) ) / rn;
+      launch_convert( &cx, cnt, inner_dtype, g->mx_r->f.ptr( level ), F64, g->mx_t->f.ptr( level ), s );
+      check_cuda( cudaMemsetAsync( g->mx_c->f.ptr( level ), 0, g->mx_c->f.bytes( level ), cx.stream ), "cudaMemset" );
+      run_cycle( g, g->mx_c, g->mx_r, level );
+      launch_axpy_to_f64( &cx, cnt, (double*) x->f.ptr( level ), inner_dtype, g->mx_c->f.ptr( level ), 1.0 / s );
+   }
+   stencil( op, level, F64, OP_RESID, kSolveFlag, 0, x->f.ptr( level ), b->f.ptr( level ), nullptr, g->mx_t->f.ptr( level ) );
+   launch_dot( &cx, m, level, F64, kSolveFlag, g->mx_t->f.ptr( level ), g->mx_t->f.ptr( level ), d_out );
+   HYB_CATCH
+}
+
+// fill every owned DoF (and its copies) of one level with seeded uniform values in [-1, 1]
+extern "C" int hyb_fn_fill_random( hyb_fn* fn, int level, uint64_t seed )
+{
+   HYB_TRY
+   require( fn, "fn is NULL" );
+   require_level( fn->f, level );
+   launch_fill_uniform( &fn->ctx->c, fn->f.mesh->level( level ).size, fn->f.dtype, fn->f.ptr( level ), seed );
+   sync_copies( fn, level );
    HYB_CATCH
 }

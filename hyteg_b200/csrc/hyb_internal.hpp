@@ -168,11 +168,45 @@ struct OpLevel {
    float*  d_invd_cf = nullptr;
 };
 
+// scalar coefficient k(x) of -div(k grad u): constant, or exp(amp sin(2 pi f (x+p0)) cos(2 pi f (y+p1))
+// sin(2 pi f (z+p2)))
+struct Coefficient {
+   int    kind  = 0;  // 0 constant, 1 exp-sin-cos-sin
+   double value = 1.0;
+   double amp   = 0.5;
+   double freq  = 1.0;
+   double phase[3] = { 0, 0, 0 };
+};
+
+// per-cell geometry of elementwise operators: computational vertex coordinates and, for the
+// icosahedral shell blending, the classified vertices of IcosahedralShellMap
+struct CellGeom {
+   double P[4][3];
+   double ray[3], bxc[3];
+   double volT, rad_ray, rad_ref;
+   int    blend;
+};
+
+struct ElemLevel {
+   void* d_acc  = nullptr;  // accumulation buffer (level size, accumulation precision)
+   int   acc_dtype = -1;
+   void* d_invd[3] = { nullptr, nullptr, nullptr };  // inverse diagonal per DoF, per storage dtype
+   int2* d_hrows    = nullptr;                         // anchor rows (y, z) per (y, z) parity
+   int   hoff[5]    = { 0, 0, 0, 0, 0 };
+};
+
 struct Operator {
    Mesh*                     mesh = nullptr;
    int                       kind = 0;
    int                       minL = 0, maxL = 0;
    std::map< int, OpLevel >  lv;
+   // elementwise operators
+   bool                      elementwise = false;
+   int                       blending    = 0;
+   Coefficient               coeff;
+   CellGeom*                 d_geom = nullptr;
+   std::vector< CellGeom >   geom;
+   std::map< int, ElemLevel > el;
    ~Operator();
 };
 
@@ -218,6 +252,9 @@ struct StencilArgs {
 };
 
 void launch_stencil( Context* ctx, Mesh* m, Operator* A, int L, int dtype, const StencilArgs& a );
+void launch_elementwise( Context* ctx, Mesh* m, Operator* A, int L, int dtype, const StencilArgs& a );
+void build_elementwise_operator( Operator* A );  // host tables (cell geometry, shell classification)
+void ensure_elementwise_level( Context* ctx, Operator* A, int L, int dtype );  // device buffers + diagonal
 
 enum PointOp : int {
    PT_LINCOMB = 0,  // dst = a0*s0 + a1*s1 + a2*s2 (nsrc terms)
@@ -250,7 +287,8 @@ void launch_dot( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const v
 void launch_restrict( Context* ctx, Mesh* m, int Lfine, int dtype, uint32_t flag, const void* fine, void* coarse );
 void launch_prolongate( Context* ctx, Mesh* m, int Lcoarse, int dtype, uint32_t flag, const void* coarse, void* fine, int add );
 void launch_axpy_to_f64( Context* ctx, int64_t count, double* x, int src_dtype, const void* c, double a );
-void prepare_device( Context* ctx, Mesh* m, Operator* op, int minL, int maxL );
+void prepare_device( Context* ctx, Mesh* m, Operator* op, int minL, int maxL, int dtype );
+void launch_fill_uniform( Context* ctx, int64_t count, int dtype, void* dst, uint64_t seed );
 void launch_cg_scalar( Context* ctx, double* state, int stage, double rtol, double atol );
 
 // host helpers

@@ -1,0 +1,562 @@
+// Elementwise P1 operator for -div(k grad u) with optional icosahedral-shell blending (sm_100a).
+//
+// Reference: P1ElementwiseOperator with the HyTeG form p1_div_k_grad_blending_q3
+// (src/hyteg/elementwiseoperators/P1ElementwiseOperator.cpp, src/hyteg/forms/form_hyteg_generated/p1/
+// p1_div_k_grad_blending_q3.cpp): every micro-cell gets its 4x4 element matrix from a 5-point
+// degree-3 quadrature (Yu's rule: centroid weight -2/15, four points with barycentric weights
+// (1/2, 1/6, 1/6, 1/6) and weight 3/40), the coefficient is evaluated at the blended (physical)
+// quadrature point and the blending Jacobian enters the gradients and the volume factor.
+//
+// GPU scheme: the micro-cells of a macro-cell are grouped by the parity of their anchor index; two
+// anchors of the same parity differ by at least 2 in some coordinate, so the micro-cells of one
+// parity class never share a vertex and a thread can add its element contributions without atomics.
+// Eight passes (one per parity) accumulate A x into a scratch array laid out like the function; a
+// combine kernel then applies the same epilogues as the constant-stencil path (apply, residual,
+// Jacobi, Chebyshev steps) with a per-DoF inverse diagonal, summing the cell copies of face, edge
+// and vertex DoFs into their owners (the additive communication of the reference).  Deterministic:
+// the order of every sum is fixed.  The path is FP64-compute-bound.
+#include "hyb_internal.hpp"
+
+#include <cmath>
+#include <stdexcept>
+
+namespace hyb {
+
+// ---------------------------------------------------------------------------------------------
+// host: cell geometry and IcosahedralShellMap classification
+// ---------------------------------------------------------------------------------------------
+static void cross3( const double* a, const double* b, double* c )
+{
+   c[0] = a[1] * b[2] - a[2] * b[1];
+   c[1] = a[2] * b[0] - a[0] * b[2];
+   c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// IcosahedralShellMap::classifyVertices (geometry/IcosahedralShellMap.hpp:606-705): the two vertices
+// on a radial ray become ref/ray (ref is the single outer vertex of an outward tet, the single inner
+// vertex of an inward tet); skew tets borrow the classification of a non-skew tet of the same prism.
+static void classify_shell( const Topology& t, int c, CellGeom& g, int depth = 0 )
+{
+   if ( depth > 4 ) throw std::runtime_error( "shell blending: cannot classify macro-cell" );
+   double P[4][3], rad[4];
+   for ( int k = 0; k < 4; ++k )
+   {
+      for ( int d = 0; d < 3; ++d ) P[k][d] = t.vx[t.cv[c][k]][d];
+      rad[k] = std::sqrt( P[k][0] * P[k][0] + P[k][1] * P[k][1] + P[k][2] * P[k][2] );
+   }
+   double inner = rad[0], outer = rad[0];
+   for ( int k = 1; k < 4; ++k ) inner = std::min( inner, rad[k] ), outer = std::max( outer, rad[k] );
+   const double eps     = ( outer - inner ) * 0.001;
+   int          n_outer = 0;
+   for ( int k = 0; k < 4; ++k ) n_outer += ( outer - rad[k] ) < eps ? 1 : 0;
+   int iref = -1, iray = -1;
+   for ( int k = 0; k < 4 && iref < 0; ++k )
+      for ( int j = k + 1; j < 4 && iref < 0; ++j )
+      {
+         double cr[3];
+         cross3( P[k], P[j], cr );
+         const double s = rad[k] * rad[j];
+         if ( std::fabs( cr[0] ) / s <= 1e-14 && std::fabs( cr[1] ) / s <= 1e-14 && std::fabs( cr[2] ) / s <= 1e-14 ) iref = k, iray = j;
+      }
+   if ( iref < 0 ) throw std::runtime_error( "shell blending: no radial vertex pair in a macro-cell (not a shell mesh?)" );
+   if ( n_outer == 2 )
+   {
+      const int vref = t.cv[c][iref], vray = t.cv[c][iray];
+      for ( int f : t.cf[c] )
+      {
+         const auto& fv     = t.fv[f];
+         const bool  hasRef = fv[0] == vref || fv[1] == vref || fv[2] == vref;
+         const bool  hasRay = fv[0] == vray || fv[1] == vray || fv[2] == vray;
+         if ( !( hasRef && hasRay ) )
+            for ( int cc : t.f_cells[f] )
+               if ( cc != c ) return classify_shell( t, cc, g, depth + 1 );
+      }
+      throw std::runtime_error( "shell blending: no non-skew neighbour" );
+   }
+   int rest[2], nr = 0;
+   for ( int k = 0; k < 4; ++k )
+      if ( k != iref && k != iray ) rest[nr++] = k;
+   const int ithr = rest[1], ifor = rest[0];
+   if ( ( n_outer == 1 && rad[iref] < rad[iray] ) || ( n_outer == 3 && rad[iref] > rad[iray] ) ) std::swap( iref, iray );
+   double a[3], b[3];
+   for ( int d = 0; d < 3; ++d )
+   {
+      g.ray[d] = P[iray][d];
+      a[d]     = P[ithr][d] - P[iray][d];
+      b[d]     = P[ifor][d] - P[iray][d];
+   }
+   cross3( a, b, g.bxc );
+   g.volT    = ( P[iref][0] - P[iray][0] ) * g.bxc[0] + ( P[iref][1] - P[iray][1] ) * g.bxc[1] + ( P[iref][2] - P[iray][2] ) * g.bxc[2];
+   g.rad_ray = rad[iray];
+   g.rad_ref = rad[iref];
+}
+
+void build_elementwise_operator( Operator* A )
+{
+   const Topology& t = A->mesh->topo;
+   A->geom.assign( t.nC, CellGeom{} );
+   for ( int c = 0; c < t.nC; ++c )
+   {
+      CellGeom& g = A->geom[c];
+      for ( int k = 0; k < 4; ++k )
+         for ( int d = 0; d < 3; ++d ) g.P[k][d] = t.vx[t.cv[c][k]][d];
+      g.blend = A->blending;
+      if ( A->blending == 1 ) classify_shell( t, c, g );
+   }
+}
+
+// ---------------------------------------------------------------------------------------------
+// device: blending, coefficient and element matrix
+// ---------------------------------------------------------------------------------------------
+__constant__ double c_yu5_pts[5][3] = { { 0.25, 0.25, 0.25 },
+                                        { 1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0 },
+                                        { 0.5, 1.0 / 6.0, 1.0 / 6.0 },
+                                        { 1.0 / 6.0, 0.5, 1.0 / 6.0 },
+                                        { 1.0 / 6.0, 1.0 / 6.0, 0.5 } };
+__constant__ double c_yu5_w[5]      = { -2.0 / 15.0, 3.0 / 40.0, 3.0 / 40.0, 3.0 / 40.0, 3.0 / 40.0 };
+
+template < typename A >
+__device__ __forceinline__ A coeff_eval( const Coefficient& k, const A* P )
+{
+   if ( k.kind == 0 ) return A( k.value );
+   const A tp = A( 2.0 * 3.14159265358979323846 * k.freq );
+   return exp( A( k.amp ) * sin( tp * ( P[0] + A( k.phase[0] ) ) ) * cos( tp * ( P[1] + A( k.phase[1] ) ) ) *
+               sin( tp * ( P[2] + A( k.phase[2] ) ) ) );
+}
+
+// IcosahedralShellMap: F(x) = x r(x)/|x|, r(x) = r_ray + lambda(x) (r_ref - r_ray) with lambda the
+// barycentric weight of the ref vertex; DF = s I + x (grad s)^T with s = r/|x|.
+template < typename A >
+__device__ __forceinline__ void shell_map( const CellGeom& g, const A* X, A* F, A DF[3][3] )
+{
+   const A dx = X[0] - A( g.ray[0] ), dy = X[1] - A( g.ray[1] ), dz = X[2] - A( g.ray[2] );
+   const A lam_s = ( dx * A( g.bxc[0] ) + dy * A( g.bxc[1] ) + dz * A( g.bxc[2] ) ) / A( g.volT );
+   const A sgn   = lam_s < A( 0 ) ? A( -1 ) : A( 1 );
+   const A dr    = A( g.rad_ref ) - A( g.rad_ray );
+   const A R     = A( g.rad_ray ) + fabs( lam_s ) * dr;
+   const A r2    = X[0] * X[0] + X[1] * X[1] + X[2] * X[2];
+   const A r     = sqrt( r2 );
+   const A s     = R / r;
+   A       gs[3];
+   for ( int j = 0; j < 3; ++j ) gs[j] = ( dr * sgn * A( g.bxc[j] ) / A( g.volT ) ) / r - R * X[j] / ( r2 * r );
+   for ( int i = 0; i < 3; ++i )
+   {
+      F[i] = X[i] * s;
+      for ( int j = 0; j < 3; ++j ) DF[i][j] = ( i == j ? s : A( 0 ) ) + X[i] * gs[j];
+   }
+}
+
+template < typename A >
+__device__ __forceinline__ void p1_divkgrad_element( const CellGeom& g, const Coefficient& kc, const A X[4][3], A K[4][4] )
+{
+   A J[3][3];
+   for ( int r = 0; r < 3; ++r )
+      for ( int c = 0; c < 3; ++c ) J[r][c] = X[c + 1][r] - X[0][r];
+   for ( int i = 0; i < 4; ++i )
+      for ( int j = 0; j < 4; ++j ) K[i][j] = A( 0 );
+#pragma unroll 1
+   for ( int q = 0; q < 5; ++q )
+   {
+      A Xq[3];
+      for ( int r = 0; r < 3; ++r )
+         Xq[r] = X[0][r] + J[r][0] * A( c_yu5_pts[q][0] ) + J[r][1] * A( c_yu5_pts[q][1] ) + J[r][2] * A( c_yu5_pts[q][2] );
+      A M[3][3], Fq[3];
+      if ( g.blend == 1 )
+      {
+         A DF[3][3];
+         shell_map( g, Xq, Fq, DF );
+         for ( int r = 0; r < 3; ++r )
+            for ( int c = 0; c < 3; ++c ) M[r][c] = DF[r][0] * J[0][c] + DF[r][1] * J[1][c] + DF[r][2] * J[2][c];
+      }
+      else
+      {
+         for ( int r = 0; r < 3; ++r )
+         {
+            Fq[r] = Xq[r];
+            for ( int c = 0; c < 3; ++c ) M[r][c] = J[r][c];
+         }
+      }
+      // inverse of M: rows of M^-1 are the reference gradients mapped to physical space
+      const A c00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
+      const A c01 = M[1][2] * M[2][0] - M[1][0] * M[2][2];
+      const A c02 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
+      const A det = M[0][0] * c00 + M[0][1] * c01 + M[0][2] * c02;
+      const A id  = A( 1 ) / det;
+      A       Mi[3][3];
+      Mi[0][0] = c00 * id;
+      Mi[1][0] = c01 * id;
+      Mi[2][0] = c02 * id;
+      Mi[0][1] = ( M[0][2] * M[2][1] - M[0][1] * M[2][2] ) * id;
+      Mi[1][1] = ( M[0][0] * M[2][2] - M[0][2] * M[2][0] ) * id;
+      Mi[2][1] = ( M[0][1] * M[2][0] - M[0][0] * M[2][1] ) * id;
+      Mi[0][2] = ( M[0][1] * M[1][2] - M[0][2] * M[1][1] ) * id;
+      Mi[1][2] = ( M[0][2] * M[1][0] - M[0][0] * M[1][2] ) * id;
+      Mi[2][2] = ( M[0][0] * M[1][1] - M[0][1] * M[1][0] ) * id;
+      // gradient of phi_i (i = 1..3) is row i-1 of Mi; phi_0 is minus their sum
+      A G[4][3];
+      for ( int d = 0; d < 3; ++d )
+      {
+         G[1][d] = Mi[0][d];
+         G[2][d] = Mi[1][d];
+         G[3][d] = Mi[2][d];
+         G[0][d] = -( G[1][d] + G[2][d] + G[3][d] );
+      }
+      const A f = A( c_yu5_w[q] ) * coeff_eval( kc, Fq ) * fabs( det );
+      for ( int i = 0; i < 4; ++i )
+         for ( int j = i; j < 4; ++j ) K[i][j] += f * ( G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2] );
+   }
+   for ( int i = 0; i < 4; ++i )
+      for ( int j = 0; j < i; ++j ) K[i][j] = K[j][i];
+}
+
+}  // namespace hyb
+
+namespace hyb {
+
+// micro-cell types: vertex offsets and anchor range shift (CellDoFIndexing.hpp:155-198)
+__constant__ int c_mc_off[6][4][3] = {
+    { { 0, 0, 0 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } }, { { 1, 0, 0 }, { 1, 1, 0 }, { 0, 1, 0 }, { 1, 0, 1 } },
+    { { 1, 0, 0 }, { 0, 1, 0 }, { 1, 0, 1 }, { 0, 0, 1 } }, { { 1, 1, 0 }, { 1, 1, 1 }, { 0, 1, 1 }, { 1, 0, 1 } },
+    { { 1, 0, 1 }, { 0, 1, 1 }, { 0, 0, 1 }, { 0, 1, 0 } }, { { 0, 1, 0 }, { 1, 1, 0 }, { 1, 0, 1 }, { 0, 1, 1 } } };
+__constant__ int c_mc_shift[6] = { 0, 1, 1, 2, 1, 1 };
+
+__device__ __forceinline__ double ld_any( const double* p ) { return *p; }
+__device__ __forceinline__ float  ld_any( const float* p ) { return *p; }
+__device__ __forceinline__ float  ld_any( const __half* p ) { return __half2float( *p ); }
+__device__ __forceinline__ void   st_any( double* p, double v ) { *p = v; }
+__device__ __forceinline__ void   st_any( float* p, float v ) { *p = v; }
+__device__ __forceinline__ void   st_any( __half* p, float v ) { *p = __float2half_rn( v ); }
+
+// One parity pass: warp per half-grid row (y, z) of anchors with y = py mod 2, z = pz mod 2, lanes
+// over x = px + 2k.  MODE 0 accumulates A src, MODE 1 the diagonal.
+template < typename T, typename A, int MODE >
+__global__ void __launch_bounds__( 256 ) k_elem_pass( int n, int nrows, const int2* __restrict__ rows, const int64_t* __restrict__ cell_off,
+                                                       const CellGeom* __restrict__ geom, Coefficient kc, int px,
+                                                       const T* __restrict__ src, A* __restrict__ acc )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int r    = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   if ( r >= nrows ) return;
+   const int2     yz = rows[r];
+   const int      y = yz.x, z = yz.y;
+   const CellGeom g  = geom[c];
+   const int64_t  base = cell_off[c];
+   const A        inv_n = A( 1.0 / double( n ) );
+   A              st[3][3];  // computational steps per index direction (coordinateFromIndex)
+   for ( int k = 0; k < 3; ++k )
+      for ( int d = 0; d < 3; ++d ) st[k][d] = ( A( g.P[k + 1][d] ) - A( g.P[0][d] ) ) * inv_n;
+   for ( int x = px + 2 * lane; x + y + z <= n - 1; x += 64 )
+      for ( int ty = 0; ty < 6; ++ty )
+      {
+         if ( x + y + z > n - 1 - c_mc_shift[ty] ) continue;
+         int64_t idx[4];
+         A       X[4][3];
+         for ( int m = 0; m < 4; ++m )
+         {
+            const int vx = x + c_mc_off[ty][m][0], vy = y + c_mc_off[ty][m][1], vz = z + c_mc_off[ty][m][2];
+            idx[m]       = base + cidx( n, vx, vy, vz );
+            for ( int d = 0; d < 3; ++d ) X[m][d] = A( g.P[0][d] ) + st[0][d] * A( vx ) + st[1][d] * A( vy ) + st[2][d] * A( vz );
+         }
+         A K[4][4];
+         p1_divkgrad_element( g, kc, X, K );
+         if constexpr ( MODE == 0 )
+         {
+            A xl[4];
+            for ( int m = 0; m < 4; ++m ) xl[m] = A( ld_any( src + idx[m] ) );
+            for ( int i = 0; i < 4; ++i ) acc[idx[i]] += K[i][0] * xl[0] + K[i][1] * xl[1] + K[i][2] * xl[2] + K[i][3] * xl[3];
+         }
+         else
+            for ( int i = 0; i < 4; ++i ) acc[idx[i]] += K[i][i];
+      }
+}
+
+// Combine: cell interior points take s = acc, face/edge/vertex owners the sum of their copies in
+// the neighbouring cells; then the operation's epilogue (the constant-stencil kernels' semantics).
+template < typename T, typename A, int OP >
+__device__ __forceinline__ A epilogue_value( int64_t i, A s, A invd, const T* src, const T* v1, T* v2, A a0, A a1, A* second )
+{
+   if constexpr ( OP == OP_APPLY || OP == OP_APPLY_ADD ) return s;
+   else if constexpr ( OP == OP_RESID ) return A( ld_any( v1 + i ) ) - s;
+   else if constexpr ( OP == OP_JAC ) return A( ld_any( src + i ) ) + a0 * ( invd * ( A( ld_any( v1 + i ) ) - s ) );
+   else if constexpr ( OP == OP_CHEB0 ) return invd * ( A( ld_any( v1 + i ) ) - s );
+   else if constexpr ( OP == OP_CHEBI )
+   {
+      *second = A( ld_any( v2 + i ) ) + a0 * A( ld_any( src + i ) );
+      return invd * s;
+   }
+   else if constexpr ( OP == OP_CHEBL ) return ( A( ld_any( v2 + i ) ) + a0 * A( ld_any( src + i ) ) ) + a1 * ( invd * s );
+   else if constexpr ( OP == OP_DINV_APPLY ) return invd * s;
+   return s;
+}
+
+template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( 256 ) k_cell_acc( int n, int nrows, const int2* __restrict__ rows, const int64_t* __restrict__ cell_off,
+                                                      const uint8_t* __restrict__ cell_bc, uint32_t flag, const A* __restrict__ acc,
+                                                      const A* __restrict__ invd, const T* src, const T* v1, T* v2, T* dst, A a0, A a1 )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int r    = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   if ( r >= nrows || !( cell_bc[c] & flag ) ) return;
+   const int2    yz   = rows[r];
+   const int64_t base = cell_off[c] + cidx( n, 0, yz.x, yz.y );
+   for ( int x = 1 + lane; x <= n - 1 - yz.x - yz.y; x += 32 )
+   {
+      const int64_t i = base + x;
+      A             second;
+      const A       val = epilogue_value< T, A, OP >( i, acc[i], invd ? invd[i] : A( 1 ), src, v1, v2, a0, a1, &second );
+      if constexpr ( OP == OP_CHEBL ) st_any( v2 + i, val );
+      else if constexpr ( OP == OP_APPLY_ADD ) st_any( dst + i, A( ld_any( dst + i ) ) + val );
+      else
+      {
+         st_any( dst + i, val );
+         if constexpr ( OP == OP_CHEBI ) st_any( v2 + i, second );
+      }
+   }
+}
+
+template < typename T, typename A >
+__device__ __forceinline__ void wt_store( int n, const int4& tk, int64_t owner, const int* inc_begin, const Incidence* inc,
+                                          const int64_t* cell_off, T* vec, A val )
+{
+   st_any( vec + owner, val );
+   for ( int q = inc_begin[tk.x]; q < inc_begin[tk.x + 1]; ++q )
+   {
+      const Incidence I = inc[q];
+      const int       x = n * I.o[0] + tk.y * I.e1[0] + tk.z * I.e2[0];
+      const int       y = n * I.o[1] + tk.y * I.e1[1] + tk.z * I.e2[1];
+      const int       z = n * I.o[2] + tk.y * I.e1[2] + tk.z * I.e2[2];
+      st_any( vec + cell_off[I.cell] + cidx( n, x, y, z ), val );
+   }
+}
+
+template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( 256 ) k_bnd_acc( int n, int ntasks, const int4* __restrict__ tasks, const int64_t* __restrict__ off,
+                                                     const int64_t* __restrict__ cell_off, const int8_t* __restrict__ bkind,
+                                                     const uint8_t* __restrict__ bc, const int* __restrict__ inc_begin,
+                                                     const Incidence* __restrict__ inc, uint32_t flag, int copy_unflagged,
+                                                     const A* __restrict__ acc, const A* __restrict__ invd, A* invd_out, const T* src,
+                                                     const T* v1, T* v2, T* dst, A a0, A a1 )
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( t >= ntasks ) return;
+   const int4    tk    = tasks[t];
+   const int     b     = tk.x;
+   const int     k     = bkind[b];
+   const int64_t owner = off[b] + ( k == 0 ? 0 : ( k == 1 ? int64_t( tk.y ) : fidx( n, tk.y, tk.z ) ) );
+   if ( !( bc[b] & flag ) )
+   {
+      if ( !copy_unflagged ) return;
+      if constexpr ( OP == OP_JAC || OP == OP_CHEB0 )
+         wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, A( ld_any( src + owner ) ) );
+      else if constexpr ( OP == OP_CHEBI ) wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, A( ld_any( v2 + owner ) ) );
+      return;
+   }
+   A s = A( 0 );
+   for ( int q = inc_begin[b]; q < inc_begin[b + 1]; ++q )
+   {
+      const Incidence I = inc[q];
+      const int       x = n * I.o[0] + tk.y * I.e1[0] + tk.z * I.e2[0];
+      const int       y = n * I.o[1] + tk.y * I.e1[1] + tk.z * I.e2[1];
+      const int       z = n * I.o[2] + tk.y * I.e1[2] + tk.z * I.e2[2];
+      s += acc[cell_off[I.cell] + cidx( n, x, y, z )];
+   }
+   if ( invd_out )  // diagonal setup: store 1/diag at the owner
+   {
+      invd_out[owner] = A( 1 ) / s;
+      return;
+   }
+   A       second;
+   const A val = epilogue_value< T, A, OP >( owner, s, invd ? invd[owner] : A( 1 ), src, v1, v2, a0, a1, &second );
+   if constexpr ( OP == OP_CHEBL ) wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, v2, val );
+   else if constexpr ( OP == OP_APPLY_ADD )
+      wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, A( ld_any( dst + owner ) ) + val );
+   else
+   {
+      wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, val );
+      if constexpr ( OP == OP_CHEBI ) wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, v2, second );
+   }
+}
+
+template < typename A >
+__global__ void k_cell_invert( int n, int nrows, const int2* __restrict__ rows, const int64_t* __restrict__ cell_off, const A* acc,
+                               A* invd )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int r    = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   if ( r >= nrows ) return;
+   const int2    yz   = rows[r];
+   const int64_t base = cell_off[c] + cidx( n, 0, yz.x, yz.y );
+   for ( int x = 1 + lane; x <= n - 1 - yz.x - yz.y; x += 32 ) invd[base + x] = A( 1 ) / acc[base + x];
+}
+
+// ---------------------------------------------------------------------------------------------
+// host launch
+// ---------------------------------------------------------------------------------------------
+template < typename A >
+static A* acc_buffer( Operator* op, int L, int64_t size )
+{
+   ElemLevel& e   = op->el[L];
+   const int  adt = sizeof( A ) == 8 ? F64 : F32;
+   if ( e.d_acc && e.acc_dtype != adt && adt == F64 )
+   {
+      check_cuda( cudaFree( e.d_acc ), "cudaFree(acc)" );
+      e.d_acc = nullptr;
+   }
+   if ( !e.d_acc )
+   {
+      check_cuda( cudaMalloc( &e.d_acc, size * sizeof( double ) ), "cudaMalloc(elementwise scratch)" );
+      e.acc_dtype = F64;
+   }
+   return reinterpret_cast< A* >( e.d_acc );
+}
+
+static void ensure_rows( Operator* op, int L )
+{
+   ElemLevel& e = op->el[L];
+   if ( e.d_hrows ) return;
+   const int                  n = 1 << L;
+   std::vector< int2 >        rows;
+   for ( int p = 0; p < 4; ++p )
+   {
+      e.hoff[p]    = int( rows.size() );
+      const int py = p & 1, pz = p >> 1;
+      for ( int z = pz; z <= n - 1; z += 2 )
+         for ( int y = py; y + z <= n - 1; y += 2 ) rows.push_back( make_int2( y, z ) );
+   }
+   e.hoff[4] = int( rows.size() );
+   check_cuda( cudaMalloc( &e.d_hrows, std::max< size_t >( rows.size(), 1 ) * sizeof( int2 ) ), "cudaMalloc(rows)" );
+   if ( !rows.empty() )
+      check_cuda( cudaMemcpy( e.d_hrows, rows.data(), rows.size() * sizeof( int2 ), cudaMemcpyHostToDevice ), "upload rows" );
+}
+
+template < typename T, typename A, int MODE >
+static void run_passes( Context* ctx, Mesh* m, Operator* op, int L, const T* src, A* acc )
+{
+   P1Level&   P = m->level( L );
+   ElemLevel& e = op->el[L];
+   check_cuda( cudaMemsetAsync( acc, 0, P.size * sizeof( A ), ctx->stream ), "cudaMemset(acc)" );
+   const int nC = m->topo.nC;
+   for ( int p = 0; p < 8; ++p )
+   {
+      const int px = p & 1, q = p >> 1;  // q = (py, pz) row table
+      const int nr = e.hoff[q + 1] - e.hoff[q];
+      if ( nr <= 0 ) continue;
+      dim3 grid( ( nr + 7 ) / 8, nC );
+      k_elem_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( P.n, nr, e.d_hrows + e.hoff[q], P.d_off + P.nB, op->d_geom,
+                                                                   op->coeff, px, src, acc );
+      ++ctx->launches;
+   }
+   check_cuda( cudaGetLastError(), "elementwise pass launch" );
+}
+
+template < typename T, typename A >
+static void ensure_level_t( Context* ctx, Operator* op, int L, int dtype )
+{
+   Mesh*    m = op->mesh;
+   P1Level& P = m->level( L );
+   ensure_device( m, P );
+   if ( !op->d_geom )
+   {
+      check_cuda( cudaMalloc( &op->d_geom, op->geom.size() * sizeof( CellGeom ) ), "cudaMalloc(geometry)" );
+      check_cuda( cudaMemcpy( op->d_geom, op->geom.data(), op->geom.size() * sizeof( CellGeom ), cudaMemcpyHostToDevice ),
+                  "upload geometry" );
+   }
+   ensure_rows( op, L );
+   ElemLevel& e = op->el[L];
+   A*         acc = acc_buffer< A >( op, L, P.size );
+   if ( e.d_invd[dtype] ) return;
+   A* invd = nullptr;
+   check_cuda( cudaMalloc( &invd, P.size * sizeof( A ) ), "cudaMalloc(inverse diagonal)" );
+   check_cuda( cudaMemsetAsync( invd, 0, P.size * sizeof( A ), ctx->stream ), "cudaMemset" );
+   e.d_invd[dtype] = invd;
+   // diagonal: sum of element-matrix diagonals, owners summing their cell copies
+   run_passes< T, A, 1 >( ctx, m, op, L, nullptr, acc );
+   const int nrows = int( P.rows.size() );
+   if ( nrows > 0 )
+   {
+      dim3 grid( ( nrows + 7 ) / 8, m->topo.nC );
+      k_cell_invert< A ><<< grid, 256, 0, ctx->stream >>>( P.n, nrows, P.d_rows, P.d_off + P.nB, acc, invd );
+   }
+   if ( !P.tasks.empty() )
+      k_bnd_acc< T, A, OP_APPLY ><<< ( int( P.tasks.size() ) + 255 ) / 256, 256, 0, ctx->stream >>>(
+          P.n, int( P.tasks.size() ), P.d_tasks, P.d_off, P.d_off + P.nB, P.d_bkind, P.d_bc, P.d_inc_begin, P.d_inc, kAll, 0, acc,
+          nullptr, invd, nullptr, nullptr, nullptr, nullptr, A( 0 ), A( 0 ) );
+   check_cuda( cudaGetLastError(), "diagonal launch" );
+}
+
+void ensure_elementwise_level( Context* ctx, Operator* op, int L, int dtype )
+{
+   if ( dtype == F64 ) ensure_level_t< double, double >( ctx, op, L, dtype );
+   else if ( dtype == F32 ) ensure_level_t< float, float >( ctx, op, L, dtype );
+   else ensure_level_t< __half, float >( ctx, op, L, dtype );
+}
+
+template < typename T, typename A, int OP >
+static void run_elem( Context* ctx, Mesh* m, Operator* op, int L, int dtype, const StencilArgs& a )
+{
+   P1Level& P   = m->level( L );
+   A*       acc = acc_buffer< A >( op, L, P.size );
+   const A* inv = reinterpret_cast< const A* >( op->el[L].d_invd[dtype] );
+   run_passes< T, A, 0 >( ctx, m, op, L, (const T*) a.src, acc );
+   const int nrows = int( P.rows.size() );
+   {
+      struct Join
+      {
+         Context* c;
+         ~Join()
+         {
+            cudaEventRecord( c->ev_join, c->aux );
+            cudaStreamWaitEvent( c->stream, c->ev_join, 0 );
+         }
+      };
+      check_cuda( cudaEventRecord( ctx->ev_fork, ctx->stream ), "fork" );
+      check_cuda( cudaStreamWaitEvent( ctx->aux, ctx->ev_fork, 0 ), "fork" );
+      Join j{ ctx };
+      if ( nrows > 0 )
+      {
+         dim3 grid( ( nrows + 7 ) / 8, m->topo.nC );
+         k_cell_acc< T, A, OP ><<< grid, 256, 0, ctx->stream >>>( P.n, nrows, P.d_rows, P.d_off + P.nB, P.d_bc + P.nB, a.flag, acc, inv,
+                                                                   (const T*) a.src, (const T*) a.v1, (T*) a.v2, (T*) a.dst, A( a.a0 ),
+                                                                   A( a.a1 ) );
+         ++ctx->launches;
+      }
+      if ( !P.tasks.empty() )
+      {
+         k_bnd_acc< T, A, OP ><<< ( int( P.tasks.size() ) + 255 ) / 256, 256, 0, ctx->aux >>>(
+             P.n, int( P.tasks.size() ), P.d_tasks, P.d_off, P.d_off + P.nB, P.d_bkind, P.d_bc, P.d_inc_begin, P.d_inc, a.flag,
+             a.copy_unflagged, acc, inv, nullptr, (const T*) a.src, (const T*) a.v1, (T*) a.v2, (T*) a.dst, A( a.a0 ), A( a.a1 ) );
+         ++ctx->launches;
+      }
+   }
+   check_cuda( cudaGetLastError(), "elementwise combine launch" );
+}
+
+template < typename T, typename A >
+static void dispatch_elem( Context* ctx, Mesh* m, Operator* op, int L, int dtype, const StencilArgs& a )
+{
+   switch ( a.op )
+   {
+   case OP_APPLY: run_elem< T, A, OP_APPLY >( ctx, m, op, L, dtype, a ); break;
+   case OP_APPLY_ADD: run_elem< T, A, OP_APPLY_ADD >( ctx, m, op, L, dtype, a ); break;
+   case OP_RESID: run_elem< T, A, OP_RESID >( ctx, m, op, L, dtype, a ); break;
+   case OP_JAC: run_elem< T, A, OP_JAC >( ctx, m, op, L, dtype, a ); break;
+   case OP_CHEB0: run_elem< T, A, OP_CHEB0 >( ctx, m, op, L, dtype, a ); break;
+   case OP_CHEBI: run_elem< T, A, OP_CHEBI >( ctx, m, op, L, dtype, a ); break;
+   case OP_CHEBL: run_elem< T, A, OP_CHEBL >( ctx, m, op, L, dtype, a ); break;
+   case OP_DINV_APPLY: run_elem< T, A, OP_DINV_APPLY >( ctx, m, op, L, dtype, a ); break;
+   default: throw std::invalid_argument( "unknown operation" );
+   }
+}
+
+void launch_elementwise( Context* ctx, Mesh* m, Operator* op, int L, int dtype, const StencilArgs& a )
+{
+   ensure_elementwise_level( ctx, op, L, dtype );
+   if ( dtype == F64 ) dispatch_elem< double, double >( ctx, m, op, L, dtype, a );
+   else if ( dtype == F32 ) dispatch_elem< float, float >( ctx, m, op, L, dtype, a );
+   else dispatch_elem< __half, float >( ctx, m, op, L, dtype, a );
+}
+
+}  // namespace hyb

@@ -258,9 +258,11 @@ __device__ __forceinline__ Row3< T, A > load_row( const T* s, int n, int yy, int
    return r;
 }
 
+__device__ __forceinline__ void prefetch_l2( const void* p ) { asm volatile( "prefetch.global.L2 [%0];" ::"l"( p ) ); }
+
 template < typename T, typename A, int OP >
 __global__ void __launch_bounds__( 256 ) k_cell_march( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
-                                                        const T* __restrict__ v1, T* v2, T* dst, A a0, A a1 )
+                                                        const T* __restrict__ v1, T* v2, T* dst, A a0, A a1, int prefetch_distance )
 {
    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
    const int item = blockIdx.x * 8 + warp;
@@ -279,9 +281,18 @@ __global__ void __launch_bounds__( 256 ) k_cell_march( LevelView v, OpView< A > 
    Row3< T, A > c0 = load_row< T, A >( s, n, ya, z, x );
    Row3< T, A > tm = load_row< T, A >( s, n, ya - 1, z + 1, x );
    Row3< T, A > b0 = load_row< T, A >( s, n, ya, z - 1, x );
+   const int pd = prefetch_distance;
 #pragma unroll 2
    for ( int y = ya; y <= yb; ++y )
    {
+      if ( pd > 0 )
+      {
+         // pull the rows needed pd steps ahead into L2 (addresses stay inside the cell array)
+         const int yp = y + pd;
+         if ( yp + 1 + z <= n && x <= n - yp - 1 - z ) prefetch_l2( s + cidx( n, x, yp + 1, z ) );
+         if ( yp + z + 1 <= n && x <= n - yp - z - 1 ) prefetch_l2( s + cidx( n, x, yp, z + 1 ) );
+         if ( yp + 1 + z - 1 <= n && x <= n - yp - z ) prefetch_l2( s + cidx( n, x, yp + 1, z - 1 ) );
+      }
       const Row3< T, A > cp = load_row< T, A >( s, n, y + 1, z, x );
       const Row3< T, A > t0 = load_row< T, A >( s, n, y, z + 1, x );
       const Row3< T, A > bp = load_row< T, A >( s, n, y + 1, z - 1, x );
@@ -370,6 +381,7 @@ __host__ __device__ __forceinline__ TileRange tile_range( int n, int r0, int r1,
 }
 
 constexpr int kTmaThreads = 256;
+constexpr int kTmaStages  = 3;
 constexpr int kSpinLimit  = 1 << 22;
 
 template < typename T, typename A, int OP >
@@ -378,14 +390,13 @@ __global__ void __launch_bounds__( kTmaThreads ) k_cell_tma( LevelView v, OpView
                                                              int nC, int64_t stage_elems, const int4* __restrict__ tiles, int* err )
 {
    extern __shared__ __align__( 128 ) unsigned char smem_raw[];
-   __shared__ uint64_t bars[2];
-   T*                  stage[2] = { reinterpret_cast< T* >( smem_raw ), reinterpret_cast< T* >( smem_raw ) + stage_elems };
+   __shared__ uint64_t bars[kTmaStages];
+   T*                  stage0 = reinterpret_cast< T* >( smem_raw );
    const int           tid = threadIdx.x, n = v.n;
    const int           total = ntiles * nC;
    if ( tid == 0 )
    {
-      mbar_init( &bars[0], 1 );
-      mbar_init( &bars[1], 1 );
+      for ( int s = 0; s < kTmaStages; ++s ) mbar_init( &bars[s], 1 );
       asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
    }
    __syncthreads();
@@ -396,35 +407,43 @@ __global__ void __launch_bounds__( kTmaThreads ) k_cell_tma( LevelView v, OpView
       const int4    tl = tiles[t % ntiles];
       const int     z = tl.x, ya = tl.y, yb = tl.z;
       const T*      g  = src + v.cell_off[c];
+      T*            sm = stage0 + int64_t( st ) * stage_elems;
       TileRange     rs = tile_range< T >( n, ya - 1, yb + 1, z );
       TileRange     rt = tile_range< T >( n, ya - 1, yb, z + 1 );
       TileRange     rb = tile_range< T >( n, ya, yb + 1, z - 1 );
       const int64_t ns = rs.end - rs.first, nt = rt.end - rt.first, nb = rb.end - rb.first;
       mbar_expect_tx( &bars[st], uint32_t( ( ns + nt + nb ) * sizeof( T ) ) );
-      bulk_copy_g2s( stage[st], g + rs.first, uint32_t( ns * sizeof( T ) ), &bars[st] );
-      bulk_copy_g2s( stage[st] + ns, g + rt.first, uint32_t( nt * sizeof( T ) ), &bars[st] );
-      bulk_copy_g2s( stage[st] + ns + nt, g + rb.first, uint32_t( nb * sizeof( T ) ), &bars[st] );
+      bulk_copy_g2s( sm, g + rs.first, uint32_t( ns * sizeof( T ) ), &bars[st] );
+      bulk_copy_g2s( sm + ns, g + rt.first, uint32_t( nt * sizeof( T ) ), &bars[st] );
+      bulk_copy_g2s( sm + ns + nt, g + rb.first, uint32_t( nb * sizeof( T ) ), &bars[st] );
    };
-   auto active = [&]( int t ) { return ( v.cell_bc[t / ntiles] & flag ) != 0; };
+   auto next_active = [&]( int t ) {
+      while ( t < total && !( v.cell_bc[t / ntiles] & flag ) ) t += gridDim.x;
+      return t;
+   };
 
-   int t = blockIdx.x;
-   while ( t < total && !active( t ) ) t += gridDim.x;
-   if ( tid == 0 && t < total ) issue( t, 0 );
-   uint32_t phase[2] = { 0, 0 };
-   int      st       = 0;
+   // prologue: fill the first kTmaStages-1 stages
+   int tq[kTmaStages];
+   tq[0] = next_active( blockIdx.x );
+   for ( int s = 1; s < kTmaStages; ++s ) tq[s] = tq[s - 1] < total ? next_active( tq[s - 1] + gridDim.x ) : total;
+   if ( tid == 0 )
+      for ( int s = 0; s < kTmaStages - 1; ++s )
+         if ( tq[s] < total ) issue( tq[s], s );
+   uint32_t phase = 0;  // parity of stage 0; stage s uses the same parity within a round
+   int      st    = 0;
+   int      t     = tq[0];
+   int      ahead = tq[kTmaStages - 1];  // next item to issue
    while ( t < total )
    {
-      int tn = t + gridDim.x;
-      while ( tn < total && !active( tn ) ) tn += gridDim.x;
-      if ( tid == 0 && tn < total )
+      // refill the stage freed in the previous iteration with the item kTmaStages-1 ahead
+      if ( tid == 0 && ahead < total )
       {
          fence_proxy_async();
-         issue( tn, st ^ 1 );
+         issue( ahead, ( st + kTmaStages - 1 ) % kTmaStages );
       }
-      // bounded wait for the current stage
       int  spins    = 0;
       bool timedout = false;
-      while ( !mbar_try_wait( &bars[st], phase[st] ) )
+      while ( !mbar_try_wait( &bars[st], phase ) )
          if ( ++spins > kSpinLimit )
          {
             timedout = true;
@@ -433,73 +452,96 @@ __global__ void __launch_bounds__( kTmaThreads ) k_cell_tma( LevelView v, OpView
       if ( __syncthreads_or( timedout ) )
       {
          if ( tid == 0 ) atomicExch( err, 1 );
-         // give copies still in flight a bounded chance to land before the block exits
-         for ( int k = 0; k < kSpinLimit && !mbar_try_wait( &bars[st ^ 1], phase[st ^ 1] ); ++k ) {}
+         for ( int s = 0; s < kTmaStages; ++s )
+            for ( int k = 0; k < kSpinLimit && !mbar_try_wait( &bars[s], phase ); ++k ) {}
          return;
       }
-      phase[st] ^= 1u;
 
-      // compute the tile from shared memory
       {
          const int     c    = t / ntiles;
          const int4    tl   = tiles[t % ntiles];
          const int     z = tl.x, ya = tl.y, yb = tl.z;
          const int64_t base = v.cell_off[c];
+         T*            sm   = stage0 + int64_t( st ) * stage_elems;
          TileRange     rs   = tile_range< T >( n, ya - 1, yb + 1, z );
          TileRange     rt   = tile_range< T >( n, ya - 1, yb, z + 1 );
          TileRange     rb   = tile_range< T >( n, ya, yb + 1, z - 1 );
-         const T*      S    = stage[st] - rs.first;
-         const T*      Tt   = stage[st] + ( rs.end - rs.first ) - rt.first;
-         const T*      B    = stage[st] + ( rs.end - rs.first ) + ( rt.end - rt.first ) - rb.first;
+         const T*      S    = sm - rs.first;
+         const T*      Tt   = sm + ( rs.end - rs.first ) - rt.first;
+         const T*      B    = sm + ( rs.end - rs.first ) + ( rt.end - rt.first ) - rb.first;
          const A*      W    = o.W + size_t( c ) * kNumClasses * kNumDirs;
          const A w0 = W[0], wW = W[1], wE = W[2], wS = W[3], wN = W[4], wB = W[5], wT = W[6], wNW = W[7], wSE = W[8],
                  wTW = W[9], wBE = W[10], wTS = W[11], wBN = W[12], wTSE = W[13], wBNW = W[14];
-         const A invd = o.invd_c[c];
-         for ( int x = 1 + tid; x <= n - 1 - z - ya; x += kTmaThreads )
-         {
-            auto rd = [&]( const T* R, int yy, int zz, Row3< T, A >& r ) {
-               const T* p = R + cidx( n, x, yy, zz );
-               r.m        = A( p[-1] );
-               r.o        = A( p[0] );
-               r.p        = A( p[1] );
-            };
-            Row3< T, A > cm, c0, tm, b0, cp, t0, bp;
-            rd( S, ya - 1, z, cm );
-            rd( S, ya, z, c0 );
-            rd( Tt, ya - 1, z + 1, tm );
-            rd( B, ya, z - 1, b0 );
-            for ( int y = ya; y <= yb && x + y + z <= n - 1; ++y )
+         const A   invd = o.invd_c[c];
+         // threads -> (row group g, x): short rows get several row groups
+         const int len  = n - 1 - z - ya;
+         const int wx   = ( ( len + 31 ) / 32 ) * 32;
+         const int G    = wx >= kTmaThreads ? 1 : kTmaThreads / wx;
+         const int g    = tid / ( wx >= kTmaThreads ? kTmaThreads : wx );
+         const int xs   = wx >= kTmaThreads ? kTmaThreads : wx;
+         const int rows = yb - ya + 1;
+         const int per  = ( rows + G - 1 ) / G;
+         const int y0   = ya + g * per;
+         const int y1   = min( yb, y0 + per - 1 );
+         if ( g < G && y0 <= y1 )
+            for ( int x = 1 + tid % xs; x <= n - 1 - z - y0; x += xs )
             {
-               rd( S, y + 1, z, cp );
-               rd( Tt, y, z + 1, t0 );
-               rd( B, y + 1, z - 1, bp );
-               A acc = w0 * c0.o;
-               acc += wW * c0.m;
-               acc += wE * c0.p;
-               acc += wS * cm.o;
-               acc += wN * cp.o;
-               acc += wB * b0.o;
-               acc += wT * t0.o;
-               acc += wNW * cp.m;
-               acc += wSE * cm.p;
-               acc += wTW * t0.m;
-               acc += wBE * b0.p;
-               acc += wTS * tm.o;
-               acc += wBN * bp.o;
-               acc += wTSE * tm.p;
-               acc += wBNW * bp.m;
-               stencil_epilogue< T, A, OP >( base + cidx( n, x, y, z ), acc, invd, src, v1, v2, dst, a0, a1 );
-               cm = c0;
-               c0 = cp;
-               tm = t0;
-               b0 = bp;
+               auto rd = [&]( const T* R, int yy, int zz, Row3< T, A >& r ) {
+                  const T* p = R + cidx( n, x, yy, zz );
+                  r.m        = A( p[-1] );
+                  r.o        = A( p[0] );
+                  r.p        = A( p[1] );
+               };
+               Row3< T, A > cm, c0, tm, b0, cp, t0, bp;
+               rd( S, y0 - 1, z, cm );
+               rd( S, y0, z, c0 );
+               rd( Tt, y0 - 1, z + 1, tm );
+               rd( B, y0, z - 1, b0 );
+               for ( int y = y0; y <= y1 && x + y + z <= n - 1; ++y )
+               {
+                  rd( S, y + 1, z, cp );
+                  rd( Tt, y, z + 1, t0 );
+                  rd( B, y + 1, z - 1, bp );
+                  A acc = w0 * c0.o;
+                  acc += wW * c0.m;
+                  acc += wE * c0.p;
+                  acc += wS * cm.o;
+                  acc += wN * cp.o;
+                  acc += wB * b0.o;
+                  acc += wT * t0.o;
+                  acc += wNW * cp.m;
+                  acc += wSE * cm.p;
+                  acc += wTW * t0.m;
+                  acc += wBE * b0.p;
+                  acc += wTS * tm.o;
+                  acc += wBN * bp.o;
+                  acc += wTSE * tm.p;
+                  acc += wBNW * bp.m;
+                  stencil_epilogue< T, A, OP >( base + cidx( n, x, y, z ), acc, invd, src, v1, v2, dst, a0, a1 );
+                  cm = c0;
+                  c0 = cp;
+                  tm = t0;
+                  b0 = bp;
+               }
             }
-         }
       }
-      __syncthreads();  // every thread is done with stage st before it is refilled
-      st ^= 1;
-      t = tn;
+      __syncthreads();  // stage st is free again
+      st = ( st + 1 ) % kTmaStages;
+      if ( st == 0 ) phase ^= 1u;
+      t     = next_active( t + gridDim.x );
+      ahead = ahead < total ? next_active( ahead + gridDim.x ) : total;
    }
+}
+
+static int march_prefetch_distance()
+{
+   static int d = -1;
+   if ( d < 0 )
+   {
+      const char* e = getenv( "HYB_PREFETCH" );
+      d             = e ? std::max( 0, atoi( e ) ) : 8;
+   }
+   return d;
 }
 
 static int cell_kernel_variant()
@@ -598,7 +640,7 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
          const auto rb = tile_range< T >( v.n, tl[1], tl[2] + 1, tl[0] - 1 );
          stage         = std::max( stage, ( rs.end - rs.first ) + ( rt.end - rt.first ) + ( rb.end - rb.first ) );
       }
-      const size_t smem = size_t( 2 * stage ) * sizeof( T );
+      const size_t smem = size_t( kTmaStages ) * size_t( stage ) * sizeof( T );
       static int   s_sms = 0, s_set = 0;
       static size_t s_smem_set = 0;
       if ( !s_sms ) check_cuda( cudaDeviceGetAttribute( &s_sms, cudaDevAttrMultiProcessorCount, 0 ), "device attribute" );
@@ -620,7 +662,8 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
    else if ( cell_kernel_variant() >= 1 && v.nmarch > 0 && nC > 0 )
    {
       dim3 grid( ( v.nmarch + 7 ) / 8, nC );
-      k_cell_march< T, A, OP ><<< grid, 256, 0, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ) );
+      k_cell_march< T, A, OP ><<< grid, 256, 0, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ),
+                                                                  march_prefetch_distance() );
       ++ctx->launches;
    }
    else if ( v.nrows > 0 && nC > 0 )
@@ -658,6 +701,11 @@ static void dispatch_stencil( Context* ctx, const LevelView& v, const OpView< A 
 void launch_stencil( Context* ctx, Mesh* m, Operator* Op, int L, int dtype, const StencilArgs& a )
 {
    ensure_constants();
+   if ( Op->elementwise )
+   {
+      launch_elementwise( ctx, m, Op, L, dtype, a );
+      return;
+   }
    LevelView v  = make_view( m, L );
    OpLevel&  ol = Op->lv.at( L );
    ensure_device_op( ol );
@@ -884,6 +932,33 @@ void launch_axpy_to_f64( Context* ctx, int64_t count, double* x, int src_dtype, 
    else k_axpy_to_f64< __half ><<< blocks, 256, 0, ctx->stream >>>( count, x, (const __half*) c, a );
    ++ctx->launches;
    check_cuda( cudaGetLastError(), "axpy launch" );
+}
+
+// seeded uniform values in [-1, 1] (splitmix64 of seed and slot index), every slot of a level
+template < typename T >
+__global__ void k_fill_uniform( int64_t count, T* dst, uint64_t seed )
+{
+   for ( int64_t i = blockIdx.x * int64_t( blockDim.x ) + threadIdx.x; i < count; i += int64_t( gridDim.x ) * blockDim.x )
+   {
+      uint64_t z = seed + 0x9E3779B97F4A7C15ull * uint64_t( i + 1 );
+      z          = ( z ^ ( z >> 30 ) ) * 0xBF58476D1CE4E5B9ull;
+      z          = ( z ^ ( z >> 27 ) ) * 0x94D049BB133111EBull;
+      z ^= z >> 31;
+      const double u = double( z >> 11 ) * ( 1.0 / 9007199254740992.0 );
+      using Acc = typename AccT< T >::type;
+      stv( dst + i, Acc( 2.0 * u - 1.0 ) );
+   }
+}
+
+void launch_fill_uniform( Context* ctx, int64_t count, int dtype, void* dst, uint64_t seed )
+{
+   if ( count <= 0 ) return;
+   const int blocks = int( std::min< int64_t >( ( count + 255 ) / 256, 148 * 16 ) );
+   if ( dtype == F64 ) k_fill_uniform< double ><<< blocks, 256, 0, ctx->stream >>>( count, (double*) dst, seed );
+   else if ( dtype == F32 ) k_fill_uniform< float ><<< blocks, 256, 0, ctx->stream >>>( count, (float*) dst, seed );
+   else k_fill_uniform< __half ><<< blocks, 256, 0, ctx->stream >>>( count, (__half*) dst, seed );
+   ++ctx->launches;
+   check_cuda( cudaGetLastError(), "fill launch" );
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1182,14 +1257,19 @@ void launch_prolongate( Context* ctx, Mesh* m, int Lc, int dtype, uint32_t flag,
 }
 
 // allocate every lazily created device table for levels minL..maxL (needed before graph capture)
-void prepare_device( Context* ctx, Mesh* m, Operator* op, int minL, int maxL )
+void prepare_device( Context* ctx, Mesh* m, Operator* op, int minL, int maxL, int dtype )
 {
    ensure_constants();
    int most = 1;
    for ( int L = minL; L <= maxL; ++L )
    {
       LevelView v = make_view( m, L );
-      if ( op ) ensure_device_op( op->lv.at( L ) );
+      if ( op && !op->elementwise ) ensure_device_op( op->lv.at( L ) );
+      if ( op && op->elementwise )
+      {
+         ensure_elementwise_level( ctx, op, L, dtype );
+         if ( L == minL && dtype != F64 ) ensure_elementwise_level( ctx, op, L, F64 );
+      }
       const int nb = ( ( v.nrows + 7 ) / 8 ) * m->topo.nC + ( v.ntasks + 255 ) / 256 + 1;
       most         = std::max( most, nb );
    }

@@ -1,0 +1,385 @@
+// Serving loop: continuous admission of multigrid solve requests on one GPU.
+//
+// A request names a resident mesh, an operator (P1 Laplace or elementwise -div(k grad u) with
+// optional shell blending), a level, a right-hand side, a tolerance and the precision mode
+// (plain FP64 cycles, or FP64 defect correction around FP32 cycles).  Requests wait in a FIFO queue
+// and are admitted into "slots" as slots and the HBM budget allow.  A slot is a resident multigrid
+// hierarchy (operator tables, functions on every level, the solver with its CUDA graph) keyed by
+// (mesh, operator, coefficient, blending, level, precision); a finished request leaves its slot
+// idle so the next request with the same key reuses it without any setup (the captured graph is
+// replayed).  Every slot owns a context with its own stream, so the cycles of different solves
+// overlap on the device.  Each scheduler step launches one cycle on every running slot whose last
+// residual check has come back, followed by an asynchronous residual norm (device dot, copy to
+// pinned host memory, event); finished slots are retired as their events complete.  Kernels and
+// reduction orders inside a slot do not depend on what else runs, so a request's result is the same
+// alone and in a mix.
+#include "hyb_internal.hpp"
+#include "../../include/hyteg_b200.h"
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <random>
+#include <stdexcept>
+#include <vector>
+
+namespace hyb {
+double gmg_slot_bytes_estimate( Mesh* m, int minL, int maxL, int dtype, int elementwise );
+}
+
+struct ServeKey
+{
+   hyb_mesh* mesh;
+   int       kind;
+   int       blending;
+   int       level;
+   int       mixed;
+   double    k[6];
+   bool      operator<( const ServeKey& o ) const
+   {
+      if ( mesh != o.mesh ) return mesh < o.mesh;
+      if ( kind != o.kind ) return kind < o.kind;
+      if ( blending != o.blending ) return blending < o.blending;
+      if ( level != o.level ) return level < o.level;
+      if ( mixed != o.mixed ) return mixed < o.mixed;
+      return std::memcmp( k, o.k, sizeof( k ) ) < 0;
+   }
+   bool operator==( const ServeKey& o ) const { return !( *this < o ) && !( o < *this ); }
+};
+
+struct ServeRequest
+{
+   int64_t             id;
+   ServeKey            key;
+   hyb_coeff           coeff;
+   std::vector< double > rhs;  // packed host rhs (empty: seeded uniform [-1,1] on owned non-Dirichlet DoFs)
+   uint64_t            seed;
+   double              rtol;
+   int                 max_cycles;
+   double*             x_out;
+   double              t_arrival = 0, t_admit = -1, t_done = -1;
+   int                 state     = 0;  // 0 queued, 1 running, 2 done, 3 failed
+   int                 cycles    = 0;
+   double              r0 = 0, rn = 0;
+};
+
+struct ServeSlot
+{
+   ServeKey  key;
+   hyb_ctx*  ctx  = nullptr;
+   hyb_op*   op   = nullptr;
+   hyb_gmg*  gmg  = nullptr;
+   hyb_fn*   x    = nullptr;
+   hyb_fn*   b    = nullptr;
+   hyb_fn*   tmp  = nullptr;
+   double*   d_norm = nullptr;
+   double*   h_norm = nullptr;
+   cudaEvent_t ev = nullptr;
+   int64_t   req  = -1;
+   bool      pending = false;
+   double    bytes   = 0;
+   double    last_used = 0;
+   double    scale     = 1.0;  // mixed mode: residual scaling of the cycle in flight
+};
+
+struct hyb_serve
+{
+   hyb_ctx*                              ctx = nullptr;
+   hyb_serve_params                      p{};
+   std::deque< int64_t >                 queue;
+   std::map< int64_t, ServeRequest >     reqs;
+   std::vector< std::unique_ptr< ServeSlot > > slots;
+   double                                used_bytes = 0;
+   int64_t                               next_id    = 0;
+   std::chrono::steady_clock::time_point t0         = std::chrono::steady_clock::now();
+   double now() const { return std::chrono::duration< double >( std::chrono::steady_clock::now() - t0 ).count(); }
+};
+
+extern "C" int hyb_internal_residual_async( hyb_op* op, hyb_fn* x, hyb_fn* b, hyb_fn* tmp, int level, double* d_out );
+extern "C" int hyb_internal_mixed_step_async( hyb_gmg* g, int inner_dtype, hyb_op* op, hyb_fn* x, hyb_fn* b, int level, double rn,
+                                              double* d_out );
+extern "C" int hyb_fn_fill_random( hyb_fn* fn, int level, uint64_t seed );
+
+static thread_local std::string s_err;
+
+namespace {
+
+void ok( int rc )
+{
+   if ( rc != HYB_OK ) throw std::runtime_error( hyb_last_error() );
+}
+
+void free_slot( hyb_serve* s, ServeSlot* sl )
+{
+   if ( sl->ctx ) hyb_ctx_synchronize( sl->ctx );
+   if ( sl->ev ) cudaEventDestroy( sl->ev );
+   if ( sl->h_norm ) cudaFreeHost( sl->h_norm );
+   if ( sl->d_norm ) cudaFree( sl->d_norm );
+   hyb_gmg_destroy( sl->gmg );
+   hyb_fn_destroy( sl->x );
+   hyb_fn_destroy( sl->b );
+   hyb_fn_destroy( sl->tmp );
+   hyb_op_destroy( sl->op );
+   hyb_ctx_destroy( sl->ctx );
+   s->used_bytes -= sl->bytes;
+}
+
+// bytes a slot holds: x, b (all levels), tmp and the solver's temporaries (about six more vectors
+// per level), plus the elementwise scratch
+double slot_bytes( ServeKey k )
+{
+   int64_t total = 0;
+   for ( int L = 0; L <= k.level; ++L )
+   {
+      int64_t n = 0;
+      hyb_layout_packed_size( k.mesh, L, &n );
+      total += n;
+   }
+   return double( total ) * 8.0 * ( k.mixed ? 12.0 : 10.0 );
+}
+
+ServeSlot* make_slot( hyb_serve* s, const ServeRequest& r )
+{
+   auto sl = std::make_unique< ServeSlot >();
+   sl->key = r.key;
+   int dev = 0;
+   cudaGetDevice( &dev );
+   ok( hyb_ctx_create( dev, nullptr, &sl->ctx ) );
+   const int L = r.key.level;
+   if ( r.key.kind == HYB_P1_CONST_LAPLACE ) ok( hyb_op_create( sl->ctx, r.key.mesh, HYB_P1_CONST_LAPLACE, 0, L, &sl->op ) );
+   else ok( hyb_op_create_divkgrad( sl->ctx, r.key.mesh, 0, L, &r.coeff, r.key.blending, &sl->op ) );
+   hyb_gmg_params gp;
+   hyb_gmg_params_default( &gp );
+   gp.min_level             = 0;
+   gp.max_level             = L;
+   gp.pre_smooth            = s->p.pre_smooth;
+   gp.post_smooth           = s->p.post_smooth;
+   gp.smoother              = HYB_SMOOTHER_CHEBYSHEV;
+   gp.cheb_order            = 3;
+   gp.cheb_power_iterations = s->p.power_iterations;
+   gp.use_graph             = 1;
+   ok( hyb_gmg_create( sl->ctx, sl->op, &gp, &sl->gmg ) );
+   ok( hyb_fn_create( sl->ctx, r.key.mesh, HYB_F64, 0, L, &sl->x ) );
+   ok( hyb_fn_create( sl->ctx, r.key.mesh, HYB_F64, 0, L, &sl->b ) );
+   ok( hyb_fn_create( sl->ctx, r.key.mesh, HYB_F64, L, L, &sl->tmp ) );
+   if ( cudaMalloc( &sl->d_norm, sizeof( double ) ) != cudaSuccess ) throw std::runtime_error( "cudaMalloc(norm)" );
+   if ( cudaMallocHost( &sl->h_norm, sizeof( double ) ) != cudaSuccess ) throw std::runtime_error( "cudaMallocHost(norm)" );
+   if ( cudaEventCreateWithFlags( &sl->ev, cudaEventDisableTiming ) != cudaSuccess ) throw std::runtime_error( "cudaEventCreate" );
+   sl->bytes = slot_bytes( r.key );
+   s->used_bytes += sl->bytes;
+   s->slots.push_back( std::move( sl ) );
+   return s->slots.back().get();
+}
+
+// queue the work of the next cycle (or the initial residual when rn < 0) and its residual check
+void launch_cycle( hyb_serve* s, ServeSlot* sl, ServeRequest& r, double rn )
+{
+   const int L = r.key.level;
+   if ( r.key.mixed )
+      ok( hyb_internal_mixed_step_async( sl->gmg, s->p.inner_dtype, sl->op, sl->x, sl->b, L, rn < 0 ? 0.0 : rn, sl->d_norm ) );
+   else
+   {
+      if ( rn >= 0 ) ok( hyb_gmg_solve( sl->gmg, sl->x, sl->b, L ) );
+      ok( hyb_internal_residual_async( sl->op, sl->x, sl->b, sl->tmp, L, sl->d_norm ) );
+   }
+   void* st = nullptr;
+   hyb_ctx_stream( sl->ctx, &st );
+   if ( cudaMemcpyAsync( sl->h_norm, sl->d_norm, sizeof( double ), cudaMemcpyDeviceToHost, (cudaStream_t) st ) != cudaSuccess ||
+        cudaEventRecord( sl->ev, (cudaStream_t) st ) != cudaSuccess )
+      throw std::runtime_error( "residual check enqueue failed" );
+   sl->pending = true;
+}
+
+void admit( hyb_serve* s, ServeSlot* sl, ServeRequest& r )
+{
+   const int L = r.key.level;
+   sl->req     = r.id;
+   for ( int l = 0; l <= L; ++l ) ok( hyb_fn_interpolate_const( sl->x, 0.0, l, HYB_ALL ) );
+   if ( r.rhs.empty() ) ok( hyb_fn_fill_random( sl->b, L, r.seed ) );
+   else ok( hyb_fn_upload( sl->b, L, r.rhs.data() ) );
+   r.state   = 1;
+   r.t_admit = s->now();
+   r.cycles  = -1;  // the first check is the initial residual
+   launch_cycle( s, sl, r, -1.0 );
+}
+
+}  // namespace
+
+extern "C" {
+
+int hyb_serve_params_default( hyb_serve_params* p )
+{
+   if ( !p ) return HYB_EINVAL;
+   *p                  = hyb_serve_params{};
+   p->max_slots        = 32;
+   p->hbm_budget_bytes = 0;  // 0: 80 % of the free device memory at creation
+   p->inner_dtype      = HYB_F32;
+   p->pre_smooth       = 3;
+   p->post_smooth      = 3;
+   p->power_iterations = 20;
+   return HYB_OK;
+}
+
+int hyb_serve_create( hyb_ctx* ctx, const hyb_serve_params* params, hyb_serve** out )
+{
+   try
+   {
+      if ( !ctx || !params || !out ) throw std::invalid_argument( "NULL argument" );
+      if ( params->max_slots < 1 ) throw std::invalid_argument( "max_slots must be >= 1" );
+      if ( params->inner_dtype != HYB_F32 && params->inner_dtype != HYB_F16 ) throw std::invalid_argument( "inner dtype must be F32 or F16" );
+      auto* s = new hyb_serve();
+      s->ctx  = ctx;
+      s->p    = *params;
+      if ( s->p.hbm_budget_bytes <= 0 )
+      {
+         size_t fr = 0, tot = 0;
+         cudaMemGetInfo( &fr, &tot );
+         s->p.hbm_budget_bytes = 0.8 * double( fr );
+      }
+      *out = s;
+      return HYB_OK;
+   } catch ( const std::exception& e )
+   {
+      s_err = e.what();
+      return HYB_EINVAL;
+   }
+}
+
+int hyb_serve_destroy( hyb_serve* s )
+{
+   if ( !s ) return HYB_OK;
+   for ( auto& sl : s->slots ) free_slot( s, sl.get() );
+   delete s;
+   return HYB_OK;
+}
+
+double hyb_serve_now( hyb_serve* s ) { return s ? s->now() : 0.0; }
+
+int hyb_serve_submit( hyb_serve* s, const hyb_request* rq, int64_t* id )
+{
+   if ( !s || !rq || !rq->mesh ) return HYB_EINVAL;
+   if ( rq->op_kind != HYB_P1_CONST_LAPLACE && rq->op_kind != HYB_P1_ELEM_DIVKGRAD ) return HYB_EINVAL;
+   if ( rq->level < 1 || rq->level > 12 || !( rq->rtol > 0 ) || rq->max_cycles < 1 ) return HYB_EINVAL;
+   ServeRequest r;
+   r.id            = s->next_id++;
+   r.key.mesh      = rq->mesh;
+   r.key.kind      = rq->op_kind;
+   r.key.blending  = rq->op_kind == HYB_P1_ELEM_DIVKGRAD ? rq->blending : 0;
+   r.key.level     = rq->level;
+   r.key.mixed     = rq->mixed ? 1 : 0;
+   const double kk[6] = { double( rq->coeff.kind ), rq->coeff.value, rq->coeff.amp, rq->coeff.phase[0], rq->coeff.phase[1],
+                          rq->coeff.phase[2] };
+   for ( int i = 0; i < 6; ++i ) r.key.k[i] = rq->op_kind == HYB_P1_ELEM_DIVKGRAD ? kk[i] : 0.0;
+   r.coeff      = rq->coeff;
+   r.seed       = rq->seed;
+   r.rtol       = rq->rtol;
+   r.max_cycles = rq->max_cycles;
+   r.x_out      = rq->x_out;
+   r.t_arrival  = rq->arrival_time >= 0 ? rq->arrival_time : s->now();
+   if ( rq->rhs )
+   {
+      int64_t n = 0;
+      if ( hyb_layout_packed_size( rq->mesh, rq->level, &n ) != HYB_OK ) return HYB_EINVAL;
+      r.rhs.assign( rq->rhs, rq->rhs + n );
+   }
+   if ( slot_bytes( r.key ) > s->p.hbm_budget_bytes ) return HYB_ENOMEM;  // can never be admitted
+   const int64_t rid = r.id;
+   s->reqs.emplace( rid, std::move( r ) );
+   s->queue.push_back( rid );
+   if ( id ) *id = rid;
+   return HYB_OK;
+}
+
+int hyb_serve_step( hyb_serve* s, int* running, int* queued )
+{
+   if ( !s ) return HYB_EINVAL;
+   try
+   {
+      // 1. finished residual checks: retire or launch the next cycle
+      for ( auto& up : s->slots )
+      {
+         ServeSlot* sl = up.get();
+         if ( sl->req < 0 || !sl->pending ) continue;
+         if ( cudaEventQuery( sl->ev ) != cudaSuccess ) continue;
+         sl->pending      = false;
+         ServeRequest& r  = s->reqs.at( sl->req );
+         const double  rn = std::sqrt( std::max( 0.0, *sl->h_norm ) );
+         if ( r.cycles < 0 ) r.r0 = rn;
+         r.cycles += 1;
+         r.rn            = rn;
+         const bool conv = r.r0 == 0.0 || rn / r.r0 < r.rtol;
+         if ( conv || r.cycles >= r.max_cycles || !std::isfinite( rn ) )
+         {
+            if ( r.x_out ) ok( hyb_fn_download( sl->x, r.key.level, r.x_out ) );
+            r.t_done      = s->now();
+            r.state       = ( conv && std::isfinite( rn ) ) ? 2 : 3;
+            sl->req       = -1;
+            sl->last_used = r.t_done;
+         }
+         else
+            launch_cycle( s, sl, r, rn );
+      }
+      // 2. admission in arrival order, as slots and the memory budget allow
+      while ( !s->queue.empty() )
+      {
+         ServeRequest& r    = s->reqs.at( s->queue.front() );
+         ServeSlot*    slot = nullptr;
+         for ( auto& up : s->slots )
+            if ( up->req < 0 && up->key == r.key )
+            {
+               slot = up.get();
+               break;
+            }
+         if ( !slot )
+         {
+            const double need = slot_bytes( r.key );
+            // evict idle slots of other keys (least recently used first) until the new one fits
+            while ( ( s->used_bytes + need > s->p.hbm_budget_bytes || int( s->slots.size() ) >= s->p.max_slots ) )
+            {
+               int victim = -1;
+               for ( size_t i = 0; i < s->slots.size(); ++i )
+                  if ( s->slots[i]->req < 0 && ( victim < 0 || s->slots[i]->last_used < s->slots[victim]->last_used ) ) victim = int( i );
+               if ( victim < 0 ) break;
+               free_slot( s, s->slots[victim].get() );
+               s->slots.erase( s->slots.begin() + victim );
+            }
+            if ( s->used_bytes + need > s->p.hbm_budget_bytes || int( s->slots.size() ) >= s->p.max_slots ) break;
+            slot = make_slot( s, r );
+         }
+         admit( s, slot, r );
+         s->queue.pop_front();
+      }
+      int run = 0;
+      for ( auto& up : s->slots ) run += up->req >= 0;
+      if ( running ) *running = run;
+      if ( queued ) *queued = int( s->queue.size() );
+      return HYB_OK;
+   } catch ( const std::exception& e )
+   {
+      s_err = e.what();
+      return HYB_EDEVICE;
+   }
+}
+
+int hyb_serve_status( hyb_serve* s, int64_t id, int* state, double* t_arrival, double* t_admit, double* t_done, int* cycles,
+                      double* rel_res )
+{
+   if ( !s ) return HYB_EINVAL;
+   auto it = s->reqs.find( id );
+   if ( it == s->reqs.end() ) return HYB_EINVAL;
+   const ServeRequest& r = it->second;
+   if ( state ) *state = r.state;
+   if ( t_arrival ) *t_arrival = r.t_arrival;
+   if ( t_admit ) *t_admit = r.t_admit;
+   if ( t_done ) *t_done = r.t_done;
+   if ( cycles ) *cycles = std::max( r.cycles, 0 );
+   if ( rel_res ) *rel_res = r.r0 > 0 ? r.rn / r.r0 : 0.0;
+   return HYB_OK;
+}
+
+const char* hyb_serve_last_error( void ) { return s_err.c_str(); }
+
+}  // extern "C"

@@ -287,12 +287,17 @@ void build_level( Mesh* m, int L )
             for ( int y0 = 1; y0 <= ylast; y0 += YC ) P.march.push_back( { z, x0, y0, std::min( ylast, y0 + YC - 1 ) } );
          }
    }
-   // shared-memory staged tiles: TY interior rows of one slice per tile
+   // shared-memory staged tiles: rows y0..y1 of one slice, about 768 interior points per tile
    {
-      const int TY = n >= 512 ? 4 : 8;
-      P.tile_rows  = TY;
       for ( int z = 1; z <= n - 3; ++z )
-         for ( int y0 = 1; y0 <= n - 2 - z; y0 += TY ) P.tiles.push_back( { z, y0, std::min( n - 2 - z, y0 + TY - 1 ), 0 } );
+         for ( int y0 = 1; y0 <= n - 2 - z; )
+         {
+            const int len = n - 1 - z - y0;  // interior points of row y0
+            const int ty  = std::max( 2, std::min( 64, 768 / std::max( len, 1 ) ) );
+            const int y1  = std::min( n - 2 - z, y0 + ty - 1 );
+            P.tiles.push_back( { z, y0, y1, 0 } );
+            y0 = y1 + 1;
+         }
    }
    // cell interior rows (y, z), memory order
    for ( int z = 1; z <= n - 2; ++z )
@@ -529,6 +534,13 @@ Operator::~Operator()
       cudaFree( kv.second.d_invd_bf );
       cudaFree( kv.second.d_invd_cf );
    }
+   for ( auto& kv : el )
+   {
+      cudaFree( kv.second.d_acc );
+      for ( void* p : kv.second.d_invd ) cudaFree( p );
+      cudaFree( kv.second.d_hrows );
+   }
+   cudaFree( d_geom );
 }
 
 size_t Function::bytes( int L ) const { return size_t( mesh->level( L ).size ) * dtype_size( dtype ); }

@@ -49,6 +49,26 @@ extern "C" {
 #define HYB_P1_CONST_LAPLACE 1 /* P1ConstantLaplaceOperator, constant_stencil_operator/P1ConstantOperator.hpp:167 */
 #define HYB_P1_CONST_MASS 2    /* P1ConstantMassOperator, same file */
 
+#define HYB_P1_ELEM_DIVKGRAD 3 /* P1ElementwiseBlendingDivKGradOperator (elementwiseoperators/P1ElementwiseOperator.hpp:329-373)
+                                  with the form p1_div_k_grad_blending_q3 */
+
+/* blending maps (geometry/) */
+#define HYB_BLEND_NONE 0
+#define HYB_BLEND_SHELL 1 /* IcosahedralShellMap (geometry/IcosahedralShellMap.hpp) */
+
+/* coefficient families k(x) */
+#define HYB_COEFF_CONSTANT 0 /* k = value */
+#define HYB_COEFF_EXPSIN 1   /* k = exp(amp sin(2 pi f (x+p0)) cos(2 pi f (y+p1)) sin(2 pi f (z+p2))) */
+
+typedef struct hyb_coeff
+{
+   int    kind;
+   double value;
+   double amp;
+   double freq;
+   double phase[3];
+} hyb_coeff;
+
 /* smoother kinds */
 #define HYB_SMOOTHER_JACOBI 0    /* solvers/WeightedJacobiSmoother.hpp:46-66 */
 #define HYB_SMOOTHER_CHEBYSHEV 1 /* solvers/ChebyshevSmoother.hpp:112-240 */
@@ -85,6 +105,9 @@ int hyb_mesh_create( hyb_ctx* ctx, int nverts, const double* coords /* 3*nverts 
                      hyb_mesh** out );
 /* MeshInfo::meshCuboid (src/hyteg/mesh/MeshGenCuboid.cpp:35-172) */
 int hyb_mesh_create_cuboid( hyb_ctx* ctx, const double* lo, const double* hi, int nx, int ny, int nz, hyb_mesh** out );
+/* MeshInfo::meshSphericalShell(ntan, nrad, rmin, rmax) with the default SHELLMESH_CLASSIC flavour
+ * (src/hyteg/mesh/MeshGenSphericalShell.cpp:642-765); ntan-1 must be a power of two */
+int hyb_mesh_create_spherical_shell( hyb_ctx* ctx, int ntan, int nrad, double rmin, double rmax, hyb_mesh** out );
 /* MeshInfo::fromGmshFile, MSH 2.2 and 4.1 tetrahedral meshes (src/hyteg/mesh/GmshReaderForMSH22.hpp) */
 int hyb_mesh_create_gmsh( hyb_ctx* ctx, const char* path, hyb_mesh** out );
 int hyb_mesh_destroy( hyb_mesh* mesh );
@@ -96,6 +119,8 @@ int hyb_mesh_set_bc_type( hyb_mesh* mesh, int flag, uint32_t dof_type );
 int hyb_mesh_counts( const hyb_mesh* mesh, int* counts );
 /* kind 0 vertex, 1 edge, 2 face, 3 cell: vertex ids of primitive `id` in its local order (-1 padded) */
 int hyb_mesh_primitive_vertices( const hyb_mesh* mesh, int kind, int id, int* out4 );
+/* coordinates of all macro-vertices in id order (3 doubles each) */
+int hyb_mesh_vertex_coords( const hyb_mesh* mesh, double* out );
 /* mesh boundary flag of a primitive */
 int hyb_mesh_primitive_flag( const hyb_mesh* mesh, int kind, int id, int* flag );
 
@@ -144,6 +169,11 @@ int hyb_fn_device_ptr( hyb_fn* fn, int level, void** ptr, int64_t* nslots );
  * Operator<Src,Dst>::apply(src, dst, level, flag, updateType) (operators/Operator.hpp:74-81),
  * P1Operator::apply (p1functionspace/P1Operator.hpp:192-320). */
 int hyb_op_create( hyb_ctx* ctx, hyb_mesh* mesh, int kind, int min_level, int max_level, hyb_op** out );
+/* elementwise -div(k grad u) with the coefficient k (NULL: k = 1) and optional blending; every micro-cell's
+ * element matrix comes from 5-point degree-3 quadrature (p1_div_k_grad_blending_q3); smoothers use the
+ * assembled inverse diagonal (P1ElementwiseOperator::computeInverseDiagonalOperatorValues) */
+int hyb_op_create_divkgrad( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, const hyb_coeff* k, int blending,
+                            hyb_op** out );
 int hyb_op_destroy( hyb_op* op );
 int hyb_op_apply( hyb_op* op, hyb_fn* src, hyb_fn* dst, int level, uint32_t flag, int update );
 /* WeightedJacobiSmoothable::smooth_jac(dst, rhs, src, relax, level, flag) (solvers/Smoothables.hpp:33-40,
@@ -208,8 +238,54 @@ int hyb_cg_solve( hyb_op* op, hyb_fn* x, hyb_fn* b, int level, int max_iter, dou
  * max_outer steps; res_history receives ||r_0|| .. ||r_k|| (max_outer+1 entries). */
 int hyb_mixed_solve( hyb_gmg* inner, int inner_dtype, hyb_op* op, hyb_fn* x, hyb_fn* b, int level, int inner_cycles,
                      int max_outer, double rtol, double* res_history, int* outer_iters );
+/* fill every DoF of one level with seeded uniform values in [-1, 1] (device-side, reproducible) */
+int hyb_fn_fill_random( hyb_fn* fn, int level, uint64_t seed );
 /* discrete L2 norm of b - A x over the flagged DoFs */
 int hyb_residual_norm( hyb_op* op, hyb_fn* x, hyb_fn* b, hyb_fn* tmp, int level, uint32_t flag, double* out );
+
+/* ---------------------------------------------------------------- serving
+ * Continuous admission of solve requests (no counterpart in the reference, which solves one problem per
+ * run): requests wait in a FIFO queue and are admitted into resident multigrid "slots" keyed by (mesh,
+ * operator, coefficient, blending, level, precision) as slots and the HBM budget allow; idle slots are
+ * reused (no setup, the captured graph is replayed) or evicted least-recently-used; every slot runs on
+ * its own stream, so solves overlap on the device.  Chebyshev(3) V(pre,post) cycles with a CG coarse
+ * solve; mixed requests run FP64 defect correction around cycles in `inner_dtype`. */
+typedef struct hyb_serve hyb_serve;
+typedef struct hyb_serve_params
+{
+   int    max_slots;
+   double hbm_budget_bytes; /* 0: 80 % of the free device memory at creation */
+   int    inner_dtype;      /* HYB_F32 or HYB_F16 for mixed requests */
+   int    pre_smooth, post_smooth;
+   int    power_iterations; /* spectral-radius estimate per level when a slot is created */
+} hyb_serve_params;
+typedef struct hyb_request
+{
+   hyb_mesh*     mesh;
+   int           op_kind;  /* HYB_P1_CONST_LAPLACE or HYB_P1_ELEM_DIVKGRAD */
+   hyb_coeff     coeff;    /* HYB_P1_ELEM_DIVKGRAD only */
+   int           blending; /* HYB_P1_ELEM_DIVKGRAD only */
+   int           level;
+   const double* rhs;      /* packed level layout, or NULL for seeded uniform values */
+   uint64_t      seed;
+   double        rtol;     /* stop when ||r||/||r_0|| < rtol */
+   int           max_cycles;
+   int           mixed;        /* 0 plain FP64 cycles, 1 mixed-precision defect correction */
+   double        arrival_time; /* seconds on the server clock (hyb_serve_now); < 0: now */
+   double*       x_out;        /* packed solution on completion, or NULL */
+} hyb_request;
+int    hyb_serve_params_default( hyb_serve_params* p );
+int    hyb_serve_create( hyb_ctx* ctx, const hyb_serve_params* params, hyb_serve** out );
+int    hyb_serve_destroy( hyb_serve* s );
+double hyb_serve_now( hyb_serve* s );
+/* HYB_ENOMEM if the request could never fit the budget */
+int hyb_serve_submit( hyb_serve* s, const hyb_request* r, int64_t* id );
+/* one scheduler pass: retire finished solves, launch next cycles, admit queued requests */
+int hyb_serve_step( hyb_serve* s, int* running, int* queued );
+/* state: 0 queued, 1 running, 2 converged, 3 stopped without converging */
+int hyb_serve_status( hyb_serve* s, int64_t id, int* state, double* t_arrival, double* t_admit, double* t_done, int* cycles,
+                      double* rel_res );
+const char* hyb_serve_last_error( void );
 
 #ifdef __cplusplus
 }

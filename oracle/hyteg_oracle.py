@@ -782,3 +782,259 @@ def cell_prolongate(coarse, Lc, nc14, fine=None):
                    0.5 * coarse[cell_index(nc, a[:, 0], a[:, 1], a[:, 2])] + 0.5 * coarse[cell_index(nc, b[:, 0], b[:, 1], b[:, 2])])
     out[cell_index(nf, fp[:, 0], fp[:, 1], fp[:, 2])] += _cell_class_weight(fp, nf, nc14) * val
     return out
+
+
+# ---------------------------------------------------------------------------------------------
+# spherical shell (MeshGenSphericalShell.cpp, SHELLMESH_CLASSIC)
+# ---------------------------------------------------------------------------------------------
+def mesh_spherical_shell(ntan, nrad, rmin, rmax):
+    """meshSphericalShell(ntan, nrad, rmin, rmax): layers equidistant in radius
+    (MeshGenSphericalShell.cpp:642-660), icosahedral diamonds refined by great-circle midpoints
+    (setupCoordsClassic, :420-560), vertices numbered poles first (vertIdx2Tuple / tuple2VertIdx,
+    :76-195) and every local cell split into six tetrahedra with hemisphere-specific tables
+    (:581-640, getCell :326-380)."""
+    assert nrad >= 2 and 0 < rmin < rmax
+    layers = [rmin + ((rmax - rmin) / (nrad - 1)) * k for k in range(nrad)]
+    nt = ntan
+    assert nt >= 2 and ((nt - 1) & (nt - 2)) == 0
+    fifthpi = 0.4 * math.asin(1.0)
+    w = 2.0 * math.acos(1.0 / (2.0 * math.sin(fifthpi)))
+    ico = np.zeros((12, 3))
+    ico[0] = (0, 0, 1.0)
+    ico[11] = (0, 0, -1.0)
+    for k in range(1, 6):
+        phi = 2.0 * (k - 0.5) * fifthpi
+        ico[k] = (math.sin(w) * math.cos(phi), math.sin(w) * math.sin(phi), math.cos(w))
+        phl = 2.0 * (k - 1) * fifthpi
+        ico[k + 5] = (math.sin(w) * math.cos(phl), math.sin(w) * math.sin(phl), -math.cos(w))
+    dia = [(0, 5, 6, 1), (0, 1, 7, 2), (0, 2, 8, 3), (0, 3, 9, 4), (0, 4, 10, 5),
+           (11, 7, 1, 6), (11, 8, 2, 7), (11, 9, 3, 8), (11, 10, 4, 9), (11, 6, 5, 10)]
+    N = np.zeros((nt, nt, 10, 3))
+
+    def mid(a, b):
+        s = a + b
+        return s / math.sqrt(float(s @ s))
+
+    for d in range(10):
+        L_, R_ = (1, 3) if d < 5 else (3, 1)
+        N[0, 0, d] = ico[dia[d][0]]
+        N[nt - 1, 0, d] = ico[dia[d][L_]]
+        N[nt - 1, nt - 1, d] = ico[dia[d][2]]
+        N[0, nt - 1, d] = ico[dia[d][R_]]
+        m = 1
+        while m < nt - 1:
+            l = (nt - 1) // m
+            l2 = l // 2
+            for j1 in range(m + 1):
+                for j2 in range(m):
+                    i1, i2 = j1 * l, j2 * l + l2
+                    N[i1, i2, d] = mid(N[i1, i2 - l2, d], N[i1, i2 + l2, d])
+            for j1 in range(m + 1):
+                for j2 in range(m):
+                    i1, i2 = j2 * l + l2, j1 * l
+                    N[i1, i2, d] = mid(N[i1 - l2, i2, d], N[i1 + l2, i2, d])
+            for j1 in range(m):
+                for j2 in range(m):
+                    i1, i2 = j1 * l + l2, j2 * l + l2
+                    N[i1, i2, d] = mid(N[i1 - l2, i2 + l2, d], N[i1 + l2, i2 - l2, d])
+            m *= 2
+    nv = (10 * (nt - 1) ** 2 + 2) * nrad
+    coords = np.zeros((nv, 3))
+    for v in range(nv):
+        if v >= 2 * nrad:
+            idx = v - 2 * nrad
+            ir, idx = divmod(idx, 10 * (nt - 1) ** 2)
+            d, idx = divmod(idx, (nt - 1) ** 2)
+            is2, is1 = divmod(idx, nt - 1)
+            is2 += 1
+        elif v < nrad:
+            is1, is2, d, ir = 0, 0, 0, v
+        else:
+            is1, is2, d, ir = 0, 0, 5, v - nrad
+        coords[v] = N[is1, is2, d] * layers[ir]
+
+    def vidx(is1, is2, d, ir):
+        if is1 == 0 and is2 == 0:
+            return ir if d < 5 else nrad + ir
+        if is2 == 0:
+            is1, is2 = 0, is1
+            d = (d + 4) % 5 if d < 5 else (d + 4) % 5 + 5
+        elif is1 == nt - 1:
+            is1, is2 = (nt - 1) - is2, nt - 1
+            d = (d + 4) % 5 + 5 if d < 5 else d % 5
+        return ir * (nt - 1) ** 2 * 10 + d * (nt - 1) ** 2 + (is2 - 1) * (nt - 1) + is1 + 2 * nrad
+
+    off = [(0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1), (0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0)]
+    north = [(0, 1, 3, 7), (4, 7, 5, 0), (0, 5, 1, 7), (1, 2, 3, 6), (5, 7, 6, 1), (3, 6, 7, 1)]
+    south = [(4, 7, 5, 1), (0, 1, 3, 4), (4, 3, 7, 1), (7, 6, 5, 2), (3, 1, 2, 7), (5, 2, 1, 7)]
+    tets = []
+    for e in range((nt - 1) ** 2 * (nrad - 1) * 60):
+        idx = e
+        ir, idx = divmod(idx, 60 * (nt - 1) ** 2)
+        d, idx = divmod(idx, 6 * (nt - 1) ** 2)
+        is2, idx = divmod(idx, 6 * (nt - 1))
+        is1, it = divmod(idx, 6)
+        vk = []
+        for o in off:
+            ks1 = is1 + (o[0] if d <= 4 else o[1])
+            ks2 = is2 + (o[1] if d <= 4 else o[0])
+            vk.append(vidx(ks1, ks2, d, ir + o[2]))
+        tab = north if d <= 4 else south
+        tets.append(tuple(vk[t] for t in tab[it]))
+    return coords, tets
+
+
+# ---------------------------------------------------------------------------------------------
+# variable-coefficient diffusion with blending (p1_div_k_grad_blending_q3)
+# ---------------------------------------------------------------------------------------------
+# Yu's 5-point degree-3 rule on the reference tetrahedron (volume 1/6): centroid weight -2/15,
+# four points with barycentric weights (1/2, 1/6, 1/6, 1/6) and weight 3/40 each.
+YU5_POINTS = np.array([[0.25, 0.25, 0.25], [1 / 6, 1 / 6, 1 / 6], [0.5, 1 / 6, 1 / 6], [1 / 6, 0.5, 1 / 6],
+                       [1 / 6, 1 / 6, 0.5]])
+YU5_WEIGHTS = np.array([-2.0 / 15.0, 3.0 / 40.0, 3.0 / 40.0, 3.0 / 40.0, 3.0 / 40.0])
+_GHAT = np.array([[-1.0, -1.0, -1.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]])
+
+
+def k_expsin(amp=0.5, phase=(0.0, 0.0, 0.0)):
+    """k(x) = exp(amp sin(2 pi (x+px)) cos(2 pi (y+py)) sin(2 pi (z+pz)))."""
+    tp = 2.0 * math.pi
+
+    def k(P):
+        return np.exp(amp * np.sin(tp * (P[..., 0] + phase[0])) * np.cos(tp * (P[..., 1] + phase[1]))
+                      * np.sin(tp * (P[..., 2] + phase[2])))
+    return k
+
+
+def p1_divkgrad_element(X, kfun, blend=None, rule=(YU5_POINTS, YU5_WEIGHTS)):
+    """Element matrices of -div(k grad u) for P1 on tets X (m, 4, 3) given in computational
+    coordinates; blend (optional) maps computational to physical space (F, DF)."""
+    J = np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], axis=2)
+    K = np.zeros((X.shape[0], 4, 4))
+    for xi, w in zip(*rule):
+        Xq = X[:, 0] + np.einsum("kij,j->ki", J, xi)
+        if blend is None:
+            M, Fq = J, Xq
+        else:
+            M, Fq = np.einsum("kij,kjl->kil", blend.DF(Xq), J), blend.F(Xq)
+        det = np.abs(np.linalg.det(M))
+        G = np.einsum("id,kdj->kij", _GHAT, np.linalg.inv(M))
+        K += (w * kfun(Fq) * det)[:, None, None] * np.einsum("kid,kjd->kij", G, G)
+    return K
+
+
+class TestMap:
+    """Smooth non-affine blending used to pin the form: F(x) = x (1 + a x0 x1)."""
+
+    def __init__(self, a):
+        self.a = a
+
+    def F(self, X):
+        return X * (1.0 + self.a * X[:, 0] * X[:, 1])[:, None]
+
+    def DF(self, X):
+        s = 1.0 + self.a * X[:, 0] * X[:, 1]
+        g = np.stack([self.a * X[:, 1], self.a * X[:, 0], np.zeros(len(X))], axis=1)
+        return s[:, None, None] * np.eye(3)[None] + X[:, :, None] * g[:, None, :]
+
+
+class IcosahedralShellMap:
+    """Blending of a shell macro-cell (geometry/IcosahedralShellMap.hpp:109-146, classifyVertices
+    :606-705): the barycentric weight of refVertex in the tet (ray, ref, thr, for) sets the radius
+    between the ray and ref radii; points are projected radially."""
+
+    def __init__(self, mesh: MacroMesh, c, tol=1e-14):
+        ref, ray, thr, fo = self._classify(mesh, c, tol)
+        self.ref, self.ray, self.thr, self.fo = ref, ray, thr, fo
+        self.rad_ref, self.rad_ray = np.linalg.norm(ref), np.linalg.norm(ray)
+        self.bxc = np.cross(thr - ray, fo - ray)
+        self.volT = float((ref - ray) @ self.bxc)
+
+    @staticmethod
+    def _classify(mesh, c, tol):
+        P = mesh.vcoords[list(mesh.cells[c])]
+        rad = np.linalg.norm(P, axis=1)
+        inner, outer = rad.min(), rad.max()
+        eps = (outer - inner) * 0.001
+        n_outer = int(np.sum((outer - rad) < eps))
+        pair = None
+        for k in range(4):
+            for j in range(k + 1, 4):
+                cr = np.cross(P[k], P[j])
+                if np.all(np.abs(cr) / (rad[k] * rad[j]) <= tol):
+                    pair = (k, j)
+                    break
+            if pair:
+                break
+        assert pair is not None, "no radial vertex pair"
+        iref, iray = pair
+        if n_outer == 2:  # skew: use a non-skew neighbour of the same prism
+            vref, vray = mesh.cells[c][iref], mesh.cells[c][iray]
+            for f in mesh.cell_faces[c]:
+                fv = mesh.faces[f]
+                if not (vref in fv and vray in fv):
+                    other = [cc for cc in mesh.f_cells[f] if cc != c]
+                    return IcosahedralShellMap._classify(mesh, other[0], tol)
+            raise AssertionError("no non-skew neighbour")
+        rest = [k for k in range(4) if k not in (iref, iray)]
+        ithr, ifor = rest[-1], rest[0]
+        if (n_outer == 1 and rad[iref] < rad[iray]) or (n_outer == 3 and rad[iref] > rad[iray]):
+            iref, iray = iray, iref
+        return P[iref].copy(), P[iray].copy(), P[ithr].copy(), P[ifor].copy()
+
+    def F(self, X):
+        bary = np.abs(((X - self.ray) @ self.bxc) / self.volT)
+        new_rad = self.rad_ray + bary * (self.rad_ref - self.rad_ray)
+        return X * (new_rad / np.linalg.norm(X, axis=1))[:, None]
+
+    def DF(self, X):
+        r = np.linalg.norm(X, axis=1)
+        bary = ((X - self.ray) @ self.bxc) / self.volT
+        sgn = np.sign(bary)
+        R = self.rad_ray + np.abs(bary) * (self.rad_ref - self.rad_ray)
+        gradR = (self.rad_ref - self.rad_ray) * (sgn[:, None] * self.bxc[None, :] / self.volT)
+        s = R / r
+        grads = gradR / r[:, None] - (R / r ** 3)[:, None] * X
+        return s[:, None, None] * np.eye(3)[None] + X[:, :, None] * grads[:, None, :]
+
+
+class P1DivKGrad(P1ConstantLaplace):
+    """P1ElementwiseBlendingDivKGradOperator (elementwiseoperators/P1ElementwiseOperator.cpp) with
+    p1_div_k_grad_blending_q3: assembled from micro-cell element matrices with the coefficient k and,
+    for blending="shell", the IcosahedralShellMap of every macro-cell."""
+
+    def __init__(self, mesh, minL, maxL, kfun, blending=None):
+        self.mesh, self.minL, self.maxL = mesh, minL, maxL
+        self.maps = [IcosahedralShellMap(mesh, c) for c in range(mesh.nC)] if blending == "shell" else None
+        self.levels = {L: Level(mesh, L) for L in range(minL, maxL + 1)}
+        self.A = {}
+        for L in range(minL, maxL + 1):
+            lev = self.levels[L]
+            rows, cols, vals = [], [], []
+            for c in range(mesh.nC):
+                slots, X = lev.micro_cells(c)
+                K = p1_divkgrad_element(X.reshape(-1, 4, 3), kfun, None if self.maps is None else _PerPointMap(self.maps[c]))
+                rows.append(np.repeat(slots, 4, axis=1).ravel())
+                cols.append(np.tile(slots, (1, 4)).ravel())
+                vals.append(K.reshape(K.shape[0], 16).ravel())
+            A = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                              shape=(lev.size, lev.size)).tocsr()
+            A.sum_duplicates()
+            self.A[L] = A
+        self.invdiag = {}
+        for L, A in self.A.items():
+            d = A.diagonal()
+            inv = np.zeros_like(d)
+            own = self.levels[L].owned
+            inv[own] = 1.0 / d[own]
+            self.invdiag[L] = inv
+
+
+class _PerPointMap:
+    def __init__(self, m):
+        self.m = m
+
+    def F(self, X):
+        return self.m.F(X)
+
+    def DF(self, X):
+        return self.m.DF(X)

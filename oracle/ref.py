@@ -63,3 +63,16 @@ def p1_diffusion_element(X):
     A = np.zeros(16)
     lib().ref_p1_diffusion_element(_p(np.ascontiguousarray(X, dtype=np.float64).ravel()), _p(A))
     return A.reshape(4, 4)
+
+
+def p1_divkgrad_blending_element(X, map_kind=0, map_a=0.0, k_amp=0.5, k_phase=(0.0, 0.0, 0.0)):
+    """Element matrix from the reference's p1_div_k_grad_blending_q3 form with a test blending map
+    (0 identity, 1 F(x) = x (1 + a x0 x1)) and k = exp(amp sin cos sin)."""
+    L = lib()
+    f = L.ref_p1_divkgrad_blending_element
+    dp = C.POINTER(C.c_double)
+    f.argtypes = [dp, C.c_int, C.c_double, C.c_double, dp, dp]
+    A = np.zeros(16)
+    ph = np.asarray(k_phase, dtype=np.float64)
+    f(_p(np.ascontiguousarray(X, dtype=np.float64).ravel()), map_kind, map_a, k_amp, _p(ph), _p(A))
+    return A.reshape(4, 4)

@@ -9,6 +9,8 @@
 //   src/hyteg/forms/form_fenics_generated/p1_tet_diffusion.h (tabulate_tensor)
 #include <map>
 #include <omp.h>
+#include <cmath>
+#include <memory>
 
 #include "apply_3D_macrocell_vertexdof_to_vertexdof_replace.hpp"
 #include "hyteg/forms/form_fenics_generated/p1_tet_diffusion.h"
@@ -68,3 +70,54 @@ void ref_p1_diffusion_element( const double* coords12, double* A16 )
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// HyTeG-generated P1 variable-coefficient diffusion form with blending
+// (src/hyteg/forms/form_hyteg_generated/p1/p1_div_k_grad_blending_q3.cpp)
+// ---------------------------------------------------------------------------------------------
+#include "hyteg/forms/form_hyteg_generated/p1/p1_div_k_grad_blending_q3.hpp"
+
+namespace {
+// test blending maps: 0 identity; 1 F(x) = x (1 + a x0 x1) (a smooth non-affine map of the tests)
+struct TestMap : public hyteg::GeometryMap
+{
+   int    kind = 0;
+   double a    = 0;
+   void   evalF( const hyteg::Point3D& x, hyteg::Point3D& F ) const override
+   {
+      const double s = kind == 1 ? 1.0 + a * x[0] * x[1] : 1.0;
+      F              = hyteg::Point3D( x[0] * s, x[1] * s, x[2] * s );
+   }
+   double evalDF( const hyteg::Point3D& x, hyteg::Matrix3r& D ) const override
+   {
+      const double s    = kind == 1 ? 1.0 + a * x[0] * x[1] : 1.0;
+      const double g[3] = { kind == 1 ? a * x[1] : 0.0, kind == 1 ? a * x[0] : 0.0, 0.0 };
+      for ( int i = 0; i < 3; ++i )
+         for ( int j = 0; j < 3; ++j ) D( i, j ) = ( i == j ? s : 0.0 ) + x[i] * g[j];
+      return D( 0, 0 ) * ( D( 1, 1 ) * D( 2, 2 ) - D( 1, 2 ) * D( 2, 1 ) ) - D( 0, 1 ) * ( D( 1, 0 ) * D( 2, 2 ) - D( 1, 2 ) * D( 2, 0 ) ) +
+             D( 0, 2 ) * ( D( 1, 0 ) * D( 2, 1 ) - D( 1, 1 ) * D( 2, 0 ) );
+   }
+};
+}  // namespace
+
+extern "C" void ref_p1_divkgrad_blending_element( const double* coords12, int map_kind, double map_a, double k_amp,
+                                                   const double* k_phase3, double* A16 )
+{
+   auto   map   = std::make_shared< TestMap >();
+   map->kind    = map_kind;
+   map->a       = map_a;
+   const double amp = k_amp;
+   const double ph[3] = { k_phase3[0], k_phase3[1], k_phase3[2] };
+   auto k3 = [amp, ph]( const hyteg::Point3D& p ) {
+      const double tp = 2.0 * 3.14159265358979323846;
+      return std::exp( amp * std::sin( tp * ( p[0] + ph[0] ) ) * std::cos( tp * ( p[1] + ph[1] ) ) * std::sin( tp * ( p[2] + ph[2] ) ) );
+   };
+   auto                                   k2 = []( const hyteg::Point3D& ) { return 1.0; };
+   hyteg::forms::p1_div_k_grad_blending_q3 form( k3, k2 );
+   form.setGeometryMap( map );
+   std::array< hyteg::Point3D, 4 > c;
+   for ( int v = 0; v < 4; ++v ) c[v] = hyteg::Point3D( coords12[3 * v], coords12[3 * v + 1], coords12[3 * v + 2] );
+   hyteg::Matrix< double, 4, 4 > M;
+   form.integrateAll( c, M );
+   for ( int i = 0; i < 16; ++i ) A16[i] = M.a[i];
+}

@@ -102,3 +102,21 @@ def test_gmsh_reader(tmp_path):
     pm = H.PrimitiveStorage.from_gmsh(str(p))
     assert pm.counts() == (5, 9, 7, 2)
     assert pm.primitive_vertices(3, 0) == [0, 1, 2, 3]
+
+
+@pytest.mark.parametrize("ntan", [2, 3, 5])
+def test_spherical_shell_matches_reference_generator(ntan):
+    """MeshGenTest.cpp:120-122 counts for (5, 3): 486 vertices, 2724 edges, 4160 faces, 1920 cells."""
+    coords, tets = O.mesh_spherical_shell(ntan, 3, 0.55, 1.0)
+    om = O.MacroMesh(coords, tets)
+    pm = H.PrimitiveStorage.spherical_shell(ntan, 3, 0.55, 1.0)
+    assert pm.counts() == (om.nV, om.nE, om.nF, om.nC)
+    if ntan == 5:
+        assert pm.counts() == (486, 2724, 4160, 1920)
+    for i, v in enumerate(om.cells):
+        assert pm.primitive_vertices(3, i) == list(v)
+    np.testing.assert_allclose(pm.vertex_coords(), coords, rtol=0, atol=1e-15)
+    r = np.linalg.norm(coords, axis=1)
+    assert np.allclose(np.sort(np.unique(np.round(r, 12))), [0.55, 0.775, 1.0])
+    with pytest.raises(H.HybError):
+        H.PrimitiveStorage.spherical_shell(4, 3, 0.55, 1.0)  # ntan-1 not a power of two (SHELLMESH_CLASSIC)

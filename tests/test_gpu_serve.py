@@ -1,0 +1,112 @@
+"""GPU tests of the solve server (continuous admission into resident multigrid slots).
+
+Every slot owns its vectors, hierarchy, captured cycle graph and stream, and every reduction is
+deterministic (no atomics), so a request must give the SAME bits whether it ran alone or inside a
+mix of concurrent requests, and the same bits as the plain solver API driven with the same
+parameters (Chebyshev(3) V(3,3) cycles, 20 power iterations, stop at ||r||/||r0|| < rtol)."""
+
+import numpy as np
+import pytest
+
+import hyteg_b200 as H
+
+pytestmark = pytest.mark.gpu
+
+K_SPEC = ("expsin", 0.5, (0.13, 0.27, 0.41))
+
+
+def _meshes(ctx):
+    return {"cube": H.PrimitiveStorage.cuboid(ctx=ctx), "shell": H.PrimitiveStorage.spherical_shell(3, 2, 0.55, 1.0, ctx=ctx)}
+
+
+def _requests():
+    # (mesh, level, kind, k, blending, seed, mixed)
+    return [
+        ("cube", 4, "laplace", None, None, 11, False),
+        ("cube", 5, "laplace", None, None, 12, False),
+        ("shell", 3, "divkgrad", K_SPEC, "shell", 13, False),
+        ("cube", 4, "laplace", None, None, 14, True),
+        ("shell", 3, "divkgrad", 2.0, "shell", 15, False),
+        ("cube", 5, "laplace", None, None, 16, True),
+        ("cube", 4, "divkgrad", K_SPEC, None, 17, False),
+        ("cube", 4, "laplace", None, None, 18, False),
+    ]
+
+
+def _submit(srv, meshes, req, rtol=1e-8):
+    m, L, kind, k, bl, seed, mixed = req
+    return srv.submit(meshes[m], L, kind=kind, k=k, blending=bl, seed=seed, rtol=rtol, max_cycles=40, mixed=mixed,
+                      want_solution=True)
+
+
+def _solve_alone(ctx, meshes, req):
+    srv = H.SolveServer(ctx, max_slots=4)
+    rid = _submit(srv, meshes, req)
+    srv.drain()
+    st = srv.status(rid)
+    x = srv.solution(rid).copy()
+    srv.close()
+    return st, x
+
+
+def test_serve_mix_equals_alone(ctx):
+    meshes = _meshes(ctx)
+    reqs = _requests()
+    srv = H.SolveServer(ctx, max_slots=6)
+    ids = [_submit(srv, meshes, r) for r in reqs]
+    srv.drain()
+    for r, rid in zip(reqs, ids):
+        st = srv.status(rid)
+        assert st["state"] == H.CONVERGED, (r, st)
+        assert st["rel_res"] < 1e-8
+        assert st["t_arrival"] <= st["t_admit"] <= st["t_done"]
+        st1, x1 = _solve_alone(ctx, meshes, r)
+        assert st1["cycles"] == st["cycles"], r
+        np.testing.assert_array_equal(srv.solution(rid), x1)
+    srv.close()
+
+
+def test_serve_matches_plain_solver(ctx):
+    """A plain FP64 request reproduces GeometricMultigridSolver.solve_cycles bit for bit."""
+    pm = H.PrimitiveStorage.cuboid(ctx=ctx)
+    L = 5
+    srv = H.SolveServer(ctx, max_slots=2)
+    rid = srv.submit(pm, L, seed=7, rtol=1e-8, max_cycles=40, want_solution=True)
+    srv.drain()
+    st = srv.status(rid)
+    A = H.P1ConstantLaplaceOperator(pm, 0, L, ctx)
+    gmg = H.GeometricMultigridSolver(ctx, A, 0, L, 3, 3, smoother="chebyshev", chebyshev_order=3, power_iterations=20)
+    x = H.P1Function("x", pm, 0, L, ctx)
+    b = H.P1Function("b", pm, 0, L, ctx)
+    b.fill_random(L, 7)
+    hist = gmg.solve_cycles(x, b, L, 40, rtol=1e-8)
+    assert len(hist) - 1 == st["cycles"]
+    assert abs(hist[-1] / hist[0] - st["rel_res"]) <= 1e-12 * max(1e-30, st["rel_res"])
+    np.testing.assert_array_equal(x.download(L), srv.solution(rid))
+    srv.close()
+
+
+def test_serve_mixed_precision_reaches_fp64_accuracy(ctx):
+    pm = H.PrimitiveStorage.cuboid(ctx=ctx)
+    L = 5
+    srv = H.SolveServer(ctx, max_slots=2)
+    a = srv.submit(pm, L, seed=3, rtol=1e-9, max_cycles=40, want_solution=True)
+    b = srv.submit(pm, L, seed=3, rtol=1e-9, max_cycles=40, mixed=True, want_solution=True)
+    srv.drain()
+    assert srv.status(a)["state"] == H.CONVERGED and srv.status(b)["state"] == H.CONVERGED
+    xa, xb = srv.solution(a), srv.solution(b)
+    assert np.abs(xa - xb).max() <= 1e-7 * np.abs(xa).max()
+    srv.close()
+
+
+def test_serve_budget_evicts_and_rejects(ctx):
+    pm = H.PrimitiveStorage.cuboid(ctx=ctx)
+    per = pm.packed_size(4) * 8 * 10 * 1.2  # about one L4 slot
+    srv = H.SolveServer(ctx, max_slots=8, hbm_budget_bytes=per * 1.5)
+    ids = [srv.submit(pm, 4, kind="divkgrad" if i % 2 else "laplace", seed=i, rtol=1e-8, want_solution=True) for i in range(4)]
+    srv.drain()
+    for i, rid in enumerate(ids):
+        assert srv.status(rid)["state"] == H.CONVERGED
+    with pytest.raises(H.HybError):
+        srv.submit(pm, 7, seed=1)  # can never fit the budget
+    srv.close()

@@ -184,3 +184,42 @@ def test_cg_solves_small_system():
     g = O.GMG(op, tr, L, L, cg_tol=1e-12)
     g.cg(x, b, L)
     assert O.residual_norm(op, x, b, L) / np.linalg.norm(b[mask]) < 1e-11
+
+
+def test_divkgrad_with_unit_coefficient_is_the_laplacian():
+    """p1_div_k_grad with k = 1 and no blending reproduces the P1 Laplace operator."""
+    coords, tets = M.octahedron_8()
+    m = O.MacroMesh(coords, tets)
+    lap = O.P1ConstantLaplace(m, 2, 2)
+    dk = O.P1DivKGrad(m, 2, 2, lambda P: np.ones(P.shape[:-1]))
+    own = np.flatnonzero(lap.levels[2].owned_mask(O.ALL))
+    D = (lap.A[2] - dk.A[2]).tocsr()[own][:, own]
+    assert abs(D).max() < 1e-13
+
+
+@pytest.mark.skipif(not R.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("map_kind,a", [(0, 0.0), (1, 0.3)])
+def test_divkgrad_element_matches_reference_form(map_kind, a):
+    """p1_div_k_grad_blending_q3 compiled from the reference sources, with a test blending map."""
+    rng = np.random.default_rng(11)
+    X = rng.uniform(0, 1, (5, 4, 3))
+    K = O.p1_divkgrad_element(X, O.k_expsin(0.5, (0.1, 0.2, 0.3)), None if map_kind == 0 else O.TestMap(a))
+    Kr = np.stack([R.p1_divkgrad_blending_element(x, map_kind, a, 0.5, (0.1, 0.2, 0.3)) for x in X])
+    np.testing.assert_allclose(K, Kr, rtol=0, atol=1e-13 * np.abs(Kr).max())
+
+
+def test_shell_map_derivative_and_vertices():
+    coords, tets = O.mesh_spherical_shell(3, 3, 0.55, 1.0)
+    m = O.MacroMesh(coords, tets)
+    rng = np.random.default_rng(4)
+    for c in (0, 17, 123, 300, 479):
+        B = O.IcosahedralShellMap(m, c)
+        P = m.vcoords[list(m.cells[c])]
+        np.testing.assert_allclose(B.F(P), P, atol=1e-15)
+        X = P.mean(axis=0)[None] + 0.01 * rng.standard_normal((4, 3))
+        D = B.DF(X)
+        h = 1e-6
+        for j in range(3):
+            e = np.zeros(3)
+            e[j] = h
+            np.testing.assert_allclose(D[:, :, j], (B.F(X + e) - B.F(X - e)) / (2 * h), atol=1e-8)
