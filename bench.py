@@ -47,6 +47,9 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--level", type=int, default=LEVEL)
     p.add_argument("--no-vcycle", action="store_true")
+    p.add_argument("--no-mixed", action="store_true")
+    p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--serve-requests", type=int, default=200)
     return p.parse_args()
 
 
@@ -163,6 +166,117 @@ def cpu_reference_apply(L, seconds=10.0, max_steps=None, threads=None):
             break
     cell_inner = ncell * O.tet_size(n - 3) if n >= 4 else 0
     return cell_inner * k / el / 1e6, k, threads, el
+
+
+def mixed_precision_leg(H, ctx, pm, A, L, rtol=1e-8):
+    """Time to ||r||/||r0|| < rtol from a zero guess: plain FP64 V(3,3) Chebyshev(3) cycles against
+    FP64 defect correction around the same cycles in FP32 and FP16 storage (FP32 accumulation).
+    Each solution's error is measured against an FP64 solution converged to 1e-13."""
+    import torch
+
+    b = H.P1Function("b_mp", pm, 0, L, ctx)
+    b.fill_random(L, 2024)
+    out = {"rtol": rtol, "level": L, "cycle": "V(3,3) Chebyshev(3), CG coarse level 0 (FP64)", "rhs": "seeded uniform [-1,1]"}
+    gmg = H.GeometricMultigridSolver(ctx, A, 0, L, preSmoothSteps=3, postSmoothSteps=3, smoother="chebyshev",
+                                     chebyshev_order=3, power_iterations=20)
+    xr = H.P1Function("x_ref", pm, 0, L, ctx)
+    gmg.solve_cycles(xr, b, L, 40, rtol=1e-13)
+    x_ref = xr.download(L)
+    nref = float(np.linalg.norm(x_ref))
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        ctx.synchronize()
+        return r, time.perf_counter() - t0
+
+    runs = {}
+    x = H.P1Function("x_mp", pm, 0, L, ctx)
+    for name in ("fp64", "fp32", "fp16"):
+        best = None
+        for rep in range(2):  # first run also captures the cycle graphs of this precision
+            for lv in range(0, L + 1):
+                x.interpolate(0.0, lv, H.All)
+            if name == "fp64":
+                hist, sec = timed(lambda: gmg.solve_cycles(x, b, L, 60, rtol=rtol))
+            else:
+                hist, sec = timed(lambda: gmg.mixed_solve(A, x, b, L, inner_dtype="float" + name[2:], inner_cycles=1,
+                                                          max_outer=60, rtol=rtol))
+            if best is None or sec < best[1]:
+                best = (hist, sec)
+        hist, sec = best
+        err = float(np.linalg.norm(x.download(L) - x_ref)) / nref
+        runs[name] = {"seconds": sec, "cycles": len(hist) - 1, "rel_residual": float(hist[-1] / hist[0]),
+                      "rel_error_vs_fp64_solution": err}
+    for name in ("fp32", "fp16"):
+        runs[name]["speedup_vs_fp64"] = runs["fp64"]["seconds"] / runs[name]["seconds"]
+    out["runs"] = runs
+    return out
+
+
+def serving_leg(H, ctx, nreq=200, seed=7):
+    """A bounded sample of the serving stream: `nreq` requests (Poisson arrivals at a rate above what
+    the GPU sustains), each a P1 Poisson or div-k-grad solve on the 6-tet cube (levels 3-7) or the
+    icosahedral shell ntan=3 (levels 3-5, shell blending for div-k-grad), k = exp(0.5 sin cos sin)
+    with one of two phases, rtol 1e-8, mixed precision (FP32 inner, FP64 outer).  Every hierarchy is
+    set up once before timing (warm slots).  Baseline: the same requests one after another as plain
+    FP64 solves on the same warm hierarchies."""
+    rng = np.random.default_rng(seed)
+    meshes = {"cube": H.PrimitiveStorage.cuboid(ctx=ctx), "shell": H.PrimitiveStorage.spherical_shell(3, 2, 0.55, 1.0, ctx=ctx)}
+    phases = [(0.13, 0.27, 0.41), (0.71, 0.05, 0.33)]
+    reqs = []
+    for i in range(nreq):
+        m = "cube" if rng.random() < 0.5 else "shell"
+        L = int(rng.integers(3, 8 if m == "cube" else 6))
+        kind = "laplace" if rng.random() < 0.3 else "divkgrad"
+        ph = phases[int(rng.integers(0, 2))]
+        reqs.append((m, L, kind, ("expsin", 0.5, ph) if kind == "divkgrad" else None,
+                     "shell" if (m == "shell" and kind == "divkgrad") else None, int(rng.integers(1, 2**31))))
+    keys = sorted(set((r[0], r[1], r[2], r[3], r[4]) for r in reqs), key=str)
+
+    def run(mixed, sequential):
+        srv = H.SolveServer(ctx, max_slots=len(keys) + 2)
+        for k in keys:  # warm every slot (operator, radii, captured cycle graphs)
+            srv.submit(meshes[k[0]], k[1], kind=k[2], k=k[3], blending=k[4], seed=1, rtol=1e-8, mixed=mixed)
+        srv.drain()
+        ctx.synchronize()
+        ids = []
+        t0 = srv.now()
+        if sequential:
+            for r in reqs:
+                ids.append(srv.submit(meshes[r[0]], r[1], kind=r[2], k=r[3], blending=r[4], seed=r[5], rtol=1e-8,
+                                      max_cycles=60, mixed=mixed))
+                srv.drain()
+        else:
+            gaps = rng.exponential(0.0005, nreq)  # mean inter-arrival 0.5 ms
+            arrivals = t0 + np.cumsum(gaps)
+            i = 0
+            while True:
+                now = srv.now()
+                while i < nreq and arrivals[i] <= now:
+                    r = reqs[i]
+                    ids.append(srv.submit(meshes[r[0]], r[1], kind=r[2], k=r[3], blending=r[4], seed=r[5], rtol=1e-8,
+                                          max_cycles=60, mixed=mixed, arrival_time=float(arrivals[i])))
+                    i += 1
+                run_, q = srv.step()
+                if i >= nreq and run_ == 0 and q == 0:
+                    break
+        t1 = srv.now()
+        sts = [srv.status(j) for j in ids]
+        srv.close()
+        lat = np.array([s["t_done"] - s["t_arrival"] for s in sts])
+        ok = sum(1 for s in sts if s["state"] == H.CONVERGED)
+        return {"solves_per_s": nreq / (t1 - t0), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3), "converged": ok, "seconds": t1 - t0}
+
+    served = run(mixed=True, sequential=False)
+    seq = run(mixed=False, sequential=True)
+    return {"requests": nreq, "distinct_hierarchies": len(keys),
+            "sample": "cube L3-7 / shell(ntan=3,nrad=2) L3-5, P1 Poisson 30% / div-k-grad 70%, 2 coefficient phases, "
+                      "Poisson arrivals mean 0.5 ms",
+            "served_mixed": served, "sequential_plain_fp64": seq,
+            "speedup_solves_per_s": served["solves_per_s"] / seq["solves_per_s"]}
 
 
 def run_reference(args, rank, world):
@@ -284,6 +398,8 @@ def run_ours(args, rank, world, local):
 
     if rank != 0:
         return
+    mixed = None if args.no_mixed else mixed_precision_leg(H, ctx, pm, A, L)
+    serving = None if args.no_serve else serving_leg(H, ctx, nreq=args.serve_requests)
     peak, peak_kind = measured_peak()
     alg_bytes = 2 * 8 * ndof  # read x, write y per inner DoF
     achieved = alg_bytes / (ms * 1e-3) / 1e9
@@ -298,13 +414,17 @@ def run_ours(args, rank, world, local):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "traffic": profile_traffic(),
                      "algorithmic_bytes_per_launch": alg_bytes,
-                     "kernel": "k_cell_stencil<double,OP_APPLY> + k_bnd_stencil (one apply)"},
+                     "kernel": "k_cell_zstream<double,OP_APPLY> + k_bnd_stencil (one apply)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": packed * 8, "d2h_bytes_per_step": packed * 8},
         "gpu_launches": launches,
         "clocks": clk.summary(),
     }
     if vcycle:
         line["vcycle"] = vcycle
+    if mixed:
+        line["mixed_precision"] = mixed
+    if serving:
+        line["serving"] = serving
     if cpu:
         rate, k, threads, el = cpu
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",

@@ -1293,8 +1293,19 @@ static void set_coefficients( hyb_gmg* g )
 {
    g->coeff.clear();
    for ( size_t i = 0; i < g->radii.size(); ++i )
-      g->coeff.push_back( chebyshev_coefficients( g->p.cheb_order, g->p.cheb_lower_factor * g->radii[i],
-                                                  g->p.cheb_upper_factor * g->radii[i] ) );
+   {
+      // the coarsest level is solved by CG, never smoothed: its radius is not used
+      if ( i == 0 )
+      {
+         g->coeff.push_back( {} );
+         continue;
+      }
+      const double r = g->radii[i];
+      if ( !( r > 0 ) || !std::isfinite( r ) )
+         throw std::runtime_error( "spectral radius estimate of level " + std::to_string( g->p.min_level + int( i ) ) +
+                                   " is not positive: " + std::to_string( r ) );
+      g->coeff.push_back( chebyshev_coefficients( g->p.cheb_order, g->p.cheb_lower_factor * r, g->p.cheb_upper_factor * r ) );
+   }
    if ( g->gexec ) cudaGraphExecDestroy( g->gexec ), g->gexec = nullptr;
 }
 

@@ -100,6 +100,9 @@ struct Topology {
 };
 
 // per-level host + device tables of the P1 layout
+// tile of the z-streamed cell sweep: 32 x-points (one per lane) by 8 rows (one per warp)
+constexpr int kZTileX = 32, kZTileY = 8;
+
 struct P1Level {
    int     L = 0, n = 0;
    int64_t size = 0;         // slots incl. padding
@@ -116,10 +119,11 @@ struct P1Level {
    // y-marching work items of the cell stencil sweep: (z, x0, y_first, y_last); a warp covers
    // x0..x0+31 of slice z and marches over rows y_first..y_last
    std::vector< std::array< int, 4 > > march;
-   // shared-memory staged sweep: tiles (z, y_first, y_last) covering the interior rows of a slice,
-   // and the largest shared-memory stage (bytes, FP64) any tile needs
-   std::vector< std::array< int, 4 > > tiles;
-   int                                 tile_rows = 0;
+   // z-streamed sweep: units {x0, y0, z_first, z_last}, each a kZTileX x kZTileY tile of slice
+   // columns over a range of slices; block b of the sweep runs units zbegin[b]..zbegin[b+1]-1
+   // (assigned longest-first to the least loaded block)
+   std::vector< std::array< int, 4 > > zunits;
+   std::vector< int >                  zbegin;
    int64_t n_owned_cell = 0;
    // device copies
    int64_t*   d_off       = nullptr;  // all primitives
@@ -128,7 +132,8 @@ struct P1Level {
    int4*      d_tasks     = nullptr;
    int2*      d_rows      = nullptr;
    int4*      d_march     = nullptr;
-   int4*      d_tiles     = nullptr;
+   int4*      d_zunits    = nullptr;
+   int*       d_zbegin    = nullptr;
    uint8_t*   d_bc        = nullptr;  // bc type per primitive (v, e, f, c order)
    int8_t*    d_bkind     = nullptr;  // 0 vertex, 1 edge, 2 face per boundary primitive
    float*     d_ncell_cls = nullptr;  // per cell, per class: number of macro-cells around the sub-primitive
@@ -295,6 +300,7 @@ void launch_cg_scalar( Context* ctx, double* state, int stage, double rtol, doub
 void check_cuda( cudaError_t e, const char* what );
 void build_level( Mesh* m, int L );
 void ensure_device( Mesh* m, P1Level& P );
+void build_zunits( P1Level& P, int nblocks );
 void build_operator_level( Operator* A, int L );
 void ensure_device_op( OpLevel& ol );
 

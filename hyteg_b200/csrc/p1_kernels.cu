@@ -26,9 +26,12 @@ __constant__ uint16_t c_cls_mask[kNumClasses];
 __constant__ int8_t   c_mask_to_cls[16];
 
 static bool g_const_ready = false;
+static void zstream_attributes_all();
+// constant tables and kernel attributes; called before any stream capture (prepare_device)
 static void ensure_constants()
 {
    if ( g_const_ready ) return;
+   zstream_attributes_all();
    check_cuda( cudaMemcpyToSymbol( c_dirs, kDirs, sizeof( kDirs ) ), "constants(dirs)" );
    check_cuda( cudaMemcpyToSymbol( c_cls_mask, kClassDirMask, sizeof( kClassDirMask ) ), "constants(mask)" );
    int8_t m2c[16];
@@ -107,9 +110,9 @@ struct LevelView
    const float*     ncell_cls;
    int              nmarch;
    const int4*      march;
-   int              ntiles;
-   const int4*      tiles;
-   const std::vector< std::array< int, 4 > >* host_tiles;
+   int              nzblocks;
+   const int4*      zunits;
+   const int*       zbegin;
 };
 
 template < typename A >
@@ -140,9 +143,9 @@ static LevelView make_view( Mesh* m, int L )
    v.ncell_cls = P.d_ncell_cls;
    v.nmarch     = int( P.march.size() );
    v.march      = P.d_march;
-   v.ntiles     = int( P.tiles.size() );
-   v.tiles      = P.d_tiles;
-   v.host_tiles = &P.tiles;
+   v.nzblocks   = int( P.zbegin.size() ) - 1;
+   v.zunits     = P.d_zunits;
+   v.zbegin     = P.d_zbegin;
    return v;
 }
 
@@ -324,15 +327,25 @@ __global__ void __launch_bounds__( 256 ) k_cell_march( LevelView v, OpView< A > 
 
 
 // ---------------------------------------------------------------------------------------------
-// Shared-memory staged cell sweep (cp.async.bulk + mbarrier, two stages).
+// z-streamed cell sweep (cp.async.bulk + mbarrier ring), the default for n >= 32.
 //
-// A tile is TY interior rows y_first..y_last of slice z of one macro-cell.  Its input lives in three
-// contiguous ranges of the cell array: rows y_first-1..y_last+1 of slice z, rows y_first-1..y_last of
-// slice z+1 and rows y_first..y_last+1 of slice z-1.  One thread issues the three bulk copies of the
-// next tile into the other stage while the block computes the current one; every thread owns one
-// x (or a few) and marches over the tile's rows, rolling the rows through registers and reading
-// three new rows per step from shared memory.  Bytes in flight no longer depend on registers.
-// Each wait on an mbarrier is bounded; if it runs out the block records an error and returns.
+// A unit is the tile x0..x0+31, y0..y0+7 of slices z_first..z_last of one macro-cell.  A producer
+// warp streams the tile's rows of every slice, with a one-point halo in x and y, into a ring of
+// shared-memory stages: lane r issues one bulk copy for row y0-1+r (10 rows per stage), and the
+// stage's full barrier completes when all bytes have landed.  Eight consumer warps (one per tile
+// row, one x per lane) march up the slices.  Of the 15 stencil values, four in slice z-1 and four
+// in slice z were read in the previous step and roll through registers, so a step reads three
+// values of slice z and four of slice z+1 from shared memory, and slice z is released (empty
+// barrier, one arrival per consumer warp) as soon as step z ends.  With S stages, S-2 slices are
+// in flight per block, independent of registers.
+//
+// Global rows start at arbitrary element offsets, while a bulk copy needs 16-byte aligned source,
+// destination and size: each row copy is widened to 16-byte boundaries and its shift (0..al-1
+// elements) is published with the stage as 3-bit fields of one word.
+//
+// Every wait is bounded by the global timer.  When one runs out the block records an error in
+// *err, raises a block-wide abort flag, stops issuing copies, waits (bounded) for the copies it
+// has in flight and returns.
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smem_addr( const void* p ) { return uint32_t( __cvta_generic_to_shared( p ) ); }
 
@@ -344,6 +357,11 @@ __device__ __forceinline__ void mbar_init( uint64_t* bar, uint32_t count )
 __device__ __forceinline__ void mbar_expect_tx( uint64_t* bar, uint32_t bytes )
 {
    asm volatile( "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"( smem_addr( bar ) ), "r"( bytes ) : "memory" );
+}
+
+__device__ __forceinline__ void mbar_arrive( uint64_t* bar )
+{
+   asm volatile( "mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"( smem_addr( bar ) ) : "memory" );
 }
 
 __device__ __forceinline__ bool mbar_try_wait( uint64_t* bar, uint32_t parity )
@@ -363,174 +381,359 @@ __device__ __forceinline__ void bulk_copy_g2s( void* dst, const void* src, uint3
                  : "memory" );
 }
 
-__device__ __forceinline__ void fence_proxy_async() { asm volatile( "fence.proxy.async.shared::cta;" ::: "memory" ); }
-
-// element range [first, end) of rows r0..r1 of slice zz, widened to 16-byte boundaries
-struct TileRange
+// 16-byte asynchronous global->shared copy (L2 only) and the mbarrier arrival that fires once all
+// earlier cp.async of this thread have landed (the barrier's expected count covers it: noinc)
+__device__ __forceinline__ void cp_async16( void* dst, const void* src )
 {
-   int64_t first, end;
-};
-
-template < typename T >
-__host__ __device__ __forceinline__ TileRange tile_range( int n, int r0, int r1, int zz )
-{
-   constexpr int64_t al = 16 / sizeof( T );
-   const int64_t     a  = cidx( n, 0, r0, zz );
-   const int64_t     b  = cidx( n, 0, r1 + 1, zz );
-   return TileRange{ a / al * al, ( b + al - 1 ) / al * al };
+   asm volatile( "cp.async.cg.shared.global [%0], [%1], 16;" ::"r"( smem_addr( dst ) ), "l"( src ) : "memory" );
 }
 
-constexpr int kTmaThreads = 256;
-constexpr int kTmaStages  = 3;
-constexpr int kSpinLimit  = 1 << 22;
+__device__ __forceinline__ void cp_async_arrive( uint64_t* bar )
+{
+   asm volatile( "cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"( smem_addr( bar ) ) : "memory" );
+}
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+   uint64_t t;
+   asm volatile( "mov.u64 %0, %%globaltimer;" : "=l"( t ) );
+   return t;
+}
+
+// A healthy wait lasts microseconds; one second means the copy or the partner warps are gone.
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
+
+// bounded wait for the completion of phase `parity`; false if it ran out or (when abort_flag is
+// given) another warp of the block aborted
+__device__ __forceinline__ bool mbar_wait_bounded( uint64_t* bar, uint32_t parity, const volatile int* abort_flag )
+{
+   if ( mbar_try_wait( bar, parity ) ) return true;
+   const uint64_t t0 = global_ns();
+   for ( ;; )
+   {
+      if ( mbar_try_wait( bar, parity ) ) return true;
+      if ( abort_flag && *abort_flag ) return false;
+      if ( global_ns() - t0 > kWaitLimitNs ) return false;
+   }
+}
+
+// Ops whose epilogue reads a second vector at the point (b for residual, Jacobi and the first
+// Chebyshev step, the running update for the later ones, dst itself for apply-add) stage that
+// vector's tile rows (no halo) in the same stage, so no step waits on a global load.
+template < int OP >
+__host__ __device__ constexpr bool zstream_aux()
+{
+   return OP == OP_APPLY_ADD || OP == OP_RESID || OP == OP_JAC || OP == OP_CHEB0 || OP == OP_CHEBI || OP == OP_CHEBL;
+}
+
+template < typename T, bool AUX >
+struct ZCfg
+{
+   static constexpr int al    = 16 / int( sizeof( T ) );                         // elements per 16 bytes
+   static constexpr int RW    = ( kZTileX + 2 + 2 * al + al - 1 ) / al * al;    // source row width (elements)
+   static constexpr int RWA   = ( kZTileX + 2 * al + al - 1 ) / al * al;        // second-vector row width
+   static constexpr int rows  = kZTileY + 2;                                   // tile rows + halo
+   static constexpr int aux0  = rows * RW;                                     // second-vector rows start here
+   static constexpr int stage = aux0 + ( AUX ? kZTileY * RWA : 0 );            // elements per stage
+   static constexpr int S     = sizeof( T ) == 8 ? 12 : ( sizeof( T ) == 4 ? 16 : 24 );  // ring depth
+   static constexpr size_t smem_bytes = size_t( S ) * stage * sizeof( T );
+};
+constexpr int kZWarps   = kZTileY;
+constexpr int kZThreads = ( kZWarps + 1 ) * 32;  // consumer warps + one producer warp
+
+// producer warp: streams the rows of every slice of the block's units into the ring.  Lane r < 10
+// copies source row y0-1+r; with AUX, lane 10+r copies row y0+r of the second vector (slices
+// z_first..z_last only, rows with interior points only).
+//
+// Two ways to fill a stage: `bulk` issues one cp.async.bulk per row segment (the full barrier
+// expects one arrival plus the bytes); otherwise the 32 lanes copy the row segments in 16-byte
+// cp.async pieces, one row per warp instruction, and each lane arrives on the full barrier when its
+// copies have landed (the barrier expects 32 arrivals).
+template < typename T, bool AUX >
+__device__ __forceinline__ void zstream_produce( const LevelView& v, uint32_t flag, const T* __restrict__ src,
+                                                 const T* __restrict__ aux, int nC, T* ring, uint64_t* full, uint64_t* empty,
+                                                 uint32_t* shw, volatile int* abort_flag, int* err, bool bulk )
+{
+   using Cfg = ZCfg< T, AUX >;
+   constexpr int S = Cfg::S, AL = Cfg::al;
+   const int     lane = threadIdx.x & 31, n = v.n;
+   const int     u0 = v.zbegin[blockIdx.x], u1 = v.zbegin[blockIdx.x + 1];
+   int           ld = 0;  // sequence number of the next slice load
+   bool          ok = true;
+   for ( int c = 0; c < nC && ok; ++c )
+   {
+      if ( !( v.cell_bc[c] & flag ) ) continue;
+      const int64_t cb = v.cell_off[c];
+      for ( int u = u0; u < u1 && ok; ++u )
+      {
+         const int4 U = v.zunits[u];  // x0, y0, z_first, z_last
+         for ( int zz = U.z - 1; zz <= U.w + 1; ++zz, ++ld )
+         {
+            const int st = ld % S;
+            if ( ld >= S && !mbar_wait_bounded( &empty[st], uint32_t( ( ld / S - 1 ) & 1 ), abort_flag ) )
+            {
+               ok = false;
+               break;
+            }
+            uint32_t bytes = 0, sh = 0;
+            int64_t  a0 = 0;
+            int      dsto = 0;
+            const T* gsrc = src;
+            if ( lane < Cfg::rows )
+            {
+               const int yy = U.y - 1 + lane;
+               if ( yy + zz <= n && n - yy - zz >= U.x - 1 )
+               {
+                  const int64_t s0 = cidx( n, U.x - 1, yy, zz );
+                  const int     xe = min( U.x + kZTileX, n - yy - zz );  // last x of the segment
+                  const int64_t e1 = s0 + ( xe - ( U.x - 1 ) ) + 1;       // one past the segment
+                  sh               = uint32_t( s0 & ( AL - 1 ) );
+                  a0               = s0 - sh;
+                  bytes            = uint32_t( ( ( e1 + AL - 1 ) / AL * AL - a0 ) * int64_t( sizeof( T ) ) );
+                  dsto             = lane * Cfg::RW;
+               }
+            }
+            else if ( AUX && lane < Cfg::rows + kZTileY && zz >= U.z && zz <= U.w )
+            {
+               const int r = lane - Cfg::rows, yy = U.y + r;
+               if ( n - 1 - yy - zz >= U.x )
+               {
+                  const int64_t s0 = cidx( n, U.x, yy, zz );
+                  const int     xe = min( U.x + kZTileX - 1, n - 1 - yy - zz );
+                  const int64_t e1 = s0 + ( xe - U.x ) + 1;
+                  sh               = uint32_t( s0 & ( AL - 1 ) );
+                  a0               = s0 - sh;
+                  bytes            = uint32_t( ( ( e1 + AL - 1 ) / AL * AL - a0 ) * int64_t( sizeof( T ) ) );
+                  dsto             = Cfg::aux0 + r * Cfg::RWA;
+                  gsrc             = aux;
+               }
+            }
+            const uint32_t total = __reduce_add_sync( 0xffffffffu, bytes );
+            const uint32_t w0    = __reduce_or_sync( 0xffffffffu, lane < Cfg::rows ? sh << ( 3 * lane ) : 0u );
+            const uint32_t w1 =
+                __reduce_or_sync( 0xffffffffu, ( lane >= Cfg::rows && lane < Cfg::rows + kZTileY ) ? sh << ( 3 * ( lane - Cfg::rows ) ) : 0u );
+            if ( bulk )
+            {
+               if ( lane == 0 )
+               {
+                  shw[2 * st]     = w0;
+                  shw[2 * st + 1] = w1;
+                  mbar_expect_tx( &full[st], total );
+               }
+               __syncwarp();
+               if ( bytes ) bulk_copy_g2s( ring + st * Cfg::stage + dsto, gsrc + cb + a0, bytes, &full[st] );
+            }
+            else
+            {
+               if ( lane == 0 )
+               {
+                  shw[2 * st]     = w0;
+                  shw[2 * st + 1] = w1;
+               }
+               T* sbase = ring + st * Cfg::stage;
+               for ( int r = 0; r < Cfg::rows + ( AUX ? kZTileY : 0 ); ++r )
+               {
+                  const uint32_t rb = __shfl_sync( 0xffffffffu, bytes, r );
+                  if ( rb == 0 ) continue;
+                  const int64_t ra0 = __shfl_sync( 0xffffffffu, a0, r );
+                  const int     rd  = __shfl_sync( 0xffffffffu, dsto, r );
+                  const T*      gp  = ( r < Cfg::rows ? src : aux ) + cb + ra0;
+                  if ( uint32_t( lane ) * 16u < rb ) cp_async16( sbase + rd + lane * AL, gp + lane * AL );
+               }
+               cp_async_arrive( &full[st] );
+            }
+         }
+      }
+   }
+   if ( !ok && lane == 0 )
+   {
+      atomicExch( err, 1 );
+      *abort_flag = 1;
+   }
+   // drain: the latest load issued on every stage has landed before the block may exit
+   if ( lane == 0 )
+      for ( int s = 0; s < S && s < ld; ++s )
+      {
+         const int j = s + ( ( ld - 1 - s ) / S ) * S;
+         if ( !mbar_wait_bounded( &full[s], uint32_t( ( j / S ) & 1 ), nullptr ) ) atomicExch( err, 1 );
+      }
+}
+
+// epilogue of the z-streamed sweep: the centre of src and the second vector come from the stage
+template < typename T, typename A, int OP >
+__device__ __forceinline__ void zstream_epilogue( int64_t i, A s, A invd, A centre, A aux, T* v2, T* dst, A a0, A a1 )
+{
+   if constexpr ( OP == OP_APPLY ) stv( dst + i, s );
+   else if constexpr ( OP == OP_APPLY_ADD ) stv( dst + i, aux + s );
+   else if constexpr ( OP == OP_RESID ) stv( dst + i, aux - s );
+   else if constexpr ( OP == OP_JAC ) stv( dst + i, centre + a0 * ( invd * ( aux - s ) ) );
+   else if constexpr ( OP == OP_CHEB0 ) stv( dst + i, invd * ( aux - s ) );
+   else if constexpr ( OP == OP_CHEBI )
+   {
+      stv( dst + i, invd * s );
+      stv( v2 + i, aux + a0 * centre );
+   }
+   else if constexpr ( OP == OP_CHEBL ) stv( v2 + i, ( aux + a0 * centre ) + a1 * ( invd * s ) );
+   else if constexpr ( OP == OP_DINV_APPLY ) stv( dst + i, invd * s );
+}
 
 template < typename T, typename A, int OP >
-__global__ void __launch_bounds__( kTmaThreads ) k_cell_tma( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
-                                                             const T* __restrict__ v1, T* v2, T* dst, A a0, A a1, int ntiles,
-                                                             int nC, int64_t stage_elems, const int4* __restrict__ tiles, int* err )
+__global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
+                                                                  const T* __restrict__ v1, T* v2, T* dst, A a0, A a1, int nC,
+                                                                  int* err, int bulk )
 {
-   extern __shared__ __align__( 128 ) unsigned char smem_raw[];
-   __shared__ uint64_t bars[kTmaStages];
-   T*                  stage0 = reinterpret_cast< T* >( smem_raw );
-   const int           tid = threadIdx.x, n = v.n;
-   const int           total = ntiles * nC;
-   if ( tid == 0 )
+   constexpr bool AUX = zstream_aux< OP >();
+   using Cfg          = ZCfg< T, AUX >;
+   constexpr int S = Cfg::S, RW = Cfg::RW;
+   extern __shared__ __align__( 128 ) unsigned char zs_raw[];
+   T*                  ring = reinterpret_cast< T* >( zs_raw );
+   __shared__ uint64_t full[S], empty[S];
+   __shared__ uint32_t shw[2 * S];
+   __shared__ int      abort_flag;
+   const int           warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n = v.n;
+   if ( threadIdx.x == 0 )
    {
-      for ( int s = 0; s < kTmaStages; ++s ) mbar_init( &bars[s], 1 );
+      for ( int s = 0; s < S; ++s )
+      {
+         mbar_init( &full[s], bulk ? 1 : 32 );
+         mbar_init( &empty[s], kZWarps );
+      }
+      abort_flag = 0;
       asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
    }
    __syncthreads();
-
-   // issue the three bulk copies of work item t into stage st (thread 0 only)
-   auto issue = [&]( int t, int st ) {
-      const int     c  = t / ntiles;
-      const int4    tl = tiles[t % ntiles];
-      const int     z = tl.x, ya = tl.y, yb = tl.z;
-      const T*      g  = src + v.cell_off[c];
-      T*            sm = stage0 + int64_t( st ) * stage_elems;
-      TileRange     rs = tile_range< T >( n, ya - 1, yb + 1, z );
-      TileRange     rt = tile_range< T >( n, ya - 1, yb, z + 1 );
-      TileRange     rb = tile_range< T >( n, ya, yb + 1, z - 1 );
-      const int64_t ns = rs.end - rs.first, nt = rt.end - rt.first, nb = rb.end - rb.first;
-      mbar_expect_tx( &bars[st], uint32_t( ( ns + nt + nb ) * sizeof( T ) ) );
-      bulk_copy_g2s( sm, g + rs.first, uint32_t( ns * sizeof( T ) ), &bars[st] );
-      bulk_copy_g2s( sm + ns, g + rt.first, uint32_t( nt * sizeof( T ) ), &bars[st] );
-      bulk_copy_g2s( sm + ns + nt, g + rb.first, uint32_t( nb * sizeof( T ) ), &bars[st] );
-   };
-   auto next_active = [&]( int t ) {
-      while ( t < total && !( v.cell_bc[t / ntiles] & flag ) ) t += gridDim.x;
-      return t;
-   };
-
-   // prologue: fill the first kTmaStages-1 stages
-   int tq[kTmaStages];
-   tq[0] = next_active( blockIdx.x );
-   for ( int s = 1; s < kTmaStages; ++s ) tq[s] = tq[s - 1] < total ? next_active( tq[s - 1] + gridDim.x ) : total;
-   if ( tid == 0 )
-      for ( int s = 0; s < kTmaStages - 1; ++s )
-         if ( tq[s] < total ) issue( tq[s], s );
-   uint32_t phase = 0;  // parity of stage 0; stage s uses the same parity within a round
-   int      st    = 0;
-   int      t     = tq[0];
-   int      ahead = tq[kTmaStages - 1];  // next item to issue
-   while ( t < total )
+   volatile int* abrt = &abort_flag;
+   if ( warp == kZWarps )
    {
-      // refill the stage freed in the previous iteration with the item kTmaStages-1 ahead
-      if ( tid == 0 && ahead < total )
-      {
-         fence_proxy_async();
-         issue( ahead, ( st + kTmaStages - 1 ) % kTmaStages );
-      }
-      int  spins    = 0;
-      bool timedout = false;
-      while ( !mbar_try_wait( &bars[st], phase ) )
-         if ( ++spins > kSpinLimit )
-         {
-            timedout = true;
-            break;
-         }
-      if ( __syncthreads_or( timedout ) )
-      {
-         if ( tid == 0 ) atomicExch( err, 1 );
-         for ( int s = 0; s < kTmaStages; ++s )
-            for ( int k = 0; k < kSpinLimit && !mbar_try_wait( &bars[s], phase ); ++k ) {}
-         return;
-      }
-
-      {
-         const int     c    = t / ntiles;
-         const int4    tl   = tiles[t % ntiles];
-         const int     z = tl.x, ya = tl.y, yb = tl.z;
-         const int64_t base = v.cell_off[c];
-         T*            sm   = stage0 + int64_t( st ) * stage_elems;
-         TileRange     rs   = tile_range< T >( n, ya - 1, yb + 1, z );
-         TileRange     rt   = tile_range< T >( n, ya - 1, yb, z + 1 );
-         TileRange     rb   = tile_range< T >( n, ya, yb + 1, z - 1 );
-         const T*      S    = sm - rs.first;
-         const T*      Tt   = sm + ( rs.end - rs.first ) - rt.first;
-         const T*      B    = sm + ( rs.end - rs.first ) + ( rt.end - rt.first ) - rb.first;
-         const A*      W    = o.W + size_t( c ) * kNumClasses * kNumDirs;
-         const A w0 = W[0], wW = W[1], wE = W[2], wS = W[3], wN = W[4], wB = W[5], wT = W[6], wNW = W[7], wSE = W[8],
-                 wTW = W[9], wBE = W[10], wTS = W[11], wBN = W[12], wTSE = W[13], wBNW = W[14];
-         const A   invd = o.invd_c[c];
-         // threads -> (row group g, x): short rows get several row groups
-         const int len  = n - 1 - z - ya;
-         const int wx   = ( ( len + 31 ) / 32 ) * 32;
-         const int G    = wx >= kTmaThreads ? 1 : kTmaThreads / wx;
-         const int g    = tid / ( wx >= kTmaThreads ? kTmaThreads : wx );
-         const int xs   = wx >= kTmaThreads ? kTmaThreads : wx;
-         const int rows = yb - ya + 1;
-         const int per  = ( rows + G - 1 ) / G;
-         const int y0   = ya + g * per;
-         const int y1   = min( yb, y0 + per - 1 );
-         if ( g < G && y0 <= y1 )
-            for ( int x = 1 + tid % xs; x <= n - 1 - z - y0; x += xs )
-            {
-               auto rd = [&]( const T* R, int yy, int zz, Row3< T, A >& r ) {
-                  const T* p = R + cidx( n, x, yy, zz );
-                  r.m        = A( p[-1] );
-                  r.o        = A( p[0] );
-                  r.p        = A( p[1] );
-               };
-               Row3< T, A > cm, c0, tm, b0, cp, t0, bp;
-               rd( S, y0 - 1, z, cm );
-               rd( S, y0, z, c0 );
-               rd( Tt, y0 - 1, z + 1, tm );
-               rd( B, y0, z - 1, b0 );
-               for ( int y = y0; y <= y1 && x + y + z <= n - 1; ++y )
-               {
-                  rd( S, y + 1, z, cp );
-                  rd( Tt, y, z + 1, t0 );
-                  rd( B, y + 1, z - 1, bp );
-                  A acc = w0 * c0.o;
-                  acc += wW * c0.m;
-                  acc += wE * c0.p;
-                  acc += wS * cm.o;
-                  acc += wN * cp.o;
-                  acc += wB * b0.o;
-                  acc += wT * t0.o;
-                  acc += wNW * cp.m;
-                  acc += wSE * cm.p;
-                  acc += wTW * t0.m;
-                  acc += wBE * b0.p;
-                  acc += wTS * tm.o;
-                  acc += wBN * bp.o;
-                  acc += wTSE * tm.p;
-                  acc += wBNW * bp.m;
-                  stencil_epilogue< T, A, OP >( base + cidx( n, x, y, z ), acc, invd, src, v1, v2, dst, a0, a1 );
-                  cm = c0;
-                  c0 = cp;
-                  tm = t0;
-                  b0 = bp;
-               }
-            }
-      }
-      __syncthreads();  // stage st is free again
-      st = ( st + 1 ) % kTmaStages;
-      if ( st == 0 ) phase ^= 1u;
-      t     = next_active( t + gridDim.x );
-      ahead = ahead < total ? next_active( ahead + gridDim.x ) : total;
+      const T* aux = ( OP == OP_CHEBI || OP == OP_CHEBL ) ? v2 : ( OP == OP_APPLY_ADD ? dst : v1 );
+      zstream_produce< T, AUX >( v, flag, src, aux, nC, ring, full, empty, shw, abrt, err, bulk != 0 );
+      return;
    }
+
+   // consumer warp `warp` owns tile row y0 + warp; stage row r holds global row y0 - 1 + r
+   const int u0 = v.zbegin[blockIdx.x], u1 = v.zbegin[blockIdx.x + 1];
+   const int rS = warp, rC = warp + 1, rN = warp + 2;  // rows y-1, y, y+1 of the stage
+   auto at = [&]( int st, uint32_t word, int r, int dx ) -> A {
+      return A( ring[st * Cfg::stage + r * RW + int( ( word >> ( 3 * r ) ) & 7u ) + lane + 1 + dx] );
+   };
+   auto fail = [&]() {
+      if ( lane == 0 )
+      {
+         atomicExch( err, 1 );
+         *abrt = 1;
+      }
+   };
+   int ld = 0;
+   for ( int c = 0; c < nC; ++c )
+   {
+      if ( !( v.cell_bc[c] & flag ) ) continue;
+      const int64_t base = v.cell_off[c];
+      const A*      W    = o.W + size_t( c ) * kNumClasses * kNumDirs;  // interior class 0
+      const A w0 = W[0], wW = W[1], wE = W[2], wS = W[3], wN = W[4], wB = W[5], wT = W[6], wNW = W[7], wSE = W[8], wTW = W[9],
+              wBE = W[10], wTS = W[11], wBN = W[12], wTSE = W[13], wBNW = W[14];
+      const A invd = o.invd_c[c];
+      for ( int u = u0; u < u1; ++u )
+      {
+         const int4 U = v.zunits[u];
+         const int  x = U.x + lane, y = U.y + warp;
+         // prologue: slice z_first-1 (load ld) and slice z_first (load ld+1)
+         const int sm = ld % S, s0 = ( ld + 1 ) % S;
+         if ( !mbar_wait_bounded( &full[sm], uint32_t( ( ld / S ) & 1 ), abrt ) ||
+              !mbar_wait_bounded( &full[s0], uint32_t( ( ( ld + 1 ) / S ) & 1 ), abrt ) )
+            return fail();
+         const uint32_t wm = shw[2 * sm], wc = shw[2 * s0];
+         A B = at( sm, wm, rC, 0 ), BE = at( sm, wm, rC, 1 ), BN = at( sm, wm, rN, 0 ), BNW = at( sm, wm, rN, -1 );
+         A C = at( s0, wc, rC, 0 ), Wv = at( s0, wc, rC, -1 ), Sv = at( s0, wc, rS, 0 ), SE = at( s0, wc, rS, 1 );
+         __syncwarp();
+         if ( lane == 0 ) mbar_arrive( &empty[sm] );
+         for ( int z = U.z; z <= U.w; ++z )
+         {
+            const int lz = ld + 1 + ( z - U.z ), lp = lz + 1;
+            const int sz = lz % S, sp = lp % S;
+            if ( !mbar_wait_bounded( &full[sp], uint32_t( ( lp / S ) & 1 ), abrt ) ) return fail();
+            const uint32_t wz = shw[2 * sz], wp = shw[2 * sp];
+            const A        E = at( sz, wz, rC, 1 ), N = at( sz, wz, rN, 0 ), NW = at( sz, wz, rN, -1 );
+            const A        Tt = at( sp, wp, rC, 0 ), TW = at( sp, wp, rC, -1 ), TS = at( sp, wp, rS, 0 ), TSE = at( sp, wp, rS, 1 );
+            if ( x + y + z <= n - 1 )
+            {
+               A auxv = A( 0 );
+               if constexpr ( AUX )
+                  auxv = A( ring[sz * Cfg::stage + Cfg::aux0 + warp * Cfg::RWA + int( ( shw[2 * sz + 1] >> ( 3 * warp ) ) & 7u ) + lane] );
+               A acc = w0 * C;
+               acc += wW * Wv;
+               acc += wE * E;
+               acc += wS * Sv;
+               acc += wN * N;
+               acc += wB * B;
+               acc += wT * Tt;
+               acc += wNW * NW;
+               acc += wSE * SE;
+               acc += wTW * TW;
+               acc += wBE * BE;
+               acc += wTS * TS;
+               acc += wBN * BN;
+               acc += wTSE * TSE;
+               acc += wBNW * BNW;
+               zstream_epilogue< T, A, OP >( base + cidx( n, x, y, z ), acc, invd, C, auxv, v2, dst, a0, a1 );
+            }
+            B   = C;
+            BE  = E;
+            BN  = N;
+            BNW = NW;
+            C   = Tt;
+            Wv  = TW;
+            Sv  = TS;
+            SE  = TSE;
+            __syncwarp();
+            if ( lane == 0 ) mbar_arrive( &empty[sz] );
+         }
+         // slice z_last+1 is no longer needed either
+         __syncwarp();
+         if ( lane == 0 ) mbar_arrive( &empty[( ld + 2 + ( U.w - U.z ) ) % S] );
+         ld += U.w - U.z + 3;
+      }
+   }
+}
+
+template < typename T, typename A, int OP >
+static void zstream_attribute()
+{
+   check_cuda( cudaFuncSetAttribute( k_cell_zstream< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int( ZCfg< T, zstream_aux< OP >() >::smem_bytes ) ),
+               "cudaFuncSetAttribute(z-stream shared memory)" );
+}
+
+template < typename T, typename A >
+static void zstream_attributes()
+{
+   zstream_attribute< T, A, OP_APPLY >();
+   zstream_attribute< T, A, OP_APPLY_ADD >();
+   zstream_attribute< T, A, OP_RESID >();
+   zstream_attribute< T, A, OP_JAC >();
+   zstream_attribute< T, A, OP_CHEB0 >();
+   zstream_attribute< T, A, OP_CHEBI >();
+   zstream_attribute< T, A, OP_CHEBL >();
+   zstream_attribute< T, A, OP_DINV_APPLY >();
+}
+
+static void zstream_attributes_all()
+{
+   zstream_attributes< double, double >();
+   zstream_attributes< float, float >();
+   zstream_attributes< __half, float >();
+}
+
+// z-stream stages are filled with cp.async.bulk row copies; HYB_ZCOPY=async selects 16-byte
+// cp.async pieces instead (measured slower on B200: the producer warp issues one instruction per row)
+static int zstream_bulk()
+{
+   static int b = -1;
+   if ( b < 0 )
+   {
+      const char* e = getenv( "HYB_ZCOPY" );
+      b             = ( e && std::string( e ) == "async" ) ? 0 : 1;
+   }
+   return b;
 }
 
 static int march_prefetch_distance()
@@ -629,34 +832,11 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
    T*       v2  = (T*) a.v2;
    T*       dst = (T*) a.dst;
    Fork     fk( ctx );
-   if ( cell_kernel_variant() == 2 && v.n >= 32 && v.ntiles > 0 && nC > 0 )
+   if ( cell_kernel_variant() == 2 && v.n >= 32 && v.nzblocks > 0 && nC > 0 )
    {
-      // stage size: largest tile of this level (elements of T)
-      int64_t stage = 0;
-      for ( const auto& tl : *v.host_tiles )
-      {
-         const auto rs = tile_range< T >( v.n, tl[1] - 1, tl[2] + 1, tl[0] );
-         const auto rt = tile_range< T >( v.n, tl[1] - 1, tl[2], tl[0] + 1 );
-         const auto rb = tile_range< T >( v.n, tl[1], tl[2] + 1, tl[0] - 1 );
-         stage         = std::max( stage, ( rs.end - rs.first ) + ( rt.end - rt.first ) + ( rb.end - rb.first ) );
-      }
-      const size_t smem = size_t( kTmaStages ) * size_t( stage ) * sizeof( T );
-      static int   s_sms = 0, s_set = 0;
-      static size_t s_smem_set = 0;
-      if ( !s_sms ) check_cuda( cudaDeviceGetAttribute( &s_sms, cudaDevAttrMultiProcessorCount, 0 ), "device attribute" );
-      if ( smem > s_smem_set )
-      {
-         check_cuda( cudaFuncSetAttribute( k_cell_tma< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize, int( smem ) ),
-                     "cudaFuncSetAttribute(smem)" );
-         s_smem_set = smem;
-      }
-      (void) s_set;
-      int per_sm = 0;
-      check_cuda( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &per_sm, k_cell_tma< T, A, OP >, kTmaThreads, smem ), "occupancy" );
-      const int total = v.ntiles * nC;
-      const int grid  = std::max( 1, std::min( total, std::max( 1, per_sm ) * s_sms ) );
-      k_cell_tma< T, A, OP ><<< grid, kTmaThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ),
-                                                                          v.ntiles, nC, stage, v.tiles, ctx->d_error );
+      constexpr size_t smem = ZCfg< T, zstream_aux< OP >() >::smem_bytes;  // attribute set by ensure_constants
+      k_cell_zstream< T, A, OP ><<< v.nzblocks, kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ),
+                                                                                 A( a.a1 ), nC, ctx->d_error, zstream_bulk() );
       ++ctx->launches;
    }
    else if ( cell_kernel_variant() >= 1 && v.nmarch > 0 && nC > 0 )

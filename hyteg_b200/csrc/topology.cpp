@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstring>
 #include <fstream>
+#include <queue>
 #include <set>
 #include <sstream>
 #include <stdexcept>
@@ -287,18 +288,6 @@ void build_level( Mesh* m, int L )
             for ( int y0 = 1; y0 <= ylast; y0 += YC ) P.march.push_back( { z, x0, y0, std::min( ylast, y0 + YC - 1 ) } );
          }
    }
-   // shared-memory staged tiles: rows y0..y1 of one slice, about 768 interior points per tile
-   {
-      for ( int z = 1; z <= n - 3; ++z )
-         for ( int y0 = 1; y0 <= n - 2 - z; )
-         {
-            const int len = n - 1 - z - y0;  // interior points of row y0
-            const int ty  = std::max( 2, std::min( 64, 768 / std::max( len, 1 ) ) );
-            const int y1  = std::min( n - 2 - z, y0 + ty - 1 );
-            P.tiles.push_back( { z, y0, y1, 0 } );
-            y0 = y1 + 1;
-         }
-   }
    // cell interior rows (y, z), memory order
    for ( int z = 1; z <= n - 2; ++z )
       for ( int y = 1; y + z <= n - 2; ++y )
@@ -308,6 +297,63 @@ void build_level( Mesh* m, int L )
       }
 
    m->levels[L] = std::move( lv );
+}
+
+// Work units of the z-streamed sweep.  A unit is the tile x0..x0+31, y0..y0+7 of slices
+// z_first..z_last (interior points only: x, y, z >= 1, x+y+z <= n-1).  The slice range is cut into
+// chunks of zc slices, zc the largest power of two in [8, 64] that still gives at least three units
+// per block; units are then handed out longest-first to the least loaded block, so every block
+// ends at about the same time.
+void build_zunits( P1Level& P, int nblocks )
+{
+   const int n = P.n;
+   P.zunits.clear();
+   P.zbegin.assign( 1, 0 );
+   if ( n < 4 ) return;
+   struct Unit
+   {
+      std::array< int, 4 > u;
+      int64_t              work;
+   };
+   auto make = [&]( int zc ) {
+      std::vector< Unit > us;
+      for ( int y0 = 1; y0 <= n - 3; y0 += kZTileY )
+         for ( int x0 = 1; x0 + y0 <= n - 2; x0 += kZTileX )
+         {
+            const int zmax = n - 1 - x0 - y0;
+            for ( int za = 1; za <= zmax; za += zc )
+            {
+               const int zb = std::min( zmax, za + zc - 1 );
+               int64_t   w  = 0;
+               for ( int z = za; z <= zb; ++z )
+                  for ( int y = y0; y < y0 + kZTileY; ++y )
+                     w += std::max( 0, std::min( kZTileX, n - y - z - x0 ) );
+               us.push_back( { { x0, y0, za, zb }, w } );
+            }
+         }
+      return us;
+   };
+   int                 zc = 64;
+   std::vector< Unit > us = make( zc );
+   while ( zc > 8 && int64_t( us.size() ) < 3 * int64_t( nblocks ) ) us = make( zc /= 2 );
+   if ( const char* e = getenv( "HYB_ZCHUNK" ) ) us = make( std::max( 1, atoi( e ) ) );
+   std::stable_sort( us.begin(), us.end(), []( const Unit& a, const Unit& b ) { return a.work > b.work; } );
+   const int nb = std::max( 1, std::min( nblocks, int( us.size() ) ) );
+   std::vector< std::vector< std::array< int, 4 > > >                                       per( nb );
+   std::priority_queue< std::pair< int64_t, int >, std::vector< std::pair< int64_t, int > >, std::greater<> > heap;
+   for ( int b = 0; b < nb; ++b ) heap.push( { 0, b } );
+   for ( const Unit& u : us )
+   {
+      auto [load, b] = heap.top();
+      heap.pop();
+      per[b].push_back( u.u );
+      heap.push( { load + u.work, b } );
+   }
+   for ( int b = 0; b < nb; ++b )
+   {
+      for ( const auto& u : per[b] ) P.zunits.push_back( u );
+      P.zbegin.push_back( int( P.zunits.size() ) );
+   }
 }
 
 void ensure_device( Mesh* m, P1Level& P )
@@ -333,9 +379,14 @@ void ensure_device( Mesh* m, P1Level& P )
    std::vector< int4 > mi( P.march.size() );
    for ( size_t i = 0; i < mi.size(); ++i ) mi[i] = make_int4( P.march[i][0], P.march[i][1], P.march[i][2], P.march[i][3] );
    up( &P.d_march, mi.data(), mi.size() );
-   std::vector< int4 > ti( P.tiles.size() );
-   for ( size_t i = 0; i < ti.size(); ++i ) ti[i] = make_int4( P.tiles[i][0], P.tiles[i][1], P.tiles[i][2], 0 );
-   up( &P.d_tiles, ti.data(), ti.size() );
+   int dev = 0, sms = 0;
+   check_cuda( cudaGetDevice( &dev ), "cudaGetDevice" );
+   check_cuda( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev ), "device attribute" );
+   build_zunits( P, 2 * std::max( sms, 1 ) );
+   std::vector< int4 > zu( P.zunits.size() );
+   for ( size_t i = 0; i < zu.size(); ++i ) zu[i] = make_int4( P.zunits[i][0], P.zunits[i][1], P.zunits[i][2], P.zunits[i][3] );
+   up( &P.d_zunits, zu.data(), zu.size() );
+   up( &P.d_zbegin, P.zbegin.data(), P.zbegin.size() );
    std::vector< uint8_t > bc( nP );
    std::vector< int8_t >  bk( P.nB );
    for ( int v = 0; v < t.nV; ++v ) bc[v] = uint8_t( t.bc( t.flag_v[v] ) ), bk[v] = 0;
@@ -378,7 +429,8 @@ Mesh::~Mesh()
       cudaFree( P.d_tasks );
       cudaFree( P.d_rows );
       cudaFree( P.d_march );
-      cudaFree( P.d_tiles );
+      cudaFree( P.d_zunits );
+      cudaFree( P.d_zbegin );
       cudaFree( P.d_bc );
       cudaFree( P.d_bkind );
       cudaFree( P.d_ncell_cls );
