@@ -123,6 +123,7 @@ _SIGS = {
     "hyb_residual_norm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32,
                                     C.POINTER(C.c_double)]),
     "hyb_fn_fill_random": (C.c_int, [C.c_void_p, C.c_int, C.c_uint64]),
+    "hyb_fn_dot_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.POINTER(C.c_double)]),
     "hyb_serve_params_default": (C.c_int, [C.c_void_p]),
     "hyb_serve_create": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
     "hyb_serve_destroy": (C.c_int, [C.c_void_p]),
@@ -348,6 +349,12 @@ class P1Function:
     def dotGlobal(self, other, level, flag=All):
         v = C.c_double()
         _check(lib().hyb_fn_dot(self.h, other.h, level, flag, C.byref(v)))
+        return v.value
+
+    def dotGlobalNoAlloc(self, other, level, flag=All):
+        """dotGlobal without any device allocation (fixed static scratch; see hyb_fn_dot_noalloc)."""
+        v = C.c_double()
+        _check(lib().hyb_fn_dot_noalloc(self.h, other.h, level, flag, C.byref(v)))
         return v.value
 
     def copyFrom(self, other, level):

@@ -663,6 +663,20 @@ int hyb_fn_dot( hyb_fn* a, hyb_fn* b, int level, uint32_t flag, double* out )
    HYB_CATCH
 }
 
+// Same result as hyb_fn_dot without allocating device memory (fixed static scratch; see
+// launch_dot_noalloc for the set-up, the size limit and the overlap rule).
+int hyb_fn_dot_noalloc( hyb_fn* a, hyb_fn* b, int level, uint32_t flag, double* out )
+{
+   HYB_TRY
+   require( a && b && out, "NULL argument" );
+   require( a->f.mesh == b->f.mesh && a->f.dtype == b->f.dtype, "incompatible functions" );
+   require_level( a->f, level );
+   require_level( b->f, level );
+   set_device( a->ctx->c );
+   launch_dot_noalloc( &a->ctx->c, a->f.mesh, level, a->f.dtype, flag, a->f.ptr( level ), b->f.ptr( level ), out );
+   HYB_CATCH
+}
+
 int hyb_fn_copy_from( hyb_fn* dst, hyb_fn* src, int level )
 {
    HYB_TRY

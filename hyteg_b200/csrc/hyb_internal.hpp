@@ -289,6 +289,7 @@ void launch_flat_lincomb( Context* ctx, int64_t count, int dtype, void* dst, int
 void launch_convert( Context* ctx, int64_t count, int dst_dtype, void* dst, int src_dtype, const void* src, double scale = 1.0 );
 // deterministic dot over owned flagged DoFs -> *out (device)
 void launch_dot( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const void* a, const void* b, double* out );
+void launch_dot_noalloc( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const void* a, const void* b, double* host_out );
 void launch_restrict( Context* ctx, Mesh* m, int Lfine, int dtype, uint32_t flag, const void* fine, void* coarse );
 void launch_prolongate( Context* ctx, Mesh* m, int Lcoarse, int dtype, uint32_t flag, const void* coarse, void* fine, int add );
 void launch_axpy_to_f64( Context* ctx, int64_t count, double* x, int src_dtype, const void* c, double a );

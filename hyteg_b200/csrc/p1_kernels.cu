@@ -16,6 +16,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -1246,6 +1247,91 @@ void launch_dot( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const v
    if ( dtype == F64 ) run_dot< double >( ctx, v, nC, flag, a, b, out );
    else if ( dtype == F32 ) run_dot< float >( ctx, v, nC, flag, a, b, out );
    else run_dot< __half >( ctx, v, nC, flag, a, b, out );
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free dot product.
+//
+// Some callers cannot let a call allocate device memory: a host runtime that reserves the device
+// memory up front and hands it out through its own allocator (a cudaMalloc behind its back can
+// fail or fragment the reserve), or a latency-critical loop that must not pay the implicit
+// device synchronisation of cudaMalloc/cudaFree.  launch_dot grows the context's partials buffer
+// on demand; this variant runs the same dot kernels but keeps the per-block partial sums and the
+// result in one file-scope device array of fixed size.
+//  * set-up: the first call on a device (that device current) resolves the array's address once
+//    with cudaGetSymbolAddress, and the first call in the process also uploads the constant tables;
+//    make that first call before any stream capture.
+//  * limit: at most kNoAllocPartials block partials (cell-row blocks plus boundary blocks of the
+//    level); larger levels are rejected with an error.
+//  * nothing has to start at zero: every block of the sweep writes its own partial and the final
+//    kernel overwrites the result slot.
+//  * the array is shared by all callers on the device, so calls that overlap in time (other
+//    streams, other host threads) race on it and must be serialised by the caller.
+// ---------------------------------------------------------------------------------------------
+constexpr int kNoAllocPartials = 1 << 16;
+static __device__ __align__( 256 ) double g_noalloc_dot[kNoAllocPartials + 1];  // partials, result
+
+static double* noalloc_scratch( int device )
+{
+   static std::mutex mu;
+   static double*    ptrs[256] = {};
+   if ( device < 0 || device >= 256 ) throw std::invalid_argument( "device ordinal out of range" );
+   std::lock_guard< std::mutex > lock( mu );
+   if ( !ptrs[device] )
+   {
+      void* p = nullptr;
+      check_cuda( cudaGetSymbolAddress( &p, g_noalloc_dot ), "cudaGetSymbolAddress(allocation-free dot scratch)" );
+      ptrs[device] = static_cast< double* >( p );
+   }
+   return ptrs[device];
+}
+
+template < typename T >
+static void run_dot_fixed( Context* ctx, const LevelView& v, int nC, uint32_t flag, const void* a, const void* b, double* p,
+                           double* out )
+{
+   const int nb_cells = ( v.nrows > 0 && nC > 0 ) ? ( ( v.nrows + 7 ) / 8 ) * nC : 0;
+   const int nb_bnd   = v.ntasks > 0 ? ( v.ntasks + 255 ) / 256 : 0;
+   {
+      Fork fk( ctx );
+      if ( nb_cells )
+      {
+         dim3 grid( ( v.nrows + 7 ) / 8, nC );
+         k_dot_cells< T ><<< grid, 256, 0, ctx->stream >>>( v, flag, (const T*) a, (const T*) b, p );
+         ++ctx->launches;
+      }
+      if ( nb_bnd )
+      {
+         k_dot_bnd< T ><<< nb_bnd, 256, 0, fk.aux() >>>( v, flag, (const T*) a, (const T*) b, p + nb_cells );
+         ++ctx->launches;
+      }
+   }
+   k_sum_partials<<< 1, 1024, 0, ctx->stream >>>( p, nb_cells + nb_bnd, out );
+   ++ctx->launches;
+   check_cuda( cudaGetLastError(), "dot launch" );
+}
+
+void launch_dot_noalloc( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const void* a, const void* b, double* host_out )
+{
+   auto it = m->levels.find( L );
+   if ( it == m->levels.end() || !it->second->d_off )
+      throw std::invalid_argument( "allocation-free dot: the level's index tables are not on the device yet "
+                                   "(run any operation on this level first)" );
+   ensure_constants();
+   double*         scratch  = noalloc_scratch( ctx->device );
+   const LevelView v        = make_view( m, L );
+   const int       nC       = m->topo.nC;
+   const int64_t   nb_cells = ( v.nrows > 0 && nC > 0 ) ? int64_t( ( v.nrows + 7 ) / 8 ) * nC : 0;
+   const int64_t   nb_bnd   = v.ntasks > 0 ? ( v.ntasks + 255 ) / 256 : 0;
+   if ( nb_cells + nb_bnd > kNoAllocPartials )
+      throw std::invalid_argument( "allocation-free dot: this level needs " + std::to_string( nb_cells + nb_bnd ) +
+                                   " block partials, the fixed scratch holds " + std::to_string( kNoAllocPartials ) );
+   double* out = scratch + kNoAllocPartials;
+   if ( dtype == F64 ) run_dot_fixed< double >( ctx, v, nC, flag, a, b, scratch, out );
+   else if ( dtype == F32 ) run_dot_fixed< float >( ctx, v, nC, flag, a, b, scratch, out );
+   else run_dot_fixed< __half >( ctx, v, nC, flag, a, b, scratch, out );
+   check_cuda( cudaMemcpyAsync( host_out, out, sizeof( double ), cudaMemcpyDeviceToHost, ctx->stream ), "dot readback" );
+   check_cuda( cudaStreamSynchronize( ctx->stream ), "dot sync" );
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -158,6 +158,14 @@ int hyb_fn_mult_elementwise( hyb_fn* dst, hyb_fn* a, hyb_fn* b, int level, uint3
 int hyb_fn_invert_elementwise( hyb_fn* fn, int level, uint32_t flag );
 /* dotGlobal(other, level, flag) (VertexDoFFunction.cpp:1710-1790); deterministic */
 int hyb_fn_dot( hyb_fn* a, hyb_fn* b, int level, uint32_t flag, double* out );
+/* Allocation-free hyb_fn_dot (no counterpart in the reference): the same deterministic kernels and
+ * result, with the per-block partial sums in a fixed file-scope device array (65536 partials, 512 KiB)
+ * instead of a buffer grown with cudaMalloc, for callers whose device memory is reserved up front by
+ * their own allocator.  The first call on a device resolves the array's address (make it before
+ * any stream capture).  The level's index tables must already be on the device (any earlier
+ * operation on that level puts them there).  Levels needing more partials return HYB_EINVAL.  The
+ * array is shared per device: overlapping calls race and must be serialised by the caller. */
+int hyb_fn_dot_noalloc( hyb_fn* a, hyb_fn* b, int level, uint32_t flag, double* out );
 /* copyFrom between value types (VertexDoFFunction.hpp:150-151) */
 int hyb_fn_copy_from( hyb_fn* dst, hyb_fn* src, int level );
 /* swap(other, level) */
