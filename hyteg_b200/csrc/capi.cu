@@ -1068,6 +1068,8 @@ struct hyb_gmg
    std::vector< double >                radii;
    std::vector< std::vector< double > > coeff;
    std::vector< int >                   swaps;  // Jacobi swaps per level in the current cycle
+   // CG iterations unrolled into a captured cycle (measured by coarse_probe; -1: not yet)
+   int coarse_cap = -1;
    // graph cache
    cudaGraphExec_t gexec   = nullptr;
    void*           g_x     = nullptr;
@@ -1177,6 +1179,14 @@ static void smooth( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int L )
    }
 }
 
+// A captured coarse solve launches the kernels of every unrolled iteration even after the
+// device-side stopping test has ended it, so captured cycles unroll only the probed iteration
+// count (with margin); cycles run with host checks stop on their own and keep coarse_max_iter.
+static int coarse_iterations( const hyb_gmg* g, bool host_checks )
+{
+   return ( host_checks || g->coarse_cap < 0 ) ? g->p.coarse_max_iter : g->coarse_cap;
+}
+
 static void cycle_rec( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int L, int invoked, bool host_checks )
 {
    hyb_op*   op = g->op;
@@ -1190,11 +1200,12 @@ static void cycle_rec( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int L, int invoked, boo
          const int64_t cnt = x->f.mesh->level( L ).size;
          launch_convert( &cx, cnt, F64, g->cgb64->f.ptr( L ), dt, b->f.ptr( L ) );
          check_cuda( cudaMemsetAsync( g->cgx64->f.ptr( L ), 0, g->cgx64->f.bytes( L ), cx.stream ), "cudaMemset" );
-         cg_run( op, g->cg64, g->cgx64, g->cgb64, L, g->p.coarse_max_iter, g->p.coarse_rtol, g->p.coarse_atol, host_checks );
+         cg_run( op, g->cg64, g->cgx64, g->cgb64, L, coarse_iterations( g, host_checks ), g->p.coarse_rtol, g->p.coarse_atol,
+                 host_checks );
          launch_convert( &cx, cnt, dt, x->f.ptr( L ), F64, g->cgx64->f.ptr( L ) );
       }
       else
-         cg_run( op, g->cg, x, b, L, g->p.coarse_max_iter, g->p.coarse_rtol, g->p.coarse_atol, host_checks );
+         cg_run( op, g->cg, x, b, L, coarse_iterations( g, host_checks ), g->p.coarse_rtol, g->p.coarse_atol, host_checks );
       return;
    }
    const int pre = g->p.pre_smooth + g->p.smooth_increment * ( invoked - L );
@@ -1334,6 +1345,38 @@ static void seeded_vector( hyb_fn* x, int L, uint64_t seed )
    hyb_fn_upload( x, L, packed.data() );
 }
 
+// Iterations the coarse CG takes to reach coarse_rtol on this hierarchy, measured once on a seeded
+// right-hand side (CG iteration counts on a fixed matrix barely depend on the right-hand side);
+// captured cycles unroll twice that plus ten, at most coarse_max_iter, and none when the probe
+// needed none.
+static void coarse_probe( hyb_gmg* g, int dt )
+{
+   const int L   = g->p.min_level;
+   const int pdt = g->cgx64 ? F64 : dt;
+   hyb_fn*   xp  = new_fn( g->ctx, g->op->o.mesh, pdt, L, L );
+   hyb_fn*   bp  = new_fn( g->ctx, g->op->o.mesh, pdt, L, L );
+   try
+   {
+      seeded_vector( bp, L, 4242u );
+      CGState& st = g->cgx64 ? g->cg64 : g->cg;
+      cg_run( g->op, st, xp, bp, L, g->p.coarse_max_iter, g->p.coarse_rtol, g->p.coarse_atol, true );
+      double   it = 0;
+      Context& c  = g->ctx->c;
+      check_cuda( cudaMemcpyAsync( &it, st.st + 7, sizeof( double ), cudaMemcpyDeviceToHost, c.stream ), "cg readback" );
+      check_cuda( cudaStreamSynchronize( c.stream ), "cg sync" );
+      // a coarse problem that is solved before the first iteration (no unknowns, e.g. every
+      // coarse DoF on the Dirichlet boundary) needs no unrolled iterations at all
+      g->coarse_cap = it == 0.0 ? 0 : std::min( g->p.coarse_max_iter, 2 * int( it ) + 10 );
+   } catch ( ... )
+   {
+      hyb_fn_destroy( xp );
+      hyb_fn_destroy( bp );
+      throw;
+   }
+   hyb_fn_destroy( xp );
+   hyb_fn_destroy( bp );
+}
+
 }  // namespace hyb
 
 extern "C" {
@@ -1434,6 +1477,7 @@ static void gmg_prepare( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int level )
       hyb_fn_destroy( aux );
       set_coefficients( g );
    }
+   if ( g->p.use_graph && g->coarse_cap < 0 ) coarse_probe( g, x->f.dtype );
 }
 
 int hyb_gmg_solve( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int level )

@@ -100,8 +100,8 @@ struct Topology {
 };
 
 // per-level host + device tables of the P1 layout
-// tile of the z-streamed cell sweep: 32 x-points (one per lane) by 8 rows (one per warp)
-constexpr int kZTileX = 32, kZTileY = 8;
+// tile of the z-streamed cell sweep: 64 x-points (two per lane) by 8 rows (one per warp)
+constexpr int kZTileX = 64, kZTileY = 8;
 
 struct P1Level {
    int     L = 0, n = 0;

@@ -330,11 +330,13 @@ __global__ void __launch_bounds__( 256 ) k_cell_march( LevelView v, OpView< A > 
 // ---------------------------------------------------------------------------------------------
 // z-streamed cell sweep (cp.async.bulk + mbarrier ring), the default for n >= 32.
 //
-// A unit is the tile x0..x0+31, y0..y0+7 of slices z_first..z_last of one macro-cell.  A producer
+// A unit is the tile x0..x0+63, y0..y0+7 of slices z_first..z_last of one macro-cell.  A producer
 // warp streams the tile's rows of every slice, with a one-point halo in x and y, into a ring of
 // shared-memory stages: lane r issues one bulk copy for row y0-1+r (10 rows per stage), and the
 // stage's full barrier completes when all bytes have landed.  Eight consumer warps (one per tile
-// row, one x per lane) march up the slices.  Of the 15 stencil values, four in slice z-1 and four
+// row, two x per lane) march up the slices.  Each slice load costs the producer a fixed few hundred
+// cycles of issue and barrier hand-off whatever its size, so tiles are as wide as the consumers'
+// registers allow and row offsets advance by additions instead of being recomputed.  Of the 15 stencil values, four in slice z-1 and four
 // in slice z were read in the previous step and roll through registers, so a step reads three
 // values of slice z and four of slice z+1 from shared memory, and slice z is released (empty
 // barrier, one arrival per consumer warp) as soon as step z ends.  With S stages, S-2 slices are
@@ -382,18 +384,6 @@ __device__ __forceinline__ void bulk_copy_g2s( void* dst, const void* src, uint3
                  : "memory" );
 }
 
-// 16-byte asynchronous global->shared copy (L2 only) and the mbarrier arrival that fires once all
-// earlier cp.async of this thread have landed (the barrier's expected count covers it: noinc)
-__device__ __forceinline__ void cp_async16( void* dst, const void* src )
-{
-   asm volatile( "cp.async.cg.shared.global [%0], [%1], 16;" ::"r"( smem_addr( dst ) ), "l"( src ) : "memory" );
-}
-
-__device__ __forceinline__ void cp_async_arrive( uint64_t* bar )
-{
-   asm volatile( "cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"( smem_addr( bar ) ) : "memory" );
-}
-
 __device__ __forceinline__ uint64_t global_ns()
 {
    uint64_t t;
@@ -436,29 +426,38 @@ struct ZCfg
    static constexpr int rows  = kZTileY + 2;                                   // tile rows + halo
    static constexpr int aux0  = rows * RW;                                     // second-vector rows start here
    static constexpr int stage = aux0 + ( AUX ? kZTileY * RWA : 0 );            // elements per stage
-   static constexpr int S     = sizeof( T ) == 8 ? 12 : ( sizeof( T ) == 4 ? 16 : 24 );  // ring depth
+   static constexpr int S     = AUX ? 8 : 10;                                   // ring depth
    static constexpr size_t smem_bytes = size_t( S ) * stage * sizeof( T );
 };
-constexpr int kZWarps   = kZTileY;
-constexpr int kZThreads = ( kZWarps + 1 ) * 32;  // consumer warps + one producer warp
+constexpr int kZWarps     = kZTileY;
+// Two producer warps (load l is issued by producer l % 2): one warp's issue and hand-off chain per
+// slice load is what limits a single-producer ring (measured on B200: 0.163 -> 0.136 ms for the
+// level-8 cube apply in FP64, 0.154 -> 0.108 ms in FP32).
+constexpr int kZProducers = 2;
+constexpr int kZThreads   = ( kZWarps + kZProducers ) * 32;  // consumer warps + producer warps
+constexpr int kZPts     = kZTileX / 32;         // x-points per consumer lane
+
+// offset of slice z+1 minus offset of slice z in a macro-cell array (tri(n+1-z) points in slice z)
+__device__ __forceinline__ int64_t slice_step( int n, int z ) { return int64_t( n + 1 - z ) * ( n + 2 - z ) / 2; }
 
 // producer warp: streams the rows of every slice of the block's units into the ring.  Lane r < 10
 // copies source row y0-1+r; with AUX, lane 10+r copies row y0+r of the second vector (slices
-// z_first..z_last only, rows with interior points only).
-//
-// Two ways to fill a stage: `bulk` issues one cp.async.bulk per row segment (the full barrier
-// expects one arrival plus the bytes); otherwise the 32 lanes copy the row segments in 16-byte
-// cp.async pieces, one row per warp instruction, and each lane arrives on the full barrier when its
-// copies have landed (the barrier expects 32 arrivals).
+// z_first..z_last only, rows with interior points only).  Row offsets advance by additions from
+// slice to slice: cidx(0, y, z+1) = cidx(0, y, z) + tri(n+1-z) - y.
 template < typename T, bool AUX >
 __device__ __forceinline__ void zstream_produce( const LevelView& v, uint32_t flag, const T* __restrict__ src,
                                                  const T* __restrict__ aux, int nC, T* ring, uint64_t* full, uint64_t* empty,
-                                                 uint32_t* shw, volatile int* abort_flag, int* err, bool bulk )
+                                                 uint32_t* shw, volatile int* abort_flag, int* err )
 {
    using Cfg = ZCfg< T, AUX >;
    constexpr int S = Cfg::S, AL = Cfg::al;
-   const int     lane = threadIdx.x & 31, n = v.n;
+   static_assert( S % kZProducers == 0, "every stage must belong to one producer warp" );
+   const int     lane = threadIdx.x & 31, n = v.n, me = ( threadIdx.x >> 5 ) - kZWarps;
    const int     u0 = v.zbegin[blockIdx.x], u1 = v.zbegin[blockIdx.x + 1];
+   const bool    is_src = lane < Cfg::rows, is_aux = AUX && lane >= Cfg::rows && lane < Cfg::rows + kZTileY;
+   const int     dsto   = is_src ? lane * Cfg::RW : Cfg::aux0 + ( lane - Cfg::rows ) * Cfg::RWA;
+   const T*      gbase  = is_src ? src : aux;
+   const int     shbit  = is_src ? 3 * lane : ( is_aux ? 3 * ( lane - Cfg::rows ) : 0 );
    int           ld = 0;  // sequence number of the next slice load
    bool          ok = true;
    for ( int c = 0; c < nC && ok; ++c )
@@ -467,9 +466,13 @@ __device__ __forceinline__ void zstream_produce( const LevelView& v, uint32_t fl
       const int64_t cb = v.cell_off[c];
       for ( int u = u0; u < u1 && ok; ++u )
       {
-         const int4 U = v.zunits[u];  // x0, y0, z_first, z_last
-         for ( int zz = U.z - 1; zz <= U.w + 1; ++zz, ++ld )
+         const int4 U  = v.zunits[u];  // x0, y0, z_first, z_last
+         const int  yy = is_src ? U.y - 1 + lane : U.y + ( lane - Cfg::rows );
+         const int  xa = is_src ? U.x - 1 : U.x;  // first x of the row segment
+         int64_t    rb = cidx( n, 0, yy, U.z - 1 );
+         for ( int zz = U.z - 1; zz <= U.w + 1; rb += slice_step( n, zz ) - yy, ++zz, ++ld )
          {
+            if ( ld % kZProducers != me ) continue;
             const int st = ld % S;
             if ( ld >= S && !mbar_wait_bounded( &empty[st], uint32_t( ( ld / S - 1 ) & 1 ), abort_flag ) )
             {
@@ -477,72 +480,29 @@ __device__ __forceinline__ void zstream_produce( const LevelView& v, uint32_t fl
                break;
             }
             uint32_t bytes = 0, sh = 0;
-            int64_t  a0 = 0;
-            int      dsto = 0;
-            const T* gsrc = src;
-            if ( lane < Cfg::rows )
+            int64_t  a0    = 0;
+            // last x of the segment: the halo point (source) or the last interior point (second vector)
+            const int  xe   = is_src ? min( U.x + kZTileX, n - yy - zz ) : min( U.x + kZTileX - 1, n - 1 - yy - zz );
+            const bool live = ( is_src && yy + zz <= n && xe >= xa ) || ( is_aux && zz >= U.z && zz <= U.w && xe >= xa );
+            if ( live )
             {
-               const int yy = U.y - 1 + lane;
-               if ( yy + zz <= n && n - yy - zz >= U.x - 1 )
-               {
-                  const int64_t s0 = cidx( n, U.x - 1, yy, zz );
-                  const int     xe = min( U.x + kZTileX, n - yy - zz );  // last x of the segment
-                  const int64_t e1 = s0 + ( xe - ( U.x - 1 ) ) + 1;       // one past the segment
-                  sh               = uint32_t( s0 & ( AL - 1 ) );
-                  a0               = s0 - sh;
-                  bytes            = uint32_t( ( ( e1 + AL - 1 ) / AL * AL - a0 ) * int64_t( sizeof( T ) ) );
-                  dsto             = lane * Cfg::RW;
-               }
-            }
-            else if ( AUX && lane < Cfg::rows + kZTileY && zz >= U.z && zz <= U.w )
-            {
-               const int r = lane - Cfg::rows, yy = U.y + r;
-               if ( n - 1 - yy - zz >= U.x )
-               {
-                  const int64_t s0 = cidx( n, U.x, yy, zz );
-                  const int     xe = min( U.x + kZTileX - 1, n - 1 - yy - zz );
-                  const int64_t e1 = s0 + ( xe - U.x ) + 1;
-                  sh               = uint32_t( s0 & ( AL - 1 ) );
-                  a0               = s0 - sh;
-                  bytes            = uint32_t( ( ( e1 + AL - 1 ) / AL * AL - a0 ) * int64_t( sizeof( T ) ) );
-                  dsto             = Cfg::aux0 + r * Cfg::RWA;
-                  gsrc             = aux;
-               }
+               const int64_t s0 = rb + xa;
+               const int64_t e1 = rb + xe + 1;  // one past the segment
+               sh               = uint32_t( s0 & ( AL - 1 ) );
+               a0               = s0 - sh;
+               bytes            = uint32_t( ( ( e1 + AL - 1 ) / AL * AL - a0 ) * int64_t( sizeof( T ) ) );
             }
             const uint32_t total = __reduce_add_sync( 0xffffffffu, bytes );
-            const uint32_t w0    = __reduce_or_sync( 0xffffffffu, lane < Cfg::rows ? sh << ( 3 * lane ) : 0u );
-            const uint32_t w1 =
-                __reduce_or_sync( 0xffffffffu, ( lane >= Cfg::rows && lane < Cfg::rows + kZTileY ) ? sh << ( 3 * ( lane - Cfg::rows ) ) : 0u );
-            if ( bulk )
+            const uint32_t w0    = __reduce_or_sync( 0xffffffffu, is_src ? sh << shbit : 0u );
+            const uint32_t w1    = AUX ? __reduce_or_sync( 0xffffffffu, is_aux ? sh << shbit : 0u ) : 0u;
+            if ( lane == 0 )
             {
-               if ( lane == 0 )
-               {
-                  shw[2 * st]     = w0;
-                  shw[2 * st + 1] = w1;
-                  mbar_expect_tx( &full[st], total );
-               }
-               __syncwarp();
-               if ( bytes ) bulk_copy_g2s( ring + st * Cfg::stage + dsto, gsrc + cb + a0, bytes, &full[st] );
+               shw[2 * st]     = w0;
+               shw[2 * st + 1] = w1;
+               mbar_expect_tx( &full[st], total );
             }
-            else
-            {
-               if ( lane == 0 )
-               {
-                  shw[2 * st]     = w0;
-                  shw[2 * st + 1] = w1;
-               }
-               T* sbase = ring + st * Cfg::stage;
-               for ( int r = 0; r < Cfg::rows + ( AUX ? kZTileY : 0 ); ++r )
-               {
-                  const uint32_t rb = __shfl_sync( 0xffffffffu, bytes, r );
-                  if ( rb == 0 ) continue;
-                  const int64_t ra0 = __shfl_sync( 0xffffffffu, a0, r );
-                  const int     rd  = __shfl_sync( 0xffffffffu, dsto, r );
-                  const T*      gp  = ( r < Cfg::rows ? src : aux ) + cb + ra0;
-                  if ( uint32_t( lane ) * 16u < rb ) cp_async16( sbase + rd + lane * AL, gp + lane * AL );
-               }
-               cp_async_arrive( &full[st] );
-            }
+            __syncwarp();
+            if ( bytes ) bulk_copy_g2s( ring + st * Cfg::stage + dsto, gbase + cb + a0, bytes, &full[st] );
          }
       }
    }
@@ -553,7 +513,7 @@ __device__ __forceinline__ void zstream_produce( const LevelView& v, uint32_t fl
    }
    // drain: the latest load issued on every stage has landed before the block may exit
    if ( lane == 0 )
-      for ( int s = 0; s < S && s < ld; ++s )
+      for ( int s = me; s < S && s < ld; s += kZProducers )
       {
          const int j = s + ( ( ld - 1 - s ) / S ) * S;
          if ( !mbar_wait_bounded( &full[s], uint32_t( ( j / S ) & 1 ), nullptr ) ) atomicExch( err, 1 );
@@ -578,10 +538,18 @@ __device__ __forceinline__ void zstream_epilogue( int64_t i, A s, A invd, A cent
    else if constexpr ( OP == OP_DINV_APPLY ) stv( dst + i, invd * s );
 }
 
+// the eight values of one point that roll over from one slice step to the next
+template < typename A >
+struct ZPoint
+{
+   A B, BE, BN, BNW;  // slice z-1: (x,y), (x+1,y), (x,y+1), (x-1,y+1)
+   A C, W, S, SE;     // slice z:   (x,y), (x-1,y), (x,y-1), (x+1,y-1)
+};
+
 template < typename T, typename A, int OP >
 __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
                                                                   const T* __restrict__ v1, T* v2, T* dst, A a0, A a1, int nC,
-                                                                  int* err, int bulk )
+                                                                  int* err )
 {
    constexpr bool AUX = zstream_aux< OP >();
    using Cfg          = ZCfg< T, AUX >;
@@ -590,13 +558,14 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, O
    T*                  ring = reinterpret_cast< T* >( zs_raw );
    __shared__ uint64_t full[S], empty[S];
    __shared__ uint32_t shw[2 * S];
+   __shared__ A        wsm[kZWarps][16];  // per consumer warp: the cell's 15 weights and 1/diagonal
    __shared__ int      abort_flag;
    const int           warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n = v.n;
    if ( threadIdx.x == 0 )
    {
       for ( int s = 0; s < S; ++s )
       {
-         mbar_init( &full[s], bulk ? 1 : 32 );
+         mbar_init( &full[s], 1 );
          mbar_init( &empty[s], kZWarps );
       }
       abort_flag = 0;
@@ -604,18 +573,19 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, O
    }
    __syncthreads();
    volatile int* abrt = &abort_flag;
-   if ( warp == kZWarps )
+   if ( warp >= kZWarps )
    {
       const T* aux = ( OP == OP_CHEBI || OP == OP_CHEBL ) ? v2 : ( OP == OP_APPLY_ADD ? dst : v1 );
-      zstream_produce< T, AUX >( v, flag, src, aux, nC, ring, full, empty, shw, abrt, err, bulk != 0 );
+      zstream_produce< T, AUX >( v, flag, src, aux, nC, ring, full, empty, shw, abrt, err );
       return;
    }
 
-   // consumer warp `warp` owns tile row y0 + warp; stage row r holds global row y0 - 1 + r
+   // consumer warp `warp` owns tile row y0 + warp; stage row r holds global row y0 - 1 + r; lane
+   // owns x = x0 + lane + 32 k, k < kZPts
    const int u0 = v.zbegin[blockIdx.x], u1 = v.zbegin[blockIdx.x + 1];
    const int rS = warp, rC = warp + 1, rN = warp + 2;  // rows y-1, y, y+1 of the stage
-   auto at = [&]( int st, uint32_t word, int r, int dx ) -> A {
-      return A( ring[st * Cfg::stage + r * RW + int( ( word >> ( 3 * r ) ) & 7u ) + lane + 1 + dx] );
+   auto at = [&]( const T* st, uint32_t word, int r, int k, int dx ) -> A {
+      return A( st[r * RW + int( ( word >> ( 3 * r ) ) & 7u ) + lane + 32 * k + 1 + dx] );
    };
    auto fail = [&]() {
       if ( lane == 0 )
@@ -629,10 +599,13 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, O
    {
       if ( !( v.cell_bc[c] & flag ) ) continue;
       const int64_t base = v.cell_off[c];
-      const A*      W    = o.W + size_t( c ) * kNumClasses * kNumDirs;  // interior class 0
-      const A w0 = W[0], wW = W[1], wE = W[2], wS = W[3], wN = W[4], wB = W[5], wT = W[6], wNW = W[7], wSE = W[8], wTW = W[9],
-              wBE = W[10], wTS = W[11], wBN = W[12], wTSE = W[13], wBNW = W[14];
-      const A invd = o.invd_c[c];
+      // the weights are read from shared memory at every use (broadcast, shared by the lane's
+      // points) rather than held in 30 registers
+      A* w = wsm[warp];
+      __syncwarp();
+      if ( lane < kNumDirs ) w[lane] = o.W[size_t( c ) * kNumClasses * kNumDirs + lane];  // interior class 0
+      if ( lane == kNumDirs ) w[kNumDirs] = o.invd_c[c];
+      __syncwarp();
       for ( int u = u0; u < u1; ++u )
       {
          const int4 U = v.zunits[u];
@@ -642,49 +615,76 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, O
          if ( !mbar_wait_bounded( &full[sm], uint32_t( ( ld / S ) & 1 ), abrt ) ||
               !mbar_wait_bounded( &full[s0], uint32_t( ( ( ld + 1 ) / S ) & 1 ), abrt ) )
             return fail();
-         const uint32_t wm = shw[2 * sm], wc = shw[2 * s0];
-         A B = at( sm, wm, rC, 0 ), BE = at( sm, wm, rC, 1 ), BN = at( sm, wm, rN, 0 ), BNW = at( sm, wm, rN, -1 );
-         A C = at( s0, wc, rC, 0 ), Wv = at( s0, wc, rC, -1 ), Sv = at( s0, wc, rS, 0 ), SE = at( s0, wc, rS, 1 );
+         ZPoint< A > P[kZPts];
+         {
+            const T*       Rm = ring + sm * Cfg::stage;
+            const T*       R0 = ring + s0 * Cfg::stage;
+            const uint32_t wm = shw[2 * sm], wc = shw[2 * s0];
+#pragma unroll
+            for ( int k = 0; k < kZPts; ++k )
+            {
+               P[k].B   = at( Rm, wm, rC, k, 0 );
+               P[k].BE  = at( Rm, wm, rC, k, 1 );
+               P[k].BN  = at( Rm, wm, rN, k, 0 );
+               P[k].BNW = at( Rm, wm, rN, k, -1 );
+               P[k].C   = at( R0, wc, rC, k, 0 );
+               P[k].W   = at( R0, wc, rC, k, -1 );
+               P[k].S   = at( R0, wc, rS, k, 0 );
+               P[k].SE  = at( R0, wc, rS, k, 1 );
+            }
+         }
          __syncwarp();
          if ( lane == 0 ) mbar_arrive( &empty[sm] );
-         for ( int z = U.z; z <= U.w; ++z )
+         int64_t out = base + cidx( n, x, y, U.z );  // output offset of point k = 0, advanced per slice
+         // unrolled by two so that the rolled values alternate registers instead of being copied
+#pragma unroll 2
+         for ( int z = U.z; z <= U.w; out += slice_step( n, z ) - y, ++z )
          {
             const int lz = ld + 1 + ( z - U.z ), lp = lz + 1;
             const int sz = lz % S, sp = lp % S;
             if ( !mbar_wait_bounded( &full[sp], uint32_t( ( lp / S ) & 1 ), abrt ) ) return fail();
+            const T*       Rz = ring + sz * Cfg::stage;
+            const T*       Rp = ring + sp * Cfg::stage;
             const uint32_t wz = shw[2 * sz], wp = shw[2 * sp];
-            const A        E = at( sz, wz, rC, 1 ), N = at( sz, wz, rN, 0 ), NW = at( sz, wz, rN, -1 );
-            const A        Tt = at( sp, wp, rC, 0 ), TW = at( sp, wp, rC, -1 ), TS = at( sp, wp, rS, 0 ), TSE = at( sp, wp, rS, 1 );
-            if ( x + y + z <= n - 1 )
+            const uint32_t wa = AUX ? shw[2 * sz + 1] : 0u;
+#pragma unroll
+            for ( int k = 0; k < kZPts; ++k )
             {
-               A auxv = A( 0 );
-               if constexpr ( AUX )
-                  auxv = A( ring[sz * Cfg::stage + Cfg::aux0 + warp * Cfg::RWA + int( ( shw[2 * sz + 1] >> ( 3 * warp ) ) & 7u ) + lane] );
-               A acc = w0 * C;
-               acc += wW * Wv;
-               acc += wE * E;
-               acc += wS * Sv;
-               acc += wN * N;
-               acc += wB * B;
-               acc += wT * Tt;
-               acc += wNW * NW;
-               acc += wSE * SE;
-               acc += wTW * TW;
-               acc += wBE * BE;
-               acc += wTS * TS;
-               acc += wBN * BN;
-               acc += wTSE * TSE;
-               acc += wBNW * BNW;
-               zstream_epilogue< T, A, OP >( base + cidx( n, x, y, z ), acc, invd, C, auxv, v2, dst, a0, a1 );
+               const A E = at( Rz, wz, rC, k, 1 ), N = at( Rz, wz, rN, k, 0 ), NW = at( Rz, wz, rN, k, -1 );
+               const A Tt = at( Rp, wp, rC, k, 0 ), TW = at( Rp, wp, rC, k, -1 ), TS = at( Rp, wp, rS, k, 0 ),
+                       TSE = at( Rp, wp, rS, k, 1 );
+               ZPoint< A >& p = P[k];
+               if ( x + 32 * k + y + z <= n - 1 )
+               {
+                  A auxv = A( 0 );
+                  if constexpr ( AUX )
+                     auxv = A( Rz[Cfg::aux0 + warp * Cfg::RWA + int( ( wa >> ( 3 * warp ) ) & 7u ) + lane + 32 * k] );
+                  A acc = w[0] * p.C;
+                  acc += w[1] * p.W;
+                  acc += w[2] * E;
+                  acc += w[3] * p.S;
+                  acc += w[4] * N;
+                  acc += w[5] * p.B;
+                  acc += w[6] * Tt;
+                  acc += w[7] * NW;
+                  acc += w[8] * p.SE;
+                  acc += w[9] * TW;
+                  acc += w[10] * p.BE;
+                  acc += w[11] * TS;
+                  acc += w[12] * p.BN;
+                  acc += w[13] * TSE;
+                  acc += w[14] * p.BNW;
+                  zstream_epilogue< T, A, OP >( out + 32 * k, acc, w[kNumDirs], p.C, auxv, v2, dst, a0, a1 );
+               }
+               p.B   = p.C;
+               p.BE  = E;
+               p.BN  = N;
+               p.BNW = NW;
+               p.C   = Tt;
+               p.W   = TW;
+               p.S   = TS;
+               p.SE  = TSE;
             }
-            B   = C;
-            BE  = E;
-            BN  = N;
-            BNW = NW;
-            C   = Tt;
-            Wv  = TW;
-            Sv  = TS;
-            SE  = TSE;
             __syncwarp();
             if ( lane == 0 ) mbar_arrive( &empty[sz] );
          }
@@ -722,19 +722,6 @@ static void zstream_attributes_all()
    zstream_attributes< double, double >();
    zstream_attributes< float, float >();
    zstream_attributes< __half, float >();
-}
-
-// z-stream stages are filled with cp.async.bulk row copies; HYB_ZCOPY=async selects 16-byte
-// cp.async pieces instead (measured slower on B200: the producer warp issues one instruction per row)
-static int zstream_bulk()
-{
-   static int b = -1;
-   if ( b < 0 )
-   {
-      const char* e = getenv( "HYB_ZCOPY" );
-      b             = ( e && std::string( e ) == "async" ) ? 0 : 1;
-   }
-   return b;
 }
 
 static int march_prefetch_distance()
@@ -837,7 +824,7 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
    {
       constexpr size_t smem = ZCfg< T, zstream_aux< OP >() >::smem_bytes;  // attribute set by ensure_constants
       k_cell_zstream< T, A, OP ><<< v.nzblocks, kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ),
-                                                                                 A( a.a1 ), nC, ctx->d_error, zstream_bulk() );
+                                                                                 A( a.a1 ), nC, ctx->d_error );
       ++ctx->launches;
    }
    else if ( cell_kernel_variant() >= 1 && v.nmarch > 0 && nC > 0 )

@@ -301,9 +301,10 @@ void build_level( Mesh* m, int L )
 
 // Work units of the z-streamed sweep.  A unit is the tile x0..x0+31, y0..y0+7 of slices
 // z_first..z_last (interior points only: x, y, z >= 1, x+y+z <= n-1).  The slice range is cut into
-// chunks of zc slices, zc the largest power of two in [8, 64] that still gives at least three units
-// per block; units are then handed out longest-first to the least loaded block, so every block
-// ends at about the same time.
+// chunks of zc slices, zc the largest power of two in [8, 32] that still gives at least one unit
+// per two blocks (every chunk re-reads two halo slices, and every slice load costs a fixed hand-off,
+// so long chunks win over finer balance); units are then handed out longest-first to the least
+// loaded block.
 void build_zunits( P1Level& P, int nblocks )
 {
    const int n = P.n;
@@ -333,10 +334,10 @@ void build_zunits( P1Level& P, int nblocks )
          }
       return us;
    };
-   int                 zc = 64;
+   int                 zc = 32;
    std::vector< Unit > us = make( zc );
-   while ( zc > 8 && int64_t( us.size() ) < 3 * int64_t( nblocks ) ) us = make( zc /= 2 );
-   if ( const char* e = getenv( "HYB_ZCHUNK" ) ) us = make( std::max( 1, atoi( e ) ) );
+   while ( zc > 8 && 2 * int64_t( us.size() ) < int64_t( nblocks ) ) us = make( zc /= 2 );
+   if ( const char* e = getenv( "HYB_ZCHUNK" ); e && atoi( e ) > 0 ) us = make( atoi( e ) );
    std::stable_sort( us.begin(), us.end(), []( const Unit& a, const Unit& b ) { return a.work > b.work; } );
    const int nb = std::max( 1, std::min( nblocks, int( us.size() ) ) );
    std::vector< std::vector< std::array< int, 4 > > >                                       per( nb );
