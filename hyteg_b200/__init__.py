@@ -123,6 +123,7 @@ _SIGS = {
     "hyb_residual_norm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32,
                                     C.POINTER(C.c_double)]),
     "hyb_fn_fill_random": (C.c_int, [C.c_void_p, C.c_int, C.c_uint64]),
+    "hyb_op_store_element_matrices": (C.c_int, [C.c_void_p]),
     "hyb_fn_dot_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.POINTER(C.c_double)]),
     "hyb_serve_params_default": (C.c_int, [C.c_void_p]),
     "hyb_serve_create": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
@@ -455,6 +456,10 @@ class P1ElementwiseBlendingDivKGradOperator(_ConstantOperator):
         _check(lib().hyb_op_create_divkgrad(ctx.h, storage.h, min_level, max_level, C.byref(c),
                                             1 if blending == "shell" else 0, C.byref(h)))
         self.h = h
+
+    def computeAndStoreLocalElementMatrices(self):
+        """Element matrices are computed once per level and read back by every later apply."""
+        _check(lib().hyb_op_store_element_matrices(self.h))
 
 
 class P1toP1LinearRestriction:

@@ -186,6 +186,11 @@ int hyb_ctx_synchronize( hyb_ctx* ctx )
    if ( e )
    {
       cudaMemset( ctx->c.d_error, 0, sizeof( int ) );
+      if ( e == 2 )
+      {
+         g_err = "a kernel's index self-check failed (an access outside its buffers was skipped)";
+         return HYB_EINTERNAL;
+      }
       g_err = "a device-side bounded wait ran out (shared-memory staging did not complete)";
       return HYB_ETIMEOUT;
    }
@@ -735,6 +740,15 @@ int hyb_op_create( hyb_ctx* ctx, hyb_mesh* mesh, int kind, int min_level, int ma
       throw;
    }
    *out = h;
+   HYB_CATCH
+}
+
+int hyb_op_store_element_matrices( hyb_op* op )
+{
+   HYB_TRY
+   require( op, "NULL argument" );
+   require( op->o.elementwise, "only elementwise operators store element matrices" );
+   op->o.store_matrices = true;
    HYB_CATCH
 }
 

@@ -198,6 +198,9 @@ struct ElemLevel {
    void* d_invd[3] = { nullptr, nullptr, nullptr };  // inverse diagonal per DoF, per storage dtype
    int2* d_hrows    = nullptr;                         // anchor rows (y, z) per (y, z) parity
    int   hoff[5]    = { 0, 0, 0, 0, 0 };
+   // stored element matrices (computeAndStoreLocalElementMatrices): the 10 upper-triangle entries
+   // of every micro-cell's 4x4 matrix, value-major, in double ([0]) and float ([1])
+   void* d_K[2] = { nullptr, nullptr };
 };
 
 struct Operator {
@@ -207,6 +210,7 @@ struct Operator {
    std::map< int, OpLevel >  lv;
    // elementwise operators
    bool                      elementwise = false;
+   bool                      store_matrices = false;  // element matrices computed once and read back
    int                       blending    = 0;
    Coefficient               coeff;
    CellGeom*                 d_geom = nullptr;

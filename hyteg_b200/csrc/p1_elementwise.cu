@@ -229,10 +229,14 @@ __device__ __forceinline__ void   st_any( __half* p, float v ) { *p = __float2ha
 
 // One parity pass: warp per half-grid row (y, z) of anchors with y = py mod 2, z = pz mod 2, lanes
 // over x = px + 2k.  MODE 0 accumulates A src, MODE 1 the diagonal.
+// MODE 0: y += K x with K computed on the fly; 1: diagonal of K; 2: compute K and store its upper
+// triangle; 3: y += K x with K read from storage.  Stored entry v of micro-cell (cell c, type ty,
+// anchor a) sits at kst[v * kstride + (c * 6 + ty) * tet(n) + cidx(n - 1, a)].
 template < typename T, typename A, int MODE >
 __global__ void __launch_bounds__( 256 ) k_elem_pass( int n, int nrows, const int2* __restrict__ rows, const int64_t* __restrict__ cell_off,
                                                        const CellGeom* __restrict__ geom, Coefficient kc, int px,
-                                                       const T* __restrict__ src, A* __restrict__ acc )
+                                                       const T* __restrict__ src, A* __restrict__ acc, A* __restrict__ kst,
+                                                       int64_t kstride, int64_t level_size, int* err )
 {
    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
    const int r    = blockIdx.x * 8 + warp;
@@ -259,14 +263,42 @@ __global__ void __launch_bounds__( 256 ) k_elem_pass( int n, int nrows, const in
             for ( int d = 0; d < 3; ++d ) X[m][d] = A( g.P[0][d] ) + st[0][d] * A( vx ) + st[1][d] * A( vy ) + st[2][d] * A( vz );
          }
          A K[4][4];
+         const int64_t slot = ( int64_t( c ) * 6 + ty ) * tet_size( n ) + cidx( n - 1, x, y, z );
+         // self-check: every node inside the level's vector and every stored slot inside its array;
+         // a violation is recorded (error word 2) and the micro-cell skipped
+         {
+            bool bad = ( MODE >= 2 ) && ( slot < 0 || slot >= kstride );
+            for ( int m = 0; m < 4; ++m ) bad |= idx[m] < 0 || idx[m] >= level_size;
+            if ( bad )
+            {
+               atomicExch( err, 2 );
+               continue;
+            }
+         }
+         if constexpr ( MODE == 3 )
+         {
+            int v = 0;
+            for ( int i = 0; i < 4; ++i )
+               for ( int j = i; j < 4; ++j, ++v ) K[i][j] = K[j][i] = kst[v * kstride + slot];
+            A xl[4];
+            for ( int m = 0; m < 4; ++m ) xl[m] = A( ld_any( src + idx[m] ) );
+            for ( int i = 0; i < 4; ++i ) acc[idx[i]] += K[i][0] * xl[0] + K[i][1] * xl[1] + K[i][2] * xl[2] + K[i][3] * xl[3];
+            continue;
+         }
          p1_divkgrad_element( g, kc, X, K );
-         if constexpr ( MODE == 0 )
+         if constexpr ( MODE == 2 )
+         {
+            int v = 0;
+            for ( int i = 0; i < 4; ++i )
+               for ( int j = i; j < 4; ++j, ++v ) kst[v * kstride + slot] = K[i][j];
+         }
+         else if constexpr ( MODE == 0 )
          {
             A xl[4];
             for ( int m = 0; m < 4; ++m ) xl[m] = A( ld_any( src + idx[m] ) );
             for ( int i = 0; i < 4; ++i ) acc[idx[i]] += K[i][0] * xl[0] + K[i][1] * xl[1] + K[i][2] * xl[2] + K[i][3] * xl[3];
          }
-         else
+         else if constexpr ( MODE == 1 )
             for ( int i = 0; i < 4; ++i ) acc[idx[i]] += K[i][i];
       }
 }
@@ -432,12 +464,20 @@ static void ensure_rows( Operator* op, int L )
       check_cuda( cudaMemcpy( e.d_hrows, rows.data(), rows.size() * sizeof( int2 ), cudaMemcpyHostToDevice ), "upload rows" );
 }
 
+// entries per stored value: every (cell, micro-cell type, anchor) slot of the level
+static int64_t kstride( Mesh* m, int L ) { return int64_t( m->topo.nC ) * 6 * tet_size( int64_t( 1 ) << L ); }
+
+template < typename A >
+static A* stored_matrices( Operator* op, int L ) { return reinterpret_cast< A* >( op->el[L].d_K[sizeof( A ) == 8 ? 0 : 1] ); }
+
 template < typename T, typename A, int MODE >
 static void run_passes( Context* ctx, Mesh* m, Operator* op, int L, const T* src, A* acc )
 {
    P1Level&   P = m->level( L );
    ElemLevel& e = op->el[L];
-   check_cuda( cudaMemsetAsync( acc, 0, P.size * sizeof( A ), ctx->stream ), "cudaMemset(acc)" );
+   if ( MODE != 2 ) check_cuda( cudaMemsetAsync( acc, 0, P.size * sizeof( A ), ctx->stream ), "cudaMemset(acc)" );
+   A*            kst = stored_matrices< A >( op, L );
+   const int64_t ks  = kstride( m, L );
    const int nC = m->topo.nC;
    for ( int p = 0; p < 8; ++p )
    {
@@ -446,7 +486,7 @@ static void run_passes( Context* ctx, Mesh* m, Operator* op, int L, const T* src
       if ( nr <= 0 ) continue;
       dim3 grid( ( nr + 7 ) / 8, nC );
       k_elem_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( P.n, nr, e.d_hrows + e.hoff[q], P.d_off + P.nB, op->d_geom,
-                                                                   op->coeff, px, src, acc );
+                                                                   op->coeff, px, src, acc, kst, ks, P.size, ctx->d_error );
       ++ctx->launches;
    }
    check_cuda( cudaGetLastError(), "elementwise pass launch" );
@@ -467,6 +507,12 @@ static void ensure_level_t( Context* ctx, Operator* op, int L, int dtype )
    ensure_rows( op, L );
    ElemLevel& e = op->el[L];
    A*         acc = acc_buffer< A >( op, L, P.size );
+   void*&     K   = e.d_K[sizeof( A ) == 8 ? 0 : 1];
+   if ( op->store_matrices && !K )
+   {
+      check_cuda( cudaMalloc( &K, size_t( 10 ) * size_t( kstride( m, L ) ) * sizeof( A ) ), "cudaMalloc(element matrices)" );
+      run_passes< T, A, 2 >( ctx, m, op, L, nullptr, acc );
+   }
    if ( e.d_invd[dtype] ) return;
    A* invd = nullptr;
    check_cuda( cudaMalloc( &invd, P.size * sizeof( A ) ), "cudaMalloc(inverse diagonal)" );
@@ -500,7 +546,8 @@ static void run_elem( Context* ctx, Mesh* m, Operator* op, int L, int dtype, con
    P1Level& P   = m->level( L );
    A*       acc = acc_buffer< A >( op, L, P.size );
    const A* inv = reinterpret_cast< const A* >( op->el[L].d_invd[dtype] );
-   run_passes< T, A, 0 >( ctx, m, op, L, (const T*) a.src, acc );
+   if ( stored_matrices< A >( op, L ) ) run_passes< T, A, 3 >( ctx, m, op, L, (const T*) a.src, acc );
+   else run_passes< T, A, 0 >( ctx, m, op, L, (const T*) a.src, acc );
    const int nrows = int( P.rows.size() );
    {
       struct Join

@@ -659,21 +659,21 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, O
                   A auxv = A( 0 );
                   if constexpr ( AUX )
                      auxv = A( Rz[Cfg::aux0 + warp * Cfg::RWA + int( ( wa >> ( 3 * warp ) ) & 7u ) + lane + 32 * k] );
-                  A acc = w[0] * p.C;
-                  acc += w[1] * p.W;
-                  acc += w[2] * E;
-                  acc += w[3] * p.S;
-                  acc += w[4] * N;
-                  acc += w[5] * p.B;
-                  acc += w[6] * Tt;
-                  acc += w[7] * NW;
-                  acc += w[8] * p.SE;
-                  acc += w[9] * TW;
-                  acc += w[10] * p.BE;
-                  acc += w[11] * TS;
-                  acc += w[12] * p.BN;
-                  acc += w[13] * TSE;
-                  acc += w[14] * p.BNW;
+                  // three independent partial sums: the dependent FMA chain is 7 deep instead of 15
+                  A s0 = w[0] * p.C, s1 = w[5] * p.B, s2 = w[10] * p.BE;
+                  s0 += w[1] * p.W;
+                  s1 += w[6] * Tt;
+                  s2 += w[11] * TS;
+                  s0 += w[2] * E;
+                  s1 += w[7] * NW;
+                  s2 += w[12] * p.BN;
+                  s0 += w[3] * p.S;
+                  s1 += w[8] * p.SE;
+                  s2 += w[13] * TSE;
+                  s0 += w[4] * N;
+                  s1 += w[9] * TW;
+                  s2 += w[14] * p.BNW;
+                  const A acc = s0 + ( s1 + s2 );
                   zstream_epilogue< T, A, OP >( out + 32 * k, acc, w[kNumDirs], p.C, auxv, v2, dst, a0, a1 );
                }
                p.B   = p.C;

@@ -129,16 +129,23 @@ void free_slot( hyb_serve* s, ServeSlot* sl )
 
 // bytes a slot holds: x, b (all levels), tmp and the solver's temporaries (about six more vectors
 // per level), plus the elementwise scratch
+// (plus, for div-k-grad, the stored element matrices: 10 values per micro-cell slot and level, in
+// FP64 and for mixed slots also in FP32)
 double slot_bytes( ServeKey k )
 {
    int64_t total = 0;
+   double  mats  = 0;
+   int     counts[4] = { 0, 0, 0, 0 };  // vertices, edges, faces, cells
+   hyb_mesh_counts( k.mesh, counts );
+   const int nC = counts[3];
    for ( int L = 0; L <= k.level; ++L )
    {
       int64_t n = 0;
       hyb_layout_packed_size( k.mesh, L, &n );
       total += n;
+      if ( k.kind == HYB_P1_ELEM_DIVKGRAD ) mats += double( nC ) * 6.0 * double( hyb::tet_size( int64_t( 1 ) << L ) ) * 10.0;
    }
-   return double( total ) * 8.0 * ( k.mixed ? 12.0 : 10.0 );
+   return double( total ) * 8.0 * ( k.mixed ? 12.0 : 10.0 ) + mats * ( k.mixed ? 12.0 : 8.0 );
 }
 
 ServeSlot* make_slot( hyb_serve* s, const ServeRequest& r )
@@ -150,7 +157,12 @@ ServeSlot* make_slot( hyb_serve* s, const ServeRequest& r )
    ok( hyb_ctx_create( dev, nullptr, &sl->ctx ) );
    const int L = r.key.level;
    if ( r.key.kind == HYB_P1_CONST_LAPLACE ) ok( hyb_op_create( sl->ctx, r.key.mesh, HYB_P1_CONST_LAPLACE, 0, L, &sl->op ) );
-   else ok( hyb_op_create_divkgrad( sl->ctx, r.key.mesh, 0, L, &r.coeff, r.key.blending, &sl->op ) );
+   else
+   {
+      // resident hierarchies are solved many times: compute the element matrices once
+      ok( hyb_op_create_divkgrad( sl->ctx, r.key.mesh, 0, L, &r.coeff, r.key.blending, &sl->op ) );
+      ok( hyb_op_store_element_matrices( sl->op ) );
+   }
    hyb_gmg_params gp;
    hyb_gmg_params_default( &gp );
    gp.min_level             = 0;

@@ -591,6 +591,7 @@ Operator::~Operator()
    {
       cudaFree( kv.second.d_acc );
       for ( void* p : kv.second.d_invd ) cudaFree( p );
+      for ( void* p : kv.second.d_K ) cudaFree( p );
       cudaFree( kv.second.d_hrows );
    }
    cudaFree( d_geom );

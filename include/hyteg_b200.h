@@ -182,6 +182,11 @@ int hyb_op_create( hyb_ctx* ctx, hyb_mesh* mesh, int kind, int min_level, int ma
  * assembled inverse diagonal (P1ElementwiseOperator::computeInverseDiagonalOperatorValues) */
 int hyb_op_create_divkgrad( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, const hyb_coeff* k, int blending,
                             hyb_op** out );
+/* P1ElementwiseOperator::computeAndStoreLocalElementMatrices (elementwiseoperators/P1ElementwiseOperator.hpp:138):
+ * from now on every level's element matrices are computed once (when the level is first used) and read back
+ * by every later apply instead of being recomputed; 80 bytes per micro-cell per level in FP64 (40 in FP32).
+ * Call it before capturing any graph that applies the operator. */
+int hyb_op_store_element_matrices( hyb_op* op );
 int hyb_op_destroy( hyb_op* op );
 int hyb_op_apply( hyb_op* op, hyb_fn* src, hyb_fn* dst, int level, uint32_t flag, int update );
 /* WeightedJacobiSmoothable::smooth_jac(dst, rhs, src, relax, level, flag) (solvers/Smoothables.hpp:33-40,

@@ -1038,3 +1038,176 @@ class _PerPointMap:
 
     def DF(self, X):
         return self.m.DF(X)
+
+
+# ---------------------------------------------------------------------------------------------
+# P2: quadratic Lagrange elements (4 vertex DoFs, 6 edge-midpoint DoFs)
+# ---------------------------------------------------------------------------------------------
+# Xiao-Gimbutas degree-4 rule on the tetrahedron, 11 points, given by barycentric coordinates
+# (l0, l1, l2, l3); the rule the reference's p2_div_k_grad_blending_q4 form is generated with
+# (forms/form_hyteg_generated/p2/p2_div_k_grad_blending_q4.hpp:95-105).  The weights are not
+# transcribed: xg4_weights() derives them from exactness for all polynomials of degree <= 4.
+XG4_BARY = np.array([
+    [0.17469405869723054, 0.04049050672759043, 0.01356070187980288, 0.7712547326953761],
+    [0.08140491840285922, 0.752508507009655, 0.06809937093820666, 0.09798720364927911],
+    [0.3044484024344971, 0.2402766649280726, 0.126801725915392, 0.3284732067220384],
+    [0.7412288820936226, 0.0672232948933834, 0.03518392977359872, 0.1563638932393953],
+    [0.053341239535745266, 0.419266313879513, 0.04778143555908666, 0.4796110110256551],
+    [0.4329534904813558, 0.4507658760912768, 0.05945661629943383, 0.05682401712793367],
+    [0.5380072039161857, 0.1294113737889104, 0.3301904148374645, 0.002391007457439365],
+    [0.008991260093335729, 0.1215419913339278, 0.3064939884296903, 0.5629727601430461],
+    [0.10660417256199362, 0.09720464458758327, 0.68439041545304, 0.1118007673973831],
+    [0.3292329597426468, 0.02956949520647961, 0.3179035602133946, 0.323293984837479],
+    [0.10384411641099309, 0.4327102390477686, 0.3538232392092971, 0.1096224053319412],
+])
+XG4_POINTS = XG4_BARY[:, 1:].copy()  # reference coordinates (xi1, xi2, xi3) = (l1, l2, l3)
+
+
+def xg4_weights(points=XG4_POINTS, degree=4):
+    """Weights of a cubature on the reference tetrahedron from the moment equations
+    sum_q w_q xi^a = a1! a2! a3! / (|a| + 3)! for all |a| <= degree (least squares; exact for a
+    rule of that degree)."""
+    rows, rhs = [], []
+    for a in range(degree + 1):
+        for b in range(degree + 1 - a):
+            for c in range(degree + 1 - a - b):
+                rows.append(points[:, 0] ** a * points[:, 1] ** b * points[:, 2] ** c)
+                rhs.append(math.factorial(a) * math.factorial(b) * math.factorial(c) / math.factorial(a + b + c + 3))
+    w, *_ = np.linalg.lstsq(np.array(rows), np.array(rhs), rcond=None)
+    return w
+
+
+XG4_WEIGHTS = xg4_weights()
+# element DoFs: vertices 0..3, then the edges in this order (FEniCS ordering,
+# edgedofspace/EdgeDoFIndexing.hpp getEdgeDoFDataIndicesFromMicroVerticesFEniCSOrdering)
+P2_EDGES = ((2, 3), (1, 3), (1, 2), (0, 3), (0, 2), (0, 1))
+_LGRAD = np.array([[-1.0, -1.0, -1.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 1.0]])
+
+
+def p2_ref_gradients(xi):
+    """Gradients (10, 3) of the quadratic Lagrange basis at reference point xi."""
+    lam = np.array([1.0 - xi[0] - xi[1] - xi[2], xi[0], xi[1], xi[2]])
+    G = np.zeros((10, 3))
+    for i in range(4):
+        G[i] = (4.0 * lam[i] - 1.0) * _LGRAD[i]
+    for e, (i, j) in enumerate(P2_EDGES):
+        G[4 + e] = 4.0 * (lam[i] * _LGRAD[j] + lam[j] * _LGRAD[i])
+    return G
+
+
+def p2_divkgrad_element(X, kfun, blend=None, rule=None):
+    """Element matrices (m, 10, 10) of -div(k grad u) for P2 on tets X (m, 4, 3) in computational
+    coordinates, blending map optional (same structure as p1_divkgrad_element)."""
+    pts, wts = rule if rule is not None else (XG4_POINTS, XG4_WEIGHTS)
+    J = np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], axis=2)
+    K = np.zeros((X.shape[0], 10, 10))
+    for xi, w in zip(pts, wts):
+        Xq = X[:, 0] + np.einsum("kij,j->ki", J, xi)
+        if blend is None:
+            M, Fq = J, Xq
+        else:
+            M, Fq = np.einsum("kij,kjl->kil", blend.DF(Xq), J), blend.F(Xq)
+        det = np.abs(np.linalg.det(M))
+        G = np.einsum("id,kdj->kij", p2_ref_gradients(xi), np.linalg.inv(M))
+        K += (w * kfun(Fq) * det)[:, None, None] * np.einsum("kid,kjd->kij", G, G)
+    return K
+
+
+def p2_micro_cells(lev1, c):
+    """P2 elements of level L on the nodes of Level L+1 (lev1): every level-L micro-cell of macro-cell
+    c with owner slots (k, 10) of its vertex and edge-midpoint nodes (element DoF order) and its
+    vertex coordinates (k, 4, 3).  A P2 function on level L has exactly the node set of level L+1."""
+    n = lev1.n // 2
+    slots, xyz = [], []
+    for _, offs, shift in MICRO_CELL_TYPES:
+        w = n - shift
+        if w <= 0:
+            continue
+        base = tet_points(w)
+        V = [2 * (base + np.array(o, dtype=np.int64)) for o in offs]
+        nodes = V + [(V[i] + V[j]) // 2 for i, j in P2_EDGES]
+        slots.append(np.stack([lev1.owner(c, v[:, 0], v[:, 1], v[:, 2]) for v in nodes], axis=1))
+        xyz.append(np.stack([lev1.coords(c, v[:, 0], v[:, 1], v[:, 2]) for v in V], axis=1))
+    return np.concatenate(slots), np.concatenate(xyz)
+
+
+class P2DivKGrad(P1ConstantLaplace):
+    """P2ElementwiseBlendingDivKGradOperator (elementwiseoperators/P2ElementwiseOperator.cpp:109-318,
+    typedef .hpp:475) with p2_div_k_grad_blending_q4, assembled from the 10x10 element matrices of every
+    micro-cell.  P2 level L lives on the node set of level L+1: levels[L] is Level(mesh, L+1)."""
+
+    def __init__(self, mesh, minL, maxL, kfun, blending=None):
+        self.mesh, self.minL, self.maxL = mesh, minL, maxL
+        self.maps = [IcosahedralShellMap(mesh, c) for c in range(mesh.nC)] if blending == "shell" else None
+        self.levels = {L: Level(mesh, L + 1) for L in range(minL, maxL + 1)}
+        self.A = {}
+        for L in range(minL, maxL + 1):
+            lev = self.levels[L]
+            rows, cols, vals = [], [], []
+            for c in range(mesh.nC):
+                slots, X = p2_micro_cells(lev, c)
+                K = p2_divkgrad_element(X, kfun, None if self.maps is None else _PerPointMap(self.maps[c]))
+                rows.append(np.repeat(slots, 10, axis=1).ravel())
+                cols.append(np.tile(slots, (1, 10)).ravel())
+                vals.append(K.reshape(K.shape[0], 100).ravel())
+            A = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                              shape=(lev.size, lev.size)).tocsr()
+            A.sum_duplicates()
+            self.A[L] = A
+        self.invdiag = {}
+        for L, A in self.A.items():
+            d = A.diagonal()
+            inv = np.zeros_like(d)
+            own = self.levels[L].owned
+            inv[own] = 1.0 / d[own]
+            self.invdiag[L] = inv
+
+
+def p2_basis(mu):
+    """Quadratic Lagrange basis (k, 10) at barycentric points mu (k, 4), element DoF order."""
+    out = [mu[:, i] * (2.0 * mu[:, i] - 1.0) for i in range(4)]
+    out += [4.0 * mu[:, i] * mu[:, j] for i, j in P2_EDGES]
+    return np.stack(out, axis=1)
+
+
+def p2_prolongation_matrix(lev_c1, lev_f1):
+    """Quadratic interpolation from P2 level L-1 (nodes of Level L, lev_c1) to P2 level L (nodes of
+    Level L+1, lev_f1): P2toP2QuadraticProlongation (P2toP2QuadraticProlongation.cpp:217-424).
+    Every fine node takes the coarse quadratic of a level-(L-1) micro-cell containing it; shared
+    nodes get identical rows from every containing micro-cell (continuity), kept once."""
+    nc = lev_c1.n // 2  # micro-cells per edge on coarse P2 level
+    mus = tet_points(5)  # barycentric numerators (a1, a2, a3) with a0 = 4 - a1 - a2 - a3
+    rows, cols, vals = [], [], []
+    seen = np.zeros(lev_f1.size, dtype=bool)
+    for c in range(lev_c1.mesh.nC):
+        for _, offs, shift in MICRO_CELL_TYPES:
+            w = nc - shift
+            if w <= 0:
+                continue
+            base = tet_points(w)
+            Vc = [2 * (base + np.array(o, dtype=np.int64)) for o in offs]  # coarse nodes in Level-L coords
+            cnodes = Vc + [(Vc[i] + Vc[j]) // 2 for i, j in P2_EDGES]
+            cslots = np.stack([lev_c1.owner(c, v[:, 0], v[:, 1], v[:, 2]) for v in cnodes], axis=1)
+            for a in mus:
+                a0 = 4 - a.sum()
+                mu = np.array([a0, a[0], a[1], a[2]], dtype=float) / 4.0
+                # fine node in Level-(L+1) coords: 2 * (barycentric combination of coarse vertices)
+                Pf = (a0 * 2 * Vc[0] + a[0] * 2 * Vc[1] + a[1] * 2 * Vc[2] + a[2] * 2 * Vc[3]) // 4
+                fs = lev_f1.owner(c, Pf[:, 0], Pf[:, 1], Pf[:, 2])
+                new = ~seen[fs]
+                # one row per fine owner: drop duplicates inside this batch too
+                _, first = np.unique(fs, return_index=True)
+                keep = np.zeros(len(fs), dtype=bool)
+                keep[first] = True
+                keep &= new
+                if not keep.any():
+                    continue
+                seen[fs[keep]] = True
+                N = p2_basis(mu[None])[0]
+                for j in range(10):
+                    if N[j] != 0.0:
+                        rows.append(fs[keep])
+                        cols.append(cslots[keep, j])
+                        vals.append(np.full(keep.sum(), N[j]))
+    return sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                         shape=(lev_f1.size, lev_c1.size)).tocsr()

@@ -121,3 +121,33 @@ extern "C" void ref_p1_divkgrad_blending_element( const double* coords12, int ma
    form.integrateAll( c, M );
    for ( int i = 0; i < 16; ++i ) A16[i] = M.a[i];
 }
+
+// ---------------------------------------------------------------------------------------------
+// HyTeG-generated P2 variable-coefficient diffusion form with blending
+// (src/hyteg/forms/form_hyteg_generated/p2/p2_div_k_grad_blending_q4.cpp), same test maps and
+// coefficient as the P1 form above.  Element DoFs: 4 vertices, then the edges (2,3), (1,3), (1,2),
+// (0,3), (0,2), (0,1).
+// ---------------------------------------------------------------------------------------------
+#include "hyteg/forms/form_hyteg_generated/p2/p2_div_k_grad_blending_q4.hpp"
+
+extern "C" void ref_p2_divkgrad_blending_element( const double* coords12, int map_kind, double map_a, double k_amp,
+                                                   const double* k_phase3, double* A100 )
+{
+   auto map  = std::make_shared< TestMap >();
+   map->kind = map_kind;
+   map->a    = map_a;
+   const double amp   = k_amp;
+   const double ph[3] = { k_phase3[0], k_phase3[1], k_phase3[2] };
+   auto k3 = [amp, ph]( const hyteg::Point3D& p ) {
+      const double tp = 2.0 * 3.14159265358979323846;
+      return std::exp( amp * std::sin( tp * ( p[0] + ph[0] ) ) * std::cos( tp * ( p[1] + ph[1] ) ) * std::sin( tp * ( p[2] + ph[2] ) ) );
+   };
+   auto                                   k2 = []( const hyteg::Point3D& ) { return 1.0; };
+   hyteg::forms::p2_div_k_grad_blending_q4 form( k2, k3 );  // (2D callback, 3D callback)
+   form.setGeometryMap( map );
+   std::array< hyteg::Point3D, 4 > c;
+   for ( int v = 0; v < 4; ++v ) c[v] = hyteg::Point3D( coords12[3 * v], coords12[3 * v + 1], coords12[3 * v + 2] );
+   hyteg::Matrix< double, 10, 10 > M;
+   form.integrateAll( c, M );
+   for ( int i = 0; i < 100; ++i ) A100[i] = M.a[i];
+}

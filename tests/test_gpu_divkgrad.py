@@ -102,3 +102,32 @@ def test_divkgrad_shell_vcycle_factors(ctx):
     np.testing.assert_allclose(hist[0], ref[0], rtol=1e-12)
     np.testing.assert_allclose(hist[1:] / hist[:-1], ref[1:] / ref[:-1], rtol=0, atol=1e-6)
     assert hist[-1] / hist[0] < 1e-2
+
+
+@pytest.mark.parametrize("case", ["cube", "shell"])
+@pytest.mark.parametrize("dtype,tol", [("float64", 1e-13), ("float32", 1e-6)])
+def test_divkgrad_stored_element_matrices(ctx, case, dtype, tol):
+    """computeAndStoreLocalElementMatrices: applies and smoother sweeps read the stored matrices and
+    agree with the recomputing operator (same matrices; only the mirrored lower triangle may round
+    differently)."""
+    L = 4
+    mesh = M.cube_6() if case == "cube" else O.mesh_spherical_shell(3, 2, 0.55, 1.0)
+    bl = "shell" if case == "shell" else None
+    coords, tets = mesh
+    pm = H.PrimitiveStorage.from_tets(coords, tets, ctx)
+    A = H.P1ElementwiseBlendingDivKGradOperator(pm, L, L, ctx, k=K_SPEC, blending=bl)
+    S = H.P1ElementwiseBlendingDivKGradOperator(pm, L, L, ctx, k=K_SPEC, blending=bl)
+    S.computeAndStoreLocalElementMatrices()
+    fx, fb = H.P1Function("x", pm, L, L, ctx, dtype), H.P1Function("b", pm, L, L, ctx, dtype)
+    fx.fill_random(L, 3)
+    fb.fill_random(L, 4)
+    ya, ys = H.P1Function("ya", pm, L, L, ctx, dtype), H.P1Function("ys", pm, L, L, ctx, dtype)
+    for flag in (H.Inner, H.All):
+        A.apply(fx, ya, L, flag)
+        S.apply(fx, ys, L, flag)
+        a, s = ya.download(L), ys.download(L)
+        assert np.abs(a - s).max() <= tol * np.abs(a).max()
+    A.smooth_jac(ya, fb, fx, 0.6, L, H.Inner)
+    S.smooth_jac(ys, fb, fx, 0.6, L, H.Inner)
+    a, s = ya.download(L), ys.download(L)
+    assert np.abs(a - s).max() <= tol * np.abs(a).max()

@@ -99,10 +99,20 @@ def test_serve_mixed_precision_reaches_fp64_accuracy(ctx):
     srv.close()
 
 
+def _slot_bytes(pm, L, divkgrad):
+    """The server's footprint estimate of a plain slot: ten FP64 vectors over all levels, plus the
+    stored element matrices (10 values per micro-cell slot) of a div-k-grad operator."""
+    vec = sum(pm.packed_size(l) for l in range(L + 1)) * 8 * 10
+    mats = sum(pm.counts()[3] * 6 * ((1 << l) + 2) * ((1 << l) + 1) * (1 << l) // 6 * 10 for l in range(L + 1)) * 8
+    return vec + (mats if divkgrad else 0)
+
+
 def test_serve_budget_evicts_and_rejects(ctx):
     pm = H.PrimitiveStorage.cuboid(ctx=ctx)
-    per = pm.packed_size(4) * 8 * 10 * 1.2  # about one L4 slot
-    srv = H.SolveServer(ctx, max_slots=8, hbm_budget_bytes=per * 1.5)
+    # room for the div-k-grad slot but not for it and a Laplace slot together: every switch of
+    # operator evicts the idle slot of the other kind
+    budget = _slot_bytes(pm, 4, True) + 0.5 * _slot_bytes(pm, 4, False)
+    srv = H.SolveServer(ctx, max_slots=8, hbm_budget_bytes=budget)
     ids = [srv.submit(pm, 4, kind="divkgrad" if i % 2 else "laplace", seed=i, rtol=1e-8, want_solution=True) for i in range(4)]
     srv.drain()
     for i, rid in enumerate(ids):
