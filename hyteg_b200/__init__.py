@@ -124,6 +124,9 @@ _SIGS = {
                                     C.POINTER(C.c_double)]),
     "hyb_fn_fill_random": (C.c_int, [C.c_void_p, C.c_int, C.c_uint64]),
     "hyb_op_store_element_matrices": (C.c_int, [C.c_void_p]),
+    "hyb_fn_create_p2": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "hyb_op_create_p2_divkgrad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                            C.POINTER(C.c_void_p)]),
     "hyb_fn_dot_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.POINTER(C.c_double)]),
     "hyb_serve_params_default": (C.c_int, [C.c_void_p]),
     "hyb_serve_create": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
@@ -291,6 +294,9 @@ _CALLBACK = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_void_p)
 class P1Function:
     """P1Function<ValueType> on levels min_level..max_level (device storage, HyTeG layout)."""
 
+    _lshift = 0
+    _create = "hyb_fn_create"
+
     def __init__(self, name, storage, min_level, max_level, ctx, dtype="float64"):
         self.name = name
         self.storage = storage
@@ -298,13 +304,17 @@ class P1Function:
         self.min_level, self.max_level = min_level, max_level
         self.dtype = _DTYPES[dtype] if isinstance(dtype, str) else int(dtype)
         h = C.c_void_p()
-        _check(lib().hyb_fn_create(ctx.h, storage.h, self.dtype, min_level, max_level, C.byref(h)))
+        _check(getattr(lib(), self._create)(ctx.h, storage.h, self.dtype, min_level, max_level, C.byref(h)))
         self.h = h
+
+    def packed_size(self, level):
+        """Values of the packed level vector (upload/download)."""
+        return self.storage.packed_size(level + self._lshift)
 
     # data movement -----------------------------------------------------------------------
     def upload(self, level, packed):
         a = np.ascontiguousarray(packed, dtype=np.float64)
-        if a.size != self.storage.packed_size(level):
+        if a.size != self.packed_size(level):
             raise ValueError("packed vector has the wrong size for this level")
         _check(lib().hyb_fn_upload(self.h, level, _ptr(a)))
 
@@ -313,7 +323,7 @@ class P1Function:
         _check(lib().hyb_fn_fill_random(self.h, level, seed))
 
     def download(self, level):
-        a = np.zeros(self.storage.packed_size(level), dtype=np.float64)
+        a = np.zeros(self.packed_size(level), dtype=np.float64)
         _check(lib().hyb_fn_download(self.h, level, _ptr(a)))
         return a
 
@@ -462,6 +472,48 @@ class P1ElementwiseBlendingDivKGradOperator(_ConstantOperator):
         _check(lib().hyb_op_store_element_matrices(self.h))
 
 
+class P2Function(P1Function):
+    """P2Function<ValueType>: quadratic Lagrange DoFs of level l (micro-vertices and micro-edge
+    midpoints), stored on the node set of level l+1; packed vectors use the level-(l+1) vertex layout."""
+
+    _lshift = 1
+    _create = "hyb_fn_create_p2"
+
+
+class P2ElementwiseBlendingDivKGradOperator(_ConstantOperator):
+    """-div(k grad u), elementwise P2 with the form p2_div_k_grad_blending_q4 (same k and blending
+    conventions as the P1 class)."""
+
+    def __init__(self, storage, min_level, max_level, ctx, k=None, blending=None):
+        self.storage, self.ctx = storage, ctx
+        self.min_level, self.max_level = min_level, max_level
+        c = _Coeff()
+        c.kind, c.value, c.amp, c.freq = 0, 1.0, 0.5, 1.0
+        if isinstance(k, (int, float)):
+            c.value = float(k)
+        elif k is not None:
+            c.kind = 1
+            c.amp = float(k[1])
+            for d in range(3):
+                c.phase[d] = float(k[2][d])
+            if len(k) > 3:
+                c.freq = float(k[3])
+        h = C.c_void_p()
+        _check(lib().hyb_op_create_p2_divkgrad(ctx.h, storage.h, min_level, max_level, C.byref(c),
+                                               1 if blending == "shell" else 0, C.byref(h)))
+        self.h = h
+
+    def computeAndStoreLocalElementMatrices(self):
+        _check(lib().hyb_op_store_element_matrices(self.h))
+
+
+class P2ConstantLaplaceOperator(P2ElementwiseBlendingDivKGradOperator):
+    """The P2 Laplacian (k = 1, no blending): the matrix of P2ConstantLaplaceOperator, applied elementwise."""
+
+    def __init__(self, storage, min_level, max_level, ctx):
+        super().__init__(storage, min_level, max_level, ctx)
+
+
 class P1toP1LinearRestriction:
     def restrict(self, function, sourceLevel, flag):
         _check(lib().hyb_restrict(function.h, sourceLevel, flag))
@@ -473,6 +525,10 @@ class P1toP1LinearProlongation:
 
     def prolongateAndAdd(self, function, sourceLevel, flag):
         _check(lib().hyb_prolongate(function.h, sourceLevel, flag, Add))
+
+
+P2toP2QuadraticRestriction = P1toP1LinearRestriction  # hyb_restrict dispatches on the function's space
+P2toP2QuadraticProlongation = P1toP1LinearProlongation
 
 
 def chebyshev_coefficients(order, lower, upper):

@@ -138,6 +138,14 @@ static void require_level( const Function& f, int L )
 
 static void set_device( Context& c ) { check_cuda( cudaSetDevice( c.device ), "cudaSetDevice" ); }
 
+// P2 objects keep P2 level l on the node set of storage level l+1 (lshift 1); entry points take the
+// caller's level and work on storage levels
+static int  lv( const hyb_fn* f, int level ) { return level + f->f.lshift; }
+static void same_space( const hyb_fn* a, const hyb_fn* b )
+{
+   require( a->f.lshift == b->f.lshift, "P1 and P2 functions mixed in one call" );
+}
+
 extern "C" {
 
 const char* hyb_version( void ) { return "hyteg_b200 0.1 (sm_100a)"; }
@@ -431,6 +439,17 @@ int hyb_fn_create( hyb_ctx* ctx, hyb_mesh* mesh, int dtype, int min_level, int m
    HYB_CATCH
 }
 
+int hyb_fn_create_p2( hyb_ctx* ctx, hyb_mesh* mesh, int dtype, int min_level, int max_level, hyb_fn** out )
+{
+   HYB_TRY
+   require( min_level >= 0 && min_level <= max_level && max_level <= 13, "invalid level range" );
+   // P2 level l has the node set of P1 level l+1: stored there
+   const int rc = hyb_fn_create( ctx, mesh, dtype, min_level + 1, max_level + 1, out );
+   if ( rc != HYB_OK ) return rc;
+   ( *out )->f.lshift = 1;
+   HYB_CATCH
+}
+
 int hyb_fn_destroy( hyb_fn* fn )
 {
    HYB_TRY
@@ -491,6 +510,7 @@ int hyb_fn_upload( hyb_fn* fn, int level, const double* host_packed )
 {
    HYB_TRY
    require( fn && host_packed, "NULL argument" );
+   level = lv( fn, level );
    require_level( fn->f, level );
    const P1Level&        P = fn->f.mesh->level( level );
    std::vector< double > padded( P.size, 0.0 );
@@ -505,6 +525,7 @@ int hyb_fn_download( hyb_fn* fn, int level, double* host_packed )
 {
    HYB_TRY
    require( fn && host_packed, "NULL argument" );
+   level = lv( fn, level );
    require_level( fn->f, level );
    const P1Level& P      = fn->f.mesh->level( level );
    auto           padded = from_device( fn, level );
@@ -513,13 +534,16 @@ int hyb_fn_download( hyb_fn* fn, int level, double* host_packed )
    HYB_CATCH
 }
 
+// L: the caller's level (translated to the storage level here)
 static void pointwise( hyb_fn* dst, int L, uint32_t flag, int op, int n, const double* sc, hyb_fn* const* srcs )
 {
+   L = lv( dst, L );
    require_level( dst->f, L );
    require( n >= 0 && n <= 3, "at most three source functions" );
    for ( int k = 0; k < n; ++k )
    {
       require( srcs[k] != nullptr, "source function is NULL" );
+      same_space( dst, srcs[k] );
       require( srcs[k]->f.mesh == dst->f.mesh, "functions live on different meshes" );
       require( srcs[k]->f.dtype == dst->f.dtype, "functions of different value types (use hyb_fn_copy_from)" );
       require_level( srcs[k]->f, L );
@@ -551,6 +575,7 @@ int hyb_fn_interpolate_const( hyb_fn* fn, double value, int level, uint32_t flag
 {
    HYB_TRY
    require( fn, "fn is NULL" );
+   level = lv( fn, level );
    require_level( fn->f, level );
    if ( flag == kAll )
    {
@@ -558,7 +583,7 @@ int hyb_fn_interpolate_const( hyb_fn* fn, double value, int level, uint32_t flag
       launch_flat_lincomb( &fn->ctx->c, fn->f.mesh->level( level ).size, fn->f.dtype, fn->f.ptr( level ), 0, nullptr, a );
    }
    else
-      pointwise( fn, level, flag, PT_SET, 0, &value, nullptr );
+      pointwise( fn, level - fn->f.lshift, flag, PT_SET, 0, &value, nullptr );  // pointwise takes the caller level
    HYB_CATCH
 }
 
@@ -566,6 +591,7 @@ int hyb_fn_interpolate_callback( hyb_fn* fn, double ( *f )( const double*, void*
 {
    HYB_TRY
    require( fn && f, "NULL argument" );
+   level = lv( fn, level );
    require_level( fn->f, level );
    const Topology& t      = fn->f.mesh->topo;
    const P1Level&  P      = fn->f.mesh->level( level );
@@ -648,9 +674,10 @@ int hyb_fn_invert_elementwise( hyb_fn* fn, int level, uint32_t flag )
 {
    HYB_TRY
    require( fn, "fn is NULL" );
+   level = lv( fn, level );
    hyb_fn* s[1]  = { fn };
    double  sc[1] = { 1 };
-   pointwise( fn, level, flag, PT_INVERT, 1, sc, s );
+   pointwise( fn, level - fn->f.lshift, flag, PT_INVERT, 1, sc, s );  // pointwise takes the caller level
    HYB_CATCH
 }
 
@@ -658,6 +685,8 @@ int hyb_fn_dot( hyb_fn* a, hyb_fn* b, int level, uint32_t flag, double* out )
 {
    HYB_TRY
    require( a && b && out, "NULL argument" );
+   same_space( a, b );
+   level = lv( a, level );
    require( a->f.mesh == b->f.mesh && a->f.dtype == b->f.dtype, "incompatible functions" );
    require_level( a->f, level );
    require_level( b->f, level );
@@ -674,6 +703,8 @@ int hyb_fn_dot_noalloc( hyb_fn* a, hyb_fn* b, int level, uint32_t flag, double* 
 {
    HYB_TRY
    require( a && b && out, "NULL argument" );
+   same_space( a, b );
+   level = lv( a, level );
    require( a->f.mesh == b->f.mesh && a->f.dtype == b->f.dtype, "incompatible functions" );
    require_level( a->f, level );
    require_level( b->f, level );
@@ -686,6 +717,8 @@ int hyb_fn_copy_from( hyb_fn* dst, hyb_fn* src, int level )
 {
    HYB_TRY
    require( dst && src, "NULL argument" );
+   same_space( dst, src );
+   level = lv( dst, level );
    require( dst->f.mesh == src->f.mesh, "functions live on different meshes" );
    require_level( dst->f, level );
    require_level( src->f, level );
@@ -698,6 +731,8 @@ int hyb_fn_swap( hyb_fn* a, hyb_fn* b, int level )
 {
    HYB_TRY
    require( a && b, "NULL argument" );
+   same_space( a, b );
+   level = lv( a, level );
    require( a->f.mesh == b->f.mesh && a->f.dtype == b->f.dtype, "incompatible functions" );
    require_level( a->f, level );
    require_level( b->f, level );
@@ -709,6 +744,7 @@ int hyb_fn_device_ptr( hyb_fn* fn, int level, void** ptr, int64_t* nslots )
 {
    HYB_TRY
    require( fn, "fn is NULL" );
+   level = lv( fn, level );
    require_level( fn->f, level );
    if ( ptr ) *ptr = fn->f.ptr( level );
    if ( nslots ) *nslots = fn->f.mesh->level( level ).size;
@@ -740,6 +776,19 @@ int hyb_op_create( hyb_ctx* ctx, hyb_mesh* mesh, int kind, int min_level, int ma
       throw;
    }
    *out = h;
+   HYB_CATCH
+}
+
+int hyb_op_create_p2_divkgrad( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, const hyb_coeff* k, int blending,
+                               hyb_op** out )
+{
+   HYB_TRY
+   require( min_level >= 0 && min_level <= max_level && max_level <= 13, "invalid level range" );
+   const int rc = hyb_op_create_divkgrad( ctx, mesh, min_level + 1, max_level + 1, k, blending, out );
+   if ( rc != HYB_OK ) return rc;
+   ( *out )->o.order = 2;
+   ( *out )->o.kind  = HYB_P2_ELEM_DIVKGRAD;
+   ensure_p2_constants();
    HYB_CATCH
 }
 
@@ -802,6 +851,7 @@ static void check_op_fn( hyb_op* op, hyb_fn* f, int L )
 {
    require( f != nullptr, "function is NULL" );
    require( f->f.mesh == op->o.mesh, "function and operator live on different meshes" );
+   require( f->f.lshift == op->o.order - 1, "P1 function given to a P2 operator or the other way round" );
    require_level( f->f, L );
    require( L >= op->o.minL && L <= op->o.maxL, "level outside the operator's level range" );
 }
@@ -826,6 +876,7 @@ int hyb_op_apply( hyb_op* op, hyb_fn* src, hyb_fn* dst, int level, uint32_t flag
 {
    HYB_TRY
    require( op, "op is NULL" );
+   level += op->o.order - 1;  // P2 level l is stored on storage level l+1
    check_op_fn( op, src, level );
    check_op_fn( op, dst, level );
    require( src != dst, "src and dst must differ" );
@@ -840,6 +891,7 @@ int hyb_op_smooth_jac( hyb_op* op, hyb_fn* dst, hyb_fn* rhs, hyb_fn* src, double
 {
    HYB_TRY
    require( op, "op is NULL" );
+   level += op->o.order - 1;  // P2 level l is stored on storage level l+1
    check_op_fn( op, dst, level );
    check_op_fn( op, rhs, level );
    check_op_fn( op, src, level );
@@ -854,6 +906,7 @@ int hyb_op_inverse_diagonal( hyb_op* op, hyb_fn* out, int level, uint32_t flag )
 {
    HYB_TRY
    require( op, "op is NULL" );
+   level += op->o.order - 1;  // P2 level l is stored on storage level l+1
    check_op_fn( op, out, level );
    if ( op->o.elementwise )
    {
@@ -907,10 +960,15 @@ int hyb_restrict( hyb_fn* fn, int source_level, uint32_t flag )
 {
    HYB_TRY
    require( fn, "fn is NULL" );
+   source_level = lv( fn, source_level );
    require_level( fn->f, source_level );
    require_level( fn->f, source_level - 1 );
-   launch_restrict( &fn->ctx->c, fn->f.mesh, source_level, fn->f.dtype, flag, fn->f.ptr( source_level ),
-                    fn->f.ptr( source_level - 1 ) );
+   if ( fn->f.lshift )
+      launch_p2_restrict( &fn->ctx->c, fn->f.mesh, source_level, fn->f.dtype, flag, fn->f.ptr( source_level ),
+                          fn->f.ptr( source_level - 1 ) );
+   else
+      launch_restrict( &fn->ctx->c, fn->f.mesh, source_level, fn->f.dtype, flag, fn->f.ptr( source_level ),
+                       fn->f.ptr( source_level - 1 ) );
    HYB_CATCH
 }
 
@@ -918,11 +976,16 @@ int hyb_prolongate( hyb_fn* fn, int source_level, uint32_t flag, int update )
 {
    HYB_TRY
    require( fn, "fn is NULL" );
+   source_level = lv( fn, source_level );
    require_level( fn->f, source_level );
    require_level( fn->f, source_level + 1 );
    require( update == HYB_REPLACE || update == HYB_ADD, "update must be HYB_REPLACE or HYB_ADD" );
-   launch_prolongate( &fn->ctx->c, fn->f.mesh, source_level, fn->f.dtype, flag, fn->f.ptr( source_level ),
-                      fn->f.ptr( source_level + 1 ), update == HYB_ADD );
+   if ( fn->f.lshift )
+      launch_p2_prolongate( &fn->ctx->c, fn->f.mesh, source_level, fn->f.dtype, flag, fn->f.ptr( source_level ),
+                            fn->f.ptr( source_level + 1 ), update == HYB_ADD );
+   else
+      launch_prolongate( &fn->ctx->c, fn->f.mesh, source_level, fn->f.dtype, flag, fn->f.ptr( source_level ),
+                         fn->f.ptr( source_level + 1 ), update == HYB_ADD );
    HYB_CATCH
 }
 
@@ -1226,11 +1289,13 @@ static void cycle_rec( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int L, int invoked, boo
    for ( int i = 0; i < pre; ++i ) smooth( g, x, b, L );
    // residual, restricted straight into b on level L-1 (b.assign({1},{tmp},L-1,flag) of the reference)
    stencil( op, L, dt, OP_RESID, kSolveFlag, 0, x->f.ptr( L ), b->f.ptr( L ), nullptr, g->tmp->f.ptr( L ) );
-   launch_restrict( &cx, op->o.mesh, L, dt, kSolveFlag, g->tmp->f.ptr( L ), b->f.ptr( L - 1 ) );
+   if ( op->o.order == 2 ) launch_p2_restrict( &cx, op->o.mesh, L, dt, kSolveFlag, g->tmp->f.ptr( L ), b->f.ptr( L - 1 ) );
+   else launch_restrict( &cx, op->o.mesh, L, dt, kSolveFlag, g->tmp->f.ptr( L ), b->f.ptr( L - 1 ) );
    check_cuda( cudaMemsetAsync( x->f.ptr( L - 1 ), 0, x->f.bytes( L - 1 ), cx.stream ), "x.interpolate(0)" );
    cycle_rec( g, x, b, L - 1, invoked, host_checks );
    if ( g->p.cycle == HYB_WCYCLE ) cycle_rec( g, x, b, L - 1, invoked, host_checks );
-   launch_prolongate( &cx, op->o.mesh, L - 1, dt, kSolveFlag, x->f.ptr( L - 1 ), x->f.ptr( L ), 1 );
+   if ( op->o.order == 2 ) launch_p2_prolongate( &cx, op->o.mesh, L - 1, dt, kSolveFlag, x->f.ptr( L - 1 ), x->f.ptr( L ), 1 );
+   else launch_prolongate( &cx, op->o.mesh, L - 1, dt, kSolveFlag, x->f.ptr( L - 1 ), x->f.ptr( L ), 1 );
    const int post = g->p.post_smooth + g->p.smooth_increment * ( invoked - L );
    for ( int i = 0; i < post; ++i ) smooth( g, x, b, L );
 }
@@ -1424,7 +1489,9 @@ int hyb_gmg_create( hyb_ctx* ctx, hyb_op* op, const hyb_gmg_params* params, hyb_
 {
    HYB_TRY
    require( ctx && op && params && out, "NULL argument" );
-   const hyb_gmg_params& p = *params;
+   hyb_gmg_params p = *params;
+   p.min_level += op->o.order - 1;  // P2 levels are stored one storage level up
+   p.max_level += op->o.order - 1;
    require( p.min_level >= op->o.minL && p.max_level <= op->o.maxL && p.min_level <= p.max_level,
             "multigrid levels outside the operator's level range" );
    require( p.smoother == HYB_SMOOTHER_JACOBI || p.smoother == HYB_SMOOTHER_CHEBYSHEV, "unknown smoother" );
@@ -1497,6 +1564,9 @@ static void gmg_prepare( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int level )
 int hyb_gmg_solve( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int level )
 {
    HYB_TRY
+   require( g && x && b, "NULL argument" );
+   require( x->f.lshift == g->op->o.order - 1 && b->f.lshift == x->f.lshift, "P1 and P2 objects mixed" );
+   level += g->op->o.order - 1;
    gmg_prepare( g, x, b, level );
    run_cycle( g, x, b, level );
    HYB_CATCH
@@ -1506,6 +1576,9 @@ int hyb_gmg_solve_cycles( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int level, int max_c
                           int* cycles_done )
 {
    HYB_TRY
+   require( g && x && b, "NULL argument" );
+   require( x->f.lshift == g->op->o.order - 1 && b->f.lshift == x->f.lshift, "P1 and P2 objects mixed" );
+   level += g->op->o.order - 1;
    gmg_prepare( g, x, b, level );
    require( max_cycles >= 0, "negative cycle count" );
    double r0   = residual_norm( g->op, x, b, g->tmp, level, kSolveFlag );
@@ -1531,6 +1604,7 @@ int hyb_estimate_radius( hyb_op* op, hyb_fn* x, hyb_fn* tmp, int level, int iter
 {
    HYB_TRY
    require( op && x && tmp && radius, "NULL argument" );
+   level += op->o.order - 1;
    check_op_fn( op, x, level );
    check_op_fn( op, tmp, level );
    require( iterations >= 1, "iterations must be >= 1" );
@@ -1551,6 +1625,7 @@ int hyb_cg_solve( hyb_op* op, hyb_fn* x, hyb_fn* b, int level, int max_iter, dou
 {
    HYB_TRY
    require( op && x && b, "NULL argument" );
+   level += op->o.order - 1;
    check_op_fn( op, x, level );
    check_op_fn( op, b, level );
    require( x->f.dtype == b->f.dtype, "value types differ" );
@@ -1579,6 +1654,8 @@ int hyb_cg_solve( hyb_op* op, hyb_fn* x, hyb_fn* b, int level, int max_iter, dou
 int hyb_residual_norm( hyb_op* op, hyb_fn* x, hyb_fn* b, hyb_fn* tmp, int level, uint32_t flag, double* out )
 {
    HYB_TRY
+   require( op, "op is NULL" );
+   level += op->o.order - 1;
    require( op && x && b && tmp && out, "NULL argument" );
    check_op_fn( op, x, level );
    check_op_fn( op, b, level );
@@ -1621,6 +1698,8 @@ extern "C" int hyb_mixed_solve( hyb_gmg* g, int inner_dtype, hyb_op* op, hyb_fn*
    require( x->f.dtype == F64 && b->f.dtype == F64, "x and b must hold FP64 values" );
    require( g->op == op || g->op->o.mesh == op->o.mesh, "inner solver lives on another mesh" );
    require( inner_cycles >= 1 && max_outer >= 0, "invalid iteration counts" );
+   require( op->o.order == g->op->o.order, "inner solver and operator of different orders" );
+   level += op->o.order - 1;
    check_op_fn( op, x, level );
    check_op_fn( op, b, level );
    require( level >= g->p.min_level && level <= g->p.max_level, "level outside the inner multigrid range" );
@@ -1710,6 +1789,7 @@ extern "C" int hyb_fn_fill_random( hyb_fn* fn, int level, uint64_t seed )
 {
    HYB_TRY
    require( fn, "fn is NULL" );
+   level = lv( fn, level );
    require_level( fn->f, level );
    launch_fill_uniform( &fn->ctx->c, fn->f.mesh->level( level ).size, fn->f.dtype, fn->f.ptr( level ), seed );
    sync_copies( fn, level );

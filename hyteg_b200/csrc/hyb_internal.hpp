@@ -154,6 +154,7 @@ struct Mesh {
 struct Function {
    Mesh*                mesh  = nullptr;
    int                  dtype = F64;
+   int                  lshift = 0;  // 1 for P2: user level L is stored on the nodes of storage level L+1
    int                  minL = 0, maxL = 0;
    std::vector< void* > data;  // device buffer per level (index L - minL)
    void*                ptr( int L ) const { return data.at( L - minL ); }
@@ -211,6 +212,8 @@ struct Operator {
    // elementwise operators
    bool                      elementwise = false;
    bool                      store_matrices = false;  // element matrices computed once and read back
+   // 1: P1 operator; 2: P2 operator whose level L lives on the node set of storage level L+1
+   int                       order = 1;
    int                       blending    = 0;
    Coefficient               coeff;
    CellGeom*                 d_geom = nullptr;
@@ -262,6 +265,9 @@ struct StencilArgs {
 
 void launch_stencil( Context* ctx, Mesh* m, Operator* A, int L, int dtype, const StencilArgs& a );
 void launch_elementwise( Context* ctx, Mesh* m, Operator* A, int L, int dtype, const StencilArgs& a );
+void ensure_p2_constants();
+void launch_p2_restrict( Context* ctx, Mesh* m, int Lf, int dtype, uint32_t flag, const void* fine, void* coarse );
+void launch_p2_prolongate( Context* ctx, Mesh* m, int Lc, int dtype, uint32_t flag, const void* coarse, void* fine, int add );
 void build_elementwise_operator( Operator* A );  // host tables (cell geometry, shell classification)
 void ensure_elementwise_level( Context* ctx, Operator* A, int L, int dtype );  // device buffers + diagonal
 

@@ -303,6 +303,278 @@ __global__ void __launch_bounds__( 256 ) k_elem_pass( int n, int nrows, const in
       }
 }
 
+// ---------------------------------------------------------------------------------------------
+// P2 elementwise operators (P2ElementwiseOperator::apply / computeDiagonalOperatorValues,
+// elementwiseoperators/P2ElementwiseOperator.cpp:109-318,418-567) with p2_div_k_grad_blending_q4.
+// A P2 function on level L is stored on the node set of level L+1: the level-L micro-cell with
+// vertices v0..v3 has its ten nodes at 2 v_i (vertices) and v_i + v_j (edge midpoints, edge order
+// (2,3), (1,3), (1,2), (0,3), (0,2), (0,1)) in storage coordinates.  Element integrals use the
+// degree-4, 11-point Xiao-Gimbutas rule on the tetrahedron, the rule the reference's form is
+// generated with; its weights are derived here from exactness for all polynomials of degree <= 4.
+// ---------------------------------------------------------------------------------------------
+__constant__ double c_xg4_pts[11][3];
+__constant__ double c_xg4_w[11];
+__constant__ double c_p2_rgrad[11][10][3];  // reference gradients of the ten basis functions per point
+__constant__ int    c_p2_edge[6][2] = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
+
+// barycentric coordinates (l0, l1, l2, l3) of the rule's points (kept identical to the reference's
+// generated form: the element integrals must agree); reference coordinates are (l1, l2, l3)
+static const double kXG4Bary[11][4] = {
+    { 0.17469405869723054, 0.04049050672759043, 0.01356070187980288, 0.7712547326953761 },
+    { 0.08140491840285922, 0.752508507009655, 0.06809937093820666, 0.09798720364927911 },
+    { 0.3044484024344971, 0.2402766649280726, 0.126801725915392, 0.3284732067220384 },
+    { 0.7412288820936226, 0.0672232948933834, 0.03518392977359872, 0.1563638932393953 },
+    { 0.053341239535745266, 0.419266313879513, 0.04778143555908666, 0.4796110110256551 },
+    { 0.4329534904813558, 0.4507658760912768, 0.05945661629943383, 0.05682401712793367 },
+    { 0.5380072039161857, 0.1294113737889104, 0.3301904148374645, 0.002391007457439365 },
+    { 0.008991260093335729, 0.1215419913339278, 0.3064939884296903, 0.5629727601430461 },
+    { 0.10660417256199362, 0.09720464458758327, 0.68439041545304, 0.1118007673973831 },
+    { 0.3292329597426468, 0.02956949520647961, 0.3179035602133946, 0.323293984837479 },
+    { 0.10384411641099309, 0.4327102390477686, 0.3538232392092971, 0.1096224053319412 } };
+
+// weights w solving sum_q w_q xi_q^a = a1! a2! a3! / (|a|+3)! for all |a| <= 4 in the least-squares
+// sense (Householder QR of the 35 x 11 moment matrix; exact for a degree-4 rule)
+static void xg4_weights( double w[11] )
+{
+   const int           m = 35, n = 11;
+   std::vector< double > A( m * n ), b( m );
+   auto fact = []( int k ) {
+      double f = 1;
+      for ( int i = 2; i <= k; ++i ) f *= i;
+      return f;
+   };
+   int row = 0;
+   for ( int a = 0; a <= 4; ++a )
+      for ( int bb = 0; bb <= 4 - a; ++bb )
+         for ( int c = 0; c <= 4 - a - bb; ++c, ++row )
+         {
+            for ( int q = 0; q < n; ++q )
+               A[row * n + q] = std::pow( kXG4Bary[q][1], a ) * std::pow( kXG4Bary[q][2], bb ) * std::pow( kXG4Bary[q][3], c );
+            b[row] = fact( a ) * fact( bb ) * fact( c ) / fact( a + bb + c + 3 );
+         }
+   for ( int k = 0; k < n; ++k )
+   {
+      double nrm = 0;
+      for ( int i = k; i < m; ++i ) nrm += A[i * n + k] * A[i * n + k];
+      nrm = std::sqrt( nrm );
+      const double alpha = A[k * n + k] > 0 ? -nrm : nrm;
+      std::vector< double > v( m, 0.0 );
+      for ( int i = k; i < m; ++i ) v[i] = A[i * n + k];
+      v[k] -= alpha;
+      double vv = 0;
+      for ( int i = k; i < m; ++i ) vv += v[i] * v[i];
+      if ( vv == 0 ) continue;
+      for ( int j = k; j < n; ++j )
+      {
+         double d = 0;
+         for ( int i = k; i < m; ++i ) d += v[i] * A[i * n + j];
+         for ( int i = k; i < m; ++i ) A[i * n + j] -= 2 * d / vv * v[i];
+      }
+      double d = 0;
+      for ( int i = k; i < m; ++i ) d += v[i] * b[i];
+      for ( int i = k; i < m; ++i ) b[i] -= 2 * d / vv * v[i];
+   }
+   for ( int k = n - 1; k >= 0; --k )
+   {
+      double s = b[k];
+      for ( int j = k + 1; j < n; ++j ) s -= A[k * n + j] * w[j];
+      w[k] = s / A[k * n + k];
+   }
+}
+
+void ensure_p2_constants()
+{
+   static bool done = false;
+   if ( done ) return;
+   double pts[11][3], w[11], g[11][10][3];
+   xg4_weights( w );
+   const double lg[4][3] = { { -1, -1, -1 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } };
+   const int    ed[6][2] = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
+   for ( int q = 0; q < 11; ++q )
+   {
+      for ( int d = 0; d < 3; ++d ) pts[q][d] = kXG4Bary[q][d + 1];
+      const double lam[4] = { 1.0 - pts[q][0] - pts[q][1] - pts[q][2], pts[q][0], pts[q][1], pts[q][2] };
+      for ( int i = 0; i < 4; ++i )
+         for ( int d = 0; d < 3; ++d ) g[q][i][d] = ( 4.0 * lam[i] - 1.0 ) * lg[i][d];
+      for ( int e = 0; e < 6; ++e )
+         for ( int d = 0; d < 3; ++d )
+            g[q][4 + e][d] = 4.0 * ( lam[ed[e][0]] * lg[ed[e][1]][d] + lam[ed[e][1]] * lg[ed[e][0]][d] );
+   }
+   check_cuda( cudaMemcpyToSymbol( c_xg4_pts, pts, sizeof( pts ) ), "P2 constants (points)" );
+   check_cuda( cudaMemcpyToSymbol( c_xg4_w, w, sizeof( w ) ), "P2 constants (weights)" );
+   check_cuda( cudaMemcpyToSymbol( c_p2_rgrad, g, sizeof( g ) ), "P2 constants (gradients)" );
+   done = true;
+}
+
+// mapped quantities of quadrature point q of a micro-cell: Mi = (DF J)^-1 and s = w k |det(DF J)|
+template < typename A >
+__device__ __forceinline__ void p2_point( const CellGeom& g, const Coefficient& kc, const A X0[3], const A J[3][3], int q, A Mi[3][3],
+                                          A& s )
+{
+   A Xq[3];
+   for ( int r = 0; r < 3; ++r )
+      Xq[r] = X0[r] + J[r][0] * A( c_xg4_pts[q][0] ) + J[r][1] * A( c_xg4_pts[q][1] ) + J[r][2] * A( c_xg4_pts[q][2] );
+   A M[3][3], Fq[3];
+   if ( g.blend == 1 )
+   {
+      A DF[3][3];
+      shell_map( g, Xq, Fq, DF );
+      for ( int r = 0; r < 3; ++r )
+         for ( int c = 0; c < 3; ++c ) M[r][c] = DF[r][0] * J[0][c] + DF[r][1] * J[1][c] + DF[r][2] * J[2][c];
+   }
+   else
+      for ( int r = 0; r < 3; ++r )
+      {
+         Fq[r] = Xq[r];
+         for ( int c = 0; c < 3; ++c ) M[r][c] = J[r][c];
+      }
+   const A c00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
+   const A c01 = M[1][2] * M[2][0] - M[1][0] * M[2][2];
+   const A c02 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
+   const A det = M[0][0] * c00 + M[0][1] * c01 + M[0][2] * c02;
+   const A id  = A( 1 ) / det;
+   Mi[0][0]    = c00 * id;
+   Mi[1][0]    = c01 * id;
+   Mi[2][0]    = c02 * id;
+   Mi[0][1]    = ( M[0][2] * M[2][1] - M[0][1] * M[2][2] ) * id;
+   Mi[1][1]    = ( M[0][0] * M[2][2] - M[0][2] * M[2][0] ) * id;
+   Mi[2][1]    = ( M[0][1] * M[2][0] - M[0][0] * M[2][1] ) * id;
+   Mi[0][2]    = ( M[0][1] * M[1][2] - M[0][2] * M[1][1] ) * id;
+   Mi[1][2]    = ( M[0][2] * M[1][0] - M[0][0] * M[1][2] ) * id;
+   Mi[2][2]    = ( M[0][0] * M[1][1] - M[0][1] * M[1][0] ) * id;
+   s           = A( c_xg4_w[q] ) * coeff_eval( kc, Fq ) * fabs( det );
+}
+
+// physical gradient of basis function i at point q: row (reference gradient) times Mi
+template < typename A >
+__device__ __forceinline__ void p2_grad( int q, int i, const A Mi[3][3], A G[3] )
+{
+   for ( int d = 0; d < 3; ++d )
+      G[d] = A( c_p2_rgrad[q][i][0] ) * Mi[0][d] + A( c_p2_rgrad[q][i][1] ) * Mi[1][d] + A( c_p2_rgrad[q][i][2] ) * Mi[2][d];
+}
+
+// One parity pass over the level-L micro-cells (anchors of parity (px, py, pz); ne = 2^L), nodes
+// on storage level L+1.  MODE 0: y += K x computed matrix-free (per point the gradient of the local
+// solution, then its pairing with every basis gradient); 1: diagonal of K; 2: store the 55 upper-
+// triangle entries of K; 3: y += K x from the stored entries.  Stored entry v of micro-cell (cell c,
+// type ty, anchor a) sits at kst[v * kstride + (c * 6 + ty) * tet(ne) + cidx(ne - 1, a)].
+template < typename T, typename A, int MODE >
+__global__ void __launch_bounds__( 256 ) k_p2_pass( int ne, int nrows, const int2* __restrict__ rows, const int64_t* __restrict__ cell_off,
+                                                     const CellGeom* __restrict__ geom, Coefficient kc, int px,
+                                                     const T* __restrict__ src, A* __restrict__ acc, A* __restrict__ kst,
+                                                     int64_t kstride, int64_t level_size, int* err )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int r    = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   if ( r >= nrows ) return;
+   const int2     yz = rows[r];
+   const int      y = yz.x, z = yz.y, ns = 2 * ne;
+   const CellGeom g    = geom[c];
+   const int64_t  base = cell_off[c];
+   const A        inv_n = A( 1.0 / double( ne ) );
+   A              st[3][3];
+   for ( int k = 0; k < 3; ++k )
+      for ( int d = 0; d < 3; ++d ) st[k][d] = ( A( g.P[k + 1][d] ) - A( g.P[0][d] ) ) * inv_n;
+   for ( int x = px + 2 * lane; x + y + z <= ne - 1; x += 64 )
+      for ( int ty = 0; ty < 6; ++ty )
+      {
+         if ( x + y + z > ne - 1 - c_mc_shift[ty] ) continue;
+         int V[4][3];
+         for ( int m = 0; m < 4; ++m )
+         {
+            V[m][0] = x + c_mc_off[ty][m][0];
+            V[m][1] = y + c_mc_off[ty][m][1];
+            V[m][2] = z + c_mc_off[ty][m][2];
+         }
+         int64_t idx[10];
+         for ( int m = 0; m < 4; ++m ) idx[m] = base + cidx( ns, 2 * V[m][0], 2 * V[m][1], 2 * V[m][2] );
+         for ( int e = 0; e < 6; ++e )
+         {
+            const int a = c_p2_edge[e][0], b = c_p2_edge[e][1];
+            idx[4 + e]  = base + cidx( ns, V[a][0] + V[b][0], V[a][1] + V[b][1], V[a][2] + V[b][2] );
+         }
+         const int64_t slot = ( int64_t( c ) * 6 + ty ) * tet_size( ne ) + cidx( ne - 1, x, y, z );
+         {
+            // self-check: nodes inside the level's vector, stored slot inside its array
+            bool bad = ( MODE >= 2 ) && ( slot < 0 || slot >= kstride );
+            for ( int m = 0; m < 10; ++m ) bad |= idx[m] < 0 || idx[m] >= level_size;
+            if ( bad )
+            {
+               atomicExch( err, 2 );
+               continue;
+            }
+         }
+         A xl[10], yl[10];
+         if constexpr ( MODE == 0 || MODE == 3 )
+            for ( int m = 0; m < 10; ++m ) xl[m] = A( ld_any( src + idx[m] ) );
+         for ( int m = 0; m < 10; ++m ) yl[m] = A( 0 );
+         if constexpr ( MODE == 3 )
+         {
+            int v = 0;
+            for ( int i = 0; i < 10; ++i )
+               for ( int j = i; j < 10; ++j, ++v )
+               {
+                  const A k = kst[v * kstride + slot];
+                  yl[i] += k * xl[j];
+                  if ( j != i ) yl[j] += k * xl[i];
+               }
+         }
+         else
+         {
+            A X0[3], J[3][3];
+            for ( int d = 0; d < 3; ++d )
+            {
+               X0[d] = A( g.P[0][d] ) + st[0][d] * A( V[0][0] ) + st[1][d] * A( V[0][1] ) + st[2][d] * A( V[0][2] );
+               for ( int k = 0; k < 3; ++k )
+                  J[d][k] = st[0][d] * A( V[k + 1][0] - V[0][0] ) + st[1][d] * A( V[k + 1][1] - V[0][1] ) +
+                            st[2][d] * A( V[k + 1][2] - V[0][2] );
+            }
+            A K[MODE == 2 ? 55 : 1];
+            if constexpr ( MODE == 2 )
+               for ( int v = 0; v < 55; ++v ) K[v] = A( 0 );
+#pragma unroll 1
+            for ( int q = 0; q < 11; ++q )
+            {
+               A Mi[3][3], s;
+               p2_point( g, kc, X0, J, q, Mi, s );
+               if constexpr ( MODE == 0 )
+               {
+                  A gs[3] = { A( 0 ), A( 0 ), A( 0 ) };
+                  for ( int j = 0; j < 10; ++j )
+                     for ( int d = 0; d < 3; ++d ) gs[d] += xl[j] * A( c_p2_rgrad[q][j][d] );
+                  A gp[3], h[3];
+                  for ( int d = 0; d < 3; ++d ) gp[d] = gs[0] * Mi[0][d] + gs[1] * Mi[1][d] + gs[2] * Mi[2][d];
+                  for ( int r2 = 0; r2 < 3; ++r2 ) h[r2] = s * ( Mi[r2][0] * gp[0] + Mi[r2][1] * gp[1] + Mi[r2][2] * gp[2] );
+                  for ( int i = 0; i < 10; ++i )
+                     yl[i] += A( c_p2_rgrad[q][i][0] ) * h[0] + A( c_p2_rgrad[q][i][1] ) * h[1] + A( c_p2_rgrad[q][i][2] ) * h[2];
+               }
+               else if constexpr ( MODE == 1 )
+                  for ( int i = 0; i < 10; ++i )
+                  {
+                     A G[3];
+                     p2_grad( q, i, Mi, G );
+                     yl[i] += s * ( G[0] * G[0] + G[1] * G[1] + G[2] * G[2] );
+                  }
+               else
+               {
+                  A G[10][3];
+                  for ( int i = 0; i < 10; ++i ) p2_grad( q, i, Mi, G[i] );
+                  int v = 0;
+                  for ( int i = 0; i < 10; ++i )
+                     for ( int j = i; j < 10; ++j, ++v ) K[v] += s * ( G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2] );
+               }
+            }
+            if constexpr ( MODE == 2 )
+            {
+               for ( int v = 0; v < 55; ++v ) kst[v * kstride + slot] = K[v];
+               continue;
+            }
+         }
+         for ( int i = 0; i < 10; ++i ) acc[idx[i]] += yl[i];
+      }
+}
+
 // Combine: cell interior points take s = acc, face/edge/vertex owners the sum of their copies in
 // the neighbouring cells; then the operation's epilogue (the constant-stencil kernels' semantics).
 template < typename T, typename A, int OP >
@@ -445,11 +717,16 @@ static A* acc_buffer( Operator* op, int L, int64_t size )
    return reinterpret_cast< A* >( e.d_acc );
 }
 
+// micro-cells per macro-edge of the elements living on storage level L (P2 elements of level L-1
+// have their nodes on storage level L)
+static int element_n( const Operator* op, int L ) { return op->order == 2 ? ( 1 << ( L - 1 ) ) : ( 1 << L ); }
+static int element_values( const Operator* op ) { return op->order == 2 ? 55 : 10; }
+
 static void ensure_rows( Operator* op, int L )
 {
    ElemLevel& e = op->el[L];
    if ( e.d_hrows ) return;
-   const int                  n = 1 << L;
+   const int                  n = element_n( op, L );
    std::vector< int2 >        rows;
    for ( int p = 0; p < 4; ++p )
    {
@@ -465,7 +742,7 @@ static void ensure_rows( Operator* op, int L )
 }
 
 // entries per stored value: every (cell, micro-cell type, anchor) slot of the level
-static int64_t kstride( Mesh* m, int L ) { return int64_t( m->topo.nC ) * 6 * tet_size( int64_t( 1 ) << L ); }
+static int64_t kstride( Mesh* m, const Operator* op, int L ) { return int64_t( m->topo.nC ) * 6 * tet_size( int64_t( element_n( op, L ) ) ); }
 
 template < typename A >
 static A* stored_matrices( Operator* op, int L ) { return reinterpret_cast< A* >( op->el[L].d_K[sizeof( A ) == 8 ? 0 : 1] ); }
@@ -477,7 +754,7 @@ static void run_passes( Context* ctx, Mesh* m, Operator* op, int L, const T* src
    ElemLevel& e = op->el[L];
    if ( MODE != 2 ) check_cuda( cudaMemsetAsync( acc, 0, P.size * sizeof( A ), ctx->stream ), "cudaMemset(acc)" );
    A*            kst = stored_matrices< A >( op, L );
-   const int64_t ks  = kstride( m, L );
+   const int64_t ks  = kstride( m, op, L );
    const int nC = m->topo.nC;
    for ( int p = 0; p < 8; ++p )
    {
@@ -485,8 +762,13 @@ static void run_passes( Context* ctx, Mesh* m, Operator* op, int L, const T* src
       const int nr = e.hoff[q + 1] - e.hoff[q];
       if ( nr <= 0 ) continue;
       dim3 grid( ( nr + 7 ) / 8, nC );
-      k_elem_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( P.n, nr, e.d_hrows + e.hoff[q], P.d_off + P.nB, op->d_geom,
-                                                                   op->coeff, px, src, acc, kst, ks, P.size, ctx->d_error );
+      if ( op->order == 2 )
+         k_p2_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( element_n( op, L ), nr, e.d_hrows + e.hoff[q], P.d_off + P.nB,
+                                                                    op->d_geom, op->coeff, px, src, acc, kst, ks, P.size,
+                                                                    ctx->d_error );
+      else
+         k_elem_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( P.n, nr, e.d_hrows + e.hoff[q], P.d_off + P.nB, op->d_geom,
+                                                                      op->coeff, px, src, acc, kst, ks, P.size, ctx->d_error );
       ++ctx->launches;
    }
    check_cuda( cudaGetLastError(), "elementwise pass launch" );
@@ -510,7 +792,8 @@ static void ensure_level_t( Context* ctx, Operator* op, int L, int dtype )
    void*&     K   = e.d_K[sizeof( A ) == 8 ? 0 : 1];
    if ( op->store_matrices && !K )
    {
-      check_cuda( cudaMalloc( &K, size_t( 10 ) * size_t( kstride( m, L ) ) * sizeof( A ) ), "cudaMalloc(element matrices)" );
+      check_cuda( cudaMalloc( &K, size_t( element_values( op ) ) * size_t( kstride( m, op, L ) ) * sizeof( A ) ),
+                  "cudaMalloc(element matrices)" );
       run_passes< T, A, 2 >( ctx, m, op, L, nullptr, acc );
    }
    if ( e.d_invd[dtype] ) return;

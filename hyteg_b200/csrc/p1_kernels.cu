@@ -1509,10 +1509,299 @@ void launch_prolongate( Context* ctx, Mesh* m, int Lc, int dtype, uint32_t flag,
    else run_prolong< __half, float >( ctx, cv, fv, nC, flag, coarse, fine, add );
 }
 
+// ---------------------------------------------------------------------------------------------
+// P2 quadratic transfers (P2toP2QuadraticProlongation::prolongateAdditively3D,
+// P2toP2QuadraticProlongation.cpp:217-424; P2toP2QuadraticRestriction::restrictAdditively3D,
+// P2toP2QuadraticRestriction.cpp:131-286), on the P2 storage: P2 level l lives on storage level l+1.
+// A fine node F (storage level Lc+1) lies in the coarse micro-cell of anchor A = F / 4 (and offset
+// pattern F mod 4) and takes the coarse quadratic there: sum_k w_k u(2A + o_k) over the nodes with
+// non-zero basis value (at most ten; on a macro-cell face only the nodes of that face, so every
+// referenced coarse node lies in the same macro-cell).  Restriction is the transpose: the coarse
+// node J pulls w r(2J + d) over its stencil (per parity class of J), each fine value divided by the
+// number of macro-cells sharing its primitive, and owners of face/edge/vertex nodes sum over their
+// macro-cells (the reference's scaling plus additive communication).
+// ---------------------------------------------------------------------------------------------
+constexpr int kP2RMax = 320;
+__constant__ int         c_p2p_n[64];
+__constant__ signed char c_p2p_o[64][10][3];
+__constant__ double      c_p2p_w[64][10];
+__constant__ int         c_p2r_begin[9];
+__constant__ signed char c_p2r_d[kP2RMax][3];
+__constant__ double      c_p2r_w[kP2RMax];
+
+static void ensure_p2_transfer_tables()
+{
+   static bool done = false;
+   if ( done ) return;
+   // micro-cell types (vertex offsets), the same table as the refinement itself
+   static const int mc[6][4][3] = { { { 0, 0, 0 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } }, { { 1, 0, 0 }, { 1, 1, 0 }, { 0, 1, 0 }, { 1, 0, 1 } },
+                                    { { 1, 0, 0 }, { 0, 1, 0 }, { 1, 0, 1 }, { 0, 0, 1 } }, { { 1, 1, 0 }, { 1, 1, 1 }, { 0, 1, 1 }, { 1, 0, 1 } },
+                                    { { 1, 0, 1 }, { 0, 1, 1 }, { 0, 0, 1 }, { 0, 1, 0 } }, { { 0, 1, 0 }, { 1, 1, 0 }, { 1, 0, 1 }, { 0, 1, 1 } } };
+   static const int ed[6][2] = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
+   int              pn[64];
+   signed char      po[64][10][3] = {};
+   double           pw[64][10]    = {};
+   for ( int pat = 0; pat < 64; ++pat )
+   {
+      const int r[3] = { pat & 3, ( pat >> 2 ) & 3, pat >> 4 };
+      const int F[3] = { 4 + r[0], 4 + r[1], 4 + r[2] }, A[3] = { 1, 1, 1 };
+      bool      found = false;
+      for ( int e = 0; e < 8 && !found; ++e )
+      {
+         const int a[3] = { A[0] - ( e & 1 ), A[1] - ( ( e >> 1 ) & 1 ), A[2] - ( e >> 2 ) };
+         for ( int ty = 0; ty < 6 && !found; ++ty )
+         {
+            // barycentric coordinates x4 from the unimodular offset matrix (integer inverse)
+            int E[3][3];
+            for ( int i = 0; i < 3; ++i )
+               for ( int k = 0; k < 3; ++k ) E[i][k] = mc[ty][k + 1][i] - mc[ty][0][i];
+            const int det = E[0][0] * ( E[1][1] * E[2][2] - E[1][2] * E[2][1] ) - E[0][1] * ( E[1][0] * E[2][2] - E[1][2] * E[2][0] ) +
+                            E[0][2] * ( E[1][0] * E[2][1] - E[1][1] * E[2][0] );
+            const int inv[3][3] = { { ( E[1][1] * E[2][2] - E[1][2] * E[2][1] ) * det, ( E[0][2] * E[2][1] - E[0][1] * E[2][2] ) * det,
+                                      ( E[0][1] * E[1][2] - E[0][2] * E[1][1] ) * det },
+                                    { ( E[1][2] * E[2][0] - E[1][0] * E[2][2] ) * det, ( E[0][0] * E[2][2] - E[0][2] * E[2][0] ) * det,
+                                      ( E[0][2] * E[1][0] - E[0][0] * E[1][2] ) * det },
+                                    { ( E[1][0] * E[2][1] - E[1][1] * E[2][0] ) * det, ( E[0][1] * E[2][0] - E[0][0] * E[2][1] ) * det,
+                                      ( E[0][0] * E[1][1] - E[0][1] * E[1][0] ) * det } };  // det = +-1
+            int rel[3];
+            for ( int i = 0; i < 3; ++i ) rel[i] = F[i] - 4 * ( a[i] + mc[ty][0][i] );
+            int mu4[4] = { 4, 0, 0, 0 };
+            for ( int k = 0; k < 3; ++k )
+            {
+               mu4[k + 1] = inv[k][0] * rel[0] + inv[k][1] * rel[1] + inv[k][2] * rel[2];
+               mu4[0] -= mu4[k + 1];
+            }
+            bool inside = true;
+            for ( int k = 0; k < 4; ++k ) inside &= mu4[k] >= 0 && mu4[k] <= 4;
+            if ( !inside ) continue;
+            found = true;
+            double mu[4], N[10];
+            int    node[10][3];
+            for ( int k = 0; k < 4; ++k ) mu[k] = mu4[k] / 4.0;
+            for ( int k = 0; k < 4; ++k )
+            {
+               N[k] = mu[k] * ( 2.0 * mu[k] - 1.0 );
+               for ( int i = 0; i < 3; ++i ) node[k][i] = 2 * ( a[i] + mc[ty][k][i] );
+            }
+            for ( int k = 0; k < 6; ++k )
+            {
+               N[4 + k] = 4.0 * mu[ed[k][0]] * mu[ed[k][1]];
+               for ( int i = 0; i < 3; ++i ) node[4 + k][i] = ( node[ed[k][0]][i] + node[ed[k][1]][i] ) / 2;
+            }
+            pn[pat] = 0;
+            for ( int k = 0; k < 10; ++k )
+               if ( N[k] != 0.0 )
+               {
+                  for ( int i = 0; i < 3; ++i ) po[pat][pn[pat]][i] = static_cast< signed char >( node[k][i] - 2 * A[i] );
+                  pw[pat][pn[pat]++] = N[k];
+               }
+         }
+      }
+      if ( !found ) throw std::logic_error( "P2 transfer table: no micro-cell contains a fine node" );
+   }
+   // restriction stencils: class p = J mod 2, entries (d = r - 2 o, w)
+   int         begin[9] = {};
+   signed char rd[kP2RMax][3];
+   double      rw[kP2RMax];
+   int         cnt = 0;
+   for ( int p = 0; p < 8; ++p )
+   {
+      begin[p] = cnt;
+      for ( int pat = 0; pat < 64; ++pat )
+         for ( int k = 0; k < pn[pat]; ++k )
+         {
+            const int o[3] = { po[pat][k][0], po[pat][k][1], po[pat][k][2] };
+            if ( ( ( o[0] & 1 ) | ( ( o[1] & 1 ) << 1 ) | ( ( o[2] & 1 ) << 2 ) ) != p ) continue;
+            if ( cnt >= kP2RMax ) throw std::logic_error( "P2 restriction stencil table overflow" );
+            const int r[3] = { pat & 3, ( pat >> 2 ) & 3, pat >> 4 };
+            for ( int i = 0; i < 3; ++i ) rd[cnt][i] = static_cast< signed char >( r[i] - 2 * o[i] );
+            rw[cnt++] = pw[pat][k];
+         }
+   }
+   begin[8] = cnt;
+   check_cuda( cudaMemcpyToSymbol( c_p2p_n, pn, sizeof( pn ) ), "P2 transfer tables" );
+   check_cuda( cudaMemcpyToSymbol( c_p2p_o, po, sizeof( po ) ), "P2 transfer tables" );
+   check_cuda( cudaMemcpyToSymbol( c_p2p_w, pw, sizeof( pw ) ), "P2 transfer tables" );
+   check_cuda( cudaMemcpyToSymbol( c_p2r_begin, begin, sizeof( begin ) ), "P2 transfer tables" );
+   check_cuda( cudaMemcpyToSymbol( c_p2r_d, rd, sizeof( rd ) ), "P2 transfer tables" );
+   check_cuda( cudaMemcpyToSymbol( c_p2r_w, rw, sizeof( rw ) ), "P2 transfer tables" );
+   done = true;
+}
+
+// coarse quadratic at fine cell-local node (x, y, z); nc = coarse storage micro-edges per edge
+template < typename T, typename A >
+__device__ __forceinline__ A p2_interp( const T* c, int nc, int x, int y, int z )
+{
+   const int ax = x >> 2, ay = y >> 2, az = z >> 2;
+   const int pat = ( x & 3 ) | ( ( y & 3 ) << 2 ) | ( ( z & 3 ) << 4 );
+   A         v   = A( 0 );
+   for ( int k = 0; k < c_p2p_n[pat]; ++k )
+      v += A( c_p2p_w[pat][k] ) *
+           A( ldv( c + cidx( nc, 2 * ax + c_p2p_o[pat][k][0], 2 * ay + c_p2p_o[pat][k][1], 2 * az + c_p2p_o[pat][k][2] ) ) );
+   return v;
+}
+
+template < typename T, typename A >
+__global__ void __launch_bounds__( 256 ) k_p2_prolong_cells( LevelView cv, LevelView fv, uint32_t flag, const T* __restrict__ coarse,
+                                                              T* fine, int add )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int r    = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   if ( r >= fv.nrows ) return;
+   if ( !( fv.cell_bc[c] & flag ) ) return;
+   const int2    yz   = fv.rows[r];
+   const int     y = yz.x, z = yz.y;
+   const T*      cc   = coarse + cv.cell_off[c];
+   const int64_t fb   = fv.cell_off[c] + cidx( fv.n, 0, y, z );
+   const int     xmax = fv.n - 1 - y - z;
+   for ( int x = 1 + lane; x <= xmax; x += 32 )
+   {
+      const A val = p2_interp< T, A >( cc, cv.n, x, y, z );
+      stv( fine + fb + x, add ? A( ldc( fine + fb + x ) ) + val : val );
+   }
+}
+
+template < typename T, typename A >
+__global__ void __launch_bounds__( 256 ) k_p2_prolong_bnd( LevelView cv, LevelView fv, uint32_t flag, const T* __restrict__ coarse,
+                                                            T* fine, int add )
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( t >= fv.ntasks ) return;
+   const int4 tk = fv.tasks[t];
+   const int  b = tk.x, i = tk.y, j = tk.z;
+   if ( !( fv.bc[b] & flag ) ) return;
+   const Incidence I = fv.inc[fv.inc_begin[b]];
+   int             x, y, z;
+   inc_point( I, fv.n, i, j, x, y, z );
+   const A       val   = p2_interp< T, A >( coarse + cv.cell_off[I.cell], cv.n, x, y, z );
+   const int64_t owner = owner_slot( fv, b, i, j );
+   write_through( fv, fine, b, i, j, owner, add ? A( ldc( fine + owner ) ) + val : val );
+}
+
+// one macro-cell's share of the restriction at coarse cell-local node (x, y, z)
+template < typename T, typename A >
+__device__ __forceinline__ A p2_restrict_share( const T* f, const float* ncc, int nf, int x, int y, int z )
+{
+   const int p = ( x & 1 ) | ( ( y & 1 ) << 1 ) | ( ( z & 1 ) << 2 );
+   A         s = A( 0 );
+   for ( int k = c_p2r_begin[p]; k < c_p2r_begin[p + 1]; ++k )
+   {
+      const int X = 2 * x + c_p2r_d[k][0], Y = 2 * y + c_p2r_d[k][1], Z = 2 * z + c_p2r_d[k][2];
+      if ( X < 0 || Y < 0 || Z < 0 || X + Y + Z > nf ) continue;
+      s += A( c_p2r_w[k] ) / A( ncc[point_class( nf, X, Y, Z )] ) * A( ldv( f + cidx( nf, X, Y, Z ) ) );
+   }
+   return s;
+}
+
+template < typename T, typename A >
+__global__ void __launch_bounds__( 256 ) k_p2_restrict_cells( LevelView cv, LevelView fv, uint32_t flag, const T* __restrict__ fine,
+                                                               T* coarse )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int r    = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   if ( r >= cv.nrows ) return;
+   if ( !( cv.cell_bc[c] & flag ) ) return;
+   const int2    yz   = cv.rows[r];
+   const int     y = yz.x, z = yz.y;
+   const T*      f    = fine + fv.cell_off[c];
+   const float*  ncc  = fv.ncell_cls + size_t( c ) * kNumClasses;
+   const int64_t cb   = cv.cell_off[c] + cidx( cv.n, 0, y, z );
+   const int     xmax = cv.n - 1 - y - z;
+   for ( int x = 1 + lane; x <= xmax; x += 32 ) stv( coarse + cb + x, p2_restrict_share< T, A >( f, ncc, fv.n, x, y, z ) );
+}
+
+template < typename T, typename A >
+__global__ void __launch_bounds__( 256 ) k_p2_restrict_bnd( LevelView cv, LevelView fv, uint32_t flag, const T* __restrict__ fine,
+                                                             T* coarse )
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( t >= cv.ntasks ) return;
+   const int4 tk = cv.tasks[t];
+   const int  b = tk.x, i = tk.y, j = tk.z;
+   if ( !( cv.bc[b] & flag ) ) return;
+   A acc = A( 0 );
+   for ( int q = cv.inc_begin[b]; q < cv.inc_begin[b + 1]; ++q )
+   {
+      const Incidence I = cv.inc[q];
+      int             x, y, z;
+      inc_point( I, cv.n, i, j, x, y, z );
+      acc += p2_restrict_share< T, A >( fine + fv.cell_off[I.cell], fv.ncell_cls + size_t( I.cell ) * kNumClasses, fv.n, x, y, z );
+   }
+   write_through( cv, coarse, b, i, j, owner_slot( cv, b, i, j ), acc );
+}
+
+template < typename T, typename A >
+static void run_p2_restrict( Context* ctx, const LevelView& cv, const LevelView& fv, int nC, uint32_t flag, const void* fine,
+                             void* coarse )
+{
+   Fork fk( ctx );
+   if ( cv.nrows > 0 && nC > 0 )
+   {
+      dim3 grid( ( cv.nrows + 7 ) / 8, nC );
+      k_p2_restrict_cells< T, A ><<< grid, 256, 0, ctx->stream >>>( cv, fv, flag, (const T*) fine, (T*) coarse );
+      ++ctx->launches;
+   }
+   if ( cv.ntasks > 0 )
+   {
+      k_p2_restrict_bnd< T, A ><<< ( cv.ntasks + 255 ) / 256, 256, 0, fk.aux() >>>( cv, fv, flag, (const T*) fine, (T*) coarse );
+      ++ctx->launches;
+   }
+   check_cuda( cudaGetLastError(), "P2 restrict launch" );
+}
+
+// Lf: fine STORAGE level (P2 level Lf-1 restricted to P2 level Lf-2)
+void launch_p2_restrict( Context* ctx, Mesh* m, int Lf, int dtype, uint32_t flag, const void* fine, void* coarse )
+{
+   ensure_constants();
+   ensure_p2_transfer_tables();
+   LevelView fv = make_view( m, Lf );
+   LevelView cv = make_view( m, Lf - 1 );
+   const int nC = m->topo.nC;
+   if ( dtype == F64 ) run_p2_restrict< double, double >( ctx, cv, fv, nC, flag, fine, coarse );
+   else if ( dtype == F32 ) run_p2_restrict< float, float >( ctx, cv, fv, nC, flag, fine, coarse );
+   else run_p2_restrict< __half, float >( ctx, cv, fv, nC, flag, fine, coarse );
+}
+
+template < typename T, typename A >
+static void run_p2_prolong( Context* ctx, const LevelView& cv, const LevelView& fv, int nC, uint32_t flag, const void* coarse,
+                            void* fine, int add )
+{
+   Fork fk( ctx );
+   if ( fv.nrows > 0 && nC > 0 )
+   {
+      dim3 grid( ( fv.nrows + 7 ) / 8, nC );
+      k_p2_prolong_cells< T, A ><<< grid, 256, 0, ctx->stream >>>( cv, fv, flag, (const T*) coarse, (T*) fine, add );
+      ++ctx->launches;
+   }
+   if ( fv.ntasks > 0 )
+   {
+      k_p2_prolong_bnd< T, A ><<< ( fv.ntasks + 255 ) / 256, 256, 0, fk.aux() >>>( cv, fv, flag, (const T*) coarse, (T*) fine,
+                                                                                        add );
+      ++ctx->launches;
+   }
+   check_cuda( cudaGetLastError(), "P2 prolongate launch" );
+}
+
+// Lc: coarse STORAGE level
+void launch_p2_prolongate( Context* ctx, Mesh* m, int Lc, int dtype, uint32_t flag, const void* coarse, void* fine, int add )
+{
+   ensure_constants();
+   ensure_p2_transfer_tables();
+   LevelView cv = make_view( m, Lc );
+   LevelView fv = make_view( m, Lc + 1 );
+   const int nC = m->topo.nC;
+   if ( dtype == F64 ) run_p2_prolong< double, double >( ctx, cv, fv, nC, flag, coarse, fine, add );
+   else if ( dtype == F32 ) run_p2_prolong< float, float >( ctx, cv, fv, nC, flag, coarse, fine, add );
+   else run_p2_prolong< __half, float >( ctx, cv, fv, nC, flag, coarse, fine, add );
+}
+
 // allocate every lazily created device table for levels minL..maxL (needed before graph capture)
 void prepare_device( Context* ctx, Mesh* m, Operator* op, int minL, int maxL, int dtype )
 {
    ensure_constants();
+   if ( op && op->order == 2 ) ensure_p2_transfer_tables();
    int most = 1;
    for ( int L = minL; L <= maxL; ++L )
    {

@@ -51,6 +51,7 @@ extern "C" {
 
 #define HYB_P1_ELEM_DIVKGRAD 3 /* P1ElementwiseBlendingDivKGradOperator (elementwiseoperators/P1ElementwiseOperator.hpp:329-373)
                                   with the form p1_div_k_grad_blending_q3 */
+#define HYB_P2_ELEM_DIVKGRAD 4 /* P2ElementwiseBlendingDivKGradOperator (elementwiseoperators/P2ElementwiseOperator.hpp:475) */
 
 /* blending maps (geometry/) */
 #define HYB_BLEND_NONE 0
@@ -138,6 +139,11 @@ int64_t hyb_layout_face_index( int level, int i, int j );
 /* ---------------------------------------------------------------- functions
  * P1Function<ValueType> (p1functionspace/P1Function.hpp, VertexDoFFunction.hpp). */
 int hyb_fn_create( hyb_ctx* ctx, hyb_mesh* mesh, int dtype, int min_level, int max_level, hyb_fn** out );
+/* P2Function<T>(name, storage, minLevel, maxLevel) (p2functionspace/P2Function.hpp:35-429): quadratic
+ * Lagrange DoFs (micro-vertices and micro-edge midpoints of level l).  Stored on the node set of level
+ * l+1, so every hyb_fn_* / hyb_op_* / solver call takes the P2 level and packed uploads and downloads
+ * use the vertex-DoF layout of level l+1 (hyb_layout_packed_size( mesh, l+1 ) values). */
+int hyb_fn_create_p2( hyb_ctx* ctx, hyb_mesh* mesh, int dtype, int min_level, int max_level, hyb_fn** out );
 int hyb_fn_destroy( hyb_fn* fn );
 /* host <-> device in the packed layout; host values are doubles.  Upload refreshes every copy of
  * an owned DoF from its owner (communicate). */
@@ -186,6 +192,13 @@ int hyb_op_create_divkgrad( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max
  * from now on every level's element matrices are computed once (when the level is first used) and read back
  * by every later apply instead of being recomputed; 80 bytes per micro-cell per level in FP64 (40 in FP32).
  * Call it before capturing any graph that applies the operator. */
+/* P2ElementwiseBlendingDivKGradOperator (elementwiseoperators/P2ElementwiseOperator.hpp:475) with the form
+ * p2_div_k_grad_blending_q4 (11-point degree-4 quadrature) on P2 functions (hyb_fn_create_p2); with k = NULL
+ * and no blending it is the P2 Laplacian (the matrix of P2ConstantLaplaceOperator).  hyb_restrict and
+ * hyb_prolongate on P2 functions are the quadratic transfers (P2toP2QuadraticRestriction /
+ * P2toP2QuadraticProlongation), used by the multigrid solver for P2 operators. */
+int hyb_op_create_p2_divkgrad( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, const hyb_coeff* k, int blending,
+                               hyb_op** out );
 int hyb_op_store_element_matrices( hyb_op* op );
 int hyb_op_destroy( hyb_op* op );
 int hyb_op_apply( hyb_op* op, hyb_fn* src, hyb_fn* dst, int level, uint32_t flag, int update );

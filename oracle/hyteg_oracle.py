@@ -1211,3 +1211,15 @@ def p2_prolongation_matrix(lev_c1, lev_f1):
                         vals.append(np.full(keep.sum(), N[j]))
     return sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
                          shape=(lev_f1.size, lev_c1.size)).tocsr()
+
+
+class P2Transfer(Transfer):
+    """P2toP2QuadraticProlongation / P2toP2QuadraticRestriction as matrices: P quadratic interpolation,
+    R = P^T (the reference's per-cell scaling plus additive communication sums every fine DoF once)."""
+
+    def __init__(self, op: P2DivKGrad):
+        self.op = op
+        self.R, self.P = {}, {}
+        for L in range(op.minL + 1, op.maxL + 1):
+            self.P[L] = p2_prolongation_matrix(op.levels[L - 1], op.levels[L])
+            self.R[L] = self.P[L].T.tocsr()

@@ -76,3 +76,16 @@ def p1_divkgrad_blending_element(X, map_kind=0, map_a=0.0, k_amp=0.5, k_phase=(0
     ph = np.asarray(k_phase, dtype=np.float64)
     f(_p(np.ascontiguousarray(X, dtype=np.float64).ravel()), map_kind, map_a, k_amp, _p(ph), _p(A))
     return A.reshape(4, 4)
+
+
+def p2_divkgrad_blending_element(X, map_kind=0, map_a=0.0, k_amp=0.5, k_phase=(0.0, 0.0, 0.0)):
+    """10x10 element matrix from the reference's p2_div_k_grad_blending_q4 form (same test maps and
+    coefficient as p1_divkgrad_blending_element); DoFs: vertices, then edges (2,3),(1,3),(1,2),(0,3),(0,2),(0,1)."""
+    L = lib()
+    f = L.ref_p2_divkgrad_blending_element
+    dp = C.POINTER(C.c_double)
+    f.argtypes = [dp, C.c_int, C.c_double, C.c_double, dp, dp]
+    A = np.zeros(100)
+    ph = np.asarray(k_phase, dtype=np.float64)
+    f(_p(np.ascontiguousarray(X, dtype=np.float64).ravel()), map_kind, map_a, k_amp, _p(ph), _p(A))
+    return A.reshape(10, 10)

@@ -223,3 +223,62 @@ def test_shell_map_derivative_and_vertices():
             e = np.zeros(3)
             e[j] = h
             np.testing.assert_allclose(D[:, :, j], (B.F(X + e) - B.F(X - e)) / (2 * h), atol=1e-8)
+
+
+# ------------------------------------------------------------------------------------------ P2
+def test_xg4_rule_is_degree_four():
+    """The 11-point rule with weights from the moment equations integrates every monomial of degree
+    <= 4 on the reference tetrahedron exactly (to rounding) and has positive weights."""
+    import math
+
+    P, w = O.XG4_POINTS, O.XG4_WEIGHTS
+    assert (w > 0).all()
+    for a in range(5):
+        for b in range(5 - a):
+            for c in range(5 - a - b):
+                exact = math.factorial(a) * math.factorial(b) * math.factorial(c) / math.factorial(a + b + c + 3)
+                assert abs((w * P[:, 0] ** a * P[:, 1] ** b * P[:, 2] ** c).sum() - exact) < 1e-15
+
+
+@pytest.mark.skipif(not R.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("map_kind,a", [(0, 0.0), (1, 0.3)])
+def test_p2_divkgrad_element_matches_reference_form(map_kind, a):
+    """p2_div_k_grad_blending_q4 compiled from the reference sources, with a test blending map."""
+    rng = np.random.default_rng(12)
+    X = rng.uniform(0, 1, (5, 4, 3))
+    ph = (0.31, 0.12, 0.77)
+    K = O.p2_divkgrad_element(X, O.k_expsin(0.5, ph), None if map_kind == 0 else O.TestMap(a))
+    Kr = np.stack([R.p2_divkgrad_blending_element(x, map_kind, a, 0.5, ph) for x in X])
+    np.testing.assert_allclose(K, Kr, rtol=0, atol=1e-13 * np.abs(Kr).max())
+
+
+def _slot_coords(lev):
+    X = np.full((lev.size, 3), np.nan)
+    pts = O.tet_points(lev.n + 1)
+    for c in range(lev.mesh.nC):
+        X[lev.owner(c, pts[:, 0], pts[:, 1], pts[:, 2])] = lev.coords(c, pts[:, 0], pts[:, 1], pts[:, 2])
+    return X
+
+
+@pytest.mark.parametrize("name", ["cube_6", "octahedron_8", "tilted_tet"])
+def test_p2_operator_and_transfer_properties(name):
+    """P2 on the node set of level L+1: linear functions are annihilated on inner DoFs, quadratic
+    prolongation reproduces quadratics, and (k = 1, affine) A_{L-1} = P^T A_L P (Galerkin)."""
+    coords, tets = M.ALL[name]()
+    op = O.P2DivKGrad(O.MacroMesh(coords, tets), 1, 3, lambda P: np.ones(len(P)))
+    for L in (1, 2, 3):
+        lev = op.levels[L]
+        X = _slot_coords(lev)
+        u = lev.sync(np.nan_to_num(1.0 + 2 * X[:, 0] - 0.5 * X[:, 1] + 0.25 * X[:, 2]))
+        assert np.abs((op.A[L] @ u)[lev.owned_mask(O.INNER)]).max() < 1e-13
+    for L in (2, 3):
+        Pm = O.p2_prolongation_matrix(op.levels[L - 1], op.levels[L])
+        Xc, Xf = _slot_coords(op.levels[L - 1]), _slot_coords(op.levels[L])
+        q = lambda X: 1 + X[:, 0] ** 2 - 2 * X[:, 1] * X[:, 2] + 0.5 * X[:, 2] + X[:, 0] * X[:, 1]
+        uf = Pm @ op.levels[L - 1].sync(np.nan_to_num(q(Xc)))
+        ownf = op.levels[L].owned_mask(O.ALL)
+        assert np.abs(uf[ownf] - q(Xf)[ownf]).max() < 1e-13
+        ownc = op.levels[L - 1].owned_mask(O.ALL)
+        Ac = op.A[L - 1][ownc][:, ownc]
+        Pf = Pm[ownf][:, ownc]
+        assert abs(Pf.T @ op.A[L][ownf][:, ownf] @ Pf - Ac).max() < 1e-13 * abs(Ac).max()
