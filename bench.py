@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--no-vcycle", action="store_true")
     p.add_argument("--no-mixed", action="store_true")
     p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--no-p2", action="store_true")
     p.add_argument("--serve-requests", type=int, default=200)
     return p.parse_args()
 
@@ -284,6 +285,84 @@ def serving_leg(H, ctx, nreq=200, seed=7):
             "speedup_solves_per_s": served["solves_per_s"] / seq["solves_per_s"]}
 
 
+def p2_leg(H, ctx, level=5, cycle_level=3):
+    """Configuration 2's operator: P2 -div(k grad u) with the icosahedral-shell blending map on the
+    shell ntan=5, nrad=3 (1920 macro-cells), k = exp(0.5 sin(2 pi x) cos(2 pi y) sin(2 pi z)), FP64.
+    Times one apply at `level` (element integrals recomputed every apply, as the reference's
+    elementwise operator does) and with stored element matrices one level lower, and one V(3,3)
+    Chebyshev(3) cycle on levels 0..cycle_level.  The reference counts 11,678 flops per micro-cell for
+    assembling the 10x10 matrix (p2_div_k_grad_blending_q4.hpp:91-98) plus 200 for the matvec; that
+    count gives the GFLOP/s figure (this implementation needs fewer: it never forms the matrix)."""
+    import torch
+
+    K = ("expsin", 0.5, (0.0, 0.0, 0.0))
+    pm = H.PrimitiveStorage.spherical_shell(5, 3, 0.55, 1.0, ctx=ctx)
+    nC = pm.counts()[3]
+
+    def time_apply(A, L, reps):
+        x = H.P2Function("x", pm, L, L, ctx)
+        y = H.P2Function("y", pm, L, L, ctx)
+        x.fill_random(L, 1)
+        A.apply(x, y, L, H.Inner)
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            A.apply(x, y, L, H.Inner)
+        ctx.synchronize()
+        return (time.perf_counter() - t0) / reps
+
+    out = {"mesh": "spherical shell ntan=5 nrad=3 (1920 macro-cells), IcosahedralShellMap blending",
+           "coefficient": "exp(0.5 sin(2 pi x) cos(2 pi y) sin(2 pi z))", "dtype": "f64"}
+    A = H.P2ElementwiseBlendingDivKGradOperator(pm, level, level, ctx, k=K, blending="shell")
+    sec = time_apply(A, level, 3)
+    mc = nC * (1 << level) ** 3
+    out["apply"] = {"level": level, "micro_cells": mc, "dofs": pm.packed_size(level + 1), "ms": sec * 1e3,
+                    "Mcells_per_s": mc / sec / 1e6, "gflops_reference_count": mc * 11878 / sec / 1e9}
+    del A
+    Ls = level - 1
+    S = H.P2ElementwiseBlendingDivKGradOperator(pm, Ls, Ls, ctx, k=K, blending="shell")
+    S.computeAndStoreLocalElementMatrices()
+    sec = time_apply(S, Ls, 5)
+    mcs = nC * (1 << Ls) ** 3
+    out["apply_stored"] = {"level": Ls, "micro_cells": mcs, "ms": sec * 1e3, "Mcells_per_s": mcs / sec / 1e6,
+                           "bytes_per_micro_cell": 55 * 8}
+    del S
+    Ac = H.P2ElementwiseBlendingDivKGradOperator(pm, 0, cycle_level, ctx, k=K, blending="shell")
+    Ac.computeAndStoreLocalElementMatrices()
+    g = H.GeometricMultigridSolver(ctx, Ac, 0, cycle_level, 3, 3, smoother="chebyshev", chebyshev_order=3,
+                                   power_iterations=20)
+    x = H.P2Function("xv", pm, 0, cycle_level, ctx)
+    b = H.P2Function("bv", pm, 0, cycle_level, ctx)
+    b.fill_random(cycle_level, 3)
+    hist = g.solve_cycles(x, b, cycle_level, 2)  # setup, capture, two cycles
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    n = 3
+    for _ in range(n):
+        g.solve(Ac, x, b, cycle_level)
+    ctx.synchronize()
+    out["vcycle"] = {"levels": f"0..{cycle_level}", "ms_per_cycle": (time.perf_counter() - t0) / n * 1e3,
+                     "cycle": "V(3,3) Chebyshev(3), stored element matrices, CG coarse", "factors": list(hist[1:] / hist[:-1])}
+    return out
+
+
+def p2_cpu_reference(cells=400000):
+    """The reference's per-micro-cell work of the P2 elementwise apply (integrateAll of the generated
+    form + 10x10 matvec), compiled from its sources, on the host cores (test blending map)."""
+    import ctypes as C
+
+    from oracle import ref as R
+
+    if not R.available():
+        return None
+    f = R.lib().ref_p2_elem_apply_bench
+    f.restype, f.argtypes = C.c_double, [C.c_long, C.c_int, C.c_double]
+    threads = os.cpu_count() or 1
+    sec = f(cells, threads, 0.5)
+    return {"Mcells_per_s": cells / sec / 1e6, "cores": threads, "kind": "reference",
+            "sample": f"{cells} micro-cells of p2_div_k_grad_blending_q4 integrateAll + matvec, OpenMP"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -405,6 +484,10 @@ def run_ours(args, rank, world, local):
         return
     mixed = None if args.no_mixed else mixed_precision_leg(H, ctx, pm, A, L)
     serving = None if args.no_serve else serving_leg(H, ctx, nreq=args.serve_requests)
+    p2 = None
+    if not args.no_p2:
+        p2 = p2_leg(H, ctx)
+        p2["cpu_baseline"] = p2_cpu_reference()
     peak, peak_kind = measured_peak()
     alg_bytes = 2 * 8 * ndof  # read x, write y per inner DoF
     achieved = alg_bytes / (ms * 1e-3) / 1e9
@@ -430,6 +513,8 @@ def run_ours(args, rank, world, local):
         line["mixed_precision"] = mixed
     if serving:
         line["serving"] = serving
+    if p2:
+        line["p2_divkgrad_shell"] = p2
     if cpu:
         rate, k, threads, el = cpu
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",

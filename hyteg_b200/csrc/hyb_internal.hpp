@@ -100,8 +100,11 @@ struct Topology {
 };
 
 // per-level host + device tables of the P1 layout
-// tile of the z-streamed cell sweep: 64 x-points (two per lane) by 8 rows (one per warp)
-constexpr int kZTileX = 64, kZTileY = 8;
+// tiles of the z-streamed cell sweep: kZTileY rows (one per warp) by 64 x-points (two per lane); the
+// second width serves 4- and 2-byte values (128-wide tiles were measured slower on the level-8 cube:
+// register spills and fewer work units)
+constexpr int kZTileY = 8;
+constexpr int kZWidths[2] = { 64, 64 };
 
 struct P1Level {
    int     L = 0, n = 0;
@@ -122,8 +125,8 @@ struct P1Level {
    // z-streamed sweep: units {x0, y0, z_first, z_last}, each a kZTileX x kZTileY tile of slice
    // columns over a range of slices; block b of the sweep runs units zbegin[b]..zbegin[b+1]-1
    // (assigned longest-first to the least loaded block)
-   std::vector< std::array< int, 4 > > zunits;
-   std::vector< int >                  zbegin;
+   std::vector< std::array< int, 4 > > zunits[2];  // per tile width kZWidths[w]
+   std::vector< int >                  zbegin[2];
    int64_t n_owned_cell = 0;
    // device copies
    int64_t*   d_off       = nullptr;  // all primitives
@@ -132,8 +135,8 @@ struct P1Level {
    int4*      d_tasks     = nullptr;
    int2*      d_rows      = nullptr;
    int4*      d_march     = nullptr;
-   int4*      d_zunits    = nullptr;
-   int*       d_zbegin    = nullptr;
+   int4*      d_zunits[2] = { nullptr, nullptr };
+   int*       d_zbegin[2] = { nullptr, nullptr };
    uint8_t*   d_bc        = nullptr;  // bc type per primitive (v, e, f, c order)
    int8_t*    d_bkind     = nullptr;  // 0 vertex, 1 edge, 2 face per boundary primitive
    float*     d_ncell_cls = nullptr;  // per cell, per class: number of macro-cells around the sub-primitive
@@ -197,8 +200,8 @@ struct ElemLevel {
    void* d_acc  = nullptr;  // accumulation buffer (level size, accumulation precision)
    int   acc_dtype = -1;
    void* d_invd[3] = { nullptr, nullptr, nullptr };  // inverse diagonal per DoF, per storage dtype
-   int2* d_hrows    = nullptr;                         // anchor rows (y, z) per (y, z) parity
-   int   hoff[5]    = { 0, 0, 0, 0, 0 };
+   int*  d_anch     = nullptr;                         // micro-cell anchors x | y << 10 | z << 20, by parity class
+   int   aoff[9]    = {};                              // class p = px | py << 1 | pz << 2 spans aoff[p]..aoff[p+1]-1
    // stored element matrices (computeAndStoreLocalElementMatrices): the 10 upper-triangle entries
    // of every micro-cell's 4x4 matrix, value-major, in double ([0]) and float ([1])
    void* d_K[2] = { nullptr, nullptr };
@@ -311,7 +314,7 @@ void launch_cg_scalar( Context* ctx, double* state, int stage, double rtol, doub
 void check_cuda( cudaError_t e, const char* what );
 void build_level( Mesh* m, int L );
 void ensure_device( Mesh* m, P1Level& P );
-void build_zunits( P1Level& P, int nblocks );
+void build_zunits( P1Level& P, int nblocks, int w );
 void build_operator_level( Operator* A, int L );
 void ensure_device_op( OpLevel& ol );
 

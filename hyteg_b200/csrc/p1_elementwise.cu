@@ -233,24 +233,22 @@ __device__ __forceinline__ void   st_any( __half* p, float v ) { *p = __float2ha
 // triangle; 3: y += K x with K read from storage.  Stored entry v of micro-cell (cell c, type ty,
 // anchor a) sits at kst[v * kstride + (c * 6 + ty) * tet(n) + cidx(n - 1, a)].
 template < typename T, typename A, int MODE >
-__global__ void __launch_bounds__( 256 ) k_elem_pass( int n, int nrows, const int2* __restrict__ rows, const int64_t* __restrict__ cell_off,
-                                                       const CellGeom* __restrict__ geom, Coefficient kc, int px,
+__global__ void __launch_bounds__( 256 ) k_elem_pass( int n, int nanch, const int* __restrict__ anch, const int64_t* __restrict__ cell_off,
+                                                       const CellGeom* __restrict__ geom, Coefficient kc,
                                                        const T* __restrict__ src, A* __restrict__ acc, A* __restrict__ kst,
                                                        int64_t kstride, int64_t level_size, int* err )
 {
-   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-   const int r    = blockIdx.x * 8 + warp;
-   const int c    = blockIdx.y;
-   if ( r >= nrows ) return;
-   const int2     yz = rows[r];
-   const int      y = yz.x, z = yz.y;
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;  // one micro-cell anchor per thread
+   const int c = blockIdx.y;
+   if ( t >= nanch ) return;
+   const int      a = anch[t];
+   const int      x = a & 1023, y = ( a >> 10 ) & 1023, z = a >> 20;
    const CellGeom g  = geom[c];
    const int64_t  base = cell_off[c];
    const A        inv_n = A( 1.0 / double( n ) );
    A              st[3][3];  // computational steps per index direction (coordinateFromIndex)
    for ( int k = 0; k < 3; ++k )
       for ( int d = 0; d < 3; ++d ) st[k][d] = ( A( g.P[k + 1][d] ) - A( g.P[0][d] ) ) * inv_n;
-   for ( int x = px + 2 * lane; x + y + z <= n - 1; x += 64 )
       for ( int ty = 0; ty < 6; ++ty )
       {
          if ( x + y + z > n - 1 - c_mc_shift[ty] ) continue;
@@ -459,24 +457,22 @@ __device__ __forceinline__ void p2_grad( int q, int i, const A Mi[3][3], A G[3] 
 // triangle entries of K; 3: y += K x from the stored entries.  Stored entry v of micro-cell (cell c,
 // type ty, anchor a) sits at kst[v * kstride + (c * 6 + ty) * tet(ne) + cidx(ne - 1, a)].
 template < typename T, typename A, int MODE >
-__global__ void __launch_bounds__( 256 ) k_p2_pass( int ne, int nrows, const int2* __restrict__ rows, const int64_t* __restrict__ cell_off,
-                                                     const CellGeom* __restrict__ geom, Coefficient kc, int px,
+__global__ void __launch_bounds__( 256 ) k_p2_pass( int ne, int nanch, const int* __restrict__ anch, const int64_t* __restrict__ cell_off,
+                                                     const CellGeom* __restrict__ geom, Coefficient kc,
                                                      const T* __restrict__ src, A* __restrict__ acc, A* __restrict__ kst,
                                                      int64_t kstride, int64_t level_size, int* err )
 {
-   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-   const int r    = blockIdx.x * 8 + warp;
-   const int c    = blockIdx.y;
-   if ( r >= nrows ) return;
-   const int2     yz = rows[r];
-   const int      y = yz.x, z = yz.y, ns = 2 * ne;
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;  // one micro-cell anchor per thread
+   const int c = blockIdx.y;
+   if ( t >= nanch ) return;
+   const int      a = anch[t];
+   const int      x = a & 1023, y = ( a >> 10 ) & 1023, z = a >> 20, ns = 2 * ne;
    const CellGeom g    = geom[c];
    const int64_t  base = cell_off[c];
    const A        inv_n = A( 1.0 / double( ne ) );
    A              st[3][3];
    for ( int k = 0; k < 3; ++k )
       for ( int d = 0; d < 3; ++d ) st[k][d] = ( A( g.P[k + 1][d] ) - A( g.P[0][d] ) ) * inv_n;
-   for ( int x = px + 2 * lane; x + y + z <= ne - 1; x += 64 )
       for ( int ty = 0; ty < 6; ++ty )
       {
          if ( x + y + z > ne - 1 - c_mc_shift[ty] ) continue;
@@ -722,23 +718,27 @@ static A* acc_buffer( Operator* op, int L, int64_t size )
 static int element_n( const Operator* op, int L ) { return op->order == 2 ? ( 1 << ( L - 1 ) ) : ( 1 << L ); }
 static int element_values( const Operator* op ) { return op->order == 2 ? 55 : 10; }
 
+// micro-cell anchors (x, y, z), x + y + z <= n - 1, grouped by coordinate parity: the micro-cells of
+// anchors of one parity class share no vertex (nor, for P2, any node), so a pass over one class
+// updates its nodes without conflicts
 static void ensure_rows( Operator* op, int L )
 {
    ElemLevel& e = op->el[L];
-   if ( e.d_hrows ) return;
-   const int                  n = element_n( op, L );
-   std::vector< int2 >        rows;
-   for ( int p = 0; p < 4; ++p )
+   if ( e.d_anch ) return;
+   const int          n = element_n( op, L );
+   std::vector< int > anch;
+   for ( int p = 0; p < 8; ++p )
    {
-      e.hoff[p]    = int( rows.size() );
-      const int py = p & 1, pz = p >> 1;
+      e.aoff[p]    = int( anch.size() );
+      const int px = p & 1, py = ( p >> 1 ) & 1, pz = p >> 2;
       for ( int z = pz; z <= n - 1; z += 2 )
-         for ( int y = py; y + z <= n - 1; y += 2 ) rows.push_back( make_int2( y, z ) );
+         for ( int y = py; y + z <= n - 1; y += 2 )
+            for ( int x = px; x + y + z <= n - 1; x += 2 ) anch.push_back( x | ( y << 10 ) | ( z << 20 ) );
    }
-   e.hoff[4] = int( rows.size() );
-   check_cuda( cudaMalloc( &e.d_hrows, std::max< size_t >( rows.size(), 1 ) * sizeof( int2 ) ), "cudaMalloc(rows)" );
-   if ( !rows.empty() )
-      check_cuda( cudaMemcpy( e.d_hrows, rows.data(), rows.size() * sizeof( int2 ), cudaMemcpyHostToDevice ), "upload rows" );
+   e.aoff[8] = int( anch.size() );
+   check_cuda( cudaMalloc( &e.d_anch, std::max< size_t >( anch.size(), 1 ) * sizeof( int ) ), "cudaMalloc(anchors)" );
+   if ( !anch.empty() )
+      check_cuda( cudaMemcpy( e.d_anch, anch.data(), anch.size() * sizeof( int ), cudaMemcpyHostToDevice ), "upload anchors" );
 }
 
 // entries per stored value: every (cell, micro-cell type, anchor) slot of the level
@@ -758,17 +758,15 @@ static void run_passes( Context* ctx, Mesh* m, Operator* op, int L, const T* src
    const int nC = m->topo.nC;
    for ( int p = 0; p < 8; ++p )
    {
-      const int px = p & 1, q = p >> 1;  // q = (py, pz) row table
-      const int nr = e.hoff[q + 1] - e.hoff[q];
-      if ( nr <= 0 ) continue;
-      dim3 grid( ( nr + 7 ) / 8, nC );
+      const int na = e.aoff[p + 1] - e.aoff[p];
+      if ( na <= 0 ) continue;
+      dim3 grid( ( na + 255 ) / 256, nC );
       if ( op->order == 2 )
-         k_p2_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( element_n( op, L ), nr, e.d_hrows + e.hoff[q], P.d_off + P.nB,
-                                                                    op->d_geom, op->coeff, px, src, acc, kst, ks, P.size,
-                                                                    ctx->d_error );
+         k_p2_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( element_n( op, L ), na, e.d_anch + e.aoff[p], P.d_off + P.nB,
+                                                                    op->d_geom, op->coeff, src, acc, kst, ks, P.size, ctx->d_error );
       else
-         k_elem_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( P.n, nr, e.d_hrows + e.hoff[q], P.d_off + P.nB, op->d_geom,
-                                                                      op->coeff, px, src, acc, kst, ks, P.size, ctx->d_error );
+         k_elem_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( P.n, na, e.d_anch + e.aoff[p], P.d_off + P.nB, op->d_geom,
+                                                                      op->coeff, src, acc, kst, ks, P.size, ctx->d_error );
       ++ctx->launches;
    }
    check_cuda( cudaGetLastError(), "elementwise pass launch" );

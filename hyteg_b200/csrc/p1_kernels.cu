@@ -111,9 +111,9 @@ struct LevelView
    const float*     ncell_cls;
    int              nmarch;
    const int4*      march;
-   int              nzblocks;
-   const int4*      zunits;
-   const int*       zbegin;
+   int              nzblocks[2];  // per tile width kZWidths[w]
+   const int4*      zunits[2];
+   const int*       zbegin[2];
 };
 
 template < typename A >
@@ -144,9 +144,12 @@ static LevelView make_view( Mesh* m, int L )
    v.ncell_cls = P.d_ncell_cls;
    v.nmarch     = int( P.march.size() );
    v.march      = P.d_march;
-   v.nzblocks   = int( P.zbegin.size() ) - 1;
-   v.zunits     = P.d_zunits;
-   v.zbegin     = P.d_zbegin;
+   for ( int wi = 0; wi < 2; ++wi )
+   {
+      v.nzblocks[wi] = int( P.zbegin[wi].size() ) - 1;
+      v.zunits[wi]   = P.d_zunits[wi];
+      v.zbegin[wi]   = P.d_zbegin[wi];
+   }
    return v;
 }
 
@@ -420,6 +423,9 @@ __host__ __device__ constexpr bool zstream_aux()
 template < typename T, bool AUX >
 struct ZCfg
 {
+   static constexpr int wi      = sizeof( T ) == 8 ? 0 : 1;                      // tile width index
+   static constexpr int kZTileX = kZWidths[wi];                                 // x-points per tile row
+   static constexpr int pts     = kZTileX / 32;                                 // x-points per consumer lane
    static constexpr int al    = 16 / int( sizeof( T ) );                         // elements per 16 bytes
    static constexpr int RW    = ( kZTileX + 2 + 2 * al + al - 1 ) / al * al;    // source row width (elements)
    static constexpr int RWA   = ( kZTileX + 2 * al + al - 1 ) / al * al;        // second-vector row width
@@ -435,7 +441,6 @@ constexpr int kZWarps     = kZTileY;
 // level-8 cube apply in FP64, 0.154 -> 0.108 ms in FP32).
 constexpr int kZProducers = 2;
 constexpr int kZThreads   = ( kZWarps + kZProducers ) * 32;  // consumer warps + producer warps
-constexpr int kZPts     = kZTileX / 32;         // x-points per consumer lane
 
 // offset of slice z+1 minus offset of slice z in a macro-cell array (tri(n+1-z) points in slice z)
 __device__ __forceinline__ int64_t slice_step( int n, int z ) { return int64_t( n + 1 - z ) * ( n + 2 - z ) / 2; }
@@ -450,10 +455,12 @@ __device__ __forceinline__ void zstream_produce( const LevelView& v, uint32_t fl
                                                  uint32_t* shw, volatile int* abort_flag, int* err )
 {
    using Cfg = ZCfg< T, AUX >;
-   constexpr int S = Cfg::S, AL = Cfg::al;
+   constexpr int S = Cfg::S, AL = Cfg::al, kZTileX = Cfg::kZTileX;
    static_assert( S % kZProducers == 0, "every stage must belong to one producer warp" );
    const int     lane = threadIdx.x & 31, n = v.n, me = ( threadIdx.x >> 5 ) - kZWarps;
-   const int     u0 = v.zbegin[blockIdx.x], u1 = v.zbegin[blockIdx.x + 1];
+   const int*    zb = v.zbegin[Cfg::wi];
+   const int4*   zu = v.zunits[Cfg::wi];
+   const int     u0 = zb[blockIdx.x], u1 = zb[blockIdx.x + 1];
    const bool    is_src = lane < Cfg::rows, is_aux = AUX && lane >= Cfg::rows && lane < Cfg::rows + kZTileY;
    const int     dsto   = is_src ? lane * Cfg::RW : Cfg::aux0 + ( lane - Cfg::rows ) * Cfg::RWA;
    const T*      gbase  = is_src ? src : aux;
@@ -466,7 +473,7 @@ __device__ __forceinline__ void zstream_produce( const LevelView& v, uint32_t fl
       const int64_t cb = v.cell_off[c];
       for ( int u = u0; u < u1 && ok; ++u )
       {
-         const int4 U  = v.zunits[u];  // x0, y0, z_first, z_last
+         const int4 U  = zu[u];  // x0, y0, z_first, z_last
          const int  yy = is_src ? U.y - 1 + lane : U.y + ( lane - Cfg::rows );
          const int  xa = is_src ? U.x - 1 : U.x;  // first x of the row segment
          int64_t    rb = cidx( n, 0, yy, U.z - 1 );
@@ -582,7 +589,10 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, O
 
    // consumer warp `warp` owns tile row y0 + warp; stage row r holds global row y0 - 1 + r; lane
    // owns x = x0 + lane + 32 k, k < kZPts
-   const int u0 = v.zbegin[blockIdx.x], u1 = v.zbegin[blockIdx.x + 1];
+   constexpr int kZPts = Cfg::pts;
+   const int*    zb    = v.zbegin[Cfg::wi];
+   const int4*   zu    = v.zunits[Cfg::wi];
+   const int     u0 = zb[blockIdx.x], u1 = zb[blockIdx.x + 1];
    const int rS = warp, rC = warp + 1, rN = warp + 2;  // rows y-1, y, y+1 of the stage
    auto at = [&]( const T* st, uint32_t word, int r, int k, int dx ) -> A {
       return A( st[r * RW + int( ( word >> ( 3 * r ) ) & 7u ) + lane + 32 * k + 1 + dx] );
@@ -608,7 +618,7 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, O
       __syncwarp();
       for ( int u = u0; u < u1; ++u )
       {
-         const int4 U = v.zunits[u];
+         const int4 U = zu[u];
          const int  x = U.x + lane, y = U.y + warp;
          // prologue: slice z_first-1 (load ld) and slice z_first (load ld+1)
          const int sm = ld % S, s0 = ( ld + 1 ) % S;
@@ -820,10 +830,10 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
    T*       v2  = (T*) a.v2;
    T*       dst = (T*) a.dst;
    Fork     fk( ctx );
-   if ( cell_kernel_variant() == 2 && v.n >= 32 && v.nzblocks > 0 && nC > 0 )
+   if ( cell_kernel_variant() == 2 && v.n >= 32 && v.nzblocks[ZCfg< T, false >::wi] > 0 && nC > 0 )
    {
       constexpr size_t smem = ZCfg< T, zstream_aux< OP >() >::smem_bytes;  // attribute set by ensure_constants
-      k_cell_zstream< T, A, OP ><<< v.nzblocks, kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ),
+      k_cell_zstream< T, A, OP ><<< v.nzblocks[ZCfg< T, false >::wi], kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ),
                                                                                  A( a.a1 ), nC, ctx->d_error );
       ++ctx->launches;
    }

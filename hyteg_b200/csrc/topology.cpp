@@ -305,11 +305,13 @@ void build_level( Mesh* m, int L )
 // per two blocks (every chunk re-reads two halo slices, and every slice load costs a fixed hand-off,
 // so long chunks win over finer balance); units are then handed out longest-first to the least
 // loaded block.
-void build_zunits( P1Level& P, int nblocks )
+void build_zunits( P1Level& P, int nblocks, int wi )
 {
-   const int n = P.n;
-   P.zunits.clear();
-   P.zbegin.assign( 1, 0 );
+   const int n = P.n, kZTileX = kZWidths[wi];
+   auto&     zunits = P.zunits[wi];
+   auto&     zbegin = P.zbegin[wi];
+   zunits.clear();
+   zbegin.assign( 1, 0 );
    if ( n < 4 ) return;
    struct Unit
    {
@@ -352,8 +354,8 @@ void build_zunits( P1Level& P, int nblocks )
    }
    for ( int b = 0; b < nb; ++b )
    {
-      for ( const auto& u : per[b] ) P.zunits.push_back( u );
-      P.zbegin.push_back( int( P.zunits.size() ) );
+      for ( const auto& u : per[b] ) zunits.push_back( u );
+      zbegin.push_back( int( zunits.size() ) );
    }
 }
 
@@ -383,11 +385,15 @@ void ensure_device( Mesh* m, P1Level& P )
    int dev = 0, sms = 0;
    check_cuda( cudaGetDevice( &dev ), "cudaGetDevice" );
    check_cuda( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev ), "device attribute" );
-   build_zunits( P, 2 * std::max( sms, 1 ) );
-   std::vector< int4 > zu( P.zunits.size() );
-   for ( size_t i = 0; i < zu.size(); ++i ) zu[i] = make_int4( P.zunits[i][0], P.zunits[i][1], P.zunits[i][2], P.zunits[i][3] );
-   up( &P.d_zunits, zu.data(), zu.size() );
-   up( &P.d_zbegin, P.zbegin.data(), P.zbegin.size() );
+   for ( int wi = 0; wi < 2; ++wi )
+   {
+      build_zunits( P, 2 * std::max( sms, 1 ), wi );
+      const auto&         U = P.zunits[wi];
+      std::vector< int4 > zu( U.size() );
+      for ( size_t i = 0; i < zu.size(); ++i ) zu[i] = make_int4( U[i][0], U[i][1], U[i][2], U[i][3] );
+      up( &P.d_zunits[wi], zu.data(), zu.size() );
+      up( &P.d_zbegin[wi], P.zbegin[wi].data(), P.zbegin[wi].size() );
+   }
    std::vector< uint8_t > bc( nP );
    std::vector< int8_t >  bk( P.nB );
    for ( int v = 0; v < t.nV; ++v ) bc[v] = uint8_t( t.bc( t.flag_v[v] ) ), bk[v] = 0;
@@ -430,8 +436,7 @@ Mesh::~Mesh()
       cudaFree( P.d_tasks );
       cudaFree( P.d_rows );
       cudaFree( P.d_march );
-      cudaFree( P.d_zunits );
-      cudaFree( P.d_zbegin );
+      for ( int wi = 0; wi < 2; ++wi ) cudaFree( P.d_zunits[wi] ), cudaFree( P.d_zbegin[wi] );
       cudaFree( P.d_bc );
       cudaFree( P.d_bkind );
       cudaFree( P.d_ncell_cls );
@@ -592,7 +597,7 @@ Operator::~Operator()
       cudaFree( kv.second.d_acc );
       for ( void* p : kv.second.d_invd ) cudaFree( p );
       for ( void* p : kv.second.d_K ) cudaFree( p );
-      cudaFree( kv.second.d_hrows );
+      cudaFree( kv.second.d_anch );
    }
    cudaFree( d_geom );
 }

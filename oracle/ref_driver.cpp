@@ -151,3 +151,46 @@ extern "C" void ref_p2_divkgrad_blending_element( const double* coords12, int ma
    form.integrateAll( c, M );
    for ( int i = 0; i < 100; ++i ) A100[i] = M.a[i];
 }
+
+// CPU timing of the reference's per-micro-cell work in P2ElementwiseOperator::apply
+// (P2ElementwiseOperator.cpp:203-220: integrateAll of p2_div_k_grad_blending_q4, then y += K x on the
+// ten element DoFs) over `ncells` micro-cells of a refined tetrahedron, with the smooth test blending
+// map standing in for the shell map, OpenMP over micro-cells.  Returns the wall-clock seconds.
+#include <chrono>
+#include <omp.h>
+extern "C" double ref_p2_elem_apply_bench( long ncells, int threads, double k_amp )
+{
+   const double ph[3] = { 0.13, 0.27, 0.41 };
+   auto         t0    = std::chrono::steady_clock::now();
+   double       sink  = 0;
+#pragma omp parallel num_threads( threads ) reduction( + : sink )
+   {
+      auto map  = std::make_shared< TestMap >();
+      map->kind = 1;
+      map->a    = 0.1;
+      auto k3   = [k_amp, &ph]( const hyteg::Point3D& p ) {
+         const double tp = 2.0 * 3.14159265358979323846;
+         return std::exp( k_amp * std::sin( tp * ( p[0] + ph[0] ) ) * std::cos( tp * ( p[1] + ph[1] ) ) * std::sin( tp * ( p[2] + ph[2] ) ) );
+      };
+      auto                                   k2 = []( const hyteg::Point3D& ) { return 1.0; };
+      hyteg::forms::p2_div_k_grad_blending_q4 form( k2, k3 );
+      form.setGeometryMap( map );
+      double x[10], y[10] = {};
+      for ( int i = 0; i < 10; ++i ) x[i] = 0.1 * ( i + 1 );
+      const double h = 1.0 / 64.0;
+#pragma omp for schedule( static )
+      for ( long c = 0; c < ncells; ++c )
+      {
+         const double o[3] = { h * double( c % 61 ), h * double( ( c / 61 ) % 59 ), h * double( ( c / 3599 ) % 53 ) };
+         std::array< hyteg::Point3D, 4 > v = { hyteg::Point3D( o[0], o[1], o[2] ), hyteg::Point3D( o[0] + h, o[1], o[2] ),
+                                               hyteg::Point3D( o[0], o[1] + h, o[2] ), hyteg::Point3D( o[0], o[1], o[2] + h ) };
+         hyteg::Matrix< double, 10, 10 > K;
+         form.integrateAll( v, K );
+         for ( int i = 0; i < 10; ++i )
+            for ( int j = 0; j < 10; ++j ) y[i] += K( i, j ) * x[j];
+      }
+      for ( int i = 0; i < 10; ++i ) sink += y[i];
+   }
+   const double s = std::chrono::duration< double >( std::chrono::steady_clock::now() - t0 ).count();
+   return sink == 12345.678 ? -s : s;  // keep the work observable
+}
