@@ -127,6 +127,10 @@ struct P1Level {
    // (assigned longest-first to the least loaded block)
    std::vector< std::array< int, 4 > > zunits[2];  // per tile width kZWidths[w]
    std::vector< int >                  zbegin[2];
+   // full-row sweep: units {ty, y0, z_first, z_last} (rows y0..y0+ty-1 of slices z_first..z_last),
+   // one list per band height ty = 1 << h (h = 0..3), blocks as for zunits
+   std::vector< std::array< int, 4 > > runits[4];
+   std::vector< int >                  rbegin[4];
    int64_t n_owned_cell = 0;
    // device copies
    int64_t*   d_off       = nullptr;  // all primitives
@@ -137,6 +141,8 @@ struct P1Level {
    int4*      d_march     = nullptr;
    int4*      d_zunits[2] = { nullptr, nullptr };
    int*       d_zbegin[2] = { nullptr, nullptr };
+   int4*      d_runits[4] = {};
+   int*       d_rbegin[4] = {};
    uint8_t*   d_bc        = nullptr;  // bc type per primitive (v, e, f, c order)
    int8_t*    d_bkind     = nullptr;  // 0 vertex, 1 edge, 2 face per boundary primitive
    float*     d_ncell_cls = nullptr;  // per cell, per class: number of macro-cells around the sub-primitive
@@ -315,6 +321,7 @@ void check_cuda( cudaError_t e, const char* what );
 void build_level( Mesh* m, int L );
 void ensure_device( Mesh* m, P1Level& P );
 void build_zunits( P1Level& P, int nblocks, int w );
+void build_runits( P1Level& P, int nblocks, int h );
 void build_operator_level( Operator* A, int L );
 void ensure_device_op( OpLevel& ol );
 

@@ -111,6 +111,9 @@ struct LevelView
    const float*     ncell_cls;
    int              nmarch;
    const int4*      march;
+   int              nrblocks[4];  // full-row sweep blocks per band height 1 << h
+   const int4*      runits[4];
+   const int*       rbegin[4];
    int              nzblocks[2];  // per tile width kZWidths[w]
    const int4*      zunits[2];
    const int*       zbegin[2];
@@ -144,6 +147,12 @@ static LevelView make_view( Mesh* m, int L )
    v.ncell_cls = P.d_ncell_cls;
    v.nmarch     = int( P.march.size() );
    v.march      = P.d_march;
+   for ( int h = 0; h < 4; ++h )
+   {
+      v.nrblocks[h] = int( P.rbegin[h].size() ) - 1;
+      v.runits[h]   = P.d_runits[h];
+      v.rbegin[h]   = P.d_rbegin[h];
+   }
    for ( int wi = 0; wi < 2; ++wi )
    {
       v.nzblocks[wi] = int( P.zbegin[wi].size() ) - 1;
@@ -706,9 +715,226 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, O
    }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Full-row z-streamed cell sweep (selectable with HYB_CELL_KERNEL=zrow).
+//
+// A unit is the band of rows y0..y0+ty-1 of slices z_first..z_last of one macro-cell, x over the
+// whole row.  The rows y0-1..y0+ty of a slice are contiguous in the cell array, so one bulk copy
+// fills a stage (one more copies the band of the second vector), and a slice load carries up to
+// ty x (n-1) points: the copy engine sees few large copies and the producer/consumer hand-off is
+// paid a few times per band rather than per 64-point tile.  Consumer warp w serves band row
+// w mod ty and every (8/ty)-th 32-lane x chunk; all 15 stencil values are read from the three
+// resident slices (z-1, z, z+1) in shared memory, so slice z-1 is released after step z and a ring
+// of kRStages keeps two slices in flight.  ty is the largest of 8, 4, 2, 1 whose ring fits the
+// shared-memory budget for the level's row length and the value type.  Waits are bounded as in the
+// tiled sweep.
+// ---------------------------------------------------------------------------------------------
+constexpr int    kRStages   = 5;
+constexpr size_t kRSmemMax  = 110 * 1024;  // two blocks per SM
+
+template < typename T >
+__host__ __device__ constexpr int64_t zrow_src_cap( int n, int ty )
+{
+   return ( int64_t( ty + 2 ) * ( n + 1 ) + 2 * ( 16 / int( sizeof( T ) ) ) + 15 ) / 16 * 16;
+}
+template < typename T >
+__host__ __device__ constexpr int64_t zrow_aux_cap( int n, int ty )
+{
+   return ( int64_t( ty ) * ( n + 1 ) + 2 * ( 16 / int( sizeof( T ) ) ) + 15 ) / 16 * 16;
+}
+template < typename T, bool AUX >
+static int zrow_band_h( int n )
+{
+   for ( int h = 3; h >= 0; --h )
+   {
+      const int64_t stage = zrow_src_cap< T >( n, 1 << h ) + ( AUX ? zrow_aux_cap< T >( n, 1 << h ) : 0 );
+      if ( size_t( kRStages ) * size_t( stage ) * sizeof( T ) <= kRSmemMax ) return h;
+   }
+   return -1;
+}
+
+// offset of row y of slice z from the start of row 0 of slice z: cidx(0, y, z) - cidx(0, 0, z)
+__device__ __forceinline__ int64_t row_off( int n, int y, int z ) { return int64_t( y ) * ( n + 2 - z ) - int64_t( y ) * ( y + 1 ) / 2; }
+
+template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zrow( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
+                                                               const T* __restrict__ v1, T* v2, T* dst, A a0, A a1, int nC, int h,
+                                                               int64_t src_cap, int64_t stage, int* err )
+{
+   constexpr bool AUX = zstream_aux< OP >();
+   constexpr int  AL  = 16 / int( sizeof( T ) );
+   constexpr int  S   = kRStages;
+   extern __shared__ __align__( 128 ) unsigned char zr_raw[];
+   T*                  ring = reinterpret_cast< T* >( zr_raw );
+   __shared__ uint64_t full[S], empty[S];
+   __shared__ uint32_t shw[S];  // source shift | second-vector shift << 8
+   __shared__ int      abort_flag;
+   const int           warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n = v.n;
+   const int*          rb   = v.rbegin[h];
+   const int4*         ru   = v.runits[h];
+   const int           u0 = rb[blockIdx.x], u1 = rb[blockIdx.x + 1];
+   if ( threadIdx.x == 0 )
+   {
+      for ( int s = 0; s < S; ++s )
+      {
+         mbar_init( &full[s], 1 );
+         mbar_init( &empty[s], kZWarps );
+      }
+      abort_flag = 0;
+      asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
+   }
+   __syncthreads();
+   volatile int* abrt = &abort_flag;
+
+   if ( warp >= kZWarps )
+   {
+      // producers: lane 0 of producer warp p issues the loads l with l % kZProducers == p
+      const int me = warp - kZWarps;
+      if ( lane != 0 ) return;
+      const T* aux = ( OP == OP_CHEBI || OP == OP_CHEBL ) ? v2 : ( OP == OP_APPLY_ADD ? dst : v1 );
+      int      ld  = 0;
+      bool     ok  = true;
+      for ( int c = 0; c < nC && ok; ++c )
+      {
+         if ( !( v.cell_bc[c] & flag ) ) continue;
+         const int64_t cb = v.cell_off[c];
+         for ( int u = u0; u < u1 && ok; ++u )
+         {
+            const int4 U = ru[u];  // ty, y0, z_first, z_last
+            for ( int zz = U.z - 1; zz <= U.w + 1; ++zz, ++ld )
+            {
+               if ( ld % kZProducers != me ) continue;
+               const int st = ld % S;
+               if ( ld >= S && !mbar_wait_bounded( &empty[st], uint32_t( ( ld / S - 1 ) & 1 ), abrt ) )
+               {
+                  ok = false;
+                  break;
+               }
+               const int64_t slice = cidx( n, 0, 0, zz );
+               const int     ya = U.y - 1, yb = min( U.y + U.x, n - zz );  // rows ya..yb of the slice
+               const int64_t s0 = slice + row_off( n, ya, zz ), e1 = slice + row_off( n, yb + 1, zz );
+               const int     sh = int( s0 & ( AL - 1 ) );
+               const int64_t a0 = s0 - sh;
+               uint32_t      bytes = uint32_t( ( ( e1 + AL - 1 ) / AL * AL - a0 ) * int64_t( sizeof( T ) ) );
+               uint32_t      abytes = 0;
+               int64_t       aa0    = 0;
+               int           ash    = 0;
+               if ( AUX && zz >= U.z && zz <= U.w && U.y <= n - 2 - zz )
+               {
+                  const int     ye = min( U.y + U.x - 1, n - 2 - zz );  // interior rows of the band
+                  const int64_t t0 = slice + row_off( n, U.y, zz ), t1 = slice + row_off( n, ye + 1, zz );
+                  ash              = int( t0 & ( AL - 1 ) );
+                  aa0              = t0 - ash;
+                  abytes           = uint32_t( ( ( t1 + AL - 1 ) / AL * AL - aa0 ) * int64_t( sizeof( T ) ) );
+               }
+               shw[st] = uint32_t( sh ) | ( uint32_t( ash ) << 8 );
+               mbar_expect_tx( &full[st], bytes + abytes );
+               T* sbase = ring + st * stage;
+               bulk_copy_g2s( sbase, src + cb + a0, bytes, &full[st] );
+               if ( abytes ) bulk_copy_g2s( sbase + src_cap, aux + cb + aa0, abytes, &full[st] );
+            }
+         }
+      }
+      if ( !ok )
+      {
+         atomicExch( err, 1 );
+         *abrt = 1;
+      }
+      for ( int s = me; s < S && s < ld; s += kZProducers )
+      {
+         const int j = s + ( ( ld - 1 - s ) / S ) * S;
+         if ( !mbar_wait_bounded( &full[s], uint32_t( ( j / S ) & 1 ), nullptr ) ) atomicExch( err, 1 );
+      }
+      return;
+   }
+
+   // consumers
+   __shared__ A wsm[kZWarps][16];
+   auto fail = [&]() {
+      if ( lane == 0 )
+      {
+         atomicExch( err, 1 );
+         *abrt = 1;
+      }
+   };
+   auto wait_load = [&]( int l ) { return mbar_wait_bounded( &full[l % S], uint32_t( ( l / S ) & 1 ), abrt ); };
+   auto release   = [&]( int l ) {
+      __syncwarp();
+      if ( lane == 0 ) mbar_arrive( &empty[l % S] );
+   };
+   int ld = 0;
+   for ( int c = 0; c < nC; ++c )
+   {
+      if ( !( v.cell_bc[c] & flag ) ) continue;
+      const int64_t base = v.cell_off[c];
+      A*            w    = wsm[warp];
+      __syncwarp();
+      if ( lane < kNumDirs ) w[lane] = o.W[size_t( c ) * kNumClasses * kNumDirs + lane];
+      if ( lane == kNumDirs ) w[kNumDirs] = o.invd_c[c];
+      __syncwarp();
+      for ( int u = u0; u < u1; ++u )
+      {
+         const int4 U  = ru[u];
+         const int  ty = U.x, r = warp % ty, q = warp / ty, xs = 32 * ( kZWarps / ty );
+         const int  y  = U.y + r;
+         if ( !wait_load( ld ) || !wait_load( ld + 1 ) ) return fail();
+         for ( int z = U.z; z <= U.w; ++z )
+         {
+            const int lm = ld + ( z - U.z ), l0 = lm + 1, lp = lm + 2;
+            if ( !wait_load( lp ) ) return fail();
+            if ( y <= n - 2 - z )
+            {
+               // stage pointers to row y' of slices z-1, z, z+1 (x = 0 at the returned address)
+               auto row = [&]( int l, int zz, int yy ) -> const T* {
+                  const T* sb = ring + ( l % S ) * stage;
+                  return sb + int( shw[l % S] & 0xffu ) + ( row_off( n, yy, zz ) - row_off( n, U.y - 1, zz ) );
+               };
+               const T* Rm0 = row( lm, z - 1, y );
+               const T* Rm1 = row( lm, z - 1, y + 1 );
+               const T* Rs  = row( l0, z, y - 1 );
+               const T* R0  = row( l0, z, y );
+               const T* Rn  = row( l0, z, y + 1 );
+               const T* Rps = row( lp, z + 1, y - 1 );
+               const T* Rp0 = row( lp, z + 1, y );
+               const T* Ra  = nullptr;
+               if constexpr ( AUX )
+                  Ra = ring + ( l0 % S ) * stage + src_cap + int( shw[l0 % S] >> 8 ) + ( row_off( n, y, z ) - row_off( n, U.y, z ) );
+               const int64_t obase = base + cidx( n, 0, y, z );
+               for ( int x = 1 + lane + 32 * q; x <= n - 1 - y - z; x += xs )
+               {
+                  A s0 = w[0] * A( R0[x] ), s1 = w[5] * A( Rm0[x] ), s2 = w[10] * A( Rm0[x + 1] );
+                  s0 += w[1] * A( R0[x - 1] );
+                  s1 += w[6] * A( Rp0[x] );
+                  s2 += w[11] * A( Rps[x] );
+                  s0 += w[2] * A( R0[x + 1] );
+                  s1 += w[7] * A( Rn[x - 1] );
+                  s2 += w[12] * A( Rm1[x] );
+                  s0 += w[3] * A( Rs[x] );
+                  s1 += w[8] * A( Rs[x + 1] );
+                  s2 += w[13] * A( Rps[x + 1] );
+                  s0 += w[4] * A( Rn[x] );
+                  s1 += w[9] * A( Rp0[x - 1] );
+                  s2 += w[14] * A( Rm1[x - 1] );
+                  const A acc  = s0 + ( s1 + s2 );
+                  A       auxv = A( 0 );
+                  if constexpr ( AUX ) auxv = A( Ra[x] );
+                  zstream_epilogue< T, A, OP >( obase + x, acc, w[kNumDirs], A( R0[x] ), auxv, v2, dst, a0, a1 );
+               }
+            }
+            release( lm );  // slice z-1 is no longer needed
+         }
+         release( ld + ( U.w - U.z ) + 1 );  // slice z_last
+         release( ld + ( U.w - U.z ) + 2 );  // slice z_last + 1
+         ld += U.w - U.z + 3;
+      }
+   }
+}
+
 template < typename T, typename A, int OP >
 static void zstream_attribute()
 {
+   check_cuda( cudaFuncSetAttribute( k_cell_zrow< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize, int( kRSmemMax ) ),
+               "cudaFuncSetAttribute(full-row sweep shared memory)" );
    check_cuda( cudaFuncSetAttribute( k_cell_zstream< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      int( ZCfg< T, zstream_aux< OP >() >::smem_bytes ) ),
                "cudaFuncSetAttribute(z-stream shared memory)" );
@@ -751,7 +977,9 @@ static int cell_kernel_variant()
    if ( v < 0 )
    {
       const char* e = getenv( "HYB_CELL_KERNEL" );
-      v             = ( e && std::string( e ) == "rows" ) ? 0 : ( e && std::string( e ) == "march" ) ? 1 : 2;
+      // default: the tiled z-stream sweep; "zrow" selects the full-row sweep (measured slower on the
+      // level-8 cube: 0.187 vs 0.134 ms per FP64 apply), "march" and "rows" the register sweeps
+      v = ( e && std::string( e ) == "rows" ) ? 0 : ( e && std::string( e ) == "march" ) ? 1 : ( e && std::string( e ) == "zrow" ) ? 3 : 2;
    }
    return v;
 }
@@ -830,7 +1058,17 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
    T*       v2  = (T*) a.v2;
    T*       dst = (T*) a.dst;
    Fork     fk( ctx );
-   if ( cell_kernel_variant() == 2 && v.n >= 32 && v.nzblocks[ZCfg< T, false >::wi] > 0 && nC > 0 )
+   const int zh = ( cell_kernel_variant() == 3 && v.n >= 32 ) ? zrow_band_h< T, zstream_aux< OP >() >( v.n ) : -1;
+   if ( zh >= 0 && v.nrblocks[zh] > 0 && nC > 0 )
+   {
+      const int64_t scap  = zrow_src_cap< T >( v.n, 1 << zh );
+      const int64_t stage = scap + ( zstream_aux< OP >() ? zrow_aux_cap< T >( v.n, 1 << zh ) : 0 );
+      const size_t  smem  = size_t( kRStages ) * size_t( stage ) * sizeof( T );
+      k_cell_zrow< T, A, OP ><<< v.nrblocks[zh], kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ),
+                                                                                  A( a.a1 ), nC, zh, scap, stage, ctx->d_error );
+      ++ctx->launches;
+   }
+   else if ( cell_kernel_variant() >= 2 && v.n >= 32 && v.nzblocks[ZCfg< T, false >::wi] > 0 && nC > 0 )
    {
       constexpr size_t smem = ZCfg< T, zstream_aux< OP >() >::smem_bytes;  // attribute set by ensure_constants
       k_cell_zstream< T, A, OP ><<< v.nzblocks[ZCfg< T, false >::wi], kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ),

@@ -359,6 +359,60 @@ void build_zunits( P1Level& P, int nblocks, int wi )
    }
 }
 
+// Work units of the full-row sweep: the rows y0..y0+ty-1 (interior rows only) of slices
+// z_first..z_last, ty = 1 << h; chunking of the slice range and longest-first assignment as for the
+// tiled sweep.
+void build_runits( P1Level& P, int nblocks, int h )
+{
+   const int n = P.n, ty = 1 << h;
+   auto&     units = P.runits[h];
+   auto&     begin = P.rbegin[h];
+   units.clear();
+   begin.assign( 1, 0 );
+   if ( n < 4 ) return;
+   struct Unit
+   {
+      std::array< int, 4 > u;
+      int64_t              work;
+   };
+   auto make = [&]( int zc ) {
+      std::vector< Unit > us;
+      for ( int y0 = 1; y0 <= n - 3; y0 += ty )
+      {
+         const int zmax = n - 2 - y0;
+         for ( int za = 1; za <= zmax; za += zc )
+         {
+            const int zb = std::min( zmax, za + zc - 1 );
+            int64_t   w  = 0;
+            for ( int z = za; z <= zb; ++z )
+               for ( int y = y0; y < y0 + ty; ++y ) w += std::max( 0, n - 1 - y - z );
+            us.push_back( { { ty, y0, za, zb }, w } );
+         }
+      }
+      return us;
+   };
+   int                 zc = 32;
+   std::vector< Unit > us = make( zc );
+   while ( zc > 4 && 2 * int64_t( us.size() ) < int64_t( nblocks ) ) us = make( zc /= 2 );
+   std::stable_sort( us.begin(), us.end(), []( const Unit& a, const Unit& b ) { return a.work > b.work; } );
+   const int nb = std::max( 1, std::min( nblocks, int( us.size() ) ) );
+   std::vector< std::vector< std::array< int, 4 > > >                                       per( nb );
+   std::priority_queue< std::pair< int64_t, int >, std::vector< std::pair< int64_t, int > >, std::greater<> > heap;
+   for ( int b = 0; b < nb; ++b ) heap.push( { 0, b } );
+   for ( const Unit& u : us )
+   {
+      auto [load, b] = heap.top();
+      heap.pop();
+      per[b].push_back( u.u );
+      heap.push( { load + u.work, b } );
+   }
+   for ( int b = 0; b < nb; ++b )
+   {
+      for ( const auto& u : per[b] ) units.push_back( u );
+      begin.push_back( int( units.size() ) );
+   }
+}
+
 void ensure_device( Mesh* m, P1Level& P )
 {
    if ( P.d_off ) return;
@@ -385,6 +439,15 @@ void ensure_device( Mesh* m, P1Level& P )
    int dev = 0, sms = 0;
    check_cuda( cudaGetDevice( &dev ), "cudaGetDevice" );
    check_cuda( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev ), "device attribute" );
+   for ( int h = 0; h < 4; ++h )
+   {
+      build_runits( P, 2 * std::max( sms, 1 ), h );
+      const auto&         U = P.runits[h];
+      std::vector< int4 > ru( U.size() );
+      for ( size_t i = 0; i < ru.size(); ++i ) ru[i] = make_int4( U[i][0], U[i][1], U[i][2], U[i][3] );
+      up( &P.d_runits[h], ru.data(), ru.size() );
+      up( &P.d_rbegin[h], P.rbegin[h].data(), P.rbegin[h].size() );
+   }
    for ( int wi = 0; wi < 2; ++wi )
    {
       build_zunits( P, 2 * std::max( sms, 1 ), wi );
@@ -437,6 +500,7 @@ Mesh::~Mesh()
       cudaFree( P.d_rows );
       cudaFree( P.d_march );
       for ( int wi = 0; wi < 2; ++wi ) cudaFree( P.d_zunits[wi] ), cudaFree( P.d_zbegin[wi] );
+      for ( int h = 0; h < 4; ++h ) cudaFree( P.d_runits[h] ), cudaFree( P.d_rbegin[h] );
       cudaFree( P.d_bc );
       cudaFree( P.d_bkind );
       cudaFree( P.d_ncell_cls );
