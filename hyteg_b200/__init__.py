@@ -125,6 +125,9 @@ _SIGS = {
     "hyb_fn_fill_random": (C.c_int, [C.c_void_p, C.c_int, C.c_uint64]),
     "hyb_op_store_element_matrices": (C.c_int, [C.c_void_p]),
     "hyb_fn_create_p2": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "hyb_p2_layout_sizes": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "hyb_p2_fn_download_reference": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "hyb_p2_fn_upload_reference": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "hyb_op_create_p2_divkgrad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                             C.POINTER(C.c_void_p)]),
     "hyb_fn_dot_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.POINTER(C.c_double)]),
@@ -478,6 +481,24 @@ class P2Function(P1Function):
 
     _lshift = 1
     _create = "hyb_fn_create_p2"
+
+    def reference_layout_sizes(self, level):
+        """(vertex-DoF values, edge-DoF values) of the reference's P2Function memory of `level`."""
+        v, e = C.c_int64(), C.c_int64()
+        _check(lib().hyb_p2_layout_sizes(self.storage.h, level, C.byref(v), C.byref(e)))
+        return v.value, e.value
+
+    def download_reference(self, level):
+        """The vertex-DoF part followed by the edge-DoF part, in the reference's memory layout."""
+        a = np.zeros(sum(self.reference_layout_sizes(level)), dtype=np.float64)
+        _check(lib().hyb_p2_fn_download_reference(self.h, level, _ptr(a)))
+        return a
+
+    def upload_reference(self, level, values):
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        if a.size != sum(self.reference_layout_sizes(level)):
+            raise ValueError("vector has the wrong size for the reference P2 layout of this level")
+        _check(lib().hyb_p2_fn_upload_reference(self.h, level, _ptr(a)))
 
 
 class P2ElementwiseBlendingDivKGradOperator(_ConstantOperator):

@@ -535,6 +535,146 @@ int hyb_fn_download( hyb_fn* fn, int level, double* host_packed )
 }
 
 // L: the caller's level (translated to the storage level here)
+// ---------------------------------------------------------------------------------------------
+// P2 functions in the reference's own packed layout: the vertex-DoF arrays of level l (the P1
+// layout, hyb_layout_*), then every primitive's edge-DoF array (EdgeDoFFunction.cpp:1642-1690 sizes;
+// own DoFs at the front: macroedge::index, macroface::index blocks X, XY, Y, macrocell blocks X, Y,
+// Z, XY, XZ, YZ, XYZ, EdgeDoFIndexing.hpp:363-373,579-611,922-985).  Every DoF sits on the node set of
+// level l+1 where it is stored: vertex DoF v at 2v, the edge DoF of micro-edge (v, v+d) at 2v+d.
+// Ghost-layer entries are not maintained and export as zero.
+// ---------------------------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+int64_t edge_dof_size( const Topology& t, int kind, int id, int n )
+{
+   const auto tri  = []( int64_t w ) { return w * ( w + 1 ) / 2; };
+   const auto tetw = []( int64_t w ) { return w * ( w + 1 ) * ( w + 2 ) / 6; };
+   if ( kind == 0 ) return int64_t( t.v_edges[id].size() + t.v_faces[id].size() );
+   if ( kind == 1 )
+   {
+      const int64_t nf = int64_t( t.e_faces[id].size() ), nc = int64_t( t.e_cells[id].size() );
+      return n == 1 ? 1 + 2 * nf + nc : n + nf * ( 3 * n - 1 ) + nc * ( 7 * n - 7 );
+   }
+   if ( kind == 2 )
+   {
+      const int64_t nc = int64_t( t.f_cells[id].size() );
+      return 3 * tri( n ) + ( nc ? nc * ( 3 * tri( n ) + tri( n - 1 ) + 3 * tri( n - 1 ) ) : 0 );
+   }
+   return 6 * tetw( n ) + tetw( n - 1 );
+}
+
+// visit every own edge DoF of primitive (kind, id) of level l (n = 2^l micro-edges per macro-edge):
+// f(index in the primitive's edge-DoF array, storage-local coordinates on level l+1)
+template < typename F >
+void for_edge_dofs( int kind, int n, F&& f )
+{
+   if ( kind == 1 )
+      for ( int x = 0; x < n; ++x ) f( int64_t( x ), 2 * x + 1, 0, 0 );
+   else if ( kind == 2 )
+   {
+      const int64_t ts = int64_t( n ) * ( n + 1 ) / 2;
+      for ( int y = 0; y < n; ++y )
+         for ( int x = 0; x + y < n; ++x )
+         {
+            const int64_t k = fidx( n - 1, x, y );
+            f( k, 2 * x + 1, 2 * y, 0 );               // X
+            f( ts + k, 2 * x + 1, 2 * y + 1, 0 );      // XY
+            f( 2 * ts + k, 2 * x, 2 * y + 1, 0 );      // Y
+         }
+   }
+   else if ( kind == 3 )
+   {
+      const int64_t tb = tet_size( n );
+      for ( int z = 0; z < n; ++z )
+         for ( int y = 0; y + z < n; ++y )
+            for ( int x = 0; x + y + z < n; ++x )
+            {
+               const int64_t k = cidx( n - 1, x, y, z );
+               f( k, 2 * x + 1, 2 * y, 2 * z );                  // X
+               f( tb + k, 2 * x, 2 * y + 1, 2 * z );             // Y
+               f( 2 * tb + k, 2 * x, 2 * y, 2 * z + 1 );         // Z
+               f( 3 * tb + k, 2 * x + 1, 2 * y + 1, 2 * z );     // XY
+               f( 4 * tb + k, 2 * x + 1, 2 * y, 2 * z + 1 );     // XZ
+               f( 5 * tb + k, 2 * x, 2 * y + 1, 2 * z + 1 );     // YZ
+               if ( x + y + z < n - 1 ) f( 6 * tb + cidx( n - 2, x, y, z ), 2 * x + 1, 2 * y + 1, 2 * z + 1 );  // XYZ
+            }
+   }
+}
+
+// vertex DoFs of the P1 layout of level l: f(index in the primitive's array, storage-local coordinates)
+template < typename F >
+void for_vertex_dofs( int kind, int n, F&& f )
+{
+   if ( kind == 0 ) f( int64_t( 0 ), 0, 0, 0 );
+   else if ( kind == 1 )
+      for ( int x = 0; x <= n; ++x ) f( int64_t( x ), 2 * x, 0, 0 );
+   else if ( kind == 2 )
+      for ( int y = 0; y <= n; ++y )
+         for ( int x = 0; x + y <= n; ++x ) f( fidx( n, x, y ), 2 * x, 2 * y, 0 );
+   else
+      for ( int z = 0; z <= n; ++z )
+         for ( int y = 0; y + z <= n; ++y )
+            for ( int x = 0; x + y + z <= n; ++x ) f( cidx( n, x, y, z ), 2 * x, 2 * y, 2 * z );
+}
+
+int64_t storage_slot( const P1Level& S, int p, int kind, int X, int Y, int Z )
+{
+   const int ns = S.n;
+   if ( kind == 0 ) return S.off[p];
+   if ( kind == 1 ) return S.off[p] + X;
+   if ( kind == 2 ) return S.off[p] + fidx( ns, X, Y );
+   return S.off[p] + cidx( ns, X, Y, Z );
+}
+
+// Slot holding the value of the node at storage-local coordinates (X, Y, Z) of primitive (kind, id).
+// Only cell arrays keep copies of every node of their closure, so a lower-dimensional primitive reads
+// it from its first neighbour cell: the node's integer barycentric weights on the primitive's
+// vertices become cell-local coordinates.
+int64_t closure_slot( const Topology& t, const P1Level& S, int kind, int id, int X, int Y, int Z )
+{
+   const int ns = S.n;
+   const int cellbase = t.nV + t.nE + t.nF;
+   if ( kind == 3 ) return S.off[cellbase + id] + cidx( ns, X, Y, Z );
+   int gv[3], w[3], nv = 0;
+   int c = -1;
+   if ( kind == 0 )
+   {
+      gv[0] = id, w[0] = ns, nv = 1;
+      c     = t.v_cells[id].empty() ? -1 : t.v_cells[id][0];
+   }
+   else if ( kind == 1 )
+   {
+      gv[0] = t.ev[id][0], w[0] = ns - X, gv[1] = t.ev[id][1], w[1] = X, nv = 2;
+      c = t.e_cells[id].empty() ? -1 : t.e_cells[id][0];
+   }
+   else
+   {
+      gv[0] = t.fv[id][0], w[0] = ns - X - Y, gv[1] = t.fv[id][1], w[1] = X, gv[2] = t.fv[id][2], w[2] = Y, nv = 3;
+      c = t.f_cells[id].empty() ? -1 : t.f_cells[id][0];
+   }
+   require( c >= 0, "primitive without a neighbour cell" );
+   int xyz[3] = { 0, 0, 0 };
+   for ( int i = 0; i < nv; ++i )
+      for ( int d = 1; d < 4; ++d )
+         if ( t.cv[c][d] == gv[i] ) xyz[d - 1] = w[i];
+   return S.off[cellbase + c] + cidx( ns, xyz[0], xyz[1], xyz[2] );
+}
+
+// (kind, id, global primitive index p) in the packed order: vertices, edges, faces, cells
+template < typename F >
+void for_primitives( const Topology& t, F&& f )
+{
+   int p = 0;
+   for ( int i = 0; i < t.nV; ++i ) f( 0, i, p++ );
+   for ( int i = 0; i < t.nE; ++i ) f( 1, i, p++ );
+   for ( int i = 0; i < t.nF; ++i ) f( 2, i, p++ );
+   for ( int i = 0; i < t.nC; ++i ) f( 3, i, p++ );
+}
+}  // namespace
+
+extern "C" {
+
 static void pointwise( hyb_fn* dst, int L, uint32_t flag, int op, int n, const double* sc, hyb_fn* const* srcs )
 {
    L = lv( dst, L );
@@ -569,6 +709,65 @@ static void pointwise( hyb_fn* dst, int L, uint32_t flag, int op, int n, const d
    a.a1   = n > 1 ? sc[1] : 0.0;
    a.a2   = n > 2 ? sc[2] : 0.0;
    launch_point( &dst->ctx->c, dst->f.mesh, L, dst->f.dtype, a );
+}
+
+int hyb_p2_layout_sizes( hyb_mesh* mesh, int level, int64_t* vertex_part, int64_t* edge_part )
+{
+   HYB_TRY
+   require( mesh && vertex_part && edge_part, "NULL argument" );
+   require( level >= 0 && level <= 13, "invalid level" );
+   *vertex_part = mesh->m.level( level ).packed_size;
+   int64_t e    = 0;
+   for_primitives( mesh->m.topo, [&]( int kind, int id, int ) { e += edge_dof_size( mesh->m.topo, kind, id, 1 << level ); } );
+   *edge_part = e;
+   HYB_CATCH
+}
+
+int hyb_p2_fn_download_reference( hyb_fn* fn, int level, double* out )
+{
+   HYB_TRY
+   require( fn && out, "NULL argument" );
+   require( fn->f.lshift == 1, "not a P2 function" );
+   require_level( fn->f, level + 1 );
+   const Topology& t  = fn->f.mesh->topo;
+   const P1Level&  V  = fn->f.mesh->level( level );      // packed vertex-DoF layout of level l
+   const P1Level&  S  = fn->f.mesh->level( level + 1 );  // storage
+   const int       n  = 1 << level;
+   const auto      st = from_device( fn, level + 1 );
+   std::fill( out, out + V.packed_size, 0.0 );
+   int64_t eoff = V.packed_size;
+   for_primitives( t, [&]( int kind, int id, int p ) {
+      const int64_t vb = V.packed_off[p];
+      for_vertex_dofs( kind, n, [&]( int64_t k, int X, int Y, int Z ) { out[vb + k] = st[closure_slot( t, S, kind, id, X, Y, Z )]; } );
+      const int64_t es = edge_dof_size( t, kind, id, n );
+      std::fill( out + eoff, out + eoff + es, 0.0 );
+      for_edge_dofs( kind, n, [&]( int64_t k, int X, int Y, int Z ) { out[eoff + k] = st[closure_slot( t, S, kind, id, X, Y, Z )]; } );
+      eoff += es;
+   } );
+   HYB_CATCH
+}
+
+int hyb_p2_fn_upload_reference( hyb_fn* fn, int level, const double* in )
+{
+   HYB_TRY
+   require( fn && in, "NULL argument" );
+   require( fn->f.lshift == 1, "not a P2 function" );
+   require_level( fn->f, level + 1 );
+   const Topology& t = fn->f.mesh->topo;
+   const P1Level&  V = fn->f.mesh->level( level );
+   const P1Level&  S = fn->f.mesh->level( level + 1 );
+   const int       n = 1 << level;
+   std::vector< double > st( S.size, 0.0 );
+   int64_t               eoff = V.packed_size;
+   for_primitives( t, [&]( int kind, int id, int p ) {
+      const int64_t vb = V.packed_off[p];
+      for_vertex_dofs( kind, n, [&]( int64_t k, int X, int Y, int Z ) { st[storage_slot( S, p, kind, X, Y, Z )] = in[vb + k]; } );
+      for_edge_dofs( kind, n, [&]( int64_t k, int X, int Y, int Z ) { st[storage_slot( S, p, kind, X, Y, Z )] = in[eoff + k]; } );
+      eoff += edge_dof_size( t, kind, id, n );
+   } );
+   to_device( fn, level + 1, st );
+   sync_copies( fn, level + 1 );  // copies in the cell and face arrays take their owners' values
+   HYB_CATCH
 }
 
 int hyb_fn_interpolate_const( hyb_fn* fn, double value, int level, uint32_t flag )

@@ -144,6 +144,19 @@ int hyb_fn_create( hyb_ctx* ctx, hyb_mesh* mesh, int dtype, int min_level, int m
  * l+1, so every hyb_fn_* / hyb_op_* / solver call takes the P2 level and packed uploads and downloads
  * use the vertex-DoF layout of level l+1 (hyb_layout_packed_size( mesh, l+1 ) values). */
 int hyb_fn_create_p2( hyb_ctx* ctx, hyb_mesh* mesh, int dtype, int min_level, int max_level, hyb_fn** out );
+/* A P2 function of level l in the reference's own memory layout (P2Function = VertexDoFFunction +
+ * EdgeDoFFunction, p2functionspace/P2Function.hpp:35-60): first the vertex-DoF arrays of level l in
+ * the packed order of hyb_layout_* (`vertex_part` values), then the edge-DoF array of every primitive
+ * in the order vertices, edges, faces, cells (`edge_part` values; per-primitive sizes
+ * edgeDoFMacro{Vertex,Edge,Face,Cell}FunctionMemorySize, edgedofspace/EdgeDoFFunction.cpp:1642-1690).
+ * Inside a primitive's edge-DoF array the own DoFs come first in the reference's order
+ * (edgedof::macroedge::index, macroface::index blocks X, XY, Y, macrocell::xIndex ... xyzIndex,
+ * edgedofspace/EdgeDoFIndexing.hpp:361-366,579-594,922-980); the ghost layers that follow (and a
+ * vertex's whole edge-DoF array) are communication buffers: download writes them as zero and upload
+ * ignores them.  Upload then refreshes every copy of an owned DoF from its owner. */
+int hyb_p2_layout_sizes( hyb_mesh* mesh, int level, int64_t* vertex_part, int64_t* edge_part );
+int hyb_p2_fn_download_reference( hyb_fn* fn, int level, double* out );
+int hyb_p2_fn_upload_reference( hyb_fn* fn, int level, const double* in );
 int hyb_fn_destroy( hyb_fn* fn );
 /* host <-> device in the packed layout; host values are doubles.  Upload refreshes every copy of
  * an owned DoF from its owner (communicate). */

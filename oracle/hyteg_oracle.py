@@ -1223,3 +1223,74 @@ class P2Transfer(Transfer):
         for L in range(op.minL + 1, op.maxL + 1):
             self.P[L] = p2_prolongation_matrix(op.levels[L - 1], op.levels[L])
             self.R[L] = self.P[L].T.tocsr()
+
+
+# ---------------------------------------------------------------------------------------------
+# the reference's P2Function memory layout (VertexDoFFunction + EdgeDoFFunction of level l)
+# ---------------------------------------------------------------------------------------------
+
+def edgedof_memory_sizes(mesh: MacroMesh, L: int):
+    """Per-primitive edge-DoF array sizes in the order vertices, edges, faces, cells
+    (edgeDoFMacro{Vertex,Edge,Face,Cell}FunctionMemorySize, EdgeDoFFunction.cpp:1642-1690)."""
+    n = 1 << L
+    out = [len(mesh.v_edges[v]) + len(mesh.v_faces[v]) for v in range(mesh.nV)]
+    for e in range(mesh.nE):
+        nf, nc = len(mesh.e_faces[e]), len(mesh.e_cells[e])
+        out.append(1 + 2 * nf + nc if L == 0 else n + nf * (3 * n - 1) + nc * (7 * n - 7))
+    for f in range(mesh.nF):
+        ghost = 3 * tri_size(n) + tri_size(n - 1) + 3 * tri_size(n - 1)
+        out.append(3 * tri_size(n) + len(mesh.f_cells[f]) * ghost)
+    out += [6 * tet_size(n) + tet_size(n - 1)] * mesh.nC
+    return out
+
+
+def p2_reference_dof_coords(mesh: MacroMesh, L: int):
+    """Physical coordinates (k, 3) of every entry of the reference's P2 memory of level L: the
+    vertex-DoF arrays (P1 layout, closure entries) then the edge-DoF arrays (own micro-edge
+    midpoints: edgedof::macroedge::index, macroface::index X / XY / Y, macrocell::xIndex..xyzIndex,
+    EdgeDoFIndexing.hpp:361-366,579-594,922-980).  Ghost-layer entries are NaN."""
+    n = 1 << L
+    lev = Level(mesh, L)
+    X = mesh.vcoords
+    vpart = np.full((lev.size, 3), np.nan)
+    for v in range(mesh.nV):
+        vpart[lev.off_v[v]] = X[v]
+    for e, (a, b) in enumerate(mesh.edges):
+        t = np.arange(n + 1)[:, None] / n
+        vpart[lev.off_e[e] + np.arange(n + 1)] = X[a] + t * (X[b] - X[a])
+    for f, (a, b, c) in enumerate(mesh.faces):
+        for j in range(n + 1):
+            for i in range(n + 1 - j):
+                vpart[lev.off_f[f] + face_index(n, i, j)] = X[a] + i / n * (X[b] - X[a]) + j / n * (X[c] - X[a])
+    for c in range(mesh.nC):
+        pts = tet_points(n + 1)
+        vpart[lev.off_c[c] + cell_index(n, pts[:, 0], pts[:, 1], pts[:, 2])] = lev.coords(c, pts[:, 0], pts[:, 1], pts[:, 2])
+    sizes = edgedof_memory_sizes(mesh, L)
+    epart = np.full((sum(sizes), 3), np.nan)
+    base = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    p = mesh.nV
+    for e, (a, b) in enumerate(mesh.edges):
+        t = (np.arange(n)[:, None] + 0.5) / n
+        epart[base[p + e] + np.arange(n)] = X[a] + t * (X[b] - X[a])
+    p += mesh.nE
+    ts = tri_size(n)
+    for f, (a, b, c) in enumerate(mesh.faces):
+        for y in range(n):
+            for x in range(n - y):
+                k = base[p + f] + face_index(n - 1, x, y)
+                for blk, (dx, dy) in enumerate(((0.5, 0.0), (0.5, 0.5), (0.0, 0.5))):  # X, XY, Y
+                    epart[k + blk * ts] = X[a] + (x + dx) / n * (X[b] - X[a]) + (y + dy) / n * (X[c] - X[a])
+    p += mesh.nF
+    tb = tet_size(n)
+    shifts = ((0.5, 0, 0), (0, 0.5, 0), (0, 0, 0.5), (0.5, 0.5, 0), (0.5, 0, 0.5), (0, 0.5, 0.5))  # X Y Z XY XZ YZ
+    for c in range(mesh.nC):
+        pts = tet_points(n)
+        k = base[p + c] + cell_index(n - 1, pts[:, 0], pts[:, 1], pts[:, 2])
+        for blk, d in enumerate(shifts):
+            q = pts + np.array(d)
+            epart[k + blk * tb] = lev.coords(c, q[:, 0], q[:, 1], q[:, 2])
+        if n > 1:
+            pts = tet_points(n - 1)
+            q = pts + 0.5
+            epart[base[p + c] + 6 * tb + cell_index(n - 2, pts[:, 0], pts[:, 1], pts[:, 2])] = lev.coords(c, q[:, 0], q[:, 1], q[:, 2])
+    return np.concatenate([vpart, epart])

@@ -155,3 +155,30 @@ def test_p2_gmg_chebyshev_factors(ctx, case):
     np.testing.assert_allclose(got[0], hist[0], rtol=1e-12)
     np.testing.assert_allclose(got[1:] / got[:-1], hist[1:] / hist[:-1], rtol=0, atol=1e-6)
     assert _relerr(fx.download(L), xs[L], lev.owned_mask(O.ALL)) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["cube_6", "octahedron_8"])
+@pytest.mark.parametrize("L", [0, 1, 3])
+def test_p2_reference_layout_download_upload(ctx, name, L):
+    """hyb_p2_fn_download_reference puts every DoF where the reference's P2Function memory keeps it
+    (the oracle gives each entry's coordinates), writes ghost entries as zero, and upload_reference
+    restores the function bit for bit."""
+    coords, tets = M.ALL[name]()
+    om = O.MacroMesh(coords, tets)
+    pm = H.PrimitiveStorage.from_tets(coords, tets, ctx)
+    f = lambda x, y, z: 1.0 + 0.5 * x - 2.0 * y * y + 3.0 * x * z + 0.25 * np.sin(3.0 * x + 7.0 * y - 5.0 * z)
+    u = H.P2Function("u", pm, L, L, ctx)
+    u.interpolate(f, L)
+    got = u.download_reference(L)
+    X = O.p2_reference_dof_coords(om, L)
+    assert got.size == X.shape[0] == sum(u.reference_layout_sizes(L))
+    own = ~np.isnan(X[:, 0])
+    np.testing.assert_allclose(got[own], f(X[own, 0], X[own, 1], X[own, 2]), rtol=0, atol=1e-14)
+    assert not got[~own].any()
+    w = H.P2Function("w", pm, L, L, ctx)
+    w.upload_reference(L, got)
+    lev1 = O.Level(om, L + 1)  # storage: owned slots and their copies in the cell arrays
+    keep = lev1.owned_mask(O.ALL)
+    keep[lev1.copy_map()[0]] = True
+    np.testing.assert_array_equal(w.download(L)[keep], u.download(L)[keep])
+    np.testing.assert_array_equal(w.download_reference(L), got)

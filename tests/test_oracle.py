@@ -282,3 +282,29 @@ def test_p2_operator_and_transfer_properties(name):
         Ac = op.A[L - 1][ownc][:, ownc]
         Pf = Pm[ownf][:, ownc]
         assert abs(Pf.T @ op.A[L][ownf][:, ownf] @ Pf - Ac).max() < 1e-13 * abs(Ac).max()
+
+
+@pytest.mark.parametrize("name", ["cube_6", "octahedron_8", "tilted_tet"])
+def test_p2_reference_layout_covers_every_node(name):
+    """The reference's P2 memory of level L (vertex-DoF arrays + edge-DoF arrays) addresses exactly
+    the nodes of level L+1: every non-ghost entry is a node, and every node has an entry."""
+    coords, tets = M.ALL[name]()
+    mesh = O.MacroMesh(coords, tets)
+    for L in (0, 1, 2):
+        X = O.p2_reference_dof_coords(mesh, L)
+        lev1 = O.Level(mesh, L + 1)
+        nodes = _slot_coords(lev1)[lev1.owned_mask(O.ALL)]
+        key = lambda A: {tuple(r) for r in np.round(A, 12)}
+        assert key(X[~np.isnan(X[:, 0])]) == key(nodes)
+        assert len(key(nodes)) == len(nodes)
+
+
+def test_p2_reference_edgedof_sizes_example():
+    """The layout example of edgedof::macroface::index (EdgeDoFIndexing.hpp:598-611): at level 2 a
+    face with one neighbour cell holds 30 own entries and 54 ghost entries."""
+    coords, tets = M.ALL["tilted_tet"]()
+    mesh = O.MacroMesh(coords, tets)
+    sizes = O.edgedof_memory_sizes(mesh, 2)
+    assert sizes[mesh.nV + mesh.nE: mesh.nV + mesh.nE + mesh.nF] == [84] * mesh.nF
+    assert sizes[-1] == 6 * 20 + 10  # cell: 6 tet(4) + tet(3)
+    assert sizes[mesh.nV] == 4 + 2 * 11 + 1 * 21  # edge of one cell, two faces: n + nf(3n-1) + nc(7n-7)
