@@ -122,10 +122,12 @@ struct P1Level {
    // y-marching work items of the cell stencil sweep: (z, x0, y_first, y_last); a warp covers
    // x0..x0+31 of slice z and marches over rows y_first..y_last
    std::vector< std::array< int, 4 > > march;
-   // z-streamed sweep: units {x0, y0, z_first, z_last}, each a kZTileX x kZTileY tile of slice
-   // columns over a range of slices; block b of the sweep runs units zbegin[b]..zbegin[b+1]-1
-   // (assigned longest-first to the least loaded block)
+   // z-streamed sweep: units {x0, y0, z_first, z_last} of macro-cell zcell[i], each a kZTileX x
+   // kZTileY tile of slice columns over a range of slices; block b of the sweep runs units
+   // zbegin[b]..zbegin[b+1]-1 (the units of all cells, assigned longest-first to the least loaded
+   // block)
    std::vector< std::array< int, 4 > > zunits[2];  // per tile width kZWidths[w]
+   std::vector< int >                  zcell[2];
    std::vector< int >                  zbegin[2];
    // full-row sweep: units {ty, y0, z_first, z_last} (rows y0..y0+ty-1 of slices z_first..z_last),
    // one list per band height ty = 1 << h (h = 0..3), blocks as for zunits
@@ -140,6 +142,7 @@ struct P1Level {
    int2*      d_rows      = nullptr;
    int4*      d_march     = nullptr;
    int4*      d_zunits[2] = { nullptr, nullptr };
+   int*       d_zcell[2]  = { nullptr, nullptr };
    int*       d_zbegin[2] = { nullptr, nullptr };
    int4*      d_runits[4] = {};
    int*       d_rbegin[4] = {};
@@ -320,7 +323,7 @@ void launch_cg_scalar( Context* ctx, double* state, int stage, double rtol, doub
 void check_cuda( cudaError_t e, const char* what );
 void build_level( Mesh* m, int L );
 void ensure_device( Mesh* m, P1Level& P );
-void build_zunits( P1Level& P, int nblocks, int w );
+void build_zunits( P1Level& P, int nblocks, int w, int ncells );
 void build_runits( P1Level& P, int nblocks, int h );
 void build_operator_level( Operator* A, int L );
 void ensure_device_op( OpLevel& ol );

@@ -116,6 +116,7 @@ struct LevelView
    const int*       rbegin[4];
    int              nzblocks[2];  // per tile width kZWidths[w]
    const int4*      zunits[2];
+   const int*       zcell[2];
    const int*       zbegin[2];
 };
 
@@ -157,6 +158,7 @@ static LevelView make_view( Mesh* m, int L )
    {
       v.nzblocks[wi] = int( P.zbegin[wi].size() ) - 1;
       v.zunits[wi]   = P.d_zunits[wi];
+      v.zcell[wi]    = P.d_zcell[wi];
       v.zbegin[wi]   = P.d_zbegin[wi];
    }
    return v;
@@ -469,6 +471,7 @@ __device__ __forceinline__ void zstream_produce( const LevelView& v, uint32_t fl
    const int     lane = threadIdx.x & 31, n = v.n, me = ( threadIdx.x >> 5 ) - kZWarps;
    const int*    zb = v.zbegin[Cfg::wi];
    const int4*   zu = v.zunits[Cfg::wi];
+   const int*    zcl = v.zcell[Cfg::wi];
    const int     u0 = zb[blockIdx.x], u1 = zb[blockIdx.x + 1];
    const bool    is_src = lane < Cfg::rows, is_aux = AUX && lane >= Cfg::rows && lane < Cfg::rows + kZTileY;
    const int     dsto   = is_src ? lane * Cfg::RW : Cfg::aux0 + ( lane - Cfg::rows ) * Cfg::RWA;
@@ -476,12 +479,12 @@ __device__ __forceinline__ void zstream_produce( const LevelView& v, uint32_t fl
    const int     shbit  = is_src ? 3 * lane : ( is_aux ? 3 * ( lane - Cfg::rows ) : 0 );
    int           ld = 0;  // sequence number of the next slice load
    bool          ok = true;
-   for ( int c = 0; c < nC && ok; ++c )
    {
-      if ( !( v.cell_bc[c] & flag ) ) continue;
-      const int64_t cb = v.cell_off[c];
       for ( int u = u0; u < u1 && ok; ++u )
       {
+         const int c = zcl[u];
+         if ( c >= nC || !( v.cell_bc[c] & flag ) ) continue;
+         const int64_t cb = v.cell_off[c];
          const int4 U  = zu[u];  // x0, y0, z_first, z_last
          const int  yy = is_src ? U.y - 1 + lane : U.y + ( lane - Cfg::rows );
          const int  xa = is_src ? U.x - 1 : U.x;  // first x of the row segment
@@ -601,6 +604,7 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, O
    constexpr int kZPts = Cfg::pts;
    const int*    zb    = v.zbegin[Cfg::wi];
    const int4*   zu    = v.zunits[Cfg::wi];
+   const int*    zcl   = v.zcell[Cfg::wi];
    const int     u0 = zb[blockIdx.x], u1 = zb[blockIdx.x + 1];
    const int rS = warp, rC = warp + 1, rN = warp + 2;  // rows y-1, y, y+1 of the stage
    auto at = [&]( const T* st, uint32_t word, int r, int k, int dx ) -> A {
@@ -614,19 +618,24 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, O
       }
    };
    int ld = 0;
-   for ( int c = 0; c < nC; ++c )
+   // the weights are read from shared memory at every use (broadcast, shared by the lane's points)
+   // rather than held in 30 registers
+   A* w = wsm[warp];
+   int cw = -1;  // cell whose weights are in w
    {
-      if ( !( v.cell_bc[c] & flag ) ) continue;
-      const int64_t base = v.cell_off[c];
-      // the weights are read from shared memory at every use (broadcast, shared by the lane's
-      // points) rather than held in 30 registers
-      A* w = wsm[warp];
-      __syncwarp();
-      if ( lane < kNumDirs ) w[lane] = o.W[size_t( c ) * kNumClasses * kNumDirs + lane];  // interior class 0
-      if ( lane == kNumDirs ) w[kNumDirs] = o.invd_c[c];
-      __syncwarp();
       for ( int u = u0; u < u1; ++u )
       {
+         const int c = zcl[u];
+         if ( c >= nC || !( v.cell_bc[c] & flag ) ) continue;
+         const int64_t base = v.cell_off[c];
+         if ( c != cw )
+         {
+            __syncwarp();
+            if ( lane < kNumDirs ) w[lane] = o.W[size_t( c ) * kNumClasses * kNumDirs + lane];  // interior class 0
+            if ( lane == kNumDirs ) w[kNumDirs] = o.invd_c[c];
+            __syncwarp();
+            cw = c;
+         }
          const int4 U = zu[u];
          const int  x = U.x + lane, y = U.y + warp;
          // prologue: slice z_first-1 (load ld) and slice z_first (load ld+1)

@@ -305,14 +305,16 @@ void build_level( Mesh* m, int L )
 // per two blocks (every chunk re-reads two halo slices, and every slice load costs a fixed hand-off,
 // so long chunks win over finer balance); units are then handed out longest-first to the least
 // loaded block.
-void build_zunits( P1Level& P, int nblocks, int wi )
+void build_zunits( P1Level& P, int nblocks, int wi, int ncells )
 {
    const int n = P.n, kZTileX = kZWidths[wi];
    auto&     zunits = P.zunits[wi];
+   auto&     zcell  = P.zcell[wi];
    auto&     zbegin = P.zbegin[wi];
    zunits.clear();
+   zcell.clear();
    zbegin.assign( 1, 0 );
-   if ( n < 4 ) return;
+   if ( n < 4 || ncells < 1 ) return;
    struct Unit
    {
       std::array< int, 4 > u;
@@ -336,25 +338,34 @@ void build_zunits( P1Level& P, int nblocks, int wi )
          }
       return us;
    };
+   // longest slice ranges that still give every block about two units (all cells together)
    int                 zc = 32;
    std::vector< Unit > us = make( zc );
-   while ( zc > 8 && 2 * int64_t( us.size() ) < int64_t( nblocks ) ) us = make( zc /= 2 );
+   while ( zc > 8 && 2 * int64_t( us.size() ) * ncells < int64_t( nblocks ) ) us = make( zc /= 2 );
    if ( const char* e = getenv( "HYB_ZCHUNK" ); e && atoi( e ) > 0 ) us = make( atoi( e ) );
    std::stable_sort( us.begin(), us.end(), []( const Unit& a, const Unit& b ) { return a.work > b.work; } );
-   const int nb = std::max( 1, std::min( nblocks, int( us.size() ) ) );
-   std::vector< std::vector< std::array< int, 4 > > >                                       per( nb );
+   const int64_t items = int64_t( us.size() ) * ncells;
+   const int     nb    = int( std::max< int64_t >( 1, std::min< int64_t >( nblocks, items ) ) );
+   std::vector< std::vector< std::pair< int, int > > >                                      per( nb );  // (cell, unit)
    std::priority_queue< std::pair< int64_t, int >, std::vector< std::pair< int64_t, int > >, std::greater<> > heap;
    for ( int b = 0; b < nb; ++b ) heap.push( { 0, b } );
-   for ( const Unit& u : us )
-   {
-      auto [load, b] = heap.top();
-      heap.pop();
-      per[b].push_back( u.u );
-      heap.push( { load + u.work, b } );
-   }
+   for ( size_t k = 0; k < us.size(); ++k )  // longest first; the cells of one unit shape in turn
+      for ( int c = 0; c < ncells; ++c )
+      {
+         auto [load, b] = heap.top();
+         heap.pop();
+         per[b].push_back( { c, int( k ) } );
+         heap.push( { load + us[k].work, b } );
+      }
    for ( int b = 0; b < nb; ++b )
    {
-      for ( const auto& u : per[b] ) zunits.push_back( u );
+      // cell-major inside a block: a warp reloads its cell's weights only when the cell changes
+      std::stable_sort( per[b].begin(), per[b].end(), []( const auto& a, const auto& b ) { return a.first < b.first; } );
+      for ( const auto& cu : per[b] )
+      {
+         zunits.push_back( us[cu.second].u );
+         zcell.push_back( cu.first );
+      }
       zbegin.push_back( int( zunits.size() ) );
    }
 }
@@ -450,11 +461,12 @@ void ensure_device( Mesh* m, P1Level& P )
    }
    for ( int wi = 0; wi < 2; ++wi )
    {
-      build_zunits( P, 2 * std::max( sms, 1 ), wi );
+      build_zunits( P, 2 * std::max( sms, 1 ), wi, t.nC );
       const auto&         U = P.zunits[wi];
       std::vector< int4 > zu( U.size() );
       for ( size_t i = 0; i < zu.size(); ++i ) zu[i] = make_int4( U[i][0], U[i][1], U[i][2], U[i][3] );
       up( &P.d_zunits[wi], zu.data(), zu.size() );
+      up( &P.d_zcell[wi], P.zcell[wi].data(), P.zcell[wi].size() );
       up( &P.d_zbegin[wi], P.zbegin[wi].data(), P.zbegin[wi].size() );
    }
    std::vector< uint8_t > bc( nP );
@@ -499,7 +511,7 @@ Mesh::~Mesh()
       cudaFree( P.d_tasks );
       cudaFree( P.d_rows );
       cudaFree( P.d_march );
-      for ( int wi = 0; wi < 2; ++wi ) cudaFree( P.d_zunits[wi] ), cudaFree( P.d_zbegin[wi] );
+      for ( int wi = 0; wi < 2; ++wi ) cudaFree( P.d_zunits[wi] ), cudaFree( P.d_zcell[wi] ), cudaFree( P.d_zbegin[wi] );
       for ( int h = 0; h < 4; ++h ) cudaFree( P.d_runits[h] ), cudaFree( P.d_rbegin[h] );
       cudaFree( P.d_bc );
       cudaFree( P.d_bkind );
