@@ -1725,6 +1725,23 @@ int hyb_gmg_set_radii( hyb_gmg* g, const double* radii )
    HYB_CATCH
 }
 
+// the setup a solver derives from its operator alone (Chebyshev radii, coarse iteration cap),
+// copied to another solver of the same operator kind, level range and precision: the copy skips the
+// power iterations and the coarse probe and runs the same cycles bit for bit
+int hyb_internal_gmg_copy_setup( hyb_gmg* dst, const hyb_gmg* src )
+{
+   HYB_TRY
+   require( dst && src, "NULL argument" );
+   require( dst->p.min_level == src->p.min_level && dst->p.max_level == src->p.max_level, "level ranges differ" );
+   if ( !src->radii.empty() )
+   {
+      dst->radii = src->radii;
+      set_coefficients( dst );
+   }
+   dst->coarse_cap = src->coarse_cap;
+   HYB_CATCH
+}
+
 int hyb_gmg_get_radii( hyb_gmg* g, double* radii )
 {
    HYB_TRY

@@ -214,6 +214,10 @@ struct ElemLevel {
    // stored element matrices (computeAndStoreLocalElementMatrices): the 10 upper-triangle entries
    // of every micro-cell's 4x4 matrix, value-major, in double ([0]) and float ([1])
    void* d_K[2] = { nullptr, nullptr };
+   // P1 operators with stored matrices keep them assembled: the 15 stencil weights of every
+   // cell-array slot (the partial stencil of that cell at copies of face/edge/vertex DoFs),
+   // weight-major over the level's slots, in double ([0]) and float ([1])
+   void* d_S[2] = { nullptr, nullptr };
 };
 
 struct Operator {

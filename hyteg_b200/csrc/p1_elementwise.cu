@@ -219,6 +219,13 @@ __constant__ int c_mc_off[6][4][3] = {
     { { 1, 0, 0 }, { 0, 1, 0 }, { 1, 0, 1 }, { 0, 0, 1 } }, { { 1, 1, 0 }, { 1, 1, 1 }, { 0, 1, 1 }, { 1, 0, 1 } },
     { { 1, 0, 1 }, { 0, 1, 1 }, { 0, 0, 1 }, { 0, 1, 0 } }, { { 0, 1, 0 }, { 1, 1, 0 }, { 1, 0, 1 }, { 0, 1, 1 } } };
 __constant__ int c_mc_shift[6] = { 0, 1, 1, 2, 1, 1 };
+// stencil direction (index into kVarDirs) from vertex i to vertex j of micro-cell type ty
+__constant__ int8_t c_mc_dir[6][4][4];
+// the 15 stencil directions in the order of the constant-stencil weights
+static const int kVarDirs[15][3] = { { 0, 0, 0 },  { -1, 0, 0 }, { 1, 0, 0 },  { 0, -1, 0 }, { 0, 1, 0 },
+                                     { 0, 0, -1 }, { 0, 0, 1 },  { -1, 1, 0 }, { 1, -1, 0 }, { -1, 0, 1 },
+                                     { 1, 0, -1 }, { 0, -1, 1 }, { 0, 1, -1 }, { 1, -1, 1 }, { -1, 1, -1 } };
+__constant__ int8_t c_var_dir[15][3];
 
 __device__ __forceinline__ double ld_any( const double* p ) { return *p; }
 __device__ __forceinline__ float  ld_any( const float* p ) { return *p; }
@@ -230,7 +237,8 @@ __device__ __forceinline__ void   st_any( __half* p, float v ) { *p = __float2ha
 // One parity pass: warp per half-grid row (y, z) of anchors with y = py mod 2, z = pz mod 2, lanes
 // over x = px + 2k.  MODE 0 accumulates A src, MODE 1 the diagonal.
 // MODE 0: y += K x with K computed on the fly; 1: diagonal of K; 2: compute K and store its upper
-// triangle; 3: y += K x with K read from storage.  Stored entry v of micro-cell (cell c, type ty,
+// triangle; 3: y += K x with K read from storage; 4: add K into the assembled stencils of the
+// cell-array slots of its vertices (kst = stencils, kstride = level size).  Stored entry v of micro-cell (cell c, type ty,
 // anchor a) sits at kst[v * kstride + (c * 6 + ty) * tet(n) + cidx(n - 1, a)].
 template < typename T, typename A, int MODE >
 __global__ void __launch_bounds__( 256 ) k_elem_pass( int n, int nanch, const int* __restrict__ anch, const int64_t* __restrict__ cell_off,
@@ -265,7 +273,7 @@ __global__ void __launch_bounds__( 256 ) k_elem_pass( int n, int nanch, const in
          // self-check: every node inside the level's vector and every stored slot inside its array;
          // a violation is recorded (error word 2) and the micro-cell skipped
          {
-            bool bad = ( MODE >= 2 ) && ( slot < 0 || slot >= kstride );
+            bool bad = ( MODE == 2 || MODE == 3 ) && ( slot < 0 || slot >= kstride );
             for ( int m = 0; m < 4; ++m ) bad |= idx[m] < 0 || idx[m] >= level_size;
             if ( bad )
             {
@@ -298,6 +306,9 @@ __global__ void __launch_bounds__( 256 ) k_elem_pass( int n, int nanch, const in
          }
          else if constexpr ( MODE == 1 )
             for ( int i = 0; i < 4; ++i ) acc[idx[i]] += K[i][i];
+         else if constexpr ( MODE == 4 )
+            for ( int i = 0; i < 4; ++i )
+               for ( int j = 0; j < 4; ++j ) kst[int64_t( c_mc_dir[ty][i][j] ) * kstride + idx[i]] += K[i][j];
       }
 }
 
@@ -679,6 +690,102 @@ __global__ void __launch_bounds__( 256 ) k_bnd_acc( int n, int ntasks, const int
    }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Assembled stencils (P1 operators with stored matrices): A src at cell-local (x, y, z) of a cell is
+// sum_d S_d(slot) src(x + dir_d), S_d the sum of the element-matrix entries of the cell's micro-cells
+// that couple the point with its neighbour in direction d (the same sum the elementwise apply forms,
+// P1ElementwiseOperator.cpp:169-260, taken once at setup instead of every apply).  One read of 15
+// weights per point replaces the 6 micro-cells x 10 entries an elementwise sweep reads.
+// ---------------------------------------------------------------------------------------------
+template < typename T, typename A, bool INTERIOR >
+__device__ __forceinline__ A var_apply( const A* __restrict__ S, int64_t ssize, const T* __restrict__ src, int64_t base, int n, int x,
+                                        int y, int z )
+{
+   const int64_t slot = base + cidx( n, x, y, z );
+   A             acc  = A( 0 );
+#pragma unroll
+   for ( int d = 0; d < 15; ++d )
+   {
+      const int dx = c_var_dir[d][0], dy = c_var_dir[d][1], dz = c_var_dir[d][2];
+      const int xx = x + dx, yy = y + dy, zz = z + dz;
+      if ( !INTERIOR && ( xx < 0 || yy < 0 || zz < 0 || xx + yy + zz > n ) ) continue;
+      acc += S[d * ssize + slot] * A( ld_any( src + base + cidx( n, xx, yy, zz ) ) );
+   }
+   return acc;
+}
+
+template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( 256 ) k_var_cell( int n, int nrows, const int2* __restrict__ rows, const int64_t* __restrict__ cell_off,
+                                                      const uint8_t* __restrict__ cell_bc, uint32_t flag, const A* __restrict__ S,
+                                                      int64_t ssize, const A* __restrict__ invd, const T* src, const T* v1, T* v2, T* dst,
+                                                      A a0, A a1 )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int r    = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   if ( r >= nrows || !( cell_bc[c] & flag ) ) return;
+   const int2    yz   = rows[r];
+   const int64_t cb   = cell_off[c];
+   const int64_t base = cb + cidx( n, 0, yz.x, yz.y );
+   for ( int x = 1 + lane; x <= n - 1 - yz.x - yz.y; x += 32 )
+   {
+      const int64_t i = base + x;
+      A             second;
+      const A       s   = var_apply< T, A, true >( S, ssize, src, cb, n, x, yz.x, yz.y );
+      const A       val = epilogue_value< T, A, OP >( i, s, invd[i], src, v1, v2, a0, a1, &second );
+      if constexpr ( OP == OP_CHEBL ) st_any( v2 + i, val );
+      else if constexpr ( OP == OP_APPLY_ADD ) st_any( dst + i, A( ld_any( dst + i ) ) + val );
+      else
+      {
+         st_any( dst + i, val );
+         if constexpr ( OP == OP_CHEBI ) st_any( v2 + i, second );
+      }
+   }
+}
+
+template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( 256 ) k_var_bnd( int n, int ntasks, const int4* __restrict__ tasks, const int64_t* __restrict__ off,
+                                                     const int64_t* __restrict__ cell_off, const int8_t* __restrict__ bkind,
+                                                     const uint8_t* __restrict__ bc, const int* __restrict__ inc_begin,
+                                                     const Incidence* __restrict__ inc, uint32_t flag, int copy_unflagged,
+                                                     const A* __restrict__ S, int64_t ssize, const A* __restrict__ invd, const T* src,
+                                                     const T* v1, T* v2, T* dst, A a0, A a1 )
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( t >= ntasks ) return;
+   const int4    tk    = tasks[t];
+   const int     b     = tk.x;
+   const int     k     = bkind[b];
+   const int64_t owner = off[b] + ( k == 0 ? 0 : ( k == 1 ? int64_t( tk.y ) : fidx( n, tk.y, tk.z ) ) );
+   if ( !( bc[b] & flag ) )
+   {
+      if ( !copy_unflagged ) return;
+      if constexpr ( OP == OP_JAC || OP == OP_CHEB0 )
+         wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, A( ld_any( src + owner ) ) );
+      else if constexpr ( OP == OP_CHEBI ) wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, A( ld_any( v2 + owner ) ) );
+      return;
+   }
+   A s = A( 0 );
+   for ( int q = inc_begin[b]; q < inc_begin[b + 1]; ++q )
+   {
+      const Incidence I = inc[q];
+      const int       x = n * I.o[0] + tk.y * I.e1[0] + tk.z * I.e2[0];
+      const int       y = n * I.o[1] + tk.y * I.e1[1] + tk.z * I.e2[1];
+      const int       z = n * I.o[2] + tk.y * I.e1[2] + tk.z * I.e2[2];
+      s += var_apply< T, A, false >( S, ssize, src, cell_off[I.cell], n, x, y, z );
+   }
+   A       second;
+   const A val = epilogue_value< T, A, OP >( owner, s, invd[owner], src, v1, v2, a0, a1, &second );
+   if constexpr ( OP == OP_CHEBL ) wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, v2, val );
+   else if constexpr ( OP == OP_APPLY_ADD )
+      wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, A( ld_any( dst + owner ) ) + val );
+   else
+   {
+      wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, val );
+      if constexpr ( OP == OP_CHEBI ) wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, v2, second );
+   }
+}
+
 template < typename A >
 __global__ void k_cell_invert( int n, int nrows, const int2* __restrict__ rows, const int64_t* __restrict__ cell_off, const A* acc,
                                A* invd )
@@ -712,6 +819,38 @@ static A* acc_buffer( Operator* op, int L, int64_t size )
    }
    return reinterpret_cast< A* >( e.d_acc );
 }
+
+// stencil direction of every vertex pair of every micro-cell type (vertex offsets as c_mc_off)
+static void ensure_var_tables()
+{
+   static bool done = false;
+   if ( done ) return;
+   static const int off[6][4][3] = {
+       { { 0, 0, 0 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } }, { { 1, 0, 0 }, { 1, 1, 0 }, { 0, 1, 0 }, { 1, 0, 1 } },
+       { { 1, 0, 0 }, { 0, 1, 0 }, { 1, 0, 1 }, { 0, 0, 1 } }, { { 1, 1, 0 }, { 1, 1, 1 }, { 0, 1, 1 }, { 1, 0, 1 } },
+       { { 1, 0, 1 }, { 0, 1, 1 }, { 0, 0, 1 }, { 0, 1, 0 } }, { { 0, 1, 0 }, { 1, 1, 0 }, { 1, 0, 1 }, { 0, 1, 1 } } };
+   int8_t dir[6][4][4], vd[15][3];
+   for ( int d = 0; d < 15; ++d )
+      for ( int k = 0; k < 3; ++k ) vd[d][k] = int8_t( kVarDirs[d][k] );
+   for ( int t = 0; t < 6; ++t )
+      for ( int i = 0; i < 4; ++i )
+         for ( int j = 0; j < 4; ++j )
+         {
+            int found = -1;
+            for ( int d = 0; d < 15; ++d )
+               if ( off[t][j][0] - off[t][i][0] == kVarDirs[d][0] && off[t][j][1] - off[t][i][1] == kVarDirs[d][1] &&
+                    off[t][j][2] - off[t][i][2] == kVarDirs[d][2] )
+                  found = d;
+            if ( found < 0 ) throw std::runtime_error( "micro-cell edge outside the 15-point stencil" );
+            dir[t][i][j] = int8_t( found );
+         }
+   check_cuda( cudaMemcpyToSymbol( c_mc_dir, dir, sizeof( dir ) ), "upload stencil directions" );
+   check_cuda( cudaMemcpyToSymbol( c_var_dir, vd, sizeof( vd ) ), "upload stencil directions" );
+   done = true;
+}
+
+template < typename A >
+static A* assembled_stencils( Operator* op, int L ) { return reinterpret_cast< A* >( op->el[L].d_S[sizeof( A ) == 8 ? 0 : 1] ); }
 
 // micro-cells per macro-edge of the elements living on storage level L (P2 elements of level L-1
 // have their nodes on storage level L)
@@ -752,9 +891,9 @@ static void run_passes( Context* ctx, Mesh* m, Operator* op, int L, const T* src
 {
    P1Level&   P = m->level( L );
    ElemLevel& e = op->el[L];
-   if ( MODE != 2 ) check_cuda( cudaMemsetAsync( acc, 0, P.size * sizeof( A ), ctx->stream ), "cudaMemset(acc)" );
-   A*            kst = stored_matrices< A >( op, L );
-   const int64_t ks  = kstride( m, op, L );
+   if ( MODE != 2 && MODE != 4 ) check_cuda( cudaMemsetAsync( acc, 0, P.size * sizeof( A ), ctx->stream ), "cudaMemset(acc)" );
+   A*            kst = MODE == 4 ? assembled_stencils< A >( op, L ) : stored_matrices< A >( op, L );
+   const int64_t ks  = MODE == 4 ? P.size : kstride( m, op, L );
    const int nC = m->topo.nC;
    for ( int p = 0; p < 8; ++p )
    {
@@ -788,7 +927,24 @@ static void ensure_level_t( Context* ctx, Operator* op, int L, int dtype )
    ElemLevel& e = op->el[L];
    A*         acc = acc_buffer< A >( op, L, P.size );
    void*&     K   = e.d_K[sizeof( A ) == 8 ? 0 : 1];
-   if ( op->store_matrices && !K )
+   if ( op->store_matrices && op->order == 1 )
+   {
+      // P1: the stored matrices are kept assembled, summed in double once and rounded for float
+      ensure_var_tables();
+      const int64_t cnt = int64_t( 15 ) * P.size;
+      if ( !e.d_S[0] )
+      {
+         check_cuda( cudaMalloc( &e.d_S[0], cnt * sizeof( double ) ), "cudaMalloc(assembled stencils)" );
+         check_cuda( cudaMemsetAsync( e.d_S[0], 0, cnt * sizeof( double ), ctx->stream ), "cudaMemset" );
+         run_passes< double, double, 4 >( ctx, m, op, L, nullptr, nullptr );
+      }
+      if ( sizeof( A ) == 4 && !e.d_S[1] )
+      {
+         check_cuda( cudaMalloc( &e.d_S[1], cnt * sizeof( float ) ), "cudaMalloc(assembled stencils)" );
+         launch_convert( ctx, cnt, F32, e.d_S[1], F64, e.d_S[0] );
+      }
+   }
+   else if ( op->store_matrices && !K )
    {
       check_cuda( cudaMalloc( &K, size_t( element_values( op ) ) * size_t( kstride( m, op, L ) ) * sizeof( A ) ),
                   "cudaMalloc(element matrices)" );
@@ -822,8 +978,46 @@ void ensure_elementwise_level( Context* ctx, Operator* op, int L, int dtype )
 }
 
 template < typename T, typename A, int OP >
+static void run_var( Context* ctx, Mesh* m, Operator* op, int L, int dtype, const StencilArgs& a )
+{
+   P1Level& P = m->level( L );
+   const A* S   = assembled_stencils< A >( op, L );
+   const A* inv = reinterpret_cast< const A* >( op->el[L].d_invd[dtype] );
+   struct Join
+   {
+      Context* c;
+      ~Join()
+      {
+         cudaEventRecord( c->ev_join, c->aux );
+         cudaStreamWaitEvent( c->stream, c->ev_join, 0 );
+      }
+   };
+   check_cuda( cudaEventRecord( ctx->ev_fork, ctx->stream ), "fork" );
+   check_cuda( cudaStreamWaitEvent( ctx->aux, ctx->ev_fork, 0 ), "fork" );
+   Join      j{ ctx };
+   const int nrows = int( P.rows.size() );
+   if ( nrows > 0 )
+   {
+      dim3 grid( ( nrows + 7 ) / 8, m->topo.nC );
+      k_var_cell< T, A, OP ><<< grid, 256, 0, ctx->stream >>>( P.n, nrows, P.d_rows, P.d_off + P.nB, P.d_bc + P.nB, a.flag, S, P.size, inv,
+                                                                (const T*) a.src, (const T*) a.v1, (T*) a.v2, (T*) a.dst, A( a.a0 ),
+                                                                A( a.a1 ) );
+      ++ctx->launches;
+   }
+   if ( !P.tasks.empty() )
+   {
+      k_var_bnd< T, A, OP ><<< ( int( P.tasks.size() ) + 255 ) / 256, 256, 0, ctx->aux >>>(
+          P.n, int( P.tasks.size() ), P.d_tasks, P.d_off, P.d_off + P.nB, P.d_bkind, P.d_bc, P.d_inc_begin, P.d_inc, a.flag,
+          a.copy_unflagged, S, P.size, inv, (const T*) a.src, (const T*) a.v1, (T*) a.v2, (T*) a.dst, A( a.a0 ), A( a.a1 ) );
+      ++ctx->launches;
+   }
+   check_cuda( cudaGetLastError(), "assembled stencil launch" );
+}
+
+template < typename T, typename A, int OP >
 static void run_elem( Context* ctx, Mesh* m, Operator* op, int L, int dtype, const StencilArgs& a )
 {
+   if ( op->order == 1 && assembled_stencils< A >( op, L ) ) return run_var< T, A, OP >( ctx, m, op, L, dtype, a );
    P1Level& P   = m->level( L );
    A*       acc = acc_buffer< A >( op, L, P.size );
    const A* inv = reinterpret_cast< const A* >( op->el[L].d_invd[dtype] );

@@ -2,12 +2,13 @@
 //
 // A request names a resident mesh, an operator (P1 Laplace or elementwise -div(k grad u) with
 // optional shell blending), a level, a right-hand side, a tolerance and the precision mode
-// (plain FP64 cycles, or FP64 defect correction around FP32 cycles).  Requests wait in a FIFO queue
-// and are admitted into "slots" as slots and the HBM budget allow.  A slot is a resident multigrid
-// hierarchy (operator tables, functions on every level, the solver with its CUDA graph) keyed by
-// (mesh, operator, coefficient, blending, level, precision); a finished request leaves its slot
-// idle so the next request with the same key reuses it without any setup (the captured graph is
-// replayed).  Every slot owns a context with its own stream, so the cycles of different solves
+// (plain FP64 cycles, or FP64 defect correction around FP32 cycles).  Requests wait in a queue and
+// are admitted in arrival order into "slots" as slots and the HBM budget allow (a request whose key
+// has only busy slots waits for one of them and lets later requests pass).  A slot is a resident
+// multigrid hierarchy (operator tables, functions on every level, the solver with its CUDA graph)
+// keyed by (mesh, operator, coefficient, blending, level, precision); a finished request leaves its
+// slot idle so the next request with the same key reuses it without any setup (the captured graph
+// is replayed), and a further slot of a key copies the solver setup of the first.  Every slot owns a context with its own stream, so the cycles of different solves
 // overlap on the device.  Each scheduler step launches one cycle on every running slot whose last
 // residual check has come back, followed by an asynchronous residual norm (device dot, copy to
 // pinned host memory, event); finished slots are retired as their events complete.  Kernels and
@@ -83,6 +84,7 @@ struct ServeSlot
    double    bytes   = 0;
    double    last_used = 0;
    double    scale     = 1.0;  // mixed mode: residual scaling of the cycle in flight
+   bool      solved    = false;  // the solver setup (Chebyshev radii, coarse cap) exists
 };
 
 struct hyb_serve
@@ -102,6 +104,7 @@ extern "C" int hyb_internal_residual_async( hyb_op* op, hyb_fn* x, hyb_fn* b, hy
 extern "C" int hyb_internal_mixed_step_async( hyb_gmg* g, int inner_dtype, hyb_op* op, hyb_fn* x, hyb_fn* b, int level, double rn,
                                               double* d_out );
 extern "C" int hyb_fn_fill_random( hyb_fn* fn, int level, uint64_t seed );
+extern "C" int hyb_internal_gmg_copy_setup( hyb_gmg* dst, const hyb_gmg* src );
 
 static thread_local std::string s_err;
 
@@ -129,21 +132,18 @@ void free_slot( hyb_serve* s, ServeSlot* sl )
 
 // bytes a slot holds: x, b (all levels), tmp and the solver's temporaries (about six more vectors
 // per level), plus the elementwise scratch
-// (plus, for div-k-grad, the stored element matrices: 10 values per micro-cell slot and level, in
-// FP64 and for mixed slots also in FP32)
+// (plus, for div-k-grad, the stored matrices, kept as assembled stencils: 15 values per DoF slot and
+// level, in FP64 and for mixed slots also in FP32)
 double slot_bytes( ServeKey k )
 {
    int64_t total = 0;
    double  mats  = 0;
-   int     counts[4] = { 0, 0, 0, 0 };  // vertices, edges, faces, cells
-   hyb_mesh_counts( k.mesh, counts );
-   const int nC = counts[3];
    for ( int L = 0; L <= k.level; ++L )
    {
       int64_t n = 0;
       hyb_layout_packed_size( k.mesh, L, &n );
       total += n;
-      if ( k.kind == HYB_P1_ELEM_DIVKGRAD ) mats += double( nC ) * 6.0 * double( hyb::tet_size( int64_t( 1 ) << L ) ) * 10.0;
+      if ( k.kind == HYB_P1_ELEM_DIVKGRAD ) mats += double( n ) * 15.0;
    }
    return double( total ) * 8.0 * ( k.mixed ? 12.0 : 10.0 ) + mats * ( k.mixed ? 12.0 : 8.0 );
 }
@@ -174,6 +174,14 @@ ServeSlot* make_slot( hyb_serve* s, const ServeRequest& r )
    gp.cheb_power_iterations = s->p.power_iterations;
    gp.use_graph             = 1;
    ok( hyb_gmg_create( sl->ctx, sl->op, &gp, &sl->gmg ) );
+   // a second slot of a key takes the first one's solver setup instead of repeating it
+   for ( auto& up : s->slots )
+      if ( up->key == r.key && up->solved )
+      {
+         ok( hyb_internal_gmg_copy_setup( sl->gmg, up->gmg ) );
+         sl->solved = true;
+         break;
+      }
    ok( hyb_fn_create( sl->ctx, r.key.mesh, HYB_F64, 0, L, &sl->x ) );
    ok( hyb_fn_create( sl->ctx, r.key.mesh, HYB_F64, 0, L, &sl->b ) );
    ok( hyb_fn_create( sl->ctx, r.key.mesh, HYB_F64, L, L, &sl->tmp ) );
@@ -330,26 +338,36 @@ int hyb_serve_step( hyb_serve* s, int* running, int* queued )
             r.state       = ( conv && std::isfinite( rn ) ) ? 2 : 3;
             sl->req       = -1;
             sl->last_used = r.t_done;
+            sl->solved    = true;
          }
          else
             launch_cycle( s, sl, r, rn );
       }
-      // 2. admission in arrival order, as slots and the memory budget allow
-      while ( !s->queue.empty() )
+      // 2. admission in arrival order, as slots and the memory budget allow.  A request takes an idle
+      //    slot of its key, else a new slot where the budget and the slot limit leave room.  Idle
+      //    slots of other keys are evicted (least recently used first) only for a key that has no
+      //    slot at all; a request whose key has busy slots waits for one of them, and requests
+      //    behind it that can start do.
+      for ( auto qi = s->queue.begin(); qi != s->queue.end(); )
       {
-         ServeRequest& r    = s->reqs.at( s->queue.front() );
+         ServeRequest& r    = s->reqs.at( *qi );
          ServeSlot*    slot = nullptr;
+         bool          has_key = false;
          for ( auto& up : s->slots )
-            if ( up->req < 0 && up->key == r.key )
+            if ( up->key == r.key )
             {
-               slot = up.get();
-               break;
+               has_key = true;
+               if ( up->req < 0 )
+               {
+                  slot = up.get();
+                  break;
+               }
             }
          if ( !slot )
          {
             const double need = slot_bytes( r.key );
-            // evict idle slots of other keys (least recently used first) until the new one fits
-            while ( ( s->used_bytes + need > s->p.hbm_budget_bytes || int( s->slots.size() ) >= s->p.max_slots ) )
+            auto         room = [&]() { return s->used_bytes + need <= s->p.hbm_budget_bytes && int( s->slots.size() ) < s->p.max_slots; };
+            while ( !room() && !has_key )
             {
                int victim = -1;
                for ( size_t i = 0; i < s->slots.size(); ++i )
@@ -358,11 +376,15 @@ int hyb_serve_step( hyb_serve* s, int* running, int* queued )
                free_slot( s, s->slots[victim].get() );
                s->slots.erase( s->slots.begin() + victim );
             }
-            if ( s->used_bytes + need > s->p.hbm_budget_bytes || int( s->slots.size() ) >= s->p.max_slots ) break;
+            if ( !room() )
+            {
+               ++qi;
+               continue;
+            }
             slot = make_slot( s, r );
          }
          admit( s, slot, r );
-         s->queue.pop_front();
+         qi = s->queue.erase( qi );
       }
       int run = 0;
       for ( auto& up : s->slots ) run += up->req >= 0;

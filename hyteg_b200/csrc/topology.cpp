@@ -673,6 +673,7 @@ Operator::~Operator()
       cudaFree( kv.second.d_acc );
       for ( void* p : kv.second.d_invd ) cudaFree( p );
       for ( void* p : kv.second.d_K ) cudaFree( p );
+      for ( void* p : kv.second.d_S ) cudaFree( p );
       cudaFree( kv.second.d_anch );
    }
    cudaFree( d_geom );

@@ -105,11 +105,12 @@ def test_divkgrad_shell_vcycle_factors(ctx):
 
 
 @pytest.mark.parametrize("case", ["cube", "shell"])
-@pytest.mark.parametrize("dtype,tol", [("float64", 1e-13), ("float32", 1e-6)])
+@pytest.mark.parametrize("dtype,tol", [("float64", 1e-13), ("float32", 2e-6)])
 def test_divkgrad_stored_element_matrices(ctx, case, dtype, tol):
-    """computeAndStoreLocalElementMatrices: applies and smoother sweeps read the stored matrices and
-    agree with the recomputing operator (same matrices; only the mirrored lower triangle may round
-    differently)."""
+    """computeAndStoreLocalElementMatrices: applies and smoother sweeps use the stored matrices (kept
+    assembled as per-DoF stencils, summed in double) and agree with the recomputing FP64 operator on
+    the same stored input values: FP64 within 1e-13 (summation order only), FP32 within its rounding
+    of weights, input and result."""
     L = 4
     mesh = M.cube_6() if case == "cube" else O.mesh_spherical_shell(3, 2, 0.55, 1.0)
     bl = "shell" if case == "shell" else None
@@ -121,13 +122,17 @@ def test_divkgrad_stored_element_matrices(ctx, case, dtype, tol):
     fx, fb = H.P1Function("x", pm, L, L, ctx, dtype), H.P1Function("b", pm, L, L, ctx, dtype)
     fx.fill_random(L, 3)
     fb.fill_random(L, 4)
-    ya, ys = H.P1Function("ya", pm, L, L, ctx, dtype), H.P1Function("ys", pm, L, L, ctx, dtype)
+    # FP64 copies of the stored inputs: the recomputing operator in FP64 is the reference
+    gx, gb = H.P1Function("gx", pm, L, L, ctx), H.P1Function("gb", pm, L, L, ctx)
+    gx.upload(L, fx.download(L))
+    gb.upload(L, fb.download(L))
+    ya, ys = H.P1Function("ya", pm, L, L, ctx), H.P1Function("ys", pm, L, L, ctx, dtype)
     for flag in (H.Inner, H.All):
-        A.apply(fx, ya, L, flag)
+        A.apply(gx, ya, L, flag)
         S.apply(fx, ys, L, flag)
         a, s = ya.download(L), ys.download(L)
         assert np.abs(a - s).max() <= tol * np.abs(a).max()
-    A.smooth_jac(ya, fb, fx, 0.6, L, H.Inner)
+    A.smooth_jac(ya, gb, gx, 0.6, L, H.Inner)
     S.smooth_jac(ys, fb, fx, 0.6, L, H.Inner)
     a, s = ya.download(L), ys.download(L)
     assert np.abs(a - s).max() <= tol * np.abs(a).max()

@@ -101,9 +101,9 @@ def test_serve_mixed_precision_reaches_fp64_accuracy(ctx):
 
 def _slot_bytes(pm, L, divkgrad):
     """The server's footprint estimate of a plain slot: ten FP64 vectors over all levels, plus the
-    stored element matrices (10 values per micro-cell slot) of a div-k-grad operator."""
+    stored matrices of a div-k-grad operator (assembled stencils: 15 values per DoF)."""
     vec = sum(pm.packed_size(l) for l in range(L + 1)) * 8 * 10
-    mats = sum(pm.counts()[3] * 6 * ((1 << l) + 2) * ((1 << l) + 1) * (1 << l) // 6 * 10 for l in range(L + 1)) * 8
+    mats = sum(pm.packed_size(l) * 15 for l in range(L + 1)) * 8
     return vec + (mats if divkgrad else 0)
 
 
