@@ -534,7 +534,7 @@ def run_ours(args, rank, world, local):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "traffic": profile_traffic(),
                      "algorithmic_bytes_per_launch": alg_bytes,
-                     "kernel": "k_cell_zstream<double,OP_APPLY> + k_bnd_stencil (one apply)"},
+                     "kernel": "k_cell_zsum<double,OP_APPLY> + k_bnd_stencil (one apply)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": packed * 8, "d2h_bytes_per_step": packed * 8},
         "gpu_launches": launches,
         "clocks": clk.summary(),

@@ -100,11 +100,12 @@ struct Topology {
 };
 
 // per-level host + device tables of the P1 layout
-// tiles of the z-streamed cell sweep: kZTileY rows (one per warp) by 64 x-points (two per lane); the
-// second width serves 4- and 2-byte values (128-wide tiles were measured slower on the level-8 cube:
-// register spills and fewer work units)
+// tiles of the z-streamed cell sweeps, 64 x-points (two per lane) by kZHeights[t] rows: t = 0 the
+// rolled-register sweep (one row per warp), t = 1 the partial-sum sweep (two rows per warp)
+// (128-wide tiles were measured slower on the level-8 cube: register spills and fewer work units)
 constexpr int kZTileY = 8;
-constexpr int kZWidths[2] = { 64, 64 };
+constexpr int kZWidths[2]  = { 64, 64 };
+constexpr int kZHeights[2] = { 8, 16 };
 
 struct P1Level {
    int     L = 0, n = 0;

@@ -19,6 +19,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 
 namespace hyb {
 
@@ -342,7 +343,7 @@ __global__ void __launch_bounds__( 256 ) k_cell_march( LevelView v, OpView< A > 
 
 
 // ---------------------------------------------------------------------------------------------
-// z-streamed cell sweep (cp.async.bulk + mbarrier ring), the default for n >= 32.
+// Rolled-register z-streamed cell sweep (cp.async.bulk + mbarrier ring; HYB_CELL_KERNEL=zstream).
 //
 // A unit is the tile x0..x0+63, y0..y0+7 of slices z_first..z_last of one macro-cell.  A producer
 // warp streams the tile's rows of every slice, with a one-point halo in x and y, into a ring of
@@ -434,7 +435,7 @@ __host__ __device__ constexpr bool zstream_aux()
 template < typename T, bool AUX >
 struct ZCfg
 {
-   static constexpr int wi      = sizeof( T ) == 8 ? 0 : 1;                      // tile width index
+   static constexpr int wi      = 0;                                            // tile table index
    static constexpr int kZTileX = kZWidths[wi];                                 // x-points per tile row
    static constexpr int pts     = kZTileX / 32;                                 // x-points per consumer lane
    static constexpr int al    = 16 / int( sizeof( T ) );                         // elements per 16 bytes
@@ -725,6 +726,271 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, O
 }
 
 // ---------------------------------------------------------------------------------------------
+// Partial-sum z-streamed cell sweep (the default for levels with n >= 32).
+//
+// Same units, ring, producers and bounded waits as the rolled sweep, with tiles of 64 x-points by
+// 16 rows (two rows per consumer warp, two x-points per lane: four points per lane per slice).
+// Each slice s is read once, at seven positions around each point, and gives three partial sums:
+// the top terms of point s-1 (which completes it and writes the result), the middle terms of
+// point s and the bottom terms of point s+1.  A point carries two running sums (plus its centre
+// value and second-vector value for the smoother epilogues) from slice to slice instead of eight
+// rolled source values, and a stage is released as soon as it has been read.
+// ---------------------------------------------------------------------------------------------
+constexpr int kZSRows = 2;  // tile rows per consumer warp
+
+template < typename T, bool AUX >
+struct ZSCfg
+{
+   static constexpr int wi    = 1;                                             // tile table index
+   static constexpr int TX    = kZWidths[wi];                                  // x-points per tile row
+   static constexpr int TY    = kZHeights[wi];                                 // tile rows
+   static constexpr int pts   = TX / 32;                                       // x-points per lane and row
+   static constexpr int al    = 16 / int( sizeof( T ) );                       // elements per 16 bytes
+   static constexpr int RW    = ( TX + 2 + 2 * al + al - 1 ) / al * al;        // source row width (elements)
+   static constexpr int RWA   = ( TX + 2 * al + al - 1 ) / al * al;            // second-vector row width
+   static constexpr int rows  = TY + 2;                                        // tile rows + halo
+   static constexpr int aux0  = rows * RW;                                     // second-vector rows start here
+   static constexpr int stage = aux0 + ( AUX ? TY * RWA : 0 );                 // elements per stage
+   static constexpr int S     = AUX ? 5 : 8;                                    // ring depth
+   static constexpr int NR    = rows + ( AUX ? TY : 0 );                        // row copies per stage
+   static constexpr size_t smem_bytes = size_t( S ) * stage * sizeof( T );
+   static_assert( kZWarps * kZSRows == TY, "two tile rows per consumer warp" );
+   static_assert( NR <= 64, "a producer lane issues at most two row copies per stage" );
+};
+
+// producer warp of the partial-sum sweep: row copy r < rows is source row y0-1+r, r >= rows is
+// second-vector row y0+(r-rows); lane l issues copies l and l+32.  Shifts are published as 3-bit
+// fields of two 64-bit words per stage (source rows, second-vector rows).
+template < typename T, bool AUX >
+__device__ __forceinline__ void zsum_produce( const LevelView& v, uint32_t flag, const T* __restrict__ src, const T* __restrict__ aux,
+                                              int nC, T* ring, uint64_t* full, uint64_t* empty, unsigned long long* shw,
+                                              volatile int* abort_flag, int* err )
+{
+   using Cfg = ZSCfg< T, AUX >;
+   constexpr int S = Cfg::S, AL = Cfg::al, TX = Cfg::TX;
+   const int     lane = threadIdx.x & 31, n = v.n, me = ( threadIdx.x >> 5 ) - kZWarps;
+   const int*    zb  = v.zbegin[Cfg::wi];
+   const int4*   zu  = v.zunits[Cfg::wi];
+   const int*    zcl = v.zcell[Cfg::wi];
+   const int     u0 = zb[blockIdx.x], u1 = zb[blockIdx.x + 1];
+   int           ld = 0;
+   bool          ok = true;
+   for ( int u = u0; u < u1 && ok; ++u )
+   {
+      const int c = zcl[u];
+      if ( c >= nC || !( v.cell_bc[c] & flag ) ) continue;
+      const int64_t cb = v.cell_off[c];
+      const int4    U  = zu[u];  // x0, y0, z_first, z_last
+      for ( int zz = U.z - 1; zz <= U.w + 1; ++zz, ++ld )
+      {
+         if ( ld % kZProducers != me ) continue;
+         const int st = ld % S;
+         if ( ld >= S && !mbar_wait_bounded( &empty[st], uint32_t( ( ld / S - 1 ) & 1 ), abort_flag ) )
+         {
+            ok = false;
+            break;
+         }
+         uint32_t           bytes[2] = { 0u, 0u };
+         int64_t            a0[2]    = { 0, 0 };
+         int                dst[2]   = { 0, 0 };
+         unsigned long long w0 = 0ull, w1 = 0ull;
+#pragma unroll
+         for ( int h = 0; h < 2; ++h )
+         {
+            const int  r      = lane + 32 * h;
+            const bool is_src = r < Cfg::rows, is_aux = AUX && r >= Cfg::rows && r < Cfg::NR;
+            if ( !is_src && !is_aux ) continue;
+            const int  yy   = is_src ? U.y - 1 + r : U.y + ( r - Cfg::rows );
+            const int  xa   = is_src ? U.x - 1 : U.x;
+            const int  xe   = is_src ? min( U.x + TX, n - yy - zz ) : min( U.x + TX - 1, n - 1 - yy - zz );
+            const bool live = ( is_src && yy + zz <= n && xe >= xa ) || ( is_aux && zz >= U.z && zz <= U.w && xe >= xa );
+            dst[h]          = is_src ? r * Cfg::RW : Cfg::aux0 + ( r - Cfg::rows ) * Cfg::RWA;
+            if ( !live ) continue;
+            const int64_t rb = cidx( n, 0, yy, zz );
+            const int64_t s0 = rb + xa;
+            const int64_t e1 = rb + xe + 1;  // one past the segment
+            const uint32_t sh = uint32_t( s0 & ( AL - 1 ) );
+            a0[h]             = s0 - sh;
+            bytes[h]          = uint32_t( ( ( e1 + AL - 1 ) / AL * AL - a0[h] ) * int64_t( sizeof( T ) ) );
+            if ( is_src ) w0 |= ( unsigned long long )( sh ) << ( 3 * r );
+            else w1 |= ( unsigned long long )( sh ) << ( 3 * ( r - Cfg::rows ) );
+         }
+         const uint32_t total = __reduce_add_sync( 0xffffffffu, bytes[0] + bytes[1] );
+         const uint32_t w0lo = __reduce_or_sync( 0xffffffffu, uint32_t( w0 ) ), w0hi = __reduce_or_sync( 0xffffffffu, uint32_t( w0 >> 32 ) );
+         const uint32_t w1lo = __reduce_or_sync( 0xffffffffu, uint32_t( w1 ) ), w1hi = __reduce_or_sync( 0xffffffffu, uint32_t( w1 >> 32 ) );
+         if ( lane == 0 )
+         {
+            shw[2 * st]     = ( ( unsigned long long )( w0hi ) << 32 ) | w0lo;
+            shw[2 * st + 1] = ( ( unsigned long long )( w1hi ) << 32 ) | w1lo;
+            mbar_expect_tx( &full[st], total );
+         }
+         __syncwarp();
+#pragma unroll
+         for ( int h = 0; h < 2; ++h )
+            if ( bytes[h] )
+            {
+               const bool is_src = lane + 32 * h < Cfg::rows;
+               bulk_copy_g2s( ring + st * Cfg::stage + dst[h], ( is_src ? src : aux ) + cb + a0[h], bytes[h], &full[st] );
+            }
+      }
+   }
+   if ( !ok && lane == 0 )
+   {
+      atomicExch( err, 1 );
+      *abort_flag = 1;
+   }
+   // drain: the latest load issued on every stage has landed before the block may exit
+   if ( lane == 0 )
+      for ( int s = me; s < S && s < ld; s += kZProducers )
+      {
+         const int j = s + ( ( ld - 1 - s ) / S ) * S;
+         if ( !mbar_wait_bounded( &full[s], uint32_t( ( j / S ) & 1 ), nullptr ) ) atomicExch( err, 1 );
+      }
+}
+
+template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zsum( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
+                                                               const T* __restrict__ v1, T* v2, T* dst, A a0, A a1, int nC, int* err )
+{
+   constexpr bool AUX = zstream_aux< OP >();
+   using Cfg          = ZSCfg< T, AUX >;
+   constexpr int S = Cfg::S, RW = Cfg::RW, P = Cfg::pts;
+   extern __shared__ __align__( 128 ) unsigned char zs_raw[];
+   T*                            ring = reinterpret_cast< T* >( zs_raw );
+   __shared__ uint64_t           full[S], empty[S];
+   __shared__ unsigned long long shw[2 * S];
+   __shared__ A                  wsm[kZWarps][16];  // per consumer warp: the cell's 15 weights and 1/diagonal
+   __shared__ int                abort_flag;
+   const int                     warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n = v.n;
+   if ( threadIdx.x == 0 )
+   {
+      for ( int s = 0; s < S; ++s )
+      {
+         mbar_init( &full[s], 1 );
+         mbar_init( &empty[s], kZWarps );
+      }
+      abort_flag = 0;
+      asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
+   }
+   __syncthreads();
+   volatile int* abrt = &abort_flag;
+   if ( warp >= kZWarps )
+   {
+      const T* aux = ( OP == OP_CHEBI || OP == OP_CHEBL ) ? v2 : ( OP == OP_APPLY_ADD ? dst : v1 );
+      zsum_produce< T, AUX >( v, flag, src, aux, nC, ring, full, empty, shw, abrt, err );
+      return;
+   }
+   const int*  zb  = v.zbegin[Cfg::wi];
+   const int4* zu  = v.zunits[Cfg::wi];
+   const int*  zcl = v.zcell[Cfg::wi];
+   const int   u0 = zb[blockIdx.x], u1 = zb[blockIdx.x + 1];
+   A*          w  = wsm[warp];
+   int         cw = -1;  // cell whose weights are in w
+   int         ld = 0;   // load number of the first slice of the next unit
+   for ( int u = u0; u < u1; ++u )
+   {
+      const int c = zcl[u];
+      if ( c >= nC || !( v.cell_bc[c] & flag ) ) continue;
+      const int64_t base = v.cell_off[c];
+      if ( c != cw )
+      {
+         __syncwarp();
+         if ( lane < kNumDirs ) w[lane] = o.W[size_t( c ) * kNumClasses * kNumDirs + lane];  // interior class 0
+         if ( lane == kNumDirs ) w[kNumDirs] = o.invd_c[c];
+         __syncwarp();
+         cw = c;
+      }
+      const int4 U = zu[u];
+      const int  x = U.x + lane;
+      // running sums of the point (x + 32 k, y_j) with y_j = U.y + 2 warp + j: acc of the point being
+      // completed, bot (bottom terms) of the next one; cen / axv: centre and second-vector value
+      A       acc[kZSRows][P], bot[kZSRows][P], cen[kZSRows][P], axv[kZSRows][P];
+      int64_t out[kZSRows];  // offset of (x, y_j, z) of the point being completed
+#pragma unroll
+      for ( int j = 0; j < kZSRows; ++j )
+      {
+         out[j] = base + cidx( n, x, U.y + kZSRows * warp + j, U.z );
+#pragma unroll
+         for ( int k = 0; k < P; ++k ) acc[j][k] = bot[j][k] = cen[j][k] = axv[j][k] = A( 0 );
+      }
+      // fold slice s (load number l) into the sums: FIN completes point s-1 with the top terms,
+      // MID starts point s, BOT gives the bottom terms of point s+1
+      auto step = [&]( int l, int s, auto fin_c, auto mid_c, auto bot_c ) -> bool {
+         constexpr bool FIN = decltype( fin_c )::value, MID = decltype( mid_c )::value, BOT = decltype( bot_c )::value;
+         const int      st  = l % S;
+         if ( !mbar_wait_bounded( &full[st], uint32_t( ( l / S ) & 1 ), abrt ) ) return false;
+         const T*                 R  = ring + st * Cfg::stage;
+         const unsigned long long wd = shw[2 * st];
+         const unsigned long long wa = AUX ? shw[2 * st + 1] : 0ull;
+#pragma unroll
+         for ( int j = 0; j < kZSRows; ++j )
+         {
+            const int rs = kZSRows * warp + j, rc = rs + 1, rn = rs + 2;  // stage rows of y-1, y, y+1
+            const T*  Rs = R + rs * RW + int( ( wd >> ( 3 * rs ) ) & 7ull ) + lane + 1;
+            const T*  Rc = R + rc * RW + int( ( wd >> ( 3 * rc ) ) & 7ull ) + lane + 1;
+            const T*  Rn = R + rn * RW + int( ( wd >> ( 3 * rn ) ) & 7ull ) + lane + 1;
+            const int y  = U.y + rs;
+#pragma unroll
+            for ( int k = 0; k < P; ++k )
+            {
+               const int q  = 32 * k;
+               const A   pc = A( Rc[q] ), pw = A( Rc[q - 1] ), pe = A( Rc[q + 1] );  // (x, y), (x-1, y), (x+1, y)
+               const A   ps = A( Rs[q] ), pse = A( Rs[q + 1] );                      // (x, y-1), (x+1, y-1)
+               const A   pn = A( Rn[q] ), pnw = A( Rn[q - 1] );                      // (x, y+1), (x-1, y+1)
+               if constexpr ( FIN )
+               {
+                  A t0 = w[6] * pc, t1 = w[9] * pw;
+                  t0 += w[11] * ps;
+                  t1 += w[13] * pse;
+                  const A sum = acc[j][k] + ( t0 + t1 );
+                  if ( x + q + y + s - 1 <= n - 1 )
+                     zstream_epilogue< T, A, OP >( out[j] + q, sum, w[kNumDirs], cen[j][k], axv[j][k], v2, dst, a0, a1 );
+               }
+               if constexpr ( MID )
+               {
+                  A m0 = w[0] * pc, m1 = w[1] * pw, m2 = w[2] * pe;
+                  m0 += w[3] * ps;
+                  m1 += w[4] * pn;
+                  m2 += w[7] * pnw;
+                  m0 += w[8] * pse;
+                  acc[j][k] = bot[j][k] + ( m0 + ( m1 + m2 ) );
+                  cen[j][k] = pc;
+                  if constexpr ( AUX )
+                     axv[j][k] = A( R[Cfg::aux0 + rs * Cfg::RWA + int( ( wa >> ( 3 * rs ) ) & 7ull ) + lane + q] );
+               }
+               if constexpr ( BOT )
+               {
+                  A b0 = w[5] * pc, b1 = w[10] * pe;
+                  b0 += w[12] * pn;
+                  b1 += w[14] * pnw;
+                  bot[j][k] = b0 + b1;
+               }
+            }
+            if constexpr ( FIN ) out[j] += slice_step( n, s - 1 ) - y;
+         }
+         __syncwarp();
+         if ( lane == 0 ) mbar_arrive( &empty[st] );
+         return true;
+      };
+      using F = std::false_type;
+      using Tr = std::true_type;
+      bool good = step( ld, U.z - 1, F{}, F{}, Tr{} ) && step( ld + 1, U.z, F{}, Tr{}, Tr{} );
+      for ( int s = U.z + 1; good && s <= U.w; ++s ) good = step( ld + 1 + ( s - U.z ), s, Tr{}, Tr{}, Tr{} );
+      good = good && step( ld + 2 + ( U.w - U.z ), U.w + 1, Tr{}, F{}, F{} );
+      if ( !good )
+      {
+         if ( lane == 0 )
+         {
+            atomicExch( err, 1 );
+            *abrt = 1;
+         }
+         return;
+      }
+      ld += U.w - U.z + 3;
+   }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Full-row z-streamed cell sweep (selectable with HYB_CELL_KERNEL=zrow).
 //
 // A unit is the band of rows y0..y0+ty-1 of slices z_first..z_last of one macro-cell, x over the
@@ -947,6 +1213,9 @@ static void zstream_attribute()
    check_cuda( cudaFuncSetAttribute( k_cell_zstream< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      int( ZCfg< T, zstream_aux< OP >() >::smem_bytes ) ),
                "cudaFuncSetAttribute(z-stream shared memory)" );
+   check_cuda( cudaFuncSetAttribute( k_cell_zsum< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int( ZSCfg< T, zstream_aux< OP >() >::smem_bytes ) ),
+               "cudaFuncSetAttribute(partial-sum sweep shared memory)" );
 }
 
 template < typename T, typename A >
@@ -986,9 +1255,14 @@ static int cell_kernel_variant()
    if ( v < 0 )
    {
       const char* e = getenv( "HYB_CELL_KERNEL" );
-      // default: the tiled z-stream sweep; "zrow" selects the full-row sweep (measured slower on the
-      // level-8 cube: 0.187 vs 0.134 ms per FP64 apply), "march" and "rows" the register sweeps
-      v = ( e && std::string( e ) == "rows" ) ? 0 : ( e && std::string( e ) == "march" ) ? 1 : ( e && std::string( e ) == "zrow" ) ? 3 : 2;
+      // default: the partial-sum z-streamed sweep (level-8 cube, FP64 apply: 0.111 ms); "zstream"
+      // selects the rolled-register sweep (0.128 ms), "zrow" the full-row sweep (0.187 ms), "march"
+      // and "rows" the register sweeps without shared-memory staging
+      v = ( e && std::string( e ) == "rows" )    ? 0
+          : ( e && std::string( e ) == "march" ) ? 1
+          : ( e && std::string( e ) == "zrow" )  ? 3
+          : ( e && std::string( e ) == "zstream" ) ? 2
+                                                   : 4;
    }
    return v;
 }
@@ -1075,6 +1349,13 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
       const size_t  smem  = size_t( kRStages ) * size_t( stage ) * sizeof( T );
       k_cell_zrow< T, A, OP ><<< v.nrblocks[zh], kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ),
                                                                                   A( a.a1 ), nC, zh, scap, stage, ctx->d_error );
+      ++ctx->launches;
+   }
+   else if ( cell_kernel_variant() == 4 && v.n >= 32 && v.nzblocks[1] > 0 && nC > 0 )
+   {
+      constexpr size_t smem = ZSCfg< T, zstream_aux< OP >() >::smem_bytes;  // attribute set by ensure_constants
+      k_cell_zsum< T, A, OP ><<< v.nzblocks[1], kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ),
+                                                                                  nC, ctx->d_error );
       ++ctx->launches;
    }
    else if ( cell_kernel_variant() >= 2 && v.n >= 32 && v.nzblocks[ZCfg< T, false >::wi] > 0 && nC > 0 )

@@ -299,7 +299,7 @@ void build_level( Mesh* m, int L )
    m->levels[L] = std::move( lv );
 }
 
-// Work units of the z-streamed sweep.  A unit is the tile x0..x0+31, y0..y0+7 of slices
+// Work units of the z-streamed sweeps.  A unit is the tile x0..x0+63, y0..y0+kZHeights[wi]-1 of slices
 // z_first..z_last (interior points only: x, y, z >= 1, x+y+z <= n-1).  The slice range is cut into
 // chunks of zc slices, zc the largest power of two in [8, 32] that still gives at least one unit
 // per two blocks (every chunk re-reads two halo slices, and every slice load costs a fixed hand-off,
@@ -307,7 +307,7 @@ void build_level( Mesh* m, int L )
 // loaded block.
 void build_zunits( P1Level& P, int nblocks, int wi, int ncells )
 {
-   const int n = P.n, kZTileX = kZWidths[wi];
+   const int n = P.n, kZTileX = kZWidths[wi], kTY = kZHeights[wi];
    auto&     zunits = P.zunits[wi];
    auto&     zcell  = P.zcell[wi];
    auto&     zbegin = P.zbegin[wi];
@@ -322,7 +322,7 @@ void build_zunits( P1Level& P, int nblocks, int wi, int ncells )
    };
    auto make = [&]( int zc ) {
       std::vector< Unit > us;
-      for ( int y0 = 1; y0 <= n - 3; y0 += kZTileY )
+      for ( int y0 = 1; y0 <= n - 3; y0 += kTY )
          for ( int x0 = 1; x0 + y0 <= n - 2; x0 += kZTileX )
          {
             const int zmax = n - 1 - x0 - y0;
@@ -331,7 +331,7 @@ void build_zunits( P1Level& P, int nblocks, int wi, int ncells )
                const int zb = std::min( zmax, za + zc - 1 );
                int64_t   w  = 0;
                for ( int z = za; z <= zb; ++z )
-                  for ( int y = y0; y < y0 + kZTileY; ++y )
+                  for ( int y = y0; y < y0 + kTY; ++y )
                      w += std::max( 0, std::min( kZTileX, n - y - z - x0 ) );
                us.push_back( { { x0, y0, za, zb }, w } );
             }
