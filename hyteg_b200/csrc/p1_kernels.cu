@@ -726,7 +726,7 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, O
 }
 
 // ---------------------------------------------------------------------------------------------
-// Partial-sum z-streamed cell sweep (the default for levels with n >= 32).
+// Partial-sum z-streamed cell sweep (FP64 apply on levels with n >= 256).
 //
 // Same units, ring, producers and bounded waits as the rolled sweep, with tiles of 64 x-points by
 // 16 rows (two rows per consumer warp, two x-points per lane: four points per lane per slice).
@@ -1249,22 +1249,15 @@ static int march_prefetch_distance()
    return d;
 }
 
+// HYB_CELL_KERNEL forces one cell sweep for every operation ("zsum", "zstream", "zrow", "march",
+// "rows"); it is read at every launch so that a tuning run can switch between calls.  Unset, the
+// sweep is chosen per operation (automatic, -1).
 static int cell_kernel_variant()
 {
-   static int v = -1;
-   if ( v < 0 )
-   {
-      const char* e = getenv( "HYB_CELL_KERNEL" );
-      // default: the partial-sum z-streamed sweep (level-8 cube, FP64 apply: 0.111 ms); "zstream"
-      // selects the rolled-register sweep (0.128 ms), "zrow" the full-row sweep (0.187 ms), "march"
-      // and "rows" the register sweeps without shared-memory staging
-      v = ( e && std::string( e ) == "rows" )    ? 0
-          : ( e && std::string( e ) == "march" ) ? 1
-          : ( e && std::string( e ) == "zrow" )  ? 3
-          : ( e && std::string( e ) == "zstream" ) ? 2
-                                                   : 4;
-   }
-   return v;
+   const char* e = getenv( "HYB_CELL_KERNEL" );
+   if ( !e || !*e ) return -1;
+   const std::string s( e );
+   return s == "rows" ? 0 : s == "march" ? 1 : s == "zstream" ? 2 : s == "zrow" ? 3 : s == "zsum" ? 4 : -1;
 }
 
 
@@ -1341,7 +1334,13 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
    T*       v2  = (T*) a.v2;
    T*       dst = (T*) a.dst;
    Fork     fk( ctx );
-   const int zh = ( cell_kernel_variant() == 3 && v.n >= 32 ) ? zrow_band_h< T, zstream_aux< OP >() >( v.n ) : -1;
+   // automatic choice: the partial-sum sweep for FP64 operations without a second vector (apply) on
+   // levels with n >= 256, the rolled-register sweep otherwise (same-process A/B on the cube: level 8
+   // FP64 apply 0.111 vs 0.125 ms; level 7 FP64 apply 0.034 vs 0.033 ms; Jacobi and FP32 sweeps
+   // faster with the rolled sweep at levels 6-8)
+   int var = cell_kernel_variant();
+   if ( var < 0 ) var = ( !zstream_aux< OP >() && sizeof( T ) == 8 && v.n >= 256 ) ? 4 : 2;
+   const int zh = ( var == 3 && v.n >= 32 ) ? zrow_band_h< T, zstream_aux< OP >() >( v.n ) : -1;
    if ( zh >= 0 && v.nrblocks[zh] > 0 && nC > 0 )
    {
       const int64_t scap  = zrow_src_cap< T >( v.n, 1 << zh );
@@ -1351,21 +1350,21 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
                                                                                   A( a.a1 ), nC, zh, scap, stage, ctx->d_error );
       ++ctx->launches;
    }
-   else if ( cell_kernel_variant() == 4 && v.n >= 32 && v.nzblocks[1] > 0 && nC > 0 )
+   else if ( var == 4 && v.n >= 32 && v.nzblocks[1] > 0 && nC > 0 )
    {
       constexpr size_t smem = ZSCfg< T, zstream_aux< OP >() >::smem_bytes;  // attribute set by ensure_constants
       k_cell_zsum< T, A, OP ><<< v.nzblocks[1], kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ),
                                                                                   nC, ctx->d_error );
       ++ctx->launches;
    }
-   else if ( cell_kernel_variant() >= 2 && v.n >= 32 && v.nzblocks[ZCfg< T, false >::wi] > 0 && nC > 0 )
+   else if ( var >= 2 && v.n >= 32 && v.nzblocks[ZCfg< T, false >::wi] > 0 && nC > 0 )
    {
       constexpr size_t smem = ZCfg< T, zstream_aux< OP >() >::smem_bytes;  // attribute set by ensure_constants
       k_cell_zstream< T, A, OP ><<< v.nzblocks[ZCfg< T, false >::wi], kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ),
                                                                                  A( a.a1 ), nC, ctx->d_error );
       ++ctx->launches;
    }
-   else if ( cell_kernel_variant() >= 1 && v.nmarch > 0 && nC > 0 )
+   else if ( var >= 1 && v.nmarch > 0 && nC > 0 )
    {
       dim3 grid( ( v.nmarch + 7 ) / 8, nC );
       k_cell_march< T, A, OP ><<< grid, 256, 0, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ),
