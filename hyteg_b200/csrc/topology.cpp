@@ -328,12 +328,11 @@ void build_zunits( P1Level& P, int nblocks, int wi, int ncells )
             const int zmax = n - 1 - x0 - y0;
             for ( int za = 1; za <= zmax; za += zc )
             {
+               // cost: the slice steps of the unit (its slices plus the two halo slices and the
+               // prologue); every step issues the whole tile, clipped lanes included, so the
+               // number of interior points would underestimate the units along the diagonal
                const int zb = std::min( zmax, za + zc - 1 );
-               int64_t   w  = 0;
-               for ( int z = za; z <= zb; ++z )
-                  for ( int y = y0; y < y0 + kTY; ++y )
-                     w += std::max( 0, std::min( kZTileX, n - y - z - x0 ) );
-               us.push_back( { { x0, y0, za, zb }, w } );
+               us.push_back( { { x0, y0, za, zb }, int64_t( zb - za + 3 ) } );
             }
          }
       return us;
