@@ -800,6 +800,82 @@ __global__ void k_cell_invert( int n, int nrows, const int2* __restrict__ rows, 
 }
 
 // ---------------------------------------------------------------------------------------------
+// P2 apply from stored element matrices: ten lanes per micro-cell anchor (three anchors per warp,
+// lanes 30-31 idle).  Lane i owns element node i: it loads its node value, gathers the other nine
+// with shuffles, reads row i of the symmetric matrix (its upper triangle is stored value-major) and
+// adds row i times x into its node.  The ten nodes of a micro-cell are distinct, the six
+// micro-cells of an anchor are taken in turn by the same lanes, and anchors of one parity class
+// share no node, so the read-modify-writes are race-free.  One lane per anchor (the recomputing
+// pass) left most of a block idle on these levels: 10 x more lanes in flight per pass.
+// ---------------------------------------------------------------------------------------------
+template < typename T, typename A >
+__global__ void __launch_bounds__( 256 ) k_p2_stored_pass( int ne, int nanch, const int* __restrict__ anch,
+                                                            const int64_t* __restrict__ cell_off, const T* __restrict__ src,
+                                                            A* __restrict__ acc, const A* __restrict__ kst, int64_t kstride,
+                                                            int64_t level_size, int* err )
+{
+   const int lane = threadIdx.x & 31, grp = lane / 10, i = lane - 10 * grp;  // grp 3: lanes 30, 31
+   const int t    = ( blockIdx.x * ( blockDim.x >> 5 ) + ( threadIdx.x >> 5 ) ) * 3 + grp;
+   const int c    = blockIdx.y;
+   const bool live = grp < 3 && t < nanch;
+   const int  g0   = 10 * grp;  // first lane of the group
+   int        x = 0, y = 0, z = 0;
+   if ( live )
+   {
+      const int a = anch[t];
+      x = a & 1023, y = ( a >> 10 ) & 1023, z = a >> 20;
+   }
+   const int     ns   = 2 * ne;
+   const int64_t base = cell_off[c];
+   // row i of the symmetric 10x10 matrix in the value-major upper-triangle storage: entry (r, s),
+   // r <= s, is value r * 10 - r * (r - 1) / 2 + (s - r)
+   int vrow[10];
+#pragma unroll
+   for ( int j = 0; j < 10; ++j )
+   {
+      const int r = min( i, j ), q = max( i, j );
+      vrow[j]     = r * 10 - r * ( r - 1 ) / 2 + ( q - r );
+   }
+#pragma unroll 1
+   for ( int ty = 0; ty < 6; ++ty )
+   {
+      const bool cell = live && x + y + z <= ne - 1 - c_mc_shift[ty];
+      // node i of the micro-cell: vertex i (i < 4) at 2 V_i, edge (a, b) at V_a + V_b
+      int64_t idx = 0;
+      if ( cell )
+      {
+         int P[3];
+         if ( i < 4 )
+            for ( int d = 0; d < 3; ++d ) P[d] = 2 * ( ( d == 0 ? x : d == 1 ? y : z ) + c_mc_off[ty][i][d] );
+         else
+         {
+            const int ea = c_p2_edge[i - 4][0], eb = c_p2_edge[i - 4][1];
+            for ( int d = 0; d < 3; ++d )
+               P[d] = 2 * ( d == 0 ? x : d == 1 ? y : z ) + c_mc_off[ty][ea][d] + c_mc_off[ty][eb][d];
+         }
+         idx = base + cidx( ns, P[0], P[1], P[2] );
+      }
+      const int64_t slot = ( int64_t( c ) * 6 + ty ) * tet_size( ne ) + ( cell ? cidx( ne - 1, x, y, z ) : 0 );
+      // self-check: every node inside the level's vector and the stored slot inside its array; a
+      // violation in any lane of the group skips the micro-cell and records error word 2
+      const bool     bad  = cell && ( idx < 0 || idx >= level_size || slot < 0 || slot >= kstride );
+      const unsigned bmsk = __ballot_sync( 0xffffffffu, bad );
+      const bool     gbad = grp < 3 && ( ( bmsk >> g0 ) & 0x3ffu ) != 0u;
+      if ( bad ) atomicExch( err, 2 );
+      const bool go = cell && !gbad;
+      const A    xi = go ? A( ld_any( src + idx ) ) : A( 0 );
+      A          yi = A( 0 );
+#pragma unroll
+      for ( int j = 0; j < 10; ++j )
+      {
+         const A xj = __shfl_sync( 0xffffffffu, xi, grp < 3 ? g0 + j : lane );
+         if ( go ) yi += kst[int64_t( vrow[j] ) * kstride + slot] * xj;
+      }
+      if ( go ) acc[idx] += yi;
+   }
+}
+
+// ---------------------------------------------------------------------------------------------
 // host launch
 // ---------------------------------------------------------------------------------------------
 template < typename A >
@@ -900,7 +976,13 @@ static void run_passes( Context* ctx, Mesh* m, Operator* op, int L, const T* src
       const int na = e.aoff[p + 1] - e.aoff[p];
       if ( na <= 0 ) continue;
       dim3 grid( ( na + 255 ) / 256, nC );
-      if ( op->order == 2 )
+      if ( op->order == 2 && MODE == 3 )
+      {
+         const dim3 g3( ( na + 23 ) / 24, nC );  // 24 anchors (8 warps x 3 groups) per block
+         k_p2_stored_pass< T, A ><<< g3, 256, 0, ctx->stream >>>( element_n( op, L ), na, e.d_anch + e.aoff[p], P.d_off + P.nB, src,
+                                                                  acc, kst, ks, P.size, ctx->d_error );
+      }
+      else if ( op->order == 2 )
          k_p2_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( element_n( op, L ), na, e.d_anch + e.aoff[p], P.d_off + P.nB,
                                                                     op->d_geom, op->coeff, src, acc, kst, ks, P.size, ctx->d_error );
       else
