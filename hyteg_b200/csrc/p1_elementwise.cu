@@ -466,12 +466,14 @@ __device__ __forceinline__ void p2_grad( int q, int i, const A Mi[3][3], A G[3] 
 // on storage level L+1.  MODE 0: y += K x computed matrix-free (per point the gradient of the local
 // solution, then its pairing with every basis gradient); 1: diagonal of K; 2: store the 55 upper-
 // triangle entries of K; 3: y += K x from the stored entries.  Stored entry v of micro-cell (cell c,
-// type ty, anchor a) sits at kst[v * kstride + (c * 6 + ty) * tet(ne) + cidx(ne - 1, a)].
+// type ty, anchor t of the pass's parity class p) sits at
+// kst[55 * (6 nC aoff[p] + (c * 6 + ty) * nanch + t) + v] (kbase = 6 nC aoff[p]): the 55 entries of
+// a micro-cell are contiguous, so the lanes that read one micro-cell's rows share its 440 bytes.
 template < typename T, typename A, int MODE >
 __global__ void __launch_bounds__( 256 ) k_p2_pass( int ne, int nanch, const int* __restrict__ anch, const int64_t* __restrict__ cell_off,
                                                      const CellGeom* __restrict__ geom, Coefficient kc,
                                                      const T* __restrict__ src, A* __restrict__ acc, A* __restrict__ kst,
-                                                     int64_t kstride, int64_t level_size, int* err )
+                                                     int64_t kstride, int64_t kbase, int64_t level_size, int* err )
 {
    const int t = blockIdx.x * blockDim.x + threadIdx.x;  // one micro-cell anchor per thread
    const int c = blockIdx.y;
@@ -501,7 +503,7 @@ __global__ void __launch_bounds__( 256 ) k_p2_pass( int ne, int nanch, const int
             const int a = c_p2_edge[e][0], b = c_p2_edge[e][1];
             idx[4 + e]  = base + cidx( ns, V[a][0] + V[b][0], V[a][1] + V[b][1], V[a][2] + V[b][2] );
          }
-         const int64_t slot = ( int64_t( c ) * 6 + ty ) * tet_size( ne ) + cidx( ne - 1, x, y, z );
+         const int64_t slot = kbase + ( int64_t( c ) * 6 + ty ) * nanch + t;
          {
             // self-check: nodes inside the level's vector, stored slot inside its array
             bool bad = ( MODE >= 2 ) && ( slot < 0 || slot >= kstride );
@@ -522,7 +524,7 @@ __global__ void __launch_bounds__( 256 ) k_p2_pass( int ne, int nanch, const int
             for ( int i = 0; i < 10; ++i )
                for ( int j = i; j < 10; ++j, ++v )
                {
-                  const A k = kst[v * kstride + slot];
+                  const A k = kst[slot * 55 + v];
                   yl[i] += k * xl[j];
                   if ( j != i ) yl[j] += k * xl[i];
                }
@@ -574,7 +576,7 @@ __global__ void __launch_bounds__( 256 ) k_p2_pass( int ne, int nanch, const int
             }
             if constexpr ( MODE == 2 )
             {
-               for ( int v = 0; v < 55; ++v ) kst[v * kstride + slot] = K[v];
+               for ( int v = 0; v < 55; ++v ) kst[slot * 55 + v] = K[v];
                continue;
             }
          }
@@ -802,7 +804,7 @@ __global__ void k_cell_invert( int n, int nrows, const int2* __restrict__ rows, 
 // ---------------------------------------------------------------------------------------------
 // P2 apply from stored element matrices: ten lanes per micro-cell anchor (three anchors per warp,
 // lanes 30-31 idle).  Lane i owns element node i: it loads its node value, gathers the other nine
-// with shuffles, reads row i of the symmetric matrix (its upper triangle is stored value-major) and
+// with shuffles, reads row i of the symmetric matrix (its upper triangle is stored per micro-cell) and
 // adds row i times x into its node.  The ten nodes of a micro-cell are distinct, the six
 // micro-cells of an anchor are taken in turn by the same lanes, and anchors of one parity class
 // share no node, so the read-modify-writes are race-free.  One lane per anchor (the recomputing
@@ -811,7 +813,7 @@ __global__ void k_cell_invert( int n, int nrows, const int2* __restrict__ rows, 
 template < typename T, typename A >
 __global__ void __launch_bounds__( 256 ) k_p2_stored_pass( int ne, int nanch, const int* __restrict__ anch,
                                                             const int64_t* __restrict__ cell_off, const T* __restrict__ src,
-                                                            A* __restrict__ acc, const A* __restrict__ kst, int64_t kstride,
+                                                            A* __restrict__ acc, const A* __restrict__ kst, int64_t kstride, int64_t kbase,
                                                             int64_t level_size, int* err )
 {
    const int lane = threadIdx.x & 31, grp = lane / 10, i = lane - 10 * grp;  // grp 3: lanes 30, 31
@@ -827,7 +829,7 @@ __global__ void __launch_bounds__( 256 ) k_p2_stored_pass( int ne, int nanch, co
    }
    const int     ns   = 2 * ne;
    const int64_t base = cell_off[c];
-   // row i of the symmetric 10x10 matrix in the value-major upper-triangle storage: entry (r, s),
+   // row i of the symmetric 10x10 matrix in the upper-triangle storage: entry (r, s),
    // r <= s, is value r * 10 - r * (r - 1) / 2 + (s - r)
    int vrow[10];
 #pragma unroll
@@ -855,7 +857,7 @@ __global__ void __launch_bounds__( 256 ) k_p2_stored_pass( int ne, int nanch, co
          }
          idx = base + cidx( ns, P[0], P[1], P[2] );
       }
-      const int64_t slot = ( int64_t( c ) * 6 + ty ) * tet_size( ne ) + ( cell ? cidx( ne - 1, x, y, z ) : 0 );
+      const int64_t slot = kbase + ( int64_t( c ) * 6 + ty ) * nanch + ( cell ? t : 0 );
       // self-check: every node inside the level's vector and the stored slot inside its array; a
       // violation in any lane of the group skips the micro-cell and records error word 2
       const bool     bad  = cell && ( idx < 0 || idx >= level_size || slot < 0 || slot >= kstride );
@@ -869,7 +871,7 @@ __global__ void __launch_bounds__( 256 ) k_p2_stored_pass( int ne, int nanch, co
       for ( int j = 0; j < 10; ++j )
       {
          const A xj = __shfl_sync( 0xffffffffu, xi, grp < 3 ? g0 + j : lane );
-         if ( go ) yi += kst[int64_t( vrow[j] ) * kstride + slot] * xj;
+         if ( go ) yi += kst[slot * 55 + vrow[j]] * xj;
       }
       if ( go ) acc[idx] += yi;
    }
@@ -975,16 +977,20 @@ static void run_passes( Context* ctx, Mesh* m, Operator* op, int L, const T* src
    {
       const int na = e.aoff[p + 1] - e.aoff[p];
       if ( na <= 0 ) continue;
+      // P2 stored matrices are grouped by parity class, then cell, micro-cell type and anchor, so the
+      // anchors of one pass read consecutive slots
+      const int64_t kbase = int64_t( 6 ) * nC * e.aoff[p];
       dim3 grid( ( na + 255 ) / 256, nC );
       if ( op->order == 2 && MODE == 3 )
       {
          const dim3 g3( ( na + 23 ) / 24, nC );  // 24 anchors (8 warps x 3 groups) per block
          k_p2_stored_pass< T, A ><<< g3, 256, 0, ctx->stream >>>( element_n( op, L ), na, e.d_anch + e.aoff[p], P.d_off + P.nB, src,
-                                                                  acc, kst, ks, P.size, ctx->d_error );
+                                                                  acc, kst, ks, kbase, P.size, ctx->d_error );
       }
       else if ( op->order == 2 )
          k_p2_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( element_n( op, L ), na, e.d_anch + e.aoff[p], P.d_off + P.nB,
-                                                                    op->d_geom, op->coeff, src, acc, kst, ks, P.size, ctx->d_error );
+                                                                    op->d_geom, op->coeff, src, acc, kst, ks, kbase, P.size,
+                                                                    ctx->d_error );
       else
          k_elem_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( P.n, na, e.d_anch + e.aoff[p], P.d_off + P.nB, op->d_geom,
                                                                       op->coeff, src, acc, kst, ks, P.size, ctx->d_error );
