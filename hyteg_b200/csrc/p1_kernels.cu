@@ -1300,15 +1300,31 @@ __global__ void __launch_bounds__( 256 ) k_bnd_stencil( LevelView v, OpView< A >
       else if constexpr ( OP == OP_CHEBI ) write_through( v, dst, b, i, j, owner, A( ldc( v2 + owner ) ) );
       return;
    }
-   A acc = A( 0 );
-   for ( int q = v.inc_begin[b]; q < v.inc_begin[b + 1]; ++q )
+   A         acc = A( 0 );
+   const int q0 = v.inc_begin[b], q1 = v.inc_begin[b + 1];
+   if ( q1 - q0 == 2 )
    {
-      const Incidence I = v.inc[q];
-      int             x, y, z;
-      inc_point( I, n, i, j, x, y, z );
-      acc += class_stencil< T, A >( src + v.cell_off[I.cell], o.W + ( size_t( I.cell ) * kNumClasses + I.cls ) * kNumDirs,
-                                    c_cls_mask[I.cls], n, x, y, z );
+      // a face between two cells: both class stencils written out, so the loads of the two cells
+      // are in flight together (same sum, same order as the loop)
+      const Incidence I0 = v.inc[q0], I1 = v.inc[q0 + 1];
+      int             x0, y0, z0, x1, y1, z1;
+      inc_point( I0, n, i, j, x0, y0, z0 );
+      inc_point( I1, n, i, j, x1, y1, z1 );
+      const A s0 = class_stencil< T, A >( src + v.cell_off[I0.cell], o.W + ( size_t( I0.cell ) * kNumClasses + I0.cls ) * kNumDirs,
+                                          c_cls_mask[I0.cls], n, x0, y0, z0 );
+      const A s1 = class_stencil< T, A >( src + v.cell_off[I1.cell], o.W + ( size_t( I1.cell ) * kNumClasses + I1.cls ) * kNumDirs,
+                                          c_cls_mask[I1.cls], n, x1, y1, z1 );
+      acc = ( acc + s0 ) + s1;
    }
+   else
+      for ( int q = q0; q < q1; ++q )
+      {
+         const Incidence I = v.inc[q];
+         int             x, y, z;
+         inc_point( I, n, i, j, x, y, z );
+         acc += class_stencil< T, A >( src + v.cell_off[I.cell], o.W + ( size_t( I.cell ) * kNumClasses + I.cls ) * kNumDirs,
+                                       c_cls_mask[I.cls], n, x, y, z );
+      }
    const A invd = o.invd_b[b];
    if constexpr ( OP == OP_APPLY ) write_through( v, dst, b, i, j, owner, acc );
    else if constexpr ( OP == OP_APPLY_ADD ) write_through( v, dst, b, i, j, owner, A( ldc( dst + owner ) ) + acc );

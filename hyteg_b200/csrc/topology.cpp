@@ -275,9 +275,27 @@ void build_level( Mesh* m, int L )
    for ( int v = 0; v < t.nV; ++v ) P.tasks.push_back( { v, 0, 0, 0 } );
    for ( int e = 0; e < t.nE; ++e )
       for ( int i = 1; i < n; ++i ) P.tasks.push_back( { t.nV + e, i, 0, 0 } );
+   // face DoFs: consecutive tasks step along the cell x direction of one incidence where the face
+   // contains it (i fastest if that cell maps face-local i to +-x, j fastest if it maps j), so the
+   // boundary sweep reads that cell's array in contiguous runs
    for ( int f = 0; f < t.nF; ++f )
-      for ( int j = 1; j < n; ++j )
-         for ( int i = 1; i + j < n; ++i ) P.tasks.push_back( { t.nV + t.nE + f, i, j, 0 } );
+   {
+      const int b   = t.nV + t.nE + f;
+      bool      jx  = false;
+      bool      any = false;
+      for ( int q = P.inc_begin[b]; q < P.inc_begin[b + 1] && !any; ++q )
+      {
+         const Incidence& I = P.inc[q];
+         if ( I.e1[1] == 0 && I.e1[2] == 0 ) any = true;
+         else if ( I.e2[1] == 0 && I.e2[2] == 0 ) any = true, jx = true;
+      }
+      if ( jx )
+         for ( int i = 1; i < n; ++i )
+            for ( int j = 1; i + j < n; ++j ) P.tasks.push_back( { b, i, j, 0 } );
+      else
+         for ( int j = 1; j < n; ++j )
+            for ( int i = 1; i + j < n; ++i ) P.tasks.push_back( { b, i, j, 0 } );
+   }
    // y-marching work items (interior points: x, y, z >= 1, x+y+z <= n-1)
    {
       const int YC = 16;
