@@ -126,6 +126,20 @@ _SIGS = {
     "hyb_op_store_element_matrices": (C.c_int, [C.c_void_p]),
     "hyb_fn_create_p2": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "hyb_p2_layout_sizes": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "hyb_op_create_p2p1_div": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "hyb_p2p1_div_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_int]),
+    "hyb_p1p2_divt_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_int]),
+    "hyb_op_create_p1_pspg": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "hyb_stokes_params_default": (C.c_int, [C.c_void_p]),
+    "hyb_stokes_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "hyb_stokes_destroy": (C.c_int, [C.c_void_p]),
+    "hyb_stokes_set_velocity_radii": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "hyb_stokes_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "hyb_stokes_uzawa_smooth": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "hyb_stokes_residual_norm": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                           C.POINTER(C.c_double)]),
+    "hyb_stokes_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                   C.c_double, C.c_void_p, C.POINTER(C.c_int)]),
     "hyb_p2_fn_download_reference": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "hyb_p2_fn_upload_reference": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "hyb_op_create_p2_divkgrad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
@@ -444,6 +458,25 @@ class _Coeff(C.Structure):
                 ("phase", C.c_double * 3)]
 
 
+def _coeff(k):
+    """hyb_coeff from None (k = 1), a constant, ("expsin", amp, (p0, p1, p2)[, freq]) or
+    ("radial", amp, r0, scale) for exp(amp (r0 - |x|) / scale)."""
+    c = _Coeff()
+    c.kind, c.value, c.amp, c.freq = 0, 1.0, 0.5, 1.0
+    if isinstance(k, (int, float)):
+        c.value = float(k)
+    elif k is not None and k[0] == "radial":
+        c.kind, c.amp, c.value, c.freq = 2, float(k[1]), float(k[2]), float(k[3])
+    elif k is not None:
+        c.kind = 1
+        c.amp = float(k[1])
+        for d in range(3):
+            c.phase[d] = float(k[2][d])
+        if len(k) > 3:
+            c.freq = float(k[3])
+    return c
+
+
 class P1ElementwiseBlendingDivKGradOperator(_ConstantOperator):
     """-div(k grad u), elementwise P1 with the form p1_div_k_grad_blending_q3.
 
@@ -454,17 +487,7 @@ class P1ElementwiseBlendingDivKGradOperator(_ConstantOperator):
     def __init__(self, storage, min_level, max_level, ctx, k=None, blending=None):
         self.storage, self.ctx = storage, ctx
         self.min_level, self.max_level = min_level, max_level
-        c = _Coeff()
-        c.kind, c.value, c.amp, c.freq = 0, 1.0, 0.5, 1.0
-        if isinstance(k, (int, float)):
-            c.value = float(k)
-        elif k is not None:
-            c.kind = 1
-            c.amp = float(k[1])
-            for d in range(3):
-                c.phase[d] = float(k[2][d])
-            if len(k) > 3:
-                c.freq = float(k[3])
+        c = _coeff(k)
         h = C.c_void_p()
         _check(lib().hyb_op_create_divkgrad(ctx.h, storage.h, min_level, max_level, C.byref(c),
                                             1 if blending == "shell" else 0, C.byref(h)))
@@ -508,17 +531,7 @@ class P2ElementwiseBlendingDivKGradOperator(_ConstantOperator):
     def __init__(self, storage, min_level, max_level, ctx, k=None, blending=None):
         self.storage, self.ctx = storage, ctx
         self.min_level, self.max_level = min_level, max_level
-        c = _Coeff()
-        c.kind, c.value, c.amp, c.freq = 0, 1.0, 0.5, 1.0
-        if isinstance(k, (int, float)):
-            c.value = float(k)
-        elif k is not None:
-            c.kind = 1
-            c.amp = float(k[1])
-            for d in range(3):
-                c.phase[d] = float(k[2][d])
-            if len(k) > 3:
-                c.freq = float(k[3])
+        c = _coeff(k)
         h = C.c_void_p()
         _check(lib().hyb_op_create_p2_divkgrad(ctx.h, storage.h, min_level, max_level, C.byref(c),
                                                1 if blending == "shell" else 0, C.byref(h)))
@@ -546,6 +559,113 @@ class P1toP1LinearProlongation:
 
     def prolongateAndAdd(self, function, sourceLevel, flag):
         _check(lib().hyb_prolongate(function.h, sourceLevel, flag, Add))
+
+
+class P2ToP1ElementwiseBlendingDivOperator:
+    """The coupling blocks of P2P1ElementwiseBlendingStokesOperator: div (P2ToP1ElementwiseBlending
+    Div{x,y,z}) maps three P2 velocity components of level l to a P1 pressure of level l; divT
+    (P1ToP2ElementwiseBlendingDivT{x,y,z}) is the transpose."""
+
+    def __init__(self, storage, min_level, max_level, ctx, blending=None):
+        self.storage, self.ctx = storage, ctx
+        h = C.c_void_p()
+        _check(lib().hyb_op_create_p2p1_div(ctx.h, storage.h, min_level, max_level, 1 if blending == "shell" else 0,
+                                            C.byref(h)))
+        self.h = h
+
+    def apply(self, u, p, level, flag=All, updateType=Replace):
+        arr = (C.c_void_p * 3)(*[f.h.value for f in u])
+        _check(lib().hyb_p2p1_div_apply(self.h, arr, p.h, level, flag, updateType))
+
+    def applyTranspose(self, p, u, level, flag=Inner, updateType=Replace):
+        arr = (C.c_void_p * 3)(*[f.h.value for f in u])
+        _check(lib().hyb_p1p2_divt_apply(self.h, p.h, arr, level, flag, updateType))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hyb_op_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class P1PSPGOperator(_ConstantOperator):
+    """P1PSPGOperator on the affine macro geometry; getInverseDiagonalValues gives the values of
+    P1PSPGInvDiagOperator (the Uzawa pressure scaling)."""
+
+    def __init__(self, storage, min_level, max_level, ctx):
+        self.storage, self.ctx = storage, ctx
+        self.min_level, self.max_level = min_level, max_level
+        h = C.c_void_p()
+        _check(lib().hyb_op_create_p1_pspg(ctx.h, storage.h, min_level, max_level, C.byref(h)))
+        self.h = h
+
+
+class _StokesParams(C.Structure):
+    _fields_ = [("min_level", C.c_int), ("max_level", C.c_int), ("pre_smooth", C.c_int), ("post_smooth", C.c_int),
+                ("velocity_sweeps", C.c_int), ("cheb_order", C.c_int), ("power_iterations", C.c_int),
+                ("omega", C.c_double), ("coarse_sweeps", C.c_int)]
+
+
+class StokesUzawaMultigrid:
+    """GeometricMultigridSolver< P2P1ElementwiseBlendingStokesOperator > with UzawaSmoother (block-Laplace
+    variant): the velocity block -div(eta grad) per component (eta: see _coeff, e.g.
+    ("radial", 2.99, 1.0, 0.45)), Chebyshev velocity smoothing, pressure update with the inverted PSPG
+    diagonal, quadratic/linear transfers, coarse_sweeps Uzawa steps on the coarsest level."""
+
+    def __init__(self, ctx, storage, min_level, max_level, viscosity=None, blending=None, pre=3, post=3,
+                 velocity_sweeps=3, cheb_order=3, power_iterations=20, omega=0.7, coarse_sweeps=100):
+        p = _StokesParams()
+        _check(lib().hyb_stokes_params_default(C.byref(p)))
+        p.min_level, p.max_level, p.pre_smooth, p.post_smooth = min_level, max_level, pre, post
+        p.velocity_sweeps, p.cheb_order, p.power_iterations = velocity_sweeps, cheb_order, power_iterations
+        p.omega, p.coarse_sweeps = float(omega), coarse_sweeps
+        self.params, self.ctx, self.storage = p, ctx, storage
+        c = _coeff(viscosity)
+        h = C.c_void_p()
+        _check(lib().hyb_stokes_create(ctx.h, storage.h, C.byref(c), 1 if blending == "shell" else 0, C.byref(p), C.byref(h)))
+        self.h = h
+
+    @staticmethod
+    def _arr(u):
+        return (C.c_void_p * 3)(*[f.h.value for f in u])
+
+    def set_velocity_radii(self, radii):
+        r = np.ascontiguousarray(radii, dtype=np.float64)
+        _check(lib().hyb_stokes_set_velocity_radii(self.h, _ptr(r)))
+
+    def apply(self, u, p, du, dp, level):
+        _check(lib().hyb_stokes_apply(self.h, self._arr(u), p.h, self._arr(du), dp.h, level))
+
+    def uzawa_smooth(self, u, p, bu, bp, level):
+        _check(lib().hyb_stokes_uzawa_smooth(self.h, self._arr(u), p.h, self._arr(bu), bp.h, level))
+
+    def residual_norm(self, u, p, bu, bp, level):
+        r = C.c_double()
+        _check(lib().hyb_stokes_residual_norm(self.h, self._arr(u), p.h, self._arr(bu), bp.h, level, C.byref(r)))
+        return r.value
+
+    def solve(self, u, p, bu, bp, level, max_cycles, rtol=0.0):
+        hist = np.zeros(max_cycles + 1)
+        done = C.c_int()
+        _check(lib().hyb_stokes_solve(self.h, self._arr(u), p.h, self._arr(bu), bp.h, level, max_cycles, float(rtol),
+                                      _ptr(hist), C.byref(done)))
+        return hist[: done.value + 1]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hyb_stokes_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 P2toP2QuadraticRestriction = P1toP1LinearRestriction  # hyb_restrict dispatches on the function's space

@@ -189,8 +189,11 @@ struct OpLevel {
 
 // scalar coefficient k(x) of -div(k grad u): constant, or exp(amp sin(2 pi f (x+p0)) cos(2 pi f (y+p1))
 // sin(2 pi f (z+p2)))
+// coefficient kind that selects the P1 PSPG element matrix instead of -div(k grad)
+constexpr int kCoeffPSPG = 3;
+
 struct Coefficient {
-   int    kind  = 0;  // 0 constant, 1 exp-sin-cos-sin
+   int    kind  = 0;  // 0 constant, 1 exp-sin-cos-sin, 2 radial exp(amp (value - |x|) / freq), 3 PSPG
    double value = 1.0;
    double amp   = 0.5;
    double freq  = 1.0;
@@ -219,6 +222,7 @@ struct ElemLevel {
    // cell-array slot (the partial stencil of that cell at copies of face/edge/vertex DoFs),
    // weight-major over the level's slots, in double ([0]) and float ([1])
    void* d_S[2] = { nullptr, nullptr };
+   void* d_sacc = nullptr;  // Stokes coupling blocks: three velocity accumulators and one pressure accumulator
 };
 
 struct Operator {
@@ -287,6 +291,11 @@ void launch_p2_restrict( Context* ctx, Mesh* m, int Lf, int dtype, uint32_t flag
 void launch_p2_prolongate( Context* ctx, Mesh* m, int Lc, int dtype, uint32_t flag, const void* coarse, void* fine, int add );
 void build_elementwise_operator( Operator* A );  // host tables (cell geometry, shell classification)
 void ensure_elementwise_level( Context* ctx, Operator* A, int L, int dtype );  // device buffers + diagonal
+void ensure_stokes_constants();
+// Stokes coupling blocks on P1 level Lp / P2 level Lp (storage Lp+1): divt 0 dst_p (+)= div u,
+// divt 1 dst_u[k] (+)= divT_k p
+void launch_stokes_div( Context* ctx, Operator* op, int Lp, int dtype, int divt, const void* const* u, const void* p, void* const* dst_u,
+                        void* dst_p, uint32_t flag, int add );
 
 enum PointOp : int {
    PT_LINCOMB = 0,  // dst = a0*s0 + a1*s1 + a2*s2 (nsrc terms)

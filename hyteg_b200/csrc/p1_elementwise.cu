@@ -119,6 +119,8 @@ template < typename A >
 __device__ __forceinline__ A coeff_eval( const Coefficient& k, const A* P )
 {
    if ( k.kind == 0 ) return A( k.value );
+   if ( k.kind == 2 )  // radial profile exp(amp (value - |x|) / freq)
+      return exp( A( k.amp ) * ( A( k.value ) - sqrt( P[0] * P[0] + P[1] * P[1] + P[2] * P[2] ) ) / A( k.freq ) );
    const A tp = A( 2.0 * 3.14159265358979323846 * k.freq );
    return exp( A( k.amp ) * sin( tp * ( P[0] + A( k.phase[0] ) ) ) * cos( tp * ( P[1] + A( k.phase[1] ) ) ) *
                sin( tp * ( P[2] + A( k.phase[2] ) ) ) );
@@ -144,6 +146,30 @@ __device__ __forceinline__ void shell_map( const CellGeom& g, const A* X, A* F, 
       F[i] = X[i] * s;
       for ( int j = 0; j < 3; ++j ) DF[i][j] = ( i == j ? s : A( 0 ) ) + X[i] * gs[j];
    }
+}
+
+// P1 PSPG stabilisation element matrix of an affine micro-cell (form p1_tet_pspg_tet.h, whose inverted
+// diagonal P1PSPGInvDiagOperator scales the Uzawa pressure update): -(|T|^(2/3) / 12) |T| grad l_i .
+// grad l_j, the l_i barycentric coordinates and |T| the volume.  Exact (constant integrand).
+template < typename A >
+__device__ __forceinline__ void p1_pspg_element( const A X[4][3], A K[4][4] )
+{
+   A J[3][3];
+   for ( int r = 0; r < 3; ++r )
+      for ( int c = 0; c < 3; ++c ) J[r][c] = X[c + 1][r] - X[0][r];
+   const A c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1], c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2],
+           c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+   const A det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+   // rows of J^-1 are the gradients of l_1, l_2, l_3
+   A G[4][3];
+   G[1][0] = c00 / det, G[1][1] = ( J[0][2] * J[2][1] - J[0][1] * J[2][2] ) / det, G[1][2] = ( J[0][1] * J[1][2] - J[0][2] * J[1][1] ) / det;
+   G[2][0] = c01 / det, G[2][1] = ( J[0][0] * J[2][2] - J[0][2] * J[2][0] ) / det, G[2][2] = ( J[0][2] * J[1][0] - J[0][0] * J[1][2] ) / det;
+   G[3][0] = c02 / det, G[3][1] = ( J[0][1] * J[2][0] - J[0][0] * J[2][1] ) / det, G[3][2] = ( J[0][0] * J[1][1] - J[0][1] * J[1][0] ) / det;
+   for ( int d = 0; d < 3; ++d ) G[0][d] = -( G[1][d] + G[2][d] + G[3][d] );
+   const A vol = fabs( det ) / A( 6 );
+   const A f   = -( pow( vol, A( 2.0 / 3.0 ) ) / A( 12 ) ) * vol;
+   for ( int i = 0; i < 4; ++i )
+      for ( int j = 0; j < 4; ++j ) K[i][j] = f * ( G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2] );
 }
 
 template < typename A >
@@ -291,7 +317,8 @@ __global__ void __launch_bounds__( 256 ) k_elem_pass( int n, int nanch, const in
             for ( int i = 0; i < 4; ++i ) acc[idx[i]] += K[i][0] * xl[0] + K[i][1] * xl[1] + K[i][2] * xl[2] + K[i][3] * xl[3];
             continue;
          }
-         p1_divkgrad_element( g, kc, X, K );
+         if ( kc.kind == kCoeffPSPG ) p1_pspg_element( X, K );
+         else p1_divkgrad_element( g, kc, X, K );
          if constexpr ( MODE == 2 )
          {
             int v = 0;
@@ -878,6 +905,187 @@ __global__ void __launch_bounds__( 256 ) k_p2_stored_pass( int ne, int nanch, co
 }
 
 // ---------------------------------------------------------------------------------------------
+// Stokes coupling blocks (P2P1ElementwiseBlendingStokesOperator, P2P1ElementwiseBlendingStokesOperator.hpp:
+// 113-116): div = P2ToP1ElementwiseBlendingDiv{x,y,z} (forms p2_to_p1_div_{0,1,2}_blending_q2) maps a
+// P2 velocity of level l to a P1 pressure of level l, divT (p1_to_p2_divt_{0,1,2}_blending_q2) is its
+// transpose.  Element matrix of component k: B_k[i][j] = -int psi_i d(phi_j)/dx_k over the blended
+// micro-cell, psi P1 and phi P2, with the 4-point degree-2 rule (a = (5 - sqrt 5)/20,
+// b = (5 + 3 sqrt 5)/20, weights 1/24).  Applied matrix-free: div forms the divergence of the local
+// velocity at each point; divT pairs the local pressure with every basis gradient.  The P1 nodes are
+// the micro-cell's vertices on level l, the P2 nodes the ten nodes on storage level l+1; anchors of
+// one parity class share neither, so the passes are race-free.
+// ---------------------------------------------------------------------------------------------
+__constant__ double c_q2_pts[4][3];
+__constant__ double c_q2_rgrad[4][10][3];
+
+void ensure_stokes_constants()
+{
+   static bool done = false;
+   if ( done ) return;
+   const double a = ( 5.0 - std::sqrt( 5.0 ) ) / 20.0, b = ( 5.0 + 3.0 * std::sqrt( 5.0 ) ) / 20.0;
+   const double pts[4][3] = { { a, a, a }, { b, a, a }, { a, b, a }, { a, a, b } };
+   const double lg[4][3]  = { { -1, -1, -1 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } };
+   const int    ed[6][2]  = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
+   double       g[4][10][3];
+   for ( int q = 0; q < 4; ++q )
+   {
+      const double lam[4] = { 1.0 - pts[q][0] - pts[q][1] - pts[q][2], pts[q][0], pts[q][1], pts[q][2] };
+      for ( int i = 0; i < 4; ++i )
+         for ( int d = 0; d < 3; ++d ) g[q][i][d] = ( 4.0 * lam[i] - 1.0 ) * lg[i][d];
+      for ( int e = 0; e < 6; ++e )
+         for ( int d = 0; d < 3; ++d )
+            g[q][4 + e][d] = 4.0 * ( lam[ed[e][0]] * lg[ed[e][1]][d] + lam[ed[e][1]] * lg[ed[e][0]][d] );
+   }
+   check_cuda( cudaMemcpyToSymbol( c_q2_pts, pts, sizeof( pts ) ), "Stokes constants (points)" );
+   check_cuda( cudaMemcpyToSymbol( c_q2_rgrad, g, sizeof( g ) ), "Stokes constants (gradients)" );
+   done = true;
+}
+
+// inverse of the blended Jacobian M = DF J at reference point xi and |det M|
+template < typename A >
+__device__ __forceinline__ void mapped_point( const CellGeom& g, const A X0[3], const A J[3][3], const double* xi, A Mi[3][3], A& adet )
+{
+   A Xq[3];
+   for ( int r = 0; r < 3; ++r ) Xq[r] = X0[r] + J[r][0] * A( xi[0] ) + J[r][1] * A( xi[1] ) + J[r][2] * A( xi[2] );
+   A M[3][3];
+   if ( g.blend == 1 )
+   {
+      A DF[3][3], Fq[3];
+      shell_map( g, Xq, Fq, DF );
+      for ( int r = 0; r < 3; ++r )
+         for ( int c = 0; c < 3; ++c ) M[r][c] = DF[r][0] * J[0][c] + DF[r][1] * J[1][c] + DF[r][2] * J[2][c];
+   }
+   else
+      for ( int r = 0; r < 3; ++r )
+         for ( int c = 0; c < 3; ++c ) M[r][c] = J[r][c];
+   const A c00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
+   const A c01 = M[1][2] * M[2][0] - M[1][0] * M[2][2];
+   const A c02 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
+   const A det = M[0][0] * c00 + M[0][1] * c01 + M[0][2] * c02;
+   const A id  = A( 1 ) / det;
+   Mi[0][0]    = c00 * id;
+   Mi[1][0]    = c01 * id;
+   Mi[2][0]    = c02 * id;
+   Mi[0][1]    = ( M[0][2] * M[2][1] - M[0][1] * M[2][2] ) * id;
+   Mi[1][1]    = ( M[0][0] * M[2][2] - M[0][2] * M[2][0] ) * id;
+   Mi[2][1]    = ( M[0][1] * M[2][0] - M[0][0] * M[2][1] ) * id;
+   Mi[0][2]    = ( M[0][1] * M[1][2] - M[0][2] * M[1][1] ) * id;
+   Mi[1][2]    = ( M[0][2] * M[1][0] - M[0][0] * M[1][2] ) * id;
+   Mi[2][2]    = ( M[0][0] * M[1][1] - M[0][1] * M[1][0] ) * id;
+   adet        = fabs( det );
+}
+
+// DIVT 0: p_acc[vertex i] += sum_k sum_j B_k[i][j] u_k[j];  DIVT 1: u_acc_k[node j] += sum_i B_k[i][j] p[i]
+template < typename T, typename A, int DIVT >
+__global__ void __launch_bounds__( 256 ) k_stokes_div_pass( int ne, int nanch, const int* __restrict__ anch,
+                                                             const int64_t* __restrict__ off_p, const int64_t* __restrict__ off_u,
+                                                             const CellGeom* __restrict__ geom, const T* __restrict__ u0,
+                                                             const T* __restrict__ u1, const T* __restrict__ u2,
+                                                             const T* __restrict__ p, A* accp, A* acc0, A* acc1, A* acc2,
+                                                             int64_t size_p, int64_t size_u, int* err )
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   const int c = blockIdx.y;
+   if ( t >= nanch ) return;
+   const int      a = anch[t];
+   const int      x = a & 1023, y = ( a >> 10 ) & 1023, z = a >> 20, ns = 2 * ne;
+   const CellGeom g = geom[c];
+   const int64_t  bp = off_p[c], bu = off_u[c];
+   const A        inv_n = A( 1.0 / double( ne ) );
+   A              st[3][3];
+   for ( int k = 0; k < 3; ++k )
+      for ( int d = 0; d < 3; ++d ) st[k][d] = ( A( g.P[k + 1][d] ) - A( g.P[0][d] ) ) * inv_n;
+   for ( int ty = 0; ty < 6; ++ty )
+   {
+      if ( x + y + z > ne - 1 - c_mc_shift[ty] ) continue;
+      int V[4][3];
+      for ( int m = 0; m < 4; ++m )
+         for ( int d = 0; d < 3; ++d ) V[m][d] = ( d == 0 ? x : d == 1 ? y : z ) + c_mc_off[ty][m][d];
+      int64_t ip[4], iu[10];
+      for ( int m = 0; m < 4; ++m )
+      {
+         ip[m] = bp + cidx( ne, V[m][0], V[m][1], V[m][2] );
+         iu[m] = bu + cidx( ns, 2 * V[m][0], 2 * V[m][1], 2 * V[m][2] );
+      }
+      for ( int e = 0; e < 6; ++e )
+      {
+         const int ea = c_p2_edge[e][0], eb = c_p2_edge[e][1];
+         iu[4 + e]    = bu + cidx( ns, V[ea][0] + V[eb][0], V[ea][1] + V[eb][1], V[ea][2] + V[eb][2] );
+      }
+      {
+         bool bad = false;
+         for ( int m = 0; m < 4; ++m ) bad |= ip[m] < 0 || ip[m] >= size_p;
+         for ( int m = 0; m < 10; ++m ) bad |= iu[m] < 0 || iu[m] >= size_u;
+         if ( bad )
+         {
+            atomicExch( err, 2 );
+            continue;
+         }
+      }
+      A X0[3], J[3][3];
+      for ( int d = 0; d < 3; ++d )
+      {
+         X0[d] = A( g.P[0][d] ) + st[0][d] * A( V[0][0] ) + st[1][d] * A( V[0][1] ) + st[2][d] * A( V[0][2] );
+         for ( int k = 0; k < 3; ++k )
+            J[d][k] = st[0][d] * A( V[k + 1][0] - V[0][0] ) + st[1][d] * A( V[k + 1][1] - V[0][1] ) + st[2][d] * A( V[k + 1][2] - V[0][2] );
+      }
+      if constexpr ( DIVT == 0 )
+      {
+         A ul[3][10];
+         for ( int j = 0; j < 10; ++j )
+         {
+            ul[0][j] = A( ld_any( u0 + iu[j] ) );
+            ul[1][j] = A( ld_any( u1 + iu[j] ) );
+            ul[2][j] = A( ld_any( u2 + iu[j] ) );
+         }
+         A yl[4] = { A( 0 ), A( 0 ), A( 0 ), A( 0 ) };
+         for ( int q = 0; q < 4; ++q )
+         {
+            A Mi[3][3], adet;
+            mapped_point( g, X0, J, c_q2_pts[q], Mi, adet );
+            // divergence of the local velocity: sum_k sum_j u_k[j] (grad_ref phi_j . Mi)_k
+            A dv = A( 0 );
+            for ( int j = 0; j < 10; ++j )
+               for ( int k = 0; k < 3; ++k )
+                  dv += ul[k][j] * ( A( c_q2_rgrad[q][j][0] ) * Mi[0][k] + A( c_q2_rgrad[q][j][1] ) * Mi[1][k] +
+                                     A( c_q2_rgrad[q][j][2] ) * Mi[2][k] );
+            const A f      = -A( 1.0 / 24.0 ) * adet * dv;
+            const A lam[4] = { A( 1.0 - c_q2_pts[q][0] - c_q2_pts[q][1] - c_q2_pts[q][2] ), A( c_q2_pts[q][0] ), A( c_q2_pts[q][1] ),
+                               A( c_q2_pts[q][2] ) };
+            for ( int i = 0; i < 4; ++i ) yl[i] += f * lam[i];
+         }
+         for ( int i = 0; i < 4; ++i ) accp[ip[i]] += yl[i];
+      }
+      else
+      {
+         A pl[4];
+         for ( int i = 0; i < 4; ++i ) pl[i] = A( ld_any( p + ip[i] ) );
+         A yl[3][10];
+         for ( int k = 0; k < 3; ++k )
+            for ( int j = 0; j < 10; ++j ) yl[k][j] = A( 0 );
+         for ( int q = 0; q < 4; ++q )
+         {
+            A Mi[3][3], adet;
+            mapped_point( g, X0, J, c_q2_pts[q], Mi, adet );
+            const A pq = pl[0] * A( 1.0 - c_q2_pts[q][0] - c_q2_pts[q][1] - c_q2_pts[q][2] ) + pl[1] * A( c_q2_pts[q][0] ) +
+                         pl[2] * A( c_q2_pts[q][1] ) + pl[3] * A( c_q2_pts[q][2] );
+            const A f = -A( 1.0 / 24.0 ) * adet * pq;
+            for ( int j = 0; j < 10; ++j )
+               for ( int k = 0; k < 3; ++k )
+                  yl[k][j] += f * ( A( c_q2_rgrad[q][j][0] ) * Mi[0][k] + A( c_q2_rgrad[q][j][1] ) * Mi[1][k] +
+                                    A( c_q2_rgrad[q][j][2] ) * Mi[2][k] );
+         }
+         for ( int j = 0; j < 10; ++j )
+         {
+            acc0[iu[j]] += yl[0][j];
+            acc1[iu[j]] += yl[1][j];
+            acc2[iu[j]] += yl[2][j];
+         }
+      }
+   }
+}
+
+// ---------------------------------------------------------------------------------------------
 // host launch
 // ---------------------------------------------------------------------------------------------
 template < typename A >
@@ -1159,6 +1367,108 @@ static void dispatch_elem( Context* ctx, Mesh* m, Operator* op, int L, int dtype
    case OP_DINV_APPLY: run_elem< T, A, OP_DINV_APPLY >( ctx, m, op, L, dtype, a ); break;
    default: throw std::invalid_argument( "unknown operation" );
    }
+}
+
+// owner/copy combine of an accumulation array (cell-array slots) into dst with the apply epilogue:
+// cell interiors on the main stream, face/edge/vertex owners (sum of their cell copies, written
+// through) on the second stream
+template < typename T, typename A, int OP >
+static void combine_acc( Context* ctx, Mesh* m, int L, const A* acc, uint32_t flag, T* dst )
+{
+   P1Level& P = m->level( L );
+   struct Join
+   {
+      Context* c;
+      ~Join()
+      {
+         cudaEventRecord( c->ev_join, c->aux );
+         cudaStreamWaitEvent( c->stream, c->ev_join, 0 );
+      }
+   };
+   check_cuda( cudaEventRecord( ctx->ev_fork, ctx->stream ), "fork" );
+   check_cuda( cudaStreamWaitEvent( ctx->aux, ctx->ev_fork, 0 ), "fork" );
+   Join      j{ ctx };
+   const int nrows = int( P.rows.size() );
+   if ( nrows > 0 )
+   {
+      dim3 grid( ( nrows + 7 ) / 8, m->topo.nC );
+      k_cell_acc< T, A, OP ><<< grid, 256, 0, ctx->stream >>>( P.n, nrows, P.d_rows, P.d_off + P.nB, P.d_bc + P.nB, flag, acc, nullptr,
+                                                                nullptr, nullptr, nullptr, dst, A( 0 ), A( 0 ) );
+      ++ctx->launches;
+   }
+   if ( !P.tasks.empty() )
+   {
+      k_bnd_acc< T, A, OP ><<< ( int( P.tasks.size() ) + 255 ) / 256, 256, 0, ctx->aux >>>(
+          P.n, int( P.tasks.size() ), P.d_tasks, P.d_off, P.d_off + P.nB, P.d_bkind, P.d_bc, P.d_inc_begin, P.d_inc, flag, 0, acc,
+          nullptr, nullptr, nullptr, nullptr, nullptr, dst, A( 0 ), A( 0 ) );
+      ++ctx->launches;
+   }
+   check_cuda( cudaGetLastError(), "combine launch" );
+}
+
+template < typename T, typename A >
+static void run_stokes( Context* ctx, Operator* op, int Lp, int divt, const void* const* u, const void* p, void* const* dst_u, void* dst_p,
+                        uint32_t flag, int add )
+{
+   Mesh*      m  = op->mesh;
+   const int  Ls = Lp + 1;
+   P1Level&   PP = m->level( Lp );
+   P1Level&   PU = m->level( Ls );
+   ensure_device( m, PP );
+   ensure_device( m, PU );
+   ensure_stokes_constants();
+   if ( !op->d_geom )
+   {
+      check_cuda( cudaMalloc( &op->d_geom, op->geom.size() * sizeof( CellGeom ) ), "cudaMalloc(geometry)" );
+      check_cuda( cudaMemcpy( op->d_geom, op->geom.data(), op->geom.size() * sizeof( CellGeom ), cudaMemcpyHostToDevice ),
+                  "upload geometry" );
+   }
+   ensure_rows( op, Ls );
+   ElemLevel& e = op->el[Ls];
+   if ( !e.d_sacc )
+      check_cuda( cudaMalloc( &e.d_sacc, size_t( 3 * PU.size + PP.size ) * sizeof( double ) ), "cudaMalloc(Stokes scratch)" );
+   A* acc_u = reinterpret_cast< A* >( e.d_sacc );
+   A* acc_p = acc_u + 3 * PU.size;
+   if ( divt ) check_cuda( cudaMemsetAsync( acc_u, 0, size_t( 3 * PU.size ) * sizeof( A ), ctx->stream ), "cudaMemset" );
+   else check_cuda( cudaMemsetAsync( acc_p, 0, size_t( PP.size ) * sizeof( A ), ctx->stream ), "cudaMemset" );
+   const int nC = m->topo.nC;
+   for ( int pc = 0; pc < 8; ++pc )
+   {
+      const int na = e.aoff[pc + 1] - e.aoff[pc];
+      if ( na <= 0 ) continue;
+      dim3 grid( ( na + 255 ) / 256, nC );
+      const T* u0 = u ? (const T*) u[0] : nullptr;
+      const T* u1 = u ? (const T*) u[1] : nullptr;
+      const T* u2 = u ? (const T*) u[2] : nullptr;
+      if ( divt )
+         k_stokes_div_pass< T, A, 1 ><<< grid, 256, 0, ctx->stream >>>( 1 << Lp, na, e.d_anch + e.aoff[pc], PP.d_off + PP.nB,
+                                                                         PU.d_off + PU.nB, op->d_geom, u0, u1, u2, (const T*) p, acc_p,
+                                                                         acc_u, acc_u + PU.size, acc_u + 2 * PU.size, PP.size, PU.size,
+                                                                         ctx->d_error );
+      else
+         k_stokes_div_pass< T, A, 0 ><<< grid, 256, 0, ctx->stream >>>( 1 << Lp, na, e.d_anch + e.aoff[pc], PP.d_off + PP.nB,
+                                                                         PU.d_off + PU.nB, op->d_geom, u0, u1, u2, (const T*) p, acc_p,
+                                                                         acc_u, acc_u + PU.size, acc_u + 2 * PU.size, PP.size, PU.size,
+                                                                         ctx->d_error );
+      ++ctx->launches;
+   }
+   check_cuda( cudaGetLastError(), "Stokes pass launch" );
+   if ( divt )
+      for ( int k = 0; k < 3; ++k )
+      {
+         if ( add ) combine_acc< T, A, OP_APPLY_ADD >( ctx, m, Ls, acc_u + k * PU.size, flag, (T*) dst_u[k] );
+         else combine_acc< T, A, OP_APPLY >( ctx, m, Ls, acc_u + k * PU.size, flag, (T*) dst_u[k] );
+      }
+   else if ( add ) combine_acc< T, A, OP_APPLY_ADD >( ctx, m, Lp, acc_p, flag, (T*) dst_p );
+   else combine_acc< T, A, OP_APPLY >( ctx, m, Lp, acc_p, flag, (T*) dst_p );
+}
+
+void launch_stokes_div( Context* ctx, Operator* op, int Lp, int dtype, int divt, const void* const* u, const void* p, void* const* dst_u,
+                        void* dst_p, uint32_t flag, int add )
+{
+   if ( dtype == F64 ) run_stokes< double, double >( ctx, op, Lp, divt, u, p, dst_u, dst_p, flag, add );
+   else if ( dtype == F32 ) run_stokes< float, float >( ctx, op, Lp, divt, u, p, dst_u, dst_p, flag, add );
+   else run_stokes< __half, float >( ctx, op, Lp, divt, u, p, dst_u, dst_p, flag, add );
 }
 
 void launch_elementwise( Context* ctx, Mesh* m, Operator* op, int L, int dtype, const StencilArgs& a )

@@ -52,6 +52,8 @@ extern "C" {
 #define HYB_P1_ELEM_DIVKGRAD 3 /* P1ElementwiseBlendingDivKGradOperator (elementwiseoperators/P1ElementwiseOperator.hpp:329-373)
                                   with the form p1_div_k_grad_blending_q3 */
 #define HYB_P2_ELEM_DIVKGRAD 4 /* P2ElementwiseBlendingDivKGradOperator (elementwiseoperators/P2ElementwiseOperator.hpp:475) */
+#define HYB_P2P1_DIV 5 /* P2ToP1ElementwiseBlendingDivOperator / P1ToP2ElementwiseBlendingDivTOperator (P2P1ElementwiseBlendingStokesOperator.hpp:113-116) */
+#define HYB_P1_PSPG 6  /* P1PSPGOperator; its inverted diagonal is P1PSPGInvDiagOperator (P1ConstantOperator.hpp:200-210) */
 
 /* blending maps (geometry/) */
 #define HYB_BLEND_NONE 0
@@ -60,6 +62,7 @@ extern "C" {
 /* coefficient families k(x) */
 #define HYB_COEFF_CONSTANT 0 /* k = value */
 #define HYB_COEFF_EXPSIN 1   /* k = exp(amp sin(2 pi f (x+p0)) cos(2 pi f (y+p1)) sin(2 pi f (z+p2))) */
+#define HYB_COEFF_RADIAL_EXP 2 /* k = exp(amp (value - |x|) / freq): radial viscosity profile, e.g. amp 2.99, value 1, freq 0.45 */
 
 typedef struct hyb_coeff
 {
@@ -325,6 +328,54 @@ int hyb_serve_step( hyb_serve* s, int* running, int* queued );
 int hyb_serve_status( hyb_serve* s, int64_t id, int* state, double* t_arrival, double* t_admit, double* t_done, int* cycles,
                       double* rel_res );
 const char* hyb_serve_last_error( void );
+
+/* ---------------------------------------------------------------------------------------------
+ * P2-P1 Taylor-Hood Stokes (P2P1ElementwiseBlendingStokesOperator, elementwiseoperators/
+ * P2P1ElementwiseBlendingStokesOperator.hpp:36-122, with the velocity block -div(eta grad) of each
+ * component, UzawaSmoother solvers/UzawaSmoother.hpp:321-441).  Velocity: three P2 functions
+ * (hyb_fn_create_p2); pressure: one P1 function of the same level whose every DoF is free (the
+ * reference's all-inner pressure boundary condition), so pressure calls use HYB_ALL.
+ * --------------------------------------------------------------------------------------------- */
+/* the coupling blocks on P2 level l / P1 level l: div (P2ToP1ElementwiseBlendingDiv{x,y,z}Operator,
+ * forms p2_to_p1_div_{0,1,2}_blending_q2) and divT (P1ToP2ElementwiseBlendingDivT{x,y,z}Operator,
+ * forms p1_to_p2_divt_{0,1,2}_blending_q2, the transpose) */
+int hyb_op_create_p2p1_div( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, int blending, hyb_op** out );
+/* p (update)= div u (u: three P2 functions) */
+int hyb_p2p1_div_apply( hyb_op* div, hyb_fn* const* u3, hyb_fn* p, int level, uint32_t flag, int update );
+/* u_k (update)= divT_k p */
+int hyb_p1p2_divt_apply( hyb_op* div, hyb_fn* p, hyb_fn* const* u3, int level, uint32_t flag, int update );
+/* P1PSPGOperator on the affine macro geometry; hyb_op_inverse_diagonal gives P1PSPGInvDiagOperator's values */
+int hyb_op_create_p1_pspg( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, hyb_op** out );
+
+typedef struct hyb_stokes hyb_stokes;
+typedef struct hyb_stokes_params
+{
+   int    min_level, max_level; /* P2 / P1 levels of the hierarchy */
+   int    pre_smooth, post_smooth;
+   int    velocity_sweeps;  /* velocity smoother applications per Uzawa step */
+   int    cheb_order;       /* Chebyshev order of the velocity smoother (ChebyshevSmoother) */
+   int    power_iterations; /* spectral-radius estimate of D^-1 A per level */
+   double omega;            /* Uzawa relaxation parameter (UzawaSmoother::setRelaxationParameter) */
+   int    coarse_sweeps;    /* Uzawa steps on the coarsest level (the coarse solve) */
+} hyb_stokes_params;
+int hyb_stokes_params_default( hyb_stokes_params* p );
+/* GeometricMultigridSolver< P2P1ElementwiseBlendingStokesOperator > with UzawaSmoother; viscosity:
+ * the coefficient of the velocity block (e.g. HYB_COEFF_RADIAL_EXP), NULL for eta = 1 */
+int hyb_stokes_create( hyb_ctx* ctx, hyb_mesh* mesh, const hyb_coeff* viscosity, int blending, const hyb_stokes_params* p,
+                       hyb_stokes** out );
+int hyb_stokes_destroy( hyb_stokes* s );
+/* fixes the velocity smoother's spectral radii (max_level - min_level + 1 values, P2 levels) */
+int hyb_stokes_set_velocity_radii( hyb_stokes* s, const double* radii );
+/* P2P1ElementwiseBlendingStokesOperator::apply: du = A u + divT p (velocity flag Inner), dp = div u (all) */
+int hyb_stokes_apply( hyb_stokes* s, hyb_fn* const* u3, hyb_fn* p, hyb_fn* const* du3, hyb_fn* dp, int level );
+/* one UzawaSmoother::solve step */
+int hyb_stokes_uzawa_smooth( hyb_stokes* s, hyb_fn* const* u3, hyb_fn* p, hyb_fn* const* bu3, hyb_fn* bp, int level );
+/* sqrt(|b_u - A u - divT p|^2 + |b_p - div u|^2) over the velocity's inner DoFs and all pressure DoFs */
+int hyb_stokes_residual_norm( hyb_stokes* s, hyb_fn* const* u3, hyb_fn* p, hyb_fn* const* bu3, hyb_fn* bp, int level, double* out );
+/* V-cycles (Uzawa smoothing, quadratic / linear transfers, coarse Uzawa sweeps) until the residual
+ * norm drops by rtol or max_cycles; history[0..cycles] the residual norms */
+int hyb_stokes_solve( hyb_stokes* s, hyb_fn* const* u3, hyb_fn* p, hyb_fn* const* bu3, hyb_fn* bp, int level, int max_cycles, double rtol,
+                      double* history, int* cycles_done );
 
 #ifdef __cplusplus
 }

@@ -1294,3 +1294,214 @@ def p2_reference_dof_coords(mesh: MacroMesh, L: int):
             q = pts + 0.5
             epart[base[p + c] + 6 * tb + cell_index(n - 2, pts[:, 0], pts[:, 1], pts[:, 2])] = lev.coords(c, q[:, 0], q[:, 1], q[:, 2])
     return np.concatenate([vpart, epart])
+
+
+# ---------------------------------------------------------------------------------------------
+# P2-P1 Taylor-Hood Stokes (P2P1ElementwiseBlendingStokesOperator with the velocity block
+# -div(eta grad) per component, UzawaSmoother block-Laplace variant, multigrid)
+# ---------------------------------------------------------------------------------------------
+_QA, _QB = (5.0 - 5.0 ** 0.5) / 20.0, (5.0 + 3.0 * 5.0 ** 0.5) / 20.0
+Q2_POINTS = np.array([[_QA, _QA, _QA], [_QB, _QA, _QA], [_QA, _QB, _QA], [_QA, _QA, _QB]])
+Q2_WEIGHT = 1.0 / 24.0  # the 4-point degree-2 rule on the reference tetrahedron (volume 1/6)
+
+
+def k_radial(amp=2.99, r0=1.0, scale=0.45):
+    """Radial viscosity eta(x) = exp(amp (r0 - |x|) / scale)."""
+    def k(P):
+        P = np.asarray(P, dtype=np.float64)
+        return np.exp(amp * (r0 - np.sqrt((P * P).sum(axis=-1))) / scale)
+    return k
+
+
+def p2p1_div_element(X, blend=None):
+    """Element matrices (m, 3, 4, 10) of the div blocks p2_to_p1_div_{0,1,2}_blending_q2
+    (P2ToP1ElementwiseBlendingDiv{x,y,z}Operator): B_k[i][j] = -int psi_i d(phi_j)/dx_k, psi P1
+    (micro-cell vertices), phi P2 (element DoF order), 4-point degree-2 rule; divT is the transpose."""
+    J = np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], axis=2)
+    B = np.zeros((X.shape[0], 3, 4, 10))
+    for xi in Q2_POINTS:
+        Xq = X[:, 0] + np.einsum("kij,j->ki", J, xi)
+        M = J if blend is None else np.einsum("kij,kjl->kil", blend.DF(Xq), J)
+        det = np.abs(np.linalg.det(M))
+        G = np.einsum("id,kdj->kij", p2_ref_gradients(xi), np.linalg.inv(M))  # (m, 10, 3)
+        lam = np.array([1.0 - xi.sum(), xi[0], xi[1], xi[2]])
+        B -= (Q2_WEIGHT * det)[:, None, None, None] * lam[None, None, :, None] * G.transpose(0, 2, 1)[:, :, None, :]
+    return B
+
+
+def p1_pspg_element(X):
+    """Element matrices (m, 4, 4) of the P1 PSPG form (p1_tet_pspg_tet.h) on affine tets:
+    -(|T|^(2/3) / 12) |T| grad l_i . grad l_j."""
+    J = np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], axis=2)
+    Ji = np.linalg.inv(J)
+    G = np.concatenate([-Ji.sum(axis=1, keepdims=True), Ji], axis=1)  # rows: gradients of l_0..l_3
+    vol = np.abs(np.linalg.det(J)) / 6.0
+    return (-(vol ** (2.0 / 3.0)) / 12.0 * vol)[:, None, None] * np.einsum("kid,kjd->kij", G, G)
+
+
+class P2P1Stokes:
+    """The Taylor-Hood system [A 0 0 B0^T; 0 A 0 B1^T; 0 0 A B2^T; B0 B1 B2 0] on P2 level L (velocity,
+    nodes of Level L+1) and P1 level L (pressure), A = -div(eta grad) per component, with the
+    inverted PSPG diagonal (P1PSPGInvDiagOperator, affine macro geometry) for the Uzawa step.
+    Velocity rows/columns use the inner DoFs, pressure rows/columns all DoFs."""
+
+    def __init__(self, mesh, minL, maxL, eta, blending=None):
+        self.mesh, self.minL, self.maxL = mesh, minL, maxL
+        self.Aop = P2DivKGrad(mesh, minL, maxL, eta, blending)
+        self.ulev = self.Aop.levels
+        self.plev = {L: Level(mesh, L) for L in range(minL, maxL + 1)}
+        maps = self.Aop.maps
+        self.B, self.sinv = {}, {}
+        for L in range(minL, maxL + 1):
+            ul, pl = self.ulev[L], self.plev[L]
+            rows, cols, vals = [[], [], []], [[], [], []], [[], [], []]
+            d = np.zeros(pl.size)
+            for c in range(mesh.nC):
+                uslots, X = p2_micro_cells(ul, c)
+                # P1 owners of the micro-cell vertices: level-L coordinates are half the storage ones
+                n = pl.n
+                pslots = []
+                for _, offs, shift in MICRO_CELL_TYPES:
+                    w = n - shift
+                    if w <= 0:
+                        continue
+                    base = tet_points(w)
+                    V = [base + np.array(o, dtype=np.int64) for o in offs]
+                    pslots.append(np.stack([pl.owner(c, v[:, 0], v[:, 1], v[:, 2]) for v in V], axis=1))
+                pslots = np.concatenate(pslots)
+                Be = p2p1_div_element(X, None if maps is None else _PerPointMap(maps[c]))
+                for k in range(3):
+                    rows[k].append(np.repeat(pslots, 10, axis=1).ravel())
+                    cols[k].append(np.tile(uslots, (1, 4)).ravel())
+                    vals[k].append(Be[:, k].reshape(-1))
+                # PSPG diagonal on the affine (computational) micro-cell
+                Kp = p1_pspg_element(X)
+                np.add.at(d, pslots.ravel(), np.einsum("kii->ki", Kp).ravel())
+            self.B[L] = [sp.coo_matrix((np.concatenate(vals[k]), (np.concatenate(rows[k]), np.concatenate(cols[k]))),
+                                       shape=(pl.size, ul.size)).tocsr() for k in range(3)]
+            inv = np.zeros(pl.size)
+            inv[pl.owned] = 1.0 / d[pl.owned]
+            self.sinv[L] = inv
+        self.utr = P2Transfer(self.Aop)
+        self.ptr = Transfer(P1ConstantLaplace(mesh, minL, maxL))
+
+    # --- blocks -----------------------------------------------------------------------------
+    def umask(self, L):
+        return self.ulev[L].owned_mask(INNER | NEUMANN | FREESLIP)
+
+    def pmask(self, L):
+        return self.plev[L].owned_mask(ALL)
+
+    def div(self, u, L):
+        """div u on all pressure DoFs (copies refreshed)."""
+        r = sum(self.B[L][k] @ u[k] for k in range(3))
+        out = np.zeros(self.plev[L].size)
+        m = self.pmask(L)
+        out[m] = r[m]
+        return self.plev[L].sync(out)
+
+    def divt(self, p, L, dst=None):
+        """dst_k (inner velocity DoFs) = divT_k p; other DoFs of dst kept."""
+        m = self.umask(L)
+        out = [np.zeros(self.ulev[L].size) if dst is None else dst[k].copy() for k in range(3)]
+        for k in range(3):
+            out[k][m] = (self.B[L][k].T @ p)[m]
+            self.ulev[L].sync(out[k])
+        return out
+
+    def apply(self, u, p, L):
+        m = self.umask(L)
+        du = []
+        for k in range(3):
+            r = self.Aop.A[L] @ u[k] + self.B[L][k].T @ p
+            o = np.zeros(self.ulev[L].size)
+            o[m] = r[m]
+            du.append(self.ulev[L].sync(o))
+        return du, self.div(u, L)
+
+    def residual(self, u, p, bu, bp, L):
+        m = self.umask(L)
+        ru = []
+        for k in range(3):
+            r = bu[k] - (self.Aop.A[L] @ u[k] + self.B[L][k].T @ p)
+            o = np.zeros(self.ulev[L].size)
+            o[m] = r[m]
+            ru.append(self.ulev[L].sync(o))
+        rp = bp - self.div(u, L)
+        mp = self.pmask(L)
+        rp[~mp] = 0.0
+        return ru, self.plev[L].sync(rp)
+
+    def residual_norm(self, u, p, bu, bp, L):
+        ru, rp = self.residual(u, p, bu, bp, L)
+        m, mp = self.umask(L), self.pmask(L)
+        return float(np.sqrt(sum((r[m] ** 2).sum() for r in ru) + (rp[mp] ** 2).sum()))
+
+    # --- Uzawa smoother and multigrid ---------------------------------------------------------
+    def uzawa(self, u, p, bu, bp, L, radius, order=3, sweeps=3, omega=0.7):
+        m, mp = self.umask(L), self.pmask(L)
+        ru = []
+        for k in range(3):
+            r = bu[k] - self.B[L][k].T @ p
+            o = np.zeros(self.ulev[L].size)
+            o[m] = r[m]
+            ru.append(self.ulev[L].sync(o))
+        u = [x.copy() for x in u]
+        for _ in range(sweeps):
+            for k in range(3):
+                u[k] = _cheb_apply(self.Aop, u[k], ru[k], L, radius, order)
+        rp = bp - self.div(u, L)
+        p = p.copy()
+        p[mp] += omega * (self.sinv[L] * rp)[mp]
+        return u, self.plev[L].sync(p)
+
+    def vcycle(self, u, p, bu, bp, L, radii, order=3, pre=3, post=3, sweeps=3, omega=0.7, coarse=100):
+        if L == self.minL:
+            for _ in range(coarse):
+                u, p = self.uzawa(u, p, bu, bp, L, radii[L], order, sweeps, omega)
+            return u, p
+        for _ in range(pre):
+            u, p = self.uzawa(u, p, bu, bp, L, radii[L], order, sweeps, omega)
+        ru, rp = self.residual(u, p, bu, bp, L)
+        ucl, pcl = self.ulev[L - 1], self.plev[L - 1]
+        bu_c = [self.utr.R[L] @ r for r in ru]
+        bu_c = [self._mask_sync(ucl, v, self.umask(L - 1)) for v in bu_c]
+        bp_c = self._mask_sync(pcl, self.ptr.R[L] @ rp, self.pmask(L - 1))
+        uc = [np.zeros(ucl.size) for _ in range(3)]
+        pc = np.zeros(pcl.size)
+        uc, pc = self.vcycle(uc, pc, bu_c, bp_c, L - 1, radii, order, pre, post, sweeps, omega, coarse)
+        m, mp = self.umask(L), self.pmask(L)
+        u = [x.copy() for x in u]
+        for k in range(3):
+            u[k][m] += (self.utr.P[L] @ uc[k])[m]
+            self.ulev[L].sync(u[k])
+        p = p.copy()
+        p[mp] += (self.ptr.P[L] @ pc)[mp]
+        p = self.plev[L].sync(p)
+        for _ in range(post):
+            u, p = self.uzawa(u, p, bu, bp, L, radii[L], order, sweeps, omega)
+        return u, p
+
+    @staticmethod
+    def _mask_sync(lev, v, m):
+        o = np.zeros(lev.size)
+        o[m] = v[m]
+        return lev.sync(o)
+
+
+def _cheb_apply(op, x, b, L, radius, order):
+    """One ChebyshevSmoother application (as GMG.chebyshev_step, bounds 0.3 and 1.2 times the radius)."""
+    x = x.copy()
+    lev = op.levels[L]
+    mask = lev.owned_mask(INNER | NEUMANN | FREESLIP)
+    coeff = chebyshev_coefficients(order, 0.3 * radius, 1.2 * radius)
+    tmp1, tmp2 = x.copy(), x.copy()
+    op.apply(x, tmp2, L, INNER | NEUMANN | FREESLIP)
+    tmp2[mask] = b[mask] - tmp2[mask]
+    tmp1[mask] = op.invdiag[L][mask] * tmp2[mask]
+    x[mask] = x[mask] + coeff[0] * tmp1[mask]
+    for k in range(1, len(coeff)):
+        op.apply(tmp1, tmp2, L, INNER | NEUMANN | FREESLIP)
+        tmp1[mask] = op.invdiag[L][mask] * tmp2[mask]
+        x[mask] = x[mask] + coeff[k] * tmp1[mask]
+    return x

@@ -194,3 +194,78 @@ extern "C" double ref_p2_elem_apply_bench( long ncells, int threads, double k_am
    const double s = std::chrono::duration< double >( std::chrono::steady_clock::now() - t0 ).count();
    return sink == 12345.678 ? -s : s;  // keep the work observable
 }
+
+// ---------------------------------------------------------------------------------------------
+// Stokes blocks (P2P1ElementwiseBlendingStokesOperator: div P2ToP1ElementwiseBlendingDiv{x,y,z}
+// with p2_to_p1_div_{0,1,2}_blending_q2, divT P1ToP2ElementwiseBlendingDivT{x,y,z} with
+// p1_to_p2_divt_{0,1,2}_blending_q2) and the PSPG element matrix whose inverted diagonal is the
+// Uzawa pressure scaling (P1PSPGInvDiagOperator, P1ConstantOperator.hpp:205-210, form
+// p1_tet_pspg_tet.h).  Row-major element matrices.
+// ---------------------------------------------------------------------------------------------
+#include "hyteg/forms/form_hyteg_generated/p2_to_p1/p2_to_p1_div_blending_q2.hpp"
+#include "hyteg/forms/form_hyteg_generated/p1_to_p2/p1_to_p2_divt_blending_q2.hpp"
+#include "hyteg/forms/form_fenics_generated/p1_tet_pspg_tet.h"
+
+extern "C" void ref_p2p1_div_element( const double* coords12, int map_kind, double map_a, int comp, double* A40 )
+{
+   auto map  = std::make_shared< TestMap >();
+   map->kind = map_kind;
+   map->a    = map_a;
+   std::array< hyteg::Point3D, 4 > c;
+   for ( int v = 0; v < 4; ++v ) c[v] = hyteg::Point3D( coords12[3 * v], coords12[3 * v + 1], coords12[3 * v + 2] );
+   hyteg::Matrix< double, 4, 10 > M;
+   if ( comp == 0 )
+   {
+      hyteg::forms::p2_to_p1_div_0_blending_q2 f;
+      f.setGeometryMap( map );
+      f.integrateAll( c, M );
+   }
+   else if ( comp == 1 )
+   {
+      hyteg::forms::p2_to_p1_div_1_blending_q2 f;
+      f.setGeometryMap( map );
+      f.integrateAll( c, M );
+   }
+   else
+   {
+      hyteg::forms::p2_to_p1_div_2_blending_q2 f;
+      f.setGeometryMap( map );
+      f.integrateAll( c, M );
+   }
+   for ( int i = 0; i < 40; ++i ) A40[i] = M.a[i];
+}
+
+extern "C" void ref_p1p2_divt_element( const double* coords12, int map_kind, double map_a, int comp, double* A40 )
+{
+   auto map  = std::make_shared< TestMap >();
+   map->kind = map_kind;
+   map->a    = map_a;
+   std::array< hyteg::Point3D, 4 > c;
+   for ( int v = 0; v < 4; ++v ) c[v] = hyteg::Point3D( coords12[3 * v], coords12[3 * v + 1], coords12[3 * v + 2] );
+   hyteg::Matrix< double, 10, 4 > M;
+   if ( comp == 0 )
+   {
+      hyteg::forms::p1_to_p2_divt_0_blending_q2 f;
+      f.setGeometryMap( map );
+      f.integrateAll( c, M );
+   }
+   else if ( comp == 1 )
+   {
+      hyteg::forms::p1_to_p2_divt_1_blending_q2 f;
+      f.setGeometryMap( map );
+      f.integrateAll( c, M );
+   }
+   else
+   {
+      hyteg::forms::p1_to_p2_divt_2_blending_q2 f;
+      f.setGeometryMap( map );
+      f.integrateAll( c, M );
+   }
+   for ( int i = 0; i < 40; ++i ) A40[i] = M.a[i];
+}
+
+extern "C" void ref_p1_pspg_element( const double* coords12, double* A16 )
+{
+   p1_tet_pspg_tet_cell_integral_0_otherwise form;
+   form.tabulate_tensor( A16, nullptr, coords12, 0 );
+}

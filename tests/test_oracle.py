@@ -308,3 +308,63 @@ def test_p2_reference_edgedof_sizes_example():
     assert sizes[mesh.nV + mesh.nE: mesh.nV + mesh.nE + mesh.nF] == [84] * mesh.nF
     assert sizes[-1] == 6 * 20 + 10  # cell: 6 tet(4) + tet(3)
     assert sizes[mesh.nV] == 4 + 2 * 11 + 1 * 21  # edge of one cell, two faces: n + nf(3n-1) + nc(7n-7)
+
+
+def _ref_lib():
+    import ctypes as C
+    import os
+    p = os.path.join(os.path.dirname(os.path.dirname(__file__)), "oracle", "_ref", "libhyteg_ref.so")
+    if not os.path.exists(p):
+        pytest.skip("oracle/_ref not built")
+    return C.CDLL(p)
+
+
+@pytest.mark.parametrize("kind,a", [(0, 0.0), (1, 0.3)])
+def test_stokes_div_element_matches_reference_forms(kind, a):
+    """p2_to_p1_div_{0,1,2}_blending_q2 and p1_to_p2_divt_{0,1,2}_blending_q2 (compiled from the
+    reference) equal the oracle's B_k and its transpose; identity and a non-affine test map."""
+    import ctypes as C
+    lib = _ref_lib()
+    X = np.array([[0.1, 0.0, 0.05], [1.0, 0.1, 0.0], [0.2, 0.9, 0.1], [0.05, 0.1, 1.1]])
+    B = O.p2p1_div_element(X[None], O.TestMap(a) if kind == 1 else None)[0]
+    for k in range(3):
+        out = np.zeros(40)
+        lib.ref_p2p1_div_element(X.ctypes.data_as(C.c_void_p), kind, C.c_double(a), k, out.ctypes.data_as(C.c_void_p))
+        assert np.abs(B[k] - out.reshape(4, 10)).max() < 1e-15
+        lib.ref_p1p2_divt_element(X.ctypes.data_as(C.c_void_p), kind, C.c_double(a), k, out.ctypes.data_as(C.c_void_p))
+        assert np.abs(B[k].T - out.reshape(10, 4)).max() < 1e-15
+
+
+def test_pspg_element_matches_reference_form():
+    import ctypes as C
+    lib = _ref_lib()
+    rng = np.random.default_rng(3)
+    for _ in range(5):
+        X = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], dtype=float) + 0.2 * rng.uniform(-1, 1, (4, 3))
+        out = np.zeros(16)
+        lib.ref_p1_pspg_element(X.ravel().ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p))
+        K = O.p1_pspg_element(X[None])[0]
+        assert np.abs(K - out.reshape(4, 4)).max() < 1e-15 * max(1.0, np.abs(out).max()) * 10
+
+
+def test_stokes_oracle_vcycle_converges():
+    """The Uzawa multigrid restatement converges on the unit cube (eta = 1) with the default
+    parameters (the product's defaults)."""
+    coords, tets = M.cube_6()
+    S = O.P2P1Stokes(O.MacroMesh(coords, tets), 0, 2, lambda P: np.ones(len(P)))
+    radii = {l: O.power_iteration_radius(S.Aop, l, np.random.default_rng(40 + l).uniform(-1, 1, S.ulev[l].size), 20)
+             for l in range(3)}
+    rng = np.random.default_rng(7)
+    bu = []
+    for _ in range(3):
+        x = np.zeros(S.ulev[2].size)
+        m = S.umask(2)
+        x[m] = rng.uniform(-1, 1, m.sum())
+        bu.append(S.ulev[2].sync(x))
+    bp = np.zeros(S.plev[2].size)
+    u, p = [np.zeros(S.ulev[2].size) for _ in range(3)], np.zeros(S.plev[2].size)
+    r = [S.residual_norm(u, p, bu, bp, 2)]
+    for _ in range(3):
+        u, p = S.vcycle(u, p, bu, bp, 2, radii)
+        r.append(S.residual_norm(u, p, bu, bp, 2))
+    assert r[-1] < 0.2 * r[0]
