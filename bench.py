@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-mixed", action="store_true")
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--no-p2", action="store_true")
+    p.add_argument("--no-stokes", action="store_true")
     p.add_argument("--serve-requests", type=int, default=200)
     return p.parse_args()
 
@@ -317,6 +318,42 @@ def serving_leg(H, ctx, nreq=200, seed=7):
             "speedup_vs_sequential_warm": served["solves_per_s"] / warm["solves_per_s"]}
 
 
+def stokes_leg(H, ctx, level=3, cycles=3):
+    """Configuration 4's system at a reduced level: P2-P1 Taylor-Hood Stokes on the blended shell
+    ntan=5, nrad=3 (1920 macro-cells), viscosity eta = exp(2.99 (1 - r) / 0.45), buoyancy-like
+    right-hand side (seeded uniform [0, 1] times the position vector in the velocity, zero in the
+    pressure), Uzawa multigrid (V(3,3) Uzawa steps with Chebyshev(3) velocity smoothing, quadratic /
+    linear transfers, 100 Uzawa steps on level 0), FP64.  Times `cycles` V-cycles after one warm-up
+    cycle and reports the residual-reduction factors."""
+    pm = H.PrimitiveStorage.spherical_shell(5, 3, 0.55, 1.0, ctx=ctx)
+    st = H.StokesUzawaMultigrid(ctx, pm, 0, level, viscosity=("radial", 2.99, 1.0, 0.45), blending="shell")
+    u = [H.P2Function("u%d" % k, pm, 0, level, ctx) for k in range(3)]
+    p = H.P1Function("p", pm, 0, level, ctx)
+    bu = [H.P2Function("bu%d" % k, pm, 0, level, ctx) for k in range(3)]
+    bp = H.P1Function("bp", pm, 0, level, ctx)
+    T = H.P2Function("T", pm, 0, level, ctx)
+    half = H.P2Function("half", pm, 0, level, ctx)
+    T.fill_random(level, 11)  # uniform [-1, 1] ...
+    half.interpolate(0.5, level)
+    T.assign([0.5, 1.0], [T, half], level)  # ... mapped to [0, 1]
+    for k in range(3):
+        # buoyancy: T x_k / |x| with T in [0, 1]
+        bu[k].interpolate(lambda x, y, z, k=k: [x, y, z][k] / max((x * x + y * y + z * z) ** 0.5, 1e-12), level)
+        bu[k].multElementwise([bu[k], T], level)
+    st.solve(u, p, bu, bp, level, 1)  # setup (radii, stored matrices) and one cycle
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    hist = st.solve(u, p, bu, bp, level, cycles)
+    ctx.synchronize()
+    sec = (time.perf_counter() - t0) / cycles
+    nu = pm.packed_size(level + 1)
+    return {"mesh": "spherical shell ntan=5 nrad=3 (1920 macro-cells), IcosahedralShellMap blending", "level": level,
+            "viscosity": "exp(2.99 (1 - r) / 0.45)", "velocity_dofs": 3 * nu, "pressure_dofs": pm.packed_size(level),
+            "cycle": "V(3,3) Uzawa (Chebyshev(3) x 3 velocity sweeps, omega 0.7, inverted PSPG diagonal), 100 coarse Uzawa steps",
+            "ms_per_cycle": sec * 1e3, "factors": [float(f) for f in hist[1:] / hist[:-1]], "dtype": "f64",
+            "stored_velocity_matrices": True}
+
+
 def p2_leg(H, ctx, level=5, cycle_level=3):
     """Configuration 2's operator: P2 -div(k grad u) with the icosahedral-shell blending map on the
     shell ntan=5, nrad=3 (1920 macro-cells), k = exp(0.5 sin(2 pi x) cos(2 pi y) sin(2 pi z)), FP64.
@@ -520,6 +557,9 @@ def run_ours(args, rank, world, local):
     if not args.no_p2:
         p2 = p2_leg(H, ctx)
         p2["cpu_baseline"] = p2_cpu_reference()
+    stokes = None
+    if not args.no_stokes:
+        stokes = stokes_leg(H, ctx)
     peak, peak_kind = measured_peak()
     alg_bytes = 2 * 8 * ndof  # read x, write y per inner DoF
     achieved = alg_bytes / (ms * 1e-3) / 1e9
@@ -547,6 +587,8 @@ def run_ours(args, rank, world, local):
         line["serving"] = serving
     if p2:
         line["p2_divkgrad_shell"] = p2
+    if stokes:
+        line["stokes_shell"] = stokes
     if cpu:
         rate, k, threads, el = cpu
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",

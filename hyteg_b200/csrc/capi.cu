@@ -2290,6 +2290,8 @@ int hyb_stokes_create( hyb_ctx* ctx, hyb_mesh* mesh, const hyb_coeff* viscosity,
    try
    {
       ok_rc( hyb_op_create_p2_divkgrad( ctx, mesh, params->min_level, params->max_level, viscosity, blending, &s->A ) );
+      // the velocity block is applied some hundred times per cycle: its element matrices are stored
+      ok_rc( hyb_op_store_element_matrices( s->A ) );
       ok_rc( hyb_op_create_p2p1_div( ctx, mesh, params->min_level, params->max_level, blending, &s->D ) );
       ok_rc( hyb_op_create_p1_pspg( ctx, mesh, params->min_level, params->max_level, &s->S ) );
       hyb_gmg_params gp;
