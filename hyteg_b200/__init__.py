@@ -339,10 +339,16 @@ class P1Function:
         """Seeded uniform values in [-1, 1] on every DoF of `level` (generated on the device)."""
         _check(lib().hyb_fn_fill_random(self.h, level, seed))
 
-    def download(self, level):
-        a = np.zeros(self.packed_size(level), dtype=np.float64)
-        _check(lib().hyb_fn_download(self.h, level, _ptr(a)))
-        return a
+    def download(self, level, out=None):
+        """Packed level vector; `out` (a contiguous float64 array of packed_size, e.g. in pinned
+        memory) is filled and returned instead of a new array."""
+        n = self.packed_size(level)
+        if out is None:
+            out = np.zeros(n, dtype=np.float64)
+        elif out.dtype != np.float64 or out.size != n or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous float64 array of the packed size")
+        _check(lib().hyb_fn_download(self.h, level, _ptr(out)))
+        return out
 
     # HyTeG function API ---------------------------------------------------------------------
     def interpolate(self, value, level, flag=All):

@@ -23,6 +23,7 @@ struct hyb_ctx
       cudaFree( c.d_partials );
       cudaFree( c.d_scalars );
       cudaFree( c.d_error );
+      cudaFree( c.d_stage );
       if ( c.aux ) cudaStreamSynchronize( c.aux ), cudaStreamDestroy( c.aux );
       if ( c.ev_fork ) cudaEventDestroy( c.ev_fork );
       if ( c.ev_join ) cudaEventDestroy( c.ev_join );
@@ -457,6 +458,23 @@ int hyb_fn_destroy( hyb_fn* fn )
    HYB_CATCH
 }
 
+// the context's packed staging buffer, grown to n doubles
+static double* stage_buffer( Context& c, int64_t n )
+{
+   if ( n > c.stage_cap )
+   {
+      if ( c.d_stage )
+      {
+         check_cuda( cudaStreamSynchronize( c.stream ), "stage sync" );
+         check_cuda( cudaFree( c.d_stage ), "cudaFree(stage)" );
+         c.d_stage = nullptr;
+      }
+      check_cuda( cudaMalloc( &c.d_stage, size_t( n ) * sizeof( double ) ), "cudaMalloc(transfer staging)" );
+      c.stage_cap = n;
+   }
+   return c.d_stage;
+}
+
 static void sync_copies( hyb_fn* fn, int L )
 {
    PointArgs a{};
@@ -512,12 +530,15 @@ int hyb_fn_upload( hyb_fn* fn, int level, const double* host_packed )
    require( fn && host_packed, "NULL argument" );
    level = lv( fn, level );
    require_level( fn->f, level );
-   const P1Level&        P = fn->f.mesh->level( level );
-   std::vector< double > padded( P.size, 0.0 );
-   for ( size_t p = 0; p < P.off.size(); ++p )
-      std::copy( host_packed + P.packed_off[p], host_packed + P.packed_off[p] + P.psize[p], padded.begin() + P.off[p] );
-   to_device( fn, level, padded );
+   // one contiguous host-to-device copy of the packed vector (full bandwidth from pinned memory),
+   // then a device scatter into the padded per-primitive layout and the copy refresh
+   Context&      c = fn->ctx->c;
+   const int64_t n = fn->f.mesh->level( level ).packed_size;
+   double*       st = stage_buffer( c, n );
+   check_cuda( cudaMemcpyAsync( st, host_packed, size_t( n ) * sizeof( double ), cudaMemcpyHostToDevice, c.stream ), "upload" );
+   launch_repack( &c, fn->f.mesh, level, fn->f.dtype, 1, st, fn->f.ptr( level ) );
    sync_copies( fn, level );
+   check_cuda( cudaStreamSynchronize( c.stream ), "upload sync" );
    HYB_CATCH
 }
 
@@ -527,10 +548,13 @@ int hyb_fn_download( hyb_fn* fn, int level, double* host_packed )
    require( fn && host_packed, "NULL argument" );
    level = lv( fn, level );
    require_level( fn->f, level );
-   const P1Level& P      = fn->f.mesh->level( level );
-   auto           padded = from_device( fn, level );
-   for ( size_t p = 0; p < P.off.size(); ++p )
-      std::copy( padded.begin() + P.off[p], padded.begin() + P.off[p] + P.psize[p], host_packed + P.packed_off[p] );
+   // device gather into the packed layout (as doubles), one contiguous device-to-host copy
+   Context&      c = fn->ctx->c;
+   const int64_t n = fn->f.mesh->level( level ).packed_size;
+   double*       st = stage_buffer( c, n );
+   launch_repack( &c, fn->f.mesh, level, fn->f.dtype, 0, st, fn->f.ptr( level ) );
+   check_cuda( cudaMemcpyAsync( host_packed, st, size_t( n ) * sizeof( double ), cudaMemcpyDeviceToHost, c.stream ), "download" );
+   check_cuda( cudaStreamSynchronize( c.stream ), "download sync" );
    HYB_CATCH
 }
 

@@ -137,6 +137,7 @@ struct P1Level {
    int64_t n_owned_cell = 0;
    // device copies
    int64_t*   d_off       = nullptr;  // all primitives
+   int64_t*   d_poff      = nullptr;  // packed offsets of all primitives and the packed size (nP + 1)
    int*       d_inc_begin = nullptr;
    Incidence* d_inc       = nullptr;
    int4*      d_tasks     = nullptr;
@@ -256,6 +257,8 @@ struct Context {
    int     partial_cap = 0;
    double* d_scalars = nullptr;  // small pool of device scalars
    int*    d_error   = nullptr;  // device error word (bounded waits that gave up)
+   double* d_stage   = nullptr;  // packed-vector staging for host transfers (grown on demand)
+   int64_t stage_cap = 0;
    int64_t launches = 0;         // kernel launches issued through this context
 };
 
@@ -323,6 +326,9 @@ struct PointArgs {
 void launch_point( Context* ctx, Mesh* m, int L, int dtype, const PointArgs& a );
 void launch_flat_lincomb( Context* ctx, int64_t count, int dtype, void* dst, int nsrc, const void* const* srcs, const double* scal );
 void launch_convert( Context* ctx, int64_t count, int dst_dtype, void* dst, int src_dtype, const void* src, double scale = 1.0 );
+// packed <-> padded level vector on the device: to_padded 1 scatters the packed doubles `packed` into
+// the level vector `vec` (value type dtype, padding untouched); 0 gathers vec into packed doubles
+void launch_repack( Context* ctx, Mesh* m, int L, int dtype, int to_padded, double* packed, void* vec );
 // deterministic dot over owned flagged DoFs -> *out (device)
 void launch_dot( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const void* a, const void* b, double* out );
 void launch_dot_noalloc( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const void* a, const void* b, double* host_out );

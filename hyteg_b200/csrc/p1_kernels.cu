@@ -1616,6 +1616,45 @@ __global__ void k_convert( int64_t count, TD* dst, const TS* src, double scale )
    }
 }
 
+// packed index i -> primitive p (largest p with poff[p] <= i) -> padded slot off[p] + (i - poff[p])
+template < typename T >
+__global__ void k_repack( int64_t count, int np, const int64_t* __restrict__ poff, const int64_t* __restrict__ off, int to_padded,
+                          double* packed, T* vec )
+{
+   for ( int64_t i = blockIdx.x * int64_t( blockDim.x ) + threadIdx.x; i < count; i += int64_t( gridDim.x ) * blockDim.x )
+   {
+      int lo = 0, hi = np - 1;
+      while ( lo < hi )
+      {
+         const int mid = ( lo + hi + 1 ) >> 1;
+         if ( poff[mid] <= i ) lo = mid;
+         else hi = mid - 1;
+      }
+      const int64_t slot = off[lo] + ( i - poff[lo] );
+      if ( to_padded )
+      {
+         if constexpr ( std::is_same< T, __half >::value ) vec[slot] = __float2half_rn( float( packed[i] ) );
+         else vec[slot] = T( packed[i] );
+      }
+      else packed[i] = double( ldc( vec + slot ) );
+   }
+}
+
+void launch_repack( Context* ctx, Mesh* m, int L, int dtype, int to_padded, double* packed, void* vec )
+{
+   P1Level& P = m->level( L );
+   ensure_device( m, P );
+   const int64_t count = P.packed_size;
+   if ( count <= 0 ) return;
+   const int np     = int( P.off.size() );
+   const int blocks = int( std::min< int64_t >( ( count + 255 ) / 256, 148 * 16 ) );
+   if ( dtype == F64 ) k_repack< double ><<< blocks, 256, 0, ctx->stream >>>( count, np, P.d_poff, P.d_off, to_padded, packed, (double*) vec );
+   else if ( dtype == F32 ) k_repack< float ><<< blocks, 256, 0, ctx->stream >>>( count, np, P.d_poff, P.d_off, to_padded, packed, (float*) vec );
+   else k_repack< __half ><<< blocks, 256, 0, ctx->stream >>>( count, np, P.d_poff, P.d_off, to_padded, packed, (__half*) vec );
+   ++ctx->launches;
+   check_cuda( cudaGetLastError(), "repack launch" );
+}
+
 void launch_convert( Context* ctx, int64_t count, int dd, void* dst, int sd, const void* src, double scale )
 {
    if ( count <= 0 ) return;

@@ -453,6 +453,11 @@ void ensure_device( Mesh* m, P1Level& P )
       if ( count ) check_cuda( cudaMemcpy( *dptr, host, count * sizeof( T ), cudaMemcpyHostToDevice ), "upload level tables" );
    };
    up( &P.d_off, P.off.data(), P.off.size() );
+   {
+      std::vector< int64_t > po( P.packed_off.begin(), P.packed_off.end() );
+      po.push_back( P.packed_size );
+      up( &P.d_poff, po.data(), po.size() );
+   }
    up( &P.d_inc_begin, P.inc_begin.data(), P.inc_begin.size() );
    up( &P.d_inc, P.inc.data(), P.inc.size() );
    std::vector< int4 > tk( P.tasks.size() );
@@ -523,6 +528,7 @@ Mesh::~Mesh()
    {
       P1Level& P = *kv.second;
       cudaFree( P.d_off );
+      cudaFree( P.d_poff );
       cudaFree( P.d_inc_begin );
       cudaFree( P.d_inc );
       cudaFree( P.d_tasks );
