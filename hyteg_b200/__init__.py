@@ -126,6 +126,8 @@ _SIGS = {
     "hyb_op_store_element_matrices": (C.c_int, [C.c_void_p]),
     "hyb_fn_create_p2": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "hyb_p2_layout_sizes": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "hyb_fn_upload_async": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "hyb_fn_download_async": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "hyb_op_create_p2p1_div": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "hyb_p2p1_div_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_int]),
     "hyb_p1p2_divt_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_int]),
@@ -334,6 +336,19 @@ class P1Function:
         if a.size != self.packed_size(level):
             raise ValueError("packed vector has the wrong size for this level")
         _check(lib().hyb_fn_upload(self.h, level, _ptr(a)))
+
+    def upload_async(self, level, packed):
+        """Queue the upload on the context's stream; `packed` (pinned for full bandwidth) must stay
+        valid until the context is synchronised."""
+        if packed.dtype != np.float64 or packed.size != self.packed_size(level) or not packed.flags["C_CONTIGUOUS"]:
+            raise ValueError("packed must be a contiguous float64 array of the packed size")
+        _check(lib().hyb_fn_upload_async(self.h, level, _ptr(packed)))
+
+    def download_async(self, level, out):
+        """Queue the download into `out` (contiguous float64, packed size) on the context's stream."""
+        if out.dtype != np.float64 or out.size != self.packed_size(level) or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous float64 array of the packed size")
+        _check(lib().hyb_fn_download_async(self.h, level, _ptr(out)))
 
     def fill_random(self, level, seed):
         """Seeded uniform values in [-1, 1] on every DoF of `level` (generated on the device)."""

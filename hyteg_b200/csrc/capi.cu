@@ -62,9 +62,12 @@ struct hyb_fn
 {
    hyb::Function f;
    hyb_ctx*      ctx = nullptr;
+   double*       stage     = nullptr;  // staging of the asynchronous transfers (packed doubles)
+   int64_t       stage_cap = 0;
    ~hyb_fn()
    {
       if ( ctx ) cudaStreamSynchronize( ctx->c.stream );
+      cudaFree( stage );
       for ( void* p : f.data ) cudaFree( p );
       f.data.clear();
       mesh_unref( f.mesh );
@@ -539,6 +542,54 @@ int hyb_fn_upload( hyb_fn* fn, int level, const double* host_packed )
    launch_repack( &c, fn->f.mesh, level, fn->f.dtype, 1, st, fn->f.ptr( level ) );
    sync_copies( fn, level );
    check_cuda( cudaStreamSynchronize( c.stream ), "upload sync" );
+   HYB_CATCH
+}
+
+// asynchronous transfers: queued on the function's context stream, with the function's own staging
+// buffer, so transfers of different functions on different contexts overlap (one direction each way
+// through the copy engines) and with kernels of other streams
+static double* fn_stage( hyb_fn* fn, int64_t n )
+{
+   if ( n > fn->stage_cap )
+   {
+      if ( fn->stage )
+      {
+         check_cuda( cudaStreamSynchronize( fn->ctx->c.stream ), "stage sync" );
+         check_cuda( cudaFree( fn->stage ), "cudaFree(stage)" );
+         fn->stage = nullptr;
+      }
+      check_cuda( cudaMalloc( &fn->stage, size_t( n ) * sizeof( double ) ), "cudaMalloc(transfer staging)" );
+      fn->stage_cap = n;
+   }
+   return fn->stage;
+}
+
+int hyb_fn_upload_async( hyb_fn* fn, int level, const double* host_packed )
+{
+   HYB_TRY
+   require( fn && host_packed, "NULL argument" );
+   level = lv( fn, level );
+   require_level( fn->f, level );
+   Context&      c  = fn->ctx->c;
+   const int64_t n  = fn->f.mesh->level( level ).packed_size;
+   double*       st = fn_stage( fn, n );
+   check_cuda( cudaMemcpyAsync( st, host_packed, size_t( n ) * sizeof( double ), cudaMemcpyHostToDevice, c.stream ), "upload" );
+   launch_repack( &c, fn->f.mesh, level, fn->f.dtype, 1, st, fn->f.ptr( level ) );
+   sync_copies( fn, level );
+   HYB_CATCH
+}
+
+int hyb_fn_download_async( hyb_fn* fn, int level, double* host_packed )
+{
+   HYB_TRY
+   require( fn && host_packed, "NULL argument" );
+   level = lv( fn, level );
+   require_level( fn->f, level );
+   Context&      c  = fn->ctx->c;
+   const int64_t n  = fn->f.mesh->level( level ).packed_size;
+   double*       st = fn_stage( fn, n );
+   launch_repack( &c, fn->f.mesh, level, fn->f.dtype, 0, st, fn->f.ptr( level ) );
+   check_cuda( cudaMemcpyAsync( host_packed, st, size_t( n ) * sizeof( double ), cudaMemcpyDeviceToHost, c.stream ), "download" );
    HYB_CATCH
 }
 

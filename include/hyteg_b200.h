@@ -165,6 +165,12 @@ int hyb_fn_destroy( hyb_fn* fn );
  * an owned DoF from its owner (communicate). */
 int hyb_fn_upload( hyb_fn* fn, int level, const double* host_packed );
 int hyb_fn_download( hyb_fn* fn, int level, double* host_packed );
+/* the same transfers queued on the function's context stream without waiting (no counterpart in the
+ * reference): the host buffer must stay valid (pinned memory for full bandwidth) until
+ * hyb_ctx_synchronize; each function has its own staging, so transfers of functions on different
+ * contexts overlap each other and kernels */
+int hyb_fn_upload_async( hyb_fn* fn, int level, const double* host_packed );
+int hyb_fn_download_async( hyb_fn* fn, int level, double* host_packed );
 /* interpolate(constant, level, flag) (VertexDoFFunction.cpp:384) */
 int hyb_fn_interpolate_const( hyb_fn* fn, double value, int level, uint32_t flag );
 /* interpolate(std::function<real_t(const Point3D&)>, level, flag) (VertexDoFFunction.cpp:384-470) */
