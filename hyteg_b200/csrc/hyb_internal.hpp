@@ -106,6 +106,10 @@ struct Topology {
 constexpr int kZTileY = 8;
 constexpr int kZWidths[2]  = { 64, 64 };
 constexpr int kZHeights[2] = { 8, 16 };
+// unit x0 carries a flag: the tile's rows end within 32 points for every slice of the unit, so the
+// sweep runs it with one point per lane instead of two
+constexpr int kZUnitHalf  = 1 << 30;
+constexpr int kZUnitXMask = kZUnitHalf - 1;
 
 struct P1Level {
    int     L = 0, n = 0;

@@ -486,9 +486,10 @@ __device__ __forceinline__ void zstream_produce( const LevelView& v, uint32_t fl
          const int c = zcl[u];
          if ( c >= nC || !( v.cell_bc[c] & flag ) ) continue;
          const int64_t cb = v.cell_off[c];
-         const int4 U  = zu[u];  // x0, y0, z_first, z_last
+         const int4 U  = zu[u];  // x0 (| half-width flag), y0, z_first, z_last
+         const int  ux = U.x & kZUnitXMask, tw = ( U.x & kZUnitHalf ) ? kZTileX / 2 : kZTileX;
          const int  yy = is_src ? U.y - 1 + lane : U.y + ( lane - Cfg::rows );
-         const int  xa = is_src ? U.x - 1 : U.x;  // first x of the row segment
+         const int  xa = is_src ? ux - 1 : ux;  // first x of the row segment
          int64_t    rb = cidx( n, 0, yy, U.z - 1 );
          for ( int zz = U.z - 1; zz <= U.w + 1; rb += slice_step( n, zz ) - yy, ++zz, ++ld )
          {
@@ -502,7 +503,7 @@ __device__ __forceinline__ void zstream_produce( const LevelView& v, uint32_t fl
             uint32_t bytes = 0, sh = 0;
             int64_t  a0    = 0;
             // last x of the segment: the halo point (source) or the last interior point (second vector)
-            const int  xe   = is_src ? min( U.x + kZTileX, n - yy - zz ) : min( U.x + kZTileX - 1, n - 1 - yy - zz );
+            const int  xe   = is_src ? min( ux + tw, n - yy - zz ) : min( ux + tw - 1, n - 1 - yy - zz );
             const bool live = ( is_src && yy + zz <= n && xe >= xa ) || ( is_aux && zz >= U.z && zz <= U.w && xe >= xa );
             if ( live )
             {
@@ -637,89 +638,98 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, O
             __syncwarp();
             cw = c;
          }
-         const int4 U = zu[u];
-         const int  x = U.x + lane, y = U.y + warp;
-         // prologue: slice z_first-1 (load ld) and slice z_first (load ld+1)
-         const int sm = ld % S, s0 = ( ld + 1 ) % S;
-         if ( !mbar_wait_bounded( &full[sm], uint32_t( ( ld / S ) & 1 ), abrt ) ||
-              !mbar_wait_bounded( &full[s0], uint32_t( ( ( ld + 1 ) / S ) & 1 ), abrt ) )
-            return fail();
-         ZPoint< A > P[kZPts];
-         {
-            const T*       Rm = ring + sm * Cfg::stage;
-            const T*       R0 = ring + s0 * Cfg::stage;
-            const uint32_t wm = shw[2 * sm], wc = shw[2 * s0];
-#pragma unroll
-            for ( int k = 0; k < kZPts; ++k )
+         const int4 U    = zu[u];
+         const int  x0   = U.x & kZUnitXMask;
+         const bool half = ( U.x & kZUnitHalf ) != 0;  // the tile's rows end within 32 points
+         const int  x = x0 + lane, y = U.y + warp;
+         // one unit with KP points per lane (kZPts, or 1 for half-width units)
+         auto unit = [&]( auto kp_c ) -> bool {
+            constexpr int KP = decltype( kp_c )::value;
+            // prologue: slice z_first-1 (load ld) and slice z_first (load ld+1)
+            const int sm = ld % S, s0 = ( ld + 1 ) % S;
+            if ( !mbar_wait_bounded( &full[sm], uint32_t( ( ld / S ) & 1 ), abrt ) ||
+                 !mbar_wait_bounded( &full[s0], uint32_t( ( ( ld + 1 ) / S ) & 1 ), abrt ) )
+               return false;
+            ZPoint< A > P[KP];
             {
-               P[k].B   = at( Rm, wm, rC, k, 0 );
-               P[k].BE  = at( Rm, wm, rC, k, 1 );
-               P[k].BN  = at( Rm, wm, rN, k, 0 );
-               P[k].BNW = at( Rm, wm, rN, k, -1 );
-               P[k].C   = at( R0, wc, rC, k, 0 );
-               P[k].W   = at( R0, wc, rC, k, -1 );
-               P[k].S   = at( R0, wc, rS, k, 0 );
-               P[k].SE  = at( R0, wc, rS, k, 1 );
-            }
-         }
-         __syncwarp();
-         if ( lane == 0 ) mbar_arrive( &empty[sm] );
-         int64_t out = base + cidx( n, x, y, U.z );  // output offset of point k = 0, advanced per slice
-         // unrolled by two so that the rolled values alternate registers instead of being copied
-#pragma unroll 2
-         for ( int z = U.z; z <= U.w; out += slice_step( n, z ) - y, ++z )
-         {
-            const int lz = ld + 1 + ( z - U.z ), lp = lz + 1;
-            const int sz = lz % S, sp = lp % S;
-            if ( !mbar_wait_bounded( &full[sp], uint32_t( ( lp / S ) & 1 ), abrt ) ) return fail();
-            const T*       Rz = ring + sz * Cfg::stage;
-            const T*       Rp = ring + sp * Cfg::stage;
-            const uint32_t wz = shw[2 * sz], wp = shw[2 * sp];
-            const uint32_t wa = AUX ? shw[2 * sz + 1] : 0u;
-#pragma unroll
-            for ( int k = 0; k < kZPts; ++k )
-            {
-               const A E = at( Rz, wz, rC, k, 1 ), N = at( Rz, wz, rN, k, 0 ), NW = at( Rz, wz, rN, k, -1 );
-               const A Tt = at( Rp, wp, rC, k, 0 ), TW = at( Rp, wp, rC, k, -1 ), TS = at( Rp, wp, rS, k, 0 ),
-                       TSE = at( Rp, wp, rS, k, 1 );
-               ZPoint< A >& p = P[k];
-               if ( x + 32 * k + y + z <= n - 1 )
+               const T*       Rm = ring + sm * Cfg::stage;
+               const T*       R0 = ring + s0 * Cfg::stage;
+               const uint32_t wm = shw[2 * sm], wc = shw[2 * s0];
+   #pragma unroll
+               for ( int k = 0; k < KP; ++k )
                {
-                  A auxv = A( 0 );
-                  if constexpr ( AUX )
-                     auxv = A( Rz[Cfg::aux0 + warp * Cfg::RWA + int( ( wa >> ( 3 * warp ) ) & 7u ) + lane + 32 * k] );
-                  // three independent partial sums: the dependent FMA chain is 7 deep instead of 15
-                  A s0 = w[0] * p.C, s1 = w[5] * p.B, s2 = w[10] * p.BE;
-                  s0 += w[1] * p.W;
-                  s1 += w[6] * Tt;
-                  s2 += w[11] * TS;
-                  s0 += w[2] * E;
-                  s1 += w[7] * NW;
-                  s2 += w[12] * p.BN;
-                  s0 += w[3] * p.S;
-                  s1 += w[8] * p.SE;
-                  s2 += w[13] * TSE;
-                  s0 += w[4] * N;
-                  s1 += w[9] * TW;
-                  s2 += w[14] * p.BNW;
-                  const A acc = s0 + ( s1 + s2 );
-                  zstream_epilogue< T, A, OP >( out + 32 * k, acc, w[kNumDirs], p.C, auxv, v2, dst, a0, a1 );
+                  P[k].B   = at( Rm, wm, rC, k, 0 );
+                  P[k].BE  = at( Rm, wm, rC, k, 1 );
+                  P[k].BN  = at( Rm, wm, rN, k, 0 );
+                  P[k].BNW = at( Rm, wm, rN, k, -1 );
+                  P[k].C   = at( R0, wc, rC, k, 0 );
+                  P[k].W   = at( R0, wc, rC, k, -1 );
+                  P[k].S   = at( R0, wc, rS, k, 0 );
+                  P[k].SE  = at( R0, wc, rS, k, 1 );
                }
-               p.B   = p.C;
-               p.BE  = E;
-               p.BN  = N;
-               p.BNW = NW;
-               p.C   = Tt;
-               p.W   = TW;
-               p.S   = TS;
-               p.SE  = TSE;
             }
             __syncwarp();
-            if ( lane == 0 ) mbar_arrive( &empty[sz] );
-         }
-         // slice z_last+1 is no longer needed either
-         __syncwarp();
-         if ( lane == 0 ) mbar_arrive( &empty[( ld + 2 + ( U.w - U.z ) ) % S] );
+            if ( lane == 0 ) mbar_arrive( &empty[sm] );
+            int64_t out = base + cidx( n, x, y, U.z );  // output offset of point k = 0, advanced per slice
+            // unrolled by two so that the rolled values alternate registers instead of being copied
+   #pragma unroll 2
+            for ( int z = U.z; z <= U.w; out += slice_step( n, z ) - y, ++z )
+            {
+               const int lz = ld + 1 + ( z - U.z ), lp = lz + 1;
+               const int sz = lz % S, sp = lp % S;
+               if ( !mbar_wait_bounded( &full[sp], uint32_t( ( lp / S ) & 1 ), abrt ) ) return false;
+               const T*       Rz = ring + sz * Cfg::stage;
+               const T*       Rp = ring + sp * Cfg::stage;
+               const uint32_t wz = shw[2 * sz], wp = shw[2 * sp];
+               const uint32_t wa = AUX ? shw[2 * sz + 1] : 0u;
+   #pragma unroll
+               for ( int k = 0; k < KP; ++k )
+               {
+                  const A E = at( Rz, wz, rC, k, 1 ), N = at( Rz, wz, rN, k, 0 ), NW = at( Rz, wz, rN, k, -1 );
+                  const A Tt = at( Rp, wp, rC, k, 0 ), TW = at( Rp, wp, rC, k, -1 ), TS = at( Rp, wp, rS, k, 0 ),
+                          TSE = at( Rp, wp, rS, k, 1 );
+                  ZPoint< A >& p = P[k];
+                  if ( x + 32 * k + y + z <= n - 1 )
+                  {
+                     A auxv = A( 0 );
+                     if constexpr ( AUX )
+                        auxv = A( Rz[Cfg::aux0 + warp * Cfg::RWA + int( ( wa >> ( 3 * warp ) ) & 7u ) + lane + 32 * k] );
+                     // three independent partial sums: the dependent FMA chain is 7 deep instead of 15
+                     A s0 = w[0] * p.C, s1 = w[5] * p.B, s2 = w[10] * p.BE;
+                     s0 += w[1] * p.W;
+                     s1 += w[6] * Tt;
+                     s2 += w[11] * TS;
+                     s0 += w[2] * E;
+                     s1 += w[7] * NW;
+                     s2 += w[12] * p.BN;
+                     s0 += w[3] * p.S;
+                     s1 += w[8] * p.SE;
+                     s2 += w[13] * TSE;
+                     s0 += w[4] * N;
+                     s1 += w[9] * TW;
+                     s2 += w[14] * p.BNW;
+                     const A acc = s0 + ( s1 + s2 );
+                     zstream_epilogue< T, A, OP >( out + 32 * k, acc, w[kNumDirs], p.C, auxv, v2, dst, a0, a1 );
+                  }
+                  p.B   = p.C;
+                  p.BE  = E;
+                  p.BN  = N;
+                  p.BNW = NW;
+                  p.C   = Tt;
+                  p.W   = TW;
+                  p.S   = TS;
+                  p.SE  = TSE;
+               }
+               __syncwarp();
+               if ( lane == 0 ) mbar_arrive( &empty[sz] );
+            }
+            // slice z_last+1 is no longer needed either
+            __syncwarp();
+            if ( lane == 0 ) mbar_arrive( &empty[( ld + 2 + ( U.w - U.z ) ) % S] );
+            return true;
+         };
+         const bool good = half ? unit( std::integral_constant< int, 1 >{} ) : unit( std::integral_constant< int, kZPts >{} );
+         if ( !good ) return fail();
          ld += U.w - U.z + 3;
       }
    }
@@ -780,7 +790,8 @@ __device__ __forceinline__ void zsum_produce( const LevelView& v, uint32_t flag,
       const int c = zcl[u];
       if ( c >= nC || !( v.cell_bc[c] & flag ) ) continue;
       const int64_t cb = v.cell_off[c];
-      const int4    U  = zu[u];  // x0, y0, z_first, z_last
+      const int4    U  = zu[u];  // x0 (| half-width flag), y0, z_first, z_last
+      const int     ux = U.x & kZUnitXMask, tw = ( U.x & kZUnitHalf ) ? TX / 2 : TX;
       for ( int zz = U.z - 1; zz <= U.w + 1; ++zz, ++ld )
       {
          if ( ld % kZProducers != me ) continue;
@@ -801,8 +812,8 @@ __device__ __forceinline__ void zsum_produce( const LevelView& v, uint32_t flag,
             const bool is_src = r < Cfg::rows, is_aux = AUX && r >= Cfg::rows && r < Cfg::NR;
             if ( !is_src && !is_aux ) continue;
             const int  yy   = is_src ? U.y - 1 + r : U.y + ( r - Cfg::rows );
-            const int  xa   = is_src ? U.x - 1 : U.x;
-            const int  xe   = is_src ? min( U.x + TX, n - yy - zz ) : min( U.x + TX - 1, n - 1 - yy - zz );
+            const int  xa   = is_src ? ux - 1 : ux;
+            const int  xe   = is_src ? min( ux + tw, n - yy - zz ) : min( ux + tw - 1, n - 1 - yy - zz );
             const bool live = ( is_src && yy + zz <= n && xe >= xa ) || ( is_aux && zz >= U.z && zz <= U.w && xe >= xa );
             dst[h]          = is_src ? r * Cfg::RW : Cfg::aux0 + ( r - Cfg::rows ) * Cfg::RWA;
             if ( !live ) continue;
@@ -900,84 +911,92 @@ __global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zsum( LevelView v, OpVi
          __syncwarp();
          cw = c;
       }
-      const int4 U = zu[u];
-      const int  x = U.x + lane;
-      // running sums of the point (x + 32 k, y_j) with y_j = U.y + 2 warp + j: acc of the point being
-      // completed, bot (bottom terms) of the next one; cen / axv: centre and second-vector value
-      A       acc[kZSRows][P], bot[kZSRows][P], cen[kZSRows][P], axv[kZSRows][P];
-      int64_t out[kZSRows];  // offset of (x, y_j, z) of the point being completed
-#pragma unroll
-      for ( int j = 0; j < kZSRows; ++j )
-      {
-         out[j] = base + cidx( n, x, U.y + kZSRows * warp + j, U.z );
-#pragma unroll
-         for ( int k = 0; k < P; ++k ) acc[j][k] = bot[j][k] = cen[j][k] = axv[j][k] = A( 0 );
-      }
-      // fold slice s (load number l) into the sums: FIN completes point s-1 with the top terms,
-      // MID starts point s, BOT gives the bottom terms of point s+1
-      auto step = [&]( int l, int s, auto fin_c, auto mid_c, auto bot_c ) -> bool {
-         constexpr bool FIN = decltype( fin_c )::value, MID = decltype( mid_c )::value, BOT = decltype( bot_c )::value;
-         const int      st  = l % S;
-         if ( !mbar_wait_bounded( &full[st], uint32_t( ( l / S ) & 1 ), abrt ) ) return false;
-         const T*                 R  = ring + st * Cfg::stage;
-         const unsigned long long wd = shw[2 * st];
-         const unsigned long long wa = AUX ? shw[2 * st + 1] : 0ull;
-#pragma unroll
+      const int4 U    = zu[u];
+      const int  x0   = U.x & kZUnitXMask;
+      const bool half = ( U.x & kZUnitHalf ) != 0;  // the tile's rows end within 32 points
+      const int  x    = x0 + lane;
+      // one unit with P points per lane and row (Cfg::pts, or 1 for half-width units)
+      auto unit = [&]( auto kp_c ) -> bool {
+         constexpr int P = decltype( kp_c )::value;
+         // running sums of the point (x + 32 k, y_j) with y_j = U.y + 2 warp + j: acc of the point being
+         // completed, bot (bottom terms) of the next one; cen / axv: centre and second-vector value
+         A       acc[kZSRows][P], bot[kZSRows][P], cen[kZSRows][P], axv[kZSRows][P];
+         int64_t out[kZSRows];  // offset of (x, y_j, z) of the point being completed
+   #pragma unroll
          for ( int j = 0; j < kZSRows; ++j )
          {
-            const int rs = kZSRows * warp + j, rc = rs + 1, rn = rs + 2;  // stage rows of y-1, y, y+1
-            const T*  Rs = R + rs * RW + int( ( wd >> ( 3 * rs ) ) & 7ull ) + lane + 1;
-            const T*  Rc = R + rc * RW + int( ( wd >> ( 3 * rc ) ) & 7ull ) + lane + 1;
-            const T*  Rn = R + rn * RW + int( ( wd >> ( 3 * rn ) ) & 7ull ) + lane + 1;
-            const int y  = U.y + rs;
-#pragma unroll
-            for ( int k = 0; k < P; ++k )
-            {
-               const int q  = 32 * k;
-               const A   pc = A( Rc[q] ), pw = A( Rc[q - 1] ), pe = A( Rc[q + 1] );  // (x, y), (x-1, y), (x+1, y)
-               const A   ps = A( Rs[q] ), pse = A( Rs[q + 1] );                      // (x, y-1), (x+1, y-1)
-               const A   pn = A( Rn[q] ), pnw = A( Rn[q - 1] );                      // (x, y+1), (x-1, y+1)
-               if constexpr ( FIN )
-               {
-                  A t0 = w[6] * pc, t1 = w[9] * pw;
-                  t0 += w[11] * ps;
-                  t1 += w[13] * pse;
-                  const A sum = acc[j][k] + ( t0 + t1 );
-                  if ( x + q + y + s - 1 <= n - 1 )
-                     zstream_epilogue< T, A, OP >( out[j] + q, sum, w[kNumDirs], cen[j][k], axv[j][k], v2, dst, a0, a1 );
-               }
-               if constexpr ( MID )
-               {
-                  A m0 = w[0] * pc, m1 = w[1] * pw, m2 = w[2] * pe;
-                  m0 += w[3] * ps;
-                  m1 += w[4] * pn;
-                  m2 += w[7] * pnw;
-                  m0 += w[8] * pse;
-                  acc[j][k] = bot[j][k] + ( m0 + ( m1 + m2 ) );
-                  cen[j][k] = pc;
-                  if constexpr ( AUX )
-                     axv[j][k] = A( R[Cfg::aux0 + rs * Cfg::RWA + int( ( wa >> ( 3 * rs ) ) & 7ull ) + lane + q] );
-               }
-               if constexpr ( BOT )
-               {
-                  A b0 = w[5] * pc, b1 = w[10] * pe;
-                  b0 += w[12] * pn;
-                  b1 += w[14] * pnw;
-                  bot[j][k] = b0 + b1;
-               }
-            }
-            if constexpr ( FIN ) out[j] += slice_step( n, s - 1 ) - y;
+            out[j] = base + cidx( n, x, U.y + kZSRows * warp + j, U.z );
+   #pragma unroll
+            for ( int k = 0; k < P; ++k ) acc[j][k] = bot[j][k] = cen[j][k] = axv[j][k] = A( 0 );
          }
-         __syncwarp();
-         if ( lane == 0 ) mbar_arrive( &empty[st] );
-         return true;
+         // fold slice s (load number l) into the sums: FIN completes point s-1 with the top terms,
+         // MID starts point s, BOT gives the bottom terms of point s+1
+         auto step = [&]( int l, int s, auto fin_c, auto mid_c, auto bot_c ) -> bool {
+            constexpr bool FIN = decltype( fin_c )::value, MID = decltype( mid_c )::value, BOT = decltype( bot_c )::value;
+            const int      st  = l % S;
+            if ( !mbar_wait_bounded( &full[st], uint32_t( ( l / S ) & 1 ), abrt ) ) return false;
+            const T*                 R  = ring + st * Cfg::stage;
+            const unsigned long long wd = shw[2 * st];
+            const unsigned long long wa = AUX ? shw[2 * st + 1] : 0ull;
+   #pragma unroll
+            for ( int j = 0; j < kZSRows; ++j )
+            {
+               const int rs = kZSRows * warp + j, rc = rs + 1, rn = rs + 2;  // stage rows of y-1, y, y+1
+               const T*  Rs = R + rs * RW + int( ( wd >> ( 3 * rs ) ) & 7ull ) + lane + 1;
+               const T*  Rc = R + rc * RW + int( ( wd >> ( 3 * rc ) ) & 7ull ) + lane + 1;
+               const T*  Rn = R + rn * RW + int( ( wd >> ( 3 * rn ) ) & 7ull ) + lane + 1;
+               const int y  = U.y + rs;
+   #pragma unroll
+               for ( int k = 0; k < P; ++k )
+               {
+                  const int q  = 32 * k;
+                  const A   pc = A( Rc[q] ), pw = A( Rc[q - 1] ), pe = A( Rc[q + 1] );  // (x, y), (x-1, y), (x+1, y)
+                  const A   ps = A( Rs[q] ), pse = A( Rs[q + 1] );                      // (x, y-1), (x+1, y-1)
+                  const A   pn = A( Rn[q] ), pnw = A( Rn[q - 1] );                      // (x, y+1), (x-1, y+1)
+                  if constexpr ( FIN )
+                  {
+                     A t0 = w[6] * pc, t1 = w[9] * pw;
+                     t0 += w[11] * ps;
+                     t1 += w[13] * pse;
+                     const A sum = acc[j][k] + ( t0 + t1 );
+                     if ( x + q + y + s - 1 <= n - 1 )
+                        zstream_epilogue< T, A, OP >( out[j] + q, sum, w[kNumDirs], cen[j][k], axv[j][k], v2, dst, a0, a1 );
+                  }
+                  if constexpr ( MID )
+                  {
+                     A m0 = w[0] * pc, m1 = w[1] * pw, m2 = w[2] * pe;
+                     m0 += w[3] * ps;
+                     m1 += w[4] * pn;
+                     m2 += w[7] * pnw;
+                     m0 += w[8] * pse;
+                     acc[j][k] = bot[j][k] + ( m0 + ( m1 + m2 ) );
+                     cen[j][k] = pc;
+                     if constexpr ( AUX )
+                        axv[j][k] = A( R[Cfg::aux0 + rs * Cfg::RWA + int( ( wa >> ( 3 * rs ) ) & 7ull ) + lane + q] );
+                  }
+                  if constexpr ( BOT )
+                  {
+                     A b0 = w[5] * pc, b1 = w[10] * pe;
+                     b0 += w[12] * pn;
+                     b1 += w[14] * pnw;
+                     bot[j][k] = b0 + b1;
+                  }
+               }
+               if constexpr ( FIN ) out[j] += slice_step( n, s - 1 ) - y;
+            }
+            __syncwarp();
+            if ( lane == 0 ) mbar_arrive( &empty[st] );
+            return true;
+         };
+         using F = std::false_type;
+         using Tr = std::true_type;
+         bool good = step( ld, U.z - 1, F{}, F{}, Tr{} ) && step( ld + 1, U.z, F{}, Tr{}, Tr{} );
+         for ( int s = U.z + 1; good && s <= U.w; ++s ) good = step( ld + 1 + ( s - U.z ), s, Tr{}, Tr{}, Tr{} );
+         good = good && step( ld + 2 + ( U.w - U.z ), U.w + 1, Tr{}, F{}, F{} );
+         return good;
       };
-      using F = std::false_type;
-      using Tr = std::true_type;
-      bool good = step( ld, U.z - 1, F{}, F{}, Tr{} ) && step( ld + 1, U.z, F{}, Tr{}, Tr{} );
-      for ( int s = U.z + 1; good && s <= U.w; ++s ) good = step( ld + 1 + ( s - U.z ), s, Tr{}, Tr{}, Tr{} );
-      good = good && step( ld + 2 + ( U.w - U.z ), U.w + 1, Tr{}, F{}, F{} );
-      if ( !good )
+      const bool ok = half ? unit( std::integral_constant< int, 1 >{} ) : unit( std::integral_constant< int, Cfg::pts >{} );
+      if ( !ok )
       {
          if ( lane == 0 )
          {

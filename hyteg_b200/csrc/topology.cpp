@@ -344,13 +344,22 @@ void build_zunits( P1Level& P, int nblocks, int wi, int ncells )
          for ( int x0 = 1; x0 + y0 <= n - 2; x0 += kZTileX )
          {
             const int zmax = n - 1 - x0 - y0;
-            for ( int za = 1; za <= zmax; za += zc )
+            // from slice zh on, every row of the tile ends within its first 32 points (row y0, the
+            // longest, has n - y0 - z - x0 interior points from x0 on): those slices form half-width
+            // units, run with one point per lane
+            const int zh = kZTileX > 32 ? std::max( 1, n - y0 - x0 - 32 ) : zmax + 1;
+            for ( int part = 0; part < 2; ++part )
             {
-               // cost: the slice steps of the unit (its slices plus the two halo slices and the
-               // prologue); every step issues the whole tile, clipped lanes included, so the
-               // number of interior points would underestimate the units along the diagonal
-               const int zb = std::min( zmax, za + zc - 1 );
-               us.push_back( { { x0, y0, za, zb }, int64_t( zb - za + 3 ) } );
+               const int lo = part == 0 ? 1 : std::max( 1, zh ), hi = part == 0 ? std::min( zmax, zh - 1 ) : zmax;
+               for ( int za = lo; za <= hi; za += zc )
+               {
+                  // cost: the slice steps of the unit (its slices plus the two halo slices and the
+                  // prologue) times the points per lane; every step issues the whole tile, clipped
+                  // lanes included, so the number of interior points would underestimate the units
+                  // along the diagonal
+                  const int zb = std::min( hi, za + zc - 1 );
+                  us.push_back( { { part ? ( x0 | kZUnitHalf ) : x0, y0, za, zb }, int64_t( zb - za + 3 ) * ( part ? 1 : 2 ) } );
+               }
             }
          }
       return us;
