@@ -347,7 +347,46 @@ def stokes_leg(H, ctx, level=3, cycles=3):
     ctx.synchronize()
     sec = (time.perf_counter() - t0) / cycles
     nu = pm.packed_size(level + 1)
+    # time to rtol 1e-6 one level lower: plain FP64 cycles against FP64 defect correction around FP32
+    # cycles (the configuration's "FP32 inner / FP64 outer residual")
+    Lr = level - 1
+    sr = H.StokesUzawaMultigrid(ctx, pm, 0, Lr, viscosity=("radial", 2.99, 1.0, 0.45), blending="shell")
+    si = H.StokesUzawaMultigrid(ctx, pm, 0, Lr, viscosity=("radial", 2.99, 1.0, 0.45), blending="shell")
+    runs = {}
+    for mode in ("fp64", "fp32_inner"):
+        uu = [H.P2Function("uu%d" % k, pm, 0, Lr, ctx) for k in range(3)]
+        pp = H.P1Function("pp", pm, 0, Lr, ctx)
+        bl_ = [H.P2Function("bl%d" % k, pm, 0, Lr, ctx) for k in range(3)]
+        bpl = H.P1Function("bpl", pm, 0, Lr, ctx)
+        for k in range(3):
+            bl_[k].interpolate(lambda x, y, z, k=k: [x, y, z][k] / max((x * x + y * y + z * z) ** 0.5, 1e-12), Lr)
+        if mode == "fp64":
+            sr.solve(uu, pp, bl_, bpl, Lr, 1)  # setup
+            for k in range(3):
+                uu[k].interpolate(0.0, Lr)
+            pp.interpolate(0.0, Lr)
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            h = sr.solve(uu, pp, bl_, bpl, Lr, 150, rtol=1e-6)
+        else:
+            sr.mixed_solve(si, uu, pp, bl_, bpl, Lr, max_outer=1, rtol=1e-6)  # setup of the inner solver
+            for k in range(3):
+                uu[k].interpolate(0.0, Lr)
+            pp.interpolate(0.0, Lr)
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            h = sr.mixed_solve(si, uu, pp, bl_, bpl, Lr, max_outer=150, rtol=1e-6)
+        ctx.synchronize()
+        runs[mode] = {"seconds": time.perf_counter() - t0, "cycles": len(h) - 1, "rel_residual": float(h[-1] / h[0]),
+                      "u": [uu[k].download(Lr) for k in range(3)]}
+    ref = runs["fp64"]["u"]
+    scale = max(np.abs(r).max() for r in ref)
+    for mode in runs:
+        runs[mode]["rel_diff_vs_fp64_solution"] = float(max(np.abs(runs[mode]["u"][k] - ref[k]).max() for k in range(3)) / scale)
+        del runs[mode]["u"]
+    runs["fp32_inner"]["speedup_vs_fp64"] = runs["fp64"]["seconds"] / runs["fp32_inner"]["seconds"]
     return {"mesh": "spherical shell ntan=5 nrad=3 (1920 macro-cells), IcosahedralShellMap blending", "level": level,
+            "time_to_rtol_1e-6": {"level": Lr, "rhs": "x / |x| (unit buoyancy)", **runs},
             "viscosity": "exp(2.99 (1 - r) / 0.45)", "velocity_dofs": 3 * nu, "pressure_dofs": pm.packed_size(level),
             "cycle": "V(3,3) Uzawa (Chebyshev(3) x 3 velocity sweeps, omega 0.7, inverted PSPG diagonal), 100 coarse Uzawa steps",
             "ms_per_cycle": sec * 1e3, "factors": [float(f) for f in hist[1:] / hist[:-1]], "dtype": "f64",

@@ -142,6 +142,8 @@ _SIGS = {
                                            C.POINTER(C.c_double)]),
     "hyb_stokes_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                    C.c_double, C.c_void_p, C.POINTER(C.c_int)]),
+    "hyb_stokes_mixed_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_int, C.c_int, C.c_double, C.c_void_p, C.POINTER(C.c_int)]),
     "hyb_p2_fn_download_reference": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "hyb_p2_fn_upload_reference": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "hyb_op_create_p2_divkgrad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
@@ -675,6 +677,16 @@ class StokesUzawaMultigrid:
         done = C.c_int()
         _check(lib().hyb_stokes_solve(self.h, self._arr(u), p.h, self._arr(bu), bp.h, level, max_cycles, float(rtol),
                                       _ptr(hist), C.byref(done)))
+        return hist[: done.value + 1]
+
+    def mixed_solve(self, inner, u, p, bu, bp, level, max_outer=50, rtol=1e-8, inner_dtype="float32"):
+        """Defect correction: FP64 residual of this solver, one V-cycle of `inner` (a second
+        StokesUzawaMultigrid on the same mesh and levels) in inner_dtype per iteration."""
+        dt = _DTYPES[inner_dtype] if isinstance(inner_dtype, str) else int(inner_dtype)
+        hist = np.zeros(max_outer + 1)
+        done = C.c_int()
+        _check(lib().hyb_stokes_mixed_solve(self.h, inner.h, dt, self._arr(u), p.h, self._arr(bu), bp.h, level, max_outer,
+                                            float(rtol), _ptr(hist), C.byref(done)))
         return hist[: done.value + 1]
 
     def close(self):

@@ -2437,6 +2437,89 @@ int hyb_stokes_residual_norm( hyb_stokes* s, hyb_fn* const* u, hyb_fn* p, hyb_fn
    HYB_CATCH
 }
 
+// mixedPrecisionIterativeRefinement for the Stokes system: the FP64 residual of `outer`, scaled to unit
+// RMS and rounded to the inner solver's value type, one inner V-cycle from a zero correction, the
+// correction added to the FP64 iterate.  `inner` is a second solver of the same levels whose work
+// vectors hold FP32 or FP16.
+int hyb_stokes_mixed_solve( hyb_stokes* outer, hyb_stokes* inner, int inner_dtype, hyb_fn* const* u, hyb_fn* p, hyb_fn* const* bu,
+                            hyb_fn* bp, int level, int max_outer, double rtol, double* history, int* iterations )
+{
+   HYB_TRY
+   require( outer && inner && outer != inner, "two solver instances are needed" );
+   // FP16 is refused: the inverted PSPG diagonal (of order h^-3) leaves the FP16 range
+   require( inner_dtype == F32 || inner_dtype == F64, "inner dtype must be FP32 or FP64 (FP16 overflows the pressure scaling)" );
+   stokes_fns_check( outer, u, p, level );
+   stokes_fns_check( outer, bu, bp, level );
+   require( p->f.dtype == F64, "the iterate must hold FP64 values" );
+   require( inner->mesh == outer->mesh && inner->p.min_level == outer->p.min_level && level <= inner->p.max_level,
+            "inner solver of another mesh or level range" );
+   require( max_outer >= 0, "max_outer must be >= 0" );
+   stokes_prepare( outer, u[0], bu[0], F64 );
+   Mesh*         m   = &outer->mesh->m;
+   const int     lo  = outer->p.min_level;
+   // inner iterate and right-hand side on every level (P2 velocity, P1 pressure)
+   hyb_fn* iu[3], *ibu[3];
+   for ( int k = 0; k < 3; ++k )
+   {
+      iu[k]            = new_fn( inner->ctx, m, inner_dtype, lo + 1, level + 1 );
+      ibu[k]           = new_fn( inner->ctx, m, inner_dtype, lo + 1, level + 1 );
+      iu[k]->f.lshift  = 1;
+      ibu[k]->f.lshift = 1;
+   }
+   hyb_fn* ip  = new_fn( inner->ctx, m, inner_dtype, lo, level );
+   hyb_fn* ibp = new_fn( inner->ctx, m, inner_dtype, lo, level );
+   struct Free
+   {
+      hyb_fn** a;
+      hyb_fn*  p1;
+      hyb_fn*  p2;
+      ~Free()
+      {
+         for ( int k = 0; k < 6; ++k ) hyb_fn_destroy( a[k] );
+         hyb_fn_destroy( p1 );
+         hyb_fn_destroy( p2 );
+      }
+   };
+   hyb_fn* all6[6] = { iu[0], iu[1], iu[2], ibu[0], ibu[1], ibu[2] };
+   Free    fr{ all6, ip, ibp };
+   stokes_prepare( inner, iu[0], ibu[0], inner_dtype );
+   Context&  cx = outer->ctx->c;
+   const int Ls = level + 1;
+   // owned entries of the residual (velocity inner DoFs, all pressure DoFs) for the unit-RMS scaling
+   double nown = 0;
+   {
+      const P1Level& PU = m->level( Ls );
+      const P1Level& PP = m->level( level );
+      nown = 3.0 * double( PU.packed_size ) + double( PP.packed_size );
+   }
+   double r0 = stokes_residual_norm( outer, u, p, bu, bp, level );
+   double rn = r0;
+   if ( history ) history[0] = r0;
+   int it = 0;
+   for ( ; it < max_outer; ++it )
+   {
+      if ( r0 == 0.0 || rn / r0 < rtol ) break;
+      const double sc = std::sqrt( nown ) / rn;
+      for ( int k = 0; k < 3; ++k )
+      {
+         launch_convert( &cx, m->level( Ls ).size, inner_dtype, ibu[k]->f.ptr( Ls ), F64, outer->ru[k]->f.ptr( Ls ), sc );
+         check_cuda( cudaMemsetAsync( iu[k]->f.ptr( Ls ), 0, iu[k]->f.bytes( Ls ), cx.stream ), "cudaMemset" );
+      }
+      launch_convert( &cx, m->level( level ).size, inner_dtype, ibp->f.ptr( level ), F64, outer->rp->f.ptr( level ), sc );
+      check_cuda( cudaMemsetAsync( ip->f.ptr( level ), 0, ip->f.bytes( level ), cx.stream ), "cudaMemset" );
+      if ( inner->ctx != outer->ctx ) check_cuda( cudaStreamSynchronize( cx.stream ), "sync" );
+      stokes_vcycle( inner, iu, ip, ibu, ibp, level );
+      if ( inner->ctx != outer->ctx ) check_cuda( cudaStreamSynchronize( inner->ctx->c.stream ), "sync" );
+      for ( int k = 0; k < 3; ++k )
+         launch_axpy_to_f64( &cx, m->level( Ls ).size, (double*) u[k]->f.ptr( Ls ), inner_dtype, iu[k]->f.ptr( Ls ), 1.0 / sc );
+      launch_axpy_to_f64( &cx, m->level( level ).size, (double*) p->f.ptr( level ), inner_dtype, ip->f.ptr( level ), 1.0 / sc );
+      rn = stokes_residual_norm( outer, u, p, bu, bp, level );
+      if ( history ) history[it + 1] = rn;
+   }
+   if ( iterations ) *iterations = it;
+   HYB_CATCH
+}
+
 int hyb_stokes_solve( hyb_stokes* s, hyb_fn* const* u, hyb_fn* p, hyb_fn* const* bu, hyb_fn* bp, int level, int max_cycles, double rtol,
                       double* history, int* cycles_done )
 {

