@@ -132,6 +132,10 @@ _SIGS = {
     "hyb_p2p1_div_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_int]),
     "hyb_p1p2_divt_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_int]),
     "hyb_op_create_p1_pspg": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "hyb_op_create_p2_full_viscous": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                                C.POINTER(C.c_void_p)]),
+    "hyb_p2_full_viscous_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_int]),
+    "hyb_p2_full_viscous_inverse_diagonal": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "hyb_stokes_params_default": (C.c_int, [C.c_void_p]),
     "hyb_stokes_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
     "hyb_stokes_destroy": (C.c_int, [C.c_void_p]),
@@ -603,6 +607,42 @@ class P2ToP1ElementwiseBlendingDivOperator:
     def applyTranspose(self, p, u, level, flag=Inner, updateType=Replace):
         arr = (C.c_void_p * 3)(*[f.h.value for f in u])
         _check(lib().hyb_p1p2_divt_apply(self.h, p.h, arr, level, flag, updateType))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hyb_op_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class P2ElementwiseBlendingFullViscousOperator:
+    """The full viscous velocity block 2 mu eps(u) : eps(v) - (2/3) mu div u div v on three P2
+    components (P2ElementwiseBlendingFullViscousOperator, a VectorToVectorOperator of the nine forms
+    p2_full_stokesvar_{i}_{j}_blending_q3); mu as the k argument of the other elementwise operators."""
+
+    def __init__(self, storage, min_level, max_level, ctx, viscosity=None, blending=None):
+        self.storage, self.ctx = storage, ctx
+        self.min_level, self.max_level = min_level, max_level
+        c = _coeff(viscosity)
+        h = C.c_void_p()
+        _check(lib().hyb_op_create_p2_full_viscous(ctx.h, storage.h, min_level, max_level, C.byref(c),
+                                                   1 if blending == "shell" else 0, C.byref(h)))
+        self.h = h
+
+    @staticmethod
+    def _arr(u):
+        return (C.c_void_p * 3)(*[f.h.value for f in u])
+
+    def apply(self, src, dst, level, flag=Inner, updateType=Replace):
+        _check(lib().hyb_p2_full_viscous_apply(self.h, self._arr(src), self._arr(dst), level, flag, updateType))
+
+    def getInverseDiagonalValues(self, out, level):
+        _check(lib().hyb_p2_full_viscous_inverse_diagonal(self.h, self._arr(out), level))
 
     def close(self):
         if getattr(self, "h", None):

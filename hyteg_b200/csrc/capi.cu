@@ -1130,6 +1130,8 @@ static void check_op_fn( hyb_op* op, hyb_fn* f, int L )
    require( f->f.lshift == op->o.order - 1, "P1 function given to a P2 operator or the other way round" );
    require_level( f->f, L );
    require( L >= op->o.minL && L <= op->o.maxL, "level outside the operator's level range" );
+   require( op->o.kind != HYB_P2P1_DIV && op->o.kind != HYB_P2_FULL_VISCOUS,
+            "block operators are applied through their own entry points (hyb_p2p1_div_apply, hyb_p2_full_viscous_apply)" );
 }
 
 static void stencil( hyb_op* op, int L, int dtype, int code, uint32_t flag, int copy_unflagged, const void* src, const void* v1,
@@ -2138,6 +2140,74 @@ int hyb_p1p2_divt_apply( hyb_op* d, hyb_fn* p, hyb_fn* const* u, int level, uint
    stokes_blocks_check( d, u, p, level );
    void* uu[3] = { u[0]->f.ptr( level + 1 ), u[1]->f.ptr( level + 1 ), u[2]->f.ptr( level + 1 ) };
    launch_stokes_div( &d->ctx->c, &d->o, level, p->f.dtype, 1, nullptr, p->f.ptr( level ), uu, nullptr, flag, update == HYB_ADD );
+   HYB_CATCH
+}
+
+int hyb_op_create_p2_full_viscous( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, const hyb_coeff* viscosity, int blending,
+                                   hyb_op** out )
+{
+   HYB_TRY
+   require( min_level >= 0 && min_level <= max_level && max_level <= 12, "invalid level range" );
+   const int rc = hyb_op_create_divkgrad( ctx, mesh, min_level + 1, max_level + 1, viscosity, blending, out );
+   if ( rc != HYB_OK ) return rc;
+   ( *out )->o.order = 2;
+   ( *out )->o.kind  = HYB_P2_FULL_VISCOUS;
+   HYB_CATCH
+}
+
+static void visc_fns_check( hyb_op* op, hyb_fn* const* u, int level )
+{
+   require( op && u && u[0] && u[1] && u[2], "NULL argument" );
+   require( op->o.kind == HYB_P2_FULL_VISCOUS, "not a full viscous operator" );
+   for ( int k = 0; k < 3; ++k )
+   {
+      require( u[k]->f.lshift == 1, "velocity components must be P2 functions" );
+      require( u[k]->f.dtype == u[0]->f.dtype, "component value types differ" );
+      require( u[k]->f.mesh == op->o.mesh, "functions live on another mesh" );
+      require_level( u[k]->f, level + 1 );
+   }
+   require( level + 1 >= op->o.minL && level + 1 <= op->o.maxL, "level outside the operator's range" );
+}
+
+int hyb_p2_full_viscous_apply( hyb_op* op, hyb_fn* const* src, hyb_fn* const* dst, int level, uint32_t flag, int update )
+{
+   HYB_TRY
+   visc_fns_check( op, src, level );
+   visc_fns_check( op, dst, level );
+   require( src[0]->f.dtype == dst[0]->f.dtype, "src and dst value types differ" );
+   require( update == HYB_REPLACE || update == HYB_ADD, "update must be HYB_REPLACE or HYB_ADD" );
+   for ( int i = 0; i < 3; ++i )
+      for ( int j = 0; j < 3; ++j ) require( src[i] != dst[j], "src and dst must differ" );
+   const int   Ls    = level + 1;
+   const void* u[3]  = { src[0]->f.ptr( Ls ), src[1]->f.ptr( Ls ), src[2]->f.ptr( Ls ) };
+   void*       d[3]  = { dst[0]->f.ptr( Ls ), dst[1]->f.ptr( Ls ), dst[2]->f.ptr( Ls ) };
+   launch_full_viscous( &op->ctx->c, &op->o, level, src[0]->f.dtype, 0, u, d, flag, update == HYB_ADD );
+   HYB_CATCH
+}
+
+int hyb_p2_full_viscous_inverse_diagonal( hyb_op* op, hyb_fn* const* out, int level )
+{
+   HYB_TRY
+   visc_fns_check( op, out, level );
+   const int     Ls  = level + 1;
+   ElemLevel&    e   = op->o.el[Ls];
+   const int64_t cnt = op->o.mesh->level( Ls ).size;
+   if ( !e.d_invd[F64] )
+   {
+      // the inverse diagonals of the three diagonal blocks, FP64, computed once per level
+      void* p = nullptr;
+      check_cuda( cudaMalloc( &p, size_t( 3 * cnt ) * sizeof( double ) ), "cudaMalloc(inverse diagonal)" );
+      e.d_invd[F64] = p;
+      double* dd    = reinterpret_cast< double* >( p );
+      void*   d[3]  = { dd, dd + cnt, dd + 2 * cnt };
+      launch_full_viscous( &op->ctx->c, &op->o, level, F64, 1, nullptr, d, kAll, 0 );
+   }
+   const double* dd = reinterpret_cast< const double* >( e.d_invd[F64] );
+   for ( int k = 0; k < 3; ++k )
+   {
+      launch_convert( &op->ctx->c, cnt, out[k]->f.dtype, out[k]->f.ptr( Ls ), F64, dd + k * cnt );
+      sync_copies( out[k], Ls );
+   }
    HYB_CATCH
 }
 

@@ -304,6 +304,11 @@ void ensure_stokes_constants();
 void launch_stokes_div( Context* ctx, Operator* op, int Lp, int dtype, int divt, const void* const* u, const void* p, void* const* dst_u,
                         void* dst_p, uint32_t flag, int add );
 
+// full viscous velocity block on P2 level Lp (storage Lp+1): mode 0 dst[k] (+)= sum_j A_kj u[j] on
+// flagged owners; mode 1 writes 1/diag(A_kk) into the accumulation-precision arrays dst[k] (u unused)
+void launch_full_viscous( Context* ctx, Operator* op, int Lp, int dtype, int mode, const void* const* u, void* const* dst, uint32_t flag,
+                          int add );
+
 enum PointOp : int {
    PT_LINCOMB = 0,  // dst = a0*s0 + a1*s1 + a2*s2 (nsrc terms)
    PT_ADD,          // dst += a0*s0 + a1*s1 + a2*s2

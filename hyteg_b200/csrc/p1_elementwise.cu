@@ -942,22 +942,30 @@ void ensure_stokes_constants()
 }
 
 // inverse of the blended Jacobian M = DF J at reference point xi and |det M|
+// (Fq, when given, receives the blended point)
 template < typename A >
-__device__ __forceinline__ void mapped_point( const CellGeom& g, const A X0[3], const A J[3][3], const double* xi, A Mi[3][3], A& adet )
+__device__ __forceinline__ void mapped_point( const CellGeom& g, const A X0[3], const A J[3][3], const double* xi, A Mi[3][3], A& adet,
+                                              A* Fq = nullptr )
 {
    A Xq[3];
    for ( int r = 0; r < 3; ++r ) Xq[r] = X0[r] + J[r][0] * A( xi[0] ) + J[r][1] * A( xi[1] ) + J[r][2] * A( xi[2] );
    A M[3][3];
    if ( g.blend == 1 )
    {
-      A DF[3][3], Fq[3];
-      shell_map( g, Xq, Fq, DF );
+      A DF[3][3], Fl[3];
+      shell_map( g, Xq, Fl, DF );
       for ( int r = 0; r < 3; ++r )
          for ( int c = 0; c < 3; ++c ) M[r][c] = DF[r][0] * J[0][c] + DF[r][1] * J[1][c] + DF[r][2] * J[2][c];
+      if ( Fq )
+         for ( int r = 0; r < 3; ++r ) Fq[r] = Fl[r];
    }
    else
+   {
       for ( int r = 0; r < 3; ++r )
          for ( int c = 0; c < 3; ++c ) M[r][c] = J[r][c];
+      if ( Fq )
+         for ( int r = 0; r < 3; ++r ) Fq[r] = Xq[r];
+   }
    const A c00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
    const A c01 = M[1][2] * M[2][0] - M[1][0] * M[2][2];
    const A c02 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
@@ -1469,6 +1477,223 @@ void launch_stokes_div( Context* ctx, Operator* op, int Lp, int dtype, int divt,
    if ( dtype == F64 ) run_stokes< double, double >( ctx, op, Lp, divt, u, p, dst_u, dst_p, flag, add );
    else if ( dtype == F32 ) run_stokes< float, float >( ctx, op, Lp, divt, u, p, dst_u, dst_p, flag, add );
    else run_stokes< __half, float >( ctx, op, Lp, divt, u, p, dst_u, dst_p, flag, add );
+}
+
+// ---------------------------------------------------------------------------------------------
+// Full viscous velocity block (P2ElementwiseBlendingFullViscousOperator.hpp:34-68): block (i, j) is
+// the form p2_full_stokesvar_{i}_{j}_blending_q3, int 2 mu eps(u) : eps(v) - (2/3) mu div u div v
+// with mu evaluated at the blended point, Yu's 5-point degree-3 rule.  Applied matrix-free per
+// micro-cell: at each point the velocity gradient g (g_ik = d u_i / d x_k) of the ten local nodes
+// gives the stress s = w mu |det| (g + g^T - (2/3) tr(g) I), and node a of component i receives
+// grad phi_a . s_i.  The diagonal pass sums w mu |det| (|grad phi_a|^2 + (1/3) (d_i phi_a)^2).  Same
+// parity passes as the coupling blocks (anchors of one class share no P2 node).
+// ---------------------------------------------------------------------------------------------
+__constant__ double c_yu5_rgrad[5][10][3];
+
+static void ensure_visc_constants()
+{
+   static bool done = false;
+   if ( done ) return;
+   const double lg[4][3] = { { -1, -1, -1 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } };
+   const int    ed[6][2] = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
+   const double pts[5][3] = { { 0.25, 0.25, 0.25 },
+                              { 1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0 },
+                              { 0.5, 1.0 / 6.0, 1.0 / 6.0 },
+                              { 1.0 / 6.0, 0.5, 1.0 / 6.0 },
+                              { 1.0 / 6.0, 1.0 / 6.0, 0.5 } };
+   double g[5][10][3];
+   for ( int q = 0; q < 5; ++q )
+   {
+      const double lam[4] = { 1.0 - pts[q][0] - pts[q][1] - pts[q][2], pts[q][0], pts[q][1], pts[q][2] };
+      for ( int i = 0; i < 4; ++i )
+         for ( int d = 0; d < 3; ++d ) g[q][i][d] = ( 4.0 * lam[i] - 1.0 ) * lg[i][d];
+      for ( int e = 0; e < 6; ++e )
+         for ( int d = 0; d < 3; ++d )
+            g[q][4 + e][d] = 4.0 * ( lam[ed[e][0]] * lg[ed[e][1]][d] + lam[ed[e][1]] * lg[ed[e][0]][d] );
+   }
+   check_cuda( cudaMemcpyToSymbol( c_yu5_rgrad, g, sizeof( g ) ), "viscous block constants" );
+   done = true;
+}
+
+template < typename T, typename A, int MODE >
+__global__ void __launch_bounds__( 128 ) k_visc_pass( int ne, int nanch, const int* __restrict__ anch, const int64_t* __restrict__ off_u,
+                                                       const CellGeom* __restrict__ geom, Coefficient kc, const T* __restrict__ u0,
+                                                       const T* __restrict__ u1, const T* __restrict__ u2, A* acc0, A* acc1, A* acc2,
+                                                       int64_t size_u, int* err )
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   const int c = blockIdx.y;
+   if ( t >= nanch ) return;
+   const int      a  = anch[t];
+   const int      x = a & 1023, y = ( a >> 10 ) & 1023, z = a >> 20, ns = 2 * ne;
+   const CellGeom g  = geom[c];
+   const int64_t  bu = off_u[c];
+   const A        inv_n = A( 1.0 / double( ne ) );
+   A              st[3][3];
+   for ( int k = 0; k < 3; ++k )
+      for ( int d = 0; d < 3; ++d ) st[k][d] = ( A( g.P[k + 1][d] ) - A( g.P[0][d] ) ) * inv_n;
+   for ( int ty = 0; ty < 6; ++ty )
+   {
+      if ( x + y + z > ne - 1 - c_mc_shift[ty] ) continue;
+      int V[4][3];
+      for ( int m = 0; m < 4; ++m )
+         for ( int d = 0; d < 3; ++d ) V[m][d] = ( d == 0 ? x : d == 1 ? y : z ) + c_mc_off[ty][m][d];
+      int64_t iu[10];
+      for ( int m = 0; m < 4; ++m ) iu[m] = bu + cidx( ns, 2 * V[m][0], 2 * V[m][1], 2 * V[m][2] );
+      for ( int e = 0; e < 6; ++e )
+      {
+         const int ea = c_p2_edge[e][0], eb = c_p2_edge[e][1];
+         iu[4 + e]    = bu + cidx( ns, V[ea][0] + V[eb][0], V[ea][1] + V[eb][1], V[ea][2] + V[eb][2] );
+      }
+      {
+         bool bad = false;
+         for ( int m = 0; m < 10; ++m ) bad |= iu[m] < 0 || iu[m] >= size_u;
+         if ( bad )
+         {
+            atomicExch( err, 2 );
+            continue;
+         }
+      }
+      A X0[3], J[3][3];
+      for ( int d = 0; d < 3; ++d )
+      {
+         X0[d] = A( g.P[0][d] ) + st[0][d] * A( V[0][0] ) + st[1][d] * A( V[0][1] ) + st[2][d] * A( V[0][2] );
+         for ( int k = 0; k < 3; ++k )
+            J[d][k] = st[0][d] * A( V[k + 1][0] - V[0][0] ) + st[1][d] * A( V[k + 1][1] - V[0][1] ) + st[2][d] * A( V[k + 1][2] - V[0][2] );
+      }
+      A ul[3][10];
+      if constexpr ( MODE == 0 )
+         for ( int j = 0; j < 10; ++j )
+         {
+            ul[0][j] = A( ld_any( u0 + iu[j] ) );
+            ul[1][j] = A( ld_any( u1 + iu[j] ) );
+            ul[2][j] = A( ld_any( u2 + iu[j] ) );
+         }
+      A yl[3][10];
+      for ( int k = 0; k < 3; ++k )
+         for ( int j = 0; j < 10; ++j ) yl[k][j] = A( 0 );
+      for ( int q = 0; q < 5; ++q )
+      {
+         A Mi[3][3], adet, Fq[3];
+         mapped_point( g, X0, J, c_yu5_pts[q], Mi, adet, Fq );
+         const A s = A( c_yu5_w[q] ) * coeff_eval( kc, Fq ) * adet;
+         if constexpr ( MODE == 0 )
+         {
+            A gr[3][3];
+            for ( int i = 0; i < 3; ++i )
+               for ( int k = 0; k < 3; ++k ) gr[i][k] = A( 0 );
+            for ( int b = 0; b < 10; ++b )
+            {
+               A G[3];
+               for ( int k = 0; k < 3; ++k )
+                  G[k] = A( c_yu5_rgrad[q][b][0] ) * Mi[0][k] + A( c_yu5_rgrad[q][b][1] ) * Mi[1][k] + A( c_yu5_rgrad[q][b][2] ) * Mi[2][k];
+               for ( int i = 0; i < 3; ++i )
+                  for ( int k = 0; k < 3; ++k ) gr[i][k] += ul[i][b] * G[k];
+            }
+            const A tr3 = A( 2.0 / 3.0 ) * ( gr[0][0] + gr[1][1] + gr[2][2] );
+            A       sg[3][3];
+            for ( int i = 0; i < 3; ++i )
+               for ( int k = 0; k < 3; ++k ) sg[i][k] = s * ( ( gr[i][k] + gr[k][i] ) - ( i == k ? tr3 : A( 0 ) ) );
+            for ( int b = 0; b < 10; ++b )
+            {
+               A G[3];
+               for ( int k = 0; k < 3; ++k )
+                  G[k] = A( c_yu5_rgrad[q][b][0] ) * Mi[0][k] + A( c_yu5_rgrad[q][b][1] ) * Mi[1][k] + A( c_yu5_rgrad[q][b][2] ) * Mi[2][k];
+               for ( int i = 0; i < 3; ++i ) yl[i][b] += G[0] * sg[i][0] + G[1] * sg[i][1] + G[2] * sg[i][2];
+            }
+         }
+         else
+            for ( int b = 0; b < 10; ++b )
+            {
+               A G[3];
+               for ( int k = 0; k < 3; ++k )
+                  G[k] = A( c_yu5_rgrad[q][b][0] ) * Mi[0][k] + A( c_yu5_rgrad[q][b][1] ) * Mi[1][k] + A( c_yu5_rgrad[q][b][2] ) * Mi[2][k];
+               const A gg = G[0] * G[0] + G[1] * G[1] + G[2] * G[2];
+               for ( int i = 0; i < 3; ++i ) yl[i][b] += s * ( gg + A( 1.0 / 3.0 ) * G[i] * G[i] );
+            }
+      }
+      for ( int j = 0; j < 10; ++j )
+      {
+         acc0[iu[j]] += yl[0][j];
+         acc1[iu[j]] += yl[1][j];
+         acc2[iu[j]] += yl[2][j];
+      }
+   }
+}
+
+template < typename T, typename A >
+static void run_visc( Context* ctx, Operator* op, int Lp, int mode, const void* const* u, void* const* dst, uint32_t flag, int add )
+{
+   Mesh*     m  = op->mesh;
+   const int Ls = Lp + 1;
+   P1Level&  PU = m->level( Ls );
+   ensure_device( m, PU );
+   ensure_visc_constants();
+   if ( !op->d_geom )
+   {
+      check_cuda( cudaMalloc( &op->d_geom, op->geom.size() * sizeof( CellGeom ) ), "cudaMalloc(geometry)" );
+      check_cuda( cudaMemcpy( op->d_geom, op->geom.data(), op->geom.size() * sizeof( CellGeom ), cudaMemcpyHostToDevice ),
+                  "upload geometry" );
+   }
+   ensure_rows( op, Ls );
+   ElemLevel& e = op->el[Ls];
+   if ( !e.d_sacc ) check_cuda( cudaMalloc( &e.d_sacc, size_t( 3 * PU.size ) * sizeof( double ) ), "cudaMalloc(viscous block scratch)" );
+   A* acc = reinterpret_cast< A* >( e.d_sacc );
+   check_cuda( cudaMemsetAsync( acc, 0, size_t( 3 * PU.size ) * sizeof( A ), ctx->stream ), "cudaMemset" );
+   const int nC = m->topo.nC;
+   const T*  u0 = u ? (const T*) u[0] : nullptr;
+   const T*  u1 = u ? (const T*) u[1] : nullptr;
+   const T*  u2 = u ? (const T*) u[2] : nullptr;
+   for ( int pc = 0; pc < 8; ++pc )
+   {
+      const int na = e.aoff[pc + 1] - e.aoff[pc];
+      if ( na <= 0 ) continue;
+      dim3 grid( ( na + 127 ) / 128, nC );
+      if ( mode == 0 )
+         k_visc_pass< T, A, 0 ><<< grid, 128, 0, ctx->stream >>>( 1 << Lp, na, e.d_anch + e.aoff[pc], PU.d_off + PU.nB, op->d_geom, op->coeff,
+                                                                 u0, u1, u2, acc, acc + PU.size, acc + 2 * PU.size, PU.size,
+                                                                 ctx->d_error );
+      else
+         k_visc_pass< T, A, 1 ><<< grid, 128, 0, ctx->stream >>>( 1 << Lp, na, e.d_anch + e.aoff[pc], PU.d_off + PU.nB, op->d_geom, op->coeff,
+                                                                 u0, u1, u2, acc, acc + PU.size, acc + 2 * PU.size, PU.size,
+                                                                 ctx->d_error );
+      ++ctx->launches;
+   }
+   check_cuda( cudaGetLastError(), "viscous block pass launch" );
+   if ( mode == 0 )
+   {
+      for ( int k = 0; k < 3; ++k )
+      {
+         if ( add ) combine_acc< T, A, OP_APPLY_ADD >( ctx, m, Ls, acc + k * PU.size, flag, (T*) dst[k] );
+         else combine_acc< T, A, OP_APPLY >( ctx, m, Ls, acc + k * PU.size, flag, (T*) dst[k] );
+      }
+      return;
+   }
+   // diagonal: owners sum their copies, then 1/diag on every owned node (dst: three A arrays)
+   const int nrows = int( PU.rows.size() );
+   for ( int k = 0; k < 3; ++k )
+   {
+      A* invd = reinterpret_cast< A* >( dst[k] );
+      check_cuda( cudaMemsetAsync( invd, 0, size_t( PU.size ) * sizeof( A ), ctx->stream ), "cudaMemset" );
+      if ( nrows > 0 )
+      {
+         dim3 grid( ( nrows + 7 ) / 8, nC );
+         k_cell_invert< A ><<< grid, 256, 0, ctx->stream >>>( PU.n, nrows, PU.d_rows, PU.d_off + PU.nB, acc + k * PU.size, invd );
+      }
+      if ( !PU.tasks.empty() )
+         k_bnd_acc< T, A, OP_APPLY ><<< ( int( PU.tasks.size() ) + 255 ) / 256, 256, 0, ctx->stream >>>(
+             PU.n, int( PU.tasks.size() ), PU.d_tasks, PU.d_off, PU.d_off + PU.nB, PU.d_bkind, PU.d_bc, PU.d_inc_begin, PU.d_inc, kAll, 0,
+             acc + k * PU.size, nullptr, invd, nullptr, nullptr, nullptr, nullptr, A( 0 ), A( 0 ) );
+   }
+   check_cuda( cudaGetLastError(), "viscous block diagonal launch" );
+}
+
+void launch_full_viscous( Context* ctx, Operator* op, int Lp, int dtype, int mode, const void* const* u, void* const* dst, uint32_t flag,
+                          int add )
+{
+   if ( dtype == F64 ) run_visc< double, double >( ctx, op, Lp, mode, u, dst, flag, add );
+   else if ( dtype == F32 ) run_visc< float, float >( ctx, op, Lp, mode, u, dst, flag, add );
+   else run_visc< __half, float >( ctx, op, Lp, mode, u, dst, flag, add );
 }
 
 void launch_elementwise( Context* ctx, Mesh* m, Operator* op, int L, int dtype, const StencilArgs& a )

@@ -54,6 +54,7 @@ extern "C" {
 #define HYB_P2_ELEM_DIVKGRAD 4 /* P2ElementwiseBlendingDivKGradOperator (elementwiseoperators/P2ElementwiseOperator.hpp:475) */
 #define HYB_P2P1_DIV 5 /* P2ToP1ElementwiseBlendingDivOperator / P1ToP2ElementwiseBlendingDivTOperator (P2P1ElementwiseBlendingStokesOperator.hpp:113-116) */
 #define HYB_P1_PSPG 6  /* P1PSPGOperator; its inverted diagonal is P1PSPGInvDiagOperator (P1ConstantOperator.hpp:200-210) */
+#define HYB_P2_FULL_VISCOUS 7 /* P2ElementwiseBlendingFullViscousOperator (elementwiseoperators/P2ElementwiseBlendingFullViscousOperator.hpp:34-68) */
 
 /* blending maps (geometry/) */
 #define HYB_BLEND_NONE 0
@@ -352,6 +353,18 @@ int hyb_p2p1_div_apply( hyb_op* div, hyb_fn* const* u3, hyb_fn* p, int level, ui
 int hyb_p1p2_divt_apply( hyb_op* div, hyb_fn* p, hyb_fn* const* u3, int level, uint32_t flag, int update );
 /* P1PSPGOperator on the affine macro geometry; hyb_op_inverse_diagonal gives P1PSPGInvDiagOperator's values */
 int hyb_op_create_p1_pspg( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, hyb_op** out );
+
+/* P2ElementwiseBlendingFullViscousOperator (elementwiseoperators/P2ElementwiseBlendingFullViscousOperator.hpp:
+ * 34-68): the velocity block 2 mu eps(u) : eps(v) - (2/3) mu div u div v coupling the three P2
+ * components, block (i, j) the form p2_full_stokesvar_{i}_{j}_blending_q3 (Yu's 5-point rule, mu at
+ * the blended point); applied matrix-free.  VectorToVectorOperator::apply (mixed_operator/
+ * VectorToVectorOperator.hpp) maps to hyb_p2_full_viscous_apply: dst_i (update)= sum_j A_ij src_j on
+ * the flagged owned DoFs.  hyb_p2_full_viscous_inverse_diagonal writes 1/diag(A_ii) into out_i
+ * (OperatorWithInverseDiagonal::computeInverseDiagonalOperatorValues / getInverseDiagonalValues). */
+int hyb_op_create_p2_full_viscous( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, const hyb_coeff* viscosity,
+                                   int blending, hyb_op** out );
+int hyb_p2_full_viscous_apply( hyb_op* op, hyb_fn* const* src3, hyb_fn* const* dst3, int level, uint32_t flag, int update );
+int hyb_p2_full_viscous_inverse_diagonal( hyb_op* op, hyb_fn* const* out3, int level );
 
 typedef struct hyb_stokes hyb_stokes;
 typedef struct hyb_stokes_params

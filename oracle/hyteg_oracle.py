@@ -1329,6 +1329,32 @@ def p2p1_div_element(X, blend=None):
     return B
 
 
+def p2_full_viscous_element(X, mufun, blend=None, rule=(YU5_POINTS, YU5_WEIGHTS)):
+    """Element matrices (m, 3, 3, 10, 10) of the full viscous velocity block
+    (P2ElementwiseBlendingFullViscousOperator.hpp:34-68, forms p2_full_stokesvar_{i}_{j}_blending_q3,
+    Yu's 5-point degree-3 rule): block (i, j) maps component j of the trial function to component i
+    of the test function, int 2 mu eps(phi_b e_j) : eps(phi_a e_i) - (2/3) mu div(phi_b e_j) div(phi_a e_i)
+    = int mu (delta_ij grad phi_a . grad phi_b + d_j phi_a d_i phi_b - (2/3) d_i phi_a d_j phi_b),
+    with mu evaluated at the blended quadrature point."""
+    J = np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], axis=2)
+    K = np.zeros((X.shape[0], 3, 3, 10, 10))
+    eye = np.eye(3)
+    for xi, w in zip(*rule):
+        Xq = X[:, 0] + np.einsum("kij,j->ki", J, xi)
+        if blend is None:
+            M, Fq = J, Xq
+        else:
+            M, Fq = np.einsum("kij,kjl->kil", blend.DF(Xq), J), blend.F(Xq)
+        s = w * mufun(Fq) * np.abs(np.linalg.det(M))
+        G = np.einsum("id,kdj->kij", p2_ref_gradients(xi), np.linalg.inv(M))  # (m, 10, 3)
+        lap = np.einsum("kad,kbd->kab", G, G)
+        K += s[:, None, None, None, None] * (
+            eye[None, :, :, None, None] * lap[:, None, None]
+            + np.einsum("kaj,kbi->kijab", G, G)
+            - (2.0 / 3.0) * np.einsum("kai,kbj->kijab", G, G))
+    return K
+
+
 def p1_pspg_element(X):
     """Element matrices (m, 4, 4) of the P1 PSPG form (p1_tet_pspg_tet.h) on affine tets:
     -(|T|^(2/3) / 12) |T| grad l_i . grad l_j."""
@@ -1337,6 +1363,51 @@ def p1_pspg_element(X):
     G = np.concatenate([-Ji.sum(axis=1, keepdims=True), Ji], axis=1)  # rows: gradients of l_0..l_3
     vol = np.abs(np.linalg.det(J)) / 6.0
     return (-(vol ** (2.0 / 3.0)) / 12.0 * vol)[:, None, None] * np.einsum("kid,kjd->kij", G, G)
+
+
+class P2FullViscous:
+    """P2ElementwiseBlendingFullViscousOperator (elementwiseoperators/P2ElementwiseBlendingFullViscousOperator
+    .hpp:34-68): the 3 x 3 block operator of p2_full_stokesvar_{i}_{j}_blending_q3 assembled from the
+    element matrices of every micro-cell; apply follows VectorToVectorOperator::apply (dst_i = sum_j
+    A_ij src_j on the flagged owned DoFs).  P2 level L lives on the node set of Level L+1."""
+
+    def __init__(self, mesh, minL, maxL, mufun, blending=None):
+        self.mesh, self.minL, self.maxL = mesh, minL, maxL
+        self.maps = [IcosahedralShellMap(mesh, c) for c in range(mesh.nC)] if blending == "shell" else None
+        self.levels = {L: Level(mesh, L + 1) for L in range(minL, maxL + 1)}
+        self.A, self.invdiag = {}, {}
+        for L in range(minL, maxL + 1):
+            lev = self.levels[L]
+            rows, cols, vals = [], [], [[[] for _ in range(3)] for _ in range(3)]
+            for c in range(mesh.nC):
+                slots, X = p2_micro_cells(lev, c)
+                K = p2_full_viscous_element(X, mufun, None if self.maps is None else _PerPointMap(self.maps[c]))
+                rows.append(np.repeat(slots, 10, axis=1).ravel())
+                cols.append(np.tile(slots, (1, 10)).ravel())
+                for i in range(3):
+                    for j in range(3):
+                        vals[i][j].append(K[:, i, j].reshape(K.shape[0], 100).ravel())
+            r, cc = np.concatenate(rows), np.concatenate(cols)
+            self.A[L] = [[sp.coo_matrix((np.concatenate(vals[i][j]), (r, cc)), shape=(lev.size, lev.size)).tocsr()
+                          for j in range(3)] for i in range(3)]
+            own = lev.owned
+            inv = []
+            for i in range(3):
+                d = self.A[L][i][i].diagonal()
+                v = np.zeros_like(d)
+                v[own] = 1.0 / d[own]
+                inv.append(v)
+            self.invdiag[L] = inv
+
+    def apply(self, src, dst, L, flag, add=False):
+        mask = self.levels[L].owned_mask(flag)
+        for i in range(3):
+            y = sum(self.A[L][i][j] @ src[j] for j in range(3))
+            if add:
+                dst[i][mask] += y[mask]
+            else:
+                dst[i][mask] = y[mask]
+        return dst
 
 
 class P2P1Stokes:

@@ -269,3 +269,43 @@ extern "C" void ref_p1_pspg_element( const double* coords12, double* A16 )
    p1_tet_pspg_tet_cell_integral_0_otherwise form;
    form.tabulate_tensor( A16, nullptr, coords12, 0 );
 }
+
+// ---------------------------------------------------------------------------------------------
+// Full viscous velocity block (P2ElementwiseBlendingFullViscousOperator, .hpp:34-68): block (i, j)
+// is p2_full_stokesvar_{i}_{j}_blending_q3 with the variable viscosity mu (the exp-sin test
+// coefficient here), 2 mu eps(u) : eps(v) - (2/3) mu div u div v.  Row-major 10x10 element matrix.
+// ---------------------------------------------------------------------------------------------
+#include "hyteg/forms/form_hyteg_generated/p2/p2_full_stokesvar_blending_q3.hpp"
+
+extern "C" void ref_p2_full_viscous_element( const double* coords12, int map_kind, double map_a, int bi, int bj, double k_amp,
+                                              const double* k_phase3, double* A100 )
+{
+   auto map  = std::make_shared< TestMap >();
+   map->kind = map_kind;
+   map->a    = map_a;
+   const double amp   = k_amp;
+   const double ph[3] = { k_phase3[0], k_phase3[1], k_phase3[2] };
+   std::function< double( const hyteg::Point3D& ) > mu = [amp, ph]( const hyteg::Point3D& p ) {
+      const double tp = 2.0 * 3.14159265358979323846;
+      return std::exp( amp * std::sin( tp * ( p[0] + ph[0] ) ) * std::cos( tp * ( p[1] + ph[1] ) ) * std::sin( tp * ( p[2] + ph[2] ) ) );
+   };
+   std::array< hyteg::Point3D, 4 > c;
+   for ( int v = 0; v < 4; ++v ) c[v] = hyteg::Point3D( coords12[3 * v], coords12[3 * v + 1], coords12[3 * v + 2] );
+   hyteg::Matrix< double, 10, 10 > M;
+   auto run = [&]( auto&& f ) {
+      f.setGeometryMap( map );
+      f.integrateAll( c, M );
+   };
+   using namespace hyteg::forms;
+   const int b = 3 * bi + bj;
+   if ( b == 0 ) run( p2_full_stokesvar_0_0_blending_q3( mu, mu ) );
+   else if ( b == 1 ) run( p2_full_stokesvar_0_1_blending_q3( mu, mu ) );
+   else if ( b == 2 ) run( p2_full_stokesvar_0_2_blending_q3( mu ) );
+   else if ( b == 3 ) run( p2_full_stokesvar_1_0_blending_q3( mu, mu ) );
+   else if ( b == 4 ) run( p2_full_stokesvar_1_1_blending_q3( mu, mu ) );
+   else if ( b == 5 ) run( p2_full_stokesvar_1_2_blending_q3( mu ) );
+   else if ( b == 6 ) run( p2_full_stokesvar_2_0_blending_q3( mu ) );
+   else if ( b == 7 ) run( p2_full_stokesvar_2_1_blending_q3( mu ) );
+   else run( p2_full_stokesvar_2_2_blending_q3( mu ) );
+   for ( int i = 0; i < 100; ++i ) A100[i] = M.a[i];
+}

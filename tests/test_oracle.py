@@ -335,6 +335,48 @@ def test_stokes_div_element_matches_reference_forms(kind, a):
         assert np.abs(B[k].T - out.reshape(10, 4)).max() < 1e-15
 
 
+@pytest.mark.parametrize("kind,a", [(0, 0.0), (1, 0.3)])
+def test_full_viscous_element_matches_reference_forms(kind, a):
+    """The nine blocks p2_full_stokesvar_{i}_{j}_blending_q3 (compiled from the reference) equal the
+    oracle's full viscous element matrix, with the exp-sin viscosity; identity and a non-affine
+    test map, several element shapes."""
+    import ctypes as C
+    lib = _ref_lib()
+    rng = np.random.default_rng(21)
+    ph = np.array([0.13, 0.27, 0.41])
+    for _ in range(4):
+        X = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], dtype=float) * 0.3 + rng.uniform(-0.05, 0.05, (4, 3)) + 0.2
+        K = O.p2_full_viscous_element(X[None], O.k_expsin(0.5, ph), O.TestMap(a) if kind == 1 else None)[0]
+        for i in range(3):
+            for j in range(3):
+                out = np.zeros(100)
+                lib.ref_p2_full_viscous_element(X.ctypes.data_as(C.c_void_p), kind, C.c_double(a), i, j, C.c_double(0.5),
+                                                ph.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p))
+                assert np.abs(K[i, j] - out.reshape(10, 10)).max() <= 1e-13 * np.abs(out).max()
+
+
+def test_full_viscous_oracle_properties():
+    """Rigid-body motions (constant and rotational velocities) are in the kernel of the full viscous
+    block on inner DoFs, the operator is symmetric, and its diagonal blocks differ from the
+    component Laplacian only by the grad-div terms."""
+    coords, tets = M.ALL["cube_6"]()
+    mesh = O.MacroMesh(coords, tets)
+    op = O.P2FullViscous(mesh, 2, 2, lambda P: np.ones(len(P)))
+    L = 2
+    lev = op.levels[L]
+    X = _slot_coords(lev)
+    inner = lev.owned_mask(O.INNER)
+    for u in ([np.ones(lev.size), np.zeros(lev.size), np.zeros(lev.size)],
+              [-X[:, 1], X[:, 0], np.zeros(lev.size)],
+              [np.zeros(lev.size), -X[:, 2], X[:, 1]]):
+        y = op.apply(u, [np.zeros(lev.size) for _ in range(3)], L, O.INNER)
+        for i in range(3):
+            assert np.abs(y[i][inner]).max() < 1e-11
+    for i in range(3):
+        for j in range(3):
+            assert abs(op.A[L][i][j] - op.A[L][j][i].T).max() < 1e-14
+
+
 def test_pspg_element_matches_reference_form():
     import ctypes as C
     lib = _ref_lib()
