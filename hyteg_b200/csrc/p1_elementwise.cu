@@ -656,19 +656,49 @@ __global__ void __launch_bounds__( 256 ) k_cell_acc( int n, int nrows, const int
    }
 }
 
+// cell-array slot of the copy of task tk's point in incidence I
+__device__ __forceinline__ int64_t inc_slot( int n, const int4& tk, const Incidence& I, const int64_t* __restrict__ cell_off )
+{
+   const int x = n * I.o[0] + tk.y * I.e1[0] + tk.z * I.e2[0];
+   const int y = n * I.o[1] + tk.y * I.e1[1] + tk.z * I.e2[1];
+   const int z = n * I.o[2] + tk.y * I.e1[2] + tk.z * I.e2[2];
+   return __ldg( cell_off + I.cell ) + cidx( n, x, y, z );
+}
+
+// owner and copies take val; the incidences are read four at a time ahead of their stores, so a
+// vertex with many cells does not wait on one incidence read per copy
 template < typename T, typename A >
-__device__ __forceinline__ void wt_store( int n, const int4& tk, int64_t owner, const int* inc_begin, const Incidence* inc,
-                                          const int64_t* cell_off, T* vec, A val )
+__device__ __forceinline__ void wt_store( int n, const int4& tk, int64_t owner, const int* __restrict__ inc_begin,
+                                          const Incidence* __restrict__ inc, const int64_t* __restrict__ cell_off, T* vec, A val )
 {
    st_any( vec + owner, val );
-   for ( int q = inc_begin[tk.x]; q < inc_begin[tk.x + 1]; ++q )
+   const int q1 = __ldg( inc_begin + tk.x + 1 );
+   for ( int q = __ldg( inc_begin + tk.x ); q < q1; q += 4 )
    {
-      const Incidence I = inc[q];
-      const int       x = n * I.o[0] + tk.y * I.e1[0] + tk.z * I.e2[0];
-      const int       y = n * I.o[1] + tk.y * I.e1[1] + tk.z * I.e2[1];
-      const int       z = n * I.o[2] + tk.y * I.e1[2] + tk.z * I.e2[2];
-      st_any( vec + cell_off[I.cell] + cidx( n, x, y, z ), val );
+      int64_t sl[4];
+#pragma unroll
+      for ( int u = 0; u < 4; ++u ) sl[u] = q + u < q1 ? inc_slot( n, tk, inc[q + u], cell_off ) : -1;
+#pragma unroll
+      for ( int u = 0; u < 4; ++u )
+         if ( sl[u] >= 0 ) st_any( vec + sl[u], val );
    }
+}
+
+// sum over the incidences q0..q1-1 of f(incidence), in incidence order, four incidences in flight
+template < typename A, int U = 4, typename F >
+__device__ __forceinline__ A inc_sum( int q0, int q1, const Incidence* __restrict__ inc, F f )
+{
+   A s = A( 0 );
+   for ( int q = q0; q < q1; q += U )
+   {
+      A v[U];
+#pragma unroll
+      for ( int u = 0; u < U; ++u ) v[u] = q + u < q1 ? f( inc[q + u] ) : A( 0 );
+#pragma unroll
+      for ( int u = 0; u < U; ++u )
+         if ( q + u < q1 ) s += v[u];
+   }
+   return s;
 }
 
 template < typename T, typename A, int OP >
@@ -693,15 +723,8 @@ __global__ void __launch_bounds__( 256 ) k_bnd_acc( int n, int ntasks, const int
       else if constexpr ( OP == OP_CHEBI ) wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, A( ld_any( v2 + owner ) ) );
       return;
    }
-   A s = A( 0 );
-   for ( int q = inc_begin[b]; q < inc_begin[b + 1]; ++q )
-   {
-      const Incidence I = inc[q];
-      const int       x = n * I.o[0] + tk.y * I.e1[0] + tk.z * I.e2[0];
-      const int       y = n * I.o[1] + tk.y * I.e1[1] + tk.z * I.e2[1];
-      const int       z = n * I.o[2] + tk.y * I.e1[2] + tk.z * I.e2[2];
-      s += acc[cell_off[I.cell] + cidx( n, x, y, z )];
-   }
+   const A s = inc_sum< A >( __ldg( inc_begin + b ), __ldg( inc_begin + b + 1 ), inc,
+                             [&]( const Incidence& I ) { return acc[inc_slot( n, tk, I, cell_off )]; } );
    if ( invd_out )  // diagonal setup: store 1/diag at the owner
    {
       invd_out[owner] = A( 1 ) / s;
@@ -794,15 +817,12 @@ __global__ void __launch_bounds__( 256 ) k_var_bnd( int n, int ntasks, const int
       else if constexpr ( OP == OP_CHEBI ) wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, A( ld_any( v2 + owner ) ) );
       return;
    }
-   A s = A( 0 );
-   for ( int q = inc_begin[b]; q < inc_begin[b + 1]; ++q )
-   {
-      const Incidence I = inc[q];
-      const int       x = n * I.o[0] + tk.y * I.e1[0] + tk.z * I.e2[0];
-      const int       y = n * I.o[1] + tk.y * I.e1[1] + tk.z * I.e2[1];
-      const int       z = n * I.o[2] + tk.y * I.e1[2] + tk.z * I.e2[2];
-      s += var_apply< T, A, false >( S, ssize, src, cell_off[I.cell], n, x, y, z );
-   }
+   const A s = inc_sum< A, 2 >( __ldg( inc_begin + b ), __ldg( inc_begin + b + 1 ), inc, [&]( const Incidence& I ) {
+      const int x = n * I.o[0] + tk.y * I.e1[0] + tk.z * I.e2[0];
+      const int y = n * I.o[1] + tk.y * I.e1[1] + tk.z * I.e2[1];
+      const int z = n * I.o[2] + tk.y * I.e1[2] + tk.z * I.e2[2];
+      return var_apply< T, A, false >( S, ssize, src, __ldg( cell_off + I.cell ), n, x, y, z );
+   } );
    A       second;
    const A val = epilogue_value< T, A, OP >( owner, s, invd[owner], src, v1, v2, a0, a1, &second );
    if constexpr ( OP == OP_CHEBL ) wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, v2, val );
@@ -1180,6 +1200,10 @@ static int64_t kstride( Mesh* m, const Operator* op, int L ) { return int64_t( m
 template < typename A >
 static A* stored_matrices( Operator* op, int L ) { return reinterpret_cast< A* >( op->el[L].d_K[sizeof( A ) == 8 ? 0 : 1] ); }
 
+// threads per block of a pass over na anchors per cell (grid: blocks x cells): whole warps, at most
+// maxb, so that the small levels (a few anchors per cell) do not launch mostly idle blocks
+static int pass_block( int na, int maxb ) { return std::min( maxb, ( na + 31 ) / 32 * 32 ); }
+
 template < typename T, typename A, int MODE >
 static void run_passes( Context* ctx, Mesh* m, Operator* op, int L, const T* src, A* acc )
 {
@@ -1196,20 +1220,23 @@ static void run_passes( Context* ctx, Mesh* m, Operator* op, int L, const T* src
       // P2 stored matrices are grouped by parity class, then cell, micro-cell type and anchor, so the
       // anchors of one pass read consecutive slots
       const int64_t kbase = int64_t( 6 ) * nC * e.aoff[p];
-      dim3 grid( ( na + 255 ) / 256, nC );
+      const int bs = pass_block( na, 256 );
+      dim3      grid( ( na + bs - 1 ) / bs, nC );
       if ( op->order == 2 && MODE == 3 )
       {
-         const dim3 g3( ( na + 23 ) / 24, nC );  // 24 anchors (8 warps x 3 groups) per block
-         k_p2_stored_pass< T, A ><<< g3, 256, 0, ctx->stream >>>( element_n( op, L ), na, e.d_anch + e.aoff[p], P.d_off + P.nB, src,
-                                                                  acc, kst, ks, kbase, P.size, ctx->d_error );
+         // three anchors per warp (ten lanes each), at most 8 warps per block
+         const int  wb = std::min( 8, ( na + 2 ) / 3 );
+         const dim3 g3( ( na + 3 * wb - 1 ) / ( 3 * wb ), nC );
+         k_p2_stored_pass< T, A ><<< g3, 32 * wb, 0, ctx->stream >>>( element_n( op, L ), na, e.d_anch + e.aoff[p], P.d_off + P.nB, src,
+                                                                      acc, kst, ks, kbase, P.size, ctx->d_error );
       }
       else if ( op->order == 2 )
-         k_p2_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( element_n( op, L ), na, e.d_anch + e.aoff[p], P.d_off + P.nB,
-                                                                    op->d_geom, op->coeff, src, acc, kst, ks, kbase, P.size,
-                                                                    ctx->d_error );
+         k_p2_pass< T, A, MODE ><<< grid, bs, 0, ctx->stream >>>( element_n( op, L ), na, e.d_anch + e.aoff[p], P.d_off + P.nB,
+                                                                   op->d_geom, op->coeff, src, acc, kst, ks, kbase, P.size,
+                                                                   ctx->d_error );
       else
-         k_elem_pass< T, A, MODE ><<< grid, 256, 0, ctx->stream >>>( P.n, na, e.d_anch + e.aoff[p], P.d_off + P.nB, op->d_geom,
-                                                                      op->coeff, src, acc, kst, ks, P.size, ctx->d_error );
+         k_elem_pass< T, A, MODE ><<< grid, bs, 0, ctx->stream >>>( P.n, na, e.d_anch + e.aoff[p], P.d_off + P.nB, op->d_geom,
+                                                                     op->coeff, src, acc, kst, ks, P.size, ctx->d_error );
       ++ctx->launches;
    }
    check_cuda( cudaGetLastError(), "elementwise pass launch" );
@@ -1444,17 +1471,18 @@ static void run_stokes( Context* ctx, Operator* op, int Lp, int divt, const void
    {
       const int na = e.aoff[pc + 1] - e.aoff[pc];
       if ( na <= 0 ) continue;
-      dim3 grid( ( na + 255 ) / 256, nC );
+      const int bs = pass_block( na, 256 );
+      dim3      grid( ( na + bs - 1 ) / bs, nC );
       const T* u0 = u ? (const T*) u[0] : nullptr;
       const T* u1 = u ? (const T*) u[1] : nullptr;
       const T* u2 = u ? (const T*) u[2] : nullptr;
       if ( divt )
-         k_stokes_div_pass< T, A, 1 ><<< grid, 256, 0, ctx->stream >>>( 1 << Lp, na, e.d_anch + e.aoff[pc], PP.d_off + PP.nB,
+         k_stokes_div_pass< T, A, 1 ><<< grid, bs, 0, ctx->stream >>>( 1 << Lp, na, e.d_anch + e.aoff[pc], PP.d_off + PP.nB,
                                                                          PU.d_off + PU.nB, op->d_geom, u0, u1, u2, (const T*) p, acc_p,
                                                                          acc_u, acc_u + PU.size, acc_u + 2 * PU.size, PP.size, PU.size,
                                                                          ctx->d_error );
       else
-         k_stokes_div_pass< T, A, 0 ><<< grid, 256, 0, ctx->stream >>>( 1 << Lp, na, e.d_anch + e.aoff[pc], PP.d_off + PP.nB,
+         k_stokes_div_pass< T, A, 0 ><<< grid, bs, 0, ctx->stream >>>( 1 << Lp, na, e.d_anch + e.aoff[pc], PP.d_off + PP.nB,
                                                                          PU.d_off + PU.nB, op->d_geom, u0, u1, u2, (const T*) p, acc_p,
                                                                          acc_u, acc_u + PU.size, acc_u + 2 * PU.size, PP.size, PU.size,
                                                                          ctx->d_error );
@@ -1648,13 +1676,14 @@ static void run_visc( Context* ctx, Operator* op, int Lp, int mode, const void* 
    {
       const int na = e.aoff[pc + 1] - e.aoff[pc];
       if ( na <= 0 ) continue;
-      dim3 grid( ( na + 127 ) / 128, nC );
+      const int bs = pass_block( na, 128 );
+      dim3      grid( ( na + bs - 1 ) / bs, nC );
       if ( mode == 0 )
-         k_visc_pass< T, A, 0 ><<< grid, 128, 0, ctx->stream >>>( 1 << Lp, na, e.d_anch + e.aoff[pc], PU.d_off + PU.nB, op->d_geom, op->coeff,
+         k_visc_pass< T, A, 0 ><<< grid, bs, 0, ctx->stream >>>( 1 << Lp, na, e.d_anch + e.aoff[pc], PU.d_off + PU.nB, op->d_geom, op->coeff,
                                                                  u0, u1, u2, acc, acc + PU.size, acc + 2 * PU.size, PU.size,
                                                                  ctx->d_error );
       else
-         k_visc_pass< T, A, 1 ><<< grid, 128, 0, ctx->stream >>>( 1 << Lp, na, e.d_anch + e.aoff[pc], PU.d_off + PU.nB, op->d_geom, op->coeff,
+         k_visc_pass< T, A, 1 ><<< grid, bs, 0, ctx->stream >>>( 1 << Lp, na, e.d_anch + e.aoff[pc], PU.d_off + PU.nB, op->d_geom, op->coeff,
                                                                  u0, u1, u2, acc, acc + PU.size, acc + 2 * PU.size, PU.size,
                                                                  ctx->d_error );
       ++ctx->launches;

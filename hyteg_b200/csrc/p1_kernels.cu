@@ -183,12 +183,26 @@ template < typename T, typename A >
 __device__ __forceinline__ void write_through( const LevelView& v, T* vec, int b, int i, int j, int64_t owner, A val )
 {
    stv( vec + owner, val );
-   for ( int q = v.inc_begin[b]; q < v.inc_begin[b + 1]; ++q )
+   // incidences read four at a time ahead of their stores (a vertex has many cells)
+   const int q1 = v.inc_begin[b + 1];
+   for ( int q = v.inc_begin[b]; q < q1; q += 4 )
    {
-      const Incidence I = v.inc[q];
-      int             x, y, z;
-      inc_point( I, v.n, i, j, x, y, z );
-      stv( vec + v.cell_off[I.cell] + cidx( v.n, x, y, z ), val );
+      int64_t sl[4];
+#pragma unroll
+      for ( int u = 0; u < 4; ++u )
+      {
+         sl[u] = -1;
+         if ( q + u < q1 )
+         {
+            const Incidence I = v.inc[q + u];
+            int             x, y, z;
+            inc_point( I, v.n, i, j, x, y, z );
+            sl[u] = v.cell_off[I.cell] + cidx( v.n, x, y, z );
+         }
+      }
+#pragma unroll
+      for ( int u = 0; u < 4; ++u )
+         if ( sl[u] >= 0 ) stv( vec + sl[u], val );
    }
 }
 
@@ -1336,13 +1350,25 @@ __global__ void __launch_bounds__( 256 ) k_bnd_stencil( LevelView v, OpView< A >
       acc = ( acc + s0 ) + s1;
    }
    else
-      for ( int q = q0; q < q1; ++q )
+      // edges and vertices: two incidences' stencils in flight, summed in incidence order
+      for ( int q = q0; q < q1; q += 2 )
       {
-         const Incidence I = v.inc[q];
-         int             x, y, z;
-         inc_point( I, n, i, j, x, y, z );
-         acc += class_stencil< T, A >( src + v.cell_off[I.cell], o.W + ( size_t( I.cell ) * kNumClasses + I.cls ) * kNumDirs,
-                                       c_cls_mask[I.cls], n, x, y, z );
+         A sq[2];
+#pragma unroll
+         for ( int u = 0; u < 2; ++u )
+         {
+            sq[u] = A( 0 );
+            if ( q + u < q1 )
+            {
+               const Incidence I = v.inc[q + u];
+               int             x, y, z;
+               inc_point( I, n, i, j, x, y, z );
+               sq[u] = class_stencil< T, A >( src + v.cell_off[I.cell], o.W + ( size_t( I.cell ) * kNumClasses + I.cls ) * kNumDirs,
+                                              c_cls_mask[I.cls], n, x, y, z );
+            }
+         }
+         acc += sq[0];
+         if ( q + 1 < q1 ) acc += sq[1];
       }
    const A invd = o.invd_b[b];
    if constexpr ( OP == OP_APPLY ) write_through( v, dst, b, i, j, owner, acc );
