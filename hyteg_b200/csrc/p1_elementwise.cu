@@ -885,12 +885,12 @@ __global__ void __launch_bounds__( 256 ) k_p2_stored_pass( int ne, int nanch, co
       const int r = min( i, j ), q = max( i, j );
       vrow[j]     = r * 10 - r * ( r - 1 ) / 2 + ( q - r );
    }
-#pragma unroll 1
-   for ( int ty = 0; ty < 6; ++ty )
-   {
+   // node index, stored slot and the self-check of micro-cell type ty (all lanes of the warp take
+   // part: the check is a warp vote)
+   auto prep = [&]( int ty, int64_t& idx, int64_t& slot, bool& go ) {
       const bool cell = live && x + y + z <= ne - 1 - c_mc_shift[ty];
       // node i of the micro-cell: vertex i (i < 4) at 2 V_i, edge (a, b) at V_a + V_b
-      int64_t idx = 0;
+      idx = 0;
       if ( cell )
       {
          int P[3];
@@ -904,23 +904,48 @@ __global__ void __launch_bounds__( 256 ) k_p2_stored_pass( int ne, int nanch, co
          }
          idx = base + cidx( ns, P[0], P[1], P[2] );
       }
-      const int64_t slot = kbase + ( int64_t( c ) * 6 + ty ) * nanch + ( cell ? t : 0 );
+      slot = kbase + ( int64_t( c ) * 6 + ty ) * nanch + ( cell ? t : 0 );
       // self-check: every node inside the level's vector and the stored slot inside its array; a
       // violation in any lane of the group skips the micro-cell and records error word 2
       const bool     bad  = cell && ( idx < 0 || idx >= level_size || slot < 0 || slot >= kstride );
       const unsigned bmsk = __ballot_sync( 0xffffffffu, bad );
       const bool     gbad = grp < 3 && ( ( bmsk >> g0 ) & 0x3ffu ) != 0u;
       if ( bad ) atomicExch( err, 2 );
-      const bool go = cell && !gbad;
-      const A    xi = go ? A( ld_any( src + idx ) ) : A( 0 );
-      A          yi = A( 0 );
+      go = cell && !gbad;
+   };
+   // software pipeline over the six micro-cell types: the node value and matrix row of type ty+1
+   // are loaded before type ty's product and read-modify-write, which are the only steps that must
+   // stay in order (micro-cells of one anchor share nodes)
+   int64_t idx0, slot0;
+   bool    go0;
+   prep( 0, idx0, slot0, go0 );
+   A x0 = go0 ? A( ld_any( src + idx0 ) ) : A( 0 );
+   A k0[10];
+#pragma unroll
+   for ( int j = 0; j < 10; ++j ) k0[j] = go0 ? __ldg( kst + slot0 * 55 + vrow[j] ) : A( 0 );
+#pragma unroll 1
+   for ( int ty = 0; ty < 6; ++ty )
+   {
+      int64_t idx1 = 0, slot1 = 0;
+      bool    go1 = false;
+      A       x1  = A( 0 ), k1[10];
+      if ( ty < 5 ) prep( ty + 1, idx1, slot1, go1 );
+      if ( go1 ) x1 = A( ld_any( src + idx1 ) );
+#pragma unroll
+      for ( int j = 0; j < 10; ++j ) k1[j] = go1 ? __ldg( kst + slot1 * 55 + vrow[j] ) : A( 0 );
+      A yi = A( 0 );
 #pragma unroll
       for ( int j = 0; j < 10; ++j )
       {
-         const A xj = __shfl_sync( 0xffffffffu, xi, grp < 3 ? g0 + j : lane );
-         if ( go ) yi += kst[slot * 55 + vrow[j]] * xj;
+         const A xj = __shfl_sync( 0xffffffffu, x0, grp < 3 ? g0 + j : lane );
+         if ( go0 ) yi += k0[j] * xj;
       }
-      if ( go ) acc[idx] += yi;
+      if ( go0 ) acc[idx0] += yi;
+      idx0 = idx1;
+      go0  = go1;
+      x0   = x1;
+#pragma unroll
+      for ( int j = 0; j < 10; ++j ) k0[j] = k1[j];
    }
 }
 
