@@ -671,22 +671,28 @@ class P1PSPGOperator(_ConstantOperator):
 class _StokesParams(C.Structure):
     _fields_ = [("min_level", C.c_int), ("max_level", C.c_int), ("pre_smooth", C.c_int), ("post_smooth", C.c_int),
                 ("velocity_sweeps", C.c_int), ("cheb_order", C.c_int), ("power_iterations", C.c_int),
-                ("omega", C.c_double), ("coarse_sweeps", C.c_int)]
+                ("omega", C.c_double), ("coarse_sweeps", C.c_int), ("velocity_block", C.c_int)]
 
 
 class StokesUzawaMultigrid:
     """GeometricMultigridSolver< P2P1ElementwiseBlendingStokesOperator > with UzawaSmoother (block-Laplace
     variant): the velocity block -div(eta grad) per component (eta: see _coeff, e.g.
     ("radial", 2.99, 1.0, 0.45)), Chebyshev velocity smoothing, pressure update with the inverted PSPG
-    diagonal, quadratic/linear transfers, coarse_sweeps Uzawa steps on the coarsest level."""
+    diagonal, quadratic/linear transfers, coarse_sweeps Uzawa steps on the coarsest level.
+    velocity_block="full_viscous" uses P2ElementwiseBlendingFullViscousOperator (2 eta eps(u) : eps(v) -
+    (2/3) eta div u div v, the three components coupled) with Chebyshev on the coupled block."""
 
     def __init__(self, ctx, storage, min_level, max_level, viscosity=None, blending=None, pre=3, post=3,
-                 velocity_sweeps=3, cheb_order=3, power_iterations=20, omega=0.7, coarse_sweeps=100):
+                 velocity_sweeps=3, cheb_order=3, power_iterations=20, omega=0.7, coarse_sweeps=100,
+                 velocity_block="laplace"):
+        if velocity_block not in ("laplace", "full_viscous"):
+            raise ValueError("velocity_block must be 'laplace' or 'full_viscous'")
         p = _StokesParams()
         _check(lib().hyb_stokes_params_default(C.byref(p)))
         p.min_level, p.max_level, p.pre_smooth, p.post_smooth = min_level, max_level, pre, post
         p.velocity_sweeps, p.cheb_order, p.power_iterations = velocity_sweeps, cheb_order, power_iterations
         p.omega, p.coarse_sweeps = float(omega), coarse_sweeps
+        p.velocity_block = 1 if velocity_block == "full_viscous" else 0
         self.params, self.ctx, self.storage = p, ctx, storage
         c = _coeff(viscosity)
         h = C.c_void_p()

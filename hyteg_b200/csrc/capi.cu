@@ -2255,12 +2255,27 @@ struct hyb_stokes
    hyb_fn*           rp    = nullptr;
    hyb_fn*           sinv  = nullptr;  // inverted PSPG diagonal on every level
    int               dtype = -1;
+   // full viscous velocity block (velocity_block 1): the coupled operator, Chebyshev on it with the
+   // inverse diagonals of its diagonal blocks, work vectors z and t, radii and coefficients per level
+   hyb_op*                              V = nullptr;
+   hyb_fn*                              vz[3]    = { nullptr, nullptr, nullptr };
+   hyb_fn*                              vt[3]    = { nullptr, nullptr, nullptr };
+   hyb_fn*                              vinvd[3] = { nullptr, nullptr, nullptr };
+   std::vector< double >                vradii;
+   std::vector< std::vector< double > > vcoef;
    ~hyb_stokes()
    {
       for ( hyb_fn* f : ru ) hyb_fn_destroy( f );
+      for ( int k = 0; k < 3; ++k )
+      {
+         hyb_fn_destroy( vz[k] );
+         hyb_fn_destroy( vt[k] );
+         hyb_fn_destroy( vinvd[k] );
+      }
       hyb_fn_destroy( rp );
       hyb_fn_destroy( sinv );
       if ( vel ) hyb_gmg_destroy( vel );
+      op_unref( V );
       op_unref( A );
       op_unref( D );
       op_unref( S );
@@ -2284,6 +2299,119 @@ void stokes_fns_check( hyb_stokes* s, hyb_fn* const* u, hyb_fn* p, int level )
    require( level >= s->p.min_level && level <= s->p.max_level, "level outside the multigrid range" );
 }
 
+// Chebyshev coefficients of the coupled velocity block from per-level radii (bounds 0.3 and 1.2
+// times the radius, as the scalar smoother)
+void visc_set_radii( hyb_stokes* s, const double* radii )
+{
+   const int nl = s->p.max_level - s->p.min_level + 1;
+   s->vradii.assign( radii, radii + nl );
+   s->vcoef.clear();
+   for ( int i = 0; i < nl; ++i )
+   {
+      const double r = s->vradii[i];
+      if ( !( r > 0 ) || !std::isfinite( r ) )
+         throw std::runtime_error( "spectral radius estimate of level " + std::to_string( s->p.min_level + i ) + " is not positive" );
+      s->vcoef.push_back( chebyshev_coefficients( s->p.cheb_order, 0.3 * r, 1.2 * r ) );
+   }
+}
+
+// D^-1 A of the coupled block on all DoFs (flag All), x -> aux
+void visc_dinv_apply( hyb_stokes* s, hyb_fn* const* x, hyb_fn* const* aux, int l )
+{
+   const int   Ls    = l + 1;
+   const void* xx[3] = { x[0]->f.ptr( Ls ), x[1]->f.ptr( Ls ), x[2]->f.ptr( Ls ) };
+   void*       aa[3] = { aux[0]->f.ptr( Ls ), aux[1]->f.ptr( Ls ), aux[2]->f.ptr( Ls ) };
+   launch_full_viscous( &s->ctx->c, &s->V->o, l, x[0]->f.dtype, 0, xx, aa, kAll, 0 );
+   const double one[2] = { 1.0, 1.0 };
+   for ( int k = 0; k < 3; ++k )
+   {
+      hyb_fn* src[2] = { s->vinvd[k], aux[k] };
+      pointwise( aux[k], l, kAll, PT_MULT, 2, one, src );
+   }
+}
+
+// spectral radius of D^-1 A of the coupled block: the scalar power iteration (SpectrumEstimation.hpp:
+// 56-84, flag All) with norms and Rayleigh quotient summed over the three components; seeded start
+void visc_power_iteration_impl( hyb_stokes* s, int l, int iters, double* out )
+{
+   hyb_fn** x = s->vz;
+   hyb_fn** a = s->vt;
+   for ( int k = 0; k < 3; ++k ) ok_rc( hyb_fn_fill_random( x[k], l, 7001u + 31u * uint64_t( l ) + uint64_t( k ) ) );
+   auto vdot = [&]( hyb_fn** p, hyb_fn** q ) {
+      double r = 0;
+      for ( int k = 0; k < 3; ++k ) r += dot_host( p[k], q[k], l, kAll );
+      return r;
+   };
+   auto scale = [&]( hyb_fn** dst, hyb_fn** src, double f ) {
+      const double c[1] = { f };
+      for ( int k = 0; k < 3; ++k )
+      {
+         hyb_fn* sr[1] = { src[k] };
+         pointwise( dst[k], l, kAll, PT_LINCOMB, 1, c, sr );
+      }
+   };
+   double norm = std::sqrt( vdot( x, x ) );
+   scale( x, x, 1.0 / norm );
+   visc_dinv_apply( s, x, a, l );
+   double radius = 0;
+   for ( int it = 1; it <= iters; ++it )
+   {
+      norm = std::sqrt( vdot( a, a ) );
+      scale( x, a, 1.0 / norm );
+      visc_dinv_apply( s, x, a, l );
+      radius = vdot( x, a );
+   }
+   *out = radius;
+}
+
+double visc_power_iteration( hyb_stokes* s, int l, int iters )
+{
+   double r = 0;
+   visc_power_iteration_impl( s, l, iters, &r );
+   return r;
+}
+
+// ChebyshevSmoother::solve on the coupled velocity block: z = D^-1 (r - A u), u += c_0 z, then
+// z = D^-1 A z, u += c_m z; z starts as a copy of u so that its unflagged entries are u's
+void visc_smooth( hyb_stokes* s, hyb_fn* const* u, hyb_fn* const* r, int l )
+{
+   Context&     cx = s->ctx->c;
+   const int    Ls = l + 1, dt = u[0]->f.dtype;
+   const auto&  c  = s->vcoef.at( l - s->p.min_level );
+   const double one[2] = { 1.0, 1.0 }, pm[2] = { 1.0, -1.0 };
+   void*        tt[3]  = { s->vt[0]->f.ptr( Ls ), s->vt[1]->f.ptr( Ls ), s->vt[2]->f.ptr( Ls ) };
+   const void*  uu[3]  = { u[0]->f.ptr( Ls ), u[1]->f.ptr( Ls ), u[2]->f.ptr( Ls ) };
+   const void*  zz[3]  = { s->vz[0]->f.ptr( Ls ), s->vz[1]->f.ptr( Ls ), s->vz[2]->f.ptr( Ls ) };
+   for ( int k = 0; k < 3; ++k )
+   {
+      hyb_fn* src[1] = { u[k] };
+      pointwise( s->vz[k], l, kAll, PT_LINCOMB, 1, one, src );
+   }
+   launch_full_viscous( &cx, &s->V->o, l, dt, 0, uu, tt, kSolveFlag, 0 );
+   for ( int k = 0; k < 3; ++k )
+   {
+      hyb_fn* d[2] = { r[k], s->vt[k] };
+      pointwise( s->vt[k], l, kSolveFlag, PT_LINCOMB, 2, pm, d );
+      hyb_fn* q[2] = { s->vinvd[k], s->vt[k] };
+      pointwise( s->vz[k], l, kSolveFlag, PT_MULT, 2, one, q );
+      const double c0[1] = { c[0] };
+      hyb_fn*      z[1]  = { s->vz[k] };
+      pointwise( u[k], l, kSolveFlag, PT_ADD, 1, c0, z );
+   }
+   for ( size_t m = 1; m < c.size(); ++m )
+   {
+      launch_full_viscous( &cx, &s->V->o, l, dt, 0, zz, tt, kSolveFlag, 0 );
+      for ( int k = 0; k < 3; ++k )
+      {
+         hyb_fn* q[2] = { s->vinvd[k], s->vt[k] };
+         pointwise( s->vz[k], l, kSolveFlag, PT_MULT, 2, one, q );
+         const double cm[1] = { c[m] };
+         hyb_fn*      z[1]  = { s->vz[k] };
+         pointwise( u[k], l, kSolveFlag, PT_ADD, 1, cm, z );
+      }
+   }
+}
+
 // work vectors and the solver setup in the value type of the functions
 void stokes_prepare( hyb_stokes* s, hyb_fn* u0, hyb_fn* b0, int dt )
 {
@@ -2298,6 +2426,27 @@ void stokes_prepare( hyb_stokes* s, hyb_fn* u0, hyb_fn* b0, int dt )
    s->rp   = new_fn( s->ctx, m, dt, s->p.min_level, s->p.max_level );
    s->sinv = new_fn( s->ctx, m, dt, s->p.min_level, s->p.max_level );
    for ( int L = s->p.min_level; L <= s->p.max_level; ++L ) ok_rc( hyb_op_inverse_diagonal( s->S, s->sinv, L, kAll ) );
+   if ( s->V )
+   {
+      for ( int k = 0; k < 3; ++k )
+      {
+         hyb_fn** f[3] = { &s->vz[k], &s->vt[k], &s->vinvd[k] };
+         for ( hyb_fn** g : f )
+         {
+            *g             = new_fn( s->ctx, m, dt, s->p.min_level + 1, s->p.max_level + 1 );
+            ( *g )->f.lshift = 1;
+         }
+      }
+      for ( int L = s->p.min_level; L <= s->p.max_level; ++L ) ok_rc( hyb_p2_full_viscous_inverse_diagonal( s->V, s->vinvd, L ) );
+      if ( s->vradii.empty() )
+      {
+         std::vector< double > r;
+         for ( int L = s->p.min_level; L <= s->p.max_level; ++L ) r.push_back( visc_power_iteration( s, L, s->p.power_iterations ) );
+         visc_set_radii( s, r.data() );
+      }
+      s->dtype = dt;
+      return;
+   }
    // radii of the velocity block (power iteration on D^-1 A per level, once)
    gmg_prepare( s->vel, u0, b0, s->p.max_level + 1 );
    s->dtype = dt;
@@ -2319,7 +2468,14 @@ void uzawa_smooth( hyb_stokes* s, hyb_fn* const* u, hyb_fn* p, hyb_fn* const* bu
       pointwise( s->ru[k], l, kSolveFlag, PT_LINCOMB, 2, sc, src );
    }
    for ( int it = 0; it < s->p.velocity_sweeps; ++it )
+   {
+      if ( s->V )
+      {
+         visc_smooth( s, u, s->ru, l );
+         continue;
+      }
       for ( int k = 0; k < 3; ++k ) smooth( s->vel, u[k], s->ru[k], Ls );
+   }
    const void* uu[3] = { u[0]->f.ptr( Ls ), u[1]->f.ptr( Ls ), u[2]->f.ptr( Ls ) };
    launch_stokes_div( &cx, &s->D->o, l, dt, 0, uu, nullptr, nullptr, s->rp->f.ptr( l ), kAll, 0 );
    {
@@ -2344,8 +2500,20 @@ void stokes_residual( hyb_stokes* s, hyb_fn* const* u, hyb_fn* p, hyb_fn* const*
    Context&  cx = s->ctx->c;
    const int Ls = l + 1, dt = p->f.dtype;
    void*     rr[3] = { s->ru[0]->f.ptr( Ls ), s->ru[1]->f.ptr( Ls ), s->ru[2]->f.ptr( Ls ) };
-   for ( int k = 0; k < 3; ++k )
-      stencil( s->A, Ls, dt, OP_RESID, kSolveFlag, 0, u[k]->f.ptr( Ls ), bu[k]->f.ptr( Ls ), nullptr, rr[k] );
+   if ( s->V )
+   {
+      const void*  uu[3] = { u[0]->f.ptr( Ls ), u[1]->f.ptr( Ls ), u[2]->f.ptr( Ls ) };
+      const double pm[2] = { 1.0, -1.0 };
+      launch_full_viscous( &cx, &s->V->o, l, dt, 0, uu, rr, kSolveFlag, 0 );
+      for ( int k = 0; k < 3; ++k )
+      {
+         hyb_fn* d[2] = { bu[k], s->ru[k] };
+         pointwise( s->ru[k], l, kSolveFlag, PT_LINCOMB, 2, pm, d );
+      }
+   }
+   else
+      for ( int k = 0; k < 3; ++k )
+         stencil( s->A, Ls, dt, OP_RESID, kSolveFlag, 0, u[k]->f.ptr( Ls ), bu[k]->f.ptr( Ls ), nullptr, rr[k] );
    // r_u -= divT p: divT into rp's partner is not available, so subtract through a scaled add
    const double sc[2] = { 1.0, -1.0 };
    {
@@ -2427,6 +2595,7 @@ int hyb_stokes_create( hyb_ctx* ctx, hyb_mesh* mesh, const hyb_coeff* viscosity,
    require( params->pre_smooth >= 0 && params->post_smooth >= 0 && params->velocity_sweeps >= 1 && params->coarse_sweeps >= 1,
             "invalid smoothing counts" );
    require( params->cheb_order >= 1 && params->cheb_order <= 16, "Chebyshev order must be 1..16" );
+   require( params->velocity_block == 0 || params->velocity_block == 1, "velocity_block must be 0 (per component) or 1 (full viscous)" );
    auto* s = new hyb_stokes();
    s->ctx  = ctx;
    ctx_ref( ctx );
@@ -2434,11 +2603,17 @@ int hyb_stokes_create( hyb_ctx* ctx, hyb_mesh* mesh, const hyb_coeff* viscosity,
    s->p    = *params;
    try
    {
+      ok_rc( hyb_op_create_p2p1_div( ctx, mesh, params->min_level, params->max_level, blending, &s->D ) );
+      ok_rc( hyb_op_create_p1_pspg( ctx, mesh, params->min_level, params->max_level, &s->S ) );
+      if ( params->velocity_block == 1 )
+      {
+         ok_rc( hyb_op_create_p2_full_viscous( ctx, mesh, params->min_level, params->max_level, viscosity, blending, &s->V ) );
+         *out = s;
+         return HYB_OK;
+      }
       ok_rc( hyb_op_create_p2_divkgrad( ctx, mesh, params->min_level, params->max_level, viscosity, blending, &s->A ) );
       // the velocity block is applied some hundred times per cycle: its element matrices are stored
       ok_rc( hyb_op_store_element_matrices( s->A ) );
-      ok_rc( hyb_op_create_p2p1_div( ctx, mesh, params->min_level, params->max_level, blending, &s->D ) );
-      ok_rc( hyb_op_create_p1_pspg( ctx, mesh, params->min_level, params->max_level, &s->S ) );
       hyb_gmg_params gp;
       hyb_gmg_params_default( &gp );
       gp.min_level             = params->min_level;
@@ -2468,6 +2643,11 @@ int hyb_stokes_set_velocity_radii( hyb_stokes* s, const double* radii )
 {
    HYB_TRY
    require( s && radii, "NULL argument" );
+   if ( s->V )
+   {
+      visc_set_radii( s, radii );
+      return HYB_OK;
+   }
    return hyb_gmg_set_radii( s->vel, radii );
    HYB_CATCH
 }
@@ -2479,7 +2659,13 @@ int hyb_stokes_apply( hyb_stokes* s, hyb_fn* const* u, hyb_fn* p, hyb_fn* const*
    stokes_fns_check( s, du, dp, level );
    const int Ls = level + 1, dt = p->f.dtype;
    void*     dd[3] = { du[0]->f.ptr( Ls ), du[1]->f.ptr( Ls ), du[2]->f.ptr( Ls ) };
-   for ( int k = 0; k < 3; ++k ) stencil( s->A, Ls, dt, OP_APPLY, kSolveFlag, 0, u[k]->f.ptr( Ls ), nullptr, nullptr, dd[k] );
+   if ( s->V )
+   {
+      const void* uu[3] = { u[0]->f.ptr( Ls ), u[1]->f.ptr( Ls ), u[2]->f.ptr( Ls ) };
+      launch_full_viscous( &s->ctx->c, &s->V->o, level, dt, 0, uu, dd, kSolveFlag, 0 );
+   }
+   else
+      for ( int k = 0; k < 3; ++k ) stencil( s->A, Ls, dt, OP_APPLY, kSolveFlag, 0, u[k]->f.ptr( Ls ), nullptr, nullptr, dd[k] );
    launch_stokes_div( &s->ctx->c, &s->D->o, level, dt, 1, nullptr, p->f.ptr( level ), dd, nullptr, kSolveFlag, 1 );
    const void* uu[3] = { u[0]->f.ptr( Ls ), u[1]->f.ptr( Ls ), u[2]->f.ptr( Ls ) };
    launch_stokes_div( &s->ctx->c, &s->D->o, level, dt, 0, uu, nullptr, nullptr, dp->f.ptr( level ), kAll, 0 );
@@ -2523,6 +2709,7 @@ int hyb_stokes_mixed_solve( hyb_stokes* outer, hyb_stokes* inner, int inner_dtyp
    require( p->f.dtype == F64, "the iterate must hold FP64 values" );
    require( inner->mesh == outer->mesh && inner->p.min_level == outer->p.min_level && level <= inner->p.max_level,
             "inner solver of another mesh or level range" );
+   require( ( inner->V != nullptr ) == ( outer->V != nullptr ), "inner and outer solvers have different velocity blocks" );
    require( max_outer >= 0, "max_outer must be >= 0" );
    stokes_prepare( outer, u[0], bu[0], F64 );
    Mesh*         m   = &outer->mesh->m;

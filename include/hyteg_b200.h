@@ -376,6 +376,8 @@ typedef struct hyb_stokes_params
    int    power_iterations; /* spectral-radius estimate of D^-1 A per level */
    double omega;            /* Uzawa relaxation parameter (UzawaSmoother::setRelaxationParameter) */
    int    coarse_sweeps;    /* Uzawa steps on the coarsest level (the coarse solve) */
+   int    velocity_block;   /* 0: -div(eta grad) per component (block Laplace); 1: the full viscous block
+                               P2ElementwiseBlendingFullViscousOperator, Chebyshev on the coupled block */
 } hyb_stokes_params;
 int hyb_stokes_params_default( hyb_stokes_params* p );
 /* GeometricMultigridSolver< P2P1ElementwiseBlendingStokesOperator > with UzawaSmoother; viscosity:

@@ -1416,9 +1416,12 @@ class P2P1Stokes:
     inverted PSPG diagonal (P1PSPGInvDiagOperator, affine macro geometry) for the Uzawa step.
     Velocity rows/columns use the inner DoFs, pressure rows/columns all DoFs."""
 
-    def __init__(self, mesh, minL, maxL, eta, blending=None):
+    def __init__(self, mesh, minL, maxL, eta, blending=None, full_viscous=False):
         self.mesh, self.minL, self.maxL = mesh, minL, maxL
         self.Aop = P2DivKGrad(mesh, minL, maxL, eta, blending)
+        # the full viscous velocity block (P2ElementwiseBlendingFullViscousOperator) in place of
+        # -div(eta grad) per component, smoothed by Chebyshev on the coupled block
+        self.Vop = P2FullViscous(mesh, minL, maxL, eta, blending) if full_viscous else None
         self.ulev = self.Aop.levels
         self.plev = {L: Level(mesh, L) for L in range(minL, maxL + 1)}
         maps = self.Aop.maps
@@ -1480,11 +1483,17 @@ class P2P1Stokes:
             self.ulev[L].sync(out[k])
         return out
 
+    def velocity_apply(self, u, L, k):
+        """Component k of the velocity block applied to u (all DoFs)."""
+        if self.Vop is None:
+            return self.Aop.A[L] @ u[k]
+        return sum(self.Vop.A[L][k][j] @ u[j] for j in range(3))
+
     def apply(self, u, p, L):
         m = self.umask(L)
         du = []
         for k in range(3):
-            r = self.Aop.A[L] @ u[k] + self.B[L][k].T @ p
+            r = self.velocity_apply(u, L, k) + self.B[L][k].T @ p
             o = np.zeros(self.ulev[L].size)
             o[m] = r[m]
             du.append(self.ulev[L].sync(o))
@@ -1494,7 +1503,7 @@ class P2P1Stokes:
         m = self.umask(L)
         ru = []
         for k in range(3):
-            r = bu[k] - (self.Aop.A[L] @ u[k] + self.B[L][k].T @ p)
+            r = bu[k] - (self.velocity_apply(u, L, k) + self.B[L][k].T @ p)
             o = np.zeros(self.ulev[L].size)
             o[m] = r[m]
             ru.append(self.ulev[L].sync(o))
@@ -1519,6 +1528,9 @@ class P2P1Stokes:
             ru.append(self.ulev[L].sync(o))
         u = [x.copy() for x in u]
         for _ in range(sweeps):
+            if self.Vop is not None:
+                u = _cheb_apply_vec(self.Vop, u, ru, L, radius, order)
+                continue
             for k in range(3):
                 u[k] = _cheb_apply(self.Aop, u[k], ru[k], L, radius, order)
         rp = bp - self.div(u, L)
@@ -1558,6 +1570,54 @@ class P2P1Stokes:
         o = np.zeros(lev.size)
         o[m] = v[m]
         return lev.sync(o)
+
+
+def _cheb_apply_vec(op, x, b, L, radius, order):
+    """_cheb_apply on the coupled velocity block (three components, block-diagonal D)."""
+    x = [v.copy() for v in x]
+    lev = op.levels[L]
+    mask = lev.owned_mask(INNER | NEUMANN | FREESLIP)
+    coeff = chebyshev_coefficients(order, 0.3 * radius, 1.2 * radius)
+    tmp1, tmp2 = [v.copy() for v in x], [v.copy() for v in x]
+    op.apply(x, tmp2, L, INNER | NEUMANN | FREESLIP)
+    for k in range(3):
+        tmp2[k][mask] = b[k][mask] - tmp2[k][mask]
+        tmp1[k][mask] = op.invdiag[L][k][mask] * tmp2[k][mask]
+        x[k][mask] = x[k][mask] + coeff[0] * tmp1[k][mask]
+    for c in coeff[1:]:
+        op.apply(tmp1, tmp2, L, INNER | NEUMANN | FREESLIP)
+        for k in range(3):
+            tmp1[k][mask] = op.invdiag[L][k][mask] * tmp2[k][mask]
+            x[k][mask] = x[k][mask] + c * tmp1[k][mask]
+    return x
+
+
+def power_iteration_radius_vec(op, L, x0, iters):
+    """power_iteration_radius on D^-1 A of the coupled velocity block (three components, flag All;
+    norms and the Rayleigh quotient summed over the components)."""
+    lev = op.levels[L]
+    x = [v.copy() for v in x0]
+    aux = [np.zeros_like(v) for v in x]
+    m = lev.owned_mask(ALL)
+
+    def dinv_a(src, dst):
+        op.apply(src, dst, L, ALL)
+        for k in range(3):
+            dst[k][m] = op.invdiag[L][k][m] * dst[k][m]
+
+    def vdot(a, b):
+        return sum(dot(lev, a[k], b[k], ALL) for k in range(3))
+
+    norm = math.sqrt(vdot(x, x))
+    x = [v * (1.0 / norm) for v in x]
+    dinv_a(x, aux)
+    radius = 0.0
+    for _ in range(iters):
+        norm = math.sqrt(vdot(aux, aux))
+        x = [v * (1.0 / norm) for v in aux]
+        dinv_a(x, aux)
+        radius = vdot(x, aux)
+    return radius
 
 
 def _cheb_apply(op, x, b, L, radius, order):

@@ -25,11 +25,12 @@ def _eta(case):
     return (ETA, O.k_radial(2.99, 1.0, 0.45)) if case == "shell" else (None, lambda P: np.ones(len(P)))
 
 
-def _setup(ctx, case, minL, maxL):
+def _setup(ctx, case, minL, maxL, block="laplace"):
     coords, tets = M.cube_6() if case == "cube" else O.mesh_spherical_shell(3, 2, 0.55, 1.0)
     om = O.MacroMesh(coords, tets)
     bl = "shell" if case == "shell" else None
-    S = O.P2P1Stokes(om, minL, maxL, _eta(case)[1], blending=bl)
+    S = O.P2P1Stokes(om, minL, maxL, _eta(case)[1], blending=bl, full_viscous=block == "full_viscous")
+    S.block = block
     S.case = case
     pm = H.PrimitiveStorage.from_tets(coords, tets, ctx)
     return S, pm, bl
@@ -92,17 +93,24 @@ def test_stokes_blocks_match_oracle(ctx, case, L):
 
 
 def _solver(ctx, pm, S, bl, minL, maxL, **kw):
-    radii = [O.power_iteration_radius(S.Aop, l, np.random.default_rng(40 + l).uniform(-1, 1, S.ulev[l].size), 20)
-             for l in range(minL, maxL + 1)]
-    st = H.StokesUzawaMultigrid(ctx, pm, minL, maxL, viscosity=_eta(S.case)[0], blending=bl, **kw)
+    if S.Vop is None:
+        radii = [O.power_iteration_radius(S.Aop, l, np.random.default_rng(40 + l).uniform(-1, 1, S.ulev[l].size), 20)
+                 for l in range(minL, maxL + 1)]
+    else:
+        radii = [O.power_iteration_radius_vec(S.Vop, l, [np.random.default_rng(40 + l + 7 * k).uniform(-1, 1, S.ulev[l].size)
+                                                         for k in range(3)], 20)
+                 for l in range(minL, maxL + 1)]
+    st = H.StokesUzawaMultigrid(ctx, pm, minL, maxL, viscosity=_eta(S.case)[0], blending=bl,
+                                velocity_block=S.block, **kw)
     st.set_velocity_radii(radii)
     return st, {l: radii[l - minL] for l in range(minL, maxL + 1)}
 
 
+@pytest.mark.parametrize("block", ["laplace", "full_viscous"])
 @pytest.mark.parametrize("case", ["cube", "shell"])
-def test_stokes_apply_and_uzawa_step(ctx, case):
+def test_stokes_apply_and_uzawa_step(ctx, case, block):
     L = 2 if case == "cube" else 1
-    S, pm, bl = _setup(ctx, case, 0, L)
+    S, pm, bl = _setup(ctx, case, 0, L, block)
     st, radii = _solver(ctx, pm, S, bl, 0, L)
     u0, p0 = _vel(S, L, 3), _pres(S, L, 4)
     bu0, bp0 = _vel(S, L, 5), _pres(S, L, 6)
@@ -129,10 +137,11 @@ def test_stokes_apply_and_uzawa_step(ctx, case):
     assert _relerr(p.download(L), rp, S.pmask(L)) < 1e-12
 
 
+@pytest.mark.parametrize("block", ["laplace", "full_viscous"])
 @pytest.mark.parametrize("case", ["cube", "shell"])
-def test_stokes_vcycle_factors(ctx, case):
+def test_stokes_vcycle_factors(ctx, case, block):
     L = 3 if case == "cube" else 2
-    S, pm, bl = _setup(ctx, case, 0, L)
+    S, pm, bl = _setup(ctx, case, 0, L, block)
     st, radii = _solver(ctx, pm, S, bl, 0, L)
     bu0, bp0 = _vel(S, L, 7), np.zeros(S.plev[L].size)
     u, p = _fns(pm, ctx, 0, L)
@@ -188,3 +197,18 @@ def test_stokes_mixed_refuses_fp16(ctx):
     inner = H.StokesUzawaMultigrid(ctx, pm, 0, L)
     with pytest.raises(H.HybError):
         st.mixed_solve(inner, u, p, bu, bp, L, inner_dtype="float16")
+
+
+def test_stokes_full_viscous_own_radii_converge(ctx):
+    """Without given radii the solver estimates them by the power iteration on the coupled block."""
+    L = 2
+    S, pm, bl = _setup(ctx, "cube", 0, L, "full_viscous")
+    st = H.StokesUzawaMultigrid(ctx, pm, 0, L, viscosity=_eta("cube")[0], blending=bl, velocity_block="full_viscous")
+    bu0 = _vel(S, L, 9)
+    u, p = _fns(pm, ctx, 0, L)
+    bu, bp = _fns(pm, ctx, 0, L)
+    for k in range(3):
+        bu[k].upload(L, bu0[k])
+    hist = st.solve(u, p, bu, bp, L, 6)
+    assert np.all(hist[1:] / hist[:-1] < 0.9)
+    assert hist[-1] < 1e-2 * hist[0]
