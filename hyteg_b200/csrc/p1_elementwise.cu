@@ -352,6 +352,22 @@ __constant__ double c_xg4_pts[11][3];
 __constant__ double c_xg4_w[11];
 __constant__ double c_p2_rgrad[11][10][3];  // reference gradients of the ten basis functions per point
 __constant__ int    c_p2_edge[6][2] = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
+// Stored P2 element matrices keep the 55 distinct entries of the symmetric 10x10 matrix in wrapped-
+// diagonal order: block 0 (entries 0-9) the diagonal K(i, i); block s = 1..4 (entries 10 s + e) the
+// entries K(e, (e + s) mod 10); block 5 (entries 50-54) K(e, e + 5) for e < 5.  Lane i of a ten-lane
+// group then finds its row in blocks that the group reads as whole 80-byte runs.  c_p2_wrap maps the
+// upper-triangle index r * 10 - r (r - 1) / 2 + (c - r) of (r, c), r <= c, to this order.
+__constant__ int    c_p2_wrap[55];
+
+static void p2_wrap_table( int w[55] )
+{
+   for ( int r = 0; r < 10; ++r )
+      for ( int c = r; c < 10; ++c )
+      {
+         const int ut = r * 10 - r * ( r - 1 ) / 2 + ( c - r ), d = c - r;
+         w[ut]        = d == 0 ? r : d <= 4 ? 10 * d + r : d == 5 ? 50 + r : 10 * ( 10 - d ) + c;
+      }
+}
 
 // barycentric coordinates (l0, l1, l2, l3) of the rule's points (kept identical to the reference's
 // generated form: the element integrals must agree); reference coordinates are (l1, l2, l3)
@@ -439,6 +455,9 @@ void ensure_p2_constants()
    check_cuda( cudaMemcpyToSymbol( c_xg4_pts, pts, sizeof( pts ) ), "P2 constants (points)" );
    check_cuda( cudaMemcpyToSymbol( c_xg4_w, w, sizeof( w ) ), "P2 constants (weights)" );
    check_cuda( cudaMemcpyToSymbol( c_p2_rgrad, g, sizeof( g ) ), "P2 constants (gradients)" );
+   int wrap[55];
+   p2_wrap_table( wrap );
+   check_cuda( cudaMemcpyToSymbol( c_p2_wrap, wrap, sizeof( wrap ) ), "P2 constants (stored order)" );
    done = true;
 }
 
@@ -491,9 +510,9 @@ __device__ __forceinline__ void p2_grad( int q, int i, const A Mi[3][3], A G[3] 
 
 // One parity pass over the level-L micro-cells (anchors of parity (px, py, pz); ne = 2^L), nodes
 // on storage level L+1.  MODE 0: y += K x computed matrix-free (per point the gradient of the local
-// solution, then its pairing with every basis gradient); 1: diagonal of K; 2: store the 55 upper-
-// triangle entries of K; 3: y += K x from the stored entries.  Stored entry v of micro-cell (cell c,
-// type ty, anchor t of the pass's parity class p) sits at
+// solution, then its pairing with every basis gradient); 1: diagonal of K; 2: store the 55 distinct
+// entries of K (wrapped-diagonal order, c_p2_wrap); 3: y += K x from the stored entries.  Stored entry
+// v of micro-cell (cell c, type ty, anchor t of the pass's parity class p) sits at
 // kst[55 * (6 nC aoff[p] + (c * 6 + ty) * nanch + t) + v] (kbase = 6 nC aoff[p]): the 55 entries of
 // a micro-cell are contiguous, so the lanes that read one micro-cell's rows share its 440 bytes.
 template < typename T, typename A, int MODE >
@@ -551,7 +570,7 @@ __global__ void __launch_bounds__( 256 ) k_p2_pass( int ne, int nanch, const int
             for ( int i = 0; i < 10; ++i )
                for ( int j = i; j < 10; ++j, ++v )
                {
-                  const A k = kst[slot * 55 + v];
+                  const A k = kst[slot * 55 + c_p2_wrap[v]];
                   yl[i] += k * xl[j];
                   if ( j != i ) yl[j] += k * xl[i];
                }
@@ -603,7 +622,7 @@ __global__ void __launch_bounds__( 256 ) k_p2_pass( int ne, int nanch, const int
             }
             if constexpr ( MODE == 2 )
             {
-               for ( int v = 0; v < 55; ++v ) kst[slot * 55 + v] = K[v];
+               for ( int v = 0; v < 55; ++v ) kst[slot * 55 + c_p2_wrap[v]] = K[v];
                continue;
             }
          }
@@ -851,8 +870,9 @@ __global__ void k_cell_invert( int n, int nrows, const int2* __restrict__ rows, 
 // ---------------------------------------------------------------------------------------------
 // P2 apply from stored element matrices: ten lanes per micro-cell anchor (three anchors per warp,
 // lanes 30-31 idle).  Lane i owns element node i: it loads its node value, gathers the other nine
-// with shuffles, reads row i of the symmetric matrix (its upper triangle is stored per micro-cell) and
-// adds row i times x into its node.  The ten nodes of a micro-cell are distinct, the six
+// with shuffles, reads row i of the symmetric matrix (55 distinct entries per micro-cell in
+// wrapped-diagonal order, so each of the ten loads of a group covers one 80-byte run) and adds row i
+// times x into its node.  The ten nodes of a micro-cell are distinct, the six
 // micro-cells of an anchor are taken in turn by the same lanes, and anchors of one parity class
 // share no node, so the read-modify-writes are race-free.  One lane per anchor (the recomputing
 // pass) left most of a block idle on these levels: 10 x more lanes in flight per pass.
@@ -876,15 +896,22 @@ __global__ void __launch_bounds__( 256 ) k_p2_stored_pass( int ne, int nanch, co
    }
    const int     ns   = 2 * ne;
    const int64_t base = cell_off[c];
-   // row i of the symmetric 10x10 matrix in the upper-triangle storage: entry (r, s),
-   // r <= s, is value r * 10 - r * (r - 1) / 2 + (s - r)
-   int vrow[10];
+   // row i of the symmetric matrix in the wrapped-diagonal order: term t multiplies stored entry
+   // koff[t] with the node value of lane xsrc[t] of the group (t = 0: K(i, i); t = 2s-1, 2s:
+   // K(i, i+s), K(i, i-s) from block s; t = 9: K(i, i+5) from block 5)
+   int koff[10], xsrc[10];
+   koff[0] = i;
+   xsrc[0] = i;
 #pragma unroll
-   for ( int j = 0; j < 10; ++j )
+   for ( int d = 1; d <= 4; ++d )
    {
-      const int r = min( i, j ), q = max( i, j );
-      vrow[j]     = r * 10 - r * ( r - 1 ) / 2 + ( q - r );
+      koff[2 * d - 1] = 10 * d + i;
+      xsrc[2 * d - 1] = ( i + d ) % 10;
+      koff[2 * d]     = 10 * d + ( i + 10 - d ) % 10;
+      xsrc[2 * d]     = ( i + 10 - d ) % 10;
    }
+   koff[9] = 50 + i % 5;
+   xsrc[9] = ( i + 5 ) % 10;
    // node index, stored slot and the self-check of micro-cell type ty (all lanes of the warp take
    // part: the check is a warp vote)
    auto prep = [&]( int ty, int64_t& idx, int64_t& slot, bool& go ) {
@@ -922,7 +949,7 @@ __global__ void __launch_bounds__( 256 ) k_p2_stored_pass( int ne, int nanch, co
    A x0 = go0 ? A( ld_any( src + idx0 ) ) : A( 0 );
    A k0[10];
 #pragma unroll
-   for ( int j = 0; j < 10; ++j ) k0[j] = go0 ? __ldg( kst + slot0 * 55 + vrow[j] ) : A( 0 );
+   for ( int j = 0; j < 10; ++j ) k0[j] = go0 ? __ldg( kst + slot0 * 55 + koff[j] ) : A( 0 );
 #pragma unroll 1
    for ( int ty = 0; ty < 6; ++ty )
    {
@@ -932,12 +959,12 @@ __global__ void __launch_bounds__( 256 ) k_p2_stored_pass( int ne, int nanch, co
       if ( ty < 5 ) prep( ty + 1, idx1, slot1, go1 );
       if ( go1 ) x1 = A( ld_any( src + idx1 ) );
 #pragma unroll
-      for ( int j = 0; j < 10; ++j ) k1[j] = go1 ? __ldg( kst + slot1 * 55 + vrow[j] ) : A( 0 );
+      for ( int j = 0; j < 10; ++j ) k1[j] = go1 ? __ldg( kst + slot1 * 55 + koff[j] ) : A( 0 );
       A yi = A( 0 );
 #pragma unroll
       for ( int j = 0; j < 10; ++j )
       {
-         const A xj = __shfl_sync( 0xffffffffu, x0, grp < 3 ? g0 + j : lane );
+         const A xj = __shfl_sync( 0xffffffffu, x0, grp < 3 ? g0 + xsrc[j] : lane );
          if ( go0 ) yi += k0[j] * xj;
       }
       if ( go0 ) acc[idx0] += yi;
