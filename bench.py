@@ -323,8 +323,9 @@ def stokes_leg(H, ctx, level=3, cycles=3):
     ntan=5, nrad=3 (1920 macro-cells), viscosity eta = exp(2.99 (1 - r) / 0.45), buoyancy-like
     right-hand side (seeded uniform [0, 1] times the position vector in the velocity, zero in the
     pressure), Uzawa multigrid (V(3,3) Uzawa steps with Chebyshev(3) velocity smoothing, quadratic /
-    linear transfers, 100 Uzawa steps on level 0), FP64.  Times `cycles` V-cycles after one warm-up
-    cycle and reports the residual-reduction factors."""
+    linear transfers, 100 Uzawa steps on level 0), FP64.  Times `cycles` V-cycles after two warm-up
+    cycles (setup, a first cycle, the capture of the cycle's CUDA graph) and reports the
+    residual-reduction factors."""
     pm = H.PrimitiveStorage.spherical_shell(5, 3, 0.55, 1.0, ctx=ctx)
     st = H.StokesUzawaMultigrid(ctx, pm, 0, level, viscosity=("radial", 2.99, 1.0, 0.45), blending="shell")
     u = [H.P2Function("u%d" % k, pm, 0, level, ctx) for k in range(3)]
@@ -340,7 +341,7 @@ def stokes_leg(H, ctx, level=3, cycles=3):
         # buoyancy: T x_k / |x| with T in [0, 1]
         bu[k].interpolate(lambda x, y, z, k=k: [x, y, z][k] / max((x * x + y * y + z * z) ** 0.5, 1e-12), level)
         bu[k].multElementwise([bu[k], T], level)
-    st.solve(u, p, bu, bp, level, 1)  # setup (radii, stored matrices) and one cycle
+    st.solve(u, p, bu, bp, level, 2)  # setup (radii, stored matrices), a first cycle and the cycle's graph capture
     ctx.synchronize()
     t0 = time.perf_counter()
     hist = st.solve(u, p, bu, bp, level, cycles)
@@ -361,7 +362,7 @@ def stokes_leg(H, ctx, level=3, cycles=3):
         for k in range(3):
             bl_[k].interpolate(lambda x, y, z, k=k: [x, y, z][k] / max((x * x + y * y + z * z) ** 0.5, 1e-12), Lr)
         if mode == "fp64":
-            sr.solve(uu, pp, bl_, bpl, Lr, 1)  # setup
+            sr.solve(uu, pp, bl_, bpl, Lr, 2)  # setup and graph capture
             for k in range(3):
                 uu[k].interpolate(0.0, Lr)
             pp.interpolate(0.0, Lr)
@@ -369,7 +370,7 @@ def stokes_leg(H, ctx, level=3, cycles=3):
             t0 = time.perf_counter()
             h = sr.solve(uu, pp, bl_, bpl, Lr, 150, rtol=1e-6)
         else:
-            sr.mixed_solve(si, uu, pp, bl_, bpl, Lr, max_outer=1, rtol=1e-6)  # setup of the inner solver
+            sr.mixed_solve(si, uu, pp, bl_, bpl, Lr, max_outer=2, rtol=1e-6)  # setup and graph capture of the inner solver
             for k in range(3):
                 uu[k].interpolate(0.0, Lr)
             pp.interpolate(0.0, Lr)
@@ -391,7 +392,7 @@ def stokes_leg(H, ctx, level=3, cycles=3):
     for k in range(3):
         u[k].interpolate(0.0, level)
     p.interpolate(0.0, level)
-    sv.solve(u, p, bu, bp, level, 1)  # setup (radii) and one cycle
+    sv.solve(u, p, bu, bp, level, 2)  # setup (radii), a first cycle and the graph capture
     ctx.synchronize()
     t0 = time.perf_counter()
     hv = sv.solve(u, p, bu, bp, level, 2)

@@ -2263,8 +2263,19 @@ struct hyb_stokes
    hyb_fn*                              vinvd[3] = { nullptr, nullptr, nullptr };
    std::vector< double >                vradii;
    std::vector< std::vector< double > > vcoef;
+   // captured V-cycle: the graph of the last (functions, level) key, captured on the key's second
+   // cycle (the first one creates every lazily allocated buffer outside the capture)
+   cudaGraphExec_t              gexec = nullptr;
+   std::vector< const void* >   gkey;
+   // defect correction: the inner solver's iterate and right-hand side (u0-2, bu0-2, p, bp), kept
+   // between calls with the same inner solver, level and value type so that its captured cycle stays valid
+   hyb_fn*     mx[8]    = { nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr };
+   hyb_stokes* mx_inner = nullptr;
+   int         mx_dtype = -1, mx_level = -1;
    ~hyb_stokes()
    {
+      if ( gexec ) cudaGraphExecDestroy( gexec );
+      for ( hyb_fn* f : mx ) hyb_fn_destroy( f );
       for ( hyb_fn* f : ru ) hyb_fn_destroy( f );
       for ( int k = 0; k < 3; ++k )
       {
@@ -2555,6 +2566,53 @@ void stokes_vcycle( hyb_stokes* s, hyb_fn* const* u, hyb_fn* p, hyb_fn* const* b
    for ( int it = 0; it < s->p.post_smooth; ++it ) uzawa_smooth( s, u, p, bu, bp, l );
 }
 
+// one V-cycle through a CUDA graph: the cycle's thousands of small launches (the coarsest level's
+// Uzawa steps above all) become one graph launch; the key is every level pointer of u, p, bu, bp
+void stokes_cycle( hyb_stokes* s, hyb_fn* const* u, hyb_fn* p, hyb_fn* const* bu, hyb_fn* bp, int l )
+{
+   Context&                   cx = s->ctx->c;
+   std::vector< const void* > key;
+   key.push_back( reinterpret_cast< const void* >( intptr_t( l ) ) );
+   for ( int L = s->p.min_level; L <= l; ++L )
+   {
+      for ( int k = 0; k < 3; ++k )
+      {
+         key.push_back( u[k]->f.ptr( L + 1 ) );
+         key.push_back( bu[k]->f.ptr( L + 1 ) );
+      }
+      key.push_back( p->f.ptr( L ) );
+      key.push_back( bp->f.ptr( L ) );
+   }
+   if ( key != s->gkey )
+   {
+      if ( s->gexec ) cudaGraphExecDestroy( s->gexec ), s->gexec = nullptr;
+      s->gkey = key;
+      stokes_vcycle( s, u, p, bu, bp, l );
+      return;
+   }
+   if ( !s->gexec )
+   {
+      cudaGraph_t graph = nullptr;
+      check_cuda( cudaStreamBeginCapture( cx.stream, cudaStreamCaptureModeThreadLocal ), "begin capture" );
+      try
+      {
+         stokes_vcycle( s, u, p, bu, bp, l );
+      } catch ( ... )
+      {
+         cudaStreamEndCapture( cx.stream, &graph );
+         if ( graph ) cudaGraphDestroy( graph );
+         s->gkey.clear();
+         throw;
+      }
+      check_cuda( cudaStreamEndCapture( cx.stream, &graph ), "end capture" );
+      const cudaError_t e = cudaGraphInstantiate( &s->gexec, graph, 0 );
+      cudaGraphDestroy( graph );
+      check_cuda( e, "graph instantiate" );
+   }
+   check_cuda( cudaGraphLaunch( s->gexec, cx.stream ), "graph launch" );
+   cx.launches += 1;
+}
+
 double stokes_residual_norm( hyb_stokes* s, hyb_fn* const* u, hyb_fn* p, hyb_fn* const* bu, hyb_fn* bp, int l )
 {
    stokes_residual( s, u, p, bu, bp, l );
@@ -2643,6 +2701,9 @@ int hyb_stokes_set_velocity_radii( hyb_stokes* s, const double* radii )
 {
    HYB_TRY
    require( s && radii, "NULL argument" );
+   // the captured cycle holds the Chebyshev coefficients of the old radii
+   if ( s->gexec ) cudaGraphExecDestroy( s->gexec ), s->gexec = nullptr;
+   s->gkey.clear();
    if ( s->V )
    {
       visc_set_radii( s, radii );
@@ -2714,31 +2775,27 @@ int hyb_stokes_mixed_solve( hyb_stokes* outer, hyb_stokes* inner, int inner_dtyp
    stokes_prepare( outer, u[0], bu[0], F64 );
    Mesh*         m   = &outer->mesh->m;
    const int     lo  = outer->p.min_level;
-   // inner iterate and right-hand side on every level (P2 velocity, P1 pressure)
-   hyb_fn* iu[3], *ibu[3];
-   for ( int k = 0; k < 3; ++k )
+   // inner iterate and right-hand side on every level (P2 velocity, P1 pressure), kept by the outer
+   // solver for later calls with the same inner solver, level and value type
+   if ( outer->mx_inner != inner || outer->mx_dtype != inner_dtype || outer->mx_level != level || !outer->mx[0] ||
+        outer->mx[0]->ctx != inner->ctx )
    {
-      iu[k]            = new_fn( inner->ctx, m, inner_dtype, lo + 1, level + 1 );
-      ibu[k]           = new_fn( inner->ctx, m, inner_dtype, lo + 1, level + 1 );
-      iu[k]->f.lshift  = 1;
-      ibu[k]->f.lshift = 1;
-   }
-   hyb_fn* ip  = new_fn( inner->ctx, m, inner_dtype, lo, level );
-   hyb_fn* ibp = new_fn( inner->ctx, m, inner_dtype, lo, level );
-   struct Free
-   {
-      hyb_fn** a;
-      hyb_fn*  p1;
-      hyb_fn*  p2;
-      ~Free()
+      for ( hyb_fn*& f : outer->mx ) hyb_fn_destroy( f ), f = nullptr;
+      for ( int k = 0; k < 6; ++k )
       {
-         for ( int k = 0; k < 6; ++k ) hyb_fn_destroy( a[k] );
-         hyb_fn_destroy( p1 );
-         hyb_fn_destroy( p2 );
+         outer->mx[k]           = new_fn( inner->ctx, m, inner_dtype, lo + 1, level + 1 );
+         outer->mx[k]->f.lshift = 1;
       }
-   };
-   hyb_fn* all6[6] = { iu[0], iu[1], iu[2], ibu[0], ibu[1], ibu[2] };
-   Free    fr{ all6, ip, ibp };
+      outer->mx[6]    = new_fn( inner->ctx, m, inner_dtype, lo, level );
+      outer->mx[7]    = new_fn( inner->ctx, m, inner_dtype, lo, level );
+      outer->mx_inner = inner;
+      outer->mx_dtype = inner_dtype;
+      outer->mx_level = level;
+   }
+   hyb_fn* iu[3]  = { outer->mx[0], outer->mx[1], outer->mx[2] };
+   hyb_fn* ibu[3] = { outer->mx[3], outer->mx[4], outer->mx[5] };
+   hyb_fn* ip     = outer->mx[6];
+   hyb_fn* ibp    = outer->mx[7];
    stokes_prepare( inner, iu[0], ibu[0], inner_dtype );
    Context&  cx = outer->ctx->c;
    const int Ls = level + 1;
@@ -2765,7 +2822,7 @@ int hyb_stokes_mixed_solve( hyb_stokes* outer, hyb_stokes* inner, int inner_dtyp
       launch_convert( &cx, m->level( level ).size, inner_dtype, ibp->f.ptr( level ), F64, outer->rp->f.ptr( level ), sc );
       check_cuda( cudaMemsetAsync( ip->f.ptr( level ), 0, ip->f.bytes( level ), cx.stream ), "cudaMemset" );
       if ( inner->ctx != outer->ctx ) check_cuda( cudaStreamSynchronize( cx.stream ), "sync" );
-      stokes_vcycle( inner, iu, ip, ibu, ibp, level );
+      stokes_cycle( inner, iu, ip, ibu, ibp, level );
       if ( inner->ctx != outer->ctx ) check_cuda( cudaStreamSynchronize( inner->ctx->c.stream ), "sync" );
       for ( int k = 0; k < 3; ++k )
          launch_axpy_to_f64( &cx, m->level( Ls ).size, (double*) u[k]->f.ptr( Ls ), inner_dtype, iu[k]->f.ptr( Ls ), 1.0 / sc );
@@ -2790,7 +2847,7 @@ int hyb_stokes_solve( hyb_stokes* s, hyb_fn* const* u, hyb_fn* p, hyb_fn* const*
    int c = 0;
    for ( ; c < max_cycles; ++c )
    {
-      stokes_vcycle( s, u, p, bu, bp, level );
+      stokes_cycle( s, u, p, bu, bp, level );
       const double r = stokes_residual_norm( s, u, p, bu, bp, level );
       if ( history ) history[c + 1] = r;
       if ( rtol > 0 && r <= rtol * r0 )
