@@ -720,7 +720,11 @@ __device__ __forceinline__ A inc_sum( int q0, int q1, const Incidence* __restric
    return s;
 }
 
-template < typename T, typename A, int OP >
+// Owners of face/edge/vertex DoFs: sum of the cell copies, epilogue, write-through.  G lanes per task
+// (G = 1 on fine levels, where face points with two cells dominate; G = 8 on the coarsest levels,
+// where a macro-vertex has 20-30 cells): the lanes of a task take every G-th incidence and combine
+// their partial sums by a butterfly, which leaves the same bits in every lane of the group.
+template < typename T, typename A, int OP, int G >
 __global__ void __launch_bounds__( 256 ) k_bnd_acc( int n, int ntasks, const int4* __restrict__ tasks, const int64_t* __restrict__ off,
                                                      const int64_t* __restrict__ cell_off, const int8_t* __restrict__ bkind,
                                                      const uint8_t* __restrict__ bc, const int* __restrict__ inc_begin,
@@ -728,37 +732,75 @@ __global__ void __launch_bounds__( 256 ) k_bnd_acc( int n, int ntasks, const int
                                                      const A* __restrict__ acc, const A* __restrict__ invd, A* invd_out, const T* src,
                                                      const T* v1, T* v2, T* dst, A a0, A a1 )
 {
-   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-   if ( t >= ntasks ) return;
+   static_assert( G == 1 || G == 2 || G == 4 || G == 8 || G == 16 || G == 32, "G divides the warp" );
+   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+   const int t  = gt / G, sub = gt % G;
+   if ( t >= ntasks ) return;  // a group's lanes share t: whole groups leave
    const int4    tk    = tasks[t];
    const int     b     = tk.x;
    const int     k     = bkind[b];
    const int64_t owner = off[b] + ( k == 0 ? 0 : ( k == 1 ? int64_t( tk.y ) : fidx( n, tk.y, tk.z ) ) );
+   const int     q0 = __ldg( inc_begin + b ), q1 = __ldg( inc_begin + b + 1 );
+   const unsigned gmask = G == 32 ? 0xffffffffu : ( ( 1u << G ) - 1u ) << ( ( threadIdx.x & 31 ) & ~( G - 1 ) );
+   // this lane's share of the write-through (G = 1: the owner and every copy)
+   auto store = [&]( T* vec, A val ) {
+      if constexpr ( G == 1 ) wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, vec, val );
+      else
+      {
+         if ( sub == 0 ) st_any( vec + owner, val );
+         for ( int q = q0 + sub; q < q1; q += G ) st_any( vec + inc_slot( n, tk, inc[q], cell_off ), val );
+      }
+   };
    if ( !( bc[b] & flag ) )
    {
       if ( !copy_unflagged ) return;
-      if constexpr ( OP == OP_JAC || OP == OP_CHEB0 )
-         wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, A( ld_any( src + owner ) ) );
-      else if constexpr ( OP == OP_CHEBI ) wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, A( ld_any( v2 + owner ) ) );
+      if constexpr ( OP == OP_JAC || OP == OP_CHEB0 ) store( dst, A( ld_any( src + owner ) ) );
+      else if constexpr ( OP == OP_CHEBI ) store( dst, A( ld_any( v2 + owner ) ) );
       return;
    }
-   const A s = inc_sum< A >( __ldg( inc_begin + b ), __ldg( inc_begin + b + 1 ), inc,
-                             [&]( const Incidence& I ) { return acc[inc_slot( n, tk, I, cell_off )]; } );
+   A s;
+   if constexpr ( G == 1 )
+      s = inc_sum< A >( q0, q1, inc, [&]( const Incidence& I ) { return acc[inc_slot( n, tk, I, cell_off )]; } );
+   else
+   {
+      s = A( 0 );
+      for ( int q = q0 + sub; q < q1; q += G ) s += acc[inc_slot( n, tk, inc[q], cell_off )];
+#pragma unroll
+      for ( int o = G / 2; o > 0; o >>= 1 ) s += __shfl_xor_sync( gmask, s, o, G );
+   }
    if ( invd_out )  // diagonal setup: store 1/diag at the owner
    {
-      invd_out[owner] = A( 1 ) / s;
+      if ( sub == 0 ) invd_out[owner] = A( 1 ) / s;
       return;
    }
    A       second;
-   const A val = epilogue_value< T, A, OP >( owner, s, invd ? invd[owner] : A( 1 ), src, v1, v2, a0, a1, &second );
-   if constexpr ( OP == OP_CHEBL ) wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, v2, val );
-   else if constexpr ( OP == OP_APPLY_ADD )
-      wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, A( ld_any( dst + owner ) ) + val );
+   A       val = epilogue_value< T, A, OP >( owner, s, invd ? invd[owner] : A( 1 ), src, v1, v2, a0, a1, &second );
+   if constexpr ( OP == OP_APPLY_ADD ) val = A( ld_any( dst + owner ) ) + val;
+   // every lane of the group has read the owner's values before any lane stores
+   if constexpr ( G > 1 ) __syncwarp( gmask );
+   if constexpr ( OP == OP_CHEBL || OP == OP_APPLY_ADD ) store( OP == OP_CHEBL ? v2 : dst, val );
    else
    {
-      wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, dst, val );
-      if constexpr ( OP == OP_CHEBI ) wt_store< T, A >( n, tk, owner, inc_begin, inc, cell_off, v2, second );
+      store( dst, val );
+      if constexpr ( OP == OP_CHEBI ) store( v2, second );
    }
+}
+
+// launch of the owner combine over the level's tasks, lanes per task by level size
+template < typename T, typename A, int OP >
+static void launch_bnd_acc( cudaStream_t st, const P1Level& P, uint32_t flag, int copy_unflagged, const A* acc, const A* invd, A* invd_out,
+                            const T* src, const T* v1, T* v2, T* dst, A a0, A a1 )
+{
+   const int nt = int( P.tasks.size() );
+   if ( nt <= 0 ) return;
+   if ( P.n <= 4 )
+      k_bnd_acc< T, A, OP, 8 ><<< ( 8 * nt + 255 ) / 256, 256, 0, st >>>( P.n, nt, P.d_tasks, P.d_off, P.d_off + P.nB, P.d_bkind, P.d_bc,
+                                                                          P.d_inc_begin, P.d_inc, flag, copy_unflagged, acc, invd, invd_out,
+                                                                          src, v1, v2, dst, a0, a1 );
+   else
+      k_bnd_acc< T, A, OP, 1 ><<< ( nt + 255 ) / 256, 256, 0, st >>>( P.n, nt, P.d_tasks, P.d_off, P.d_off + P.nB, P.d_bkind, P.d_bc,
+                                                                      P.d_inc_begin, P.d_inc, flag, copy_unflagged, acc, invd, invd_out, src,
+                                                                      v1, v2, dst, a0, a1 );
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1347,9 +1389,7 @@ static void ensure_level_t( Context* ctx, Operator* op, int L, int dtype )
       k_cell_invert< A ><<< grid, 256, 0, ctx->stream >>>( P.n, nrows, P.d_rows, P.d_off + P.nB, acc, invd );
    }
    if ( !P.tasks.empty() )
-      k_bnd_acc< T, A, OP_APPLY ><<< ( int( P.tasks.size() ) + 255 ) / 256, 256, 0, ctx->stream >>>(
-          P.n, int( P.tasks.size() ), P.d_tasks, P.d_off, P.d_off + P.nB, P.d_bkind, P.d_bc, P.d_inc_begin, P.d_inc, kAll, 0, acc,
-          nullptr, invd, nullptr, nullptr, nullptr, nullptr, A( 0 ), A( 0 ) );
+      launch_bnd_acc< T, A, OP_APPLY >( ctx->stream, P, kAll, 0, acc, nullptr, invd, nullptr, nullptr, nullptr, nullptr, A( 0 ), A( 0 ) );
    check_cuda( cudaGetLastError(), "diagonal launch" );
 }
 
@@ -1430,9 +1470,8 @@ static void run_elem( Context* ctx, Mesh* m, Operator* op, int L, int dtype, con
       }
       if ( !P.tasks.empty() )
       {
-         k_bnd_acc< T, A, OP ><<< ( int( P.tasks.size() ) + 255 ) / 256, 256, 0, ctx->aux >>>(
-             P.n, int( P.tasks.size() ), P.d_tasks, P.d_off, P.d_off + P.nB, P.d_bkind, P.d_bc, P.d_inc_begin, P.d_inc, a.flag,
-             a.copy_unflagged, acc, inv, nullptr, (const T*) a.src, (const T*) a.v1, (T*) a.v2, (T*) a.dst, A( a.a0 ), A( a.a1 ) );
+         launch_bnd_acc< T, A, OP >( ctx->aux, P, a.flag, a.copy_unflagged, acc, inv, nullptr, (const T*) a.src, (const T*) a.v1,
+                                     (T*) a.v2, (T*) a.dst, A( a.a0 ), A( a.a1 ) );
          ++ctx->launches;
       }
    }
@@ -1485,9 +1524,7 @@ static void combine_acc( Context* ctx, Mesh* m, int L, const A* acc, uint32_t fl
    }
    if ( !P.tasks.empty() )
    {
-      k_bnd_acc< T, A, OP ><<< ( int( P.tasks.size() ) + 255 ) / 256, 256, 0, ctx->aux >>>(
-          P.n, int( P.tasks.size() ), P.d_tasks, P.d_off, P.d_off + P.nB, P.d_bkind, P.d_bc, P.d_inc_begin, P.d_inc, flag, 0, acc,
-          nullptr, nullptr, nullptr, nullptr, nullptr, dst, A( 0 ), A( 0 ) );
+      launch_bnd_acc< T, A, OP >( ctx->aux, P, flag, 0, acc, nullptr, nullptr, nullptr, nullptr, nullptr, dst, A( 0 ), A( 0 ) );
       ++ctx->launches;
    }
    check_cuda( cudaGetLastError(), "combine launch" );
@@ -1762,9 +1799,8 @@ static void run_visc( Context* ctx, Operator* op, int Lp, int mode, const void* 
          k_cell_invert< A ><<< grid, 256, 0, ctx->stream >>>( PU.n, nrows, PU.d_rows, PU.d_off + PU.nB, acc + k * PU.size, invd );
       }
       if ( !PU.tasks.empty() )
-         k_bnd_acc< T, A, OP_APPLY ><<< ( int( PU.tasks.size() ) + 255 ) / 256, 256, 0, ctx->stream >>>(
-             PU.n, int( PU.tasks.size() ), PU.d_tasks, PU.d_off, PU.d_off + PU.nB, PU.d_bkind, PU.d_bc, PU.d_inc_begin, PU.d_inc, kAll, 0,
-             acc + k * PU.size, nullptr, invd, nullptr, nullptr, nullptr, nullptr, A( 0 ), A( 0 ) );
+         launch_bnd_acc< T, A, OP_APPLY >( ctx->stream, PU, kAll, 0, acc + k * PU.size, nullptr, invd, nullptr, nullptr, nullptr, nullptr,
+                                           A( 0 ), A( 0 ) );
    }
    check_cuda( cudaGetLastError(), "viscous block diagonal launch" );
 }
