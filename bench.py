@@ -70,6 +70,18 @@ def dist_setup(n):
     return rank, world, local
 
 
+def job_rate(ms_local, units, world, device):
+    """Whole-job throughput of one step timed on every rank: the slowest rank's time (max over ranks)
+    and units x ranks / that time, in millions of units per second."""
+    import torch
+
+    t = torch.tensor([float(ms_local)], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    return ms_max, world * units / (ms_max * 1e-3) / 1e6
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
 
@@ -557,11 +569,7 @@ def run_ours(args, rank, world, local):
     launches = ctx.launches - l0
     barrier()
     torch.cuda.synchronize()
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * ndof / (ms_max * 1e-3) / 1e6
+    ms_max, value = job_rate(ms, ndof, world, "cuda")
 
     # end to end through the public API: host vector in (pinned host memory), apply, host vector out
     # (pinned); each transfer is one contiguous copy plus a device repack
@@ -605,10 +613,7 @@ def run_ours(args, rank, world, local):
         c.synchronize()
     t_e2e = (time.perf_counter() - t0) / e2e_steps
     assert np.array_equal(py[0], py[1]) and np.array_equal(py[0], out)
-    te = torch.tensor([t_e2e], device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = world * ndof / float(te.item()) / 1e6
+    _, e2e_value = job_rate(t_e2e * 1e3, ndof, world, "cuda")
 
     # one FP64 V(3,3) Chebyshev(3) multigrid cycle on the same level (graph-captured)
     vcycle = None
