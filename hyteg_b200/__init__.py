@@ -35,6 +35,8 @@ P1_CONST_LAPLACE = 1
 P1_CONST_MASS = 2
 SMOOTHER_JACOBI = 0
 SMOOTHER_CHEBYSHEV = 1
+SMOOTHER_GAUSS_SEIDEL = 2
+SMOOTHER_SOR = 3
 VCYCLE = 0
 WCYCLE = 1
 
@@ -132,6 +134,7 @@ _SIGS = {
     "hyb_p2p1_div_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_int]),
     "hyb_p1p2_divt_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_int]),
     "hyb_op_create_p1_pspg": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "hyb_op_smooth_sor": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_uint32, C.c_int]),
     "hyb_op_create_p2_full_viscous": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                                 C.POINTER(C.c_void_p)]),
     "hyb_p2_full_viscous_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_int]),
@@ -454,6 +457,19 @@ class _ConstantOperator:
     def getInverseDiagonalValues(self, out, level, flag=All):
         _check(lib().hyb_op_inverse_diagonal(self.h, out.h, level, flag))
         return out
+
+    def smooth_sor(self, dst, rhs, relax, level, flag, backwards=False):
+        """P1Operator::smooth_sor (constant-stencil operators): in place in dst."""
+        _check(lib().hyb_op_smooth_sor(self.h, dst.h, rhs.h, float(relax), level, flag, 1 if backwards else 0))
+
+    def smooth_gs(self, dst, rhs, level, flag):
+        self.smooth_sor(dst, rhs, 1.0, level, flag)
+
+    def smooth_sor_backwards(self, dst, rhs, relax, level, flag):
+        self.smooth_sor(dst, rhs, relax, level, flag, backwards=True)
+
+    def smooth_gs_backwards(self, dst, rhs, level, flag):
+        self.smooth_sor(dst, rhs, 1.0, level, flag, backwards=True)
 
     def stencil(self, level, cell, cls=0):
         a = np.zeros(15)
@@ -793,7 +809,11 @@ class GeometricMultigridSolver:
         p.min_level, p.max_level = minLevel, maxLevel
         p.pre_smooth, p.post_smooth, p.smooth_increment = preSmoothSteps, postSmoothSteps, smoothIncrementOnCoarserGrids
         p.cycle = cycleType
-        p.smoother = SMOOTHER_CHEBYSHEV if smoother == "chebyshev" else SMOOTHER_JACOBI
+        kinds = {"jacobi": SMOOTHER_JACOBI, "chebyshev": SMOOTHER_CHEBYSHEV, "gauss_seidel": SMOOTHER_GAUSS_SEIDEL,
+                 "sor": SMOOTHER_SOR}
+        if smoother not in kinds:
+            raise ValueError("smoother must be one of " + ", ".join(kinds))
+        p.smoother = kinds[smoother]
         p.jacobi_relax = relax
         p.cheb_order, p.cheb_upper_factor, p.cheb_lower_factor = chebyshev_order, chebyshev_upper, chebyshev_lower
         p.cheb_power_iterations = power_iterations

@@ -24,6 +24,7 @@ struct hyb_ctx
       cudaFree( c.d_scalars );
       cudaFree( c.d_error );
       cudaFree( c.d_stage );
+      cudaFree( c.d_sor );
       if ( c.aux ) cudaStreamSynchronize( c.aux ), cudaStreamDestroy( c.aux );
       if ( c.ev_fork ) cudaEventDestroy( c.ev_fork );
       if ( c.ev_join ) cudaEventDestroy( c.ev_join );
@@ -1165,6 +1166,21 @@ int hyb_op_apply( hyb_op* op, hyb_fn* src, hyb_fn* dst, int level, uint32_t flag
    HYB_CATCH
 }
 
+int hyb_op_smooth_sor( hyb_op* op, hyb_fn* dst, hyb_fn* rhs, double relax, int level, uint32_t flag, int backwards )
+{
+   HYB_TRY
+   require( op, "op is NULL" );
+   level += op->o.order - 1;
+   check_op_fn( op, dst, level );
+   check_op_fn( op, rhs, level );
+   require( dst != rhs, "dst and rhs must differ" );
+   require( dst->f.dtype == rhs->f.dtype, "value types differ" );
+   require( !op->o.elementwise, "Gauss-Seidel / SOR is provided for constant-stencil operators" );
+   launch_sor( &op->ctx->c, op->o.mesh, &op->o, level, dst->f.dtype, flag, dst->f.ptr( level ), rhs->f.ptr( level ), relax,
+               backwards != 0 );
+   HYB_CATCH
+}
+
 int hyb_op_smooth_jac( hyb_op* op, hyb_fn* dst, hyb_fn* rhs, hyb_fn* src, double relax, int level, uint32_t flag )
 {
    HYB_TRY
@@ -1494,6 +1510,13 @@ static void smooth( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int L )
 {
    hyb_op* op = g->op;
    const int dt = x->f.dtype;
+   if ( g->p.smoother == HYB_SMOOTHER_GAUSS_SEIDEL || g->p.smoother == HYB_SMOOTHER_SOR )
+   {
+      // GaussSeidelSmoother::solve -> smooth_gs (relax 1), SORSmoother::solve -> smooth_sor
+      const double relax = g->p.smoother == HYB_SMOOTHER_SOR ? g->p.jacobi_relax : 1.0;
+      launch_sor( &g->ctx->c, op->o.mesh, &op->o, L, dt, kSolveFlag, x->f.ptr( L ), b->f.ptr( L ), relax, 0 );
+      return;
+   }
    if ( g->p.smoother == HYB_SMOOTHER_JACOBI )
    {
       // WeightedJacobiSmoother::solve: tmp <- x (All); x <- tmp + w D^-1 (b - A tmp).  The copy is
@@ -1773,7 +1796,11 @@ int hyb_gmg_create( hyb_ctx* ctx, hyb_op* op, const hyb_gmg_params* params, hyb_
    p.max_level += op->o.order - 1;
    require( p.min_level >= op->o.minL && p.max_level <= op->o.maxL && p.min_level <= p.max_level,
             "multigrid levels outside the operator's level range" );
-   require( p.smoother == HYB_SMOOTHER_JACOBI || p.smoother == HYB_SMOOTHER_CHEBYSHEV, "unknown smoother" );
+   require( p.smoother == HYB_SMOOTHER_JACOBI || p.smoother == HYB_SMOOTHER_CHEBYSHEV || p.smoother == HYB_SMOOTHER_GAUSS_SEIDEL ||
+                p.smoother == HYB_SMOOTHER_SOR,
+            "unknown smoother" );
+   require( ( p.smoother != HYB_SMOOTHER_GAUSS_SEIDEL && p.smoother != HYB_SMOOTHER_SOR ) || !op->o.elementwise,
+            "Gauss-Seidel / SOR smoothing is provided for constant-stencil operators" );
    require( p.cycle == HYB_VCYCLE || p.cycle == HYB_WCYCLE, "unknown cycle type" );
    require( p.pre_smooth >= 0 && p.post_smooth >= 0 && p.smooth_increment >= 0, "negative smoothing steps" );
    require( p.coarse_max_iter >= 0, "negative coarse iteration count" );

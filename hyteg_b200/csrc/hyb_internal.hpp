@@ -263,6 +263,8 @@ struct Context {
    int*    d_error   = nullptr;  // device error word (bounded waits that gave up)
    double* d_stage   = nullptr;  // packed-vector staging for host transfers (grown on demand)
    int64_t stage_cap = 0;
+   double* d_sor     = nullptr;  // new owner values of a Gauss-Seidel colour set (one per boundary task)
+   int64_t sor_cap   = 0;
    int64_t launches = 0;         // kernel launches issued through this context
 };
 
@@ -345,6 +347,11 @@ void launch_restrict( Context* ctx, Mesh* m, int Lfine, int dtype, uint32_t flag
 void launch_prolongate( Context* ctx, Mesh* m, int Lcoarse, int dtype, uint32_t flag, const void* coarse, void* fine, int add );
 void launch_axpy_to_f64( Context* ctx, int64_t count, double* x, int src_dtype, const void* c, double a );
 void prepare_device( Context* ctx, Mesh* m, Operator* op, int minL, int maxL, int dtype );
+// Gauss-Seidel / SOR sweep of a constant-stencil operator on level L (in place in x, flagged DoFs):
+// colour sets in the reference's primitive order (vertices, edges, faces, cells), reversed when
+// backwards
+void launch_sor( Context* ctx, Mesh* m, Operator* op, int L, int dtype, uint32_t flag, void* x, const void* rhs, double relax,
+                 int backwards );
 void launch_fill_uniform( Context* ctx, int64_t count, int dtype, void* dst, uint64_t seed );
 void launch_cg_scalar( Context* ctx, double* state, int stage, double rtol, double atol );
 

@@ -2435,6 +2435,154 @@ void launch_p2_prolongate( Context* ctx, Mesh* m, int Lc, int dtype, uint32_t fl
 }
 
 // allocate every lazily created device table for levels minL..maxL (needed before graph capture)
+// ---------------------------------------------------------------------------------------------
+// Gauss-Seidel / SOR (P1Operator::smooth_sor, P1Operator.hpp:339-420, with the generated
+// sor_3D_macrocell_P1 / sor_3D_macroface_P1 kernels): x <- x + relax D^-1 (b - A x) point by point.
+// The reference sweeps the macro-vertices, -edges, -faces and -cells in turn, each
+// lexicographically.  Here the same primitive order with colour sets inside each class: vertex DoFs
+// (no two are neighbours), edge DoFs by the parity of their edge index, face DoFs by (i + 2j) mod 3,
+// cell interiors by (x + 2y + 3z) mod 4.  The last is a proper colouring of the 15-point stencil
+// (the offsets give 1, 2, 3, 1, 2, 1 and 2 mod 4), so a cell colour is updated in place.  Points of
+// different faces or edges can be neighbours, so a boundary colour set is computed from the values
+// before the set (into a scratch array) and then written through: every set is deterministic.
+// Backward sweeps run the sets in reverse order.
+// ---------------------------------------------------------------------------------------------
+template < typename T, typename A >
+__global__ void __launch_bounds__( 256 ) k_sor_cell( LevelView v, OpView< A > o, uint32_t flag, int color, const T* __restrict__ rhs,
+                                                      T* x, A relax )
+{
+   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+   const int r    = blockIdx.x * 8 + warp;
+   const int c    = blockIdx.y;
+   if ( r >= v.nrows || !( v.cell_bc[c] & flag ) ) return;
+   const int2    yz   = v.rows[r];
+   const int     y = yz.x, z = yz.y, n = v.n;
+   const int64_t base = v.cell_off[c];
+   T*            s    = x + base;
+   const int64_t r00 = cidx( n, 0, y, z ), rm0 = cidx( n, 0, y - 1, z ), rp0 = cidx( n, 0, y + 1, z );
+   const int64_t r0m = cidx( n, 0, y, z - 1 ), r0p = cidx( n, 0, y, z + 1 );
+   const int64_t rmp = cidx( n, 0, y - 1, z + 1 ), rpm = cidx( n, 0, y + 1, z - 1 );
+   const A*      W    = o.W + size_t( c ) * kNumClasses * kNumDirs;  // interior class 0
+   const A       invd = o.invd_c[c];
+   const int     xmax = n - 1 - y - z;
+   const int     x0   = 1 + ( ( ( color - 1 - 2 * y - 3 * z ) % 4 ) + 4 ) % 4;  // first x >= 1 of the colour
+   for ( int xx = x0 + 4 * lane; xx <= xmax; xx += 128 )
+   {
+      A acc = W[0] * A( ldc( s + r00 + xx ) );
+      acc += W[1] * A( ldc( s + r00 + xx - 1 ) );
+      acc += W[2] * A( ldc( s + r00 + xx + 1 ) );
+      acc += W[3] * A( ldc( s + rm0 + xx ) );
+      acc += W[4] * A( ldc( s + rp0 + xx ) );
+      acc += W[5] * A( ldc( s + r0m + xx ) );
+      acc += W[6] * A( ldc( s + r0p + xx ) );
+      acc += W[7] * A( ldc( s + rp0 + xx - 1 ) );
+      acc += W[8] * A( ldc( s + rm0 + xx + 1 ) );
+      acc += W[9] * A( ldc( s + r0p + xx - 1 ) );
+      acc += W[10] * A( ldc( s + r0m + xx + 1 ) );
+      acc += W[11] * A( ldc( s + rmp + xx ) );
+      acc += W[12] * A( ldc( s + rpm + xx ) );
+      acc += W[13] * A( ldc( s + rmp + xx + 1 ) );
+      acc += W[14] * A( ldc( s + rpm + xx - 1 ) );
+      const int64_t i = base + r00 + xx;
+      stv( x + i, A( ldc( x + i ) ) + relax * ( invd * ( A( ldc( rhs + i ) ) - acc ) ) );
+   }
+}
+
+// colour of boundary task tk in its primitive class (kind 0 vertex, 1 edge, 2 face)
+__device__ __forceinline__ int sor_task_color( int kind, const int4& tk ) { return kind == 1 ? ( tk.y & 1 ) : kind == 2 ? ( tk.y + 2 * tk.z ) % 3 : 0; }
+
+template < typename T, typename A >
+__global__ void __launch_bounds__( 256 ) k_sor_bnd_new( LevelView v, OpView< A > o, uint32_t flag, int kind, int color,
+                                                         const T* __restrict__ rhs, const T* x, A relax, A* nv )
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( t >= v.ntasks ) return;
+   const int4 tk = v.tasks[t];
+   const int  b  = tk.x;
+   if ( v.bkind[b] != kind || !( v.bc[b] & flag ) || sor_task_color( kind, tk ) != color ) return;
+   const int     n     = v.n;
+   const int64_t owner = owner_slot( v, b, tk.y, tk.z );
+   A             acc   = A( 0 );
+   for ( int q = v.inc_begin[b]; q < v.inc_begin[b + 1]; ++q )
+   {
+      const Incidence I = v.inc[q];
+      int             px, py, pz;
+      inc_point( I, n, tk.y, tk.z, px, py, pz );
+      acc += class_stencil< T, A >( x + v.cell_off[I.cell], o.W + ( size_t( I.cell ) * kNumClasses + I.cls ) * kNumDirs, c_cls_mask[I.cls],
+                                    n, px, py, pz );
+   }
+   nv[t] = A( ldc( x + owner ) ) + relax * ( o.invd_b[b] * ( A( ldc( rhs + owner ) ) - acc ) );
+}
+
+template < typename T, typename A >
+__global__ void __launch_bounds__( 256 ) k_sor_bnd_write( LevelView v, uint32_t flag, int kind, int color, const A* __restrict__ nv, T* x )
+{
+   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+   if ( t >= v.ntasks ) return;
+   const int4 tk = v.tasks[t];
+   const int  b  = tk.x;
+   if ( v.bkind[b] != kind || !( v.bc[b] & flag ) || sor_task_color( kind, tk ) != color ) return;
+   write_through( v, x, b, tk.y, tk.z, owner_slot( v, b, tk.y, tk.z ), nv[t] );
+}
+
+static double* sor_scratch( Context* ctx, int64_t ntasks )
+{
+   if ( ctx->sor_cap < ntasks )
+   {
+      if ( ctx->d_sor ) check_cuda( cudaFree( ctx->d_sor ), "cudaFree(SOR scratch)" );
+      ctx->d_sor = nullptr;
+      check_cuda( cudaMalloc( &ctx->d_sor, size_t( ntasks ) * sizeof( double ) ), "cudaMalloc(SOR scratch)" );
+      ctx->sor_cap = ntasks;
+   }
+   return ctx->d_sor;
+}
+
+template < typename T, typename A >
+static void run_sor( Context* ctx, const LevelView& v, const OpView< A >& o, int nC, uint32_t flag, T* x, const T* rhs, A relax, int backwards )
+{
+   A* nv = reinterpret_cast< A* >( sor_scratch( ctx, std::max( v.ntasks, 1 ) ) );
+   // sets: (kind, colour) with kind 3 the cell interiors
+   static const int kSets[10][2] = { { 0, 0 }, { 1, 0 }, { 1, 1 }, { 2, 0 }, { 2, 1 }, { 2, 2 }, { 3, 0 }, { 3, 1 }, { 3, 2 }, { 3, 3 } };
+   for ( int k = 0; k < 10; ++k )
+   {
+      const int kind = kSets[backwards ? 9 - k : k][0], color = kSets[backwards ? 9 - k : k][1];
+      if ( kind == 3 )
+      {
+         if ( v.nrows <= 0 || nC <= 0 ) continue;
+         dim3 grid( ( v.nrows + 7 ) / 8, nC );
+         k_sor_cell< T, A ><<< grid, 256, 0, ctx->stream >>>( v, o, flag, color, rhs, x, relax );
+         ++ctx->launches;
+         continue;
+      }
+      if ( v.ntasks <= 0 ) continue;
+      const int nb = ( v.ntasks + 255 ) / 256;
+      k_sor_bnd_new< T, A ><<< nb, 256, 0, ctx->stream >>>( v, o, flag, kind, color, rhs, x, relax, nv );
+      k_sor_bnd_write< T, A ><<< nb, 256, 0, ctx->stream >>>( v, flag, kind, color, nv, x );
+      ctx->launches += 2;
+   }
+   check_cuda( cudaGetLastError(), "SOR launch" );
+}
+
+void launch_sor( Context* ctx, Mesh* m, Operator* op, int L, int dtype, uint32_t flag, void* x, const void* rhs, double relax,
+                 int backwards )
+{
+   ensure_constants();
+   if ( op->elementwise ) throw std::invalid_argument( "Gauss-Seidel / SOR is provided for constant-stencil operators" );
+   LevelView v  = make_view( m, L );
+   OpLevel&  ol = op->lv.at( L );
+   ensure_device_op( ol );
+   const int nC = m->topo.nC;
+   if ( dtype == F64 )
+      run_sor< double, double >( ctx, v, OpView< double >{ ol.d_W, ol.d_invd_b, ol.d_invd_c }, nC, flag, (double*) x, (const double*) rhs,
+                                 relax, backwards );
+   else if ( dtype == F32 )
+      run_sor< float, float >( ctx, v, OpView< float >{ ol.d_Wf, ol.d_invd_bf, ol.d_invd_cf }, nC, flag, (float*) x, (const float*) rhs,
+                               float( relax ), backwards );
+   else
+      run_sor< __half, float >( ctx, v, OpView< float >{ ol.d_Wf, ol.d_invd_bf, ol.d_invd_cf }, nC, flag, (__half*) x, (const __half*) rhs,
+                                float( relax ), backwards );
+}
+
 void prepare_device( Context* ctx, Mesh* m, Operator* op, int minL, int maxL, int dtype )
 {
    ensure_constants();
@@ -2451,6 +2599,7 @@ void prepare_device( Context* ctx, Mesh* m, Operator* op, int minL, int maxL, in
       }
       const int nb = ( ( v.nrows + 7 ) / 8 ) * m->topo.nC + ( v.ntasks + 255 ) / 256 + 1;
       most         = std::max( most, nb );
+      if ( op && !op->elementwise ) sor_scratch( ctx, std::max( v.ntasks, 1 ) );
    }
    partials( ctx, most );
 }

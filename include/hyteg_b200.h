@@ -77,6 +77,8 @@ typedef struct hyb_coeff
 /* smoother kinds */
 #define HYB_SMOOTHER_JACOBI 0    /* solvers/WeightedJacobiSmoother.hpp:46-66 */
 #define HYB_SMOOTHER_CHEBYSHEV 1 /* solvers/ChebyshevSmoother.hpp:112-240 */
+#define HYB_SMOOTHER_GAUSS_SEIDEL 2 /* solvers/GaussSeidelSmoother.hpp:31-60: smooth_gs (SOR with relax 1) */
+#define HYB_SMOOTHER_SOR 3          /* solvers/SORSmoother.hpp: smooth_sor with relax = jacobi_relax */
 
 #define HYB_VCYCLE 0 /* CycleType::VCYCLE, solvers/GeometricMultigridSolver.hpp */
 #define HYB_WCYCLE 1
@@ -227,6 +229,13 @@ int hyb_op_destroy( hyb_op* op );
 int hyb_op_apply( hyb_op* op, hyb_fn* src, hyb_fn* dst, int level, uint32_t flag, int update );
 /* WeightedJacobiSmoothable::smooth_jac(dst, rhs, src, relax, level, flag) (solvers/Smoothables.hpp:33-40,
  * P1Operator.hpp:429-447): dst = src + relax * D^-1 (rhs - A src) on flagged DoFs */
+/* P1Operator::smooth_sor / smooth_gs / smooth_sor_backwards (p1functionspace/P1Operator.hpp:322-420)
+ * for constant-stencil operators: dst <- dst + relax D^-1 (rhs - A dst) point by point on the flagged
+ * DoFs, in place.  The sweep keeps the reference's primitive order (macro-vertices, -edges, -faces,
+ * -cells; reversed when backwards) with colour sets inside each class (edge DoFs by index parity,
+ * face DoFs by (i + 2j) mod 3, cell interiors by (x + 2y + 3z) mod 4) instead of the lexicographic
+ * order inside a primitive, so iterates differ from the reference's in order, not in kind. */
+int hyb_op_smooth_sor( hyb_op* op, hyb_fn* dst, hyb_fn* rhs, double relax, int level, uint32_t flag, int backwards );
 int hyb_op_smooth_jac( hyb_op* op, hyb_fn* dst, hyb_fn* rhs, hyb_fn* src, double relax, int level, uint32_t flag );
 /* OperatorWithInverseDiagonal::getInverseDiagonalValues (solvers/Smoothables.hpp:109-119) written into out */
 int hyb_op_inverse_diagonal( hyb_op* op, hyb_fn* out, int level, uint32_t flag );
@@ -247,7 +256,7 @@ typedef struct hyb_gmg_params
    int    pre_smooth, post_smooth, smooth_increment; /* GeometricMultigridSolver.hpp:61-75 */
    int    cycle;                                     /* HYB_VCYCLE | HYB_WCYCLE */
    int    smoother;                                  /* HYB_SMOOTHER_* */
-   double jacobi_relax;                              /* WeightedJacobiSmoother relax */
+   double jacobi_relax;                              /* WeightedJacobiSmoother relax; the SOR smoother's relax */
    int    cheb_order;                                /* ChebyshevSmoother::setupCoefficients order */
    double cheb_upper_factor, cheb_lower_factor;      /* 1.2, 0.3 */
    int    cheb_power_iterations;                     /* chebyshev::estimateRadius iterations per level */

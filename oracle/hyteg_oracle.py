@@ -686,6 +686,60 @@ class GMG:
             self.smooth(x[L], b[L], L)
 
 
+def sor_color_sets(lev: Level):
+    """Slot masks of the device Gauss-Seidel's colour sets in sweep order: macro-vertex DoFs; edge DoFs
+    by the parity of their edge index; face DoFs by (i + 2j) mod 3 of their face index (i, j); cell
+    interiors by (x + 2y + 3z) mod 4 of their cell-local coordinates."""
+    m, n = lev.mesh, lev.n
+    sets = []
+    V = np.zeros(lev.size, dtype=bool)
+    V[np.asarray(lev.off_v, dtype=np.int64)] = True
+    sets.append(V)
+    for col in (0, 1):
+        S = np.zeros(lev.size, dtype=bool)
+        i = np.arange(1, n)
+        for e in range(m.nE):
+            S[lev.off_e[e] + i[i % 2 == col]] = True
+        sets.append(S)
+    ij = [(i, j) for j in range(1, n) for i in range(1, n - j)]
+    for col in (0, 1, 2):
+        S = np.zeros(lev.size, dtype=bool)
+        sel = [face_index(n, i, j) for i, j in ij if (i + 2 * j) % 3 == col]
+        for f in range(m.nF):
+            if sel:
+                S[lev.off_f[f] + np.array(sel, dtype=np.int64)] = True
+        sets.append(S)
+    pts = tet_points(n + 1)
+    inner = (pts.min(axis=1) >= 1) & (pts.sum(axis=1) <= n - 1)
+    p = pts[inner]
+    for col in range(4):
+        S = np.zeros(lev.size, dtype=bool)
+        q = p[(p[:, 0] + 2 * p[:, 1] + 3 * p[:, 2]) % 4 == col]
+        for c in range(m.nC):
+            if len(q):
+                S[lev.off_c[c] + cell_index(n, q[:, 0], q[:, 1], q[:, 2])] = True
+        sets.append(S)
+    return sets
+
+
+def sor_sweep(op, x, b, L, relax, flag, backwards=False):
+    """P1Operator::smooth_sor (P1Operator.hpp:339-420) in the device's colour-set order: for each set
+    S (reversed when backwards) x_S <- x_S + relax D^-1 (b - A x)_S with the values before the set,
+    copies refreshed after every set."""
+    lev = op.levels[L]
+    own = lev.owned_mask(flag)
+    sets = sor_color_sets(lev)
+    if backwards:
+        sets = sets[::-1]
+    x = lev.sync(x.copy())
+    for S in sets:
+        sel = S & own
+        r = b - op.A[L] @ x
+        x[sel] = x[sel] + relax * (op.invdiag[L][sel] * r[sel])
+        x = lev.sync(x)
+    return x
+
+
 def power_iteration_radius(op: P1ConstantLaplace, L, x0, iters):
     """estimateSpectralRadiusWithPowerIteration on D^-1 A (SpectrumEstimation.hpp:56-84), flag All."""
     lev = op.levels[L]

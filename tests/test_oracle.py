@@ -410,3 +410,35 @@ def test_stokes_oracle_vcycle_converges():
         u, p = S.vcycle(u, p, bu, bp, 2, radii)
         r.append(S.residual_norm(u, p, bu, bp, 2))
     assert r[-1] < 0.2 * r[0]
+
+
+@pytest.mark.parametrize("name", ["cube_6", "octahedron_8"])
+def test_sor_color_sets(name):
+    """The Gauss-Seidel colour sets cover every owned DoF exactly once, the cell-interior colours are a
+    proper colouring of the stencil (no coupling inside a set), and a sweep reduces the residual."""
+    coords, tets = M.ALL[name]()
+    op = O.P1ConstantLaplace(O.MacroMesh(coords, tets), 3, 3)
+    L = 3
+    lev = op.levels[L]
+    sets = O.sor_color_sets(lev)
+    owned = np.zeros(lev.size, dtype=bool)
+    owned[lev.owned] = True
+    count = sum(S.astype(int) for S in sets)
+    assert np.all(count[owned] == 1)
+    A = op.A[L].tocsr()
+    for S in sets[6:]:
+        idx = np.flatnonzero(S)
+        sub = A[idx][:, idx]
+        sub.setdiag(0)
+        sub.eliminate_zeros()
+        assert sub.nnz == 0
+    rng = np.random.default_rng(4)
+    x = np.zeros(lev.size)
+    m = lev.owned_mask(O.INNER)
+    x[m] = rng.uniform(-1, 1, m.sum())
+    x = lev.sync(x)
+    b = np.zeros(lev.size)
+    r0 = np.linalg.norm((b - A @ x)[m])
+    y = O.sor_sweep(op, x, b, L, 1.0, O.INNER)
+    y = O.sor_sweep(op, y, b, L, 1.0, O.INNER, backwards=True)
+    assert np.linalg.norm((b - A @ y)[m]) < 0.8 * r0
