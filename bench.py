@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--no-p2", action="store_true")
     p.add_argument("--no-stokes", action="store_true")
     p.add_argument("--serve-requests", type=int, default=200)
+    p.add_argument("--profile-vcycle", action="store_true",
+                   help="run one FP64 and one FP32 V(3,3) Chebyshev(3) cycle of the level-8 cube without graph capture "
+                        "between profiler start/stop (for ncu --profile-from-start off) and print their times")
     return p.parse_args()
 
 
@@ -526,10 +529,46 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def profile_vcycle(args):
+    """One FP64 and one FP32-storage V(3,3) Chebyshev(3) cycle on the six-tetrahedra cube at the bench
+    level, launched kernel by kernel (no graph), each inside cudaProfilerStart/Stop after a setup
+    cycle; prints the wall time per cycle of three uncaptured cycles per value type."""
+    import torch
+
+    import hyteg_b200 as H
+
+    ctx = H.Context(0)
+    pm = H.PrimitiveStorage.cuboid(ctx=ctx)
+    L = args.level
+    A = H.P1ConstantLaplaceOperator(pm, 0, L, ctx)
+    out = {}
+    for dt in ("float64", "float32"):
+        x = H.P1Function("x", pm, 0, L, ctx, dtype=dt)
+        b = H.P1Function("b", pm, 0, L, ctx, dtype=dt)
+        b.fill_random(L, 5)
+        g = H.GeometricMultigridSolver(ctx, A, 0, L, 3, 3, smoother="chebyshev", chebyshev_order=3, power_iterations=20,
+                                       use_graph=False)
+        g.solve(A, x, b, L)  # setup
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(3):
+            g.solve(A, x, b, L)
+        ctx.synchronize()
+        out[dt] = (time.perf_counter() - t0) / 3 * 1e3
+        torch.cuda.profiler.start()
+        g.solve(A, x, b, L)
+        ctx.synchronize()
+        torch.cuda.profiler.stop()
+    print(json.dumps({"profile_vcycle_ms_per_cycle_without_graph": out, "level": L}))
+
+
 def run_ours(args, rank, world, local):
     import torch
 
     import hyteg_b200 as H
+
+    if args.profile_vcycle:
+        return profile_vcycle(args)
 
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
