@@ -53,3 +53,17 @@ def test_gauss_seidel_multigrid_meets_reference_bound(ctx):
         cur = res.dotGlobal(res, L, H.Inner) / npts
         assert cur / last < 3.2e-2, cur / last
         last = cur
+
+
+@pytest.mark.parametrize("dtype,tol", [("float32", 1e-5)])
+def test_sor_sweep_low_precision(ctx, dtype, tol):
+    L = 4
+    s = Setup(ctx, "cube_6", L, L, dtype=dtype)
+    x, b = s.rand(L, 41), s.rand(L, 42)
+    fx, fb = s.fn("x"), s.fn("b")
+    fx.upload(L, x)
+    fb.upload(L, b)
+    xq, bq = fx.download(L), fb.download(L)
+    s.A.smooth_gs(fx, fb, L, O.INNER)
+    ref = O.sor_sweep(s.op, xq, bq, L, 1.0, O.INNER)
+    assert relerr(fx.download(L), ref, s.op.levels[L].owned_mask(O.ALL)) < tol
