@@ -161,8 +161,9 @@ def test_stokes_vcycle_factors(ctx, case, block):
     assert hist[-1] < hist[0]
 
 
+@pytest.mark.parametrize("block", ["laplace", "full_viscous"])
 @pytest.mark.parametrize("inner", ["float32"])
-def test_stokes_mixed_precision_reaches_fp64_accuracy(ctx, inner):
+def test_stokes_mixed_precision_reaches_fp64_accuracy(ctx, inner, block):
     """FP64 defect correction around FP32 / FP16 Uzawa V-cycles reaches the same relative residual
     (1e-6; the Uzawa multigrid's asymptotic factor on this shell is about 0.84) and the FP64 V-cycle
     solution to within the residual level (1e-4 relative, max norm, velocity)."""
@@ -173,12 +174,12 @@ def test_stokes_mixed_precision_reaches_fp64_accuracy(ctx, inner):
     bu, bp = _fns(pm, ctx, 0, L)
     for k in range(3):
         bu[k].upload(L, bu0[k])
-    st = H.StokesUzawaMultigrid(ctx, pm, 0, L, viscosity=ETA, blending=bl)
+    st = H.StokesUzawaMultigrid(ctx, pm, 0, L, viscosity=ETA, blending=bl, velocity_block=block)
     hist = st.solve(u, p, bu, bp, L, 120, rtol=1e-6)
     assert hist[-1] < 1e-6 * hist[0]
     ui = [H.P2Function("ui%d" % k, pm, 0, L, ctx) for k in range(3)]
     pi = H.P1Function("pi", pm, 0, L, ctx)
-    inner_solver = H.StokesUzawaMultigrid(ctx, pm, 0, L, viscosity=ETA, blending=bl)
+    inner_solver = H.StokesUzawaMultigrid(ctx, pm, 0, L, viscosity=ETA, blending=bl, velocity_block=block)
     mh = st.mixed_solve(inner_solver, ui, pi, bu, bp, L, max_outer=120, rtol=1e-6, inner_dtype=inner)
     assert mh[-1] < 1e-6 * mh[0]
     m = S.umask(L)
