@@ -120,3 +120,19 @@ def test_spherical_shell_matches_reference_generator(ntan):
     assert np.allclose(np.sort(np.unique(np.round(r, 12))), [0.55, 0.775, 1.0])
     with pytest.raises(H.HybError):
         H.PrimitiveStorage.spherical_shell(4, 3, 0.55, 1.0)  # ntan-1 not a power of two (SHELLMESH_CLASSIC)
+
+
+def test_python_rejects_unknown_solver_options():
+    """Option names are checked before any device work: unknown smoothers and velocity blocks raise."""
+    with pytest.raises(ValueError):
+        H.GeometricMultigridSolver(None, None, 0, 1, smoother="ilu")
+    with pytest.raises(ValueError):
+        H.StokesUzawaMultigrid(None, None, 0, 1, velocity_block="stress")
+
+
+def test_sor_and_viscous_entry_points_validate_arguments():
+    """NULL handles are refused with an error code (no device needed)."""
+    import ctypes as C
+    assert H.lib().hyb_op_smooth_sor(None, None, None, C.c_double(1.0), 1, 1, 0) != 0
+    assert H.lib().hyb_p2_full_viscous_apply(None, None, None, 1, 1, 0) != 0
+    assert H.lib().hyb_p2_full_viscous_inverse_diagonal(None, None, 1) != 0
