@@ -185,6 +185,35 @@ def cpu_reference_apply(L, seconds=10.0, max_steps=None, threads=None):
     return cell_inner * k / el / 1e6, k, threads, el
 
 
+def reference_parity(H, pm, x, y, L):
+    """Checker for the timed apply: the largest difference between this level's cell interiors of
+    y = A x and the reference's own compiled cell kernel (apply_3D_macrocell_vertexdof_to_vertexdof_
+    replace, oracle/_ref) run on the same device input x, relative to the largest reference value.
+    The stencil of each macro-cell comes from the oracle's element matrices."""
+    from oracle import hyteg_oracle as O
+    from oracle import ref as R
+
+    if not R.available():
+        return None
+    nV, nE, nF, nC = pm.counts()
+    coords = pm.vertex_coords()
+    tets = np.array([pm.primitive_vertices(3, c) for c in range(nC)], dtype=np.int64)
+    om = O.MacroMesh(coords, tets)
+    offs, _ = pm.primitive_offsets(L)
+    xs, ys = x.download(L), y.download(L)
+    n = 1 << L
+    size = O.tet_size(n + 1)
+    pts = O.tet_points(n + 1)
+    inner = (pts.min(axis=1) >= 1) & (pts.sum(axis=1) <= n - 1)
+    worst = 0.0
+    for c in range(nC):
+        o = int(offs[nV + nE + nF + c])
+        ref = R.cell_apply(np.ascontiguousarray(xs[o:o + size]), L, O.cell_stencils_by_mask(om, c, L)[0])
+        d = np.abs(ys[o:o + size][inner] - ref[inner]).max() / max(np.abs(ref[inner]).max(), 1e-300)
+        worst = max(worst, float(d))
+    return worst
+
+
 def mixed_precision_leg(H, ctx, pm, A, L, rtol=1e-8):
     """Time to ||r||/||r0|| < rtol from a zero guess: plain FP64 V(3,3) Chebyshev(3) cycles against
     FP64 defect correction around the same cycles in FP32 and FP16 storage (FP32 accumulation).
@@ -678,6 +707,8 @@ def run_ours(args, rank, world, local):
 
     if rank != 0:
         return
+    A.apply(x, y, L, H.Inner)
+    parity = reference_parity(H, pm, x, y, L)
     mixed = None if args.no_mixed else mixed_precision_leg(H, ctx, pm, A, L)
     serving = None if args.no_serve else serving_leg(H, ctx, nreq=args.serve_requests)
     p2 = None
@@ -701,11 +732,14 @@ def run_ours(args, rank, world, local):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind, "traffic": profile_traffic(),
                      "algorithmic_bytes_per_launch": alg_bytes,
-                     "kernel": "k_cell_zsum<double,OP_APPLY> + k_bnd_stencil (one apply)"},
+                     "kernel": "k_cell_sweep<double,double,OP_APPLY> + k_bnd_stencil (one apply)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": packed * 8, "d2h_bytes_per_step": packed * 8,
                 "steps": "double-buffered on two streams (upload, apply, download per step)",
                 "serial_value": world * ndof / t_serial / 1e6},
         "gpu_launches": launches,
+        "parity_rel_err": parity,
+        "parity_check": "cell interiors of the timed apply against the reference's compiled "
+                        "apply_3D_macrocell_vertexdof_to_vertexdof_replace on the same input (max norm, relative)",
         "clocks": clk.summary(),
     }
     if vcycle:

@@ -66,6 +66,7 @@ _SIGS = {
     "hyb_ctx_destroy": (C.c_int, [C.c_void_p]),
     "hyb_ctx_synchronize": (C.c_int, [C.c_void_p]),
     "hyb_ctx_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "hyb_ctx_scratch_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "hyb_ctx_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "hyb_mesh_create": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
     "hyb_mesh_create_cuboid": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
@@ -114,6 +115,7 @@ _SIGS = {
     "hyb_gmg_set_radii": (C.c_int, [C.c_void_p, C.c_void_p]),
     "hyb_gmg_get_radii": (C.c_int, [C.c_void_p, C.c_void_p]),
     "hyb_gmg_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "hyb_gmg_smooth": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
     "hyb_gmg_solve_cycles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_void_p,
                                        C.POINTER(C.c_int)]),
     "hyb_estimate_radius": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double)]),
@@ -208,6 +210,13 @@ class Context:
     def launches(self):
         v = C.c_int64()
         _check(lib().hyb_ctx_launch_count(self.h, C.byref(v)))
+        return v.value
+
+    @property
+    def scratch_bytes(self):
+        """Bytes of device scratch this context holds (partials, smoother scratch, staging)."""
+        v = C.c_int64()
+        _check(lib().hyb_ctx_scratch_bytes(self.h, C.byref(v)))
         return v.value
 
     @property
@@ -836,6 +845,10 @@ class GeometricMultigridSolver:
 
     def solve(self, A, x, b, level):
         _check(lib().hyb_gmg_solve(self.h, x.h, b.h, level))
+
+    def smooth(self, x, b, level, iterations=1):
+        """The smoother alone on one level (ChebyshevSmoother::solve / WeightedJacobiSmoother::solve)."""
+        _check(lib().hyb_gmg_smooth(self.h, x.h, b.h, level, iterations))
 
     def solve_cycles(self, x, b, level, max_cycles, rtol=0.0):
         hist = np.zeros(max_cycles + 1)

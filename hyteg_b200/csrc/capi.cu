@@ -25,6 +25,7 @@ struct hyb_ctx
       cudaFree( c.d_error );
       cudaFree( c.d_stage );
       cudaFree( c.d_sor );
+      for ( void* p : c.retired ) cudaFree( p );
       if ( c.aux ) cudaStreamSynchronize( c.aux ), cudaStreamDestroy( c.aux );
       if ( c.ev_fork ) cudaEventDestroy( c.ev_fork );
       if ( c.ev_join ) cudaEventDestroy( c.ev_join );
@@ -207,6 +208,16 @@ int hyb_ctx_synchronize( hyb_ctx* ctx )
       g_err = "a device-side bounded wait ran out (shared-memory staging did not complete)";
       return HYB_ETIMEOUT;
    }
+   HYB_CATCH
+}
+
+int hyb_ctx_scratch_bytes( const hyb_ctx* ctx, int64_t* out )
+{
+   HYB_TRY
+   require( ctx && out, "NULL argument" );
+   const Context& c = ctx->c;
+   *out = int64_t( c.partial_cap ) * 8 + c.sor_cap * 8 + c.stage_cap * 8 + c.retired_bytes + ( c.d_scalars ? 64 * 8 : 0 ) +
+          ( c.d_error ? 4 : 0 );
    HYB_CATCH
 }
 
@@ -1892,6 +1903,31 @@ int hyb_gmg_solve( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int level )
    level += g->op->o.order - 1;
    gmg_prepare( g, x, b, level );
    run_cycle( g, x, b, level );
+   HYB_CATCH
+}
+
+int hyb_gmg_smooth( hyb_gmg* g, hyb_fn* x, hyb_fn* b, int level, int iterations )
+{
+   HYB_TRY
+   require( g && x && b, "NULL argument" );
+   require( x->f.lshift == g->op->o.order - 1 && b->f.lshift == x->f.lshift, "P1 and P2 objects mixed" );
+   require( iterations >= 0, "negative iteration count" );
+   level += g->op->o.order - 1;
+   gmg_prepare( g, x, b, level );
+   require( level > g->p.min_level, "the smoother runs on the levels above the coarsest one" );
+   const int li = level - g->p.min_level;
+   g->swaps[li] = 0;
+   for ( int i = 0; i < iterations; ++i ) smooth( g, x, b, level );
+   if ( g->swaps[li] )
+   {
+      // the last Jacobi sweep wrote the partner buffer: copy back so that x keeps its storage
+      const int64_t count = x->f.mesh->level( level ).size;
+      const void*   s[1]  = { x->f.ptr( level ) };
+      const double  a[3]  = { 1, 0, 0 };
+      launch_flat_lincomb( &g->ctx->c, count, x->f.dtype, g->jt->f.ptr( level ), 1, s, a );
+      std::swap( x->f.data[level - x->f.minL], g->jt->f.data[level - g->jt->f.minL] );
+      g->swaps[li] = 0;
+   }
    HYB_CATCH
 }
 

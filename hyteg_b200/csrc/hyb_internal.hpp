@@ -14,9 +14,12 @@
 #include <cuda_fp16.h>
 
 #include <array>
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <memory>
+#include <mutex>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -100,16 +103,17 @@ struct Topology {
 };
 
 // per-level host + device tables of the P1 layout
-// tiles of the z-streamed cell sweeps, 64 x-points (two per lane) by kZHeights[t] rows: t = 0 the
-// rolled-register sweep (one row per warp), t = 1 the partial-sum sweep (two rows per warp)
-// (128-wide tiles were measured slower on the level-8 cube: register spills and fewer work units)
-constexpr int kZTileY = 8;
-constexpr int kZWidths[2]  = { 64, 64 };
-constexpr int kZHeights[2] = { 8, 16 };
-// unit x0 carries a flag: the tile's rows end within 32 points for every slice of the unit, so the
-// sweep runs it with one point per lane instead of two
-constexpr int kZUnitHalf  = 1 << 30;
-constexpr int kZUnitXMask = kZUnitHalf - 1;
+// units of the cell-interior sweep (k_cell_sweep): kSwR rows by kSwTX x-points (two per lane) over a
+// range of slices; a half-width unit (flag kSwUnitHalf on x0) has rows that all end within 32 points
+// and runs one point per lane.  Each warp of a launch owns a list of units; a launch has kSwWarps
+// warps per block and BPS = 2, 3 or 4 blocks per SM (by value type and operation), one list set per
+// BPS.
+constexpr int kSwR         = 4;
+constexpr int kSwTX        = 64;  // 32 or 64
+constexpr int kSwWarps     = 4;
+constexpr int kSwUnitHalf  = 1 << 30;
+constexpr int kSwUnitXMask = kSwUnitHalf - 1;
+constexpr int kSwLists     = 3;  // BPS 2, 3, 4
 
 struct P1Level {
    int     L = 0, n = 0;
@@ -127,17 +131,11 @@ struct P1Level {
    // y-marching work items of the cell stencil sweep: (z, x0, y_first, y_last); a warp covers
    // x0..x0+31 of slice z and marches over rows y_first..y_last
    std::vector< std::array< int, 4 > > march;
-   // z-streamed sweep: units {x0, y0, z_first, z_last} of macro-cell zcell[i], each a kZTileX x
-   // kZTileY tile of slice columns over a range of slices; block b of the sweep runs units
-   // zbegin[b]..zbegin[b+1]-1 (the units of all cells, assigned longest-first to the least loaded
-   // block)
-   std::vector< std::array< int, 4 > > zunits[2];  // per tile width kZWidths[w]
-   std::vector< int >                  zcell[2];
-   std::vector< int >                  zbegin[2];
-   // full-row sweep: units {ty, y0, z_first, z_last} (rows y0..y0+ty-1 of slices z_first..z_last),
-   // one list per band height ty = 1 << h (h = 0..3), blocks as for zunits
-   std::vector< std::array< int, 4 > > runits[4];
-   std::vector< int >                  rbegin[4];
+   // cell-interior sweep: units {x0 (| kSwUnitHalf), y0, z_first, z_last} of macro-cell swcell[b][i];
+   // warp w of a launch with b + 2 blocks per SM runs units swbegin[b][w]..swbegin[b][w+1]-1
+   std::vector< std::array< int, 4 > > swunits[kSwLists];
+   std::vector< int >                  swcell[kSwLists];
+   std::vector< int >                  swbegin[kSwLists];
    int64_t n_owned_cell = 0;
    // device copies
    int64_t*   d_off       = nullptr;  // all primitives
@@ -145,13 +143,13 @@ struct P1Level {
    int*       d_inc_begin = nullptr;
    Incidence* d_inc       = nullptr;
    int4*      d_tasks     = nullptr;
+   int4*      d_btasks    = nullptr;  // tasks grouped by boundary type (Inner, Dirichlet, Neumann, Freeslip)
+   int        bcount[4]   = {};
    int2*      d_rows      = nullptr;
    int4*      d_march     = nullptr;
-   int4*      d_zunits[2] = { nullptr, nullptr };
-   int*       d_zcell[2]  = { nullptr, nullptr };
-   int*       d_zbegin[2] = { nullptr, nullptr };
-   int4*      d_runits[4] = {};
-   int*       d_rbegin[4] = {};
+   int4*      d_swunits[kSwLists]  = {};
+   int*       d_swcell[kSwLists]   = {};
+   int*       d_swbegin[kSwLists]  = {};
    uint8_t*   d_bc        = nullptr;  // bc type per primitive (v, e, f, c order)
    int8_t*    d_bkind     = nullptr;  // 0 vertex, 1 edge, 2 face per boundary primitive
    float*     d_ncell_cls = nullptr;  // per cell, per class: number of macro-cells around the sub-primitive
@@ -265,6 +263,10 @@ struct Context {
    int64_t stage_cap = 0;
    double* d_sor     = nullptr;  // new owner values of a Gauss-Seidel colour set (one per boundary task)
    int64_t sor_cap   = 0;
+   // Buffers replaced by a larger one (partials, SOR scratch).  A CUDA graph captured earlier still
+   // holds their addresses, so they stay allocated until the context is destroyed.
+   std::vector< void* > retired;
+   int64_t              retired_bytes = 0;
    int64_t launches = 0;         // kernel launches issued through this context
 };
 
@@ -357,10 +359,42 @@ void launch_cg_scalar( Context* ctx, double* state, int stage, double rtol, doub
 
 // host helpers
 void check_cuda( cudaError_t e, const char* what );
+
+// One-time set-up per CUDA device: __constant__ tables and kernel attributes exist once per device,
+// so a process that uses several devices must run each set-up on every one of them.  run(f) calls f
+// once for the current device (thread-safe; later calls return at the cost of one atomic load).
+class PerDeviceOnce
+{
+ public:
+   template < class F >
+   void run( F&& f )
+   {
+      int dev = 0;
+      check_cuda( cudaGetDevice( &dev ), "cudaGetDevice" );
+      if ( dev < 0 || dev >= 64 ) throw std::invalid_argument( "device ordinal out of range" );
+      const uint64_t bit = uint64_t( 1 ) << dev;
+      if ( done_.load( std::memory_order_acquire ) & bit ) return;
+      std::lock_guard< std::mutex > lock( mu_ );
+      if ( done_.load( std::memory_order_relaxed ) & bit ) return;
+      f();
+      done_.fetch_or( bit, std::memory_order_release );
+   }
+   // whether the set-up has run on the current device
+   bool done_on_current_device() const
+   {
+      int dev = 0;
+      if ( cudaGetDevice( &dev ) != cudaSuccess || dev < 0 || dev >= 64 ) return false;
+      return ( done_.load( std::memory_order_acquire ) >> dev ) & 1u;
+   }
+
+ private:
+   std::atomic< uint64_t > done_{ 0 };
+   std::mutex              mu_;
+};
 void build_level( Mesh* m, int L );
 void ensure_device( Mesh* m, P1Level& P );
-void build_zunits( P1Level& P, int nblocks, int w, int ncells );
-void build_runits( P1Level& P, int nblocks, int h );
+// unit lists of the cell-interior sweep for a launch of nwarps warps (list index b)
+void build_sweep_units( P1Level& P, int b, int nwarps, int ncells );
 void build_operator_level( Operator* A, int L );
 void ensure_device_op( OpLevel& ol );
 

@@ -436,29 +436,29 @@ static void xg4_weights( double w[11] )
 
 void ensure_p2_constants()
 {
-   static bool done = false;
-   if ( done ) return;
-   double pts[11][3], w[11], g[11][10][3];
-   xg4_weights( w );
-   const double lg[4][3] = { { -1, -1, -1 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } };
-   const int    ed[6][2] = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
-   for ( int q = 0; q < 11; ++q )
-   {
-      for ( int d = 0; d < 3; ++d ) pts[q][d] = kXG4Bary[q][d + 1];
-      const double lam[4] = { 1.0 - pts[q][0] - pts[q][1] - pts[q][2], pts[q][0], pts[q][1], pts[q][2] };
-      for ( int i = 0; i < 4; ++i )
-         for ( int d = 0; d < 3; ++d ) g[q][i][d] = ( 4.0 * lam[i] - 1.0 ) * lg[i][d];
-      for ( int e = 0; e < 6; ++e )
-         for ( int d = 0; d < 3; ++d )
-            g[q][4 + e][d] = 4.0 * ( lam[ed[e][0]] * lg[ed[e][1]][d] + lam[ed[e][1]] * lg[ed[e][0]][d] );
-   }
-   check_cuda( cudaMemcpyToSymbol( c_xg4_pts, pts, sizeof( pts ) ), "P2 constants (points)" );
-   check_cuda( cudaMemcpyToSymbol( c_xg4_w, w, sizeof( w ) ), "P2 constants (weights)" );
-   check_cuda( cudaMemcpyToSymbol( c_p2_rgrad, g, sizeof( g ) ), "P2 constants (gradients)" );
-   int wrap[55];
-   p2_wrap_table( wrap );
-   check_cuda( cudaMemcpyToSymbol( c_p2_wrap, wrap, sizeof( wrap ) ), "P2 constants (stored order)" );
-   done = true;
+   static PerDeviceOnce once;
+   once.run( [] {
+      double pts[11][3], w[11], g[11][10][3];
+      xg4_weights( w );
+      const double lg[4][3] = { { -1, -1, -1 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } };
+      const int    ed[6][2] = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
+      for ( int q = 0; q < 11; ++q )
+      {
+         for ( int d = 0; d < 3; ++d ) pts[q][d] = kXG4Bary[q][d + 1];
+         const double lam[4] = { 1.0 - pts[q][0] - pts[q][1] - pts[q][2], pts[q][0], pts[q][1], pts[q][2] };
+         for ( int i = 0; i < 4; ++i )
+            for ( int d = 0; d < 3; ++d ) g[q][i][d] = ( 4.0 * lam[i] - 1.0 ) * lg[i][d];
+         for ( int e = 0; e < 6; ++e )
+            for ( int d = 0; d < 3; ++d )
+               g[q][4 + e][d] = 4.0 * ( lam[ed[e][0]] * lg[ed[e][1]][d] + lam[ed[e][1]] * lg[ed[e][0]][d] );
+      }
+      check_cuda( cudaMemcpyToSymbol( c_xg4_pts, pts, sizeof( pts ) ), "P2 constants (points)" );
+      check_cuda( cudaMemcpyToSymbol( c_xg4_w, w, sizeof( w ) ), "P2 constants (weights)" );
+      check_cuda( cudaMemcpyToSymbol( c_p2_rgrad, g, sizeof( g ) ), "P2 constants (gradients)" );
+      int wrap[55];
+      p2_wrap_table( wrap );
+      check_cuda( cudaMemcpyToSymbol( c_p2_wrap, wrap, sizeof( wrap ) ), "P2 constants (stored order)" );
+   } );
 }
 
 // mapped quantities of quadrature point q of a micro-cell: Mi = (DF J)^-1 and s = w k |det(DF J)|
@@ -1034,25 +1034,25 @@ __constant__ double c_q2_rgrad[4][10][3];
 
 void ensure_stokes_constants()
 {
-   static bool done = false;
-   if ( done ) return;
-   const double a = ( 5.0 - std::sqrt( 5.0 ) ) / 20.0, b = ( 5.0 + 3.0 * std::sqrt( 5.0 ) ) / 20.0;
-   const double pts[4][3] = { { a, a, a }, { b, a, a }, { a, b, a }, { a, a, b } };
-   const double lg[4][3]  = { { -1, -1, -1 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } };
-   const int    ed[6][2]  = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
-   double       g[4][10][3];
-   for ( int q = 0; q < 4; ++q )
-   {
-      const double lam[4] = { 1.0 - pts[q][0] - pts[q][1] - pts[q][2], pts[q][0], pts[q][1], pts[q][2] };
-      for ( int i = 0; i < 4; ++i )
-         for ( int d = 0; d < 3; ++d ) g[q][i][d] = ( 4.0 * lam[i] - 1.0 ) * lg[i][d];
-      for ( int e = 0; e < 6; ++e )
-         for ( int d = 0; d < 3; ++d )
-            g[q][4 + e][d] = 4.0 * ( lam[ed[e][0]] * lg[ed[e][1]][d] + lam[ed[e][1]] * lg[ed[e][0]][d] );
-   }
-   check_cuda( cudaMemcpyToSymbol( c_q2_pts, pts, sizeof( pts ) ), "Stokes constants (points)" );
-   check_cuda( cudaMemcpyToSymbol( c_q2_rgrad, g, sizeof( g ) ), "Stokes constants (gradients)" );
-   done = true;
+   static PerDeviceOnce once;
+   once.run( [] {
+      const double a = ( 5.0 - std::sqrt( 5.0 ) ) / 20.0, b = ( 5.0 + 3.0 * std::sqrt( 5.0 ) ) / 20.0;
+      const double pts[4][3] = { { a, a, a }, { b, a, a }, { a, b, a }, { a, a, b } };
+      const double lg[4][3]  = { { -1, -1, -1 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } };
+      const int    ed[6][2]  = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
+      double       g[4][10][3];
+      for ( int q = 0; q < 4; ++q )
+      {
+         const double lam[4] = { 1.0 - pts[q][0] - pts[q][1] - pts[q][2], pts[q][0], pts[q][1], pts[q][2] };
+         for ( int i = 0; i < 4; ++i )
+            for ( int d = 0; d < 3; ++d ) g[q][i][d] = ( 4.0 * lam[i] - 1.0 ) * lg[i][d];
+         for ( int e = 0; e < 6; ++e )
+            for ( int d = 0; d < 3; ++d )
+               g[q][4 + e][d] = 4.0 * ( lam[ed[e][0]] * lg[ed[e][1]][d] + lam[ed[e][1]] * lg[ed[e][0]][d] );
+      }
+      check_cuda( cudaMemcpyToSymbol( c_q2_pts, pts, sizeof( pts ) ), "Stokes constants (points)" );
+      check_cuda( cudaMemcpyToSymbol( c_q2_rgrad, g, sizeof( g ) ), "Stokes constants (gradients)" );
+   } );
 }
 
 // inverse of the blended Jacobian M = DF J at reference point xi and |det M|
@@ -1231,30 +1231,30 @@ static A* acc_buffer( Operator* op, int L, int64_t size )
 // stencil direction of every vertex pair of every micro-cell type (vertex offsets as c_mc_off)
 static void ensure_var_tables()
 {
-   static bool done = false;
-   if ( done ) return;
-   static const int off[6][4][3] = {
-       { { 0, 0, 0 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } }, { { 1, 0, 0 }, { 1, 1, 0 }, { 0, 1, 0 }, { 1, 0, 1 } },
-       { { 1, 0, 0 }, { 0, 1, 0 }, { 1, 0, 1 }, { 0, 0, 1 } }, { { 1, 1, 0 }, { 1, 1, 1 }, { 0, 1, 1 }, { 1, 0, 1 } },
-       { { 1, 0, 1 }, { 0, 1, 1 }, { 0, 0, 1 }, { 0, 1, 0 } }, { { 0, 1, 0 }, { 1, 1, 0 }, { 1, 0, 1 }, { 0, 1, 1 } } };
-   int8_t dir[6][4][4], vd[15][3];
-   for ( int d = 0; d < 15; ++d )
-      for ( int k = 0; k < 3; ++k ) vd[d][k] = int8_t( kVarDirs[d][k] );
-   for ( int t = 0; t < 6; ++t )
-      for ( int i = 0; i < 4; ++i )
-         for ( int j = 0; j < 4; ++j )
-         {
-            int found = -1;
-            for ( int d = 0; d < 15; ++d )
-               if ( off[t][j][0] - off[t][i][0] == kVarDirs[d][0] && off[t][j][1] - off[t][i][1] == kVarDirs[d][1] &&
-                    off[t][j][2] - off[t][i][2] == kVarDirs[d][2] )
-                  found = d;
-            if ( found < 0 ) throw std::runtime_error( "micro-cell edge outside the 15-point stencil" );
-            dir[t][i][j] = int8_t( found );
-         }
-   check_cuda( cudaMemcpyToSymbol( c_mc_dir, dir, sizeof( dir ) ), "upload stencil directions" );
-   check_cuda( cudaMemcpyToSymbol( c_var_dir, vd, sizeof( vd ) ), "upload stencil directions" );
-   done = true;
+   static PerDeviceOnce once;
+   once.run( [] {
+      static const int off[6][4][3] = {
+          { { 0, 0, 0 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } }, { { 1, 0, 0 }, { 1, 1, 0 }, { 0, 1, 0 }, { 1, 0, 1 } },
+          { { 1, 0, 0 }, { 0, 1, 0 }, { 1, 0, 1 }, { 0, 0, 1 } }, { { 1, 1, 0 }, { 1, 1, 1 }, { 0, 1, 1 }, { 1, 0, 1 } },
+          { { 1, 0, 1 }, { 0, 1, 1 }, { 0, 0, 1 }, { 0, 1, 0 } }, { { 0, 1, 0 }, { 1, 1, 0 }, { 1, 0, 1 }, { 0, 1, 1 } } };
+      int8_t dir[6][4][4], vd[15][3];
+      for ( int d = 0; d < 15; ++d )
+         for ( int k = 0; k < 3; ++k ) vd[d][k] = int8_t( kVarDirs[d][k] );
+      for ( int t = 0; t < 6; ++t )
+         for ( int i = 0; i < 4; ++i )
+            for ( int j = 0; j < 4; ++j )
+            {
+               int found = -1;
+               for ( int d = 0; d < 15; ++d )
+                  if ( off[t][j][0] - off[t][i][0] == kVarDirs[d][0] && off[t][j][1] - off[t][i][1] == kVarDirs[d][1] &&
+                       off[t][j][2] - off[t][i][2] == kVarDirs[d][2] )
+                     found = d;
+               if ( found < 0 ) throw std::runtime_error( "micro-cell edge outside the 15-point stencil" );
+               dir[t][i][j] = int8_t( found );
+            }
+      check_cuda( cudaMemcpyToSymbol( c_mc_dir, dir, sizeof( dir ) ), "upload stencil directions" );
+      check_cuda( cudaMemcpyToSymbol( c_var_dir, vd, sizeof( vd ) ), "upload stencil directions" );
+   } );
 }
 
 template < typename A >
@@ -1609,27 +1609,27 @@ __constant__ double c_yu5_rgrad[5][10][3];
 
 static void ensure_visc_constants()
 {
-   static bool done = false;
-   if ( done ) return;
-   const double lg[4][3] = { { -1, -1, -1 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } };
-   const int    ed[6][2] = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
-   const double pts[5][3] = { { 0.25, 0.25, 0.25 },
-                              { 1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0 },
-                              { 0.5, 1.0 / 6.0, 1.0 / 6.0 },
-                              { 1.0 / 6.0, 0.5, 1.0 / 6.0 },
-                              { 1.0 / 6.0, 1.0 / 6.0, 0.5 } };
-   double g[5][10][3];
-   for ( int q = 0; q < 5; ++q )
-   {
-      const double lam[4] = { 1.0 - pts[q][0] - pts[q][1] - pts[q][2], pts[q][0], pts[q][1], pts[q][2] };
-      for ( int i = 0; i < 4; ++i )
-         for ( int d = 0; d < 3; ++d ) g[q][i][d] = ( 4.0 * lam[i] - 1.0 ) * lg[i][d];
-      for ( int e = 0; e < 6; ++e )
-         for ( int d = 0; d < 3; ++d )
-            g[q][4 + e][d] = 4.0 * ( lam[ed[e][0]] * lg[ed[e][1]][d] + lam[ed[e][1]] * lg[ed[e][0]][d] );
-   }
-   check_cuda( cudaMemcpyToSymbol( c_yu5_rgrad, g, sizeof( g ) ), "viscous block constants" );
-   done = true;
+   static PerDeviceOnce once;
+   once.run( [] {
+      const double lg[4][3] = { { -1, -1, -1 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } };
+      const int    ed[6][2] = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
+      const double pts[5][3] = { { 0.25, 0.25, 0.25 },
+                                 { 1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0 },
+                                 { 0.5, 1.0 / 6.0, 1.0 / 6.0 },
+                                 { 1.0 / 6.0, 0.5, 1.0 / 6.0 },
+                                 { 1.0 / 6.0, 1.0 / 6.0, 0.5 } };
+      double g[5][10][3];
+      for ( int q = 0; q < 5; ++q )
+      {
+         const double lam[4] = { 1.0 - pts[q][0] - pts[q][1] - pts[q][2], pts[q][0], pts[q][1], pts[q][2] };
+         for ( int i = 0; i < 4; ++i )
+            for ( int d = 0; d < 3; ++d ) g[q][i][d] = ( 4.0 * lam[i] - 1.0 ) * lg[i][d];
+         for ( int e = 0; e < 6; ++e )
+            for ( int d = 0; d < 3; ++d )
+               g[q][4 + e][d] = 4.0 * ( lam[ed[e][0]] * lg[ed[e][1]][d] + lam[ed[e][1]] * lg[ed[e][0]][d] );
+      }
+      check_cuda( cudaMemcpyToSymbol( c_yu5_rgrad, g, sizeof( g ) ), "viscous block constants" );
+   } );
 }
 
 template < typename T, typename A, int MODE >

@@ -14,6 +14,7 @@
 // accumulation for fp32/fp16 storage.
 #include "hyb_internal.hpp"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
@@ -27,22 +28,28 @@ __constant__ int      c_dirs[kNumDirs][3];
 __constant__ uint16_t c_cls_mask[kNumClasses];
 __constant__ int8_t   c_mask_to_cls[16];
 
-static bool g_const_ready = false;
-static void zstream_attributes_all();
-// constant tables and kernel attributes; called before any stream capture (prepare_device)
+static void    sweep_attributes_all();
+static double* noalloc_scratch( int device );
+static PerDeviceOnce g_const_once;
+// constant tables and kernel attributes of this file, once per device; called before any stream
+// capture (prepare_device).  It also resolves the device address of the allocation-free dot's fixed
+// scratch, so that entry point itself never has to load anything.
 static void ensure_constants()
 {
-   if ( g_const_ready ) return;
-   zstream_attributes_all();
-   check_cuda( cudaMemcpyToSymbol( c_dirs, kDirs, sizeof( kDirs ) ), "constants(dirs)" );
-   check_cuda( cudaMemcpyToSymbol( c_cls_mask, kClassDirMask, sizeof( kClassDirMask ) ), "constants(mask)" );
-   int8_t m2c[16];
-   for ( int m = 0; m < 16; ++m ) m2c[m] = -1;
-   // z==0 -> bit0, y==0 -> bit1, x==0 -> bit2, x+y+z==n -> bit3
-   const int faces[kNumClasses] = { 0, 1, 2, 4, 8, 3, 5, 9, 6, 10, 12, 7, 11, 13, 14 };
-   for ( int c = 0; c < kNumClasses; ++c ) m2c[faces[c]] = int8_t( c );
-   check_cuda( cudaMemcpyToSymbol( c_mask_to_cls, m2c, sizeof( m2c ) ), "constants(classes)" );
-   g_const_ready = true;
+   g_const_once.run( [] {
+      int dev = 0;
+      check_cuda( cudaGetDevice( &dev ), "cudaGetDevice" );
+      noalloc_scratch( dev );
+      sweep_attributes_all();
+      check_cuda( cudaMemcpyToSymbol( c_dirs, kDirs, sizeof( kDirs ) ), "constants(dirs)" );
+      check_cuda( cudaMemcpyToSymbol( c_cls_mask, kClassDirMask, sizeof( kClassDirMask ) ), "constants(mask)" );
+      int8_t m2c[16];
+      for ( int m = 0; m < 16; ++m ) m2c[m] = -1;
+      // z==0 -> bit0, y==0 -> bit1, x==0 -> bit2, x+y+z==n -> bit3
+      const int faces[kNumClasses] = { 0, 1, 2, 4, 8, 3, 5, 9, 6, 10, 12, 7, 11, 13, 14 };
+      for ( int c = 0; c < kNumClasses; ++c ) m2c[faces[c]] = int8_t( c );
+      check_cuda( cudaMemcpyToSymbol( c_mask_to_cls, m2c, sizeof( m2c ) ), "constants(classes)" );
+   } );
 }
 
 // Cell-interior and boundary-primitive kernels of one operation write disjoint slots, so the
@@ -102,6 +109,8 @@ struct LevelView
    const int2*      rows;
    int              ntasks;
    const int4*      tasks;
+   const int4*      btasks;      // the same tasks grouped by their primitive's boundary type
+   int              bcount[4];   // tasks per group: Inner, Dirichlet, Neumann, Freeslip
    const int64_t*   off;       // all primitives
    const int64_t*   cell_off;  // off + nB
    const int*       inc_begin;
@@ -112,13 +121,10 @@ struct LevelView
    const float*     ncell_cls;
    int              nmarch;
    const int4*      march;
-   int              nrblocks[4];  // full-row sweep blocks per band height 1 << h
-   const int4*      runits[4];
-   const int*       rbegin[4];
-   int              nzblocks[2];  // per tile width kZWidths[w]
-   const int4*      zunits[2];
-   const int*       zcell[2];
-   const int*       zbegin[2];
+   int              nswarps[kSwLists];  // warps of a cell-sweep launch with 2, 3, 4 blocks per SM
+   const int4*      swunits[kSwLists];
+   const int*       swcell[kSwLists];
+   const int*       swbegin[kSwLists];
 };
 
 template < typename A >
@@ -139,6 +145,8 @@ static LevelView make_view( Mesh* m, int L )
    v.rows      = P.d_rows;
    v.ntasks    = int( P.tasks.size() );
    v.tasks     = P.d_tasks;
+   v.btasks    = P.d_btasks;
+   for ( int g = 0; g < 4; ++g ) v.bcount[g] = P.bcount[g];
    v.off       = P.d_off;
    v.cell_off  = P.d_off + P.nB;
    v.inc_begin = P.d_inc_begin;
@@ -149,20 +157,40 @@ static LevelView make_view( Mesh* m, int L )
    v.ncell_cls = P.d_ncell_cls;
    v.nmarch     = int( P.march.size() );
    v.march      = P.d_march;
-   for ( int h = 0; h < 4; ++h )
+   for ( int b = 0; b < kSwLists; ++b )
    {
-      v.nrblocks[h] = int( P.rbegin[h].size() ) - 1;
-      v.runits[h]   = P.d_runits[h];
-      v.rbegin[h]   = P.d_rbegin[h];
-   }
-   for ( int wi = 0; wi < 2; ++wi )
-   {
-      v.nzblocks[wi] = int( P.zbegin[wi].size() ) - 1;
-      v.zunits[wi]   = P.d_zunits[wi];
-      v.zcell[wi]    = P.d_zcell[wi];
-      v.zbegin[wi]   = P.d_zbegin[wi];
+      v.nswarps[b] = int( P.swbegin[b].size() ) - 1;
+      v.swunits[b] = P.d_swunits[b];
+      v.swcell[b]  = P.d_swcell[b];
+      v.swbegin[b] = P.d_swbegin[b];
    }
    return v;
+}
+
+// The contiguous groups of the type-sorted task list a boundary launch covers: every group when
+// unflagged owners are copied, else the groups whose boundary type is in `flag`.
+struct TaskSegments
+{
+   int start[4];
+   int count[4];
+};
+
+static TaskSegments task_segments( const LevelView& v, uint32_t flag, int all )
+{
+   static const uint32_t type_bit[4] = { kInner, kDirichlet, kNeumann, kFreeslip };
+   TaskSegments          s{};
+   int                   k = 0, at = 0;
+   for ( int g = 0; g < 4; ++g )
+   {
+      if ( v.bcount[g] > 0 && ( all || ( flag & type_bit[g] ) ) )
+      {
+         s.start[k] = at;
+         s.count[k] = v.bcount[g];
+         ++k;
+      }
+      at += v.bcount[g];
+   }
+   return s;
 }
 
 __device__ __forceinline__ int64_t owner_slot( const LevelView& v, int b, int i, int j )
@@ -226,49 +254,6 @@ __device__ __forceinline__ void stencil_epilogue( int64_t i, A s, A invd, const 
    else if constexpr ( OP == OP_DINV_APPLY ) stv( dst + i, invd * s );
 }
 
-template < typename T, typename A, int OP >
-__global__ void __launch_bounds__( 256 ) k_cell_stencil( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
-                                                          const T* __restrict__ v1, T* v2, T* dst, A a0, A a1 )
-{
-   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-   const int r    = blockIdx.x * 8 + warp;
-   const int c    = blockIdx.y;
-   if ( r >= v.nrows ) return;
-   if ( !( v.cell_bc[c] & flag ) ) return;
-   const int2    yz   = v.rows[r];
-   const int     y = yz.x, z = yz.y, n = v.n;
-   const int64_t base = v.cell_off[c];
-   const T*      s    = src + base;
-   const int64_t r00 = cidx( n, 0, y, z ), rm0 = cidx( n, 0, y - 1, z ), rp0 = cidx( n, 0, y + 1, z );
-   const int64_t r0m = cidx( n, 0, y, z - 1 ), r0p = cidx( n, 0, y, z + 1 );
-   const int64_t rmp = cidx( n, 0, y - 1, z + 1 ), rpm = cidx( n, 0, y + 1, z - 1 );
-   const A*      W   = o.W + size_t( c ) * kNumClasses * kNumDirs;  // interior class 0
-   const A w0 = W[0], wW = W[1], wE = W[2], wS = W[3], wN = W[4], wB = W[5], wT = W[6], wNW = W[7], wSE = W[8], wTW = W[9],
-           wBE = W[10], wTS = W[11], wBN = W[12], wTSE = W[13], wBNW = W[14];
-   const A   invd = o.invd_c[c];
-   const int xmax = n - 1 - y - z;
-   for ( int x = 1 + lane; x <= xmax; x += 32 )
-   {
-      A acc = w0 * A( ldv( s + r00 + x ) );
-      acc += wW * A( ldv( s + r00 + x - 1 ) );
-      acc += wE * A( ldv( s + r00 + x + 1 ) );
-      acc += wS * A( ldv( s + rm0 + x ) );
-      acc += wN * A( ldv( s + rp0 + x ) );
-      acc += wB * A( ldv( s + r0m + x ) );
-      acc += wT * A( ldv( s + r0p + x ) );
-      acc += wNW * A( ldv( s + rp0 + x - 1 ) );
-      acc += wSE * A( ldv( s + rm0 + x + 1 ) );
-      acc += wTW * A( ldv( s + r0p + x - 1 ) );
-      acc += wBE * A( ldv( s + r0m + x + 1 ) );
-      acc += wTS * A( ldv( s + rmp + x ) );
-      acc += wBN * A( ldv( s + rpm + x ) );
-      acc += wTSE * A( ldv( s + rmp + x + 1 ) );
-      acc += wBNW * A( ldv( s + rpm + x - 1 ) );
-      stencil_epilogue< T, A, OP >( base + r00 + x, acc, invd, src, v1, v2, dst, a0, a1 );
-   }
-}
-
-
 // y-marching cell sweep: a warp owns x0..x0+31 of slice z and walks the rows y_first..y_last.  The
 // rows (y-1, y, y+1) of slice z, (y-1, y) of slice z+1 and (y, y+1) of slice z-1 roll through
 // registers, so each step loads three new rows (x-1, x, x+1 per lane; neighbours hit L1) instead
@@ -295,7 +280,7 @@ __device__ __forceinline__ void prefetch_l2( const void* p ) { asm volatile( "pr
 
 template < typename T, typename A, int OP >
 __global__ void __launch_bounds__( 256 ) k_cell_march( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
-                                                        const T* __restrict__ v1, T* v2, T* dst, A a0, A a1, int prefetch_distance )
+                                                        const T* __restrict__ v1, T* v2, T* dst, A a0, A a1 )
 {
    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
    const int item = blockIdx.x * 8 + warp;
@@ -314,7 +299,7 @@ __global__ void __launch_bounds__( 256 ) k_cell_march( LevelView v, OpView< A > 
    Row3< T, A > c0 = load_row< T, A >( s, n, ya, z, x );
    Row3< T, A > tm = load_row< T, A >( s, n, ya - 1, z + 1, x );
    Row3< T, A > b0 = load_row< T, A >( s, n, ya, z - 1, x );
-   const int pd = prefetch_distance;
+   constexpr int pd = 8;  // rows pulled into L2 ahead of the march
 #pragma unroll 2
    for ( int y = ya; y <= yb; ++y )
    {
@@ -356,29 +341,6 @@ __global__ void __launch_bounds__( 256 ) k_cell_march( LevelView v, OpView< A > 
 }
 
 
-// ---------------------------------------------------------------------------------------------
-// Rolled-register z-streamed cell sweep (cp.async.bulk + mbarrier ring; HYB_CELL_KERNEL=zstream).
-//
-// A unit is the tile x0..x0+63, y0..y0+7 of slices z_first..z_last of one macro-cell.  A producer
-// warp streams the tile's rows of every slice, with a one-point halo in x and y, into a ring of
-// shared-memory stages: lane r issues one bulk copy for row y0-1+r (10 rows per stage), and the
-// stage's full barrier completes when all bytes have landed.  Eight consumer warps (one per tile
-// row, two x per lane) march up the slices.  Each slice load costs the producer a fixed few hundred
-// cycles of issue and barrier hand-off whatever its size, so tiles are as wide as the consumers'
-// registers allow and row offsets advance by additions instead of being recomputed.  Of the 15 stencil values, four in slice z-1 and four
-// in slice z were read in the previous step and roll through registers, so a step reads three
-// values of slice z and four of slice z+1 from shared memory, and slice z is released (empty
-// barrier, one arrival per consumer warp) as soon as step z ends.  With S stages, S-2 slices are
-// in flight per block, independent of registers.
-//
-// Global rows start at arbitrary element offsets, while a bulk copy needs 16-byte aligned source,
-// destination and size: each row copy is widened to 16-byte boundaries and its shift (0..al-1
-// elements) is published with the stage as 3-bit fields of one word.
-//
-// Every wait is bounded by the global timer.  When one runs out the block records an error in
-// *err, raises a block-wide abort flag, stops issuing copies, waits (bounded) for the copies it
-// has in flight and returns.
-// ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smem_addr( const void* p ) { return uint32_t( __cvta_generic_to_shared( p ) ); }
 
 __device__ __forceinline__ void mbar_init( uint64_t* bar, uint32_t count )
@@ -441,123 +403,17 @@ __device__ __forceinline__ bool mbar_wait_bounded( uint64_t* bar, uint32_t parit
 // Chebyshev step, the running update for the later ones, dst itself for apply-add) stage that
 // vector's tile rows (no halo) in the same stage, so no step waits on a global load.
 template < int OP >
-__host__ __device__ constexpr bool zstream_aux()
+__host__ __device__ constexpr bool sweep_aux()
 {
    return OP == OP_APPLY_ADD || OP == OP_RESID || OP == OP_JAC || OP == OP_CHEB0 || OP == OP_CHEBI || OP == OP_CHEBL;
 }
 
-template < typename T, bool AUX >
-struct ZCfg
-{
-   static constexpr int wi      = 0;                                            // tile table index
-   static constexpr int kZTileX = kZWidths[wi];                                 // x-points per tile row
-   static constexpr int pts     = kZTileX / 32;                                 // x-points per consumer lane
-   static constexpr int al    = 16 / int( sizeof( T ) );                         // elements per 16 bytes
-   static constexpr int RW    = ( kZTileX + 2 + 2 * al + al - 1 ) / al * al;    // source row width (elements)
-   static constexpr int RWA   = ( kZTileX + 2 * al + al - 1 ) / al * al;        // second-vector row width
-   static constexpr int rows  = kZTileY + 2;                                   // tile rows + halo
-   static constexpr int aux0  = rows * RW;                                     // second-vector rows start here
-   static constexpr int stage = aux0 + ( AUX ? kZTileY * RWA : 0 );            // elements per stage
-   static constexpr int S     = AUX ? 8 : 10;                                   // ring depth
-   static constexpr size_t smem_bytes = size_t( S ) * stage * sizeof( T );
-};
-constexpr int kZWarps     = kZTileY;
-// Two producer warps (load l is issued by producer l % 2): one warp's issue and hand-off chain per
-// slice load is what limits a single-producer ring (measured on B200: 0.163 -> 0.136 ms for the
-// level-8 cube apply in FP64, 0.154 -> 0.108 ms in FP32).
-constexpr int kZProducers = 2;
-constexpr int kZThreads   = ( kZWarps + kZProducers ) * 32;  // consumer warps + producer warps
-
 // offset of slice z+1 minus offset of slice z in a macro-cell array (tri(n+1-z) points in slice z)
 __device__ __forceinline__ int64_t slice_step( int n, int z ) { return int64_t( n + 1 - z ) * ( n + 2 - z ) / 2; }
 
-// producer warp: streams the rows of every slice of the block's units into the ring.  Lane r < 10
-// copies source row y0-1+r; with AUX, lane 10+r copies row y0+r of the second vector (slices
-// z_first..z_last only, rows with interior points only).  Row offsets advance by additions from
-// slice to slice: cidx(0, y, z+1) = cidx(0, y, z) + tri(n+1-z) - y.
-template < typename T, bool AUX >
-__device__ __forceinline__ void zstream_produce( const LevelView& v, uint32_t flag, const T* __restrict__ src,
-                                                 const T* __restrict__ aux, int nC, T* ring, uint64_t* full, uint64_t* empty,
-                                                 uint32_t* shw, volatile int* abort_flag, int* err )
-{
-   using Cfg = ZCfg< T, AUX >;
-   constexpr int S = Cfg::S, AL = Cfg::al, kZTileX = Cfg::kZTileX;
-   static_assert( S % kZProducers == 0, "every stage must belong to one producer warp" );
-   const int     lane = threadIdx.x & 31, n = v.n, me = ( threadIdx.x >> 5 ) - kZWarps;
-   const int*    zb = v.zbegin[Cfg::wi];
-   const int4*   zu = v.zunits[Cfg::wi];
-   const int*    zcl = v.zcell[Cfg::wi];
-   const int     u0 = zb[blockIdx.x], u1 = zb[blockIdx.x + 1];
-   const bool    is_src = lane < Cfg::rows, is_aux = AUX && lane >= Cfg::rows && lane < Cfg::rows + kZTileY;
-   const int     dsto   = is_src ? lane * Cfg::RW : Cfg::aux0 + ( lane - Cfg::rows ) * Cfg::RWA;
-   const T*      gbase  = is_src ? src : aux;
-   const int     shbit  = is_src ? 3 * lane : ( is_aux ? 3 * ( lane - Cfg::rows ) : 0 );
-   int           ld = 0;  // sequence number of the next slice load
-   bool          ok = true;
-   {
-      for ( int u = u0; u < u1 && ok; ++u )
-      {
-         const int c = zcl[u];
-         if ( c >= nC || !( v.cell_bc[c] & flag ) ) continue;
-         const int64_t cb = v.cell_off[c];
-         const int4 U  = zu[u];  // x0 (| half-width flag), y0, z_first, z_last
-         const int  ux = U.x & kZUnitXMask, tw = ( U.x & kZUnitHalf ) ? kZTileX / 2 : kZTileX;
-         const int  yy = is_src ? U.y - 1 + lane : U.y + ( lane - Cfg::rows );
-         const int  xa = is_src ? ux - 1 : ux;  // first x of the row segment
-         int64_t    rb = cidx( n, 0, yy, U.z - 1 );
-         for ( int zz = U.z - 1; zz <= U.w + 1; rb += slice_step( n, zz ) - yy, ++zz, ++ld )
-         {
-            if ( ld % kZProducers != me ) continue;
-            const int st = ld % S;
-            if ( ld >= S && !mbar_wait_bounded( &empty[st], uint32_t( ( ld / S - 1 ) & 1 ), abort_flag ) )
-            {
-               ok = false;
-               break;
-            }
-            uint32_t bytes = 0, sh = 0;
-            int64_t  a0    = 0;
-            // last x of the segment: the halo point (source) or the last interior point (second vector)
-            const int  xe   = is_src ? min( ux + tw, n - yy - zz ) : min( ux + tw - 1, n - 1 - yy - zz );
-            const bool live = ( is_src && yy + zz <= n && xe >= xa ) || ( is_aux && zz >= U.z && zz <= U.w && xe >= xa );
-            if ( live )
-            {
-               const int64_t s0 = rb + xa;
-               const int64_t e1 = rb + xe + 1;  // one past the segment
-               sh               = uint32_t( s0 & ( AL - 1 ) );
-               a0               = s0 - sh;
-               bytes            = uint32_t( ( ( e1 + AL - 1 ) / AL * AL - a0 ) * int64_t( sizeof( T ) ) );
-            }
-            const uint32_t total = __reduce_add_sync( 0xffffffffu, bytes );
-            const uint32_t w0    = __reduce_or_sync( 0xffffffffu, is_src ? sh << shbit : 0u );
-            const uint32_t w1    = AUX ? __reduce_or_sync( 0xffffffffu, is_aux ? sh << shbit : 0u ) : 0u;
-            if ( lane == 0 )
-            {
-               shw[2 * st]     = w0;
-               shw[2 * st + 1] = w1;
-               mbar_expect_tx( &full[st], total );
-            }
-            __syncwarp();
-            if ( bytes ) bulk_copy_g2s( ring + st * Cfg::stage + dsto, gbase + cb + a0, bytes, &full[st] );
-         }
-      }
-   }
-   if ( !ok && lane == 0 )
-   {
-      atomicExch( err, 1 );
-      *abort_flag = 1;
-   }
-   // drain: the latest load issued on every stage has landed before the block may exit
-   if ( lane == 0 )
-      for ( int s = me; s < S && s < ld; s += kZProducers )
-      {
-         const int j = s + ( ( ld - 1 - s ) / S ) * S;
-         if ( !mbar_wait_bounded( &full[s], uint32_t( ( j / S ) & 1 ), nullptr ) ) atomicExch( err, 1 );
-      }
-}
-
 // epilogue of the z-streamed sweep: the centre of src and the second vector come from the stage
 template < typename T, typename A, int OP >
-__device__ __forceinline__ void zstream_epilogue( int64_t i, A s, A invd, A centre, A aux, T* v2, T* dst, A a0, A a1 )
+__device__ __forceinline__ void sweep_epilogue( int64_t i, A s, A invd, A centre, A aux, T* v2, T* dst, A a0, A a1 )
 {
    if constexpr ( OP == OP_APPLY ) stv( dst + i, s );
    else if constexpr ( OP == OP_APPLY_ADD ) stv( dst + i, aux + s );
@@ -573,739 +429,375 @@ __device__ __forceinline__ void zstream_epilogue( int64_t i, A s, A invd, A cent
    else if constexpr ( OP == OP_DINV_APPLY ) stv( dst + i, invd * s );
 }
 
-// the eight values of one point that roll over from one slice step to the next
-template < typename A >
-struct ZPoint
+// ---------------------------------------------------------------------------------------------
+// Cell-interior sweep for levels with n >= 32 (every stencil operation, every value type).
+//
+// Work unit: the rows y0..y0+kSwR-1 and the x-points x0..x0+63 (x0..x0+31 for a half-width unit)
+// of the slices z_first..z_last of one macro-cell, interior points only (x, y, z >= 1,
+// x + y + z <= n - 1).  Every warp of a launch owns a fixed list of units (balanced on the host)
+// and runs them on its own: it streams the rows y0-1..y0+kSwR of the slices z_first-1..z_last+1,
+// with one point of halo in x, into a private ring of kSwD shared-memory stages with
+// cp.async.bulk (one copy per row, issued by one lane each, completing on the stage's mbarrier),
+// keeping kSwD-1 slice loads in flight while it computes one.  Loads run ahead across unit
+// boundaries.  The second vector of an epilogue (b of residual / Jacobi / Chebyshev, the running
+// update of later Chebyshev steps, dst for apply-add) is staged in the same stage, rows y0..y0+kSwR-1
+// without halo.
+//
+// Partial sums in y and z: lane l owns the points x = x0 + l + 32k (k < 2) of the unit's rows.  The
+// values (x-1, x, x+1) of row y of slice s are read from the stage once and give every stencil term
+// that involves them: the bottom terms (B, BE, BN, BNW) of slice s+1 in rows y and y-1, the middle
+// terms (W, C, E, S, SE, N, NW) of slice s in rows y-1, y and y+1, and the top terms (T, TW, TS,
+// TSE) of slice s-1 in rows y and y+1.  A point of slice s-1 is complete once rows y-1 and y of
+// slice s are folded in and is written right away.  A slice step therefore reads three values per
+// point plus four per column for the two halo rows, and issues exactly 15 multiply-adds per point.
+// The running sums of slices s-1, s and s+1 occupy three register slots that rotate; the slice loop
+// is unrolled by three so the rotation costs no moves.  The centre value and the second-vector value
+// of a point are read in the step of its own slice and carried to the next step.
+//
+// Each point sums its 15 terms in one fixed order (bottom terms, middle terms, top terms, each in
+// row order), whatever unit computes it, so results are deterministic.  Waits on the stages are
+// bounded by the global timer; a warp whose wait runs out records an error in *err, waits (bounded)
+// for its copies in flight and returns.
+// ---------------------------------------------------------------------------------------------
+template < typename T, int OP >
+struct SwCfg
 {
-   A B, BE, BN, BNW;  // slice z-1: (x,y), (x+1,y), (x,y+1), (x-1,y+1)
-   A C, W, S, SE;     // slice z:   (x,y), (x-1,y), (x,y-1), (x+1,y-1)
+   static constexpr bool   AUX   = sweep_aux< OP >();
+   static constexpr bool   CEN   = OP == OP_JAC || OP == OP_CHEBI || OP == OP_CHEBL;  // epilogue reads the centre value
+   // blocks per SM, by the register budget of the running sums (and of the centre and second-vector
+   // values the smoother epilogues carry)
+   static constexpr int    BPS   = sizeof( T ) == 8 ? ( ( CEN || AUX ) ? 2 : 3 ) : ( AUX ? 3 : 4 );
+   static constexpr int    al    = 16 / int( sizeof( T ) );                             // elements per 16 bytes
+   static constexpr int    RW    = ( kSwTX + 2 + 2 * al + al - 1 ) / al * al;          // source row (elements)
+   static constexpr int    RWA   = ( kSwTX + 2 * al + al - 1 ) / al * al;              // second-vector row
+   static constexpr int    rows  = kSwR + 2;                                           // tile rows + halo
+   static constexpr int    aux0  = rows * RW;                                          // second-vector rows start here
+   static constexpr int    stage = aux0 + ( AUX ? kSwR * RWA : 0 );                    // elements per stage
+   static constexpr int    Draw  = int( ( 216 * 1024 ) / ( BPS * kSwWarps ) / ( stage * int( sizeof( T ) ) ) );
+   static constexpr int    D     = Draw < 3 ? 3 : ( Draw > 8 ? 8 : Draw );             // ring depth
+   static constexpr size_t warp_elems = size_t( D ) * stage;
+   static constexpr size_t smem_bytes = kSwWarps * warp_elems * sizeof( T );
+   static_assert( ( stage * sizeof( T ) ) % 16 == 0 && ( RW * sizeof( T ) ) % 16 == 0 && ( RWA * sizeof( T ) ) % 16 == 0,
+                  "bulk copies need 16-byte aligned stage rows" );
+   static_assert( kSwR + 2 + ( AUX ? kSwR : 0 ) <= 32, "one row copy per lane" );
+   static_assert( kSwR == 4, "the row prefetch of k_cell_sweep is written out for six stage rows" );
 };
 
 template < typename T, typename A, int OP >
-__global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
-                                                                  const T* __restrict__ v1, T* v2, T* dst, A a0, A a1, int nC,
-                                                                  int* err )
+__global__ void __launch_bounds__( kSwWarps * 32, SwCfg< T, OP >::BPS )
+    k_cell_sweep( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src, const T* __restrict__ v1, T* v2, T* dst, A a0,
+                  A a1, int nC, int* err )
 {
-   constexpr bool AUX = zstream_aux< OP >();
-   using Cfg          = ZCfg< T, AUX >;
-   constexpr int S = Cfg::S, RW = Cfg::RW;
-   extern __shared__ __align__( 128 ) unsigned char zs_raw[];
-   T*                  ring = reinterpret_cast< T* >( zs_raw );
-   __shared__ uint64_t full[S], empty[S];
-   __shared__ uint32_t shw[2 * S];
-   __shared__ A        wsm[kZWarps][16];  // per consumer warp: the cell's 15 weights and 1/diagonal
-   __shared__ int      abort_flag;
+   using Cfg                = SwCfg< T, OP >;
+   constexpr bool AUX       = Cfg::AUX;
+   constexpr bool CEN       = Cfg::CEN;
+   constexpr int  D = Cfg::D, RW = Cfg::RW, RWA = Cfg::RWA, AL = Cfg::al, R = kSwR;
+   extern __shared__ __align__( 128 ) unsigned char sw_raw[];
+   __shared__ uint64_t bars[kSwWarps][D];
    const int           warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n = v.n;
-   if ( threadIdx.x == 0 )
+   T* const            ring = reinterpret_cast< T* >( sw_raw ) + size_t( warp ) * Cfg::warp_elems;
+   uint64_t* const     full = bars[warp];
+   if ( lane == 0 )
    {
-      for ( int s = 0; s < S; ++s )
-      {
-         mbar_init( &full[s], 1 );
-         mbar_init( &empty[s], kZWarps );
-      }
-      abort_flag = 0;
+      for ( int s = 0; s < D; ++s ) mbar_init( &full[s], 1 );
       asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
    }
-   __syncthreads();
-   volatile int* abrt = &abort_flag;
-   if ( warp >= kZWarps )
-   {
-      const T* aux = ( OP == OP_CHEBI || OP == OP_CHEBL ) ? v2 : ( OP == OP_APPLY_ADD ? dst : v1 );
-      zstream_produce< T, AUX >( v, flag, src, aux, nC, ring, full, empty, shw, abrt, err );
-      return;
-   }
-
-   // consumer warp `warp` owns tile row y0 + warp; stage row r holds global row y0 - 1 + r; lane
-   // owns x = x0 + lane + 32 k, k < kZPts
-   constexpr int kZPts = Cfg::pts;
-   const int*    zb    = v.zbegin[Cfg::wi];
-   const int4*   zu    = v.zunits[Cfg::wi];
-   const int*    zcl   = v.zcell[Cfg::wi];
-   const int     u0 = zb[blockIdx.x], u1 = zb[blockIdx.x + 1];
-   const int rS = warp, rC = warp + 1, rN = warp + 2;  // rows y-1, y, y+1 of the stage
-   auto at = [&]( const T* st, uint32_t word, int r, int k, int dx ) -> A {
-      return A( st[r * RW + int( ( word >> ( 3 * r ) ) & 7u ) + lane + 32 * k + 1 + dx] );
+   __syncwarp();
+   constexpr int bi  = Cfg::BPS - 2;
+   const int     gw  = blockIdx.x * kSwWarps + warp;
+   const int*    ucl = v.swcell[bi];
+   const int4*   uu  = v.swunits[bi];
+   const int     u1  = v.swbegin[bi][gw + 1];
+   const T*      aux = ( OP == OP_CHEBI || OP == OP_CHEBL ) ? v2 : ( OP == OP_APPLY_ADD ? dst : v1 );
+   auto active = [&]( int u ) {
+      const int c = ucl[u];
+      return c < nC && ( v.cell_bc[c] & flag ) != 0;
    };
+
+   // ---- loads: one cursor walks the same unit sequence as the computation, up to D loads ahead.
+   // Lane r < R+2 copies source row y0-1+r, lane R+2+r (AUX) second-vector row y0+r; each lane keeps
+   // its row's offset in the slice being loaded and advances it by additions.
+   const bool is_src = lane < R + 2, is_aux = AUX && lane >= R + 2 && lane < 2 * R + 2;
+   int        pu = v.swbegin[bi][gw];
+   int        ps = 0, pyy = 0;  // next slice of unit pu to load; this lane's row
+   int64_t    prb = 0;          // offset of that row in slice ps (cell-relative)
+   int4       PU  = make_int4( 0, 0, 0, 0 );
+   int64_t    pcb = 0;
+   auto       open = [&]() {
+      while ( pu < u1 && !active( pu ) ) ++pu;
+      if ( pu < u1 )
+      {
+         PU  = uu[pu];
+         pcb = v.cell_off[ucl[pu]];
+         ps  = PU.z - 1;
+         pyy = is_src ? PU.y - 1 + lane : PU.y + ( lane - R - 2 );
+         prb = cidx( n, 0, pyy, ps );
+      }
+   };
+   open();
+   int  issued = 0, ist = 0;  // loads issued; stage of the next one
+   auto issue  = [&]() {
+      if ( pu >= u1 ) return;
+      const int  st   = ist;
+      const int  x0   = PU.x & kSwUnitXMask, tw = ( PU.x & kSwUnitHalf ) ? 32 : kSwTX;
+      const int  xa   = is_src ? x0 - 1 : x0;
+      const int  xe   = is_src ? min( x0 + tw, n - pyy - ps ) : min( x0 + tw - 1, n - 1 - pyy - ps );
+      const bool live = ( is_src && pyy + ps <= n && xe >= xa ) || ( is_aux && ps >= PU.z && ps <= PU.w && xe >= xa );
+      uint32_t   bytes = 0;
+      int64_t    a0s   = 0;
+      if ( live )
+      {
+         const int64_t s0 = prb + xa, e1 = prb + xe + 1;
+         const int     sh = int( s0 & ( AL - 1 ) );  // the cell array starts on a 32-element boundary
+         a0s              = s0 - sh;
+         bytes            = uint32_t( ( ( e1 + AL - 1 ) / AL * AL - a0s ) * int64_t( sizeof( T ) ) );
+      }
+      const uint32_t total = __reduce_add_sync( 0xffffffffu, bytes );
+      if ( lane == 0 ) mbar_expect_tx( &full[st], total );
+      __syncwarp();
+      if ( bytes )
+         bulk_copy_g2s( ring + st * Cfg::stage + ( is_src ? lane * RW : Cfg::aux0 + ( lane - R - 2 ) * RWA ), ( is_src ? src : aux ) + pcb + a0s,
+                        bytes, &full[st] );
+      ++issued;
+      ist = ist + 1 == D ? 0 : ist + 1;
+      // cidx(0, y, z+1) = cidx(0, y, z) + tri(n+1-z) - y
+      prb += slice_step( n, ps ) - pyy;
+      if ( ++ps > PU.w + 1 )
+      {
+         ++pu;
+         open();
+      }
+   };
+   for ( int i = 0; i < D; ++i ) issue();
+
+
+   int  ld = 0, cst = 0;  // loads consumed; stage of the next one
+   uint32_t cph  = 0;     // its phase parity
    auto fail = [&]() {
       if ( lane == 0 )
       {
          atomicExch( err, 1 );
-         *abrt = 1;
+         // the copies still in flight must land before the block's shared memory is released
+         for ( int i = ld; i < issued; ++i )
+            if ( !mbar_wait_bounded( &full[i % D], uint32_t( ( i / D ) & 1 ), nullptr ) ) break;
       }
+      __syncwarp();
    };
-   int ld = 0;
-   // the weights are read from shared memory at every use (broadcast, shared by the lane's points)
-   // rather than held in 30 registers
-   A* w = wsm[warp];
-   int cw = -1;  // cell whose weights are in w
-   {
-      for ( int u = u0; u < u1; ++u )
-      {
-         const int c = zcl[u];
-         if ( c >= nC || !( v.cell_bc[c] & flag ) ) continue;
-         const int64_t base = v.cell_off[c];
-         if ( c != cw )
-         {
-            __syncwarp();
-            if ( lane < kNumDirs ) w[lane] = o.W[size_t( c ) * kNumClasses * kNumDirs + lane];  // interior class 0
-            if ( lane == kNumDirs ) w[kNumDirs] = o.invd_c[c];
-            __syncwarp();
-            cw = c;
-         }
-         const int4 U    = zu[u];
-         const int  x0   = U.x & kZUnitXMask;
-         const bool half = ( U.x & kZUnitHalf ) != 0;  // the tile's rows end within 32 points
-         const int  x = x0 + lane, y = U.y + warp;
-         // one unit with KP points per lane (kZPts, or 1 for half-width units)
-         auto unit = [&]( auto kp_c ) -> bool {
-            constexpr int KP = decltype( kp_c )::value;
-            // prologue: slice z_first-1 (load ld) and slice z_first (load ld+1)
-            const int sm = ld % S, s0 = ( ld + 1 ) % S;
-            if ( !mbar_wait_bounded( &full[sm], uint32_t( ( ld / S ) & 1 ), abrt ) ||
-                 !mbar_wait_bounded( &full[s0], uint32_t( ( ( ld + 1 ) / S ) & 1 ), abrt ) )
-               return false;
-            ZPoint< A > P[KP];
-            {
-               const T*       Rm = ring + sm * Cfg::stage;
-               const T*       R0 = ring + s0 * Cfg::stage;
-               const uint32_t wm = shw[2 * sm], wc = shw[2 * s0];
-   #pragma unroll
-               for ( int k = 0; k < KP; ++k )
-               {
-                  P[k].B   = at( Rm, wm, rC, k, 0 );
-                  P[k].BE  = at( Rm, wm, rC, k, 1 );
-                  P[k].BN  = at( Rm, wm, rN, k, 0 );
-                  P[k].BNW = at( Rm, wm, rN, k, -1 );
-                  P[k].C   = at( R0, wc, rC, k, 0 );
-                  P[k].W   = at( R0, wc, rC, k, -1 );
-                  P[k].S   = at( R0, wc, rS, k, 0 );
-                  P[k].SE  = at( R0, wc, rS, k, 1 );
-               }
-            }
-            __syncwarp();
-            if ( lane == 0 ) mbar_arrive( &empty[sm] );
-            int64_t out = base + cidx( n, x, y, U.z );  // output offset of point k = 0, advanced per slice
-            // unrolled by two so that the rolled values alternate registers instead of being copied
-   #pragma unroll 2
-            for ( int z = U.z; z <= U.w; out += slice_step( n, z ) - y, ++z )
-            {
-               const int lz = ld + 1 + ( z - U.z ), lp = lz + 1;
-               const int sz = lz % S, sp = lp % S;
-               if ( !mbar_wait_bounded( &full[sp], uint32_t( ( lp / S ) & 1 ), abrt ) ) return false;
-               const T*       Rz = ring + sz * Cfg::stage;
-               const T*       Rp = ring + sp * Cfg::stage;
-               const uint32_t wz = shw[2 * sz], wp = shw[2 * sp];
-               const uint32_t wa = AUX ? shw[2 * sz + 1] : 0u;
-   #pragma unroll
-               for ( int k = 0; k < KP; ++k )
-               {
-                  const A E = at( Rz, wz, rC, k, 1 ), N = at( Rz, wz, rN, k, 0 ), NW = at( Rz, wz, rN, k, -1 );
-                  const A Tt = at( Rp, wp, rC, k, 0 ), TW = at( Rp, wp, rC, k, -1 ), TS = at( Rp, wp, rS, k, 0 ),
-                          TSE = at( Rp, wp, rS, k, 1 );
-                  ZPoint< A >& p = P[k];
-                  if ( x + 32 * k + y + z <= n - 1 )
-                  {
-                     A auxv = A( 0 );
-                     if constexpr ( AUX )
-                        auxv = A( Rz[Cfg::aux0 + warp * Cfg::RWA + int( ( wa >> ( 3 * warp ) ) & 7u ) + lane + 32 * k] );
-                     // three independent partial sums: the dependent FMA chain is 7 deep instead of 15
-                     A s0 = w[0] * p.C, s1 = w[5] * p.B, s2 = w[10] * p.BE;
-                     s0 += w[1] * p.W;
-                     s1 += w[6] * Tt;
-                     s2 += w[11] * TS;
-                     s0 += w[2] * E;
-                     s1 += w[7] * NW;
-                     s2 += w[12] * p.BN;
-                     s0 += w[3] * p.S;
-                     s1 += w[8] * p.SE;
-                     s2 += w[13] * TSE;
-                     s0 += w[4] * N;
-                     s1 += w[9] * TW;
-                     s2 += w[14] * p.BNW;
-                     const A acc = s0 + ( s1 + s2 );
-                     zstream_epilogue< T, A, OP >( out + 32 * k, acc, w[kNumDirs], p.C, auxv, v2, dst, a0, a1 );
-                  }
-                  p.B   = p.C;
-                  p.BE  = E;
-                  p.BN  = N;
-                  p.BNW = NW;
-                  p.C   = Tt;
-                  p.W   = TW;
-                  p.S   = TS;
-                  p.SE  = TSE;
-               }
-               __syncwarp();
-               if ( lane == 0 ) mbar_arrive( &empty[sz] );
-            }
-            // slice z_last+1 is no longer needed either
-            __syncwarp();
-            if ( lane == 0 ) mbar_arrive( &empty[( ld + 2 + ( U.w - U.z ) ) % S] );
-            return true;
-         };
-         const bool good = half ? unit( std::integral_constant< int, 1 >{} ) : unit( std::integral_constant< int, kZPts >{} );
-         if ( !good ) return fail();
-         ld += U.w - U.z + 3;
-      }
-   }
-}
 
-// ---------------------------------------------------------------------------------------------
-// Partial-sum z-streamed cell sweep (FP64 apply on levels with n >= 256).
-//
-// Same units, ring, producers and bounded waits as the rolled sweep, with tiles of 64 x-points by
-// 16 rows (two rows per consumer warp, two x-points per lane: four points per lane per slice).
-// Each slice s is read once, at seven positions around each point, and gives three partial sums:
-// the top terms of point s-1 (which completes it and writes the result), the middle terms of
-// point s and the bottom terms of point s+1.  A point carries two running sums (plus its centre
-// value and second-vector value for the smoother epilogues) from slice to slice instead of eight
-// rolled source values, and a stage is released as soon as it has been read.
-// ---------------------------------------------------------------------------------------------
-constexpr int kZSRows = 2;  // tile rows per consumer warp
-
-template < typename T, bool AUX >
-struct ZSCfg
-{
-   static constexpr int wi    = 1;                                             // tile table index
-   static constexpr int TX    = kZWidths[wi];                                  // x-points per tile row
-   static constexpr int TY    = kZHeights[wi];                                 // tile rows
-   static constexpr int pts   = TX / 32;                                       // x-points per lane and row
-   static constexpr int al    = 16 / int( sizeof( T ) );                       // elements per 16 bytes
-   static constexpr int RW    = ( TX + 2 + 2 * al + al - 1 ) / al * al;        // source row width (elements)
-   static constexpr int RWA   = ( TX + 2 * al + al - 1 ) / al * al;            // second-vector row width
-   static constexpr int rows  = TY + 2;                                        // tile rows + halo
-   static constexpr int aux0  = rows * RW;                                     // second-vector rows start here
-   static constexpr int stage = aux0 + ( AUX ? TY * RWA : 0 );                 // elements per stage
-   static constexpr int S     = AUX ? 5 : 8;                                    // ring depth
-   static constexpr int NR    = rows + ( AUX ? TY : 0 );                        // row copies per stage
-   static constexpr size_t smem_bytes = size_t( S ) * stage * sizeof( T );
-   static_assert( kZWarps * kZSRows == TY, "two tile rows per consumer warp" );
-   static_assert( NR <= 64, "a producer lane issues at most two row copies per stage" );
-};
-
-// producer warp of the partial-sum sweep: row copy r < rows is source row y0-1+r, r >= rows is
-// second-vector row y0+(r-rows); lane l issues copies l and l+32.  Shifts are published as 3-bit
-// fields of two 64-bit words per stage (source rows, second-vector rows).
-template < typename T, bool AUX >
-__device__ __forceinline__ void zsum_produce( const LevelView& v, uint32_t flag, const T* __restrict__ src, const T* __restrict__ aux,
-                                              int nC, T* ring, uint64_t* full, uint64_t* empty, unsigned long long* shw,
-                                              volatile int* abort_flag, int* err )
-{
-   using Cfg = ZSCfg< T, AUX >;
-   constexpr int S = Cfg::S, AL = Cfg::al, TX = Cfg::TX;
-   const int     lane = threadIdx.x & 31, n = v.n, me = ( threadIdx.x >> 5 ) - kZWarps;
-   const int*    zb  = v.zbegin[Cfg::wi];
-   const int4*   zu  = v.zunits[Cfg::wi];
-   const int*    zcl = v.zcell[Cfg::wi];
-   const int     u0 = zb[blockIdx.x], u1 = zb[blockIdx.x + 1];
-   int           ld = 0;
-   bool          ok = true;
-   for ( int u = u0; u < u1 && ok; ++u )
+   A   w[kNumDirs], invd = A( 0 );
+   int cw = -1;
+   for ( int u = v.swbegin[bi][gw]; u < u1; ++u )
    {
-      const int c = zcl[u];
-      if ( c >= nC || !( v.cell_bc[c] & flag ) ) continue;
-      const int64_t cb = v.cell_off[c];
-      const int4    U  = zu[u];  // x0 (| half-width flag), y0, z_first, z_last
-      const int     ux = U.x & kZUnitXMask, tw = ( U.x & kZUnitHalf ) ? TX / 2 : TX;
-      for ( int zz = U.z - 1; zz <= U.w + 1; ++zz, ++ld )
-      {
-         if ( ld % kZProducers != me ) continue;
-         const int st = ld % S;
-         if ( ld >= S && !mbar_wait_bounded( &empty[st], uint32_t( ( ld / S - 1 ) & 1 ), abort_flag ) )
-         {
-            ok = false;
-            break;
-         }
-         uint32_t           bytes[2] = { 0u, 0u };
-         int64_t            a0[2]    = { 0, 0 };
-         int                dst[2]   = { 0, 0 };
-         unsigned long long w0 = 0ull, w1 = 0ull;
-#pragma unroll
-         for ( int h = 0; h < 2; ++h )
-         {
-            const int  r      = lane + 32 * h;
-            const bool is_src = r < Cfg::rows, is_aux = AUX && r >= Cfg::rows && r < Cfg::NR;
-            if ( !is_src && !is_aux ) continue;
-            const int  yy   = is_src ? U.y - 1 + r : U.y + ( r - Cfg::rows );
-            const int  xa   = is_src ? ux - 1 : ux;
-            const int  xe   = is_src ? min( ux + tw, n - yy - zz ) : min( ux + tw - 1, n - 1 - yy - zz );
-            const bool live = ( is_src && yy + zz <= n && xe >= xa ) || ( is_aux && zz >= U.z && zz <= U.w && xe >= xa );
-            dst[h]          = is_src ? r * Cfg::RW : Cfg::aux0 + ( r - Cfg::rows ) * Cfg::RWA;
-            if ( !live ) continue;
-            const int64_t rb = cidx( n, 0, yy, zz );
-            const int64_t s0 = rb + xa;
-            const int64_t e1 = rb + xe + 1;  // one past the segment
-            const uint32_t sh = uint32_t( s0 & ( AL - 1 ) );
-            a0[h]             = s0 - sh;
-            bytes[h]          = uint32_t( ( ( e1 + AL - 1 ) / AL * AL - a0[h] ) * int64_t( sizeof( T ) ) );
-            if ( is_src ) w0 |= ( unsigned long long )( sh ) << ( 3 * r );
-            else w1 |= ( unsigned long long )( sh ) << ( 3 * ( r - Cfg::rows ) );
-         }
-         const uint32_t total = __reduce_add_sync( 0xffffffffu, bytes[0] + bytes[1] );
-         const uint32_t w0lo = __reduce_or_sync( 0xffffffffu, uint32_t( w0 ) ), w0hi = __reduce_or_sync( 0xffffffffu, uint32_t( w0 >> 32 ) );
-         const uint32_t w1lo = __reduce_or_sync( 0xffffffffu, uint32_t( w1 ) ), w1hi = __reduce_or_sync( 0xffffffffu, uint32_t( w1 >> 32 ) );
-         if ( lane == 0 )
-         {
-            shw[2 * st]     = ( ( unsigned long long )( w0hi ) << 32 ) | w0lo;
-            shw[2 * st + 1] = ( ( unsigned long long )( w1hi ) << 32 ) | w1lo;
-            mbar_expect_tx( &full[st], total );
-         }
-         __syncwarp();
-#pragma unroll
-         for ( int h = 0; h < 2; ++h )
-            if ( bytes[h] )
-            {
-               const bool is_src = lane + 32 * h < Cfg::rows;
-               bulk_copy_g2s( ring + st * Cfg::stage + dst[h], ( is_src ? src : aux ) + cb + a0[h], bytes[h], &full[st] );
-            }
-      }
-   }
-   if ( !ok && lane == 0 )
-   {
-      atomicExch( err, 1 );
-      *abort_flag = 1;
-   }
-   // drain: the latest load issued on every stage has landed before the block may exit
-   if ( lane == 0 )
-      for ( int s = me; s < S && s < ld; s += kZProducers )
-      {
-         const int j = s + ( ( ld - 1 - s ) / S ) * S;
-         if ( !mbar_wait_bounded( &full[s], uint32_t( ( j / S ) & 1 ), nullptr ) ) atomicExch( err, 1 );
-      }
-}
-
-template < typename T, typename A, int OP >
-__global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zsum( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
-                                                               const T* __restrict__ v1, T* v2, T* dst, A a0, A a1, int nC, int* err )
-{
-   constexpr bool AUX = zstream_aux< OP >();
-   using Cfg          = ZSCfg< T, AUX >;
-   constexpr int S = Cfg::S, RW = Cfg::RW, P = Cfg::pts;
-   extern __shared__ __align__( 128 ) unsigned char zs_raw[];
-   T*                            ring = reinterpret_cast< T* >( zs_raw );
-   __shared__ uint64_t           full[S], empty[S];
-   __shared__ unsigned long long shw[2 * S];
-   __shared__ A                  wsm[kZWarps][16];  // per consumer warp: the cell's 15 weights and 1/diagonal
-   __shared__ int                abort_flag;
-   const int                     warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n = v.n;
-   if ( threadIdx.x == 0 )
-   {
-      for ( int s = 0; s < S; ++s )
-      {
-         mbar_init( &full[s], 1 );
-         mbar_init( &empty[s], kZWarps );
-      }
-      abort_flag = 0;
-      asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
-   }
-   __syncthreads();
-   volatile int* abrt = &abort_flag;
-   if ( warp >= kZWarps )
-   {
-      const T* aux = ( OP == OP_CHEBI || OP == OP_CHEBL ) ? v2 : ( OP == OP_APPLY_ADD ? dst : v1 );
-      zsum_produce< T, AUX >( v, flag, src, aux, nC, ring, full, empty, shw, abrt, err );
-      return;
-   }
-   const int*  zb  = v.zbegin[Cfg::wi];
-   const int4* zu  = v.zunits[Cfg::wi];
-   const int*  zcl = v.zcell[Cfg::wi];
-   const int   u0 = zb[blockIdx.x], u1 = zb[blockIdx.x + 1];
-   A*          w  = wsm[warp];
-   int         cw = -1;  // cell whose weights are in w
-   int         ld = 0;   // load number of the first slice of the next unit
-   for ( int u = u0; u < u1; ++u )
-   {
-      const int c = zcl[u];
-      if ( c >= nC || !( v.cell_bc[c] & flag ) ) continue;
-      const int64_t base = v.cell_off[c];
+      if ( !active( u ) ) continue;
+      const int c = ucl[u];
       if ( c != cw )
       {
-         __syncwarp();
-         if ( lane < kNumDirs ) w[lane] = o.W[size_t( c ) * kNumClasses * kNumDirs + lane];  // interior class 0
-         if ( lane == kNumDirs ) w[kNumDirs] = o.invd_c[c];
-         __syncwarp();
-         cw = c;
+#pragma unroll
+         for ( int d = 0; d < kNumDirs; ++d ) w[d] = o.W[size_t( c ) * kNumClasses * kNumDirs + d];  // interior class 0
+         invd = o.invd_c[c];
+         cw   = c;
       }
-      const int4 U    = zu[u];
-      const int  x0   = U.x & kZUnitXMask;
-      const bool half = ( U.x & kZUnitHalf ) != 0;  // the tile's rows end within 32 points
-      const int  x    = x0 + lane;
-      // one unit with P points per lane and row (Cfg::pts, or 1 for half-width units)
-      auto unit = [&]( auto kp_c ) -> bool {
-         constexpr int P = decltype( kp_c )::value;
-         // running sums of the point (x + 32 k, y_j) with y_j = U.y + 2 warp + j: acc of the point being
-         // completed, bot (bottom terms) of the next one; cen / axv: centre and second-vector value
-         A       acc[kZSRows][P], bot[kZSRows][P], cen[kZSRows][P], axv[kZSRows][P];
-         int64_t out[kZSRows];  // offset of (x, y_j, z) of the point being completed
-   #pragma unroll
-         for ( int j = 0; j < kZSRows; ++j )
-         {
-            out[j] = base + cidx( n, x, U.y + kZSRows * warp + j, U.z );
-   #pragma unroll
-            for ( int k = 0; k < P; ++k ) acc[j][k] = bot[j][k] = cen[j][k] = axv[j][k] = A( 0 );
-         }
-         // fold slice s (load number l) into the sums: FIN completes point s-1 with the top terms,
-         // MID starts point s, BOT gives the bottom terms of point s+1
-         auto step = [&]( int l, int s, auto fin_c, auto mid_c, auto bot_c ) -> bool {
-            constexpr bool FIN = decltype( fin_c )::value, MID = decltype( mid_c )::value, BOT = decltype( bot_c )::value;
-            const int      st  = l % S;
-            if ( !mbar_wait_bounded( &full[st], uint32_t( ( l / S ) & 1 ), abrt ) ) return false;
-            const T*                 R  = ring + st * Cfg::stage;
-            const unsigned long long wd = shw[2 * st];
-            const unsigned long long wa = AUX ? shw[2 * st + 1] : 0ull;
-   #pragma unroll
-            for ( int j = 0; j < kZSRows; ++j )
-            {
-               const int rs = kZSRows * warp + j, rc = rs + 1, rn = rs + 2;  // stage rows of y-1, y, y+1
-               const T*  Rs = R + rs * RW + int( ( wd >> ( 3 * rs ) ) & 7ull ) + lane + 1;
-               const T*  Rc = R + rc * RW + int( ( wd >> ( 3 * rc ) ) & 7ull ) + lane + 1;
-               const T*  Rn = R + rn * RW + int( ( wd >> ( 3 * rn ) ) & 7ull ) + lane + 1;
-               const int y  = U.y + rs;
-   #pragma unroll
-               for ( int k = 0; k < P; ++k )
+      const int4    U  = uu[u];
+      const int     x0 = U.x & kSwUnitXMask, y0 = U.y, za = U.z, zb = U.w;
+      const int64_t cb = v.cell_off[c];
+      const int64_t cbx = cb + x0 + lane;  // index of point (x0 + lane, 0, 0) of the cell
+      auto          unit = [&]( auto kp_c ) -> bool {
+         constexpr int KP = decltype( kp_c )::value;
+         A             acc[3][R][KP];
+         A             cen[3][R][KP];
+         A             axv[3][R][KP];
+         // cell-relative start of row y0-1+jj in the slice read last; the slice loop advances it before
+         // every step, so it starts one slice below z_first-1 (the offset formula and its recurrence
+         // cidx(0, y, z+1) = cidx(0, y, z) + tri(n+1-z) - y are one polynomial identity, so the
+         // start value for slice z_first-2 >= -1 is exact)
+         int rb[R + 2];
+#pragma unroll
+         for ( int jj = 0; jj < R + 2; ++jj ) rb[jj] = int( cidx( n, 0, y0 - 1 + jj, za - 2 ) );
+         // one slice step: slice s (the next load) folded into the sums of slot PH (points of slice s),
+         // slot (PH+2)%3 (slice s-1, completed and written when s-1 >= z_first) and slot (PH+1)%3
+         // (slice s+1).  The steps of slices z_first-1 and z_last+1 run the same code: what they add to
+         // slices outside the unit is never written.
+         auto step = [&]( int s, auto ph_c ) -> bool {
+            constexpr int PH = decltype( ph_c )::value, CS = PH, NS = ( PH + 1 ) % 3, PS = ( PH + 2 ) % 3;
+            // every lane waits; a wait that ran out on any lane fails the whole warp
+            if ( !__all_sync( 0xffffffffu, mbar_wait_bounded( &full[cst], cph, nullptr ) ) ) return false;
+            const T*   Rg   = ring + cst * Cfg::stage;
+            const int  sst  = int( slice_step( n, s - 1 ) );
+            const int  lim  = s > za ? n - x0 - y0 - s : -64;  // point (x0 + l, y0 + j, s - 1) is written iff l + j <= lim
+            // the values (x-1, x, x+1) of stage row jj; the rows are read one ahead of the arithmetic
+            // and stores of the current row, so the shared loads never wait behind global stores
+            A    va[R + 2][KP], vb[R + 2][KP], vc[R + 2][KP];
+            auto fetch = [&]( auto jj_c ) {
+               constexpr int jj   = decltype( jj_c )::value;
+               const int     rnew = rb[jj] + sst - ( y0 - 1 + jj );
+               const T*      rp   = Rg + jj * RW + ( ( rnew + x0 - 1 ) & ( AL - 1 ) ) + lane;  // rp[0] = x - 1 for k = 0
+#pragma unroll
+               for ( int k = 0; k < KP; ++k )
                {
-                  const int q  = 32 * k;
-                  const A   pc = A( Rc[q] ), pw = A( Rc[q - 1] ), pe = A( Rc[q + 1] );  // (x, y), (x-1, y), (x+1, y)
-                  const A   ps = A( Rs[q] ), pse = A( Rs[q + 1] );                      // (x, y-1), (x+1, y-1)
-                  const A   pn = A( Rn[q] ), pnw = A( Rn[q - 1] );                      // (x, y+1), (x-1, y+1)
-                  if constexpr ( FIN )
+                  vb[jj][k] = A( rp[32 * k + 1] );
+                  va[jj][k] = jj > 0 ? A( rp[32 * k] ) : A( 0 );
+                  vc[jj][k] = jj < R + 1 ? A( rp[32 * k + 2] ) : A( 0 );
+               }
+            };
+            fetch( std::integral_constant< int, 0 >{} );
+#pragma unroll
+            for ( int jj = 0; jj < R + 2; ++jj )
+            {
+               if ( jj + 1 < R + 2 )
+               {
+                  // static dispatch of the next row's fetch (jj is a compile-time value after unrolling)
+                  if ( jj == 0 ) fetch( std::integral_constant< int, 1 >{} );
+                  if ( jj == 1 ) fetch( std::integral_constant< int, 2 >{} );
+                  if ( jj == 2 ) fetch( std::integral_constant< int, 3 >{} );
+                  if ( jj == 3 ) fetch( std::integral_constant< int, 4 >{} );
+                  if ( jj == 4 ) fetch( std::integral_constant< int, 5 >{} );
+               }
+               const int j    = jj - 1;  // tile row of this stage row (-1 and R are halo rows)
+               const int rold = rb[jj];
+               const int rnew = rold + sst - ( y0 - 1 + jj );
+               rb[jj]         = rnew;
+               const int64_t io = cbx + rold;  // output index of (x0 + lane, y, s-1)
+#pragma unroll
+               for ( int k = 0; k < KP; ++k )
+               {
+                  const int q = 32 * k;
+                  const A   b = vb[jj][k], a = va[jj][k], cc = vc[jj][k];
+                  // bottom terms of slice s+1
+                  if ( j >= 0 && j < R )
                   {
-                     A t0 = w[6] * pc, t1 = w[9] * pw;
-                     t0 += w[11] * ps;
-                     t1 += w[13] * pse;
-                     const A sum = acc[j][k] + ( t0 + t1 );
-                     if ( x + q + y + s - 1 <= n - 1 )
-                        zstream_epilogue< T, A, OP >( out[j] + q, sum, w[kNumDirs], cen[j][k], axv[j][k], v2, dst, a0, a1 );
+                     acc[NS][j][k] = w[5] * b;
+                     acc[NS][j][k] += w[10] * cc;
                   }
-                  if constexpr ( MID )
+                  if ( j >= 1 )
                   {
-                     A m0 = w[0] * pc, m1 = w[1] * pw, m2 = w[2] * pe;
-                     m0 += w[3] * ps;
-                     m1 += w[4] * pn;
-                     m2 += w[7] * pnw;
-                     m0 += w[8] * pse;
-                     acc[j][k] = bot[j][k] + ( m0 + ( m1 + m2 ) );
-                     cen[j][k] = pc;
-                     if constexpr ( AUX )
-                        axv[j][k] = A( R[Cfg::aux0 + rs * Cfg::RWA + int( ( wa >> ( 3 * rs ) ) & 7ull ) + lane + q] );
+                     acc[NS][j - 1][k] += w[12] * b;
+                     acc[NS][j - 1][k] += w[14] * a;
                   }
-                  if constexpr ( BOT )
+                  // middle terms of slice s
+                  if ( j + 1 < R )
                   {
-                     A b0 = w[5] * pc, b1 = w[10] * pe;
-                     b0 += w[12] * pn;
-                     b1 += w[14] * pnw;
-                     bot[j][k] = b0 + b1;
+                     acc[CS][j + 1][k] += w[3] * b;
+                     acc[CS][j + 1][k] += w[8] * cc;
+                  }
+                  if ( j >= 0 && j < R )
+                  {
+                     acc[CS][j][k] += w[1] * a;
+                     acc[CS][j][k] += w[0] * b;
+                     acc[CS][j][k] += w[2] * cc;
+                     if constexpr ( CEN ) cen[CS][j][k] = b;
+                     if constexpr ( AUX ) axv[CS][j][k] = A( Rg[Cfg::aux0 + j * RWA + ( ( rnew + x0 ) & ( AL - 1 ) ) + lane + q] );
+                  }
+                  if ( j >= 1 )
+                  {
+                     acc[CS][j - 1][k] += w[4] * b;
+                     acc[CS][j - 1][k] += w[7] * a;
+                  }
+                  // top terms of slice s-1; a point is complete after its own row
+                  if ( j + 1 < R )
+                  {
+                     acc[PS][j + 1][k] += w[11] * b;
+                     acc[PS][j + 1][k] += w[13] * cc;
+                  }
+                  if ( j >= 0 && j < R )
+                  {
+                     acc[PS][j][k] += w[6] * b;
+                     acc[PS][j][k] += w[9] * a;
+                     if ( lane + q + j <= lim )
+                        sweep_epilogue< T, A, OP >( io + q, acc[PS][j][k], invd, cen[PS][j][k], axv[PS][j][k], v2, dst, a0, a1 );
                   }
                }
-               if constexpr ( FIN ) out[j] += slice_step( n, s - 1 ) - y;
             }
+            // every lane has read the stage: hand it back to the async proxy and refill it
+            asm volatile( "fence.proxy.async.shared::cta;" ::: "memory" );
             __syncwarp();
-            if ( lane == 0 ) mbar_arrive( &empty[st] );
+            ++ld;
+            if ( ++cst == D ) cst = 0, cph ^= 1u;
+            issue();
             return true;
          };
-         using F = std::false_type;
-         using Tr = std::true_type;
-         bool good = step( ld, U.z - 1, F{}, F{}, Tr{} ) && step( ld + 1, U.z, F{}, Tr{}, Tr{} );
-         for ( int s = U.z + 1; good && s <= U.w; ++s ) good = step( ld + 1 + ( s - U.z ), s, Tr{}, Tr{}, Tr{} );
-         good = good && step( ld + 2 + ( U.w - U.z ), U.w + 1, Tr{}, F{}, F{} );
-         return good;
+         // the slot of the points of slice p is (p - z_first + 1) mod 3; the steps run z_first-1 .. z_last+1
+         using I0 = std::integral_constant< int, 0 >;
+         using I1 = std::integral_constant< int, 1 >;
+         using I2 = std::integral_constant< int, 2 >;
+         for ( int s = za - 1;; )
+         {
+            if ( !step( s, I0{} ) ) return false;
+            if ( ++s > zb + 1 ) return true;
+            if ( !step( s, I1{} ) ) return false;
+            if ( ++s > zb + 1 ) return true;
+            if ( !step( s, I2{} ) ) return false;
+            if ( ++s > zb + 1 ) return true;
+         }
       };
-      const bool ok = half ? unit( std::integral_constant< int, 1 >{} ) : unit( std::integral_constant< int, Cfg::pts >{} );
-      if ( !ok )
-      {
-         if ( lane == 0 )
-         {
-            atomicExch( err, 1 );
-            *abrt = 1;
-         }
-         return;
-      }
-      ld += U.w - U.z + 3;
-   }
-}
-
-// ---------------------------------------------------------------------------------------------
-// Full-row z-streamed cell sweep (selectable with HYB_CELL_KERNEL=zrow).
-//
-// A unit is the band of rows y0..y0+ty-1 of slices z_first..z_last of one macro-cell, x over the
-// whole row.  The rows y0-1..y0+ty of a slice are contiguous in the cell array, so one bulk copy
-// fills a stage (one more copies the band of the second vector), and a slice load carries up to
-// ty x (n-1) points: the copy engine sees few large copies and the producer/consumer hand-off is
-// paid a few times per band rather than per 64-point tile.  Consumer warp w serves band row
-// w mod ty and every (8/ty)-th 32-lane x chunk; all 15 stencil values are read from the three
-// resident slices (z-1, z, z+1) in shared memory, so slice z-1 is released after step z and a ring
-// of kRStages keeps two slices in flight.  ty is the largest of 8, 4, 2, 1 whose ring fits the
-// shared-memory budget for the level's row length and the value type.  Waits are bounded as in the
-// tiled sweep.
-// ---------------------------------------------------------------------------------------------
-constexpr int    kRStages   = 5;
-constexpr size_t kRSmemMax  = 110 * 1024;  // two blocks per SM
-
-template < typename T >
-__host__ __device__ constexpr int64_t zrow_src_cap( int n, int ty )
-{
-   return ( int64_t( ty + 2 ) * ( n + 1 ) + 2 * ( 16 / int( sizeof( T ) ) ) + 15 ) / 16 * 16;
-}
-template < typename T >
-__host__ __device__ constexpr int64_t zrow_aux_cap( int n, int ty )
-{
-   return ( int64_t( ty ) * ( n + 1 ) + 2 * ( 16 / int( sizeof( T ) ) ) + 15 ) / 16 * 16;
-}
-template < typename T, bool AUX >
-static int zrow_band_h( int n )
-{
-   for ( int h = 3; h >= 0; --h )
-   {
-      const int64_t stage = zrow_src_cap< T >( n, 1 << h ) + ( AUX ? zrow_aux_cap< T >( n, 1 << h ) : 0 );
-      if ( size_t( kRStages ) * size_t( stage ) * sizeof( T ) <= kRSmemMax ) return h;
-   }
-   return -1;
-}
-
-// offset of row y of slice z from the start of row 0 of slice z: cidx(0, y, z) - cidx(0, 0, z)
-__device__ __forceinline__ int64_t row_off( int n, int y, int z ) { return int64_t( y ) * ( n + 2 - z ) - int64_t( y ) * ( y + 1 ) / 2; }
-
-template < typename T, typename A, int OP >
-__global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zrow( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
-                                                               const T* __restrict__ v1, T* v2, T* dst, A a0, A a1, int nC, int h,
-                                                               int64_t src_cap, int64_t stage, int* err )
-{
-   constexpr bool AUX = zstream_aux< OP >();
-   constexpr int  AL  = 16 / int( sizeof( T ) );
-   constexpr int  S   = kRStages;
-   extern __shared__ __align__( 128 ) unsigned char zr_raw[];
-   T*                  ring = reinterpret_cast< T* >( zr_raw );
-   __shared__ uint64_t full[S], empty[S];
-   __shared__ uint32_t shw[S];  // source shift | second-vector shift << 8
-   __shared__ int      abort_flag;
-   const int           warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n = v.n;
-   const int*          rb   = v.rbegin[h];
-   const int4*         ru   = v.runits[h];
-   const int           u0 = rb[blockIdx.x], u1 = rb[blockIdx.x + 1];
-   if ( threadIdx.x == 0 )
-   {
-      for ( int s = 0; s < S; ++s )
-      {
-         mbar_init( &full[s], 1 );
-         mbar_init( &empty[s], kZWarps );
-      }
-      abort_flag = 0;
-      asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
-   }
-   __syncthreads();
-   volatile int* abrt = &abort_flag;
-
-   if ( warp >= kZWarps )
-   {
-      // producers: lane 0 of producer warp p issues the loads l with l % kZProducers == p
-      const int me = warp - kZWarps;
-      if ( lane != 0 ) return;
-      const T* aux = ( OP == OP_CHEBI || OP == OP_CHEBL ) ? v2 : ( OP == OP_APPLY_ADD ? dst : v1 );
-      int      ld  = 0;
-      bool     ok  = true;
-      for ( int c = 0; c < nC && ok; ++c )
-      {
-         if ( !( v.cell_bc[c] & flag ) ) continue;
-         const int64_t cb = v.cell_off[c];
-         for ( int u = u0; u < u1 && ok; ++u )
-         {
-            const int4 U = ru[u];  // ty, y0, z_first, z_last
-            for ( int zz = U.z - 1; zz <= U.w + 1; ++zz, ++ld )
-            {
-               if ( ld % kZProducers != me ) continue;
-               const int st = ld % S;
-               if ( ld >= S && !mbar_wait_bounded( &empty[st], uint32_t( ( ld / S - 1 ) & 1 ), abrt ) )
-               {
-                  ok = false;
-                  break;
-               }
-               const int64_t slice = cidx( n, 0, 0, zz );
-               const int     ya = U.y - 1, yb = min( U.y + U.x, n - zz );  // rows ya..yb of the slice
-               const int64_t s0 = slice + row_off( n, ya, zz ), e1 = slice + row_off( n, yb + 1, zz );
-               const int     sh = int( s0 & ( AL - 1 ) );
-               const int64_t a0 = s0 - sh;
-               uint32_t      bytes = uint32_t( ( ( e1 + AL - 1 ) / AL * AL - a0 ) * int64_t( sizeof( T ) ) );
-               uint32_t      abytes = 0;
-               int64_t       aa0    = 0;
-               int           ash    = 0;
-               if ( AUX && zz >= U.z && zz <= U.w && U.y <= n - 2 - zz )
-               {
-                  const int     ye = min( U.y + U.x - 1, n - 2 - zz );  // interior rows of the band
-                  const int64_t t0 = slice + row_off( n, U.y, zz ), t1 = slice + row_off( n, ye + 1, zz );
-                  ash              = int( t0 & ( AL - 1 ) );
-                  aa0              = t0 - ash;
-                  abytes           = uint32_t( ( ( t1 + AL - 1 ) / AL * AL - aa0 ) * int64_t( sizeof( T ) ) );
-               }
-               shw[st] = uint32_t( sh ) | ( uint32_t( ash ) << 8 );
-               mbar_expect_tx( &full[st], bytes + abytes );
-               T* sbase = ring + st * stage;
-               bulk_copy_g2s( sbase, src + cb + a0, bytes, &full[st] );
-               if ( abytes ) bulk_copy_g2s( sbase + src_cap, aux + cb + aa0, abytes, &full[st] );
-            }
-         }
-      }
-      if ( !ok )
-      {
-         atomicExch( err, 1 );
-         *abrt = 1;
-      }
-      for ( int s = me; s < S && s < ld; s += kZProducers )
-      {
-         const int j = s + ( ( ld - 1 - s ) / S ) * S;
-         if ( !mbar_wait_bounded( &full[s], uint32_t( ( j / S ) & 1 ), nullptr ) ) atomicExch( err, 1 );
-      }
-      return;
-   }
-
-   // consumers
-   __shared__ A wsm[kZWarps][16];
-   auto fail = [&]() {
-      if ( lane == 0 )
-      {
-         atomicExch( err, 1 );
-         *abrt = 1;
-      }
-   };
-   auto wait_load = [&]( int l ) { return mbar_wait_bounded( &full[l % S], uint32_t( ( l / S ) & 1 ), abrt ); };
-   auto release   = [&]( int l ) {
-      __syncwarp();
-      if ( lane == 0 ) mbar_arrive( &empty[l % S] );
-   };
-   int ld = 0;
-   for ( int c = 0; c < nC; ++c )
-   {
-      if ( !( v.cell_bc[c] & flag ) ) continue;
-      const int64_t base = v.cell_off[c];
-      A*            w    = wsm[warp];
-      __syncwarp();
-      if ( lane < kNumDirs ) w[lane] = o.W[size_t( c ) * kNumClasses * kNumDirs + lane];
-      if ( lane == kNumDirs ) w[kNumDirs] = o.invd_c[c];
-      __syncwarp();
-      for ( int u = u0; u < u1; ++u )
-      {
-         const int4 U  = ru[u];
-         const int  ty = U.x, r = warp % ty, q = warp / ty, xs = 32 * ( kZWarps / ty );
-         const int  y  = U.y + r;
-         if ( !wait_load( ld ) || !wait_load( ld + 1 ) ) return fail();
-         for ( int z = U.z; z <= U.w; ++z )
-         {
-            const int lm = ld + ( z - U.z ), l0 = lm + 1, lp = lm + 2;
-            if ( !wait_load( lp ) ) return fail();
-            if ( y <= n - 2 - z )
-            {
-               // stage pointers to row y' of slices z-1, z, z+1 (x = 0 at the returned address)
-               auto row = [&]( int l, int zz, int yy ) -> const T* {
-                  const T* sb = ring + ( l % S ) * stage;
-                  return sb + int( shw[l % S] & 0xffu ) + ( row_off( n, yy, zz ) - row_off( n, U.y - 1, zz ) );
-               };
-               const T* Rm0 = row( lm, z - 1, y );
-               const T* Rm1 = row( lm, z - 1, y + 1 );
-               const T* Rs  = row( l0, z, y - 1 );
-               const T* R0  = row( l0, z, y );
-               const T* Rn  = row( l0, z, y + 1 );
-               const T* Rps = row( lp, z + 1, y - 1 );
-               const T* Rp0 = row( lp, z + 1, y );
-               const T* Ra  = nullptr;
-               if constexpr ( AUX )
-                  Ra = ring + ( l0 % S ) * stage + src_cap + int( shw[l0 % S] >> 8 ) + ( row_off( n, y, z ) - row_off( n, U.y, z ) );
-               const int64_t obase = base + cidx( n, 0, y, z );
-               for ( int x = 1 + lane + 32 * q; x <= n - 1 - y - z; x += xs )
-               {
-                  A s0 = w[0] * A( R0[x] ), s1 = w[5] * A( Rm0[x] ), s2 = w[10] * A( Rm0[x + 1] );
-                  s0 += w[1] * A( R0[x - 1] );
-                  s1 += w[6] * A( Rp0[x] );
-                  s2 += w[11] * A( Rps[x] );
-                  s0 += w[2] * A( R0[x + 1] );
-                  s1 += w[7] * A( Rn[x - 1] );
-                  s2 += w[12] * A( Rm1[x] );
-                  s0 += w[3] * A( Rs[x] );
-                  s1 += w[8] * A( Rs[x + 1] );
-                  s2 += w[13] * A( Rps[x + 1] );
-                  s0 += w[4] * A( Rn[x] );
-                  s1 += w[9] * A( Rp0[x - 1] );
-                  s2 += w[14] * A( Rm1[x - 1] );
-                  const A acc  = s0 + ( s1 + s2 );
-                  A       auxv = A( 0 );
-                  if constexpr ( AUX ) auxv = A( Ra[x] );
-                  zstream_epilogue< T, A, OP >( obase + x, acc, w[kNumDirs], A( R0[x] ), auxv, v2, dst, a0, a1 );
-               }
-            }
-            release( lm );  // slice z-1 is no longer needed
-         }
-         release( ld + ( U.w - U.z ) + 1 );  // slice z_last
-         release( ld + ( U.w - U.z ) + 2 );  // slice z_last + 1
-         ld += U.w - U.z + 3;
-      }
+      const bool ok = ( U.x & kSwUnitHalf ) ? unit( std::integral_constant< int, 1 >{} ) : unit( std::integral_constant< int, kSwTX / 32 >{} );
+      if ( !ok ) return fail();
    }
 }
 
 template < typename T, typename A, int OP >
-static void zstream_attribute()
+static void sweep_attribute( int sms )
 {
-   check_cuda( cudaFuncSetAttribute( k_cell_zrow< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize, int( kRSmemMax ) ),
-               "cudaFuncSetAttribute(full-row sweep shared memory)" );
-   check_cuda( cudaFuncSetAttribute( k_cell_zstream< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int( ZCfg< T, zstream_aux< OP >() >::smem_bytes ) ),
-               "cudaFuncSetAttribute(z-stream shared memory)" );
-   check_cuda( cudaFuncSetAttribute( k_cell_zsum< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int( ZSCfg< T, zstream_aux< OP >() >::smem_bytes ) ),
-               "cudaFuncSetAttribute(partial-sum sweep shared memory)" );
+   using Cfg = SwCfg< T, OP >;
+   check_cuda( cudaFuncSetAttribute( k_cell_sweep< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize, int( Cfg::smem_bytes ) ),
+               "cudaFuncSetAttribute(cell sweep shared memory)" );
+   int nb = 0;
+   check_cuda( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &nb, k_cell_sweep< T, A, OP >, kSwWarps * 32, Cfg::smem_bytes ),
+               "cell sweep occupancy" );
+   // the unit lists assume every block of the launch is resident at once
+   if ( nb < Cfg::BPS )
+      throw std::runtime_error( "cell sweep: " + std::to_string( nb ) + " resident blocks per SM, the unit lists need " +
+                                std::to_string( Cfg::BPS ) );
+   (void) sms;
 }
 
 template < typename T, typename A >
-static void zstream_attributes()
+static void sweep_attributes( int sms )
 {
-   zstream_attribute< T, A, OP_APPLY >();
-   zstream_attribute< T, A, OP_APPLY_ADD >();
-   zstream_attribute< T, A, OP_RESID >();
-   zstream_attribute< T, A, OP_JAC >();
-   zstream_attribute< T, A, OP_CHEB0 >();
-   zstream_attribute< T, A, OP_CHEBI >();
-   zstream_attribute< T, A, OP_CHEBL >();
-   zstream_attribute< T, A, OP_DINV_APPLY >();
+   sweep_attribute< T, A, OP_APPLY >( sms );
+   sweep_attribute< T, A, OP_APPLY_ADD >( sms );
+   sweep_attribute< T, A, OP_RESID >( sms );
+   sweep_attribute< T, A, OP_JAC >( sms );
+   sweep_attribute< T, A, OP_CHEB0 >( sms );
+   sweep_attribute< T, A, OP_CHEBI >( sms );
+   sweep_attribute< T, A, OP_CHEBL >( sms );
+   sweep_attribute< T, A, OP_DINV_APPLY >( sms );
 }
 
-static void zstream_attributes_all()
+static void sweep_attributes_all()
 {
-   zstream_attributes< double, double >();
-   zstream_attributes< float, float >();
-   zstream_attributes< __half, float >();
-}
-
-static int march_prefetch_distance()
-{
-   static int d = -1;
-   if ( d < 0 )
-   {
-      const char* e = getenv( "HYB_PREFETCH" );
-      d             = e ? std::max( 0, atoi( e ) ) : 8;
-   }
-   return d;
-}
-
-// HYB_CELL_KERNEL forces one cell sweep for every operation ("zsum", "zstream", "zrow", "march",
-// "rows"); it is read at every launch so that a tuning run can switch between calls.  Unset, the
-// sweep is chosen per operation (automatic, -1).
-static int cell_kernel_variant()
-{
-   const char* e = getenv( "HYB_CELL_KERNEL" );
-   if ( !e || !*e ) return -1;
-   const std::string s( e );
-   return s == "rows" ? 0 : s == "march" ? 1 : s == "zstream" ? 2 : s == "zrow" ? 3 : s == "zsum" ? 4 : -1;
+   int dev = 0, sms = 0;
+   check_cuda( cudaGetDevice( &dev ), "cudaGetDevice" );
+   check_cuda( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev ), "device attribute" );
+   sweep_attributes< double, double >( sms );
+   sweep_attributes< float, float >( sms );
+   sweep_attributes< __half, float >( sms );
 }
 
 
 // Stencil of one position class at cell-local (x, y, z): the 15 directions are unrolled with the
-// seven row bases computed once, so all loads of a point are independent and in flight together.
+// seven row bases derived from the point's own row by additions (row y of slice z holds n+1-z-y
+// points, slice z holds tri(n+1-z) points), so all loads of a point are independent and in flight
+// together.  Bases of directions outside the cell are never used: the class mask skips them.
+// class_stencil returns the sum; class_stencil_at also returns the cell-array offset of the point.
+template < typename A >
+struct StencilAt
+{
+   A       sum;
+   int64_t centre;
+};
+
 template < typename T, typename A >
-__device__ __forceinline__ A class_stencil( const T* s, const A* W, uint16_t mask, int n, int x, int y, int z )
+__device__ __forceinline__ StencilAt< A > class_stencil_at( const T* s, const A* W, uint16_t mask, int n, int x, int y, int z )
 {
    const int64_t r00 = cidx( n, 0, y, z );
-   const int64_t rm0 = y > 0 ? cidx( n, 0, y - 1, z ) : 0;
-   const int64_t rp0 = y + z < n ? cidx( n, 0, y + 1, z ) : 0;
-   const int64_t r0m = z > 0 ? cidx( n, 0, y, z - 1 ) : 0;
-   const int64_t r0p = y + z < n ? cidx( n, 0, y, z + 1 ) : 0;
-   const int64_t rmp = ( y > 0 && y + z <= n ) ? cidx( n, 0, y - 1, z + 1 ) : 0;
-   const int64_t rpm = ( z > 0 && y + z <= n ) ? cidx( n, 0, y + 1, z - 1 ) : 0;
+   const int64_t ly  = n + 1 - z - y;                      // points in row y of slice z
+   const int64_t tz  = int64_t( n + 1 - z ) * ( n + 2 - z ) / 2;  // points in slice z
+   const int64_t rm0 = r00 - ( ly + 1 );                  // row y-1 of slice z
+   const int64_t rp0 = r00 + ly;                          // row y+1 of slice z
+   const int64_t r0p = r00 + tz - y;                      // row y of slice z+1
+   const int64_t r0m = r00 - ( tz + ( n + 2 - z ) - y );  // row y of slice z-1 (slice z-1 holds tz + n+2-z points)
+   const int64_t rmp = r0p - ly;                          // row y-1 of slice z+1
+   const int64_t rpm = r0m + ly + 1;                      // row y+1 of slice z-1
    const int64_t idx[kNumDirs] = { r00 + x,     r00 + x - 1, r00 + x + 1, rm0 + x,     rp0 + x,
                                    r0m + x,     r0p + x,     rp0 + x - 1, rm0 + x + 1, r0p + x - 1,
                                    r0m + x + 1, rmp + x,     rpm + x,     rmp + x + 1, rpm + x - 1 };
@@ -1313,17 +805,22 @@ __device__ __forceinline__ A class_stencil( const T* s, const A* W, uint16_t mas
 #pragma unroll
    for ( int d = 0; d < kNumDirs; ++d )
       if ( mask & ( 1u << d ) ) acc += W[d] * A( ldv( s + idx[d] ) );
-   return acc;
+   return { acc, r00 + x };
 }
 
-template < typename T, typename A, int OP >
-__global__ void __launch_bounds__( 256 ) k_bnd_stencil( LevelView v, OpView< A > o, uint32_t flag, int copy_unflagged,
-                                                         const T* __restrict__ src, const T* __restrict__ v1, T* v2, T* dst,
-                                                         A a0, A a1 )
+template < typename T, typename A >
+__device__ __forceinline__ A class_stencil( const T* s, const A* W, uint16_t mask, int n, int x, int y, int z )
 {
-   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-   if ( t >= v.ntasks ) return;
-   const int4    tk    = v.tasks[t];
+   return class_stencil_at< T, A >( s, W, mask, n, x, y, z ).sum;
+}
+
+// One owned face / edge / vertex DoF (boundary task t): the sum over its neighbour cells of the
+// stencil of its position class in each cell, the operation's epilogue, and the write to the owner
+// and every copy in the neighbouring cell arrays.
+template < typename T, typename A, int OP >
+__device__ __forceinline__ void bnd_task( const LevelView& v, const OpView< A >& o, uint32_t flag, int copy_unflagged,
+                                          const T* __restrict__ src, const T* __restrict__ v1, T* v2, T* dst, A a0, A a1, int4 tk )
+{
    const int     b     = tk.x, i = tk.y, j = tk.z, n = v.n;
    const int64_t owner = owner_slot( v, b, i, j );
    if ( !( v.bc[b] & flag ) )
@@ -1338,16 +835,38 @@ __global__ void __launch_bounds__( 256 ) k_bnd_stencil( LevelView v, OpView< A >
    if ( q1 - q0 == 2 )
    {
       // a face between two cells: both class stencils written out, so the loads of the two cells
-      // are in flight together (same sum, same order as the loop)
+      // are in flight together (same sum, same order as the loop); the copies of the owner in the
+      // two cell arrays are the stencils' centres
       const Incidence I0 = v.inc[q0], I1 = v.inc[q0 + 1];
       int             x0, y0, z0, x1, y1, z1;
       inc_point( I0, n, i, j, x0, y0, z0 );
       inc_point( I1, n, i, j, x1, y1, z1 );
-      const A s0 = class_stencil< T, A >( src + v.cell_off[I0.cell], o.W + ( size_t( I0.cell ) * kNumClasses + I0.cls ) * kNumDirs,
-                                          c_cls_mask[I0.cls], n, x0, y0, z0 );
-      const A s1 = class_stencil< T, A >( src + v.cell_off[I1.cell], o.W + ( size_t( I1.cell ) * kNumClasses + I1.cls ) * kNumDirs,
-                                          c_cls_mask[I1.cls], n, x1, y1, z1 );
-      acc = ( acc + s0 ) + s1;
+      const int64_t         cb0 = v.cell_off[I0.cell], cb1 = v.cell_off[I1.cell];
+      const StencilAt< A >  s0  = class_stencil_at< T, A >( src + cb0, o.W + ( size_t( I0.cell ) * kNumClasses + I0.cls ) * kNumDirs,
+                                                           c_cls_mask[I0.cls], n, x0, y0, z0 );
+      const StencilAt< A >  s1  = class_stencil_at< T, A >( src + cb1, o.W + ( size_t( I1.cell ) * kNumClasses + I1.cls ) * kNumDirs,
+                                                           c_cls_mask[I1.cls], n, x1, y1, z1 );
+      const int64_t         c0 = s0.centre, c1 = s1.centre;
+      acc                       = ( acc + s0.sum ) + s1.sum;
+      const A invd = o.invd_b[b];
+      auto    put  = [&]( T* vec, A val ) {
+         stv( vec + owner, val );
+         stv( vec + cb0 + c0, val );
+         stv( vec + cb1 + c1, val );
+      };
+      if constexpr ( OP == OP_APPLY ) put( dst, acc );
+      else if constexpr ( OP == OP_APPLY_ADD ) put( dst, A( ldc( dst + owner ) ) + acc );
+      else if constexpr ( OP == OP_RESID ) put( dst, A( ldv( v1 + owner ) ) - acc );
+      else if constexpr ( OP == OP_JAC ) put( dst, A( ldv( src + owner ) ) + a0 * ( invd * ( A( ldv( v1 + owner ) ) - acc ) ) );
+      else if constexpr ( OP == OP_CHEB0 ) put( dst, invd * ( A( ldv( v1 + owner ) ) - acc ) );
+      else if constexpr ( OP == OP_CHEBI )
+      {
+         put( dst, invd * acc );
+         put( v2, A( ldc( v2 + owner ) ) + a0 * A( ldv( src + owner ) ) );
+      }
+      else if constexpr ( OP == OP_CHEBL ) put( v2, ( A( ldc( v2 + owner ) ) + a0 * A( ldv( src + owner ) ) ) + a1 * ( invd * acc ) );
+      else if constexpr ( OP == OP_DINV_APPLY ) put( dst, invd * acc );
+      return;
    }
    else
       // edges and vertices: two incidences' stencils in flight, summed in incidence order
@@ -1388,60 +907,76 @@ __global__ void __launch_bounds__( 256 ) k_bnd_stencil( LevelView v, OpView< A >
 }
 
 template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( 256 ) k_bnd_stencil( LevelView v, OpView< A > o, TaskSegments seg, uint32_t flag, int copy_unflagged,
+                                                         const T* __restrict__ src, const T* __restrict__ v1, T* v2, T* dst,
+                                                         A a0, A a1 )
+{
+   // tasks of the primitives whose boundary type is flagged (or all, when unflagged owners are
+   // copied): up to four contiguous groups of the type-sorted task list
+   int t = blockIdx.x * blockDim.x + threadIdx.x, at = -1;
+#pragma unroll
+   for ( int g = 0; g < 4; ++g )  // unrolled: the segment arrays are read with constant indices
+   {
+      if ( at < 0 && t < seg.count[g] ) at = seg.start[g] + t;
+      if ( at < 0 ) t -= seg.count[g];
+   }
+   if ( at < 0 ) return;
+   bnd_task< T, A, OP >( v, o, flag, copy_unflagged, src, v1, v2, dst, a0, a1, v.btasks[at] );
+}
+
+template < typename T, typename A, int OP >
 static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o, int nC, const StencilArgs& a )
 {
    const T* src = (const T*) a.src;
    const T* v1  = (const T*) a.v1;
    T*       v2  = (T*) a.v2;
    T*       dst = (T*) a.dst;
-   Fork     fk( ctx );
-   // automatic choice: the partial-sum sweep for FP64 operations without a second vector (apply) on
-   // levels with n >= 256, the rolled-register sweep otherwise (same-process A/B on the cube: level 8
-   // FP64 apply 0.111 vs 0.125 ms; level 7 FP64 apply 0.034 vs 0.033 ms; Jacobi and FP32 sweeps
-   // faster with the rolled sweep at levels 6-8)
-   int var = cell_kernel_variant();
-   if ( var < 0 ) var = ( !zstream_aux< OP >() && sizeof( T ) == 8 && v.n >= 256 ) ? 4 : 2;
-   const int zh = ( var == 3 && v.n >= 32 ) ? zrow_band_h< T, zstream_aux< OP >() >( v.n ) : -1;
-   if ( zh >= 0 && v.nrblocks[zh] > 0 && nC > 0 )
+   // the bulk-copy sweep from n = 32 on (two 64-point tiles per row and up), the y-marching sweep on
+   // the small levels, where a slice holds too few rows to fill a ring
+   using Cfg = SwCfg< T, OP >;
+   // cell interiors and boundary owners write disjoint slots and read only src (and their own
+   // slots of the second vector), so the two kernels may run in either order
+   const TaskSegments seg = task_segments( v, a.flag, a.copy_unflagged );
+   const int          nt  = seg.count[0] + seg.count[1] + seg.count[2] + seg.count[3];
+   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+   check_cuda( cudaStreamIsCapturing( ctx->stream, &cap ), "cudaStreamIsCapturing" );
+   if ( v.n >= 32 && nC > 0 && v.nswarps[Cfg::BPS - 2] > 0 && cap == cudaStreamCaptureStatusNone )
    {
-      const int64_t scap  = zrow_src_cap< T >( v.n, 1 << zh );
-      const int64_t stage = scap + ( zstream_aux< OP >() ? zrow_aux_cap< T >( v.n, 1 << zh ) : 0 );
-      const size_t  smem  = size_t( kRStages ) * size_t( stage ) * sizeof( T );
-      k_cell_zrow< T, A, OP ><<< v.nrblocks[zh], kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ),
-                                                                                  A( a.a1 ), nC, zh, scap, stage, ctx->d_error );
+      // Launched one by one, the boundary kernel goes first on the same stream: the sweep occupies
+      // every SM's registers, so a forked boundary kernel would only wait for it and add the latency of
+      // two cross-stream dependencies.  In a captured graph the fork below becomes two parallel
+      // branches, and the boundary kernel fills the SMs the sweep's last blocks leave idle.
+      if ( nt > 0 )
+      {
+         k_bnd_stencil< T, A, OP ><<< ( nt + 255 ) / 256, 256, 0, ctx->stream >>>( v, o, seg, a.flag, a.copy_unflagged, src, v1, v2, dst,
+                                                                                   A( a.a0 ), A( a.a1 ) );
+         ++ctx->launches;
+      }
+      // dynamic shared memory attribute set by ensure_constants
+      k_cell_sweep< T, A, OP ><<< v.nswarps[Cfg::BPS - 2] / kSwWarps, kSwWarps * 32, Cfg::smem_bytes, ctx->stream >>>(
+          v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ), nC, ctx->d_error );
+      ++ctx->launches;
+      check_cuda( cudaGetLastError(), "stencil launch" );
+      return;
+   }
+   // the cell kernel and the boundary kernel side by side on two streams
+   Fork fk( ctx );
+   if ( v.n >= 32 && nC > 0 && v.nswarps[Cfg::BPS - 2] > 0 )
+   {
+      k_cell_sweep< T, A, OP ><<< v.nswarps[Cfg::BPS - 2] / kSwWarps, kSwWarps * 32, Cfg::smem_bytes, ctx->stream >>>(
+          v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ), nC, ctx->d_error );
       ++ctx->launches;
    }
-   else if ( var == 4 && v.n >= 32 && v.nzblocks[1] > 0 && nC > 0 )
-   {
-      constexpr size_t smem = ZSCfg< T, zstream_aux< OP >() >::smem_bytes;  // attribute set by ensure_constants
-      k_cell_zsum< T, A, OP ><<< v.nzblocks[1], kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ),
-                                                                                  nC, ctx->d_error );
-      ++ctx->launches;
-   }
-   else if ( var >= 2 && v.n >= 32 && v.nzblocks[ZCfg< T, false >::wi] > 0 && nC > 0 )
-   {
-      constexpr size_t smem = ZCfg< T, zstream_aux< OP >() >::smem_bytes;  // attribute set by ensure_constants
-      k_cell_zstream< T, A, OP ><<< v.nzblocks[ZCfg< T, false >::wi], kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ),
-                                                                                 A( a.a1 ), nC, ctx->d_error );
-      ++ctx->launches;
-   }
-   else if ( var >= 1 && v.nmarch > 0 && nC > 0 )
+   else if ( v.nmarch > 0 && nC > 0 )
    {
       dim3 grid( ( v.nmarch + 7 ) / 8, nC );
-      k_cell_march< T, A, OP ><<< grid, 256, 0, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ),
-                                                                  march_prefetch_distance() );
+      k_cell_march< T, A, OP ><<< grid, 256, 0, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ) );
       ++ctx->launches;
    }
-   else if ( v.nrows > 0 && nC > 0 )
+   if ( nt > 0 )
    {
-      dim3 grid( ( v.nrows + 7 ) / 8, nC );
-      k_cell_stencil< T, A, OP ><<< grid, 256, 0, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ) );
-      ++ctx->launches;
-   }
-   if ( v.ntasks > 0 )
-   {
-      k_bnd_stencil< T, A, OP ><<< ( v.ntasks + 255 ) / 256, 256, 0, fk.aux() >>>( v, o, a.flag, a.copy_unflagged, src, v1, v2,
-                                                                                       dst, A( a.a0 ), A( a.a1 ) );
+      k_bnd_stencil< T, A, OP ><<< ( nt + 255 ) / 256, 256, 0, fk.aux() >>>( v, o, seg, a.flag, a.copy_unflagged, src, v1, v2, dst,
+                                                                             A( a.a0 ), A( a.a1 ) );
       ++ctx->launches;
    }
    check_cuda( cudaGetLastError(), "stencil launch" );
@@ -1831,8 +1366,10 @@ static double* partials( Context* ctx, int count )
 {
    if ( count > ctx->partial_cap )
    {
-      if ( ctx->d_partials ) check_cuda( cudaFree( ctx->d_partials ), "cudaFree(partials)" );
-      ctx->partial_cap = std::max( count, 1 << 16 );
+      // a captured graph may still read the old buffer: keep it until the context goes away
+      if ( ctx->d_partials ) ctx->retired.push_back( ctx->d_partials ), ctx->retired_bytes += int64_t( ctx->partial_cap ) * 8;
+      ctx->d_partials  = nullptr;
+      ctx->partial_cap = std::max( { count, 1 << 16, 2 * ctx->partial_cap } );
       check_cuda( cudaMalloc( &ctx->d_partials, sizeof( double ) * ctx->partial_cap ), "cudaMalloc(partials)" );
    }
    return ctx->d_partials;
@@ -1882,9 +1419,9 @@ void launch_dot( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const v
 // device synchronisation of cudaMalloc/cudaFree.  launch_dot grows the context's partials buffer
 // on demand; this variant runs the same dot kernels but keeps the per-block partial sums and the
 // result in one file-scope device array of fixed size.
-//  * set-up: the first call on a device (that device current) resolves the array's address once
-//    with cudaGetSymbolAddress, and the first call in the process also uploads the constant tables;
-//    make that first call before any stream capture.
+//  * set-up: the library's per-device set-up (run by the first operation on a device, with that
+//    device current) resolves the array's address once with cudaGetSymbolAddress, together with the
+//    constant tables; this entry point refuses to run before it, so it never loads or allocates.
 //  * limit: at most kNoAllocPartials block partials (cell-row blocks plus boundary blocks of the
 //    level); larger levels are rejected with an error.
 //  * nothing has to start at zero: every block of the sweep writes its own partial and the final
@@ -1941,7 +1478,11 @@ void launch_dot_noalloc( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag,
    if ( it == m->levels.end() || !it->second->d_off )
       throw std::invalid_argument( "allocation-free dot: the level's index tables are not on the device yet "
                                    "(run any operation on this level first)" );
-   ensure_constants();
+   // no set-up here: constant tables, kernel attributes and the scratch address were prepared by an
+   // earlier operation on this device (loading them now could allocate device memory)
+   if ( !g_const_once.done_on_current_device() )
+      throw std::invalid_argument( "allocation-free dot: no operation of this library has run on this device yet "
+                                   "(run one first, for example an apply on this level)" );
    double*         scratch  = noalloc_scratch( ctx->device );
    const LevelView v        = make_view( m, L );
    const int       nC       = m->topo.nC;
@@ -2168,101 +1709,101 @@ __constant__ double      c_p2r_w[kP2RMax];
 
 static void ensure_p2_transfer_tables()
 {
-   static bool done = false;
-   if ( done ) return;
-   // micro-cell types (vertex offsets), the same table as the refinement itself
-   static const int mc[6][4][3] = { { { 0, 0, 0 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } }, { { 1, 0, 0 }, { 1, 1, 0 }, { 0, 1, 0 }, { 1, 0, 1 } },
-                                    { { 1, 0, 0 }, { 0, 1, 0 }, { 1, 0, 1 }, { 0, 0, 1 } }, { { 1, 1, 0 }, { 1, 1, 1 }, { 0, 1, 1 }, { 1, 0, 1 } },
-                                    { { 1, 0, 1 }, { 0, 1, 1 }, { 0, 0, 1 }, { 0, 1, 0 } }, { { 0, 1, 0 }, { 1, 1, 0 }, { 1, 0, 1 }, { 0, 1, 1 } } };
-   static const int ed[6][2] = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
-   int              pn[64];
-   signed char      po[64][10][3] = {};
-   double           pw[64][10]    = {};
-   for ( int pat = 0; pat < 64; ++pat )
-   {
-      const int r[3] = { pat & 3, ( pat >> 2 ) & 3, pat >> 4 };
-      const int F[3] = { 4 + r[0], 4 + r[1], 4 + r[2] }, A[3] = { 1, 1, 1 };
-      bool      found = false;
-      for ( int e = 0; e < 8 && !found; ++e )
-      {
-         const int a[3] = { A[0] - ( e & 1 ), A[1] - ( ( e >> 1 ) & 1 ), A[2] - ( e >> 2 ) };
-         for ( int ty = 0; ty < 6 && !found; ++ty )
-         {
-            // barycentric coordinates x4 from the unimodular offset matrix (integer inverse)
-            int E[3][3];
-            for ( int i = 0; i < 3; ++i )
-               for ( int k = 0; k < 3; ++k ) E[i][k] = mc[ty][k + 1][i] - mc[ty][0][i];
-            const int det = E[0][0] * ( E[1][1] * E[2][2] - E[1][2] * E[2][1] ) - E[0][1] * ( E[1][0] * E[2][2] - E[1][2] * E[2][0] ) +
-                            E[0][2] * ( E[1][0] * E[2][1] - E[1][1] * E[2][0] );
-            const int inv[3][3] = { { ( E[1][1] * E[2][2] - E[1][2] * E[2][1] ) * det, ( E[0][2] * E[2][1] - E[0][1] * E[2][2] ) * det,
-                                      ( E[0][1] * E[1][2] - E[0][2] * E[1][1] ) * det },
-                                    { ( E[1][2] * E[2][0] - E[1][0] * E[2][2] ) * det, ( E[0][0] * E[2][2] - E[0][2] * E[2][0] ) * det,
-                                      ( E[0][2] * E[1][0] - E[0][0] * E[1][2] ) * det },
-                                    { ( E[1][0] * E[2][1] - E[1][1] * E[2][0] ) * det, ( E[0][1] * E[2][0] - E[0][0] * E[2][1] ) * det,
-                                      ( E[0][0] * E[1][1] - E[0][1] * E[1][0] ) * det } };  // det = +-1
-            int rel[3];
-            for ( int i = 0; i < 3; ++i ) rel[i] = F[i] - 4 * ( a[i] + mc[ty][0][i] );
-            int mu4[4] = { 4, 0, 0, 0 };
-            for ( int k = 0; k < 3; ++k )
-            {
-               mu4[k + 1] = inv[k][0] * rel[0] + inv[k][1] * rel[1] + inv[k][2] * rel[2];
-               mu4[0] -= mu4[k + 1];
-            }
-            bool inside = true;
-            for ( int k = 0; k < 4; ++k ) inside &= mu4[k] >= 0 && mu4[k] <= 4;
-            if ( !inside ) continue;
-            found = true;
-            double mu[4], N[10];
-            int    node[10][3];
-            for ( int k = 0; k < 4; ++k ) mu[k] = mu4[k] / 4.0;
-            for ( int k = 0; k < 4; ++k )
-            {
-               N[k] = mu[k] * ( 2.0 * mu[k] - 1.0 );
-               for ( int i = 0; i < 3; ++i ) node[k][i] = 2 * ( a[i] + mc[ty][k][i] );
-            }
-            for ( int k = 0; k < 6; ++k )
-            {
-               N[4 + k] = 4.0 * mu[ed[k][0]] * mu[ed[k][1]];
-               for ( int i = 0; i < 3; ++i ) node[4 + k][i] = ( node[ed[k][0]][i] + node[ed[k][1]][i] ) / 2;
-            }
-            pn[pat] = 0;
-            for ( int k = 0; k < 10; ++k )
-               if ( N[k] != 0.0 )
-               {
-                  for ( int i = 0; i < 3; ++i ) po[pat][pn[pat]][i] = static_cast< signed char >( node[k][i] - 2 * A[i] );
-                  pw[pat][pn[pat]++] = N[k];
-               }
-         }
-      }
-      if ( !found ) throw std::logic_error( "P2 transfer table: no micro-cell contains a fine node" );
-   }
-   // restriction stencils: class p = J mod 2, entries (d = r - 2 o, w)
-   int         begin[9] = {};
-   signed char rd[kP2RMax][3];
-   double      rw[kP2RMax];
-   int         cnt = 0;
-   for ( int p = 0; p < 8; ++p )
-   {
-      begin[p] = cnt;
+   static PerDeviceOnce once;
+   once.run( [] {
+      // micro-cell types (vertex offsets), the same table as the refinement itself
+      static const int mc[6][4][3] = { { { 0, 0, 0 }, { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } }, { { 1, 0, 0 }, { 1, 1, 0 }, { 0, 1, 0 }, { 1, 0, 1 } },
+                                       { { 1, 0, 0 }, { 0, 1, 0 }, { 1, 0, 1 }, { 0, 0, 1 } }, { { 1, 1, 0 }, { 1, 1, 1 }, { 0, 1, 1 }, { 1, 0, 1 } },
+                                       { { 1, 0, 1 }, { 0, 1, 1 }, { 0, 0, 1 }, { 0, 1, 0 } }, { { 0, 1, 0 }, { 1, 1, 0 }, { 1, 0, 1 }, { 0, 1, 1 } } };
+      static const int ed[6][2] = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
+      int              pn[64];
+      signed char      po[64][10][3] = {};
+      double           pw[64][10]    = {};
       for ( int pat = 0; pat < 64; ++pat )
-         for ( int k = 0; k < pn[pat]; ++k )
+      {
+         const int r[3] = { pat & 3, ( pat >> 2 ) & 3, pat >> 4 };
+         const int F[3] = { 4 + r[0], 4 + r[1], 4 + r[2] }, A[3] = { 1, 1, 1 };
+         bool      found = false;
+         for ( int e = 0; e < 8 && !found; ++e )
          {
-            const int o[3] = { po[pat][k][0], po[pat][k][1], po[pat][k][2] };
-            if ( ( ( o[0] & 1 ) | ( ( o[1] & 1 ) << 1 ) | ( ( o[2] & 1 ) << 2 ) ) != p ) continue;
-            if ( cnt >= kP2RMax ) throw std::logic_error( "P2 restriction stencil table overflow" );
-            const int r[3] = { pat & 3, ( pat >> 2 ) & 3, pat >> 4 };
-            for ( int i = 0; i < 3; ++i ) rd[cnt][i] = static_cast< signed char >( r[i] - 2 * o[i] );
-            rw[cnt++] = pw[pat][k];
+            const int a[3] = { A[0] - ( e & 1 ), A[1] - ( ( e >> 1 ) & 1 ), A[2] - ( e >> 2 ) };
+            for ( int ty = 0; ty < 6 && !found; ++ty )
+            {
+               // barycentric coordinates x4 from the unimodular offset matrix (integer inverse)
+               int E[3][3];
+               for ( int i = 0; i < 3; ++i )
+                  for ( int k = 0; k < 3; ++k ) E[i][k] = mc[ty][k + 1][i] - mc[ty][0][i];
+               const int det = E[0][0] * ( E[1][1] * E[2][2] - E[1][2] * E[2][1] ) - E[0][1] * ( E[1][0] * E[2][2] - E[1][2] * E[2][0] ) +
+                               E[0][2] * ( E[1][0] * E[2][1] - E[1][1] * E[2][0] );
+               const int inv[3][3] = { { ( E[1][1] * E[2][2] - E[1][2] * E[2][1] ) * det, ( E[0][2] * E[2][1] - E[0][1] * E[2][2] ) * det,
+                                         ( E[0][1] * E[1][2] - E[0][2] * E[1][1] ) * det },
+                                       { ( E[1][2] * E[2][0] - E[1][0] * E[2][2] ) * det, ( E[0][0] * E[2][2] - E[0][2] * E[2][0] ) * det,
+                                         ( E[0][2] * E[1][0] - E[0][0] * E[1][2] ) * det },
+                                       { ( E[1][0] * E[2][1] - E[1][1] * E[2][0] ) * det, ( E[0][1] * E[2][0] - E[0][0] * E[2][1] ) * det,
+                                         ( E[0][0] * E[1][1] - E[0][1] * E[1][0] ) * det } };  // det = +-1
+               int rel[3];
+               for ( int i = 0; i < 3; ++i ) rel[i] = F[i] - 4 * ( a[i] + mc[ty][0][i] );
+               int mu4[4] = { 4, 0, 0, 0 };
+               for ( int k = 0; k < 3; ++k )
+               {
+                  mu4[k + 1] = inv[k][0] * rel[0] + inv[k][1] * rel[1] + inv[k][2] * rel[2];
+                  mu4[0] -= mu4[k + 1];
+               }
+               bool inside = true;
+               for ( int k = 0; k < 4; ++k ) inside &= mu4[k] >= 0 && mu4[k] <= 4;
+               if ( !inside ) continue;
+               found = true;
+               double mu[4], N[10];
+               int    node[10][3];
+               for ( int k = 0; k < 4; ++k ) mu[k] = mu4[k] / 4.0;
+               for ( int k = 0; k < 4; ++k )
+               {
+                  N[k] = mu[k] * ( 2.0 * mu[k] - 1.0 );
+                  for ( int i = 0; i < 3; ++i ) node[k][i] = 2 * ( a[i] + mc[ty][k][i] );
+               }
+               for ( int k = 0; k < 6; ++k )
+               {
+                  N[4 + k] = 4.0 * mu[ed[k][0]] * mu[ed[k][1]];
+                  for ( int i = 0; i < 3; ++i ) node[4 + k][i] = ( node[ed[k][0]][i] + node[ed[k][1]][i] ) / 2;
+               }
+               pn[pat] = 0;
+               for ( int k = 0; k < 10; ++k )
+                  if ( N[k] != 0.0 )
+                  {
+                     for ( int i = 0; i < 3; ++i ) po[pat][pn[pat]][i] = static_cast< signed char >( node[k][i] - 2 * A[i] );
+                     pw[pat][pn[pat]++] = N[k];
+                  }
+            }
          }
-   }
-   begin[8] = cnt;
-   check_cuda( cudaMemcpyToSymbol( c_p2p_n, pn, sizeof( pn ) ), "P2 transfer tables" );
-   check_cuda( cudaMemcpyToSymbol( c_p2p_o, po, sizeof( po ) ), "P2 transfer tables" );
-   check_cuda( cudaMemcpyToSymbol( c_p2p_w, pw, sizeof( pw ) ), "P2 transfer tables" );
-   check_cuda( cudaMemcpyToSymbol( c_p2r_begin, begin, sizeof( begin ) ), "P2 transfer tables" );
-   check_cuda( cudaMemcpyToSymbol( c_p2r_d, rd, sizeof( rd ) ), "P2 transfer tables" );
-   check_cuda( cudaMemcpyToSymbol( c_p2r_w, rw, sizeof( rw ) ), "P2 transfer tables" );
-   done = true;
+         if ( !found ) throw std::logic_error( "P2 transfer table: no micro-cell contains a fine node" );
+      }
+      // restriction stencils: class p = J mod 2, entries (d = r - 2 o, w)
+      int         begin[9] = {};
+      signed char rd[kP2RMax][3];
+      double      rw[kP2RMax];
+      int         cnt = 0;
+      for ( int p = 0; p < 8; ++p )
+      {
+         begin[p] = cnt;
+         for ( int pat = 0; pat < 64; ++pat )
+            for ( int k = 0; k < pn[pat]; ++k )
+            {
+               const int o[3] = { po[pat][k][0], po[pat][k][1], po[pat][k][2] };
+               if ( ( ( o[0] & 1 ) | ( ( o[1] & 1 ) << 1 ) | ( ( o[2] & 1 ) << 2 ) ) != p ) continue;
+               if ( cnt >= kP2RMax ) throw std::logic_error( "P2 restriction stencil table overflow" );
+               const int r[3] = { pat & 3, ( pat >> 2 ) & 3, pat >> 4 };
+               for ( int i = 0; i < 3; ++i ) rd[cnt][i] = static_cast< signed char >( r[i] - 2 * o[i] );
+               rw[cnt++] = pw[pat][k];
+            }
+      }
+      begin[8] = cnt;
+      check_cuda( cudaMemcpyToSymbol( c_p2p_n, pn, sizeof( pn ) ), "P2 transfer tables" );
+      check_cuda( cudaMemcpyToSymbol( c_p2p_o, po, sizeof( po ) ), "P2 transfer tables" );
+      check_cuda( cudaMemcpyToSymbol( c_p2p_w, pw, sizeof( pw ) ), "P2 transfer tables" );
+      check_cuda( cudaMemcpyToSymbol( c_p2r_begin, begin, sizeof( begin ) ), "P2 transfer tables" );
+      check_cuda( cudaMemcpyToSymbol( c_p2r_d, rd, sizeof( rd ) ), "P2 transfer tables" );
+      check_cuda( cudaMemcpyToSymbol( c_p2r_w, rw, sizeof( rw ) ), "P2 transfer tables" );
+   } );
 }
 
 // coarse quadratic at fine cell-local node (x, y, z); nc = coarse storage micro-edges per edge
@@ -2529,10 +2070,11 @@ static double* sor_scratch( Context* ctx, int64_t ntasks )
 {
    if ( ctx->sor_cap < ntasks )
    {
-      if ( ctx->d_sor ) check_cuda( cudaFree( ctx->d_sor ), "cudaFree(SOR scratch)" );
-      ctx->d_sor = nullptr;
-      check_cuda( cudaMalloc( &ctx->d_sor, size_t( ntasks ) * sizeof( double ) ), "cudaMalloc(SOR scratch)" );
-      ctx->sor_cap = ntasks;
+      // a captured graph may still read the old buffer: keep it until the context goes away
+      if ( ctx->d_sor ) ctx->retired.push_back( ctx->d_sor ), ctx->retired_bytes += ctx->sor_cap * 8;
+      ctx->d_sor   = nullptr;
+      ctx->sor_cap = std::max( ntasks, 2 * ctx->sor_cap );
+      check_cuda( cudaMalloc( &ctx->d_sor, size_t( ctx->sor_cap ) * sizeof( double ) ), "cudaMalloc(SOR scratch)" );
    }
    return ctx->d_sor;
 }

@@ -317,135 +317,70 @@ void build_level( Mesh* m, int L )
    m->levels[L] = std::move( lv );
 }
 
-// Work units of the z-streamed sweeps.  A unit is the tile x0..x0+63, y0..y0+kZHeights[wi]-1 of slices
-// z_first..z_last (interior points only: x, y, z >= 1, x+y+z <= n-1).  The slice range is cut into
-// chunks of zc slices, zc the largest power of two in [8, 32] that still gives at least one unit
-// per two blocks (every chunk re-reads two halo slices, and every slice load costs a fixed hand-off,
-// so long chunks win over finer balance); units are then handed out longest-first to the least
-// loaded block.
-void build_zunits( P1Level& P, int nblocks, int wi, int ncells )
+// Work of the cell-interior sweep.  A unit is the tile x0..x0+kSwTX-1, y0..y0+kSwR-1 of the
+// slices z_first..z_last of one macro-cell (interior points only: x, y, z >= 1, x+y+z <= n-1).  From
+// the slice on which every row of the tile ends within 32 points of x0 the tile is half-width (one
+// point per lane).  Each tile column's slice range (full-width and half-width parts separately) is
+// cut into equal chunks of at most 32 slices: every chunk reads two halo slices, so longer chunks
+// cost fewer re-reads, and 32 slices still give every warp a few units on the level-8 cube.  The
+// units of all cells are dealt longest-first to the least loaded of the launch's nwarps warps (cost:
+// slice steps, a half-width step counted as 0.6), and each warp's list is ordered by cell, so a warp
+// reloads its cell's stencil only when the cell changes.
+
+void build_sweep_units( P1Level& P, int b, int nwarps, int ncells )
 {
-   const int n = P.n, kZTileX = kZWidths[wi], kTY = kZHeights[wi];
-   auto&     zunits = P.zunits[wi];
-   auto&     zcell  = P.zcell[wi];
-   auto&     zbegin = P.zbegin[wi];
-   zunits.clear();
-   zcell.clear();
-   zbegin.assign( 1, 0 );
-   if ( n < 4 || ncells < 1 ) return;
+   const int n     = P.n;
+   auto&     units = P.swunits[b];
+   auto&     cells = P.swcell[b];
+   auto&     begin = P.swbegin[b];
+   units.clear();
+   cells.clear();
+   begin.assign( 1, 0 );
+   if ( n < 4 || ncells < 1 || nwarps < 1 ) return;
    struct Unit
    {
       std::array< int, 4 > u;
-      int64_t              work;
+      double               work;
    };
-   auto make = [&]( int zc ) {
-      std::vector< Unit > us;
-      for ( int y0 = 1; y0 <= n - 3; y0 += kTY )
-         for ( int x0 = 1; x0 + y0 <= n - 2; x0 += kZTileX )
+   std::vector< Unit > us;
+   for ( int y0 = 1; y0 <= n - 3; y0 += kSwR )
+      for ( int x0 = 1; x0 + y0 <= n - 2; x0 += kSwTX )
+      {
+         const int zmax = n - 1 - x0 - y0;
+         // row y0, the longest of the tile, has n - y0 - z - x0 interior points from x0 on
+         const int zh = kSwTX > 32 ? std::max( 1, n - y0 - x0 - 32 ) : zmax + 1;
+         for ( int part = 0; part < 2; ++part )
          {
-            const int zmax = n - 1 - x0 - y0;
-            // from slice zh on, every row of the tile ends within its first 32 points (row y0, the
-            // longest, has n - y0 - z - x0 interior points from x0 on): those slices form half-width
-            // units, run with one point per lane
-            const int zh = kZTileX > 32 ? std::max( 1, n - y0 - x0 - 32 ) : zmax + 1;
-            for ( int part = 0; part < 2; ++part )
+            const int lo = part == 0 ? 1 : zh, hi = part == 0 ? std::min( zmax, zh - 1 ) : zmax;
+            if ( hi < lo ) continue;
+            const int len = hi - lo + 1, nch = ( len + 31 ) / 32;
+            for ( int k = 0; k < nch; ++k )
             {
-               const int lo = part == 0 ? 1 : std::max( 1, zh ), hi = part == 0 ? std::min( zmax, zh - 1 ) : zmax;
-               for ( int za = lo; za <= hi; za += zc )
-               {
-                  // cost: the slice steps of the unit (its slices plus the two halo slices and the
-                  // prologue) times the points per lane; every step issues the whole tile, clipped
-                  // lanes included, so the number of interior points would underestimate the units
-                  // along the diagonal
-                  const int zb = std::min( hi, za + zc - 1 );
-                  us.push_back( { { part ? ( x0 | kZUnitHalf ) : x0, y0, za, zb }, int64_t( zb - za + 3 ) * ( part ? 1 : 2 ) } );
-               }
+               const int za = lo + int( int64_t( len ) * k / nch ), zb = lo + int( int64_t( len ) * ( k + 1 ) / nch ) - 1;
+               us.push_back( { { part ? ( x0 | kSwUnitHalf ) : x0, y0, za, zb }, double( zb - za + 3 ) * ( part ? 0.6 : 1.0 ) } );
             }
          }
-      return us;
-   };
-   // longest slice ranges that still give every block about two units (all cells together)
-   int                 zc = 32;
-   std::vector< Unit > us = make( zc );
-   while ( zc > 8 && 2 * int64_t( us.size() ) * ncells < int64_t( nblocks ) ) us = make( zc /= 2 );
-   if ( const char* e = getenv( "HYB_ZCHUNK" ); e && atoi( e ) > 0 ) us = make( atoi( e ) );
-   std::stable_sort( us.begin(), us.end(), []( const Unit& a, const Unit& b ) { return a.work > b.work; } );
-   const int64_t items = int64_t( us.size() ) * ncells;
-   const int     nb    = int( std::max< int64_t >( 1, std::min< int64_t >( nblocks, items ) ) );
-   std::vector< std::vector< std::pair< int, int > > >                                      per( nb );  // (cell, unit)
-   std::priority_queue< std::pair< int64_t, int >, std::vector< std::pair< int64_t, int > >, std::greater<> > heap;
-   for ( int b = 0; b < nb; ++b ) heap.push( { 0, b } );
+      }
+   std::stable_sort( us.begin(), us.end(), []( const Unit& a, const Unit& c ) { return a.work > c.work; } );
+   std::vector< std::vector< std::pair< int, int > > > per( nwarps );  // (cell, unit)
+   std::priority_queue< std::pair< double, int >, std::vector< std::pair< double, int > >, std::greater<> > heap;
+   for ( int w = 0; w < nwarps; ++w ) heap.push( { 0.0, w } );
    for ( size_t k = 0; k < us.size(); ++k )  // longest first; the cells of one unit shape in turn
       for ( int c = 0; c < ncells; ++c )
       {
-         auto [load, b] = heap.top();
+         auto [load, w] = heap.top();
          heap.pop();
-         per[b].push_back( { c, int( k ) } );
-         heap.push( { load + us[k].work, b } );
+         per[w].push_back( { c, int( k ) } );
+         heap.push( { load + us[k].work, w } );
       }
-   for ( int b = 0; b < nb; ++b )
+   for ( int w = 0; w < nwarps; ++w )
    {
-      // cell-major inside a block: a warp reloads its cell's weights only when the cell changes
-      std::stable_sort( per[b].begin(), per[b].end(), []( const auto& a, const auto& b ) { return a.first < b.first; } );
-      for ( const auto& cu : per[b] )
+      std::stable_sort( per[w].begin(), per[w].end(), []( const auto& a, const auto& c ) { return a.first < c.first; } );
+      for ( const auto& cu : per[w] )
       {
-         zunits.push_back( us[cu.second].u );
-         zcell.push_back( cu.first );
+         units.push_back( us[cu.second].u );
+         cells.push_back( cu.first );
       }
-      zbegin.push_back( int( zunits.size() ) );
-   }
-}
-
-// Work units of the full-row sweep: the rows y0..y0+ty-1 (interior rows only) of slices
-// z_first..z_last, ty = 1 << h; chunking of the slice range and longest-first assignment as for the
-// tiled sweep.
-void build_runits( P1Level& P, int nblocks, int h )
-{
-   const int n = P.n, ty = 1 << h;
-   auto&     units = P.runits[h];
-   auto&     begin = P.rbegin[h];
-   units.clear();
-   begin.assign( 1, 0 );
-   if ( n < 4 ) return;
-   struct Unit
-   {
-      std::array< int, 4 > u;
-      int64_t              work;
-   };
-   auto make = [&]( int zc ) {
-      std::vector< Unit > us;
-      for ( int y0 = 1; y0 <= n - 3; y0 += ty )
-      {
-         const int zmax = n - 2 - y0;
-         for ( int za = 1; za <= zmax; za += zc )
-         {
-            const int zb = std::min( zmax, za + zc - 1 );
-            int64_t   w  = 0;
-            for ( int z = za; z <= zb; ++z )
-               for ( int y = y0; y < y0 + ty; ++y ) w += std::max( 0, n - 1 - y - z );
-            us.push_back( { { ty, y0, za, zb }, w } );
-         }
-      }
-      return us;
-   };
-   int                 zc = 32;
-   std::vector< Unit > us = make( zc );
-   while ( zc > 4 && 2 * int64_t( us.size() ) < int64_t( nblocks ) ) us = make( zc /= 2 );
-   std::stable_sort( us.begin(), us.end(), []( const Unit& a, const Unit& b ) { return a.work > b.work; } );
-   const int nb = std::max( 1, std::min( nblocks, int( us.size() ) ) );
-   std::vector< std::vector< std::array< int, 4 > > >                                       per( nb );
-   std::priority_queue< std::pair< int64_t, int >, std::vector< std::pair< int64_t, int > >, std::greater<> > heap;
-   for ( int b = 0; b < nb; ++b ) heap.push( { 0, b } );
-   for ( const Unit& u : us )
-   {
-      auto [load, b] = heap.top();
-      heap.pop();
-      per[b].push_back( u.u );
-      heap.push( { load + u.work, b } );
-   }
-   for ( int b = 0; b < nb; ++b )
-   {
-      for ( const auto& u : per[b] ) units.push_back( u );
       begin.push_back( int( units.size() ) );
    }
 }
@@ -472,6 +407,25 @@ void ensure_device( Mesh* m, P1Level& P )
    std::vector< int4 > tk( P.tasks.size() );
    for ( size_t i = 0; i < tk.size(); ++i ) tk[i] = make_int4( P.tasks[i][0], P.tasks[i][1], P.tasks[i][2], 0 );
    up( &P.d_tasks, tk.data(), tk.size() );
+   {
+      // the tasks grouped by the boundary type of their primitive (order kept inside a group), so
+      // that a stencil operation launches only the groups its flag selects
+      const uint32_t      type_bit[4] = { kInner, kDirichlet, kNeumann, kFreeslip };
+      std::vector< int4 > bt;
+      for ( int g = 0; g < 4; ++g )
+      {
+         P.bcount[g] = 0;
+         for ( const int4& q : tk )
+         {
+            const int      b  = q.x;
+            const uint32_t ty = b < t.nV ? t.bc( t.flag_v[b] )
+                                         : ( b < t.nV + t.nE ? t.bc( t.flag_e[b - t.nV] ) : t.bc( t.flag_f[b - t.nV - t.nE] ) );
+            if ( ty == type_bit[g] ) bt.push_back( q ), ++P.bcount[g];
+         }
+      }
+      if ( bt.size() != tk.size() ) throw std::logic_error( "boundary task without a single boundary type" );
+      up( &P.d_btasks, bt.data(), bt.size() );
+   }
    std::vector< int2 > rw( P.rows.size() );
    for ( size_t i = 0; i < rw.size(); ++i ) rw[i] = make_int2( P.rows[i][0], P.rows[i][1] );
    up( &P.d_rows, rw.data(), rw.size() );
@@ -481,24 +435,16 @@ void ensure_device( Mesh* m, P1Level& P )
    int dev = 0, sms = 0;
    check_cuda( cudaGetDevice( &dev ), "cudaGetDevice" );
    check_cuda( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev ), "device attribute" );
-   for ( int h = 0; h < 4; ++h )
+   for ( int b = 0; b < kSwLists; ++b )
    {
-      build_runits( P, 2 * std::max( sms, 1 ), h );
-      const auto&         U = P.runits[h];
-      std::vector< int4 > ru( U.size() );
-      for ( size_t i = 0; i < ru.size(); ++i ) ru[i] = make_int4( U[i][0], U[i][1], U[i][2], U[i][3] );
-      up( &P.d_runits[h], ru.data(), ru.size() );
-      up( &P.d_rbegin[h], P.rbegin[h].data(), P.rbegin[h].size() );
-   }
-   for ( int wi = 0; wi < 2; ++wi )
-   {
-      build_zunits( P, 2 * std::max( sms, 1 ), wi, t.nC );
-      const auto&         U = P.zunits[wi];
-      std::vector< int4 > zu( U.size() );
-      for ( size_t i = 0; i < zu.size(); ++i ) zu[i] = make_int4( U[i][0], U[i][1], U[i][2], U[i][3] );
-      up( &P.d_zunits[wi], zu.data(), zu.size() );
-      up( &P.d_zcell[wi], P.zcell[wi].data(), P.zcell[wi].size() );
-      up( &P.d_zbegin[wi], P.zbegin[wi].data(), P.zbegin[wi].size() );
+      // one list set per blocks-per-SM count (b + 2) of the sweep's instantiations
+      build_sweep_units( P, b, sms * ( b + 2 ) * kSwWarps, t.nC );
+      const auto&         U = P.swunits[b];
+      std::vector< int4 > su( U.size() );
+      for ( size_t i = 0; i < su.size(); ++i ) su[i] = make_int4( U[i][0], U[i][1], U[i][2], U[i][3] );
+      up( &P.d_swunits[b], su.data(), su.size() );
+      up( &P.d_swcell[b], P.swcell[b].data(), P.swcell[b].size() );
+      up( &P.d_swbegin[b], P.swbegin[b].data(), P.swbegin[b].size() );
    }
    std::vector< uint8_t > bc( nP );
    std::vector< int8_t >  bk( P.nB );
@@ -541,10 +487,10 @@ Mesh::~Mesh()
       cudaFree( P.d_inc_begin );
       cudaFree( P.d_inc );
       cudaFree( P.d_tasks );
+      cudaFree( P.d_btasks );
       cudaFree( P.d_rows );
       cudaFree( P.d_march );
-      for ( int wi = 0; wi < 2; ++wi ) cudaFree( P.d_zunits[wi] ), cudaFree( P.d_zcell[wi] ), cudaFree( P.d_zbegin[wi] );
-      for ( int h = 0; h < 4; ++h ) cudaFree( P.d_runits[h] ), cudaFree( P.d_rbegin[h] );
+      for ( int b = 0; b < kSwLists; ++b ) cudaFree( P.d_swunits[b] ), cudaFree( P.d_swcell[b] ), cudaFree( P.d_swbegin[b] );
       cudaFree( P.d_bc );
       cudaFree( P.d_bkind );
       cudaFree( P.d_ncell_cls );

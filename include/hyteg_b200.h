@@ -101,6 +101,9 @@ int hyb_ctx_synchronize( hyb_ctx* ctx );
 int hyb_ctx_launch_count( const hyb_ctx* ctx, int64_t* out );
 /* the context's stream (cudaStream_t) */
 int hyb_ctx_stream( const hyb_ctx* ctx, void** stream );
+/* bytes of device scratch the context holds (reduction partials, smoother scratch, transfer staging,
+ * buffers kept for captured graphs); no counterpart in the reference */
+int hyb_ctx_scratch_bytes( const hyb_ctx* ctx, int64_t* out );
 
 /* ---------------------------------------------------------------- macro mesh and primitive storage
  * Replaces MeshInfo (src/hyteg/mesh/MeshInfo.hpp:221,512,562) + SetupPrimitiveStorage
@@ -192,8 +195,9 @@ int hyb_fn_dot( hyb_fn* a, hyb_fn* b, int level, uint32_t flag, double* out );
 /* Allocation-free hyb_fn_dot (no counterpart in the reference): the same deterministic kernels and
  * result, with the per-block partial sums in a fixed file-scope device array (65536 partials, 512 KiB)
  * instead of a buffer grown with cudaMalloc, for callers whose device memory is reserved up front by
- * their own allocator.  The first call on a device resolves the array's address (make it before
- * any stream capture).  The level's index tables must already be on the device (any earlier
+ * their own allocator.  The array's address is resolved by the library's per-device set-up, which
+ * the first operation of any kind on a device runs; before that this entry point returns HYB_EINVAL
+ * rather than load anything.  The level's index tables must already be on the device (any earlier
  * operation on that level puts them there).  Levels needing more partials return HYB_EINVAL.  The
  * array is shared per device: overlapping calls race and must be serialised by the caller. */
 int hyb_fn_dot_noalloc( hyb_fn* a, hyb_fn* b, int level, uint32_t flag, double* out );
@@ -278,6 +282,11 @@ int hyb_gmg_set_radii( hyb_gmg* gmg, const double* radii );
 int hyb_gmg_get_radii( hyb_gmg* gmg, double* radii );
 /* Solver::solve(A, x, b, level) (solvers/Solver.hpp:31-35): one multigrid cycle */
 int hyb_gmg_solve( hyb_gmg* gmg, hyb_fn* x, hyb_fn* b, int level );
+/* the solver's smoother alone on one level above the coarsest: `iterations` applications of
+ * ChebyshevSmoother::solve (solvers/ChebyshevSmoother.hpp:112-240), WeightedJacobiSmoother::solve
+ * (WeightedJacobiSmoother.hpp:46-66) or the Gauss-Seidel / SOR smoother, with the solver's
+ * coefficients for that level */
+int hyb_gmg_smooth( hyb_gmg* gmg, hyb_fn* x, hyb_fn* b, int level, int iterations );
 /* up to max_cycles cycles until ||r||/||r0|| < rtol (discrete L2 over non-Dirichlet DoFs);
  * res_history receives ||r_0|| .. ||r_k|| (max_cycles+1 entries) */
 int hyb_gmg_solve_cycles( hyb_gmg* gmg, hyb_fn* x, hyb_fn* b, int level, int max_cycles, double rtol, double* res_history,

@@ -120,12 +120,15 @@ def face_index(n, i, j):
 
 def tet_points(w):
     """All (x, y, z) with x+y+z <= w-1, in HyTeG memory order (z-major, then y, then x)."""
-    pts = []
-    for z in range(w):
-        for y in range(w - z):
-            for x in range(w - z - y):
-                pts.append((x, y, z))
-    return np.array(pts, dtype=np.int64).reshape(-1, 3)
+    if w <= 0:
+        return np.zeros((0, 3), dtype=np.int64)
+    zr = np.repeat(np.arange(w, dtype=np.int64), w - np.arange(w))  # one entry per row (y, z)
+    yr = np.concatenate([np.arange(w - z, dtype=np.int64) for z in range(w)])
+    lens = w - zr - yr
+    z = np.repeat(zr, lens)
+    y = np.repeat(yr, lens)
+    x = np.arange(z.size, dtype=np.int64) - np.repeat(np.cumsum(lens) - lens, lens)
+    return np.stack([x, y, z], axis=1)
 
 
 class MacroMesh:
@@ -770,6 +773,136 @@ def residual_norm(op, x, b, L, flag=INNER | NEUMANN | FREESLIP):
     mask = lev.owned_mask(flag)
     r[mask] = b[mask] - r[mask]
     return math.sqrt(dot(lev, r, r, flag))
+
+
+# ---------------------------------------------------------------------------------------------
+# constant-stencil operator on one large level, without a global matrix
+# ---------------------------------------------------------------------------------------------
+def _face_mask(n, x, y, z):
+    """Which macro-cell faces a cell-local point lies on: bit 0 z = 0, bit 1 y = 0, bit 2 x = 0,
+    bit 3 x + y + z = n."""
+    return (z == 0) * 1 + (y == 0) * 2 + (x == 0) * 4 + (x + y + z == n) * 8
+
+
+def _mask_point(n, mask):
+    """A cell-local point on exactly the faces of `mask` (n >= 4)."""
+    fixed = [bool(mask & 4), bool(mask & 2), bool(mask & 1)]  # x, y, z pinned to 0
+    p = [0 if f else 1 for f in fixed]
+    if mask & 8:
+        free = [i for i in range(3) if not fixed[i]]
+        p[free[-1]] = n - (len(free) - 1)
+    return np.array(p, dtype=np.int64)
+
+
+def cell_stencils_by_mask(mesh: MacroMesh, c, L, element=p1_laplace_element):
+    """calculateStencilInMacroCellForm_new (P1Elements.hpp:466-529) for macro-cell c: for every face
+    set `mask` a cell point can lie on, the 15 stencil weights (centre, then STENCIL_DIRS), each the
+    sum of the element-matrix entries K[k, j] of the micro-cells of the cell that contain the point as
+    their vertex k and the neighbour as vertex j.  The cell is affine, so all points with the same
+    face set share the stencil.  Returns a (16, 15) array indexed by mask."""
+    n = 1 << L
+    P = mesh.vcoords[list(mesh.cells[c])]
+    step = (P[1:] - P[0]) / n  # micro-vertex coordinates as VertexDoFMacroCell.hpp:70-77
+    dir_index = {tuple(d): i + 1 for i, d in enumerate(STENCIL_DIRS.tolist())}
+    dir_index[(0, 0, 0)] = 0
+    # element matrix of each micro-cell type (translates of one another inside the affine cell)
+    K = []
+    for _, offs, _shift in MICRO_CELL_TYPES:
+        v = np.array(offs, dtype=np.int64)
+        X = P[0] + v.astype(np.float64) @ step
+        K.append(element(X[None])[0])
+    out = np.zeros((16, 15))
+    for mask in range(16):
+        if mask == 15:
+            continue  # no point lies on all four faces
+        p = _mask_point(n, mask)
+        for t, (_, offs, shift) in enumerate(MICRO_CELL_TYPES):
+            v = np.array(offs, dtype=np.int64)
+            for k in range(4):
+                a = p - v[k]  # anchor of the micro-cell of type t holding p as vertex k
+                if a.min() < 0 or a.sum() > n - shift - 1:
+                    continue
+                for j in range(4):
+                    out[mask, dir_index[tuple((v[j] - v[k]).tolist())]] += K[t][k, j]
+    return out
+
+
+class LargeLevelConstantOperator:
+    """P1ConstantOperator on one level without assembling the global matrix, for levels where the
+    assembled oracle does not fit (level 7 and 8 parity).
+
+    apply: cell interiors through `interior_kernel(cell_array, L, stencil15)` (the reference's compiled
+    apply_3D_macrocell_vertexdof_to_vertexdof_replace when the caller passes it; cell_stencil_apply
+    otherwise); every face, edge and vertex owner is the sum over its neighbour cells of the one-sided
+    stencil of its position in that cell, the decomposition of P1ConstantOperator::apply_face3D_generated
+    (P1ConstantOperator.cpp:239-357) and of the edge / vertex stencils (P1Operator.hpp:1044-1108), whose
+    weights are the same sums of micro-cell element-matrix entries.  Interface as P1ConstantLaplace
+    (apply / smooth_jac / invdiag / levels) for one level."""
+
+    def __init__(self, mesh, L, element=p1_laplace_element, interior_kernel=None, level=None):
+        self.mesh, self.L = mesh, L
+        lev = level if level is not None else Level(mesh, L)
+        self.levels = {L: lev}
+        n = lev.n
+        self.kernel = interior_kernel or cell_stencil_apply
+        self.st = [cell_stencils_by_mask(mesh, c, L, element) for c in range(mesh.nC)]
+        pts = lev._cell_pts
+        m = _face_mask(n, pts[:, 0], pts[:, 1], pts[:, 2])
+        self._bidx = np.nonzero(m != 0)[0]  # boundary points of a cell array (memory order)
+        self._bmask = m[self._bidx]
+        self._iidx = np.nonzero((pts.min(axis=1) >= 1) & (pts.sum(axis=1) <= n - 1))[0]
+        bp = pts[self._bidx]
+        self._owners = [lev.owner(c, bp[:, 0], bp[:, 1], bp[:, 2]) for c in range(mesh.nC)]
+        diag = np.zeros(lev.size)
+        for c in range(mesh.nC):
+            diag[lev.off_c[c] + self._iidx] = self.st[c][0, 0]
+            diag += np.bincount(self._owners[c], weights=self.st[c][self._bmask, 0], minlength=lev.size)
+        inv = np.zeros(lev.size)
+        inv[lev.owned] = 1.0 / diag[lev.owned]
+        self.invdiag = {L: inv}
+
+    def full_apply(self, src):
+        """A src on every owned slot (other slots zero).  Only owner slots of src are read, as in the
+        assembled operator: the cell arrays' copy slots are refreshed from their owners first."""
+        lev, n, L = self.levels[self.L], self.levels[self.L].n, self.L
+        src = lev.sync(np.array(src, dtype=np.float64))
+        pts = lev._cell_pts
+        size_c = tet_size(n + 1)
+        y = np.zeros(lev.size)
+        bp = pts[self._bidx]
+        for c in range(self.mesh.nC):
+            cell = np.ascontiguousarray(src[lev.off_c[c]: lev.off_c[c] + size_c])
+            inner = self.kernel(cell, L, self.st[c][0])
+            y[lev.off_c[c] + self._iidx] = inner[self._iidx]
+            acc = np.zeros(self._bidx.size)
+            for mask in np.unique(self._bmask):
+                sel = self._bmask == mask
+                P = bp[sel]
+                w = self.st[c][mask]
+                part = np.zeros(P.shape[0])
+                for di, d in enumerate(STENCIL15):
+                    if w[di] == 0.0:
+                        continue  # directions leaving the cell carry no micro-cell
+                    q = P + d
+                    part += w[di] * cell[cell_index(n, q[:, 0], q[:, 1], q[:, 2])]
+                acc[sel] = part
+            y += np.bincount(self._owners[c], weights=acc, minlength=lev.size)
+        return y
+
+    def apply(self, src, dst, L, flag, add=False):
+        y = self.full_apply(src)
+        mask = self.levels[L].owned_mask(flag)
+        if add:
+            dst[mask] += y[mask]
+        else:
+            dst[mask] = y[mask]
+        return dst
+
+    def smooth_jac(self, dst, rhs, src, relax, L, flag):
+        mask = self.levels[L].owned_mask(flag)
+        t = self.invdiag[L] * (rhs - self.full_apply(src))
+        dst[mask] = src[mask] + relax * t[mask]
+        return dst
 
 
 # ---------------------------------------------------------------------------------------------

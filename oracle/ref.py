@@ -89,3 +89,35 @@ def p2_divkgrad_blending_element(X, map_kind=0, map_a=0.0, k_amp=0.5, k_phase=(0
     ph = np.asarray(k_phase, dtype=np.float64)
     f(_p(np.ascontiguousarray(X, dtype=np.float64).ravel()), map_kind, map_a, k_amp, _p(ph), _p(A))
     return A.reshape(10, 10)
+
+
+SHELL_PATH = os.path.join(HERE, "_ref", "libhyteg_ref_shell.so")
+_shell = None
+
+
+def shell_available():
+    return os.path.exists(SHELL_PATH)
+
+
+def shell_map_eval(coords, tets, cell, pts):
+    """The reference's IcosahedralShellMap of macro-cell `cell` (classified by the reference's own
+    code from the whole mesh): F (n, 3), DF (n, 3, 3) and the determinant evalDF returns, at the
+    points pts (n, 3)."""
+    global _shell
+    if _shell is None:
+        _shell = C.CDLL(SHELL_PATH)
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        _shell.ref_shell_map_eval.argtypes = [C.c_int, dp, C.c_int, ip, C.c_int, C.c_int, dp, dp, dp, dp]
+        _shell.ref_shell_map_eval.restype = C.c_int
+    xyz = np.ascontiguousarray(coords, dtype=np.float64)
+    tt = np.ascontiguousarray(tets, dtype=np.int32)
+    x = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    F = np.zeros_like(x)
+    DF = np.zeros((x.shape[0], 3, 3))
+    det = np.zeros(x.shape[0])
+    rc = _shell.ref_shell_map_eval(len(xyz), _p(xyz), len(tt), tt.ctypes.data_as(C.POINTER(C.c_int)), int(cell), x.shape[0], _p(x),
+                                   _p(F), _p(DF), _p(det))
+    if rc:
+        raise ValueError("cell out of range")
+    return F, DF, det

@@ -282,3 +282,33 @@ def test_errors_are_reported(ctx):
     h = H.P1Function("h", s.pm, 2, 3, ctx, "float32")
     with pytest.raises(H.HybError):
         s.A.apply(f, h, 2, O.ALL)  # mixed value types
+
+
+def test_graph_replay_after_context_scratch_grows():
+    """A captured V-cycle graph keeps the addresses of the context's reduction partials (the coarse
+    CG's dot products are inside the graph).  When a later, larger reduction on the same context
+    needs a bigger partials buffer, the old buffer must stay valid for the graph: cycles replayed
+    after the growth give the same bits as on a context where nothing grew."""
+    L = 4
+    runs = []
+    for grow in (False, True):
+        c = H.Context(0)
+        s = Setup(c, "cube_6", 0, L)
+        b = s.rand(L, 21, O.INNER)
+        fx, fb = s.fn(), s.fn()
+        fb.upload(L, b)
+        gmg = H.GeometricMultigridSolver(c, s.A, 0, L, preSmoothSteps=2, postSmoothSteps=2, use_graph=True)
+        h1 = gmg.solve_cycles(fx, fb, L, 3)  # the graph is captured during these cycles
+        if grow:
+            before = c.scratch_bytes
+            # about 105,000 block partials, more than the 65,536 reserved at the start
+            big = H.PrimitiveStorage.spherical_shell(5, 3, 0.55, 1.0, ctx=c)
+            f = H.P1Function("f", big, 5, 5, c)
+            f.fill_random(5, 3)
+            f.dotGlobal(f, 5, H.All)
+            assert c.scratch_bytes > before
+        h2 = gmg.solve_cycles(fx, fb, L, 3)  # replays the captured graph
+        runs.append((h1, h2, fx.download(L)))
+        c.close()
+    np.testing.assert_array_equal(runs[0][1], runs[1][1])
+    np.testing.assert_array_equal(runs[0][2], runs[1][2])

@@ -442,3 +442,55 @@ def test_sor_color_sets(name):
     y = O.sor_sweep(op, x, b, L, 1.0, O.INNER)
     y = O.sor_sweep(op, y, b, L, 1.0, O.INNER, backwards=True)
     assert np.linalg.norm((b - A @ y)[m]) < 0.8 * r0
+
+
+@pytest.mark.parametrize("name", ["cube_6", "octahedron_8", "cube_2x1x1", "tilted_tet", "pyramid_4"])
+def test_large_level_operator_matches_assembled(name):
+    """The large-level oracle (per-cell stencils from element matrices, boundary owners summed over
+    their cells' one-sided stencils) equals the assembled operator, here with the reference's own
+    compiled cell kernel for the interiors when oracle/_ref is built."""
+    coords, tets = M.ALL[name]()
+    m = O.MacroMesh(coords, tets)
+    L = 3
+    op = O.P1ConstantLaplace(m, L, L)
+    kernel = R.cell_apply if R.available() else None
+    big = O.LargeLevelConstantOperator(m, L, interior_kernel=kernel, level=op.levels[L])
+    lev = op.levels[L]
+    rng = np.random.default_rng(5)
+    x = np.zeros(lev.size)
+    x[lev.owned] = rng.uniform(-1, 1, lev.owned.size)
+    lev.sync(x)
+    mask = lev.owned_mask(O.ALL)
+    a = op.apply(x, np.zeros_like(x), L, O.ALL)
+    b = big.apply(x, np.zeros_like(x), L, O.ALL)
+    assert np.abs(a[mask] - b[mask]).max() <= 1e-14 * np.abs(a[mask]).max()
+    np.testing.assert_allclose(big.invdiag[L][mask], op.invdiag[L][mask], rtol=1e-14)
+    # like the assembled operator it reads owner slots only: stale copies in the cell arrays (the
+    # smoothers' temporaries have them) do not change the result
+    x[~lev.owned_mask(O.ALL)] = rng.uniform(-1, 1, (~lev.owned_mask(O.ALL)).sum())
+    a = op.apply(x, np.zeros_like(x), L, O.ALL)
+    b = big.apply(x, np.zeros_like(x), L, O.ALL)
+    assert np.abs(a[mask] - b[mask]).max() <= 1e-14 * np.abs(a[mask]).max()
+
+
+@pytest.mark.skipif(not R.shell_available(), reason="oracle/_ref shell library not built")
+@pytest.mark.parametrize("ntan,nrad", [(3, 2), (5, 3)])
+def test_shell_map_matches_reference(ntan, nrad):
+    """The oracle's IcosahedralShellMap (vertex classification restated, Jacobian derived
+    independently) against the reference's own class, which classifies every macro-cell of the mesh
+    itself (skew cells included): F and DF at points inside each cell, to 1e-14 relative."""
+    coords, tets = O.mesh_spherical_shell(ntan, nrad, 0.55, 1.0)
+    m = O.MacroMesh(coords, tets)
+    rng = np.random.default_rng(ntan)
+    worst_f = worst_df = 0.0
+    for c in range(m.nC):
+        P = m.vcoords[list(m.cells[c])]
+        lam = rng.dirichlet(np.ones(4), size=5)
+        pts = lam @ P
+        F, DF, det = R.shell_map_eval(m.vcoords, np.array(m.cells), c, pts)
+        mp = O.IcosahedralShellMap(m, c)
+        Fo, DFo = mp.F(pts), mp.DF(pts)
+        worst_f = max(worst_f, np.abs(Fo - F).max() / np.abs(F).max())
+        worst_df = max(worst_df, np.abs(DFo - DF).max() / np.abs(DF).max())
+        np.testing.assert_allclose(np.linalg.det(DF), det, rtol=1e-12)
+    assert worst_f < 1e-14 and worst_df < 1e-13, (worst_f, worst_df)
