@@ -114,6 +114,8 @@ constexpr int kSwWarps     = 4;
 constexpr int kSwUnitHalf  = 1 << 30;
 constexpr int kSwUnitXMask = kSwUnitHalf - 1;
 constexpr int kSwLists     = 3;  // BPS 2, 3, 4
+// tile rows of the rolled-register sweep (k_cell_zstream): 64 x-points (two per lane) by kZTileY rows
+constexpr int kZTileY = 8;
 
 struct P1Level {
    int     L = 0, n = 0;
@@ -131,6 +133,11 @@ struct P1Level {
    // y-marching work items of the cell stencil sweep: (z, x0, y_first, y_last); a warp covers
    // x0..x0+31 of slice z and marches over rows y_first..y_last
    std::vector< std::array< int, 4 > > march;
+   // rolled-register sweep: units {x0 (| kSwUnitHalf), y0, z_first, z_last} of macro-cell zcell[i];
+   // block k runs units zbegin[k]..zbegin[k+1]-1
+   std::vector< std::array< int, 4 > > zunits;
+   std::vector< int >                  zcell;
+   std::vector< int >                  zbegin;
    // cell-interior sweep: units {x0 (| kSwUnitHalf), y0, z_first, z_last} of macro-cell swcell[b][i];
    // warp w of a launch with b + 2 blocks per SM runs units swbegin[b][w]..swbegin[b][w+1]-1
    std::vector< std::array< int, 4 > > swunits[kSwLists];
@@ -147,6 +154,9 @@ struct P1Level {
    int        bcount[4]   = {};
    int2*      d_rows      = nullptr;
    int4*      d_march     = nullptr;
+   int4*      d_zunits            = nullptr;
+   int*       d_zcell             = nullptr;
+   int*       d_zbegin            = nullptr;
    int4*      d_swunits[kSwLists]  = {};
    int*       d_swcell[kSwLists]   = {};
    int*       d_swbegin[kSwLists]  = {};
@@ -393,6 +403,8 @@ class PerDeviceOnce
 };
 void build_level( Mesh* m, int L );
 void ensure_device( Mesh* m, P1Level& P );
+// unit lists of the rolled-register sweep for a launch of nblocks blocks
+void build_zunits( P1Level& P, int nblocks, int ncells );
 // unit lists of the cell-interior sweep for a launch of nwarps warps (list index b)
 void build_sweep_units( P1Level& P, int b, int nwarps, int ncells );
 void build_operator_level( Operator* A, int L );

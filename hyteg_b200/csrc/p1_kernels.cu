@@ -121,6 +121,10 @@ struct LevelView
    const float*     ncell_cls;
    int              nmarch;
    const int4*      march;
+   int              nzblocks;  // blocks of the rolled sweep and their units (zunits/zcell from zbegin[b])
+   const int4*      zunits;
+   const int*       zcell;
+   const int*       zbegin;
    int              nswarps[kSwLists];  // warps of a cell-sweep launch with 2, 3, 4 blocks per SM
    const int4*      swunits[kSwLists];
    const int*       swcell[kSwLists];
@@ -157,6 +161,10 @@ static LevelView make_view( Mesh* m, int L )
    v.ncell_cls = P.d_ncell_cls;
    v.nmarch     = int( P.march.size() );
    v.march      = P.d_march;
+   v.nzblocks = int( P.zbegin.size() ) - 1;
+   v.zunits   = P.d_zunits;
+   v.zcell    = P.d_zcell;
+   v.zbegin   = P.d_zbegin;
    for ( int b = 0; b < kSwLists; ++b )
    {
       v.nswarps[b] = int( P.swbegin[b].size() ) - 1;
@@ -734,19 +742,330 @@ __global__ void __launch_bounds__( kSwWarps * 32, SwCfg< T, OP >::BPS )
    }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Rolled-register z-streamed cell sweep, for the operations with a second vector (residual, Jacobi,
+// Chebyshev steps, apply-add) on levels with n >= 32.
+//
+// A unit is the tile x0..x0+63, y0..y0+7 of slices z_first..z_last of one macro-cell.  Two producer
+// warps stream the tile's rows of every slice (one-point halo in x and y, plus the tile rows of the
+// second vector) into a ring of shared-memory stages with cp.async.bulk: lane r issues one copy per
+// row, each stage's full barrier completes when all bytes have landed.  Eight consumer warps (one
+// per tile row, two x per lane) march up the slices; of the 15 stencil values, four in slice z-1 and
+// four in slice z were read in the previous step and roll through registers, so a step reads three
+// values of slice z and four of slice z+1 from shared memory, and slice z is released (empty
+// barrier, one arrival per consumer warp) as soon as step z ends.  Keeping the producer work in two
+// warps and the consumers' state small (about 96 registers) gives 20 warps per SM, which these
+// register-heavy epilogues need more than the fewer shared reads of the partial-sum sweep above.
+// Global rows start at arbitrary element offsets: each row copy is widened to 16-byte boundaries
+// and its shift is published with the stage as 3-bit fields of one word.  Every wait is bounded by
+// the global timer; when one runs out the block records an error in *err, raises a block-wide abort
+// flag, stops issuing copies, waits (bounded) for the copies it has in flight and returns.
+// ---------------------------------------------------------------------------------------------
+constexpr int kZTileXR = 64;  // x-points per tile row (two per consumer lane)
+template < typename T, bool AUX >
+struct ZCfg
+{
+      static constexpr int kZTileX = kZTileXR;                                      // x-points per tile row
+   static constexpr int pts     = kZTileX / 32;                                 // x-points per consumer lane
+   static constexpr int al    = 16 / int( sizeof( T ) );                         // elements per 16 bytes
+   static constexpr int RW    = ( kZTileX + 2 + 2 * al + al - 1 ) / al * al;    // source row width (elements)
+   static constexpr int RWA   = ( kZTileX + 2 * al + al - 1 ) / al * al;        // second-vector row width
+   static constexpr int rows  = kZTileY + 2;                                   // tile rows + halo
+   static constexpr int aux0  = rows * RW;                                     // second-vector rows start here
+   static constexpr int stage = aux0 + ( AUX ? kZTileY * RWA : 0 );            // elements per stage
+   static constexpr int S     = AUX ? 8 : 10;                                   // ring depth
+   static constexpr size_t smem_bytes = size_t( S ) * stage * sizeof( T );
+};
+constexpr int kZWarps     = kZTileY;
+// Two producer warps (load l is issued by producer l % 2): one warp's issue and hand-off chain per
+// slice load is what limits a single-producer ring (measured on B200: 0.163 -> 0.136 ms for the
+// level-8 cube apply in FP64, 0.154 -> 0.108 ms in FP32).
+constexpr int kZProducers = 2;
+constexpr int kZThreads   = ( kZWarps + kZProducers ) * 32;  // consumer warps + producer warps
+
+
+// producer warp: streams the rows of every slice of the block's units into the ring.  Lane r < 10
+// copies source row y0-1+r; with AUX, lane 10+r copies row y0+r of the second vector (slices
+// z_first..z_last only, rows with interior points only).  Row offsets advance by additions from
+// slice to slice: cidx(0, y, z+1) = cidx(0, y, z) + tri(n+1-z) - y.
+template < typename T, bool AUX >
+__device__ __forceinline__ void zstream_produce( const LevelView& v, uint32_t flag, const T* __restrict__ src,
+                                                 const T* __restrict__ aux, int nC, T* ring, uint64_t* full, uint64_t* empty,
+                                                 uint32_t* shw, volatile int* abort_flag, int* err )
+{
+   using Cfg = ZCfg< T, AUX >;
+   constexpr int S = Cfg::S, AL = Cfg::al, kZTileX = Cfg::kZTileX;
+   static_assert( S % kZProducers == 0, "every stage must belong to one producer warp" );
+   const int     lane = threadIdx.x & 31, n = v.n, me = ( threadIdx.x >> 5 ) - kZWarps;
+   const int*    zb = v.zbegin;
+   const int4*   zu = v.zunits;
+   const int*    zcl = v.zcell;
+   const int     u0 = zb[blockIdx.x], u1 = zb[blockIdx.x + 1];
+   const bool    is_src = lane < Cfg::rows, is_aux = AUX && lane >= Cfg::rows && lane < Cfg::rows + kZTileY;
+   const int     dsto   = is_src ? lane * Cfg::RW : Cfg::aux0 + ( lane - Cfg::rows ) * Cfg::RWA;
+   const T*      gbase  = is_src ? src : aux;
+   const int     shbit  = is_src ? 3 * lane : ( is_aux ? 3 * ( lane - Cfg::rows ) : 0 );
+   int           ld = 0;  // sequence number of the next slice load
+   bool          ok = true;
+   {
+      for ( int u = u0; u < u1 && ok; ++u )
+      {
+         const int c = zcl[u];
+         if ( c >= nC || !( v.cell_bc[c] & flag ) ) continue;
+         const int64_t cb = v.cell_off[c];
+         const int4 U  = zu[u];  // x0 (| half-width flag), y0, z_first, z_last
+         const int  ux = U.x & kSwUnitXMask, tw = ( U.x & kSwUnitHalf ) ? kZTileX / 2 : kZTileX;
+         const int  yy = is_src ? U.y - 1 + lane : U.y + ( lane - Cfg::rows );
+         const int  xa = is_src ? ux - 1 : ux;  // first x of the row segment
+         int64_t    rb = cidx( n, 0, yy, U.z - 1 );
+         for ( int zz = U.z - 1; zz <= U.w + 1; rb += slice_step( n, zz ) - yy, ++zz, ++ld )
+         {
+            if ( ld % kZProducers != me ) continue;
+            const int st = ld % S;
+            if ( ld >= S && !mbar_wait_bounded( &empty[st], uint32_t( ( ld / S - 1 ) & 1 ), abort_flag ) )
+            {
+               ok = false;
+               break;
+            }
+            uint32_t bytes = 0, sh = 0;
+            int64_t  a0    = 0;
+            // last x of the segment: the halo point (source) or the last interior point (second vector)
+            const int  xe   = is_src ? min( ux + tw, n - yy - zz ) : min( ux + tw - 1, n - 1 - yy - zz );
+            const bool live = ( is_src && yy + zz <= n && xe >= xa ) || ( is_aux && zz >= U.z && zz <= U.w && xe >= xa );
+            if ( live )
+            {
+               const int64_t s0 = rb + xa;
+               const int64_t e1 = rb + xe + 1;  // one past the segment
+               sh               = uint32_t( s0 & ( AL - 1 ) );
+               a0               = s0 - sh;
+               bytes            = uint32_t( ( ( e1 + AL - 1 ) / AL * AL - a0 ) * int64_t( sizeof( T ) ) );
+            }
+            const uint32_t total = __reduce_add_sync( 0xffffffffu, bytes );
+            const uint32_t w0    = __reduce_or_sync( 0xffffffffu, is_src ? sh << shbit : 0u );
+            const uint32_t w1    = AUX ? __reduce_or_sync( 0xffffffffu, is_aux ? sh << shbit : 0u ) : 0u;
+            if ( lane == 0 )
+            {
+               shw[2 * st]     = w0;
+               shw[2 * st + 1] = w1;
+               mbar_expect_tx( &full[st], total );
+            }
+            __syncwarp();
+            if ( bytes ) bulk_copy_g2s( ring + st * Cfg::stage + dsto, gbase + cb + a0, bytes, &full[st] );
+         }
+      }
+   }
+   if ( !ok && lane == 0 )
+   {
+      atomicExch( err, 1 );
+      *abort_flag = 1;
+   }
+   // drain: the latest load issued on every stage has landed before the block may exit
+   if ( lane == 0 )
+      for ( int s = me; s < S && s < ld; s += kZProducers )
+      {
+         const int j = s + ( ( ld - 1 - s ) / S ) * S;
+         if ( !mbar_wait_bounded( &full[s], uint32_t( ( j / S ) & 1 ), nullptr ) ) atomicExch( err, 1 );
+      }
+}
+
+// the eight values of one point that roll over from one slice step to the next
+template < typename A >
+struct ZPoint
+{
+   A B, BE, BN, BNW;  // slice z-1: (x,y), (x+1,y), (x,y+1), (x-1,y+1)
+   A C, W, S, SE;     // slice z:   (x,y), (x-1,y), (x,y-1), (x+1,y-1)
+};
+
+template < typename T, typename A, int OP >
+__global__ void __launch_bounds__( kZThreads, 2 ) k_cell_zstream( LevelView v, OpView< A > o, uint32_t flag, const T* __restrict__ src,
+                                                                  const T* __restrict__ v1, T* v2, T* dst, A a0, A a1, int nC,
+                                                                  int* err )
+{
+   constexpr bool AUX = sweep_aux< OP >();
+   using Cfg          = ZCfg< T, AUX >;
+   constexpr int S = Cfg::S, RW = Cfg::RW;
+   extern __shared__ __align__( 128 ) unsigned char zs_raw[];
+   T*                  ring = reinterpret_cast< T* >( zs_raw );
+   __shared__ uint64_t full[S], empty[S];
+   __shared__ uint32_t shw[2 * S];
+   __shared__ A        wsm[kZWarps][16];  // per consumer warp: the cell's 15 weights and 1/diagonal
+   __shared__ int      abort_flag;
+   const int           warp = threadIdx.x >> 5, lane = threadIdx.x & 31, n = v.n;
+   if ( threadIdx.x == 0 )
+   {
+      for ( int s = 0; s < S; ++s )
+      {
+         mbar_init( &full[s], 1 );
+         mbar_init( &empty[s], kZWarps );
+      }
+      abort_flag = 0;
+      asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
+   }
+   __syncthreads();
+   volatile int* abrt = &abort_flag;
+   if ( warp >= kZWarps )
+   {
+      const T* aux = ( OP == OP_CHEBI || OP == OP_CHEBL ) ? v2 : ( OP == OP_APPLY_ADD ? dst : v1 );
+      zstream_produce< T, AUX >( v, flag, src, aux, nC, ring, full, empty, shw, abrt, err );
+      return;
+   }
+
+   // consumer warp `warp` owns tile row y0 + warp; stage row r holds global row y0 - 1 + r; lane
+   // owns x = x0 + lane + 32 k, k < kZPts
+   constexpr int kZPts = Cfg::pts;
+   const int*    zb    = v.zbegin;
+   const int4*   zu    = v.zunits;
+   const int*    zcl   = v.zcell;
+   const int     u0 = zb[blockIdx.x], u1 = zb[blockIdx.x + 1];
+   const int rS = warp, rC = warp + 1, rN = warp + 2;  // rows y-1, y, y+1 of the stage
+   auto at = [&]( const T* st, uint32_t word, int r, int k, int dx ) -> A {
+      return A( st[r * RW + int( ( word >> ( 3 * r ) ) & 7u ) + lane + 32 * k + 1 + dx] );
+   };
+   auto fail = [&]() {
+      if ( lane == 0 )
+      {
+         atomicExch( err, 1 );
+         *abrt = 1;
+      }
+   };
+   int ld = 0;
+   // the weights are read from shared memory at every use (broadcast, shared by the lane's points)
+   // rather than held in 30 registers
+   A* w = wsm[warp];
+   int cw = -1;  // cell whose weights are in w
+   {
+      for ( int u = u0; u < u1; ++u )
+      {
+         const int c = zcl[u];
+         if ( c >= nC || !( v.cell_bc[c] & flag ) ) continue;
+         const int64_t base = v.cell_off[c];
+         if ( c != cw )
+         {
+            __syncwarp();
+            if ( lane < kNumDirs ) w[lane] = o.W[size_t( c ) * kNumClasses * kNumDirs + lane];  // interior class 0
+            if ( lane == kNumDirs ) w[kNumDirs] = o.invd_c[c];
+            __syncwarp();
+            cw = c;
+         }
+         const int4 U    = zu[u];
+         const int  x0   = U.x & kSwUnitXMask;
+         const bool half = ( U.x & kSwUnitHalf ) != 0;  // the tile's rows end within 32 points
+         const int  x = x0 + lane, y = U.y + warp;
+         // one unit with KP points per lane (kZPts, or 1 for half-width units)
+         auto unit = [&]( auto kp_c ) -> bool {
+            constexpr int KP = decltype( kp_c )::value;
+            // prologue: slice z_first-1 (load ld) and slice z_first (load ld+1)
+            const int sm = ld % S, s0 = ( ld + 1 ) % S;
+            if ( !mbar_wait_bounded( &full[sm], uint32_t( ( ld / S ) & 1 ), abrt ) ||
+                 !mbar_wait_bounded( &full[s0], uint32_t( ( ( ld + 1 ) / S ) & 1 ), abrt ) )
+               return false;
+            ZPoint< A > P[KP];
+            {
+               const T*       Rm = ring + sm * Cfg::stage;
+               const T*       R0 = ring + s0 * Cfg::stage;
+               const uint32_t wm = shw[2 * sm], wc = shw[2 * s0];
+   #pragma unroll
+               for ( int k = 0; k < KP; ++k )
+               {
+                  P[k].B   = at( Rm, wm, rC, k, 0 );
+                  P[k].BE  = at( Rm, wm, rC, k, 1 );
+                  P[k].BN  = at( Rm, wm, rN, k, 0 );
+                  P[k].BNW = at( Rm, wm, rN, k, -1 );
+                  P[k].C   = at( R0, wc, rC, k, 0 );
+                  P[k].W   = at( R0, wc, rC, k, -1 );
+                  P[k].S   = at( R0, wc, rS, k, 0 );
+                  P[k].SE  = at( R0, wc, rS, k, 1 );
+               }
+            }
+            __syncwarp();
+            if ( lane == 0 ) mbar_arrive( &empty[sm] );
+            int64_t out = base + cidx( n, x, y, U.z );  // output offset of point k = 0, advanced per slice
+            // unrolled by two so that the rolled values alternate registers instead of being copied
+   #pragma unroll 2
+            for ( int z = U.z; z <= U.w; out += slice_step( n, z ) - y, ++z )
+            {
+               const int lz = ld + 1 + ( z - U.z ), lp = lz + 1;
+               const int sz = lz % S, sp = lp % S;
+               if ( !mbar_wait_bounded( &full[sp], uint32_t( ( lp / S ) & 1 ), abrt ) ) return false;
+               const T*       Rz = ring + sz * Cfg::stage;
+               const T*       Rp = ring + sp * Cfg::stage;
+               const uint32_t wz = shw[2 * sz], wp = shw[2 * sp];
+               const uint32_t wa = AUX ? shw[2 * sz + 1] : 0u;
+   #pragma unroll
+               for ( int k = 0; k < KP; ++k )
+               {
+                  const A E = at( Rz, wz, rC, k, 1 ), N = at( Rz, wz, rN, k, 0 ), NW = at( Rz, wz, rN, k, -1 );
+                  const A Tt = at( Rp, wp, rC, k, 0 ), TW = at( Rp, wp, rC, k, -1 ), TS = at( Rp, wp, rS, k, 0 ),
+                          TSE = at( Rp, wp, rS, k, 1 );
+                  ZPoint< A >& p = P[k];
+                  if ( x + 32 * k + y + z <= n - 1 )
+                  {
+                     A auxv = A( 0 );
+                     if constexpr ( AUX )
+                        auxv = A( Rz[Cfg::aux0 + warp * Cfg::RWA + int( ( wa >> ( 3 * warp ) ) & 7u ) + lane + 32 * k] );
+                     // three independent partial sums: the dependent FMA chain is 7 deep instead of 15
+                     A s0 = w[0] * p.C, s1 = w[5] * p.B, s2 = w[10] * p.BE;
+                     s0 += w[1] * p.W;
+                     s1 += w[6] * Tt;
+                     s2 += w[11] * TS;
+                     s0 += w[2] * E;
+                     s1 += w[7] * NW;
+                     s2 += w[12] * p.BN;
+                     s0 += w[3] * p.S;
+                     s1 += w[8] * p.SE;
+                     s2 += w[13] * TSE;
+                     s0 += w[4] * N;
+                     s1 += w[9] * TW;
+                     s2 += w[14] * p.BNW;
+                     const A acc = s0 + ( s1 + s2 );
+                     sweep_epilogue< T, A, OP >( out + 32 * k, acc, w[kNumDirs], p.C, auxv, v2, dst, a0, a1 );
+                  }
+                  p.B   = p.C;
+                  p.BE  = E;
+                  p.BN  = N;
+                  p.BNW = NW;
+                  p.C   = Tt;
+                  p.W   = TW;
+                  p.S   = TS;
+                  p.SE  = TSE;
+               }
+               __syncwarp();
+               if ( lane == 0 ) mbar_arrive( &empty[sz] );
+            }
+            // slice z_last+1 is no longer needed either
+            __syncwarp();
+            if ( lane == 0 ) mbar_arrive( &empty[( ld + 2 + ( U.w - U.z ) ) % S] );
+            return true;
+         };
+         const bool good = half ? unit( std::integral_constant< int, 1 >{} ) : unit( std::integral_constant< int, kZPts >{} );
+         if ( !good ) return fail();
+         ld += U.w - U.z + 3;
+      }
+   }
+}
+
 template < typename T, typename A, int OP >
 static void sweep_attribute( int sms )
 {
-   using Cfg = SwCfg< T, OP >;
-   check_cuda( cudaFuncSetAttribute( k_cell_sweep< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize, int( Cfg::smem_bytes ) ),
-               "cudaFuncSetAttribute(cell sweep shared memory)" );
-   int nb = 0;
-   check_cuda( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &nb, k_cell_sweep< T, A, OP >, kSwWarps * 32, Cfg::smem_bytes ),
-               "cell sweep occupancy" );
-   // the unit lists assume every block of the launch is resident at once
-   if ( nb < Cfg::BPS )
-      throw std::runtime_error( "cell sweep: " + std::to_string( nb ) + " resident blocks per SM, the unit lists need " +
-                                std::to_string( Cfg::BPS ) );
+   if constexpr ( sweep_aux< OP >() )
+   {
+      check_cuda( cudaFuncSetAttribute( k_cell_zstream< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int( ZCfg< T, true >::smem_bytes ) ),
+                  "cudaFuncSetAttribute(rolled sweep shared memory)" );
+   }
+   else
+   {
+      using Cfg = SwCfg< T, OP >;
+      check_cuda( cudaFuncSetAttribute( k_cell_sweep< T, A, OP >, cudaFuncAttributeMaxDynamicSharedMemorySize, int( Cfg::smem_bytes ) ),
+                  "cudaFuncSetAttribute(cell sweep shared memory)" );
+      int nb = 0;
+      check_cuda( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &nb, k_cell_sweep< T, A, OP >, kSwWarps * 32, Cfg::smem_bytes ),
+                  "cell sweep occupancy" );
+      // the unit lists assume every block of the launch is resident at once
+      if ( nb < Cfg::BPS )
+         throw std::runtime_error( "cell sweep: " + std::to_string( nb ) + " resident blocks per SM, the unit lists need " +
+                                   std::to_string( Cfg::BPS ) );
+   }
    (void) sms;
 }
 
@@ -938,9 +1257,25 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
    // slots of the second vector), so the two kernels may run in either order
    const TaskSegments seg = task_segments( v, a.flag, a.copy_unflagged );
    const int          nt  = seg.count[0] + seg.count[1] + seg.count[2] + seg.count[3];
+   // the partial-sum sweep for the operations without a second vector, the rolled-register sweep
+   // for the others (their epilogues' registers would leave the partial-sum sweep 8 warps per SM)
+   constexpr bool ROLLED = sweep_aux< OP >();
+   const bool     big    = v.n >= 32 && nC > 0 && ( ROLLED ? v.nzblocks > 0 : v.nswarps[Cfg::BPS - 2] > 0 );
+   auto           cell   = [&]() {
+      if constexpr ( ROLLED )
+      {
+         constexpr size_t smem = ZCfg< T, true >::smem_bytes;  // attribute set by ensure_constants
+         k_cell_zstream< T, A, OP ><<< v.nzblocks, kZThreads, smem, ctx->stream >>>( v, o, a.flag, src, v1, v2, dst, A( a.a0 ),
+                                                                                    A( a.a1 ), nC, ctx->d_error );
+      }
+      else
+         k_cell_sweep< T, A, OP ><<< v.nswarps[Cfg::BPS - 2] / kSwWarps, kSwWarps * 32, Cfg::smem_bytes, ctx->stream >>>(
+             v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ), nC, ctx->d_error );
+      ++ctx->launches;
+   };
    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
    check_cuda( cudaStreamIsCapturing( ctx->stream, &cap ), "cudaStreamIsCapturing" );
-   if ( v.n >= 32 && nC > 0 && v.nswarps[Cfg::BPS - 2] > 0 && cap == cudaStreamCaptureStatusNone )
+   if ( big && cap == cudaStreamCaptureStatusNone )
    {
       // Launched one by one, the boundary kernel goes first on the same stream: the sweep occupies
       // every SM's registers, so a forked boundary kernel would only wait for it and add the latency of
@@ -952,21 +1287,13 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
                                                                                    A( a.a0 ), A( a.a1 ) );
          ++ctx->launches;
       }
-      // dynamic shared memory attribute set by ensure_constants
-      k_cell_sweep< T, A, OP ><<< v.nswarps[Cfg::BPS - 2] / kSwWarps, kSwWarps * 32, Cfg::smem_bytes, ctx->stream >>>(
-          v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ), nC, ctx->d_error );
-      ++ctx->launches;
+      cell();
       check_cuda( cudaGetLastError(), "stencil launch" );
       return;
    }
    // the cell kernel and the boundary kernel side by side on two streams
    Fork fk( ctx );
-   if ( v.n >= 32 && nC > 0 && v.nswarps[Cfg::BPS - 2] > 0 )
-   {
-      k_cell_sweep< T, A, OP ><<< v.nswarps[Cfg::BPS - 2] / kSwWarps, kSwWarps * 32, Cfg::smem_bytes, ctx->stream >>>(
-          v, o, a.flag, src, v1, v2, dst, A( a.a0 ), A( a.a1 ), nC, ctx->d_error );
-      ++ctx->launches;
-   }
+   if ( big ) cell();
    else if ( v.nmarch > 0 && nC > 0 )
    {
       dim3 grid( ( v.nmarch + 7 ) / 8, nC );

@@ -317,6 +317,84 @@ void build_level( Mesh* m, int L )
    m->levels[L] = std::move( lv );
 }
 
+// Work units of the rolled-register sweep.  A unit is the tile x0..x0+63, y0..y0+kZTileY-1 of slices
+// z_first..z_last (interior points only: x, y, z >= 1, x+y+z <= n-1).  The slice range is cut into
+// chunks of zc slices, zc the largest power of two in [8, 32] that still gives at least one unit
+// per two blocks (every chunk re-reads two halo slices, and every slice load costs a fixed hand-off,
+// so long chunks win over finer balance); units are then handed out longest-first to the least
+// loaded block.
+void build_zunits( P1Level& P, int nblocks, int ncells )
+{
+   const int n = P.n, kZTileX = 64, kTY = kZTileY;
+   auto&     zunits = P.zunits;
+   auto&     zcell  = P.zcell;
+   auto&     zbegin = P.zbegin;
+   zunits.clear();
+   zcell.clear();
+   zbegin.assign( 1, 0 );
+   if ( n < 4 || ncells < 1 ) return;
+   struct Unit
+   {
+      std::array< int, 4 > u;
+      int64_t              work;
+   };
+   auto make = [&]( int zc ) {
+      std::vector< Unit > us;
+      for ( int y0 = 1; y0 <= n - 3; y0 += kTY )
+         for ( int x0 = 1; x0 + y0 <= n - 2; x0 += kZTileX )
+         {
+            const int zmax = n - 1 - x0 - y0;
+            // from slice zh on, every row of the tile ends within its first 32 points (row y0, the
+            // longest, has n - y0 - z - x0 interior points from x0 on): those slices form half-width
+            // units, run with one point per lane
+            const int zh = kZTileX > 32 ? std::max( 1, n - y0 - x0 - 32 ) : zmax + 1;
+            for ( int part = 0; part < 2; ++part )
+            {
+               const int lo = part == 0 ? 1 : std::max( 1, zh ), hi = part == 0 ? std::min( zmax, zh - 1 ) : zmax;
+               for ( int za = lo; za <= hi; za += zc )
+               {
+                  // cost: the slice steps of the unit (its slices plus the two halo slices and the
+                  // prologue) times the points per lane; every step issues the whole tile, clipped
+                  // lanes included, so the number of interior points would underestimate the units
+                  // along the diagonal
+                  const int zb = std::min( hi, za + zc - 1 );
+                  us.push_back( { { part ? ( x0 | kSwUnitHalf ) : x0, y0, za, zb }, int64_t( zb - za + 3 ) * ( part ? 1 : 2 ) } );
+               }
+            }
+         }
+      return us;
+   };
+   // longest slice ranges that still give every block about two units (all cells together)
+   int                 zc = 32;
+   std::vector< Unit > us = make( zc );
+   while ( zc > 8 && 2 * int64_t( us.size() ) * ncells < int64_t( nblocks ) ) us = make( zc /= 2 );
+   std::stable_sort( us.begin(), us.end(), []( const Unit& a, const Unit& b ) { return a.work > b.work; } );
+   const int64_t items = int64_t( us.size() ) * ncells;
+   const int     nb    = int( std::max< int64_t >( 1, std::min< int64_t >( nblocks, items ) ) );
+   std::vector< std::vector< std::pair< int, int > > >                                      per( nb );  // (cell, unit)
+   std::priority_queue< std::pair< int64_t, int >, std::vector< std::pair< int64_t, int > >, std::greater<> > heap;
+   for ( int b = 0; b < nb; ++b ) heap.push( { 0, b } );
+   for ( size_t k = 0; k < us.size(); ++k )  // longest first; the cells of one unit shape in turn
+      for ( int c = 0; c < ncells; ++c )
+      {
+         auto [load, b] = heap.top();
+         heap.pop();
+         per[b].push_back( { c, int( k ) } );
+         heap.push( { load + us[k].work, b } );
+      }
+   for ( int b = 0; b < nb; ++b )
+   {
+      // cell-major inside a block: a warp reloads its cell's weights only when the cell changes
+      std::stable_sort( per[b].begin(), per[b].end(), []( const auto& a, const auto& b ) { return a.first < b.first; } );
+      for ( const auto& cu : per[b] )
+      {
+         zunits.push_back( us[cu.second].u );
+         zcell.push_back( cu.first );
+      }
+      zbegin.push_back( int( zunits.size() ) );
+   }
+}
+
 // Work of the cell-interior sweep.  A unit is the tile x0..x0+kSwTX-1, y0..y0+kSwR-1 of the
 // slices z_first..z_last of one macro-cell (interior points only: x, y, z >= 1, x+y+z <= n-1).  From
 // the slice on which every row of the tile ends within 32 points of x0 the tile is half-width (one
@@ -435,6 +513,14 @@ void ensure_device( Mesh* m, P1Level& P )
    int dev = 0, sms = 0;
    check_cuda( cudaGetDevice( &dev ), "cudaGetDevice" );
    check_cuda( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev ), "device attribute" );
+   {
+      build_zunits( P, 2 * std::max( sms, 1 ), t.nC );
+      std::vector< int4 > zu( P.zunits.size() );
+      for ( size_t i = 0; i < zu.size(); ++i ) zu[i] = make_int4( P.zunits[i][0], P.zunits[i][1], P.zunits[i][2], P.zunits[i][3] );
+      up( &P.d_zunits, zu.data(), zu.size() );
+      up( &P.d_zcell, P.zcell.data(), P.zcell.size() );
+      up( &P.d_zbegin, P.zbegin.data(), P.zbegin.size() );
+   }
    for ( int b = 0; b < kSwLists; ++b )
    {
       // one list set per blocks-per-SM count (b + 2) of the sweep's instantiations
@@ -490,6 +576,7 @@ Mesh::~Mesh()
       cudaFree( P.d_btasks );
       cudaFree( P.d_rows );
       cudaFree( P.d_march );
+      cudaFree( P.d_zunits ), cudaFree( P.d_zcell ), cudaFree( P.d_zbegin );
       for ( int b = 0; b < kSwLists; ++b ) cudaFree( P.d_swunits[b] ), cudaFree( P.d_swcell[b] ), cudaFree( P.d_swbegin[b] );
       cudaFree( P.d_bc );
       cudaFree( P.d_bkind );
