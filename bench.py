@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--no-p2", action="store_true")
     p.add_argument("--no-stokes", action="store_true")
+    p.add_argument("--no-config1", action="store_true")
+    p.add_argument("--no-p2c", action="store_true")
     p.add_argument("--serve-requests", type=int, default=200)
     p.add_argument("--profile-vcycle", action="store_true",
                    help="run one FP64 and one FP32 V(3,3) Chebyshev(3) cycle of the level-8 cube without graph capture "
@@ -212,6 +214,55 @@ def reference_parity(H, pm, x, y, L):
         d = np.abs(ys[o:o + size][inner] - ref[inner]).max() / max(np.abs(ref[inner]).max(), 1e-300)
         worst = max(worst, float(d))
     return worst
+
+
+def config1_leg(H, ctx, L=5, cycles=10):
+    """Configuration 1 as stated: P1 Poisson on the six-tetrahedra cube, level 5, rhs = mass matrix x
+    interpolated 3 pi^2 sin(pi x) sin(pi y) sin(pi z), zero guess, V(2,2) weighted Jacobi 2/3, CG coarse
+    solve to 1e-14 on level 0, ten cycles (graph-captured).  Reports the per-cycle residual reduction,
+    the time per cycle and the FP64 apply rate on level 5 (a 0.3 MB vector: latency-bound, absolute
+    times)."""
+    import math
+
+    import torch
+
+    pm = H.PrimitiveStorage.cuboid(ctx=ctx)
+    A = H.P1ConstantLaplaceOperator(pm, 0, L, ctx)
+    M = H.P1ConstantMassOperator(pm, L, L, ctx)
+    f, b, x = (H.P1Function(nm, pm, 0, L, ctx) for nm in ("f1", "b1", "x1"))
+    pi = math.pi
+    f.interpolate(lambda X, Y, Z: 3 * pi * pi * math.sin(pi * X) * math.sin(pi * Y) * math.sin(pi * Z), L, H.All)
+    M.apply(f, b, L, H.All, H.Replace)
+    gmg = H.GeometricMultigridSolver(ctx, A, 0, L, preSmoothSteps=2, postSmoothSteps=2, smoother="jacobi",
+                                     relax=2.0 / 3.0, coarse_rtol=1e-14)
+    gmg.solve_cycles(x, b, L, 2)  # set-up and graph capture
+    best = None
+    for _ in range(3):
+        for lv in range(L + 1):
+            x.interpolate(0.0, lv, H.All)
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        hist = gmg.solve_cycles(x, b, L, cycles)
+        sec = time.perf_counter() - t0
+        best = sec if best is None else min(best, sec)
+    y = H.P1Function("y1", pm, L, L, ctx)
+    for _ in range(10):
+        A.apply(x, y, L, H.Inner)
+    ctx.synchronize()
+    n_ap = 200
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s = torch.cuda.ExternalStream(ctx.stream)
+    e0.record(s)
+    for _ in range(n_ap):
+        A.apply(x, y, L, H.Inner)
+    e1.record(s)
+    e1.synchronize()
+    ms_ap = e0.elapsed_time(e1) / n_ap
+    return {"level": L, "inner_dofs": inner_dofs(L), "cycle": "V(2,2) weighted Jacobi 2/3, CG coarse level 0 to 1e-14",
+            "rhs": "P1 mass x interpolated 3 pi^2 sin sin sin", "cycles": int(hist.size - 1),
+            "factors": [float(v) for v in hist[1:] / hist[:-1]], "rel_residual": float(hist[-1] / hist[0]),
+            "seconds_10_cycles": best, "ms_per_cycle": best * 1e3 / cycles,
+            "apply_ms": ms_ap, "apply_mdofs": inner_dofs(L) / (ms_ap * 1e-3) / 1e6}
 
 
 def mixed_precision_leg(H, ctx, pm, A, L, rtol=1e-8):
@@ -512,6 +563,58 @@ def p2_leg(H, ctx, level=5, cycle_level=3):
     return out
 
 
+def p2_constant_leg(H, ctx, level=7, cycle_level=7):
+    """P2 constant-stencil Laplacian (P2ConstantLaplaceOperator) on the six-tetrahedra cube at P2 level 7
+    (its nodes are the level-8 grid: 16,974,593 DoFs, 16,581,375 inner), FP64: one apply timed with CUDA
+    events (algorithmic bytes: read x, write y per inner DoF, 16 B), and one V(3,3) Chebyshev(3) cycle
+    with quadratic transfers on levels 0..cycle_level (graph-captured)."""
+    import torch
+
+    pm = H.PrimitiveStorage.cuboid(ctx=ctx)
+    A = H.P2ConstantLaplaceOperator(pm, 0, level, ctx)
+    x = H.P2Function("p2x", pm, level, level, ctx)
+    y = H.P2Function("p2y", pm, level, level, ctx)
+    x.fill_random(level, 11)
+    for _ in range(3):
+        A.apply(x, y, level, H.Inner)
+    ctx.synchronize()
+    s = torch.cuda.ExternalStream(ctx.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    e0.record(s)
+    for _ in range(reps):
+        A.apply(x, y, level, H.Inner)
+    e1.record(s)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    ndof = inner_dofs(level + 1)
+    peak, peak_kind = measured_peak()
+    achieved = 16 * ndof / (ms * 1e-3) / 1e9
+    out = {"mesh": "unit cube, 6 macro-tets", "level": level, "inner_dofs": ndof, "dtype": "f64",
+           "apply_ms": ms, "mdofs": ndof / (ms * 1e-3) / 1e6,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_kind": peak_kind, "kernel": "k_p2c_sweep<double,double,OP_APPLY> + k_p2c_bnd"}}
+    del x, y
+    g = H.GeometricMultigridSolver(ctx, A, 0, cycle_level, 3, 3, smoother="chebyshev", chebyshev_order=3,
+                                   power_iterations=20)
+    xv = H.P2Function("p2xv", pm, 0, cycle_level, ctx)
+    bv = H.P2Function("p2bv", pm, 0, cycle_level, ctx)
+    bv.fill_random(cycle_level, 3)
+    hist = g.solve_cycles(xv, bv, cycle_level, 2)  # set-up, capture, two cycles
+    ctx.synchronize()
+    v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    v0.record(s)
+    n = 3
+    for _ in range(n):
+        g.solve(A, xv, bv, cycle_level)
+    v1.record(s)
+    v1.synchronize()
+    out["vcycle"] = {"levels": f"0..{cycle_level}", "ms_per_cycle": v0.elapsed_time(v1) / n,
+                     "cycle": "V(3,3) Chebyshev(3), quadratic transfers, CG coarse",
+                     "factors": [float(f) for f in hist[1:] / hist[:-1]]}
+    return out
+
+
 def p2_cpu_reference(cells=400000):
     """The reference's per-micro-cell work of the P2 elementwise apply (integrateAll of the generated
     form + 10x10 matvec), compiled from its sources, on the host cores (test blending map)."""
@@ -709,6 +812,8 @@ def run_ours(args, rank, world, local):
         return
     A.apply(x, y, L, H.Inner)
     parity = reference_parity(H, pm, x, y, L)
+    config1 = None if args.no_config1 else config1_leg(H, ctx)
+    p2c = None if args.no_p2c else p2_constant_leg(H, ctx)
     mixed = None if args.no_mixed else mixed_precision_leg(H, ctx, pm, A, L)
     serving = None if args.no_serve else serving_leg(H, ctx, nreq=args.serve_requests)
     p2 = None
@@ -744,6 +849,10 @@ def run_ours(args, rank, world, local):
     }
     if vcycle:
         line["vcycle"] = vcycle
+    if config1:
+        line["config1_poisson_cube_L5"] = config1
+    if p2c:
+        line["p2_constant_cube"] = p2c
     if mixed:
         line["mixed_precision"] = mixed
     if serving:

@@ -33,6 +33,7 @@ _DTYPES = {"float64": F64, "double": F64, "f64": F64, "float32": F32, "float": F
 
 P1_CONST_LAPLACE = 1
 P1_CONST_MASS = 2
+P2_CONST_LAPLACE = 8
 SMOOTHER_JACOBI = 0
 SMOOTHER_CHEBYSHEV = 1
 SMOOTHER_GAUSS_SEIDEL = 2
@@ -593,11 +594,11 @@ class P2ElementwiseBlendingDivKGradOperator(_ConstantOperator):
         _check(lib().hyb_op_store_element_matrices(self.h))
 
 
-class P2ConstantLaplaceOperator(P2ElementwiseBlendingDivKGradOperator):
-    """The P2 Laplacian (k = 1, no blending): the matrix of P2ConstantLaplaceOperator, applied elementwise."""
+class P2ConstantLaplaceOperator(_ConstantOperator):
+    """P2ConstantLaplaceOperator (P2ConstantOperator.cpp:100-114): one constant stencil per parity class of
+    the P2 node grid and macro-cell, applied as a memory-bound stencil sweep.  Levels are P2 levels."""
 
-    def __init__(self, storage, min_level, max_level, ctx):
-        super().__init__(storage, min_level, max_level, ctx)
+    kind = P2_CONST_LAPLACE
 
 
 class P1toP1LinearRestriction:

@@ -1042,20 +1042,27 @@ int hyb_op_create( hyb_ctx* ctx, hyb_mesh* mesh, int kind, int min_level, int ma
 {
    HYB_TRY
    require( ctx && mesh && out, "NULL argument" );
-   require( kind == HYB_P1_CONST_LAPLACE || kind == HYB_P1_CONST_MASS, "unknown operator kind" );
-   require( min_level >= 0 && min_level <= max_level && max_level <= 14, "invalid level range" );
+   require( kind == HYB_P1_CONST_LAPLACE || kind == HYB_P1_CONST_MASS || kind == HYB_P2_CONST_LAPLACE, "unknown operator kind" );
+   require( min_level >= 0 && min_level <= max_level && max_level <= ( kind == HYB_P2_CONST_LAPLACE ? 13 : 14 ), "invalid level range" );
    set_device( ctx->c );
-   auto* h   = new hyb_op();
-   h->ctx    = ctx;
-   h->o.mesh = &mesh->m;
-   h->o.kind = kind;
-   h->o.minL = min_level;
-   h->o.maxL = max_level;
+   const int shift = kind == HYB_P2_CONST_LAPLACE ? 1 : 0;  // P2 level l is stored on storage level l+1
+   auto*     h     = new hyb_op();
+   h->ctx          = ctx;
+   h->o.mesh       = &mesh->m;
+   h->o.kind       = kind;
+   h->o.order      = 1 + shift;
+   h->o.minL       = min_level + shift;
+   h->o.maxL       = max_level + shift;
    ctx_ref( ctx );
    mesh_ref( &mesh->m );
    try
    {
-      for ( int L = min_level; L <= max_level; ++L ) build_operator_level( &h->o, L );
+      for ( int L = h->o.minL; L <= h->o.maxL; ++L )
+      {
+         if ( shift ) build_p2_constant_level( &h->o, L );
+         else build_operator_level( &h->o, L );
+      }
+      if ( shift ) ensure_p2_constant_device();
    } catch ( ... )
    {
       op_unref( h );
@@ -1186,7 +1193,7 @@ int hyb_op_smooth_sor( hyb_op* op, hyb_fn* dst, hyb_fn* rhs, double relax, int l
    check_op_fn( op, rhs, level );
    require( dst != rhs, "dst and rhs must differ" );
    require( dst->f.dtype == rhs->f.dtype, "value types differ" );
-   require( !op->o.elementwise, "Gauss-Seidel / SOR is provided for constant-stencil operators" );
+   require( !op->o.elementwise && op->o.order == 1, "Gauss-Seidel / SOR is provided for P1 constant-stencil operators" );
    launch_sor( &op->ctx->c, op->o.mesh, &op->o, level, dst->f.dtype, flag, dst->f.ptr( level ), rhs->f.ptr( level ), relax,
                backwards != 0 );
    HYB_CATCH
@@ -1221,6 +1228,14 @@ int hyb_op_inverse_diagonal( hyb_op* op, hyb_fn* out, int level, uint32_t flag )
       sync_copies( out, level );
       return HYB_OK;
    }
+   if ( op->o.kind == HYB_P2_CONST_LAPLACE )
+   {
+      auto padded = from_device( out, level );
+      p2_constant_inverse_diagonal( &op->o, level, flag, padded );
+      to_device( out, level, padded );
+      sync_copies( out, level );
+      return HYB_OK;
+   }
    const OpLevel&  ol = op->o.lv.at( level );
    const P1Level&  P  = op->o.mesh->level( level );
    const Topology& t  = op->o.mesh->topo;
@@ -1251,7 +1266,7 @@ int hyb_op_stencil( hyb_op* op, int level, int cell, int cls, double* out15 )
 {
    HYB_TRY
    require( op && out15, "NULL argument" );
-   require( !op->o.elementwise, "elementwise operators have no constant stencil" );
+   require( !op->o.elementwise && op->o.order == 1, "only P1 constant-stencil operators have a 15-point stencil" );
    require( level >= op->o.minL && level <= op->o.maxL, "level outside the operator's level range" );
    require( cell >= 0 && cell < op->o.mesh->topo.nC && cls >= 0 && cls < kNumClasses, "cell or class out of range" );
    const OpLevel& ol = op->o.lv.at( level );
@@ -1810,8 +1825,8 @@ int hyb_gmg_create( hyb_ctx* ctx, hyb_op* op, const hyb_gmg_params* params, hyb_
    require( p.smoother == HYB_SMOOTHER_JACOBI || p.smoother == HYB_SMOOTHER_CHEBYSHEV || p.smoother == HYB_SMOOTHER_GAUSS_SEIDEL ||
                 p.smoother == HYB_SMOOTHER_SOR,
             "unknown smoother" );
-   require( ( p.smoother != HYB_SMOOTHER_GAUSS_SEIDEL && p.smoother != HYB_SMOOTHER_SOR ) || !op->o.elementwise,
-            "Gauss-Seidel / SOR smoothing is provided for constant-stencil operators" );
+   require( ( p.smoother != HYB_SMOOTHER_GAUSS_SEIDEL && p.smoother != HYB_SMOOTHER_SOR ) || ( !op->o.elementwise && op->o.order == 1 ),
+            "Gauss-Seidel / SOR smoothing is provided for P1 constant-stencil operators" );
    require( p.cycle == HYB_VCYCLE || p.cycle == HYB_WCYCLE, "unknown cycle type" );
    require( p.pre_smooth >= 0 && p.post_smooth >= 0 && p.smooth_increment >= 0, "negative smoothing steps" );
    require( p.coarse_max_iter >= 0, "negative coarse iteration count" );

@@ -62,6 +62,14 @@ extern const int kDirs[kNumDirs][3];
 // 5..10 cell edges 0..5, 11..14 cell vertices 0..3.  Cell-local numbering follows
 // SetupPrimitiveStorage.cpp:305-315 (faces 012, 013, 023, 123; edges 01, 02, 12, 03, 13, 23).
 constexpr int kNumClasses = 15;
+// cell faces touched by each position class (bit 0: z = 0, bit 1: y = 0, bit 2: x = 0, bit 3:
+// x + y + z = n): interior, faces 012 013 023 123, edges 01 02 12 03 13 23, vertices 0..3
+constexpr int kClassFaces[kNumClasses] = { 0, 1, 2, 4, 8, 3, 5, 9, 6, 10, 12, 7, 11, 13, 14 };
+// P2 constant-stencil tables: entries of the eight parity classes' stencils (230 in all, padded),
+// then the eight interior inverse diagonals; one such block per position class and macro-cell
+constexpr int kP2cEntries    = 232;
+constexpr int kP2cInterior   = kP2cEntries + 8;
+constexpr int kP2cCellStride = kP2cInterior + ( kNumClasses - 1 ) * kP2cEntries;
 // bit mask of directions that stay inside the cell for a point of each class
 extern const uint16_t kClassDirMask[kNumClasses];
 int class_of_point(int n, int x, int y, int z);  // host version
@@ -188,6 +196,15 @@ struct Function {
 };
 
 // constant-stencil operator (P1ConstantLaplaceOperator and friends)
+// P2 constant-stencil operator, one storage level: per macro-cell and position class the stencil
+// weights of every parity class of the level-(l+1) node grid (the interior block is followed by the
+// eight interior inverse diagonals), FP64 and an FP32 copy
+struct P2cLevel {
+   std::vector< double > W;  // [nC][kP2cCellStride]
+   double* d_W  = nullptr;
+   float*  d_Wf = nullptr;
+};
+
 struct OpLevel {
    std::vector< double > W;      // [nC][15 classes][15 dirs]
    std::vector< double > invd_b; // per boundary primitive
@@ -253,6 +270,8 @@ struct Operator {
    CellGeom*                 d_geom = nullptr;
    std::vector< CellGeom >   geom;
    std::map< int, ElemLevel > el;
+   // P2 constant-stencil operators (HYB_P2_CONST_LAPLACE), by storage level
+   std::map< int, P2cLevel > p2c;
    ~Operator();
 };
 
@@ -307,6 +326,12 @@ struct StencilArgs {
 
 void launch_stencil( Context* ctx, Mesh* m, Operator* A, int L, int dtype, const StencilArgs& a );
 void launch_elementwise( Context* ctx, Mesh* m, Operator* A, int L, int dtype, const StencilArgs& a );
+// P2 constant-stencil operator (p2_constant.cu); Ls is the storage level (P2 level + 1)
+void launch_p2_constant( Context* ctx, Mesh* m, Operator* A, int Ls, int dtype, const StencilArgs& a );
+void build_p2_constant_level( Operator* A, int Ls );
+void ensure_p2_constant_device();
+void ensure_p2_constant_tables( P2cLevel& pl );
+void p2_constant_inverse_diagonal( const Operator* A, int Ls, uint32_t flag, std::vector< double >& padded );
 void ensure_p2_constants();
 void launch_p2_restrict( Context* ctx, Mesh* m, int Lf, int dtype, uint32_t flag, const void* fine, void* coarse );
 void launch_p2_prolongate( Context* ctx, Mesh* m, int Lc, int dtype, uint32_t flag, const void* coarse, void* fine, int add );

@@ -28,11 +28,6 @@ const int kDirs[kNumDirs][3] = { { 0, 0, 0 },  { -1, 0, 0 }, { 1, 0, 0 },  { 0, 
                                  { 0, 0, -1 }, { 0, 0, 1 },  { -1, 1, 0 }, { 1, -1, 0 }, { -1, 0, 1 },
                                  { 1, 0, -1 }, { 0, -1, 1 }, { 0, 1, -1 }, { 1, -1, 1 }, { -1, 1, -1 } };
 
-// cell faces touched by each position class (bit k = cell face k)
-static const int kClassFaces[kNumClasses] = { 0,  1,  2,  4,  8,              // interior, faces
-                                              3,  5,  9,  6,  10, 12,         // edges 01 02 12 03 13 23
-                                              7,  11, 13, 14 };               // vertices 0..3
-
 static bool dir_ok_for_faces( int faces, const int* d )
 {
    if ( ( faces & 1 ) && d[2] < 0 ) return false;                    // face 012: z = 0
@@ -732,6 +727,11 @@ Operator::~Operator()
       cudaFree( kv.second.d_invd_c );
       cudaFree( kv.second.d_invd_bf );
       cudaFree( kv.second.d_invd_cf );
+   }
+   for ( auto& kv : p2c )
+   {
+      cudaFree( kv.second.d_W );
+      cudaFree( kv.second.d_Wf );
    }
    for ( auto& kv : el )
    {

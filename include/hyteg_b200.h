@@ -55,6 +55,7 @@ extern "C" {
 #define HYB_P2P1_DIV 5 /* P2ToP1ElementwiseBlendingDivOperator / P1ToP2ElementwiseBlendingDivTOperator (P2P1ElementwiseBlendingStokesOperator.hpp:113-116) */
 #define HYB_P1_PSPG 6  /* P1PSPGOperator; its inverted diagonal is P1PSPGInvDiagOperator (P1ConstantOperator.hpp:200-210) */
 #define HYB_P2_FULL_VISCOUS 7 /* P2ElementwiseBlendingFullViscousOperator (elementwiseoperators/P2ElementwiseBlendingFullViscousOperator.hpp:34-68) */
+#define HYB_P2_CONST_LAPLACE 8 /* P2ConstantLaplaceOperator: P2ConstantOperator (constant_stencil_operator/P2ConstantOperator.cpp:100-114), levels are P2 levels */
 
 /* blending maps (geometry/) */
 #define HYB_BLEND_NONE 0
