@@ -65,9 +65,10 @@ constexpr int kNumClasses = 15;
 // cell faces touched by each position class (bit 0: z = 0, bit 1: y = 0, bit 2: x = 0, bit 3:
 // x + y + z = n): interior, faces 012 013 023 123, edges 01 02 12 03 13 23, vertices 0..3
 constexpr int kClassFaces[kNumClasses] = { 0, 1, 2, 4, 8, 3, 5, 9, 6, 10, 12, 7, 11, 13, 14 };
-// P2 constant-stencil tables: entries of the eight parity classes' stencils (230 in all, padded),
-// then the eight interior inverse diagonals; one such block per position class and macro-cell
-constexpr int kP2cEntries    = 232;
+// P2 constant-stencil tables: entries of the eight parity classes' stencils (230 in all; every
+// class starts on a multiple of four entries, so weights load as 16-byte vectors), then the eight
+// interior inverse diagonals; one such block per position class and macro-cell
+constexpr int kP2cEntries    = 256;
 constexpr int kP2cInterior   = kP2cEntries + 8;
 constexpr int kP2cCellStride = kP2cInterior + ( kNumClasses - 1 ) * kP2cEntries;
 // bit mask of directions that stay inside the cell for a point of each class
@@ -200,9 +201,11 @@ struct Function {
 // weights of every parity class of the level-(l+1) node grid (the interior block is followed by the
 // eight interior inverse diagonals), FP64 and an FP32 copy
 struct P2cLevel {
-   std::vector< double > W;  // [nC][kP2cCellStride]
-   double* d_W  = nullptr;
-   float*  d_Wf = nullptr;
+   std::vector< double > W;      // [nC][kP2cCellStride]
+   std::vector< int4 >   tasks;  // boundary tasks grouped by boundary type, then by primitive and parity class
+   double* d_W     = nullptr;
+   float*  d_Wf    = nullptr;
+   int4*   d_tasks = nullptr;
 };
 
 struct OpLevel {

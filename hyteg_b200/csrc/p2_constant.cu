@@ -66,6 +66,7 @@ constexpr P2Pattern make_p2_pattern()
    int       at = 0;
    for ( int k = 0; k < 8; ++k )
    {
+      at                     = ( at + 3 ) / 4 * 4;  // classes start on 16-byte (double2 / float4) boundaries
       bool      hit[5][5][5] = {};
       const int p[3]         = { 8 + ( k & 1 ), 8 + ( ( k >> 1 ) & 1 ), 8 + ( k >> 2 ) };
       for ( int t = 0; t < 6; ++t )
@@ -106,13 +107,18 @@ constexpr P2Pattern make_p2_pattern()
 }
 
 constexpr P2Pattern kP2Pat = make_p2_pattern();
-static_assert( kP2Pat.base[8] == 230 && kP2Pat.cnt[0] == 65 && kP2Pat.cnt[1] == 27 && kP2Pat.cnt[2] == 19,
+static_assert( kP2Pat.cnt[0] + kP2Pat.cnt[1] + kP2Pat.cnt[2] + kP2Pat.cnt[3] + kP2Pat.cnt[4] + kP2Pat.cnt[5] + kP2Pat.cnt[6] +
+                       kP2Pat.cnt[7] == 230 &&
+                   kP2Pat.cnt[0] == 65 && kP2Pat.cnt[1] == 27 && kP2Pat.cnt[2] == 19,
                "P2 stencil sizes of the six-type refinement" );
 static_assert( kP2Pat.base[8] <= kP2cEntries, "entry block too small" );
 static_assert( kSwR == 4 && kSwTX == 64, "the P2 sweep reuses the cell-sweep units: 4 rows by 64 x-points, x0 and y0 odd" );
 
-__constant__ P2Pattern c_p2pat;
-__constant__ int       c_p2c_faces[kNumClasses];  // kClassFaces
+__constant__ int c_p2c_faces[kNumClasses];  // kClassFaces
+// the pattern for lanes that read different classes (boundary owners): offsets (dx, dy, dz) of every
+// entry, and per class its first entry, entry count and centre entry
+__device__ char4 g_p2c_off[kP2cEntries];
+__device__ int   g_p2c_base[24];
 
 // ---------------------------------------------------------------------------------------------
 // host: tables
@@ -241,6 +247,31 @@ void build_p2_constant_level( Operator* A, int Ls )
          }
       for ( int k = 0; k < 8; ++k ) Wc[kP2cEntries + k] = 1.0 / Wc[kP2Pat.base[k] + kP2Pat.centre[k]];
    }
+   // boundary tasks in the grouping of the P1 level (by boundary type, so that a launch covers the
+   // flagged groups), inside a group sorted by primitive and by the parity class of the node in its
+   // first cell: the lanes of a warp then walk the same stencil pattern
+   const P1Level& P = A->mesh->level( Ls );
+   const int      N = P.n;
+   const uint32_t type_bit[4] = { kInner, kDirichlet, kNeumann, kFreeslip };
+   auto           btype = [&]( int b ) {
+      return b < t.nV ? t.bc( t.flag_v[b] ) : ( b < t.nV + t.nE ? t.bc( t.flag_e[b - t.nV] ) : t.bc( t.flag_f[b - t.nV - t.nE] ) );
+   };
+   auto parity = [&]( const std::array< int, 4 >& q ) {
+      const Incidence& I = P.inc[P.inc_begin[q[0]]];
+      const int        x = N * I.o[0] + q[1] * I.e1[0] + q[2] * I.e2[0];
+      const int        y = N * I.o[1] + q[1] * I.e1[1] + q[2] * I.e2[1];
+      const int        z = N * I.o[2] + q[1] * I.e1[2] + q[2] * I.e2[2];
+      return ( x & 1 ) | ( ( y & 1 ) << 1 ) | ( ( z & 1 ) << 2 );
+   };
+   for ( int g = 0; g < 4; ++g )
+   {
+      std::vector< std::pair< int64_t, int > > key;
+      for ( size_t q = 0; q < P.tasks.size(); ++q )
+         if ( btype( P.tasks[q][0] ) == type_bit[g] ) key.push_back( { int64_t( P.tasks[q][0] ) * 8 + parity( P.tasks[q] ), int( q ) } );
+      std::stable_sort( key.begin(), key.end(), []( const auto& a, const auto& c ) { return a.first < c.first; } );
+      for ( const auto& kq : key ) pl.tasks.push_back( make_int4( P.tasks[kq.second][0], P.tasks[kq.second][1], P.tasks[kq.second][2], 0 ) );
+   }
+   if ( pl.tasks.size() != P.tasks.size() ) throw std::logic_error( "boundary task without a single boundary type" );
    A->p2c[Ls] = std::move( pl );
 }
 
@@ -251,7 +282,12 @@ static void          p2c_attributes_all();
 void ensure_p2_constant_device()
 {
    g_p2c_once.run( [] {
-      check_cuda( cudaMemcpyToSymbol( c_p2pat, &kP2Pat, sizeof( kP2Pat ) ), "constants(P2 pattern)" );
+      char4 off[kP2cEntries] = {};
+      for ( int e = 0; e < kP2cEntries; ++e ) off[e] = make_char4( kP2Pat.off[e][0], kP2Pat.off[e][1], kP2Pat.off[e][2], 0 );
+      int base[24];
+      for ( int k = 0; k < 8; ++k ) base[k] = kP2Pat.base[k], base[k + 8] = kP2Pat.cnt[k], base[k + 16] = kP2Pat.centre[k];
+      check_cuda( cudaMemcpyToSymbol( g_p2c_off, off, sizeof( off ) ), "constants(P2 pattern)" );
+      check_cuda( cudaMemcpyToSymbol( g_p2c_base, base, sizeof( base ) ), "constants(P2 pattern)" );
       check_cuda( cudaMemcpyToSymbol( c_p2c_faces, kClassFaces, sizeof( kClassFaces ) ), "constants(P2 classes)" );
       p2c_attributes_all();
    } );
@@ -265,6 +301,9 @@ void ensure_p2_constant_tables( P2cLevel& pl )
    check_cuda( cudaMalloc( &pl.d_Wf, wf.size() * sizeof( float ) ), "cudaMalloc(P2 stencils)" );
    check_cuda( cudaMemcpy( pl.d_W, pl.W.data(), pl.W.size() * sizeof( double ), cudaMemcpyHostToDevice ), "upload P2 stencils" );
    check_cuda( cudaMemcpy( pl.d_Wf, wf.data(), wf.size() * sizeof( float ), cudaMemcpyHostToDevice ), "upload P2 stencils" );
+   check_cuda( cudaMalloc( &pl.d_tasks, std::max< size_t >( pl.tasks.size(), 1 ) * sizeof( int4 ) ), "cudaMalloc(P2 tasks)" );
+   if ( !pl.tasks.empty() )
+      check_cuda( cudaMemcpy( pl.d_tasks, pl.tasks.data(), pl.tasks.size() * sizeof( int4 ), cudaMemcpyHostToDevice ), "upload P2 tasks" );
 }
 
 // inverse diagonal of every owned slot flagged by `flag` (padded level layout), from the tables
@@ -324,6 +363,71 @@ struct P2cCfg
    static_assert( ROWS <= 32, "one row copy per lane" );
 };
 
+// 16-byte vectors of weights
+template < typename A >
+struct WVec;
+template <>
+struct WVec< double >
+{
+   using type              = double2;
+   static constexpr int n = 2;
+};
+template <>
+struct WVec< float >
+{
+   using type              = float4;
+   static constexpr int n = 4;
+};
+template < typename A >
+using WVec_t = typename WVec< A >::type;
+template < int I >
+__device__ __forceinline__ double vget( const double2& v )
+{
+   return I == 0 ? v.x : v.y;
+}
+template < int I >
+__device__ __forceinline__ float vget( const float4& v )
+{
+   return I == 0 ? v.x : I == 1 ? v.y : I == 2 ? v.z : v.w;
+}
+
+// the six values x0 - 2 + 2 lane + i (i < 6) of a stage row; q = row start + 2 lane, sh = the row's
+// shift (the stage row starts sh elements before x0 - 2).  FP64 and FP32 rows are read in 16- and
+// 8-byte pairs from an aligned pair boundary (conflict-free), FP16 value by value.
+__device__ __forceinline__ void load_row6( const double* q, int sh, double val[6] )
+{
+   const double2* p = reinterpret_cast< const double2* >( q );  // 2 lane even, rows of even width
+   if ( sh & 1 )
+   {
+      const double2 a = p[0], b = p[1], c = p[2], d = p[3];
+      val[0] = a.y, val[1] = b.x, val[2] = b.y, val[3] = c.x, val[4] = c.y, val[5] = d.x;
+   }
+   else
+   {
+      const double2 a = p[0], b = p[1], c = p[2];
+      val[0] = a.x, val[1] = a.y, val[2] = b.x, val[3] = b.y, val[4] = c.x, val[5] = c.y;
+   }
+}
+__device__ __forceinline__ void load_row6( const float* q, int sh, float val[6] )
+{
+   const float2* p = reinterpret_cast< const float2* >( q + ( sh & ~1 ) );
+   if ( sh & 1 )
+   {
+      const float2 a = p[0], b = p[1], c = p[2], d = p[3];
+      val[0] = a.y, val[1] = b.x, val[2] = b.y, val[3] = c.x, val[4] = c.y, val[5] = d.x;
+   }
+   else
+   {
+      const float2 a = p[0], b = p[1], c = p[2];
+      val[0] = a.x, val[1] = a.y, val[2] = b.x, val[3] = b.y, val[4] = c.x, val[5] = c.y;
+   }
+}
+__device__ __forceinline__ void load_row6( const __half* q, int sh, float val[6] )
+{
+#pragma unroll
+   for ( int i = 0; i < 6; ++i ) val[i] = __half2float( q[sh + i] );
+}
+
 template < int B, int E, typename F >
 __device__ __forceinline__ void static_for( F&& f )
 {
@@ -365,7 +469,7 @@ __global__ void __launch_bounds__( kP2cWarps * 32, 2 )
    // ---- loads: lane r < R+4 copies row y0-2+r of every slice z_first-2 .. z_last+2 of the warp's units
    const bool is_row = lane < R + 4;
    int        pu = v.swbegin[0][gw], ps = 0, pyy = 0, px0 = 0;
-   int64_t    pcb = 0;
+   int64_t    pcb = 0, prb = 0;  // cell offset; start of this lane's row in slice ps (cell-relative)
    int4       PU  = make_int4( 0, 0, 0, 0 );
    auto       open = [&]() {
       while ( pu < u1 && !active( pu ) ) ++pu;
@@ -376,6 +480,7 @@ __global__ void __launch_bounds__( kP2cWarps * 32, 2 )
          ps  = PU.z - 2;
          pyy = PU.y - 2 + lane;
          px0 = PU.x & kSwUnitXMask;
+         prb = cidx( N, 0, pyy, ps );  // the polynomial also serves rows and slices outside the cell
       }
    };
    open();
@@ -390,7 +495,7 @@ __global__ void __launch_bounds__( kP2cWarps * 32, 2 )
          const int xe = min( px0 + 65, N - pyy - ps );  // last x of the row segment
          if ( xe >= px0 - 2 && xe >= 0 )
          {
-            const int64_t rs = pcb + cidx( N, 0, pyy, ps );
+            const int64_t rs = pcb + prb;
             const int64_t g0 = rs + px0 - 2;  // x0 - 2 >= -1: at worst the slot before the row, inside the buffer
             a0s              = g0 & ~int64_t( AL - 1 );
             bytes            = uint32_t( ( ( rs + xe + 1 + AL - 1 ) / AL * AL - a0s ) * int64_t( sizeof( T ) ) );
@@ -402,6 +507,7 @@ __global__ void __launch_bounds__( kP2cWarps * 32, 2 )
       if ( bytes ) bulk_copy_g2s( ring + st * Cfg::stage + lane * RW, src + a0s, bytes, &full[st] );
       ++issued;
       ist = ist + 1 == D ? 0 : ist + 1;
+      prb += slice_step( N, ps ) - pyy;
       if ( ++ps > PU.w + 2 )
       {
          ++pu;
@@ -437,41 +543,53 @@ __global__ void __launch_bounds__( kP2cWarps * 32, 2 )
       const int4    U  = uu[u];
       const int     x0 = U.x & kSwUnitXMask, y0 = U.y, za = U.z, zb = U.w;
       const int64_t cb = v.cell_off[c];
-      A             acc[5][R][2];  // [slot: output slice s-2+slot][row][point]
+      // row starts, kept by additions from slice to slice (cidx(0, y, z+1) = cidx(0, y, z) + tri(N+1-z) - y,
+      // a polynomial identity that also holds for the rows and slices outside the cell): shw packs the
+      // shift (row start + x0 - 2 mod 8) of the eight stage rows of slice s in 3-bit fields, rbo the
+      // cell-relative starts of the four output rows of slice s - 2
+      uint32_t shw = 0;
+#pragma unroll
+      for ( int jj = 0; jj < R + 4; ++jj ) shw |= uint32_t( ( cb + cidx( N, 0, y0 - 2 + jj, za - 2 ) + x0 - 2 ) & 7 ) << ( 3 * jj );
+      int rbo[R];
+#pragma unroll
+      for ( int j = 0; j < R; ++j ) rbo[j] = int( cidx( N, 0, y0 + j, za - 4 ) );
+      A acc[5][R][2];  // [slot k: output slice s-2+k][row][point]
 #pragma unroll
       for ( int k = 0; k < 5; ++k )
 #pragma unroll
          for ( int j = 0; j < R; ++j ) acc[k][j][0] = acc[k][j][1] = A( 0 );
-      // one slice step; SP = parity of the slice s
-      auto step = [&]( int s, auto sp_c ) -> bool {
-         constexpr int SP = decltype( sp_c )::value;
+      // one slice: slice s (parity SP) folded into slots KO .. KO+4 (outputs s-2 .. s+2), then the
+      // stage is handed back and output slice s-2 (slot KO) written
+      auto slice = [&]( int s, auto sp_c, auto ko_c ) -> bool {
+         constexpr int SP = decltype( sp_c )::value, KO = decltype( ko_c )::value;
          if ( !__all_sync( 0xffffffffu, mbar_wait_bounded( &full[cst], cph, nullptr ) ) ) return false;
          const T* Rg = ring + cst * Cfg::stage;
          static_for< 0, R + 4 >( [&]( auto jj_c ) {
             constexpr int JJ = decltype( jj_c )::value;
-            const int     yy = y0 - 2 + JJ;
-            const int     sh = int( ( cb + cidx( N, 0, yy, s ) + x0 - 2 ) & ( AL - 1 ) );  // only the parity of the row start matters
-            const T*      rp = Rg + JJ * RW + sh + 2 * lane;                             // rp[i] = value at x0 - 2 + 2 lane + i
-            A             val[6];
-#pragma unroll
-            for ( int i = 0; i < 6; ++i ) val[i] = A( rp[i] );
+            const int     sh = int( ( shw >> ( 3 * JJ ) ) & ( AL - 1 ) );  // shift of the row in its stage row
+            A             val[6];  // values at x0 - 2 + 2 lane + i
+            load_row6( Rg + JJ * RW + 2 * lane, sh, val );
             static_for< 0, R >( [&]( auto j_c ) {
                constexpr int J  = decltype( j_c )::value;
                constexpr int DY = JJ - 2 - J;
                if constexpr ( DY >= -2 && DY <= 2 )
                   static_for< 0, 5 >( [&]( auto k_c ) {
-                     constexpr int KS = decltype( k_c )::value;  // slot: output slice s - 2 + KS
+                     constexpr int KS = decltype( k_c )::value;  // output slice s - 2 + KS
                      constexpr int DZ = 2 - KS;
                      static_for< 0, 2 >( [&]( auto p_c ) {
                         constexpr int PP = decltype( p_c )::value;
                         // parity class of the output point (x0 + 2 lane + PP, y0 + J, s - 2 + KS); x0, y0 odd
                         constexpr int KC = ( ( 1 + PP ) & 1 ) | ( ( ( 1 + J ) & 1 ) << 1 ) | ( ( ( SP + KS ) & 1 ) << 2 );
                         constexpr int E0 = kP2Pat.rng[KC][DZ + 2][DY + 2][0], E1 = kP2Pat.rng[KC][DZ + 2][DY + 2][1];
+                        WVec_t< A > wv;
                         static_for< E0, E1 >( [&]( auto e_c ) {
                            constexpr int EI = decltype( e_c )::value;
                            constexpr int WI = kP2Pat.base[KC] + EI;
                            constexpr int I  = kP2Pat.off[WI][0] + 2 + PP;
-                           acc[KS][J][PP] += Wsm[WI] * val[I];
+                           constexpr int VW = WVec< A >::n;
+                           // weights in 16-byte vectors: one shared load per vector of the group
+                           if constexpr ( EI == E0 || WI % VW == 0 ) wv = *reinterpret_cast< const WVec_t< A >* >( Wsm + WI / VW * VW );
+                           acc[KO + KS][J][PP] += vget< WI % VW >( wv ) * val[I];
                         } );
                      } );
                   } );
@@ -483,8 +601,7 @@ __global__ void __launch_bounds__( kP2cWarps * 32, 2 )
          ++ld;
          if ( ++cst == D ) cst = 0, cph ^= 1u;
          issue();
-         // output slice s - 2 is complete
-         const int z = s - 2;
+         const int z = s - 2;  // complete
          if ( z >= za && z <= zb )
          {
             static_for< 0, R >( [&]( auto j_c ) {
@@ -493,21 +610,34 @@ __global__ void __launch_bounds__( kP2cWarps * 32, 2 )
                const int     xl = x0 + 2 * lane;
                if ( y + z <= N - 2 )
                {
-                  const int64_t rb = cb + cidx( N, 0, y, z );
+                  const int64_t rb = cb + rbo[J];
                   static_for< 0, 2 >( [&]( auto p_c ) {
                      constexpr int PP = decltype( p_c )::value;
-                     constexpr int KX = ( ( 1 + PP ) & 1 ) | ( ( ( 1 + J ) & 1 ) << 1 );
+                     constexpr int KX = ( ( 1 + PP ) & 1 ) | ( ( ( 1 + J ) & 1 ) << 1 ) | ( ( SP & 1 ) << 2 );
                      const int     x  = xl + PP;
                      if ( x + y + z <= N - 1 )
-                     {
-                        const A invd = Wsm[kP2cEntries + ( KX | ( ( ( SP + 0 ) & 1 ) << 2 ) )];
-                        stencil_epilogue< T, A, OP >( rb + x, acc[0][J][PP], invd, src, v1, v2, dst, a0, a1 );
-                     }
+                        stencil_epilogue< T, A, OP >( rb + x, acc[KO][J][PP], Wsm[kP2cEntries + KX], src, v1, v2, dst, a0, a1 );
                   } );
                }
             } );
          }
-         // rotate the slots: output slice s - 1 moves to slot 0, a fresh slice s + 3 enters slot 4
+         // advance the row starts to slice s + 1 (stage rows) and s - 1 (output rows)
+         const uint32_t ts = uint32_t( int64_t( N + 1 - s ) * ( N + 2 - s ) / 2 );
+         uint32_t       nw = 0;
+#pragma unroll
+         for ( int jj = 0; jj < R + 4; ++jj )
+            nw |= ( ( ( shw >> ( 3 * jj ) ) + ts - uint32_t( y0 - 2 + jj ) ) & 7u ) << ( 3 * jj );
+         shw          = nw;
+         const int tz = int( int64_t( N + 3 - s ) * ( N + 4 - s ) / 2 );  // tri(N + 1 - (s - 2))
+#pragma unroll
+         for ( int j = 0; j < R; ++j ) rbo[j] += tz - ( y0 + j );
+         return true;
+      };
+      using I0 = std::integral_constant< int, 0 >;
+      using I1 = std::integral_constant< int, 1 >;
+      // after each slice, outputs s-1 .. s+2 move down one slot and slot 4 starts output s+3
+      auto step = [&]( int s, auto sp_c ) -> bool {
+         if ( !slice( s, sp_c, I0{} ) ) return false;
 #pragma unroll
          for ( int k = 0; k < 4; ++k )
 #pragma unroll
@@ -516,9 +646,7 @@ __global__ void __launch_bounds__( kP2cWarps * 32, 2 )
          for ( int j = 0; j < R; ++j ) acc[4][j][0] = acc[4][j][1] = A( 0 );
          return true;
       };
-      using I0 = std::integral_constant< int, 0 >;
-      using I1 = std::integral_constant< int, 1 >;
-      // one call site per slice parity, so both instantiations of the step are inlined
+      // one call site per parity, so both instantiations are inlined
       bool ok = true;
       for ( int s = za - 2; ok && s <= zb + 2; ++s )
       {
@@ -539,9 +667,9 @@ __device__ __forceinline__ bool p2c_inside( int faces, int dx, int dy, int dz )
 }
 
 template < typename T, typename A, int OP >
-__global__ void __launch_bounds__( 256 ) k_p2c_bnd( LevelView v, const A* __restrict__ W, TaskSegments seg, uint32_t flag,
-                                                     int copy_unflagged, const T* __restrict__ src, const T* __restrict__ v1, T* v2,
-                                                     T* dst, A a0, A a1 )
+__global__ void __launch_bounds__( 256 ) k_p2c_bnd( LevelView v, const A* __restrict__ W, const int4* __restrict__ tasks, TaskSegments seg,
+                                                     uint32_t flag, int copy_unflagged, const T* __restrict__ src, const T* __restrict__ v1,
+                                                     T* v2, T* dst, A a0, A a1 )
 {
    int t = blockIdx.x * blockDim.x + threadIdx.x, at = -1;
 #pragma unroll
@@ -551,7 +679,7 @@ __global__ void __launch_bounds__( 256 ) k_p2c_bnd( LevelView v, const A* __rest
       if ( at < 0 ) t -= seg.count[g];
    }
    if ( at < 0 ) return;
-   const int4    tk    = v.btasks[at];
+   const int4    tk    = tasks[at];
    const int     b     = tk.x, i = tk.y, j = tk.z, N = v.n;
    const int64_t owner = owner_slot( v, b, i, j );
    if ( !( v.bc[b] & flag ) )
@@ -569,17 +697,36 @@ __global__ void __launch_bounds__( 256 ) k_p2c_bnd( LevelView v, const A* __rest
       inc_point( I, N, i, j, x, y, z );
       const int      k     = ( x & 1 ) | ( ( y & 1 ) << 1 ) | ( ( z & 1 ) << 2 );
       const int      faces = c_p2c_faces[I.cls];
-      const int      e0    = c_p2pat.base[k], ne = c_p2pat.cnt[k];
+      const int      e0    = g_p2c_base[k], ne = g_p2c_base[k + 8];
       const A*       w     = W + size_t( I.cell ) * kP2cCellStride + ( I.cls == 0 ? 0 : kP2cInterior + ( I.cls - 1 ) * kP2cEntries ) + e0;
       const T*       s     = src + v.cell_off[I.cell];
       A              part  = A( 0 );
+      // cell-relative starts of the slices z-2 .. z+2 (32-bit: the host limits the level), from
+      // slice z by the slice sizes tri(N+1-z') = (N+1-z')(N+2-z')/2
+      const int w1 = N + 1;
+      int       S[5];
+      S[2] = int( cidx( N, 0, 0, z ) );
+      S[3] = S[2] + ( w1 - z ) * ( w1 - z + 1 ) / 2;
+      S[4] = S[3] + ( w1 - z - 1 ) * ( w1 - z ) / 2;
+      S[1] = S[2] - ( w1 - z + 1 ) * ( w1 - z + 2 ) / 2;
+      S[0] = S[1] - ( w1 - z + 2 ) * ( w1 - z + 3 ) / 2;
+      // entries are sorted by (dz, dy): the row start is recomputed only when that pair changes
+      int pr = 0x7fffffff, rb = 0;
       for ( int e = 0; e < ne; ++e )
       {
-         const int dx = c_p2pat.off[e0 + e][0], dy = c_p2pat.off[e0 + e][1], dz = c_p2pat.off[e0 + e][2];
-         if ( p2c_inside( faces, dx, dy, dz ) ) part += w[e] * A( ldv( s + cidx( N, x + dx, y + dy, z + dz ) ) );
+         const char4 o = g_p2c_off[e0 + e];
+         if ( !p2c_inside( faces, o.x, o.y, o.z ) ) continue;
+         const int r = o.y * 8 + o.z;
+         if ( r != pr )
+         {
+            const int yy = y + o.y, zz = z + o.z;
+            rb = S[o.z + 2] + yy * ( w1 - zz ) - ( yy * ( yy - 1 ) ) / 2;  // start of row yy of slice zz
+            pr = r;
+         }
+         part += w[e] * A( ldv( s + rb + x + o.x ) );
       }
       acc += part;
-      diag += w[c_p2pat.centre[k]];
+      diag += w[g_p2c_base[k + 16]];
    }
    const A invd = A( 1 ) / diag;
    if constexpr ( OP == OP_APPLY ) write_through( v, dst, b, i, j, owner, acc );
@@ -629,7 +776,7 @@ static void p2c_attributes_all()
 }
 
 template < typename T, typename A, int OP >
-static void run_p2c( Context* ctx, const LevelView& v, const A* W, int nC, const StencilArgs& a )
+static void run_p2c( Context* ctx, const LevelView& v, const A* W, const int4* tasks, int nC, const StencilArgs& a )
 {
    using Cfg            = P2cCfg< T, A >;
    const T*           src = (const T*) a.src;
@@ -642,13 +789,15 @@ static void run_p2c( Context* ctx, const LevelView& v, const A* W, int nC, const
    // the second vector, so the two kernels run one after the other on the context stream
    if ( nt > 0 )
    {
-      k_p2c_bnd< T, A, OP ><<< ( nt + 255 ) / 256, 256, 0, ctx->stream >>>( v, W, seg, a.flag, a.copy_unflagged, src, v1, v2, dst, A( a.a0 ),
+      k_p2c_bnd< T, A, OP ><<< ( nt + 255 ) / 256, 256, 0, ctx->stream >>>( v, W, tasks, seg, a.flag, a.copy_unflagged, src, v1, v2, dst, A( a.a0 ),
                                                                             A( a.a1 ) );
       ++ctx->launches;
    }
    const int nw = v.nswarps[0];
    if ( nw > 0 && nC > 0 && v.n >= 4 )
    {
+      // the sweep keeps cell-relative row starts in 32-bit integers
+      if ( tet_size( int64_t( v.n ) + 1 ) > int64_t( 0x7fffffff ) ) throw std::invalid_argument( "P2 constant operator: level too large" );
       k_p2c_sweep< T, A, OP ><<< nw / kP2cWarps, kP2cWarps * 32, Cfg::smem_bytes, ctx->stream >>>( v, W, a.flag, src, v1, v2, dst, A( a.a0 ),
                                                                                               A( a.a1 ), nC, ctx->d_error );
       ++ctx->launches;
@@ -657,18 +806,18 @@ static void run_p2c( Context* ctx, const LevelView& v, const A* W, int nC, const
 }
 
 template < typename T, typename A >
-static void dispatch_p2c( Context* ctx, const LevelView& v, const A* W, int nC, const StencilArgs& a )
+static void dispatch_p2c( Context* ctx, const LevelView& v, const A* W, const int4* tasks, int nC, const StencilArgs& a )
 {
    switch ( a.op )
    {
-   case OP_APPLY: return run_p2c< T, A, OP_APPLY >( ctx, v, W, nC, a );
-   case OP_APPLY_ADD: return run_p2c< T, A, OP_APPLY_ADD >( ctx, v, W, nC, a );
-   case OP_RESID: return run_p2c< T, A, OP_RESID >( ctx, v, W, nC, a );
-   case OP_JAC: return run_p2c< T, A, OP_JAC >( ctx, v, W, nC, a );
-   case OP_CHEB0: return run_p2c< T, A, OP_CHEB0 >( ctx, v, W, nC, a );
-   case OP_CHEBI: return run_p2c< T, A, OP_CHEBI >( ctx, v, W, nC, a );
-   case OP_CHEBL: return run_p2c< T, A, OP_CHEBL >( ctx, v, W, nC, a );
-   case OP_DINV_APPLY: return run_p2c< T, A, OP_DINV_APPLY >( ctx, v, W, nC, a );
+   case OP_APPLY: return run_p2c< T, A, OP_APPLY >( ctx, v, W, tasks, nC, a );
+   case OP_APPLY_ADD: return run_p2c< T, A, OP_APPLY_ADD >( ctx, v, W, tasks, nC, a );
+   case OP_RESID: return run_p2c< T, A, OP_RESID >( ctx, v, W, tasks, nC, a );
+   case OP_JAC: return run_p2c< T, A, OP_JAC >( ctx, v, W, tasks, nC, a );
+   case OP_CHEB0: return run_p2c< T, A, OP_CHEB0 >( ctx, v, W, tasks, nC, a );
+   case OP_CHEBI: return run_p2c< T, A, OP_CHEBI >( ctx, v, W, tasks, nC, a );
+   case OP_CHEBL: return run_p2c< T, A, OP_CHEBL >( ctx, v, W, tasks, nC, a );
+   case OP_DINV_APPLY: return run_p2c< T, A, OP_DINV_APPLY >( ctx, v, W, tasks, nC, a );
    default: throw std::invalid_argument( "unknown stencil operation" );
    }
 }
@@ -680,9 +829,9 @@ void launch_p2_constant( Context* ctx, Mesh* m, Operator* op, int Ls, int dtype,
    ensure_p2_constant_tables( pl );
    const LevelView v  = make_view( m, Ls );
    const int       nC = m->topo.nC;
-   if ( dtype == F64 ) dispatch_p2c< double, double >( ctx, v, pl.d_W, nC, a );
-   else if ( dtype == F32 ) dispatch_p2c< float, float >( ctx, v, pl.d_Wf, nC, a );
-   else dispatch_p2c< __half, float >( ctx, v, pl.d_Wf, nC, a );
+   if ( dtype == F64 ) dispatch_p2c< double, double >( ctx, v, pl.d_W, pl.d_tasks, nC, a );
+   else if ( dtype == F32 ) dispatch_p2c< float, float >( ctx, v, pl.d_Wf, pl.d_tasks, nC, a );
+   else dispatch_p2c< __half, float >( ctx, v, pl.d_Wf, pl.d_tasks, nC, a );
 }
 
 }  // namespace hyb

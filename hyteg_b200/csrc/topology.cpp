@@ -732,6 +732,7 @@ Operator::~Operator()
    {
       cudaFree( kv.second.d_W );
       cudaFree( kv.second.d_Wf );
+      cudaFree( kv.second.d_tasks );
    }
    for ( auto& kv : el )
    {
