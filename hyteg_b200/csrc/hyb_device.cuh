@@ -61,6 +61,7 @@ struct LevelView
    int              ntasks;
    const int4*      tasks;
    const int4*      btasks;      // the same tasks grouped by their primitive's boundary type
+   const FaceRec*   frec;        // per grouped task: its two-cell face record (cell0 < 0: none)
    int              bcount[4];   // tasks per group: Inner, Dirichlet, Neumann, Freeslip
    const int64_t*   off;       // all primitives
    const int64_t*   cell_off;  // off + nB
@@ -101,6 +102,7 @@ static inline LevelView make_view( Mesh* m, int L )
    v.ntasks    = int( P.tasks.size() );
    v.tasks     = P.d_tasks;
    v.btasks    = P.d_btasks;
+   v.frec      = P.d_frec;
    for ( int g = 0; g < 4; ++g ) v.bcount[g] = P.bcount[g];
    v.off       = P.d_off;
    v.cell_off  = P.d_off + P.nB;

@@ -75,6 +75,22 @@ constexpr int kP2cCellStride = kP2cInterior + ( kNumClasses - 1 ) * kP2cEntries;
 extern const uint16_t kClassDirMask[kNumClasses];
 int class_of_point(int n, int x, int y, int z);  // host version
 
+// A face-interior boundary task between two macro-cells, resolved once per level for the boundary
+// stencil kernel: the owner slot, the slots of the owner's copies in the two cell arrays (the centres
+// of the cells' class stencils), their rows and slices, cells and position classes, the face's
+// boundary-primitive index and type.  cell0 < 0 marks any other task.
+struct FaceRec {
+   int64_t owner;
+   int64_t c0, c1;
+   int     b;
+   int     cell0, cell1;
+   int16_t y0, z0, y1, z1;
+   int8_t  cls0, cls1;
+   uint8_t bc;
+   uint8_t pad;
+};
+static_assert( sizeof( FaceRec ) == 48, "face record layout" );
+
 struct Incidence {
    int   cell;
    int   cls;
@@ -160,6 +176,7 @@ struct P1Level {
    Incidence* d_inc       = nullptr;
    int4*      d_tasks     = nullptr;
    int4*      d_btasks    = nullptr;  // tasks grouped by boundary type (Inner, Dirichlet, Neumann, Freeslip)
+   FaceRec*   d_frec      = nullptr;  // per grouped task: its two-cell face record, if it is one
    int        bcount[4]   = {};
    int2*      d_rows      = nullptr;
    int4*      d_march     = nullptr;

@@ -862,6 +862,25 @@ __device__ __forceinline__ StencilAt< A > class_stencil_at( const T* s, const A*
    return { acc, r00 + x };
 }
 
+// the same sum for a point given by its slot c in the level buffer (cell offset included) and its row
+// y and slice z in the cell: the neighbours are c plus offsets that depend on y and z only
+template < typename T, typename A >
+__device__ __forceinline__ A class_stencil_slot( const T* src, const A* W, uint16_t mask, int n, int64_t c, int y, int z )
+{
+   const int64_t ly  = n + 1 - z - y;
+   const int64_t tz  = int64_t( n + 1 - z ) * ( n + 2 - z ) / 2;
+   const int64_t dm0 = -( ly + 1 ), dp0 = ly, d0p = tz - y, d0m = -( tz + ( n + 2 - z ) - y );
+   const int64_t dmp = d0p - ly, dpm = d0m + ly + 1;
+   const int64_t idx[kNumDirs] = { c,           c - 1,       c + 1,       c + dm0,     c + dp0,
+                                   c + d0m,     c + d0p,     c + dp0 - 1, c + dm0 + 1, c + d0p - 1,
+                                   c + d0m + 1, c + dmp,     c + dpm,     c + dmp + 1, c + dpm - 1 };
+   A acc = A( 0 );
+#pragma unroll
+   for ( int d = 0; d < kNumDirs; ++d )
+      if ( mask & ( 1u << d ) ) acc += W[d] * A( ldv( src + idx[d] ) );
+   return acc;
+}
+
 template < typename T, typename A >
 __device__ __forceinline__ A class_stencil( const T* s, const A* W, uint16_t mask, int n, int x, int y, int z )
 {
@@ -975,6 +994,36 @@ __global__ void __launch_bounds__( 256 ) k_bnd_stencil( LevelView v, OpView< A >
       if ( at < 0 ) t -= seg.count[g];
    }
    if ( at < 0 ) return;
+   // a flagged face point between two cells: everything the stencil needs comes from one record,
+   // so the value loads follow a single dependent load (the same sums, in the same order, as bnd_task)
+   const FaceRec r = v.frec[at];
+   if ( r.cell0 >= 0 && ( r.bc & flag ) )
+   {
+      const A s0 = class_stencil_slot< T, A >( src, o.W + ( size_t( r.cell0 ) * kNumClasses + r.cls0 ) * kNumDirs, c_cls_mask[r.cls0], v.n,
+                                              r.c0, r.y0, r.z0 );
+      const A s1 = class_stencil_slot< T, A >( src, o.W + ( size_t( r.cell1 ) * kNumClasses + r.cls1 ) * kNumDirs, c_cls_mask[r.cls1], v.n,
+                                              r.c1, r.y1, r.z1 );
+      const A acc  = ( A( 0 ) + s0 ) + s1;
+      const A invd = o.invd_b[r.b];
+      auto    put  = [&]( T* vec, A val ) {
+         stv( vec + r.owner, val );
+         stv( vec + r.c0, val );
+         stv( vec + r.c1, val );
+      };
+      if constexpr ( OP == OP_APPLY ) put( dst, acc );
+      else if constexpr ( OP == OP_APPLY_ADD ) put( dst, A( ldc( dst + r.owner ) ) + acc );
+      else if constexpr ( OP == OP_RESID ) put( dst, A( ldv( v1 + r.owner ) ) - acc );
+      else if constexpr ( OP == OP_JAC ) put( dst, A( ldv( src + r.owner ) ) + a0 * ( invd * ( A( ldv( v1 + r.owner ) ) - acc ) ) );
+      else if constexpr ( OP == OP_CHEB0 ) put( dst, invd * ( A( ldv( v1 + r.owner ) ) - acc ) );
+      else if constexpr ( OP == OP_CHEBI )
+      {
+         put( dst, invd * acc );
+         put( v2, A( ldc( v2 + r.owner ) ) + a0 * A( ldv( src + r.owner ) ) );
+      }
+      else if constexpr ( OP == OP_CHEBL ) put( v2, ( A( ldc( v2 + r.owner ) ) + a0 * A( ldv( src + r.owner ) ) ) + a1 * ( invd * acc ) );
+      else if constexpr ( OP == OP_DINV_APPLY ) put( dst, invd * acc );
+      return;
+   }
    bnd_task< T, A, OP >( v, o, flag, copy_unflagged, src, v1, v2, dst, a0, a1, v.btasks[at] );
 }
 

@@ -498,6 +498,33 @@ void ensure_device( Mesh* m, P1Level& P )
       }
       if ( bt.size() != tk.size() ) throw std::logic_error( "boundary task without a single boundary type" );
       up( &P.d_btasks, bt.data(), bt.size() );
+      std::vector< FaceRec > fr( bt.size() );
+      const int              n = P.n;
+      for ( size_t k = 0; k < bt.size(); ++k )
+      {
+         FaceRec&  r = fr[k];
+         const int b = bt[k].x, i = bt[k].y, j = bt[k].z;
+         r         = FaceRec{};
+         r.cell0   = -1;
+         if ( b < t.nV + t.nE || P.inc_begin[b + 1] - P.inc_begin[b] != 2 ) continue;
+         r.owner = P.off[b] + fidx( n, i, j );
+         r.b     = b;
+         r.bc    = uint8_t( t.bc( t.flag_f[b - t.nV - t.nE] ) );
+         for ( int s = 0; s < 2; ++s )
+         {
+            const Incidence& I = P.inc[P.inc_begin[b] + s];
+            const int        x = n * I.o[0] + i * I.e1[0] + j * I.e2[0];
+            const int        y = n * I.o[1] + i * I.e1[1] + j * I.e2[1];
+            const int        z = n * I.o[2] + i * I.e1[2] + j * I.e2[2];
+            const int64_t    c = P.off[P.nB + I.cell] + cidx( n, x, y, z );
+            ( s ? r.c1 : r.c0 )     = c;
+            ( s ? r.cell1 : r.cell0 ) = I.cell;
+            ( s ? r.y1 : r.y0 )     = int16_t( y );
+            ( s ? r.z1 : r.z0 )     = int16_t( z );
+            ( s ? r.cls1 : r.cls0 ) = int8_t( I.cls );
+         }
+      }
+      up( &P.d_frec, fr.data(), fr.size() );
    }
    std::vector< int2 > rw( P.rows.size() );
    for ( size_t i = 0; i < rw.size(); ++i ) rw[i] = make_int2( P.rows[i][0], P.rows[i][1] );
@@ -569,6 +596,7 @@ Mesh::~Mesh()
       cudaFree( P.d_inc );
       cudaFree( P.d_tasks );
       cudaFree( P.d_btasks );
+      cudaFree( P.d_frec );
       cudaFree( P.d_rows );
       cudaFree( P.d_march );
       cudaFree( P.d_zunits ), cudaFree( P.d_zcell ), cudaFree( P.d_zbegin );
