@@ -536,6 +536,12 @@ def p2_leg(H, ctx, level=5, cycle_level=3):
     out["apply"] = {"level": level, "micro_cells": mc, "dofs": pm.packed_size(level + 1), "ms": sec * 1e3,
                     "Mcells_per_s": mc / sec / 1e6, "gflops_reference_count": mc * 11878 / sec / 1e9}
     del A
+    # the hyteg-operators form: k stored as a P2 function (interpolated at the blended nodes)
+    An = H.P2ElementwiseDivKGradOperator(pm, level, level, ctx, k=K, blending="shell")
+    sec = time_apply(An, level, 3)
+    out["apply_nodal_coefficient"] = {"level": level, "micro_cells": mc, "ms": sec * 1e3, "Mcells_per_s": mc / sec / 1e6,
+                                      "operator": "P2ElementwiseDivKGradIcosahedralShellMap form (k as a P2 function)"}
+    del An
     Ls = level - 1
     S = H.P2ElementwiseBlendingDivKGradOperator(pm, Ls, Ls, ctx, k=K, blending="shell")
     S.computeAndStoreLocalElementMatrices()

@@ -158,6 +158,10 @@ _SIGS = {
     "hyb_p2_fn_upload_reference": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "hyb_op_create_p2_divkgrad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                             C.POINTER(C.c_void_p)]),
+    "hyb_op_create_p2_divkgrad_nodal": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                                  C.POINTER(C.c_void_p)]),
+    "hyb_op_create_p2_divkgrad_fn": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                               C.POINTER(C.c_void_p)]),
     "hyb_fn_dot_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.POINTER(C.c_double)]),
     "hyb_serve_params_default": (C.c_int, [C.c_void_p]),
     "hyb_serve_create": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
@@ -588,6 +592,29 @@ class P2ElementwiseBlendingDivKGradOperator(_ConstantOperator):
         h = C.c_void_p()
         _check(lib().hyb_op_create_p2_divkgrad(ctx.h, storage.h, min_level, max_level, C.byref(c),
                                                1 if blending == "shell" else 0, C.byref(h)))
+        self.h = h
+
+    def computeAndStoreLocalElementMatrices(self):
+        _check(lib().hyb_op_store_element_matrices(self.h))
+
+
+class P2ElementwiseDivKGradOperator(_ConstantOperator):
+    """operatorgeneration::P2ElementwiseDivKGrad / P2ElementwiseDivKGradIcosahedralShellMap (hyteg-operators):
+    -div(k grad u) with k stored as a P2 function and evaluated at the quadrature points through the P2
+    basis.  k is a P2Function (FP64, levels min_level..max_level, copied at creation) or a coefficient spec
+    as for P2ElementwiseBlendingDivKGradOperator, interpolated at the (blended) nodes of every level."""
+
+    def __init__(self, storage, min_level, max_level, ctx, k=None, blending=None):
+        self.storage, self.ctx = storage, ctx
+        self.min_level, self.max_level = min_level, max_level
+        h = C.c_void_p()
+        bl = 1 if blending == "shell" else 0
+        if isinstance(k, P2Function):
+            _check(lib().hyb_op_create_p2_divkgrad_fn(ctx.h, storage.h, min_level, max_level, k.h, bl, C.byref(h)))
+        else:
+            c = _coeff(k)
+            _check(lib().hyb_op_create_p2_divkgrad_nodal(ctx.h, storage.h, min_level, max_level, C.byref(c), bl,
+                                                         C.byref(h)))
         self.h = h
 
     def computeAndStoreLocalElementMatrices(self):

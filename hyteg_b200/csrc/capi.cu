@@ -1085,6 +1085,51 @@ int hyb_op_create_p2_divkgrad( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int 
    HYB_CATCH
 }
 
+int hyb_op_create_p2_divkgrad_nodal( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, const hyb_coeff* k, int blending,
+                                     hyb_op** out )
+{
+   HYB_TRY
+   const int rc = hyb_op_create_p2_divkgrad( ctx, mesh, min_level, max_level, k, blending, out );
+   if ( rc != HYB_OK ) return rc;
+   hyb_op* h     = *out;
+   h->o.nodal_k  = true;
+   try
+   {
+      for ( int L = h->o.minL; L <= h->o.maxL; ++L ) set_p2_nodal_coefficient( &ctx->c, &h->o, L, nullptr );
+   } catch ( ... )
+   {
+      *out = nullptr;
+      op_unref( h );
+      throw;
+   }
+   HYB_CATCH
+}
+
+int hyb_op_create_p2_divkgrad_fn( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, hyb_fn* k, int blending, hyb_op** out )
+{
+   HYB_TRY
+   require( ctx && mesh && k && out, "NULL argument" );
+   require( k->f.lshift == 1, "the coefficient must be a P2 function" );
+   require( k->f.dtype == HYB_F64, "the coefficient function must hold FP64 values" );
+   require( &mesh->m == k->f.mesh, "coefficient function and operator live on different meshes" );
+   for ( int L = min_level; L <= max_level; ++L ) require_level( k->f, L + 1 );
+   const int rc = hyb_op_create_p2_divkgrad( ctx, mesh, min_level, max_level, nullptr, blending, out );
+   if ( rc != HYB_OK ) return rc;
+   hyb_op* h    = *out;
+   h->o.nodal_k = true;
+   try
+   {
+      for ( int L = h->o.minL; L <= h->o.maxL; ++L )
+         set_p2_nodal_coefficient( &ctx->c, &h->o, L, static_cast< const double* >( k->f.ptr( L ) ) );
+   } catch ( ... )
+   {
+      *out = nullptr;
+      op_unref( h );
+      throw;
+   }
+   HYB_CATCH
+}
+
 int hyb_op_store_element_matrices( hyb_op* op )
 {
    HYB_TRY

@@ -273,6 +273,8 @@ struct ElemLevel {
    // weight-major over the level's slots, in double ([0]) and float ([1])
    void* d_S[2] = { nullptr, nullptr };
    void* d_sacc = nullptr;  // Stokes coupling blocks: three velocity accumulators and one pressure accumulator
+   // P2 operators with a stored coefficient function: k at every cell-array node of this storage level
+   double* d_kn = nullptr;
 };
 
 struct Operator {
@@ -285,6 +287,9 @@ struct Operator {
    bool                      store_matrices = false;  // element matrices computed once and read back
    // 1: P1 operator; 2: P2 operator whose level L lives on the node set of storage level L+1
    int                       order = 1;
+   // P2 elementwise operators whose coefficient is a P2 function (el[L].d_kn), evaluated at the
+   // quadrature points through the P2 basis instead of from its closed form
+   bool                      nodal_k = false;
    int                       blending    = 0;
    Coefficient               coeff;
    CellGeom*                 d_geom = nullptr;
@@ -357,6 +362,9 @@ void launch_p2_restrict( Context* ctx, Mesh* m, int Lf, int dtype, uint32_t flag
 void launch_p2_prolongate( Context* ctx, Mesh* m, int Lc, int dtype, uint32_t flag, const void* coarse, void* fine, int add );
 void build_elementwise_operator( Operator* A );  // host tables (cell geometry, shell classification)
 void ensure_elementwise_level( Context* ctx, Operator* A, int L, int dtype );  // device buffers + diagonal
+// coefficient of a P2 elementwise operator stored as a P2 function on storage level Ls: copied from
+// src (a level buffer of the same layout) or, with src NULL, the closed form at the blended nodes
+void set_p2_nodal_coefficient( Context* ctx, Operator* A, int Ls, const double* src );
 void ensure_stokes_constants();
 // Stokes coupling blocks on P1 level Lp / P2 level Lp (storage Lp+1): divt 0 dst_p (+)= div u,
 // divt 1 dst_u[k] (+)= divT_k p

@@ -351,6 +351,7 @@ __global__ void __launch_bounds__( 256 ) k_elem_pass( int n, int nanch, const in
 __constant__ double c_xg4_pts[11][3];
 __constant__ double c_xg4_w[11];
 __constant__ double c_p2_rgrad[11][10][3];  // reference gradients of the ten basis functions per point
+__constant__ double c_p2_phi[11][10];       // values of the ten basis functions per point
 __constant__ int    c_p2_edge[6][2] = { { 2, 3 }, { 1, 3 }, { 1, 2 }, { 0, 3 }, { 0, 2 }, { 0, 1 } };
 // Stored P2 element matrices keep the 55 distinct entries of the symmetric 10x10 matrix in wrapped-
 // diagonal order: block 0 (entries 0-9) the diagonal K(i, i); block s = 1..4 (entries 10 s + e) the
@@ -455,6 +456,14 @@ void ensure_p2_constants()
       check_cuda( cudaMemcpyToSymbol( c_xg4_pts, pts, sizeof( pts ) ), "P2 constants (points)" );
       check_cuda( cudaMemcpyToSymbol( c_xg4_w, w, sizeof( w ) ), "P2 constants (weights)" );
       check_cuda( cudaMemcpyToSymbol( c_p2_rgrad, g, sizeof( g ) ), "P2 constants (gradients)" );
+      double phi[11][10];
+      for ( int q = 0; q < 11; ++q )
+      {
+         const double lam[4] = { 1.0 - pts[q][0] - pts[q][1] - pts[q][2], pts[q][0], pts[q][1], pts[q][2] };
+         for ( int i = 0; i < 4; ++i ) phi[q][i] = lam[i] * ( 2.0 * lam[i] - 1.0 );
+         for ( int e = 0; e < 6; ++e ) phi[q][4 + e] = 4.0 * lam[ed[e][0]] * lam[ed[e][1]];
+      }
+      check_cuda( cudaMemcpyToSymbol( c_p2_phi, phi, sizeof( phi ) ), "P2 constants (basis values)" );
       int wrap[55];
       p2_wrap_table( wrap );
       check_cuda( cudaMemcpyToSymbol( c_p2_wrap, wrap, sizeof( wrap ) ), "P2 constants (stored order)" );
@@ -462,9 +471,11 @@ void ensure_p2_constants()
 }
 
 // mapped quantities of quadrature point q of a micro-cell: Mi = (DF J)^-1 and s = w k |det(DF J)|
+// kl: the coefficient's values at the ten nodes (a coefficient stored as a P2 function), or nullptr
+// for the closed form at the blended point
 template < typename A >
 __device__ __forceinline__ void p2_point( const CellGeom& g, const Coefficient& kc, const A X0[3], const A J[3][3], int q, A Mi[3][3],
-                                          A& s )
+                                          A& s, const A* kl )
 {
    A Xq[3];
    for ( int r = 0; r < 3; ++r )
@@ -497,7 +508,15 @@ __device__ __forceinline__ void p2_point( const CellGeom& g, const Coefficient& 
    Mi[0][2]    = ( M[0][1] * M[1][2] - M[0][2] * M[1][1] ) * id;
    Mi[1][2]    = ( M[0][2] * M[1][0] - M[0][0] * M[1][2] ) * id;
    Mi[2][2]    = ( M[0][0] * M[1][1] - M[0][1] * M[1][0] ) * id;
-   s           = A( c_xg4_w[q] ) * coeff_eval( kc, Fq ) * fabs( det );
+   A kq;
+   if ( kl )
+   {
+      kq = A( 0 );
+      for ( int i = 0; i < 10; ++i ) kq += A( c_p2_phi[q][i] ) * kl[i];
+   }
+   else
+      kq = coeff_eval( kc, Fq );
+   s = A( c_xg4_w[q] ) * kq * fabs( det );
 }
 
 // physical gradient of basis function i at point q: row (reference gradient) times Mi
@@ -519,7 +538,8 @@ template < typename T, typename A, int MODE >
 __global__ void __launch_bounds__( 256 ) k_p2_pass( int ne, int nanch, const int* __restrict__ anch, const int64_t* __restrict__ cell_off,
                                                      const CellGeom* __restrict__ geom, Coefficient kc,
                                                      const T* __restrict__ src, A* __restrict__ acc, A* __restrict__ kst,
-                                                     int64_t kstride, int64_t kbase, int64_t level_size, int* err )
+                                                     int64_t kstride, int64_t kbase, int64_t level_size, int* err,
+                                                     const double* __restrict__ kn )
 {
    const int t = blockIdx.x * blockDim.x + threadIdx.x;  // one micro-cell anchor per thread
    const int c = blockIdx.y;
@@ -560,9 +580,12 @@ __global__ void __launch_bounds__( 256 ) k_p2_pass( int ne, int nanch, const int
                continue;
             }
          }
-         A xl[10], yl[10];
+         A xl[10], yl[10], kl[10];
          if constexpr ( MODE == 0 || MODE == 3 )
             for ( int m = 0; m < 10; ++m ) xl[m] = A( ld_any( src + idx[m] ) );
+         if constexpr ( MODE != 3 )
+            if ( kn )
+               for ( int m = 0; m < 10; ++m ) kl[m] = A( kn[idx[m]] );
          for ( int m = 0; m < 10; ++m ) yl[m] = A( 0 );
          if constexpr ( MODE == 3 )
          {
@@ -592,7 +615,7 @@ __global__ void __launch_bounds__( 256 ) k_p2_pass( int ne, int nanch, const int
             for ( int q = 0; q < 11; ++q )
             {
                A Mi[3][3], s;
-               p2_point( g, kc, X0, J, q, Mi, s );
+               p2_point( g, kc, X0, J, q, Mi, s, kn ? kl : static_cast< const A* >( nullptr ) );
                if constexpr ( MODE == 0 )
                {
                   A gs[3] = { A( 0 ), A( 0 ), A( 0 ) };
@@ -1327,7 +1350,7 @@ static void run_passes( Context* ctx, Mesh* m, Operator* op, int L, const T* src
       else if ( op->order == 2 )
          k_p2_pass< T, A, MODE ><<< grid, bs, 0, ctx->stream >>>( element_n( op, L ), na, e.d_anch + e.aoff[p], P.d_off + P.nB,
                                                                    op->d_geom, op->coeff, src, acc, kst, ks, kbase, P.size,
-                                                                   ctx->d_error );
+                                                                   ctx->d_error, op->nodal_k ? e.d_kn : nullptr );
       else
          k_elem_pass< T, A, MODE ><<< grid, bs, 0, ctx->stream >>>( P.n, na, e.d_anch + e.aoff[p], P.d_off + P.nB, op->d_geom,
                                                                      op->coeff, src, acc, kst, ks, P.size, ctx->d_error );
@@ -1336,18 +1359,61 @@ static void run_passes( Context* ctx, Mesh* m, Operator* op, int L, const T* src
    check_cuda( cudaGetLastError(), "elementwise pass launch" );
 }
 
+// A coefficient stored as a P2 function (the hyteg-operators P2ElementwiseDivKGrad operators take k
+// as a P2Function interpolated at the nodes): its closed form at every cell-array node of storage
+// level ns, at the node's blended position.  Block (z, cell), threads over the rows y of slice z.
+__global__ void __launch_bounds__( 128 ) k_p2_nodal_coeff( int ns, const int64_t* __restrict__ cell_off, const CellGeom* __restrict__ geom,
+                                                            Coefficient kc, double* kn )
+{
+   const int      z = blockIdx.x, c = blockIdx.y;
+   const CellGeom g = geom[c];
+   for ( int y = threadIdx.x; y + z <= ns; y += blockDim.x )
+      for ( int x = 0; x + y + z <= ns; ++x )
+      {
+         double X[3], F[3], DF[3][3];
+         for ( int d = 0; d < 3; ++d )
+            X[d] = g.P[0][d] + ( ( g.P[1][d] - g.P[0][d] ) * x + ( g.P[2][d] - g.P[0][d] ) * y + ( g.P[3][d] - g.P[0][d] ) * z ) / double( ns );
+         if ( g.blend == 1 ) shell_map( g, X, F, DF );
+         else
+            for ( int d = 0; d < 3; ++d ) F[d] = X[d];
+         kn[cell_off[c] + cidx( ns, x, y, z )] = coeff_eval( kc, F );
+      }
+}
+
+static void upload_geometry( Operator* op )
+{
+   if ( op->d_geom ) return;
+   check_cuda( cudaMalloc( &op->d_geom, op->geom.size() * sizeof( CellGeom ) ), "cudaMalloc(geometry)" );
+   check_cuda( cudaMemcpy( op->d_geom, op->geom.data(), op->geom.size() * sizeof( CellGeom ), cudaMemcpyHostToDevice ), "upload geometry" );
+}
+
+void set_p2_nodal_coefficient( Context* ctx, Operator* op, int Ls, const double* src )
+{
+   Mesh*    m = op->mesh;
+   P1Level& P = m->level( Ls );
+   ensure_device( m, P );
+   upload_geometry( op );
+   ElemLevel& e = op->el[Ls];
+   if ( !e.d_kn ) check_cuda( cudaMalloc( &e.d_kn, P.size * sizeof( double ) ), "cudaMalloc(nodal coefficient)" );
+   check_cuda( cudaMemsetAsync( e.d_kn, 0, P.size * sizeof( double ), ctx->stream ), "cudaMemset(nodal coefficient)" );
+   if ( src )
+      check_cuda( cudaMemcpyAsync( e.d_kn, src, P.size * sizeof( double ), cudaMemcpyDeviceToDevice, ctx->stream ), "copy nodal coefficient" );
+   else
+   {
+      const dim3 grid( P.n + 1, m->topo.nC );
+      k_p2_nodal_coeff<<< grid, 128, 0, ctx->stream >>>( P.n, P.d_off + P.nB, op->d_geom, op->coeff, e.d_kn );
+      ++ctx->launches;
+      check_cuda( cudaGetLastError(), "nodal coefficient launch" );
+   }
+}
+
 template < typename T, typename A >
 static void ensure_level_t( Context* ctx, Operator* op, int L, int dtype )
 {
    Mesh*    m = op->mesh;
    P1Level& P = m->level( L );
    ensure_device( m, P );
-   if ( !op->d_geom )
-   {
-      check_cuda( cudaMalloc( &op->d_geom, op->geom.size() * sizeof( CellGeom ) ), "cudaMalloc(geometry)" );
-      check_cuda( cudaMemcpy( op->d_geom, op->geom.data(), op->geom.size() * sizeof( CellGeom ), cudaMemcpyHostToDevice ),
-                  "upload geometry" );
-   }
+   upload_geometry( op );
    ensure_rows( op, L );
    ElemLevel& e = op->el[L];
    A*         acc = acc_buffer< A >( op, L, P.size );

@@ -769,6 +769,7 @@ Operator::~Operator()
       for ( void* p : kv.second.d_K ) cudaFree( p );
       for ( void* p : kv.second.d_S ) cudaFree( p );
       cudaFree( kv.second.d_sacc );
+      cudaFree( kv.second.d_kn );
       cudaFree( kv.second.d_anch );
    }
    cudaFree( d_geom );

@@ -229,6 +229,16 @@ int hyb_op_create_divkgrad( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max
  * P2toP2QuadraticProlongation), used by the multigrid solver for P2 operators. */
 int hyb_op_create_p2_divkgrad( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, const hyb_coeff* k, int blending,
                                hyb_op** out );
+/* The hyteg-operators form of the same operator, operatorgeneration::P2ElementwiseDivKGrad and
+ * P2ElementwiseDivKGradIcosahedralShellMap (generated code in the hyteg_operators submodule, absent from the
+ * reference tree; call sites tests/hyteg/convergence/ElementwiseDivKGradCGConvergenceTest.cpp:38-39,85-92):
+ * the coefficient is a P2 function k_h and enters each quadrature point as sum_i k_h(node_i) phi_i(point)
+ * instead of its closed form.  _nodal interpolates the closed form k at the (blended) nodes of every level,
+ * as kFunction.interpolate(k, level) does there; _fn copies a caller's FP64 P2 function (levels
+ * min_level..max_level) at creation. */
+int hyb_op_create_p2_divkgrad_nodal( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, const hyb_coeff* k, int blending,
+                                     hyb_op** out );
+int hyb_op_create_p2_divkgrad_fn( hyb_ctx* ctx, hyb_mesh* mesh, int min_level, int max_level, hyb_fn* k, int blending, hyb_op** out );
 int hyb_op_store_element_matrices( hyb_op* op );
 int hyb_op_destroy( hyb_op* op );
 int hyb_op_apply( hyb_op* op, hyb_fn* src, hyb_fn* dst, int level, uint32_t flag, int update );

@@ -1350,6 +1350,66 @@ class P2DivKGrad(P1ConstantLaplace):
             self.invdiag[L] = inv
 
 
+def p2_divkgrad_element_nodal(X, knodes, blend=None):
+    """Element matrices (m, 10, 10) of -div(k_h grad u) where k_h is the P2 interpolant of k: knodes
+    (m, 10) holds k at the element's nodes (element DoF order) and k_h at a quadrature point is
+    sum_i phi_i(xi_q) knodes_i.  This is the form of the hyteg-operators P2ElementwiseDivKGrad /
+    P2ElementwiseDivKGradIcosahedralShellMap (called at tests/hyteg/convergence/
+    ElementwiseDivKGradCGConvergenceTest.cpp:85-92 with k interpolated into a P2Function), restated here:
+    the generated operator code lives in the hyteg_operators submodule, absent from the reference tree,
+    so parity with it is unpinned.  Same rule (degree-4, 11 points) and blending as p2_divkgrad_element."""
+    phi = p2_basis(XG4_BARY)  # (11, 10)
+    J = np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], axis=2)
+    K = np.zeros((X.shape[0], 10, 10))
+    for q, (xi, w) in enumerate(zip(XG4_POINTS, XG4_WEIGHTS)):
+        Xq = X[:, 0] + np.einsum("kij,j->ki", J, xi)
+        M = J if blend is None else np.einsum("kij,kjl->kil", blend.DF(Xq), J)
+        det = np.abs(np.linalg.det(M))
+        G = np.einsum("id,kdj->kij", p2_ref_gradients(xi), np.linalg.inv(M))
+        kq = knodes @ phi[q]
+        K += (w * kq * det)[:, None, None] * np.einsum("kid,kjd->kij", G, G)
+    return K
+
+
+def p2_element_nodes(X):
+    """Computational coordinates (m, 10, 3) of the ten nodes of P2 elements with vertices X (m, 4, 3)."""
+    return np.concatenate([X, np.stack([(X[:, i] + X[:, j]) / 2 for i, j in P2_EDGES], axis=1)], axis=1)
+
+
+class P2DivKGradNodal(P1ConstantLaplace):
+    """-div(k_h grad u) with k_h the P2 interpolant of kfun at the (blended) nodes of each level, assembled
+    from p2_divkgrad_element_nodal (levels[L] is Level(mesh, L+1), as for P2DivKGrad)."""
+
+    def __init__(self, mesh, minL, maxL, kfun, blending=None):
+        self.mesh, self.minL, self.maxL = mesh, minL, maxL
+        self.maps = [IcosahedralShellMap(mesh, c) for c in range(mesh.nC)] if blending == "shell" else None
+        self.levels = {L: Level(mesh, L + 1) for L in range(minL, maxL + 1)}
+        self.A = {}
+        for L in range(minL, maxL + 1):
+            lev = self.levels[L]
+            rows, cols, vals = [], [], []
+            for c in range(mesh.nC):
+                slots, X = p2_micro_cells(lev, c)
+                nodes = p2_element_nodes(X)
+                phys = nodes if self.maps is None else self.maps[c].F(nodes.reshape(-1, 3)).reshape(nodes.shape)
+                knodes = kfun(phys)
+                K = p2_divkgrad_element_nodal(X, knodes, None if self.maps is None else _PerPointMap(self.maps[c]))
+                rows.append(np.repeat(slots, 10, axis=1).ravel())
+                cols.append(np.tile(slots, (1, 10)).ravel())
+                vals.append(K.reshape(K.shape[0], 100).ravel())
+            A = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                              shape=(lev.size, lev.size)).tocsr()
+            A.sum_duplicates()
+            self.A[L] = A
+        self.invdiag = {}
+        for L, A in self.A.items():
+            d = A.diagonal()
+            inv = np.zeros_like(d)
+            own = self.levels[L].owned
+            inv[own] = 1.0 / d[own]
+            self.invdiag[L] = inv
+
+
 def p2_basis(mu):
     """Quadratic Lagrange basis (k, 10) at barycentric points mu (k, 4), element DoF order."""
     out = [mu[:, i] * (2.0 * mu[:, i] - 1.0) for i in range(4)]

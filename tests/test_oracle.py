@@ -494,3 +494,26 @@ def test_shell_map_matches_reference(ntan, nrad):
         worst_df = max(worst_df, np.abs(DFo - DF).max() / np.abs(DF).max())
         np.testing.assert_allclose(np.linalg.det(DF), det, rtol=1e-12)
     assert worst_f < 1e-14 and worst_df < 1e-13, (worst_f, worst_df)
+
+
+def test_p2_nodal_form_reduces_to_the_form_operator_for_constant_k():
+    """With a constant coefficient the P2 interpolant is exact, so the nodal-coefficient form equals the
+    form-based p2_div_k_grad_blending_q4 operator (blended shell, levels 1 and 2); for the exp-sin
+    coefficient the two differ by the interpolation error, which shrinks with the level."""
+    coords, tets = O.mesh_spherical_shell(3, 2, 0.55, 1.0)
+    om = O.MacroMesh(coords, tets)
+    two = lambda P: 2.0 * np.ones(P.shape[:-1])  # noqa: E731
+    a = O.P2DivKGrad(om, 1, 1, two, blending="shell")
+    b = O.P2DivKGradNodal(om, 1, 1, two, blending="shell")
+    d = abs(a.A[1] - b.A[1]).max() / abs(a.A[1]).max()
+    assert d < 1e-13
+    kfun = O.k_expsin(0.5, (0.13, 0.27, 0.41))
+    cube = O.MacroMesh(*O.mesh_cuboid())
+    diffs = []
+    for L in (1, 2):
+        a = O.P2DivKGrad(cube, L, L, kfun)
+        b = O.P2DivKGradNodal(cube, L, L, kfun)
+        x = np.random.default_rng(L).uniform(-1, 1, a.levels[L].size)
+        ya, yb = a.A[L] @ x, b.A[L] @ x
+        diffs.append(np.abs(ya - yb).max() / np.abs(ya).max())
+    assert diffs[1] < diffs[0]
