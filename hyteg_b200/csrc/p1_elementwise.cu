@@ -535,7 +535,7 @@ __device__ __forceinline__ void p2_grad( int q, int i, const A Mi[3][3], A G[3] 
 // kst[55 * (6 nC aoff[p] + (c * 6 + ty) * nanch + t) + v] (kbase = 6 nC aoff[p]): the 55 entries of
 // a micro-cell are contiguous, so the lanes that read one micro-cell's rows share its 440 bytes.
 template < typename T, typename A, int MODE >
-__global__ void __launch_bounds__( 256 ) k_p2_pass( int ne, int nanch, const int* __restrict__ anch, const int64_t* __restrict__ cell_off,
+__global__ void __launch_bounds__( 256, 2 ) k_p2_pass( int ne, int nanch, const int* __restrict__ anch, const int64_t* __restrict__ cell_off,
                                                      const CellGeom* __restrict__ geom, Coefficient kc,
                                                      const T* __restrict__ src, A* __restrict__ acc, A* __restrict__ kst,
                                                      int64_t kstride, int64_t kbase, int64_t level_size, int* err,
