@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--no-stokes", action="store_true")
     p.add_argument("--no-config1", action="store_true")
     p.add_argument("--no-p2c", action="store_true")
+    p.add_argument("--config4", action="store_true",
+                   help="run configuration 4 as stated (P2-P1 Stokes on the shell (5,3) at level 5, FP32 inner / FP64 "
+                        "outer Uzawa multigrid to rtol 1e-8; a few minutes) and print its own JSON line")
     p.add_argument("--config2", action="store_true",
                    help="run configuration 2 as stated (P2 div-k-grad on the shell (5,3) at level 6, Chebyshev(3) "
                         "V(3,3) to rtol 1e-10; about two minutes) and print its own JSON line")
@@ -660,6 +663,76 @@ def config2_solve(H, rtol=1e-10, level=6, max_cycles=40):
             "cycle": "V(3,3) Chebyshev(3), matrix-free elementwise apply, CG coarse level 0", "rhs": "seeded uniform [-1,1]"}
 
 
+def config4_solve(H, rtol=1e-8, level=5, max_outer=60):
+    """Configuration 4 as stated: Stokes P2-P1 Taylor-Hood on the shell (5,3) with the icosahedral shell
+    map, level 5, viscosity eta = exp(2.99 (1 - r) / 0.45), buoyancy rhs T r/|r| with T seeded uniform in
+    [0, 1] (velocity), zero pressure rhs, Uzawa multigrid V(3,3) (Chebyshev(3) velocity sweeps, pressure
+    update scaled by the inverse lumped pressure mass weighted by 1/eta, omega = 1/rho from the relaxation
+    estimate: 20 power iterations with two velocity sweeps on level 2, as the reference's apps call
+    estimateUzawaRelaxationParameter), FP32 inner cycles inside FP64 defect correction to ||r||/||r0|| <=
+    1e-8, and the plain FP64 cycles for comparison.  CUDA-event timing of set-up and solve."""
+    import torch
+
+    ctx = H.Context(0)
+    s = torch.cuda.ExternalStream(ctx.stream)
+    pm = H.PrimitiveStorage.spherical_shell(5, 3, 0.55, 1.0, ctx=ctx)
+    visc = ("radial", 2.99, 1.0, 0.45)
+    u = [H.P2Function("u%d" % k, pm, 0, level, ctx) for k in range(3)]
+    p = H.P1Function("p", pm, 0, level, ctx)
+    bu = [H.P2Function("bu%d" % k, pm, 0, level, ctx) for k in range(3)]
+    bp = H.P1Function("bp", pm, 0, level, ctx)
+    T = H.P2Function("T", pm, level, level, ctx)
+    half = H.P2Function("half", pm, level, level, ctx)
+    T.fill_random(level, 4)  # uniform [-1, 1] ...
+    half.interpolate(0.5, level)
+    T.assign([0.5, 1.0], [T, half], level)  # ... mapped to [0, 1]
+    for k in range(3):
+        bu[k].interpolate(lambda x, y, z, k=k: [x, y, z][k] / max((x * x + y * y + z * z) ** 0.5, 1e-12), level)
+        bu[k].multElementwise([bu[k], T], level)
+    del T, half
+    out = {"config": "configuration 4: Stokes P2-P1, shell (5,3) with IcosahedralShellMap, level 5",
+           "velocity_dofs": 3 * pm.packed_size(level + 1), "pressure_dofs": pm.packed_size(level), "rtol": rtol,
+           "viscosity": "exp(2.99 (1 - r) / 0.45)", "rhs": "T r/|r|, T seeded uniform [0, 1]",
+           "cycle": "V(3,3) Uzawa, Chebyshev(3) x 3 velocity sweeps, pressure update by the inverse lumped mass "
+                    "weighted by 1/eta, omega = 1/rho (estimated), 100 coarse Uzawa steps"}
+    runs = {}
+    for mode in ("fp32_inner_fp64_outer", "fp64"):
+        st = H.StokesUzawaMultigrid(ctx, pm, 0, level, viscosity=visc, blending="shell", pressure_scaling="lumped_mass")
+        rho = st.estimate_relaxation(2, 20, 2)
+        st.set_omega(1.0 / rho)
+        out["relaxation_estimate"] = {"level": 2, "power_iterations": 20, "velocity_sweeps": 2, "rho": rho, "omega": 1.0 / rho}
+        si = None
+        if mode != "fp64":
+            si = H.StokesUzawaMultigrid(ctx, pm, 0, level, viscosity=visc, blending="shell", pressure_scaling="lumped_mass")
+            si.set_omega(1.0 / rho)
+        for rep in range(2):  # the first run sets up (radii, stored matrices, graph capture)
+            for k in range(3):
+                u[k].interpolate(0.0, level)
+            p.interpolate(0.0, level)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            if mode == "fp64":
+                h = st.solve(u, p, bu, bp, level, max_outer if rep else 1, rtol=rtol)
+            else:
+                h = st.mixed_solve(si, u, p, bu, bp, level, max_outer=max_outer if rep else 1, rtol=rtol)
+            e1.record(s)
+            e1.synchronize()
+            if rep == 0:
+                setup_s = e0.elapsed_time(e1) / 1e3
+        sol = [u[k].download(level) for k in range(3)]
+        runs[mode] = {"setup_and_first_cycle_s": setup_s, "solve_s": e0.elapsed_time(e1) / 1e3, "cycles": int(len(h) - 1),
+                      "rel_residual": float(h[-1] / h[0]), "factors": [float(f) for f in h[1:] / h[:-1]], "_u": sol}
+        del st, si
+    ref = runs["fp64"]["_u"]
+    scale = max(np.abs(r).max() for r in ref)
+    for mode in runs:
+        runs[mode]["rel_diff_vs_fp64_solution"] = float(max(np.abs(runs[mode]["_u"][k] - ref[k]).max() for k in range(3)) / scale)
+        del runs[mode]["_u"]
+    runs["fp32_inner_fp64_outer"]["speedup_vs_fp64"] = runs["fp64"]["solve_s"] / runs["fp32_inner_fp64_outer"]["solve_s"]
+    out["runs"] = runs
+    return out
+
+
 def p2_cpu_reference(cells=400000):
     """The reference's per-micro-cell work of the P2 elementwise apply (integrateAll of the generated
     form + 10x10 matvec), compiled from its sources, on the host cores (test blending map)."""
@@ -748,6 +821,9 @@ def run_ours(args, rank, world, local):
         return profile_vcycle(args)
     if args.config2:
         print(json.dumps(config2_solve(H)))
+        return
+    if args.config4:
+        print(json.dumps(config4_solve(H)))
         return
 
     torch.cuda.set_device(local)

@@ -163,6 +163,8 @@ _SIGS = {
     "hyb_op_create_p2_divkgrad_fn": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                                C.POINTER(C.c_void_p)]),
     "hyb_fn_dot_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.POINTER(C.c_double)]),
+    "hyb_stokes_set_omega": (C.c_int, [C.c_void_p, C.c_double]),
+    "hyb_stokes_estimate_relaxation": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "hyb_serve_params_default": (C.c_int, [C.c_void_p]),
     "hyb_serve_create": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
     "hyb_serve_destroy": (C.c_int, [C.c_void_p]),
@@ -724,7 +726,8 @@ class P1PSPGOperator(_ConstantOperator):
 class _StokesParams(C.Structure):
     _fields_ = [("min_level", C.c_int), ("max_level", C.c_int), ("pre_smooth", C.c_int), ("post_smooth", C.c_int),
                 ("velocity_sweeps", C.c_int), ("cheb_order", C.c_int), ("power_iterations", C.c_int),
-                ("omega", C.c_double), ("coarse_sweeps", C.c_int), ("velocity_block", C.c_int)]
+                ("omega", C.c_double), ("coarse_sweeps", C.c_int), ("velocity_block", C.c_int),
+                ("pressure_scaling", C.c_int)]
 
 
 class StokesUzawaMultigrid:
@@ -737,15 +740,18 @@ class StokesUzawaMultigrid:
 
     def __init__(self, ctx, storage, min_level, max_level, viscosity=None, blending=None, pre=3, post=3,
                  velocity_sweeps=3, cheb_order=3, power_iterations=20, omega=0.7, coarse_sweeps=100,
-                 velocity_block="laplace"):
+                 velocity_block="laplace", pressure_scaling="pspg"):
         if velocity_block not in ("laplace", "full_viscous"):
             raise ValueError("velocity_block must be 'laplace' or 'full_viscous'")
+        if pressure_scaling not in ("pspg", "lumped_mass"):
+            raise ValueError("pressure_scaling must be 'pspg' or 'lumped_mass'")
         p = _StokesParams()
         _check(lib().hyb_stokes_params_default(C.byref(p)))
         p.min_level, p.max_level, p.pre_smooth, p.post_smooth = min_level, max_level, pre, post
         p.velocity_sweeps, p.cheb_order, p.power_iterations = velocity_sweeps, cheb_order, power_iterations
         p.omega, p.coarse_sweeps = float(omega), coarse_sweeps
         p.velocity_block = 1 if velocity_block == "full_viscous" else 0
+        p.pressure_scaling = 1 if pressure_scaling == "lumped_mass" else 0
         self.params, self.ctx, self.storage = p, ctx, storage
         c = _coeff(viscosity)
         h = C.c_void_p()
@@ -759,6 +765,18 @@ class StokesUzawaMultigrid:
     def set_velocity_radii(self, radii):
         r = np.ascontiguousarray(radii, dtype=np.float64)
         _check(lib().hyb_stokes_set_velocity_radii(self.h, _ptr(r)))
+
+    def set_omega(self, omega):
+        """UzawaSmoother::setRelaxationParameter"""
+        _check(lib().hyb_stokes_set_omega(self.h, float(omega)))
+        self.params.omega = float(omega)
+
+    def estimate_relaxation(self, level, iterations=20, velocity_sweeps=2):
+        """estimateUzawaRelaxationParameter: spectral radius of |S|^-1 B A~^-1 B^T by power iteration
+        (use omega = 1 / the radius with this solver's pressure scaling)"""
+        r = C.c_double()
+        _check(lib().hyb_stokes_estimate_relaxation(self.h, level, iterations, velocity_sweeps, C.byref(r)))
+        return r.value
 
     def apply(self, u, p, du, dp, level):
         _check(lib().hyb_stokes_apply(self.h, self._arr(u), p.h, self._arr(du), dp.h, level))

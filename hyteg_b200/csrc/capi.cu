@@ -2764,6 +2764,8 @@ int hyb_stokes_params_default( hyb_stokes_params* p )
    p->power_iterations = 20;
    p->omega            = 0.7;
    p->coarse_sweeps    = 100;
+   p->velocity_block   = 0;
+   p->pressure_scaling = 0;
    return HYB_OK;
 }
 
@@ -2777,6 +2779,8 @@ int hyb_stokes_create( hyb_ctx* ctx, hyb_mesh* mesh, const hyb_coeff* viscosity,
             "invalid smoothing counts" );
    require( params->cheb_order >= 1 && params->cheb_order <= 16, "Chebyshev order must be 1..16" );
    require( params->velocity_block == 0 || params->velocity_block == 1, "velocity_block must be 0 (per component) or 1 (full viscous)" );
+   require( params->pressure_scaling == 0 || params->pressure_scaling == 1,
+            "pressure_scaling must be 0 (PSPG diagonal) or 1 (lumped mass weighted by 1/eta)" );
    auto* s = new hyb_stokes();
    s->ctx  = ctx;
    ctx_ref( ctx );
@@ -2785,7 +2789,12 @@ int hyb_stokes_create( hyb_ctx* ctx, hyb_mesh* mesh, const hyb_coeff* viscosity,
    try
    {
       ok_rc( hyb_op_create_p2p1_div( ctx, mesh, params->min_level, params->max_level, blending, &s->D ) );
-      ok_rc( hyb_op_create_p1_pspg( ctx, mesh, params->min_level, params->max_level, &s->S ) );
+      if ( params->pressure_scaling == 1 )
+      {
+         ok_rc( hyb_op_create_divkgrad( ctx, mesh, params->min_level, params->max_level, viscosity, blending, &s->S ) );
+         s->S->o.coeff.element = kElemLumpedMassInvK;
+      }
+      else ok_rc( hyb_op_create_p1_pspg( ctx, mesh, params->min_level, params->max_level, &s->S ) );
       if ( params->velocity_block == 1 )
       {
          ok_rc( hyb_op_create_p2_full_viscous( ctx, mesh, params->min_level, params->max_level, viscosity, blending, &s->V ) );
@@ -2833,6 +2842,87 @@ int hyb_stokes_set_velocity_radii( hyb_stokes* s, const double* radii )
       return HYB_OK;
    }
    return hyb_gmg_set_radii( s->vel, radii );
+   HYB_CATCH
+}
+
+int hyb_stokes_set_omega( hyb_stokes* s, double omega )
+{
+   HYB_TRY
+   require( s, "NULL argument" );
+   require( omega > 0.0 && std::isfinite( omega ), "omega must be positive" );
+   // the captured cycle holds the old omega as a kernel argument
+   if ( s->gexec ) cudaGraphExecDestroy( s->gexec ), s->gexec = nullptr;
+   s->gkey.clear();
+   s->p.omega = omega;
+   HYB_CATCH
+}
+
+int hyb_stokes_estimate_relaxation( hyb_stokes* s, int level, int iterations, int velocity_sweeps, double* rho )
+{
+   HYB_TRY
+   require( s && rho, "NULL argument" );
+   require( level >= s->p.min_level && level <= s->p.max_level, "level outside the solver's level range" );
+   require( iterations >= 1 && velocity_sweeps >= 1, "iterations and velocity_sweeps must be positive" );
+   require( s->dtype < 0 || s->dtype == HYB_F64, "the estimate runs in FP64: call it on the FP64 solver" );
+   Mesh*     m = &s->mesh->m;
+   const int l = level, Ls = level + 1, dt = HYB_F64;
+   FnHolder  uh[3], bh, xh, yh;
+   hyb_fn*   u[3];
+   for ( int k = 0; k < 3; ++k )
+   {
+      uh[k].h           = new_fn( s->ctx, m, dt, s->p.min_level + 1, s->p.max_level + 1 );
+      uh[k].h->f.lshift = 1;
+      u[k]              = uh[k].h;
+   }
+   bh.h           = new_fn( s->ctx, m, dt, s->p.min_level + 1, s->p.max_level + 1 );
+   bh.h->f.lshift = 1;
+   xh.h           = new_fn( s->ctx, m, dt, s->p.min_level, s->p.max_level );
+   yh.h           = new_fn( s->ctx, m, dt, s->p.min_level, s->p.max_level );
+   hyb_fn *x = xh.h, *y = yh.h;
+   stokes_prepare( s, u[0], bh.h, dt );
+   Context&     cx     = s->ctx->c;
+   const double one[2] = { 1.0, 1.0 };
+   // y = |S|^-1 B A~^-1 B^T x (P2P1UzawaDampingFactorEstimationOperator::apply with the solver's own
+   // velocity smoother and pressure scaling; S^-1 is negative, hence the sign)
+   auto E = [&]() {
+      void* rr[3] = { s->ru[0]->f.ptr( Ls ), s->ru[1]->f.ptr( Ls ), s->ru[2]->f.ptr( Ls ) };
+      launch_stokes_div( &cx, &s->D->o, l, dt, 1, nullptr, x->f.ptr( l ), rr, nullptr, kSolveFlag, 0 );
+      for ( int k = 0; k < 3; ++k ) check_cuda( cudaMemsetAsync( u[k]->f.ptr( Ls ), 0, u[k]->f.bytes( Ls ), cx.stream ), "u = 0" );
+      for ( int it = 0; it < velocity_sweeps; ++it )
+      {
+         if ( s->V )
+         {
+            visc_smooth( s, u, s->ru, l );
+            continue;
+         }
+         for ( int k = 0; k < 3; ++k ) smooth( s->vel, u[k], s->ru[k], Ls );
+      }
+      const void* uu[3] = { u[0]->f.ptr( Ls ), u[1]->f.ptr( Ls ), u[2]->f.ptr( Ls ) };
+      launch_stokes_div( &cx, &s->D->o, l, dt, 0, uu, nullptr, nullptr, s->rp->f.ptr( l ), kAll, 0 );
+      hyb_fn* src[2] = { s->sinv, s->rp };
+      pointwise( y, l, kAll, PT_MULT, 2, one, src );
+      const double m1[1] = { -1.0 };
+      hyb_fn*      ys[1] = { y };
+      pointwise( y, l, kAll, PT_LINCOMB, 1, m1, ys );
+   };
+   auto scale_into = [&]( hyb_fn* dst, hyb_fn* src_fn, double f ) {
+      const double c[1]  = { f };
+      hyb_fn*      sr[1] = { src_fn };
+      pointwise( dst, l, kAll, PT_LINCOMB, 1, c, sr );
+   };
+   // estimateSpectralRadiusWithPowerIteration (SpectrumEstimation.hpp:56-84): x random and normalised,
+   // then x = y / |y|, y = E x; the radius is the Rayleigh quotient x . y
+   ok_rc( hyb_fn_fill_random( x, l, 42u ) );
+   scale_into( x, x, 1.0 / std::sqrt( dot_host( x, x, l, kAll ) ) );
+   E();
+   double radius = 0;
+   for ( int it = 1; it <= iterations; ++it )
+   {
+      scale_into( x, y, 1.0 / std::sqrt( dot_host( y, y, l, kAll ) ) );
+      E();
+      radius = dot_host( x, y, l, kAll );
+   }
+   *rho = radius;
    HYB_CATCH
 }
 

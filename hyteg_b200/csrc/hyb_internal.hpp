@@ -242,8 +242,12 @@ struct OpLevel {
 // coefficient kind that selects the P1 PSPG element matrix instead of -div(k grad)
 constexpr int kCoeffPSPG = 3;
 
+// element functions of the P1 elementwise operators besides -div(k grad) and PSPG (kind 3)
+constexpr int kElemLumpedMassInvK = 2;  // minus the lumped mass matrix weighted by 1/k (a Schur-complement scaling)
+
 struct Coefficient {
    int    kind  = 0;  // 0 constant, 1 exp-sin-cos-sin, 2 radial exp(amp (value - |x|) / freq), 3 PSPG
+   int    element = 0;  // 0: -div(k grad); kElemLumpedMassInvK
    double value = 1.0;
    double amp   = 0.5;
    double freq  = 1.0;

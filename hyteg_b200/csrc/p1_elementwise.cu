@@ -172,6 +172,46 @@ __device__ __forceinline__ void p1_pspg_element( const A X[4][3], A K[4][4] )
       for ( int j = 0; j < 4; ++j ) K[i][j] = f * ( G[i][0] * G[j][0] + G[i][1] * G[j][1] + G[i][2] * G[j][2] );
 }
 
+// Minus the lumped P1 mass matrix weighted by 1/k, diag_i = -int l_i / k over the (blended) micro-cell
+// (Yu's 5-point degree-3 rule): with k the viscosity, the scaling of the pressure update that follows
+// the viscosity-weighted pressure mass matrix, the usual approximation of the Schur complement
+// B A^-1 B^T for variable viscosity (negative like the PSPG diagonal, so the Uzawa update keeps its sign).
+template < typename A >
+__device__ __forceinline__ void p1_lumped_mass_inv_k_element( const CellGeom& g, const Coefficient& kc, const A X[4][3], A K[4][4] )
+{
+   A J[3][3];
+   for ( int r = 0; r < 3; ++r )
+      for ( int c = 0; c < 3; ++c ) J[r][c] = X[c + 1][r] - X[0][r];
+   for ( int i = 0; i < 4; ++i )
+      for ( int j = 0; j < 4; ++j ) K[i][j] = A( 0 );
+#pragma unroll 1
+   for ( int q = 0; q < 5; ++q )
+   {
+      const A xi[3] = { A( c_yu5_pts[q][0] ), A( c_yu5_pts[q][1] ), A( c_yu5_pts[q][2] ) };
+      A       Xq[3];
+      for ( int r = 0; r < 3; ++r ) Xq[r] = X[0][r] + J[r][0] * xi[0] + J[r][1] * xi[1] + J[r][2] * xi[2];
+      A M[3][3], Fq[3];
+      if ( g.blend == 1 )
+      {
+         A DF[3][3];
+         shell_map( g, Xq, Fq, DF );
+         for ( int r = 0; r < 3; ++r )
+            for ( int c = 0; c < 3; ++c ) M[r][c] = DF[r][0] * J[0][c] + DF[r][1] * J[1][c] + DF[r][2] * J[2][c];
+      }
+      else
+         for ( int r = 0; r < 3; ++r )
+         {
+            Fq[r] = Xq[r];
+            for ( int c = 0; c < 3; ++c ) M[r][c] = J[r][c];
+         }
+      const A det = M[0][0] * ( M[1][1] * M[2][2] - M[1][2] * M[2][1] ) - M[0][1] * ( M[1][0] * M[2][2] - M[1][2] * M[2][0] ) +
+                    M[0][2] * ( M[1][0] * M[2][1] - M[1][1] * M[2][0] );
+      const A f     = A( c_yu5_w[q] ) * fabs( det ) / coeff_eval( kc, Fq );
+      const A lam[4] = { A( 1 ) - xi[0] - xi[1] - xi[2], xi[0], xi[1], xi[2] };
+      for ( int i = 0; i < 4; ++i ) K[i][i] -= f * lam[i];
+   }
+}
+
 template < typename A >
 __device__ __forceinline__ void p1_divkgrad_element( const CellGeom& g, const Coefficient& kc, const A X[4][3], A K[4][4] )
 {
@@ -318,6 +358,7 @@ __global__ void __launch_bounds__( 256 ) k_elem_pass( int n, int nanch, const in
             continue;
          }
          if ( kc.kind == kCoeffPSPG ) p1_pspg_element( X, K );
+         else if ( kc.element == kElemLumpedMassInvK ) p1_lumped_mass_inv_k_element( g, kc, X, K );
          else p1_divkgrad_element( g, kc, X, K );
          if constexpr ( MODE == 2 )
          {

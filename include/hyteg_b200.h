@@ -407,6 +407,12 @@ typedef struct hyb_stokes_params
    int    coarse_sweeps;    /* Uzawa steps on the coarsest level (the coarse solve) */
    int    velocity_block;   /* 0: -div(eta grad) per component (block Laplace); 1: the full viscous block
                                P2ElementwiseBlendingFullViscousOperator, Chebyshev on the coupled block */
+   int    pressure_scaling; /* scaling S^-1 of the pressure update p += omega S^-1 (b_p - div u):
+                               0: the inverted PSPG diagonal (P2P1TaylorHoodStokesOperator's pspg_inv_diag_);
+                               1: the inverse lumped pressure mass matrix weighted by 1/eta (blended), the
+                               P1LumpedInvMassOperator pattern of tests/hyteg/convergence/
+                               P2P1Stokes3DUzawaConvergenceTest.cpp:125-139 with the viscosity that the
+                               Schur complement of a variable-viscosity velocity block carries */
 } hyb_stokes_params;
 int hyb_stokes_params_default( hyb_stokes_params* p );
 /* GeometricMultigridSolver< P2P1ElementwiseBlendingStokesOperator > with UzawaSmoother; viscosity:
@@ -416,6 +422,16 @@ int hyb_stokes_create( hyb_ctx* ctx, hyb_mesh* mesh, const hyb_coeff* viscosity,
 int hyb_stokes_destroy( hyb_stokes* s );
 /* fixes the velocity smoother's spectral radii (max_level - min_level + 1 values, P2 levels) */
 int hyb_stokes_set_velocity_radii( hyb_stokes* s, const double* radii );
+/* UzawaSmoother::setRelaxationParameter (solvers/UzawaSmoother.hpp): the omega of every later Uzawa step */
+int hyb_stokes_set_omega( hyb_stokes* s, double omega );
+/* estimateUzawaRelaxationParameter (solvers/UzawaSmoother.hpp:40-97) with
+ * P2P1UzawaDampingFactorEstimationOperator (mixed_operator/P2P1UzawaDampingFactorEstimationOperator.hpp):
+ * power iteration (iterations steps from a seeded random pressure) for the spectral radius rho of
+ * E = |S|^-1 B A~^-1 B^T on one level, A~^-1 being velocity_sweeps applications of the solver's own velocity
+ * smoother from zero and |S|^-1 the magnitude of its pressure scaling.  The reference passes the radius
+ * of its estimator (lumped mass in place of S) to setRelaxationParameter; for the scaling of this solver
+ * omega = 1/rho keeps the Uzawa pressure iteration I - omega |S|^-1 B A~^-1 B^T a contraction. */
+int hyb_stokes_estimate_relaxation( hyb_stokes* s, int level, int iterations, int velocity_sweeps, double* rho );
 /* P2P1ElementwiseBlendingStokesOperator::apply: du = A u + divT p (velocity flag Inner), dp = div u (all) */
 int hyb_stokes_apply( hyb_stokes* s, hyb_fn* const* u3, hyb_fn* p, hyb_fn* const* du3, hyb_fn* dp, int level );
 /* one UzawaSmoother::solve step */

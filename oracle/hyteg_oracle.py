@@ -1657,13 +1657,32 @@ class P2FullViscous:
         return dst
 
 
+def p1_lumped_mass_inv_k_diag(X, kfun, blend=None):
+    """(m, 4): minus the lumped P1 mass matrix weighted by 1/k on micro-cells X (m, 4, 3), i.e.
+    -int l_i / k over the (blended) cell with Yu's 5-point rule: the viscosity-weighted pressure mass
+    (the P1LumpedInvMassOperator pattern of P2P1Stokes3DUzawaConvergenceTest.cpp:125-139 with the 1/eta
+    weight a variable viscosity puts into the Schur complement), negative like the PSPG diagonal."""
+    J = np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], axis=2)
+    out = np.zeros((X.shape[0], 4))
+    for xi, w in zip(YU5_POINTS, YU5_WEIGHTS):
+        Xq = X[:, 0] + np.einsum("kij,j->ki", J, xi)
+        if blend is None:
+            M, Fq = J, Xq
+        else:
+            M, Fq = np.einsum("kij,kjl->kil", blend.DF(Xq), J), blend.F(Xq)
+        det = np.abs(np.linalg.det(M))
+        lam = np.array([1.0 - xi[0] - xi[1] - xi[2], xi[0], xi[1], xi[2]])
+        out -= (w * det / kfun(Fq))[:, None] * lam[None, :]
+    return out
+
+
 class P2P1Stokes:
     """The Taylor-Hood system [A 0 0 B0^T; 0 A 0 B1^T; 0 0 A B2^T; B0 B1 B2 0] on P2 level L (velocity,
     nodes of Level L+1) and P1 level L (pressure), A = -div(eta grad) per component, with the
     inverted PSPG diagonal (P1PSPGInvDiagOperator, affine macro geometry) for the Uzawa step.
     Velocity rows/columns use the inner DoFs, pressure rows/columns all DoFs."""
 
-    def __init__(self, mesh, minL, maxL, eta, blending=None, full_viscous=False):
+    def __init__(self, mesh, minL, maxL, eta, blending=None, full_viscous=False, pressure_scaling="pspg"):
         self.mesh, self.minL, self.maxL = mesh, minL, maxL
         self.Aop = P2DivKGrad(mesh, minL, maxL, eta, blending)
         # the full viscous velocity block (P2ElementwiseBlendingFullViscousOperator) in place of
@@ -1695,9 +1714,14 @@ class P2P1Stokes:
                     rows[k].append(np.repeat(pslots, 10, axis=1).ravel())
                     cols[k].append(np.tile(uslots, (1, 4)).ravel())
                     vals[k].append(Be[:, k].reshape(-1))
-                # PSPG diagonal on the affine (computational) micro-cell
-                Kp = p1_pspg_element(X)
-                np.add.at(d, pslots.ravel(), np.einsum("kii->ki", Kp).ravel())
+                if pressure_scaling == "lumped_mass":
+                    # minus the lumped pressure mass weighted by 1/eta, on the blended micro-cell
+                    np.add.at(d, pslots.ravel(),
+                              p1_lumped_mass_inv_k_diag(X, eta, None if maps is None else _PerPointMap(maps[c])).ravel())
+                else:
+                    # PSPG diagonal on the affine (computational) micro-cell
+                    Kp = p1_pspg_element(X)
+                    np.add.at(d, pslots.ravel(), np.einsum("kii->ki", Kp).ravel())
             self.B[L] = [sp.coo_matrix((np.concatenate(vals[k]), (np.concatenate(rows[k]), np.concatenate(cols[k]))),
                                        shape=(pl.size, ul.size)).tocsr() for k in range(3)]
             inv = np.zeros(pl.size)
