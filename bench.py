@@ -271,8 +271,8 @@ def config1_leg(H, ctx, L=5, cycles=10):
             "apply_ms": ms_ap, "apply_mdofs": inner_dofs(L) / (ms_ap * 1e-3) / 1e6}
 
 
-def mixed_precision_leg(H, ctx, pm, A, L, rtol=1e-8):
-    """Time to ||r||/||r0|| < rtol from a zero guess: plain FP64 V(3,3) Chebyshev(3) cycles against
+def mixed_precision_leg(H, ctx, pm, A, L, rtol=1e-10):
+    """Configuration 3: time to ||r||/||r0|| < rtol (1e-10) from a zero guess: plain FP64 V(3,3) Chebyshev(3) cycles against
     FP64 defect correction around the same cycles in FP32 and FP16 storage (FP32 accumulation).
     Each solution's error is measured against an FP64 solution converged to 1e-13."""
     import torch
