@@ -926,7 +926,8 @@ class GeometricMultigridSolver:
 # ------------------------------------------------------------------------------------------- serving
 class _ServeParams(C.Structure):
     _fields_ = [("max_slots", C.c_int), ("hbm_budget_bytes", C.c_double), ("inner_dtype", C.c_int),
-                ("pre_smooth", C.c_int), ("post_smooth", C.c_int), ("power_iterations", C.c_int)]
+                ("pre_smooth", C.c_int), ("post_smooth", C.c_int), ("power_iterations", C.c_int),
+                ("batch_width", C.c_int)]
 
 
 class _Request(C.Structure):
@@ -948,10 +949,11 @@ class SolveServer:
     """
 
     def __init__(self, ctx, max_slots=32, hbm_budget_bytes=0.0, inner_dtype="float32", pre_smooth=3, post_smooth=3,
-                 power_iterations=20):
+                 power_iterations=20, batch_width=1):
         p = _ServeParams()
         _check(lib().hyb_serve_params_default(C.byref(p)))
         p.max_slots, p.hbm_budget_bytes = max_slots, float(hbm_budget_bytes)
+        p.batch_width = int(batch_width)
         p.inner_dtype = _DTYPES[inner_dtype] if isinstance(inner_dtype, str) else int(inner_dtype)
         p.pre_smooth, p.post_smooth, p.power_iterations = pre_smooth, post_smooth, power_iterations
         self.ctx = ctx

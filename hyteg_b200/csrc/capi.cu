@@ -2170,6 +2170,152 @@ extern "C" int hyb_internal_residual_async( hyb_op* op, hyb_fn* x, hyb_fn* b, hy
    HYB_CATCH
 }
 
+// ---------------------------------------------------------------------------------------------
+// Replicated meshes: R disjoint copies of one macro mesh as one mesh, so that one launch of every
+// multigrid kernel serves the solves of R same-shaped problems (the serving loop's batches).  The
+// copy r of vertex v is vertex r nV + v; since edges and faces are ordered by their sorted vertex
+// ids and cells by their vertex tuples, the copy r of primitive i of a kind has index r n_kind + i,
+// which hyb_internal_mesh_replicate checks.
+// ---------------------------------------------------------------------------------------------
+extern "C" int hyb_internal_mesh_replicate( hyb_mesh* m, int R, hyb_mesh** out )
+{
+   HYB_TRY
+   require( m && out && R >= 1, "bad arguments" );
+   const Topology&                        t = m->m.topo;
+   std::vector< std::array< double, 3 > > c;
+   std::vector< std::array< int, 4 > >    tets;
+   c.reserve( size_t( R ) * t.nV );
+   tets.reserve( size_t( R ) * t.nC );
+   for ( int r = 0; r < R; ++r )
+   {
+      for ( int v = 0; v < t.nV; ++v ) c.push_back( t.vx[v] );
+      for ( int k = 0; k < t.nC; ++k )
+      {
+         const auto& cv = t.cv[k];
+         tets.push_back( { cv[0] + r * t.nV, cv[1] + r * t.nV, cv[2] + r * t.nV, cv[3] + r * t.nV } );
+      }
+   }
+   make_mesh( static_cast< hyb_ctx* >( m->m.owner_ctx ), c, tets, out );  // throws on failure
+   Topology& u = ( *out )->m.topo;
+   bool      same = u.nV == R * t.nV && u.nE == R * t.nE && u.nF == R * t.nF && u.nC == R * t.nC;
+   for ( int r = 0; r < R && same; ++r )
+   {
+      for ( int i = 0; i < t.nE && same; ++i ) same = u.ev[r * t.nE + i][0] == t.ev[i][0] + r * t.nV && u.ev[r * t.nE + i][1] == t.ev[i][1] + r * t.nV;
+      for ( int i = 0; i < t.nF && same; ++i )
+         for ( int k = 0; k < 3; ++k ) same = same && u.fv[r * t.nF + i][k] == t.fv[i][k] + r * t.nV;
+      for ( int i = 0; i < t.nC && same; ++i )
+         for ( int k = 0; k < 4; ++k ) same = same && u.cv[r * t.nC + i][k] == t.cv[i][k] + r * t.nV;
+   }
+   if ( !same )
+   {
+      hyb_mesh_destroy( *out );
+      *out = nullptr;
+      throw std::logic_error( "replicated mesh does not keep the primitive order copy by copy" );
+   }
+   for ( int r = 0; r < R; ++r )
+   {
+      for ( int i = 0; i < t.nV; ++i ) u.flag_v[r * t.nV + i] = t.flag_v[i];
+      for ( int i = 0; i < t.nE; ++i ) u.flag_e[r * t.nE + i] = t.flag_e[i];
+      for ( int i = 0; i < t.nF; ++i ) u.flag_f[r * t.nF + i] = t.flag_f[i];
+      for ( int i = 0; i < t.nC; ++i ) u.flag_c[r * t.nC + i] = t.flag_c[i];
+   }
+   u.bc_of_flag = t.bc_of_flag;
+   u.blending   = t.blending;
+   u.shell_rmin = t.shell_rmin;
+   u.shell_rmax = t.shell_rmax;
+   HYB_CATCH
+}
+
+// Maps of copy r of a replicated mesh at storage level Ls: *d_poff the np packed primitive offsets of
+// the original mesh, *d_off R x np padded offsets of each copy's primitives in the replicated mesh's
+// buffer, *d_tasks the replicated mesh's boundary tasks regrouped copy by copy, each copy padded to
+// *tpad tasks (a multiple of 256; padding tasks have x = -1).  Device arrays, freed with cudaFree.
+extern "C" int hyb_internal_replica_maps( hyb_mesh* orig, hyb_mesh* uni, int R, int Ls, void** d_poff, void** d_off, void** d_tasks,
+                                          int* np_out, int64_t* count, int* tpad_out )
+{
+   HYB_TRY
+   require( orig && uni && R >= 1 && d_poff && d_off && d_tasks && np_out && count && tpad_out, "bad arguments" );
+   const Topology& t  = orig->m.topo;
+   const Topology& u  = uni->m.topo;
+   require( u.nC == R * t.nC, "not a replicated mesh of this copy count" );
+   const P1Level&  Po = orig->m.level( Ls );
+   const P1Level&  Pu = uni->m.level( Ls );
+   const int       np = t.nV + t.nE + t.nF + t.nC;
+   const int       kn[4] = { t.nV, t.nE, t.nF, t.nC }, kb[4] = { 0, u.nV, u.nV + u.nE, u.nV + u.nE + u.nF };
+   std::vector< int64_t > poff( Po.packed_off.begin(), Po.packed_off.begin() + np ), off( size_t( R ) * np );
+   for ( int r = 0; r < R; ++r )
+   {
+      int j = 0;
+      for ( int k = 0; k < 4; ++k )
+         for ( int i = 0; i < kn[k]; ++i, ++j ) off[size_t( r ) * np + j] = Pu.off[kb[k] + r * kn[k] + i];
+   }
+   auto copy_of = [&]( int b ) {
+      if ( b < u.nV ) return b / t.nV;
+      if ( b < u.nV + u.nE ) return ( b - u.nV ) / t.nE;
+      return ( b - u.nV - u.nE ) / t.nF;
+   };
+   std::vector< std::vector< int4 > > per( R );
+   for ( const auto& q : Pu.tasks ) per[copy_of( q[0] )].push_back( make_int4( q[0], q[1], q[2], 0 ) );
+   size_t tmax = 0;
+   for ( const auto& v : per ) tmax = std::max( tmax, v.size() );
+   const int tpad = int( std::max< size_t >( 256, ( tmax + 255 ) / 256 * 256 ) );
+   std::vector< int4 > tasks( size_t( R ) * tpad, make_int4( -1, 0, 0, 0 ) );
+   for ( int r = 0; r < R; ++r ) std::copy( per[r].begin(), per[r].end(), tasks.begin() + size_t( r ) * tpad );
+   auto up = [&]( void** dst, const void* src, size_t bytes ) {
+      check_cuda( cudaMalloc( dst, std::max< size_t >( bytes, 16 ) ), "cudaMalloc(replica maps)" );
+      check_cuda( cudaMemcpy( *dst, src, bytes, cudaMemcpyHostToDevice ), "upload replica maps" );
+   };
+   up( d_poff, poff.data(), poff.size() * sizeof( int64_t ) );
+   up( d_off, off.data(), off.size() * sizeof( int64_t ) );
+   up( d_tasks, tasks.data(), tasks.size() * sizeof( int4 ) );
+   *np_out   = np;
+   *count    = Po.packed_size;
+   *tpad_out = tpad;
+   HYB_CATCH
+}
+
+// copy r of a function on a replicated mesh <-> a packed device vector in the original mesh's layout
+extern "C" int hyb_internal_replica_copy( hyb_fn* ufn, int level, int to_union, const void* d_poff, const void* d_off_r, int np,
+                                          int64_t count, double* d_packed )
+{
+   HYB_TRY
+   require( ufn && d_poff && d_off_r && d_packed, "NULL argument" );
+   const int Ls = lv( ufn, level );
+   require_level( ufn->f, Ls );
+   launch_repack_map( &ufn->ctx->c, count, np, static_cast< const int64_t* >( d_poff ), static_cast< const int64_t* >( d_off_r ), ufn->f.dtype,
+                      to_union, d_packed, ufn->f.ptr( Ls ) );
+   HYB_CATCH
+}
+
+// a function's level as a packed device vector and back (no host transfer)
+extern "C" int hyb_internal_fn_packed_device( hyb_fn* fn, int level, int to_padded, double* d_packed )
+{
+   HYB_TRY
+   require( fn && d_packed, "NULL argument" );
+   const int Ls = lv( fn, level );
+   require_level( fn->f, Ls );
+   launch_repack( &fn->ctx->c, fn->f.mesh, Ls, fn->f.dtype, to_padded, d_packed, fn->f.ptr( Ls ) );
+   HYB_CATCH
+}
+
+// residual r = b - A x (flagged DoFs) into tmp and its squared norm per copy into d_out[R]; with x
+// NULL, the squared norms of b itself (the initial residual of a zero guess)
+extern "C" int hyb_internal_residual_replicas_async( hyb_op* op, hyb_fn* x, hyb_fn* b, hyb_fn* tmp, int level, int R, const void* d_tasks,
+                                                     int tpad, double* d_out )
+{
+   HYB_TRY
+   Context&   c  = op->ctx->c;
+   const int  dt = b->f.dtype;
+   const void* v = b->f.ptr( level );
+   if ( x )
+   {
+      stencil( op, level, dt, OP_RESID, kSolveFlag, 0, x->f.ptr( level ), b->f.ptr( level ), nullptr, tmp->f.ptr( level ) );
+      v = tmp->f.ptr( level );
+   }
+   launch_dot_replicas( &c, op->o.mesh, level, dt, kSolveFlag, v, v, R, static_cast< const int4* >( d_tasks ), tpad, d_out );
+   HYB_CATCH
+}
+
 // one defect-correction step with the residual already in g->mx_t (FP64) and its norm rn on the
 // host: scale and convert, one inner cycle, FP64 update, new residual into g->mx_t and ||r||^2
 // into d_out

@@ -355,6 +355,12 @@ struct StencilArgs {
 
 void launch_stencil( Context* ctx, Mesh* m, Operator* A, int L, int dtype, const StencilArgs& a );
 void launch_elementwise( Context* ctx, Mesh* m, Operator* A, int L, int dtype, const StencilArgs& a );
+// per-copy dot products and packed transfers on meshes made of disjoint copies of one mesh
+// (p1_kernels.cu; the batched solves of the serving loop)
+void launch_dot_replicas( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const void* a, const void* b, int R, const int4* tasks,
+                          int tpad, double* out );
+void launch_repack_map( Context* ctx, int64_t count, int np, const int64_t* poff, const int64_t* off, int dtype, int to_padded,
+                        double* packed, void* vec );
 // P2 constant-stencil operator (p2_constant.cu); Ls is the storage level (P2 level + 1)
 void launch_p2_constant( Context* ctx, Mesh* m, Operator* A, int Ls, int dtype, const StencilArgs& a );
 void build_p2_constant_level( Operator* A, int Ls );

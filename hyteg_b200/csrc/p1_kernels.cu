@@ -1460,7 +1460,7 @@ __global__ void __launch_bounds__( 256 ) k_dot_bnd( LevelView v, uint32_t flag, 
    if ( t < v.ntasks )
    {
       const int4 tk = v.tasks[t];
-      if ( v.bc[tk.x] & flag )
+      if ( tk.x >= 0 && ( v.bc[tk.x] & flag ) )  // x < 0: padding of a per-copy task list
       {
          const int64_t o = owner_slot( v, tk.x, tk.y, tk.z );
          acc             = double( ldv( a + o ) ) * double( ldv( b + o ) );
@@ -1514,6 +1514,75 @@ static void run_dot( Context* ctx, const LevelView& v, int nC, uint32_t flag, co
    k_sum_partials<<< 1, 1024, 0, ctx->stream >>>( p, nb_cells + nb_bnd, out );
    ++ctx->launches;
    check_cuda( cudaGetLastError(), "dot launch" );
+}
+
+// sums of the partials of copy r of a replicated mesh: its cells' row blocks (contiguous, cells are
+// ordered copy by copy) and its boundary blocks (contiguous in the per-copy task list), in that order
+__global__ void __launch_bounds__( 256 ) k_sum_replicas( const double* partials, int cell_blocks, int bnd_blocks, int nb_cells_total,
+                                                          double* out )
+{
+   const int r   = blockIdx.x;
+   double    acc = 0.0;
+   for ( int i = threadIdx.x; i < cell_blocks; i += blockDim.x ) acc += partials[size_t( r ) * cell_blocks + i];
+   for ( int i = threadIdx.x; i < bnd_blocks; i += blockDim.x ) acc += partials[nb_cells_total + size_t( r ) * bnd_blocks + i];
+   acc = block_sum( acc );
+   if ( threadIdx.x == 0 ) out[r] = acc;
+}
+
+template < typename T >
+static void run_dot_replicas( Context* ctx, LevelView v, int nC, uint32_t flag, const void* a, const void* b, int R, const int4* tasks,
+                              int tpad, double* out )
+{
+   const int rb       = ( v.nrows + 7 ) / 8;  // row blocks per cell
+   const int nb_cells = v.nrows > 0 ? rb * nC : 0;
+   const int bnd_per  = tpad / 256;
+   const int nb_bnd   = bnd_per * R;
+   double*   p        = partials( ctx, nb_cells + nb_bnd + 1 );
+   if ( nb_cells )
+   {
+      dim3 grid( rb, nC );
+      k_dot_cells< T ><<< grid, 256, 0, ctx->stream >>>( v, flag, (const T*) a, (const T*) b, p );
+      ++ctx->launches;
+   }
+   if ( nb_bnd )
+   {
+      v.tasks  = tasks;
+      v.ntasks = tpad * R;
+      k_dot_bnd< T ><<< nb_bnd, 256, 0, ctx->stream >>>( v, flag, (const T*) a, (const T*) b, p + nb_cells );
+      ++ctx->launches;
+   }
+   k_sum_replicas<<< R, 256, 0, ctx->stream >>>( p, nb_cells ? rb * ( nC / R ) : 0, bnd_per, nb_cells, out );
+   ++ctx->launches;
+   check_cuda( cudaGetLastError(), "replica dot launch" );
+}
+
+// per-copy dot products on a mesh made of R disjoint copies of one mesh (cells ordered copy by copy):
+// out[r] = sum over copy r's owned flagged DoFs of a b; tasks: the boundary tasks regrouped copy by
+// copy, each copy padded to tpad (a multiple of 256) with tasks whose x is -1.  The sums per copy
+// follow a fixed order, so they do not depend on the other copies' values.
+void launch_dot_replicas( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const void* a, const void* b, int R, const int4* tasks,
+                          int tpad, double* out )
+{
+   ensure_constants();
+   LevelView v  = make_view( m, L );
+   const int nC = m->topo.nC;
+   if ( R < 1 || nC % R != 0 || tpad % 256 != 0 ) throw std::invalid_argument( "replica dot: bad copy count or task padding" );
+   if ( dtype == F64 ) run_dot_replicas< double >( ctx, v, nC, flag, a, b, R, tasks, tpad, out );
+   else if ( dtype == F32 ) run_dot_replicas< float >( ctx, v, nC, flag, a, b, R, tasks, tpad, out );
+   else run_dot_replicas< __half >( ctx, v, nC, flag, a, b, R, tasks, tpad, out );
+}
+
+// packed <-> padded with explicit primitive offsets (a copy of a replicated mesh)
+void launch_repack_map( Context* ctx, int64_t count, int np, const int64_t* poff, const int64_t* off, int dtype, int to_padded,
+                        double* packed, void* vec )
+{
+   if ( count <= 0 ) return;
+   const int blocks = int( std::min< int64_t >( ( count + 255 ) / 256, 148 * 16 ) );
+   if ( dtype == F64 ) k_repack< double ><<< blocks, 256, 0, ctx->stream >>>( count, np, poff, off, to_padded, packed, (double*) vec );
+   else if ( dtype == F32 ) k_repack< float ><<< blocks, 256, 0, ctx->stream >>>( count, np, poff, off, to_padded, packed, (float*) vec );
+   else k_repack< __half ><<< blocks, 256, 0, ctx->stream >>>( count, np, poff, off, to_padded, packed, (__half*) vec );
+   ++ctx->launches;
+   check_cuda( cudaGetLastError(), "repack launch" );
 }
 
 void launch_dot( Context* ctx, Mesh* m, int L, int dtype, uint32_t flag, const void* a, const void* b, double* out )

@@ -14,6 +14,20 @@
 // pinned host memory, event); finished slots are retired as their events complete.  Kernels and
 // reduction orders inside a slot do not depend on what else runs, so a request's result is the same
 // alone and in a mix.
+//
+// Batches (batch_width > 1): FP64 requests of one key share a batch slot of batch_width solves.  Its
+// multigrid hierarchy lives on a mesh made of batch_width disjoint copies of the request mesh
+// (hyb_internal_mesh_replicate), so every launch of a cycle (sweeps, transfers, the coarse solve)
+// serves all solves of the batch; copy r of the mesh carries the solve in batch place r.  A request
+// is placed into a free place of a batch of its key (its right-hand side is generated or uploaded on
+// the original mesh and scattered into the place, its iterate zeroed), the batch runs one V-cycle
+// for all places per scheduler pass, and per-place residual norms (dot products restricted to each
+// copy, in a fixed order) decide which solves retire; freed places take the next queued requests of
+// the key while the others keep iterating.  Places without a solve hold zero right-hand sides and
+// iterates.  Every kernel treats the copies independently except the coarse CG solve, whose step
+// lengths come from dot products over all copies: a solve's iterates in a batch therefore agree with
+// its iterates alone up to the coarse solve's tolerance (bitwise where the coarsest level has no
+// free DoF, as on the six-tetrahedra cube).
 #include "hyb_internal.hpp"
 #include "../../include/hyteg_b200.h"
 
@@ -70,6 +84,22 @@ struct ServeRequest
 struct ServeSlot
 {
    ServeKey  key;
+   // batch slots (reps > 1): the replicated mesh, one level of the original mesh for right-hand
+   // sides, the copy maps, packed staging and the solve per place
+   int                    reps    = 1;
+   hyb_mesh*              umesh   = nullptr;
+   hyb_fn*                scratch = nullptr;
+   void*                  d_poff = nullptr;
+   void*                  d_off  = nullptr;
+   void*                  d_tasks = nullptr;
+   int                    np = 0, tpad = 0;
+   int64_t                count  = 0;
+   double*                d_packed = nullptr;
+   double*                h_packed = nullptr;
+   double*                d_norms  = nullptr;  // 2 reps: ||b||^2 of fresh places, then ||r||^2 after the cycle
+   double*                h_norms  = nullptr;
+   std::vector< int64_t > rreq;
+   std::vector< char >    rfresh;
    hyb_ctx*  ctx  = nullptr;
    hyb_op*   op   = nullptr;
    hyb_gmg*  gmg  = nullptr;
@@ -105,6 +135,14 @@ extern "C" int hyb_internal_mixed_step_async( hyb_gmg* g, int inner_dtype, hyb_o
                                               double* d_out );
 extern "C" int hyb_fn_fill_random( hyb_fn* fn, int level, uint64_t seed );
 extern "C" int hyb_internal_gmg_copy_setup( hyb_gmg* dst, const hyb_gmg* src );
+extern "C" int hyb_internal_mesh_replicate( hyb_mesh* m, int R, hyb_mesh** out );
+extern "C" int hyb_internal_replica_maps( hyb_mesh* orig, hyb_mesh* uni, int R, int Ls, void** d_poff, void** d_off, void** d_tasks,
+                                          int* np_out, int64_t* count, int* tpad_out );
+extern "C" int hyb_internal_replica_copy( hyb_fn* ufn, int level, int to_union, const void* d_poff, const void* d_off_r, int np,
+                                          int64_t count, double* d_packed );
+extern "C" int hyb_internal_fn_packed_device( hyb_fn* fn, int level, int to_padded, double* d_packed );
+extern "C" int hyb_internal_residual_replicas_async( hyb_op* op, hyb_fn* x, hyb_fn* b, hyb_fn* tmp, int level, int R, const void* d_tasks,
+                                                     int tpad, double* d_out );
 
 static thread_local std::string s_err;
 
@@ -125,7 +163,16 @@ void free_slot( hyb_serve* s, ServeSlot* sl )
    hyb_fn_destroy( sl->x );
    hyb_fn_destroy( sl->b );
    hyb_fn_destroy( sl->tmp );
+   hyb_fn_destroy( sl->scratch );
    hyb_op_destroy( sl->op );
+   if ( sl->d_poff ) cudaFree( sl->d_poff );
+   if ( sl->d_off ) cudaFree( sl->d_off );
+   if ( sl->d_tasks ) cudaFree( sl->d_tasks );
+   if ( sl->d_packed ) cudaFree( sl->d_packed );
+   if ( sl->d_norms ) cudaFree( sl->d_norms );
+   if ( sl->h_packed ) cudaFreeHost( sl->h_packed );
+   if ( sl->h_norms ) cudaFreeHost( sl->h_norms );
+   hyb_mesh_destroy( sl->umesh );
    hyb_ctx_destroy( sl->ctx );
    s->used_bytes -= sl->bytes;
 }
@@ -194,6 +241,162 @@ ServeSlot* make_slot( hyb_serve* s, const ServeRequest& r )
    return s->slots.back().get();
 }
 
+ServeSlot* make_batch( hyb_serve* s, const ServeRequest& r )
+{
+   auto      sl = std::make_unique< ServeSlot >();
+   const int R  = s->p.batch_width, L = r.key.level;
+   sl->key      = r.key;
+   sl->reps     = R;
+   int dev      = 0;
+   cudaGetDevice( &dev );
+   ok( hyb_ctx_create( dev, nullptr, &sl->ctx ) );
+   ok( hyb_internal_mesh_replicate( r.key.mesh, R, &sl->umesh ) );
+   if ( r.key.kind == HYB_P1_CONST_LAPLACE ) ok( hyb_op_create( sl->ctx, sl->umesh, HYB_P1_CONST_LAPLACE, 0, L, &sl->op ) );
+   else
+   {
+      ok( hyb_op_create_divkgrad( sl->ctx, sl->umesh, 0, L, &r.coeff, r.key.blending, &sl->op ) );
+      ok( hyb_op_store_element_matrices( sl->op ) );
+   }
+   hyb_gmg_params gp;
+   hyb_gmg_params_default( &gp );
+   gp.min_level             = 0;
+   gp.max_level             = L;
+   gp.pre_smooth            = s->p.pre_smooth;
+   gp.post_smooth           = s->p.post_smooth;
+   gp.smoother              = HYB_SMOOTHER_CHEBYSHEV;
+   gp.cheb_order            = 3;
+   gp.cheb_power_iterations = s->p.power_iterations;
+   gp.use_graph             = 1;
+   ok( hyb_gmg_create( sl->ctx, sl->op, &gp, &sl->gmg ) );
+   for ( auto& up : s->slots )
+      if ( up->key == r.key && up->reps == R && up->solved )
+      {
+         ok( hyb_internal_gmg_copy_setup( sl->gmg, up->gmg ) );
+         sl->solved = true;
+         break;
+      }
+   ok( hyb_fn_create( sl->ctx, sl->umesh, HYB_F64, 0, L, &sl->x ) );
+   ok( hyb_fn_create( sl->ctx, sl->umesh, HYB_F64, 0, L, &sl->b ) );
+   ok( hyb_fn_create( sl->ctx, sl->umesh, HYB_F64, L, L, &sl->tmp ) );
+   ok( hyb_fn_create( sl->ctx, r.key.mesh, HYB_F64, L, L, &sl->scratch ) );
+   ok( hyb_internal_replica_maps( r.key.mesh, sl->umesh, R, L, &sl->d_poff, &sl->d_off, &sl->d_tasks, &sl->np, &sl->count, &sl->tpad ) );
+   if ( cudaMalloc( &sl->d_packed, size_t( std::max< int64_t >( sl->count, 1 ) ) * sizeof( double ) ) != cudaSuccess ||
+        cudaMallocHost( &sl->h_packed, size_t( std::max< int64_t >( sl->count, 1 ) ) * sizeof( double ) ) != cudaSuccess ||
+        cudaMalloc( &sl->d_norms, 2 * R * sizeof( double ) ) != cudaSuccess || cudaMallocHost( &sl->h_norms, 2 * R * sizeof( double ) ) != cudaSuccess )
+      throw std::runtime_error( "batch slot allocation failed" );
+   if ( cudaEventCreateWithFlags( &sl->ev, cudaEventDisableTiming ) != cudaSuccess ) throw std::runtime_error( "cudaEventCreate" );
+   for ( int l = 0; l <= L; ++l )
+   {
+      ok( hyb_fn_interpolate_const( sl->x, 0.0, l, HYB_ALL ) );
+      ok( hyb_fn_interpolate_const( sl->b, 0.0, l, HYB_ALL ) );
+   }
+   sl->rreq.assign( R, -1 );
+   sl->rfresh.assign( R, 0 );
+   sl->bytes = slot_bytes( r.key ) * R;
+   s->used_bytes += sl->bytes;
+   s->slots.push_back( std::move( sl ) );
+   return s->slots.back().get();
+}
+
+// a slot with no solve in it (may be evicted or, for single slots, reused)
+bool idle( const ServeSlot* sl )
+{
+   if ( sl->reps == 1 ) return sl->req < 0;
+   for ( int64_t q : sl->rreq )
+      if ( q >= 0 ) return false;
+   return !sl->pending;
+}
+
+int free_place( const ServeSlot* sl )
+{
+   for ( int i = 0; i < sl->reps; ++i )
+      if ( sl->rreq[i] < 0 ) return i;
+   return -1;
+}
+
+void* place_off( const ServeSlot* sl, int i ) { return static_cast< char* >( sl->d_off ) + size_t( i ) * sl->np * sizeof( int64_t ); }
+
+// a request into place i of a batch: right-hand side generated (or uploaded) on the original mesh and
+// scattered into copy i, the copy's iterate zeroed
+void admit_place( hyb_serve* s, ServeSlot* sl, int i, ServeRequest& r )
+{
+   const int L = r.key.level;
+   if ( r.rhs.empty() ) ok( hyb_fn_fill_random( sl->scratch, L, r.seed ) );
+   else ok( hyb_fn_upload( sl->scratch, L, r.rhs.data() ) );
+   ok( hyb_internal_fn_packed_device( sl->scratch, L, 0, sl->d_packed ) );
+   ok( hyb_internal_replica_copy( sl->b, L, 1, sl->d_poff, place_off( sl, i ), sl->np, sl->count, sl->d_packed ) );
+   void* st = nullptr;
+   hyb_ctx_stream( sl->ctx, &st );
+   if ( cudaMemsetAsync( sl->d_packed, 0, size_t( sl->count ) * sizeof( double ), (cudaStream_t) st ) != cudaSuccess )
+      throw std::runtime_error( "cudaMemsetAsync" );
+   ok( hyb_internal_replica_copy( sl->x, L, 1, sl->d_poff, place_off( sl, i ), sl->np, sl->count, sl->d_packed ) );
+   sl->rreq[i]   = r.id;
+   sl->rfresh[i] = 1;
+   r.state       = 1;
+   r.t_admit     = s->now();
+   r.cycles      = 0;
+}
+
+// one V-cycle of every place, preceded by the right-hand-side norms of fresh places (their initial
+// residual: the guess is zero), followed by every place's residual norm
+void launch_batch( hyb_serve* s, ServeSlot* sl )
+{
+   const int L = sl->key.level, R = sl->reps;
+   bool      fresh = false;
+   for ( int i = 0; i < R; ++i ) fresh = fresh || ( sl->rreq[i] >= 0 && sl->rfresh[i] );
+   if ( fresh ) ok( hyb_internal_residual_replicas_async( sl->op, nullptr, sl->b, sl->tmp, L, R, sl->d_tasks, sl->tpad, sl->d_norms ) );
+   ok( hyb_gmg_solve( sl->gmg, sl->x, sl->b, L ) );
+   ok( hyb_internal_residual_replicas_async( sl->op, sl->x, sl->b, sl->tmp, L, R, sl->d_tasks, sl->tpad, sl->d_norms + R ) );
+   void* st = nullptr;
+   hyb_ctx_stream( sl->ctx, &st );
+   if ( cudaMemcpyAsync( sl->h_norms, sl->d_norms, 2 * R * sizeof( double ), cudaMemcpyDeviceToHost, (cudaStream_t) st ) != cudaSuccess ||
+        cudaEventRecord( sl->ev, (cudaStream_t) st ) != cudaSuccess )
+      throw std::runtime_error( "residual check enqueue failed" );
+   sl->pending = true;
+}
+
+// the finished check of a batch: retire converged places (their iterate copied out)
+void retire_places( hyb_serve* s, ServeSlot* sl )
+{
+   const int R = sl->reps, L = sl->key.level;
+   void*     st = nullptr;
+   hyb_ctx_stream( sl->ctx, &st );
+   for ( int i = 0; i < R; ++i )
+   {
+      if ( sl->rreq[i] < 0 ) continue;
+      ServeRequest& r = s->reqs.at( sl->rreq[i] );
+      if ( sl->rfresh[i] )
+      {
+         r.r0          = std::sqrt( std::max( 0.0, sl->h_norms[i] ) );
+         sl->rfresh[i] = 0;
+      }
+      const double rn = std::sqrt( std::max( 0.0, sl->h_norms[R + i] ) );
+      r.cycles += 1;
+      r.rn            = rn;
+      const bool conv = r.r0 == 0.0 || rn / r.r0 < r.rtol;
+      if ( !( conv || r.cycles >= r.max_cycles || !std::isfinite( rn ) ) ) continue;
+      if ( r.x_out )
+      {
+         ok( hyb_internal_replica_copy( sl->x, L, 0, sl->d_poff, place_off( sl, i ), sl->np, sl->count, sl->d_packed ) );
+         if ( cudaMemcpyAsync( sl->h_packed, sl->d_packed, size_t( sl->count ) * sizeof( double ), cudaMemcpyDeviceToHost, (cudaStream_t) st ) !=
+                  cudaSuccess ||
+              cudaStreamSynchronize( (cudaStream_t) st ) != cudaSuccess )
+            throw std::runtime_error( "solution read-back failed" );
+         std::memcpy( r.x_out, sl->h_packed, size_t( sl->count ) * sizeof( double ) );
+      }
+      // the place's data returns to zero, so that an idle place stays idle
+      if ( cudaMemsetAsync( sl->d_packed, 0, size_t( sl->count ) * sizeof( double ), (cudaStream_t) st ) != cudaSuccess )
+         throw std::runtime_error( "cudaMemsetAsync" );
+      ok( hyb_internal_replica_copy( sl->x, L, 1, sl->d_poff, place_off( sl, i ), sl->np, sl->count, sl->d_packed ) );
+      ok( hyb_internal_replica_copy( sl->b, L, 1, sl->d_poff, place_off( sl, i ), sl->np, sl->count, sl->d_packed ) );
+      r.t_done      = s->now();
+      r.state       = ( conv && std::isfinite( rn ) ) ? 2 : 3;
+      sl->rreq[i]   = -1;
+      sl->last_used = r.t_done;
+      sl->solved    = true;
+   }
+}
+
 // queue the work of the next cycle (or the initial residual when rn < 0) and its residual check
 void launch_cycle( hyb_serve* s, ServeSlot* sl, ServeRequest& r, double rn )
 {
@@ -240,6 +443,7 @@ int hyb_serve_params_default( hyb_serve_params* p )
    p->pre_smooth       = 3;
    p->post_smooth      = 3;
    p->power_iterations = 20;
+   p->batch_width      = 1;
    return HYB_OK;
 }
 
@@ -250,6 +454,7 @@ int hyb_serve_create( hyb_ctx* ctx, const hyb_serve_params* params, hyb_serve** 
       if ( !ctx || !params || !out ) throw std::invalid_argument( "NULL argument" );
       if ( params->max_slots < 1 ) throw std::invalid_argument( "max_slots must be >= 1" );
       if ( params->inner_dtype != HYB_F32 && params->inner_dtype != HYB_F16 ) throw std::invalid_argument( "inner dtype must be F32 or F16" );
+      if ( params->batch_width < 1 || params->batch_width > 256 ) throw std::invalid_argument( "batch_width must be 1..256" );
       auto* s = new hyb_serve();
       s->ctx  = ctx;
       s->p    = *params;
@@ -322,6 +527,15 @@ int hyb_serve_step( hyb_serve* s, int* running, int* queued )
       for ( auto& up : s->slots )
       {
          ServeSlot* sl = up.get();
+         if ( sl->reps > 1 )
+         {
+            if ( sl->pending && cudaEventQuery( sl->ev ) == cudaSuccess )
+            {
+               sl->pending = false;
+               retire_places( s, sl );
+            }
+            continue;
+         }
          if ( sl->req < 0 || !sl->pending ) continue;
          if ( cudaEventQuery( sl->ev ) != cudaSuccess ) continue;
          sl->pending      = false;
@@ -351,6 +565,52 @@ int hyb_serve_step( hyb_serve* s, int* running, int* queued )
       for ( auto qi = s->queue.begin(); qi != s->queue.end(); )
       {
          ServeRequest& r    = s->reqs.at( *qi );
+         if ( s->p.batch_width > 1 && !r.key.mixed )
+         {
+            // a free place of a batch of the key (not waiting for its check), else a new batch
+            ServeSlot* batch = nullptr;
+            int        place = -1;
+            bool       has_key = false;
+            for ( auto& up : s->slots )
+               if ( up->reps > 1 && up->key == r.key )
+               {
+                  has_key = true;
+                  const int i = free_place( up.get() );
+                  if ( i >= 0 && !up->pending )
+                  {
+                     batch = up.get();
+                     place = i;
+                     break;
+                  }
+               }
+            if ( !batch && !has_key )
+            {
+               const double need = slot_bytes( r.key ) * s->p.batch_width;
+               auto room = [&]() { return s->used_bytes + need <= s->p.hbm_budget_bytes && int( s->slots.size() ) < s->p.max_slots; };
+               while ( !room() )
+               {
+                  int victim = -1;
+                  for ( size_t i = 0; i < s->slots.size(); ++i )
+                     if ( idle( s->slots[i].get() ) && ( victim < 0 || s->slots[i]->last_used < s->slots[victim]->last_used ) ) victim = int( i );
+                  if ( victim < 0 ) break;
+                  free_slot( s, s->slots[victim].get() );
+                  s->slots.erase( s->slots.begin() + victim );
+               }
+               if ( room() )
+               {
+                  batch = make_batch( s, r );
+                  place = 0;
+               }
+            }
+            if ( !batch )
+            {
+               ++qi;
+               continue;
+            }
+            admit_place( s, batch, place, r );
+            qi = s->queue.erase( qi );
+            continue;
+         }
          ServeSlot*    slot = nullptr;
          bool          has_key = false;
          for ( auto& up : s->slots )
@@ -371,7 +631,7 @@ int hyb_serve_step( hyb_serve* s, int* running, int* queued )
             {
                int victim = -1;
                for ( size_t i = 0; i < s->slots.size(); ++i )
-                  if ( s->slots[i]->req < 0 && ( victim < 0 || s->slots[i]->last_used < s->slots[victim]->last_used ) ) victim = int( i );
+                  if ( idle( s->slots[i].get() ) && ( victim < 0 || s->slots[i]->last_used < s->slots[victim]->last_used ) ) victim = int( i );
                if ( victim < 0 ) break;
                free_slot( s, s->slots[victim].get() );
                s->slots.erase( s->slots.begin() + victim );
@@ -386,8 +646,21 @@ int hyb_serve_step( hyb_serve* s, int* running, int* queued )
          admit( s, slot, r );
          qi = s->queue.erase( qi );
       }
+      // 3. the next cycle of every batch with solves in it
+      for ( auto& up : s->slots )
+         if ( up->reps > 1 && !up->pending )
+         {
+            bool any = false;
+            for ( int64_t q : up->rreq ) any = any || q >= 0;
+            if ( any ) launch_batch( s, up.get() );
+         }
       int run = 0;
-      for ( auto& up : s->slots ) run += up->req >= 0;
+      for ( auto& up : s->slots )
+      {
+         if ( up->reps == 1 ) run += up->req >= 0;
+         else
+            for ( int64_t q : up->rreq ) run += q >= 0;
+      }
       if ( running ) *running = run;
       if ( queued ) *queued = int( s->queue.size() );
       return HYB_OK;

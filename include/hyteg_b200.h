@@ -336,6 +336,9 @@ typedef struct hyb_serve_params
    int    inner_dtype;      /* HYB_F32 or HYB_F16 for mixed requests */
    int    pre_smooth, post_smooth;
    int    power_iterations; /* spectral-radius estimate per level when a slot is created */
+   int    batch_width;      /* > 1: FP64 requests of one key share batch slots of this many solves, whose
+                               multigrid runs on batch_width disjoint copies of the mesh, so that every
+                               kernel launch of a cycle serves all of them; 1: one solve per slot */
 } hyb_serve_params;
 typedef struct hyb_request
 {

@@ -120,3 +120,47 @@ def test_serve_budget_evicts_and_rejects(ctx):
     with pytest.raises(H.HybError):
         srv.submit(pm, 7, seed=1)  # can never fit the budget
     srv.close()
+
+
+def _batched(ctx, meshes, reqs, width=4, rtol=1e-8):
+    srv = H.SolveServer(ctx, max_slots=8, batch_width=width)
+    ids = [_submit(srv, meshes, r, rtol=rtol) for r in reqs]
+    srv.drain()
+    out = [(srv.status(rid), srv.solution(rid).copy()) for rid in ids]
+    srv.close()
+    return out
+
+
+def test_serve_batches_match_single_solves(ctx):
+    """Batch slots (FP64 requests of one key share one multigrid on disjoint copies of the mesh): every
+    request converges, and its solution agrees with the one-slot solve within the tolerance's reach
+    (relative max-norm difference below 1e-6 at rtol 1e-8: the two runs use spectral-radius estimates
+    from different start vectors, and on the shell the coarse CG couples the copies)."""
+    meshes = _meshes(ctx)
+    reqs = [r for r in _requests() if not r[6]] + [("cube", 4, "laplace", None, None, 19, False),
+                                                   ("cube", 4, "laplace", None, None, 20, False)]
+    got = _batched(ctx, meshes, reqs)
+    for r, (st, x) in zip(reqs, got):
+        assert st["state"] == H.CONVERGED, (r, st)
+        assert st["rel_res"] < 1e-8
+        st1, x1 = _solve_alone(ctx, meshes, r)
+        assert np.abs(x - x1).max() <= 1e-6 * np.abs(x1).max(), r
+
+
+def test_serve_batch_place_alone_equals_mix(ctx):
+    """On the six-tetrahedra cube (no free DoF on the coarsest level, so nothing couples the copies) a
+    request gives the same bits alone in its batch and among other requests of the batch; on the shell
+    the copies share the coarse CG's step lengths and the results agree within 1e-6."""
+    meshes = _meshes(ctx)
+    mix = [("cube", 4, "laplace", None, None, s, False) for s in (31, 32, 33, 34, 35)]
+    together = _batched(ctx, meshes, mix, width=4)
+    for r, (st, x) in zip(mix, together):
+        st1, x1 = _batched(ctx, meshes, [r], width=4)[0]
+        assert st1["cycles"] == st["cycles"], r
+        np.testing.assert_array_equal(x, x1)
+    shell = [("shell", 3, "divkgrad", K_SPEC, "shell", s, False) for s in (41, 42, 43)]
+    together = _batched(ctx, meshes, shell, width=2)
+    for r, (st, x) in zip(shell, together):
+        st1, x1 = _batched(ctx, meshes, [r], width=2)[0]
+        assert st["state"] == H.CONVERGED and st1["state"] == H.CONVERGED
+        assert np.abs(x - x1).max() <= 1e-6 * np.abs(x1).max(), r
