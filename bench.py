@@ -56,6 +56,11 @@ def parse():
     p.add_argument("--config4", action="store_true",
                    help="run configuration 4 as stated (P2-P1 Stokes on the shell (5,3) at level 5, FP32 inner / FP64 "
                         "outer Uzawa multigrid to rtol 1e-8; a few minutes) and print its own JSON line")
+    p.add_argument("--config5", action="store_true",
+                   help="run configuration 5 as stated (2000 requests, P1 or P2, cube or shell ntan 3/5 nrad 3, "
+                        "levels 3-7) through the serving loop and print its own JSON line")
+    p.add_argument("--config5-requests", type=int, default=2000,
+                   help="length of the configuration-5 request stream (its first N requests; 2000 as stated)")
     p.add_argument("--config2", action="store_true",
                    help="run configuration 2 as stated (P2 div-k-grad on the shell (5,3) at level 6, Chebyshev(3) "
                         "V(3,3) to rtol 1e-10; about two minutes) and print its own JSON line")
@@ -373,8 +378,8 @@ def serving_leg(H, ctx, nreq=200, seed=7):
         return {"solves_per_s": len(reqs) / (t1 - t0), "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "converged": ok, "seconds": t1 - t0}
 
-    def run(mixed, sequential):
-        srv = H.SolveServer(ctx, max_slots=4 * len(keys))
+    def run(mixed, sequential, width=1):
+        srv = H.SolveServer(ctx, max_slots=4 * len(keys), batch_width=width)
         for k in keys:  # warm every slot (operator, radii, captured cycle graphs)
             srv.submit(meshes[k[0]], k[1], kind=k[2], k=k[3], blending=k[4], seed=1, rtol=1e-8, mixed=mixed)
         srv.drain()
@@ -409,14 +414,17 @@ def serving_leg(H, ctx, nreq=200, seed=7):
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "converged": ok, "seconds": t1 - t0}
 
     served = run(mixed=True, sequential=False)
+    batched = run(mixed=False, sequential=False, width=8)
     warm = run(mixed=False, sequential=True)
     cold = plain(reqs)
     return {"requests": nreq, "distinct_hierarchies": len(keys),
             "sample": "cube L3-7 / shell(ntan=3,nrad=2) L3-5, P1 Poisson 30% / div-k-grad 70%, 2 coefficient phases, "
                       "Poisson arrivals mean 0.5 ms",
-            "served_mixed": served, "sequential_plain_fp64": cold, "sequential_warm_fp64": warm,
+            "served_mixed": served, "served_batched_fp64": batched, "batch_width": 8,
+            "sequential_plain_fp64": cold, "sequential_warm_fp64": warm,
             "speedup_solves_per_s": served["solves_per_s"] / cold["solves_per_s"],
-            "speedup_vs_sequential_warm": served["solves_per_s"] / warm["solves_per_s"]}
+            "speedup_vs_sequential_warm": served["solves_per_s"] / warm["solves_per_s"],
+            "speedup_batched_vs_sequential_warm": batched["solves_per_s"] / warm["solves_per_s"]}
 
 
 def stokes_leg(H, ctx, level=3, cycles=3):
@@ -733,6 +741,96 @@ def config4_solve(H, rtol=1e-8, level=5, max_outer=60):
     return out
 
 
+def config5_serving(H, nreq=2000, seed=5, rate_hz=400.0, plain_sample=40):
+    """Configuration 5 as stated: a stream of 2000 solve requests with Poisson arrivals (seeded, mean rate
+    400/s, above what one GPU sustains), each a P1 or P2 diffusion solve (-div(k grad u), k = exp(0.5
+    sin cos sin) with one of four phases) on the six-tetrahedra cube or the icosahedral shell with ntan in
+    {3, 5} and nrad 3 (shell blending; the classic shell mesh needs ntan - 1 a power of two, which leaves
+    3 and 5 of the range 3-5), level uniform in 3..7, rtol 1e-8.  P1 requests run FP64 defect
+    correction around FP32 cycles; P2 requests run FP64 cycles (the loop's defect correction is written
+    for P1); both on resident one-solve slots with graph-captured cycles.  Requests whose hierarchy can
+    never fit the HBM budget are rejected at submission and counted.  Reports solves/s, p50/p99 latency
+    (arrival to solution) and the rejected count; no set-up is done before the clock starts.  Baseline:
+    sequential plain FP64 solves through the plain drop-in API (operator with stored matrices, solver,
+    functions built per request, solution read back) on a seeded sample of `plain_sample` admitted
+    requests, its solves/s taken as the sample's count over its time."""
+    import torch
+
+    ctx = H.Context(0)
+    rng = np.random.default_rng(seed)
+    meshes = {"cube": H.PrimitiveStorage.cuboid(ctx=ctx)}
+    for nt in (3, 5):
+        meshes[f"shell{nt}"] = H.PrimitiveStorage.spherical_shell(nt, 3, 0.55, 1.0, ctx=ctx)
+    phases = [(0.0, 0.0, 0.0), (0.13, 0.27, 0.41), (0.71, 0.05, 0.33), (0.29, 0.83, 0.61)]
+    reqs = []
+    for i in range(nreq):
+        m = ["cube", "shell3", "shell5"][int(rng.integers(0, 3))]
+        p2 = bool(rng.random() < 0.5)
+        L = int(rng.integers(3, 8))
+        ph = phases[int(rng.integers(0, 4))]
+        reqs.append((m, L, "p2_divkgrad" if p2 else "divkgrad", ("expsin", 0.5, ph), "shell" if m != "cube" else None,
+                     int(rng.integers(1, 2**31)), not p2))
+    free0, total = torch.cuda.mem_get_info()
+    budget = 0.6 * free0  # admission budget, with room for the meshes' level tables and estimate error
+    srv = H.SolveServer(ctx, max_slots=64, hbm_budget_bytes=budget)
+    arrivals = srv.now() + np.cumsum(rng.exponential(1.0 / rate_hz, nreq))
+    min_free = free0
+    ids, admitted, rejected, i = [], [], 0, 0
+    t0 = srv.now()
+    while True:
+        now = srv.now()
+        while i < nreq and arrivals[i] <= now:
+            r = reqs[i]
+            try:
+                ids.append(srv.submit(meshes[r[0]], r[1], kind=r[2], k=r[3], blending=r[4], seed=r[5], rtol=1e-8, max_cycles=60,
+                                      mixed=r[6], arrival_time=float(arrivals[i])))
+                admitted.append(r)
+            except H.HybError:
+                rejected += 1
+            i += 1
+        run_, q = srv.step()
+        min_free = min(min_free, torch.cuda.mem_get_info()[0])
+        if i >= nreq and run_ == 0 and q == 0:
+            break
+    t1 = srv.now()
+    sts = [srv.status(j) for j in ids]
+    srv.close()
+    done = [s for s in sts if s["state"] == H.CONVERGED]
+    lat = np.array([s["t_done"] - s["t_arrival"] for s in done])
+    out = {"config": "configuration 5: serving stream", "requests": nreq, "admitted": len(ids), "rejected_hbm": rejected,
+           "converged": len(done), "seconds": t1 - t0, "solves_per_s": len(done) / (t1 - t0),
+           "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+           "cycles_mean": float(np.mean([s["cycles"] for s in done])),
+           "hbm_budget_gb": budget / 1e9, "peak_device_use_gb": (total - min_free) / 1e9,
+           "mix": "P1 (FP32 inner / FP64 outer) or P2 (FP64); cube or shell ntan 3/5 nrad 3; levels 3-7; "
+                  "k = exp(0.5 sin cos sin), 4 phases; Poisson arrivals 400/s"}
+    # sequential plain FP64 solves of a seeded sample of the admitted requests
+    pick = np.random.default_rng(seed + 1).choice(len(admitted), size=min(plain_sample, len(admitted)), replace=False)
+    tp0, okp = time.perf_counter(), 0
+    for j in sorted(pick):
+        m, L, kind, kk, bl, sd, _ = admitted[j]
+        pm = meshes[m]
+        if kind == "p2_divkgrad":
+            A = H.P2ElementwiseBlendingDivKGradOperator(pm, 0, L, ctx, k=kk, blending=bl)
+            x, b = H.P2Function("x", pm, 0, L, ctx), H.P2Function("b", pm, 0, L, ctx)
+        else:
+            A = H.P1ElementwiseBlendingDivKGradOperator(pm, 0, L, ctx, k=kk, blending=bl)
+            x, b = H.P1Function("x", pm, 0, L, ctx), H.P1Function("b", pm, 0, L, ctx)
+        A.computeAndStoreLocalElementMatrices()
+        g = H.GeometricMultigridSolver(ctx, A, 0, L, 3, 3, smoother="chebyshev", chebyshev_order=3, power_iterations=20)
+        b.fill_random(L, sd)
+        hist = g.solve_cycles(x, b, L, 60, rtol=1e-8)
+        x.download(L)
+        okp += int(hist[-1] < 1e-8 * hist[0])
+        g.close()
+        del A, g, x, b
+    tp = time.perf_counter() - tp0
+    out["sequential_plain_fp64_sample"] = {"requests": len(pick), "converged": okp, "seconds": tp,
+                                           "solves_per_s": len(pick) / tp}
+    out["speedup_vs_sequential_plain_fp64"] = out["solves_per_s"] / out["sequential_plain_fp64_sample"]["solves_per_s"]
+    return out
+
+
 def p2_cpu_reference(cells=400000):
     """The reference's per-micro-cell work of the P2 elementwise apply (integrateAll of the generated
     form + 10x10 matvec), compiled from its sources, on the host cores (test blending map)."""
@@ -824,6 +922,9 @@ def run_ours(args, rank, world, local):
         return
     if args.config4:
         print(json.dumps(config4_solve(H)))
+        return
+    if args.config5:
+        print(json.dumps(config5_serving(H, nreq=args.config5_requests)))
         return
 
     torch.cuda.set_device(local)

@@ -969,9 +969,12 @@ class SolveServer:
 
     def submit(self, storage, level, kind="laplace", k=None, blending=None, rhs=None, seed=0, rtol=1e-8,
                max_cycles=50, mixed=False, arrival_time=-1.0, want_solution=False):
+        kinds = {"laplace": P1_CONST_LAPLACE, "divkgrad": 3, "p2_divkgrad": 4, "p2_laplace": P2_CONST_LAPLACE}
+        if kind not in kinds:
+            raise ValueError("kind must be one of " + ", ".join(kinds))
         r = _Request()
         r.mesh = storage.h
-        r.op_kind = P1_CONST_LAPLACE if kind == "laplace" else 3
+        r.op_kind = kinds[kind]
         r.coeff.kind, r.coeff.value, r.coeff.amp, r.coeff.freq = 0, 1.0, 0.5, 1.0
         if isinstance(k, (int, float)):
             r.coeff.value = float(k)
@@ -991,7 +994,7 @@ class SolveServer:
             r.rhs = a.ctypes.data
         out = None
         if want_solution:
-            out = np.zeros(storage.packed_size(level))
+            out = np.zeros(storage.packed_size(level + (1 if kind.startswith("p2") else 0)))
             keep.append(out)
             r.x_out = out.ctypes.data
         rid = C.c_int64()

@@ -15,7 +15,8 @@
 // reduction orders inside a slot do not depend on what else runs, so a request's result is the same
 // alone and in a mix.
 //
-// Batches (batch_width > 1): FP64 requests of one key share a batch slot of batch_width solves.  Its
+// Batches (batch_width > 1): FP64 P1 requests of one key share a batch slot of batch_width solves
+// (P2 and mixed-precision requests keep one-solve slots).  Its
 // multigrid hierarchy lives on a mesh made of batch_width disjoint copies of the request mesh
 // (hyb_internal_mesh_replicate), so every launch of a cycle (sweeps, transfers, the coarse solve)
 // serves all solves of the batch; copy r of the mesh carries the solve in batch place r.  A request
@@ -177,6 +178,29 @@ void free_slot( hyb_serve* s, ServeSlot* sl )
    s->used_bytes -= sl->bytes;
 }
 
+// P2 requests keep P2 level l on the node set of storage level l+1
+int shift_of( int kind ) { return kind == HYB_P2_ELEM_DIVKGRAD || kind == HYB_P2_CONST_LAPLACE ? 1 : 0; }
+
+// the request's operator on a mesh (the request mesh or its replicated form), element matrices stored
+void make_op( hyb_ctx* ctx, hyb_mesh* mesh, const ServeKey& key, const hyb_coeff& coeff, hyb_op** op )
+{
+   const int L = key.level;
+   if ( key.kind == HYB_P1_CONST_LAPLACE || key.kind == HYB_P2_CONST_LAPLACE ) ok( hyb_op_create( ctx, mesh, key.kind, 0, L, op ) );
+   else
+   {
+      // resident hierarchies are solved many times: compute the element matrices once
+      if ( key.kind == HYB_P2_ELEM_DIVKGRAD ) ok( hyb_op_create_p2_divkgrad( ctx, mesh, 0, L, &coeff, key.blending, op ) );
+      else ok( hyb_op_create_divkgrad( ctx, mesh, 0, L, &coeff, key.blending, op ) );
+      ok( hyb_op_store_element_matrices( *op ) );
+   }
+}
+
+void make_fn( hyb_ctx* ctx, hyb_mesh* mesh, int kind, int lo, int hi, hyb_fn** f )
+{
+   if ( shift_of( kind ) ) ok( hyb_fn_create_p2( ctx, mesh, HYB_F64, lo, hi, f ) );
+   else ok( hyb_fn_create( ctx, mesh, HYB_F64, lo, hi, f ) );
+}
+
 // bytes a slot holds: x, b (all levels), tmp and the solver's temporaries (about six more vectors
 // per level), plus the elementwise scratch
 // (plus, for div-k-grad, the stored matrices, kept as assembled stencils: 15 values per DoF slot and
@@ -185,12 +209,16 @@ double slot_bytes( ServeKey k )
 {
    int64_t total = 0;
    double  mats  = 0;
+   const int sh = shift_of( k.kind );
    for ( int L = 0; L <= k.level; ++L )
    {
       int64_t n = 0;
-      hyb_layout_packed_size( k.mesh, L, &n );
+      hyb_layout_packed_size( k.mesh, L + sh, &n );
       total += n;
       if ( k.kind == HYB_P1_ELEM_DIVKGRAD ) mats += double( n ) * 15.0;
+      // 55 values per micro-cell; P2 level l has 8^l micro-cells per macro-cell and about 8^(l+1)/6
+      // nodes, 0.75 micro-cells per node (44 values per node with the padding of the anchor rows)
+      if ( k.kind == HYB_P2_ELEM_DIVKGRAD ) mats += double( n ) * 44.0;
    }
    return double( total ) * 8.0 * ( k.mixed ? 12.0 : 10.0 ) + mats * ( k.mixed ? 12.0 : 8.0 );
 }
@@ -203,13 +231,7 @@ ServeSlot* make_slot( hyb_serve* s, const ServeRequest& r )
    cudaGetDevice( &dev );
    ok( hyb_ctx_create( dev, nullptr, &sl->ctx ) );
    const int L = r.key.level;
-   if ( r.key.kind == HYB_P1_CONST_LAPLACE ) ok( hyb_op_create( sl->ctx, r.key.mesh, HYB_P1_CONST_LAPLACE, 0, L, &sl->op ) );
-   else
-   {
-      // resident hierarchies are solved many times: compute the element matrices once
-      ok( hyb_op_create_divkgrad( sl->ctx, r.key.mesh, 0, L, &r.coeff, r.key.blending, &sl->op ) );
-      ok( hyb_op_store_element_matrices( sl->op ) );
-   }
+   make_op( sl->ctx, r.key.mesh, r.key, r.coeff, &sl->op );
    hyb_gmg_params gp;
    hyb_gmg_params_default( &gp );
    gp.min_level             = 0;
@@ -229,9 +251,9 @@ ServeSlot* make_slot( hyb_serve* s, const ServeRequest& r )
          sl->solved = true;
          break;
       }
-   ok( hyb_fn_create( sl->ctx, r.key.mesh, HYB_F64, 0, L, &sl->x ) );
-   ok( hyb_fn_create( sl->ctx, r.key.mesh, HYB_F64, 0, L, &sl->b ) );
-   ok( hyb_fn_create( sl->ctx, r.key.mesh, HYB_F64, L, L, &sl->tmp ) );
+   make_fn( sl->ctx, r.key.mesh, r.key.kind, 0, L, &sl->x );
+   make_fn( sl->ctx, r.key.mesh, r.key.kind, 0, L, &sl->b );
+   make_fn( sl->ctx, r.key.mesh, r.key.kind, L, L, &sl->tmp );
    if ( cudaMalloc( &sl->d_norm, sizeof( double ) ) != cudaSuccess ) throw std::runtime_error( "cudaMalloc(norm)" );
    if ( cudaMallocHost( &sl->h_norm, sizeof( double ) ) != cudaSuccess ) throw std::runtime_error( "cudaMallocHost(norm)" );
    if ( cudaEventCreateWithFlags( &sl->ev, cudaEventDisableTiming ) != cudaSuccess ) throw std::runtime_error( "cudaEventCreate" );
@@ -251,12 +273,7 @@ ServeSlot* make_batch( hyb_serve* s, const ServeRequest& r )
    cudaGetDevice( &dev );
    ok( hyb_ctx_create( dev, nullptr, &sl->ctx ) );
    ok( hyb_internal_mesh_replicate( r.key.mesh, R, &sl->umesh ) );
-   if ( r.key.kind == HYB_P1_CONST_LAPLACE ) ok( hyb_op_create( sl->ctx, sl->umesh, HYB_P1_CONST_LAPLACE, 0, L, &sl->op ) );
-   else
-   {
-      ok( hyb_op_create_divkgrad( sl->ctx, sl->umesh, 0, L, &r.coeff, r.key.blending, &sl->op ) );
-      ok( hyb_op_store_element_matrices( sl->op ) );
-   }
+   make_op( sl->ctx, sl->umesh, r.key, r.coeff, &sl->op );
    hyb_gmg_params gp;
    hyb_gmg_params_default( &gp );
    gp.min_level             = 0;
@@ -275,11 +292,12 @@ ServeSlot* make_batch( hyb_serve* s, const ServeRequest& r )
          sl->solved = true;
          break;
       }
-   ok( hyb_fn_create( sl->ctx, sl->umesh, HYB_F64, 0, L, &sl->x ) );
-   ok( hyb_fn_create( sl->ctx, sl->umesh, HYB_F64, 0, L, &sl->b ) );
-   ok( hyb_fn_create( sl->ctx, sl->umesh, HYB_F64, L, L, &sl->tmp ) );
-   ok( hyb_fn_create( sl->ctx, r.key.mesh, HYB_F64, L, L, &sl->scratch ) );
-   ok( hyb_internal_replica_maps( r.key.mesh, sl->umesh, R, L, &sl->d_poff, &sl->d_off, &sl->d_tasks, &sl->np, &sl->count, &sl->tpad ) );
+   make_fn( sl->ctx, sl->umesh, r.key.kind, 0, L, &sl->x );
+   make_fn( sl->ctx, sl->umesh, r.key.kind, 0, L, &sl->b );
+   make_fn( sl->ctx, sl->umesh, r.key.kind, L, L, &sl->tmp );
+   make_fn( sl->ctx, r.key.mesh, r.key.kind, L, L, &sl->scratch );
+   ok( hyb_internal_replica_maps( r.key.mesh, sl->umesh, R, L + shift_of( r.key.kind ), &sl->d_poff, &sl->d_off, &sl->d_tasks, &sl->np,
+                                  &sl->count, &sl->tpad ) );
    if ( cudaMalloc( &sl->d_packed, size_t( std::max< int64_t >( sl->count, 1 ) ) * sizeof( double ) ) != cudaSuccess ||
         cudaMallocHost( &sl->h_packed, size_t( std::max< int64_t >( sl->count, 1 ) ) * sizeof( double ) ) != cudaSuccess ||
         cudaMalloc( &sl->d_norms, 2 * R * sizeof( double ) ) != cudaSuccess || cudaMallocHost( &sl->h_norms, 2 * R * sizeof( double ) ) != cudaSuccess )
@@ -341,12 +359,12 @@ void admit_place( hyb_serve* s, ServeSlot* sl, int i, ServeRequest& r )
 // residual: the guess is zero), followed by every place's residual norm
 void launch_batch( hyb_serve* s, ServeSlot* sl )
 {
-   const int L = sl->key.level, R = sl->reps;
+   const int L = sl->key.level, R = sl->reps, Ls = L + shift_of( sl->key.kind );
    bool      fresh = false;
    for ( int i = 0; i < R; ++i ) fresh = fresh || ( sl->rreq[i] >= 0 && sl->rfresh[i] );
-   if ( fresh ) ok( hyb_internal_residual_replicas_async( sl->op, nullptr, sl->b, sl->tmp, L, R, sl->d_tasks, sl->tpad, sl->d_norms ) );
+   if ( fresh ) ok( hyb_internal_residual_replicas_async( sl->op, nullptr, sl->b, sl->tmp, Ls, R, sl->d_tasks, sl->tpad, sl->d_norms ) );
    ok( hyb_gmg_solve( sl->gmg, sl->x, sl->b, L ) );
-   ok( hyb_internal_residual_replicas_async( sl->op, sl->x, sl->b, sl->tmp, L, R, sl->d_tasks, sl->tpad, sl->d_norms + R ) );
+   ok( hyb_internal_residual_replicas_async( sl->op, sl->x, sl->b, sl->tmp, Ls, R, sl->d_tasks, sl->tpad, sl->d_norms + R ) );
    void* st = nullptr;
    hyb_ctx_stream( sl->ctx, &st );
    if ( cudaMemcpyAsync( sl->h_norms, sl->d_norms, 2 * R * sizeof( double ), cudaMemcpyDeviceToHost, (cudaStream_t) st ) != cudaSuccess ||
@@ -406,7 +424,7 @@ void launch_cycle( hyb_serve* s, ServeSlot* sl, ServeRequest& r, double rn )
    else
    {
       if ( rn >= 0 ) ok( hyb_gmg_solve( sl->gmg, sl->x, sl->b, L ) );
-      ok( hyb_internal_residual_async( sl->op, sl->x, sl->b, sl->tmp, L, sl->d_norm ) );
+      ok( hyb_internal_residual_async( sl->op, sl->x, sl->b, sl->tmp, L + shift_of( r.key.kind ), sl->d_norm ) );
    }
    void* st = nullptr;
    hyb_ctx_stream( sl->ctx, &st );
@@ -486,18 +504,23 @@ double hyb_serve_now( hyb_serve* s ) { return s ? s->now() : 0.0; }
 int hyb_serve_submit( hyb_serve* s, const hyb_request* rq, int64_t* id )
 {
    if ( !s || !rq || !rq->mesh ) return HYB_EINVAL;
-   if ( rq->op_kind != HYB_P1_CONST_LAPLACE && rq->op_kind != HYB_P1_ELEM_DIVKGRAD ) return HYB_EINVAL;
+   if ( rq->op_kind != HYB_P1_CONST_LAPLACE && rq->op_kind != HYB_P1_ELEM_DIVKGRAD && rq->op_kind != HYB_P2_ELEM_DIVKGRAD &&
+        rq->op_kind != HYB_P2_CONST_LAPLACE )
+      return HYB_EINVAL;
+   // the defect-correction step of the serving loop is written for P1 hierarchies
+   if ( shift_of( rq->op_kind ) && rq->mixed ) return HYB_EINVAL;
+   const bool elem = rq->op_kind == HYB_P1_ELEM_DIVKGRAD || rq->op_kind == HYB_P2_ELEM_DIVKGRAD;
    if ( rq->level < 1 || rq->level > 12 || !( rq->rtol > 0 ) || rq->max_cycles < 1 ) return HYB_EINVAL;
    ServeRequest r;
    r.id            = s->next_id++;
    r.key.mesh      = rq->mesh;
    r.key.kind      = rq->op_kind;
-   r.key.blending  = rq->op_kind == HYB_P1_ELEM_DIVKGRAD ? rq->blending : 0;
+   r.key.blending  = elem ? rq->blending : 0;
    r.key.level     = rq->level;
    r.key.mixed     = rq->mixed ? 1 : 0;
    const double kk[6] = { double( rq->coeff.kind ), rq->coeff.value, rq->coeff.amp, rq->coeff.phase[0], rq->coeff.phase[1],
                           rq->coeff.phase[2] };
-   for ( int i = 0; i < 6; ++i ) r.key.k[i] = rq->op_kind == HYB_P1_ELEM_DIVKGRAD ? kk[i] : 0.0;
+   for ( int i = 0; i < 6; ++i ) r.key.k[i] = elem ? kk[i] : 0.0;
    r.coeff      = rq->coeff;
    r.seed       = rq->seed;
    r.rtol       = rq->rtol;
@@ -507,7 +530,7 @@ int hyb_serve_submit( hyb_serve* s, const hyb_request* rq, int64_t* id )
    if ( rq->rhs )
    {
       int64_t n = 0;
-      if ( hyb_layout_packed_size( rq->mesh, rq->level, &n ) != HYB_OK ) return HYB_EINVAL;
+      if ( hyb_layout_packed_size( rq->mesh, rq->level + shift_of( rq->op_kind ), &n ) != HYB_OK ) return HYB_EINVAL;
       r.rhs.assign( rq->rhs, rq->rhs + n );
    }
    if ( slot_bytes( r.key ) > s->p.hbm_budget_bytes ) return HYB_ENOMEM;  // can never be admitted
@@ -565,7 +588,7 @@ int hyb_serve_step( hyb_serve* s, int* running, int* queued )
       for ( auto qi = s->queue.begin(); qi != s->queue.end(); )
       {
          ServeRequest& r    = s->reqs.at( *qi );
-         if ( s->p.batch_width > 1 && !r.key.mixed )
+         if ( s->p.batch_width > 1 && !r.key.mixed && !shift_of( r.key.kind ) )
          {
             // a free place of a batch of the key (not waiting for its check), else a new batch
             ServeSlot* batch = nullptr;

@@ -336,14 +336,16 @@ typedef struct hyb_serve_params
    int    inner_dtype;      /* HYB_F32 or HYB_F16 for mixed requests */
    int    pre_smooth, post_smooth;
    int    power_iterations; /* spectral-radius estimate per level when a slot is created */
-   int    batch_width;      /* > 1: FP64 requests of one key share batch slots of this many solves, whose
-                               multigrid runs on batch_width disjoint copies of the mesh, so that every
-                               kernel launch of a cycle serves all of them; 1: one solve per slot */
+   int    batch_width;      /* > 1: FP64 P1 requests of one key share batch slots of this many solves,
+                               whose multigrid runs on batch_width disjoint copies of the mesh, so that
+                               every kernel launch of a cycle serves all of them (P2 and mixed requests
+                               keep one-solve slots); 1: one solve per slot */
 } hyb_serve_params;
 typedef struct hyb_request
 {
    hyb_mesh*     mesh;
-   int           op_kind;  /* HYB_P1_CONST_LAPLACE or HYB_P1_ELEM_DIVKGRAD */
+   int           op_kind;  /* HYB_P1_CONST_LAPLACE, HYB_P1_ELEM_DIVKGRAD, HYB_P2_ELEM_DIVKGRAD or HYB_P2_CONST_LAPLACE (P2:
+                              level = P2 level, rhs / x_out in the P2 packed layout, FP64 only) */
    hyb_coeff     coeff;    /* HYB_P1_ELEM_DIVKGRAD only */
    int           blending; /* HYB_P1_ELEM_DIVKGRAD only */
    int           level;

@@ -164,3 +164,21 @@ def test_serve_batch_place_alone_equals_mix(ctx):
         st1, x1 = _batched(ctx, meshes, [r], width=2)[0]
         assert st["state"] == H.CONVERGED and st1["state"] == H.CONVERGED
         assert np.abs(x - x1).max() <= 1e-6 * np.abs(x1).max(), r
+
+
+def test_serve_p2_requests(ctx):
+    """P2 requests (elementwise div-k-grad on the blended shell, the P2 constant Laplacian on the cube)
+    converge alone, and in a server with batch slots (where P2 requests keep one-solve slots) they give
+    the same bits as alone."""
+    meshes = _meshes(ctx)
+    reqs = [("shell", 2, "p2_divkgrad", K_SPEC, "shell", 51, False), ("cube", 3, "p2_laplace", None, None, 52, False),
+            ("cube", 3, "p2_laplace", None, None, 53, False), ("shell", 2, "p2_divkgrad", K_SPEC, "shell", 54, False)]
+    single = []
+    for r in reqs:
+        st, x = _solve_alone(ctx, meshes, r)
+        assert st["state"] == H.CONVERGED and st["rel_res"] < 1e-8, (r, st)
+        single.append(x)
+    got = _batched(ctx, meshes, reqs, width=2)
+    for r, x1, (st, x) in zip(reqs, single, got):
+        assert st["state"] == H.CONVERGED, (r, st)
+        assert np.array_equal(x, x1), r
