@@ -979,8 +979,11 @@ __device__ __forceinline__ void bnd_task( const LevelView& v, const OpView< A >&
    else if constexpr ( OP == OP_DINV_APPLY ) write_through( v, dst, b, i, j, owner, invd * acc );
 }
 
+// threads per block of the boundary kernel
+constexpr int kBndThreads = 256;
+
 template < typename T, typename A, int OP >
-__global__ void __launch_bounds__( 256 ) k_bnd_stencil( LevelView v, OpView< A > o, TaskSegments seg, uint32_t flag, int copy_unflagged,
+__global__ void __launch_bounds__( kBndThreads ) k_bnd_stencil( LevelView v, OpView< A > o, TaskSegments seg, uint32_t flag, int copy_unflagged,
                                                          const T* __restrict__ src, const T* __restrict__ v1, T* v2, T* dst,
                                                          A a0, A a1 )
 {
@@ -1067,7 +1070,7 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
       // branches, and the boundary kernel fills the SMs the sweep's last blocks leave idle.
       if ( nt > 0 )
       {
-         k_bnd_stencil< T, A, OP ><<< ( nt + 255 ) / 256, 256, 0, ctx->stream >>>( v, o, seg, a.flag, a.copy_unflagged, src, v1, v2, dst,
+         k_bnd_stencil< T, A, OP ><<< ( nt + kBndThreads - 1 ) / kBndThreads, kBndThreads, 0, ctx->stream >>>( v, o, seg, a.flag, a.copy_unflagged, src, v1, v2, dst,
                                                                                    A( a.a0 ), A( a.a1 ) );
          ++ctx->launches;
       }
@@ -1086,7 +1089,7 @@ static void run_stencil( Context* ctx, const LevelView& v, const OpView< A >& o,
    }
    if ( nt > 0 )
    {
-      k_bnd_stencil< T, A, OP ><<< ( nt + 255 ) / 256, 256, 0, fk.aux() >>>( v, o, seg, a.flag, a.copy_unflagged, src, v1, v2, dst,
+      k_bnd_stencil< T, A, OP ><<< ( nt + kBndThreads - 1 ) / kBndThreads, kBndThreads, 0, fk.aux() >>>( v, o, seg, a.flag, a.copy_unflagged, src, v1, v2, dst,
                                                                              A( a.a0 ), A( a.a1 ) );
       ++ctx->launches;
    }
