@@ -797,11 +797,22 @@ def config5_serving(H, nreq=2000, seed=5, rate_hz=400.0, plain_sample=40):
     srv.close()
     done = [s for s in sts if s["state"] == H.CONVERGED]
     lat = np.array([s["t_done"] - s["t_arrival"] for s in done])
+    # time in service (admission to solution) per request class; solves overlap, so the sums exceed
+    # the stream's wall time
+    classes = {}
+    for r, st in zip(admitted, sts):
+        c = classes.setdefault(f"{r[2]} {r[0]} L{r[1]}", {"n": 0, "service_s": 0.0, "cycles": 0})
+        c["n"] += 1
+        c["service_s"] += max(0.0, st["t_done"] - st["t_admit"])
+        c["cycles"] += st["cycles"]
+    rejected_classes = sorted(set(f"{r[2]} {r[0]} L{r[1]}" for r in reqs[:i] if r not in admitted))
     out = {"config": "configuration 5: serving stream", "requests": nreq, "admitted": len(ids), "rejected_hbm": rejected,
            "converged": len(done), "seconds": t1 - t0, "solves_per_s": len(done) / (t1 - t0),
            "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
            "cycles_mean": float(np.mean([s["cycles"] for s in done])),
            "hbm_budget_gb": budget / 1e9, "peak_device_use_gb": (total - min_free) / 1e9,
+           "service_by_class": dict(sorted(classes.items(), key=lambda kv: -kv[1]["service_s"])[:12]),
+           "rejected_classes": rejected_classes,
            "mix": "P1 (FP32 inner / FP64 outer) or P2 (FP64); cube or shell ntan 3/5 nrad 3; levels 3-7; "
                   "k = exp(0.5 sin cos sin), 4 phases; Poisson arrivals 400/s"}
     # sequential plain FP64 solves of a seeded sample of the admitted requests
