@@ -175,6 +175,22 @@ _SIGS = {
                                    C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int),
                                    C.POINTER(C.c_double)]),
     "hyb_serve_last_error": (C.c_char_p, []),
+    "hyb_fn_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "hyb_vtk_create": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "hyb_vtk_destroy": (C.c_int, [C.c_void_p]),
+    "hyb_vtk_set_blending": (C.c_int, [C.c_void_p, C.c_int]),
+    "hyb_vtk_set_parameter": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p]),
+    "hyb_vtk_add": (C.c_int, [C.c_void_p, C.c_void_p, C.c_char_p]),
+    "hyb_vtk_remove": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "hyb_vtk_write": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "hyb_vtk_write_packed": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.POINTER(C.c_char_p), C.POINTER(C.c_int), C.POINTER(C.c_void_p)]),
+    "hyb_checkpoint_store": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_char_p),
+                                       C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "hyb_checkpoint_function_count": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_int)]),
+    "hyb_checkpoint_function_info": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_char_p, C.c_int,
+                                               C.c_char_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "hyb_checkpoint_restore": (C.c_int, [C.c_char_p, C.c_char_p, C.c_void_p, C.c_char_p, C.c_int, C.c_int]),
 }
 
 
@@ -1040,3 +1056,115 @@ class SolveServer:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------------------------------ data export
+class VTKOutput:
+    """VTKOutput( dir, filename, storage, writeFrequency ) (dataexport/VTKOutput/VTKOutput.hpp:44-139):
+    ``add`` functions, ``write(level, timestep)`` writes <dir>/<filename>_VertexDoF_level<L>_ts<T>.vtu for
+    the P1 functions and ..._P2_level<L>_ts<T>.vtu for the P2 functions when timestep % writeFrequency
+    == 0; ``setParameter("vtkDataFormat", "ASCII" | "BINARY")``.  ``blending="shell"`` writes the points
+    under the icosahedral shell map (the storage's geometry map in the reference)."""
+
+    def __init__(self, dir, filename, storage, writeFrequency=1, blending=None):
+        h = C.c_void_p()
+        _check(lib().hyb_vtk_create(storage.h, dir.encode(), filename.encode(), int(writeFrequency), C.byref(h)))
+        self.h = h
+        self.storage = storage
+        self._fns = []
+        if blending is not None:
+            _check(lib().hyb_vtk_set_blending(h, 1 if blending == "shell" else 0))
+
+    def add(self, function, name=None):
+        _check(lib().hyb_vtk_add(self.h, function.h, (name or function.name).encode()))
+        self._fns.append(function)
+
+    def remove(self, function):
+        _check(lib().hyb_vtk_remove(self.h, function.h))
+        self._fns = [f for f in self._fns if f is not function]
+
+    def setParameter(self, key, value):
+        _check(lib().hyb_vtk_set_parameter(self.h, key.encode(), value.encode()))
+
+    def write(self, level, timestep=0):
+        _check(lib().hyb_vtk_write(self.h, level, timestep))
+
+    def close(self):
+        if self.h:
+            lib().hyb_vtk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def write_vtu_packed(storage, path, level, fields, order=1, blending=None, binary=False):
+    """Write one VTK file from host data: ``fields`` maps names to packed level vectors (the
+    ``download`` layout; P2 vectors of the level+1 node set when order=2), or to (vector, dtype)."""
+    names, dts, ptrs, keep = [], [], [], []
+    for name, v in fields.items():
+        dt = F64
+        if isinstance(v, tuple):
+            v, dt = v[0], (_DTYPES[v[1]] if isinstance(v[1], str) else int(v[1]))
+        a = np.ascontiguousarray(v, dtype=np.float64)
+        keep.append(a)
+        names.append(name.encode())
+        dts.append(dt)
+        ptrs.append(a.ctypes.data)
+    n = len(names)
+    _check(lib().hyb_vtk_write_packed(storage.h, path.encode(), level, order, 1 if blending == "shell" else 0, 1 if binary else 0, n,
+                                      (C.c_char_p * max(n, 1))(*names), (C.c_int * max(n, 1))(*dts),
+                                      (C.c_void_p * max(n, 1))(*ptrs)))
+
+
+class CheckpointExporter:
+    """registerFunction( function, minLevel, maxLevel ) / storeCheckpoint( filePath, fileName )
+    (checkpointrestore/CheckpointExporter.hpp:26-60); the file is <filePath>/<fileName>.hybckpt."""
+
+    def __init__(self):
+        self._reg = []
+
+    def registerFunction(self, function, minLevel=None, maxLevel=None):
+        lo = function.min_level if minLevel is None else minLevel
+        hi = function.max_level if maxLevel is None else maxLevel
+        self._reg = [r for r in self._reg if r[0] is not function] + [(function, lo, hi)]
+
+    def deregisterFunction(self, function):
+        self._reg = [r for r in self._reg if r[0] is not function]
+
+    def storeCheckpoint(self, filePath, fileName):
+        n = len(self._reg)
+        _check(lib().hyb_checkpoint_store(filePath.encode(), fileName.encode(), n,
+                                          (C.c_void_p * max(n, 1))(*[r[0].h.value for r in self._reg]),
+                                          (C.c_char_p * max(n, 1))(*[r[0].name.encode() for r in self._reg]),
+                                          (C.c_int * max(n, 1))(*[r[1] for r in self._reg]),
+                                          (C.c_int * max(n, 1))(*[r[2] for r in self._reg])))
+
+
+class CheckpointImporter:
+    """The importer side (ADIOS2/AdiosCheckpointImporter.hpp:97-170): ``getFunctionDetails()`` lists
+    (name, kind, valueType, minLevel, maxLevel); ``restoreFunction(function, minLevel, maxLevel)``
+    fills the function's levels from the checkpoint entry of the same name."""
+
+    def __init__(self, filePath, fileName):
+        self.dir, self.name = filePath.encode(), fileName.encode()
+
+    def getFunctionDetails(self):
+        n = C.c_int()
+        _check(lib().hyb_checkpoint_function_count(self.dir, self.name, C.byref(n)))
+        out = []
+        for i in range(n.value):
+            nb, kb, vb = C.create_string_buffer(1024), C.create_string_buffer(64), C.create_string_buffer(64)
+            lo, hi = C.c_int(), C.c_int()
+            _check(lib().hyb_checkpoint_function_info(self.dir, self.name, i, nb, 1024, kb, 64, vb, 64, C.byref(lo), C.byref(hi)))
+            out.append({"name": nb.value.decode(), "kind": kb.value.decode(), "valueType": vb.value.decode(),
+                        "minLevel": lo.value, "maxLevel": hi.value})
+        return out
+
+    def restoreFunction(self, function, minLevel=None, maxLevel=None):
+        lo = function.min_level if minLevel is None else minLevel
+        hi = function.max_level if maxLevel is None else maxLevel
+        _check(lib().hyb_checkpoint_restore(self.dir, self.name, function.h, function.name.encode(), lo, hi))

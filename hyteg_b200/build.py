@@ -18,7 +18,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libhyteg_b200.so")
 OBJ_DIR = os.path.join(HERE, "_build")
 
-SOURCES = ["topology.cpp", "mesh_gen.cpp", "p1_kernels.cu", "p1_elementwise.cu", "p2_constant.cu", "capi.cu", "serve.cu"]
+SOURCES = ["topology.cpp", "mesh_gen.cpp", "p1_kernels.cu", "p1_elementwise.cu", "p2_constant.cu", "capi.cu", "serve.cu", "dataexport.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1037,6 +1037,23 @@ int hyb_fn_device_ptr( hyb_fn* fn, int level, void** ptr, int64_t* nslots )
    HYB_CATCH
 }
 
+int hyb_fn_info( const hyb_fn* fn, int* order, int* dtype, int* min_level, int* max_level )
+{
+   HYB_TRY
+   require( fn, "fn is NULL" );
+   if ( order ) *order = 1 + fn->f.lshift;
+   if ( dtype ) *dtype = fn->f.dtype;
+   if ( min_level ) *min_level = fn->f.minL - fn->f.lshift;
+   if ( max_level ) *max_level = fn->f.maxL - fn->f.lshift;
+   HYB_CATCH
+}
+
+// the host topology of a mesh and the error message of the calling thread, for the data-export file
+extern "C" const hyb::Topology* hyb_internal_topology( const hyb_mesh* m ) { return m ? &m->m.topo : nullptr; }
+extern "C" const hyb::Topology* hyb_internal_fn_topology( const hyb_fn* fn ) { return &fn->f.mesh->topo; }
+extern "C" int64_t hyb_internal_fn_packed_size( const hyb_fn* fn, int level ) { return fn->f.mesh->level( lv( fn, level ) ).packed_size; }
+extern "C" void                 hyb_internal_set_error( const char* msg ) { g_err = msg ? msg : ""; }
+
 // ------------------------------------------------------------------------------------------- operators
 int hyb_op_create( hyb_ctx* ctx, hyb_mesh* mesh, int kind, int min_level, int max_level, hyb_op** out )
 {

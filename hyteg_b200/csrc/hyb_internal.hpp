@@ -262,6 +262,8 @@ struct CellGeom {
    double volT, rad_ray, rad_ref;
    int    blend;
 };
+// vertices and (blending 1) the IcosahedralShellMap classification of macro-cell c
+void cell_geometry( const Topology& t, int c, int blending, CellGeom& g );
 
 struct ElemLevel {
    void* d_acc  = nullptr;  // accumulation buffer (level size, accumulation precision)

@@ -91,18 +91,20 @@ static void classify_shell( const Topology& t, int c, CellGeom& g, int depth = 0
    g.rad_ref = rad[iref];
 }
 
+void cell_geometry( const Topology& t, int c, int blending, CellGeom& g )
+{
+   g = CellGeom{};
+   for ( int k = 0; k < 4; ++k )
+      for ( int d = 0; d < 3; ++d ) g.P[k][d] = t.vx[t.cv[c][k]][d];
+   g.blend = blending;
+   if ( blending == 1 ) classify_shell( t, c, g );
+}
+
 void build_elementwise_operator( Operator* A )
 {
    const Topology& t = A->mesh->topo;
    A->geom.assign( t.nC, CellGeom{} );
-   for ( int c = 0; c < t.nC; ++c )
-   {
-      CellGeom& g = A->geom[c];
-      for ( int k = 0; k < 4; ++k )
-         for ( int d = 0; d < 3; ++d ) g.P[k][d] = t.vx[t.cv[c][k]][d];
-      g.blend = A->blending;
-      if ( A->blending == 1 ) classify_shell( t, c, g );
-   }
+   for ( int c = 0; c < t.nC; ++c ) cell_geometry( t, c, A->blending, A->geom[c] );
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -208,6 +208,8 @@ int hyb_fn_copy_from( hyb_fn* dst, hyb_fn* src, int level );
 int hyb_fn_swap( hyb_fn* a, hyb_fn* b, int level );
 /* device pointer and slot count of one level (padded device layout) */
 int hyb_fn_device_ptr( hyb_fn* fn, int level, void** ptr, int64_t* nslots );
+/* order (1: P1Function, 2: P2Function), value type and level range of a function (any may be NULL) */
+int hyb_fn_info( const hyb_fn* fn, int* order, int* dtype, int* min_level, int* max_level );
 
 /* ---------------------------------------------------------------- operators
  * Operator<Src,Dst>::apply(src, dst, level, flag, updateType) (operators/Operator.hpp:74-81),
@@ -453,6 +455,44 @@ int hyb_stokes_solve( hyb_stokes* s, hyb_fn* const* u3, hyb_fn* p, hyb_fn* const
  * FP64 update; u3, p, bu3, bp hold FP64 values */
 int hyb_stokes_mixed_solve( hyb_stokes* outer, hyb_stokes* inner, int inner_dtype, hyb_fn* const* u3, hyb_fn* p, hyb_fn* const* bu3,
                             hyb_fn* bp, int level, int max_outer, double rtol, double* history, int* iterations );
+
+/* ---------------------------------------------------------------- data export and checkpoints
+ * VTKOutput (dataexport/VTKOutput/VTKOutput.hpp:44-139; VTKOutput( dir, filename, storage,
+ * writeFrequency ), add( function ), write( level, timestep ), setParameter( "vtkDataFormat",
+ * "ASCII" | "BINARY" )).  write() writes, when timestep % write_frequency == 0, one file per DoF type
+ * with added functions: <dir>/<filename>_VertexDoF_level<L>_ts<T>.vtu for P1 functions and
+ * <dir>/<filename>_P2_level<L>_ts<T>.vtu for P2 functions (an XML UnstructuredGrid piece: per macro-cell
+ * the micro-vertices of level L, for P2 of level L+1, at their positions under the storage's geometry
+ * map, the micro-tetrahedra of level L, for P2 as ten-node quadratic tetrahedra, and each function as
+ * point data).  Functions are downloaded at write time; they must stay alive while added. */
+typedef struct hyb_vtk hyb_vtk;
+int hyb_vtk_create( hyb_mesh* mesh, const char* dir, const char* filename, int write_frequency, hyb_vtk** out );
+int hyb_vtk_destroy( hyb_vtk* w );
+/* the geometry map of the point coordinates (the storage's blending map in the reference):
+ * HYB_BLEND_NONE (default) or HYB_BLEND_SHELL */
+int hyb_vtk_set_blending( hyb_vtk* w, int blending );
+int hyb_vtk_set_parameter( hyb_vtk* w, const char* key, const char* value );
+int hyb_vtk_add( hyb_vtk* w, hyb_fn* fn, const char* name );
+int hyb_vtk_remove( hyb_vtk* w, hyb_fn* fn );
+int hyb_vtk_write( hyb_vtk* w, int level, int timestep );
+/* the same file from host data: nfields packed vectors (hyb_fn_download layout) of one order at
+ * `level`, written to `path`; dtypes name each field's value type (HYB_F64 -> Float64, else Float32) */
+int hyb_vtk_write_packed( hyb_mesh* mesh, const char* path, int level, int order, int blending, int binary, int nfields,
+                          const char* const* names, const int* dtypes, const double* const* packed );
+
+/* Checkpoints (checkpointrestore/CheckpointExporter.hpp:26-60: registerFunction( function, minLevel,
+ * maxLevel ), storeCheckpoint( filePath, fileName ); ADIOS2/AdiosCheckpointImporter.hpp:97-170:
+ * getFunctionDetails(), restoreFunction( function, minLevel, maxLevel )).  ADIOS2 is not used: the
+ * checkpoint is <dir>/<filename>.hybckpt in this library's own binary format (the mesh's primitive
+ * counts and a hash of its coordinates and cells; per function its name, kind, value type, level range
+ * and the packed vector of every level).  Restoring refuses a different mesh, kind or value type and a
+ * level range the checkpoint does not hold, as the reference's importer does. */
+int hyb_checkpoint_store( const char* dir, const char* filename, int nfn, hyb_fn* const* fns, const char* const* names,
+                          const int* min_levels, const int* max_levels );
+int hyb_checkpoint_function_count( const char* dir, const char* filename, int* count );
+int hyb_checkpoint_function_info( const char* dir, const char* filename, int index, char* name, int name_cap, char* kind, int kind_cap,
+                                  char* value_type, int vtype_cap, int* min_level, int* max_level );
+int hyb_checkpoint_restore( const char* dir, const char* filename, hyb_fn* fn, const char* name, int min_level, int max_level );
 
 #ifdef __cplusplus
 }
