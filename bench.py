@@ -511,7 +511,7 @@ def stokes_leg(H, ctx, level=3, cycles=3):
     return {"mesh": "spherical shell ntan=5 nrad=3 (1920 macro-cells), IcosahedralShellMap blending", "level": level,
             "time_to_rtol_1e-6": {"level": Lr, "rhs": "x / |x| (unit buoyancy)", **runs}, "full_viscous": full_viscous,
             "viscosity": "exp(2.99 (1 - r) / 0.45)", "velocity_dofs": 3 * nu, "pressure_dofs": pm.packed_size(level),
-            "cycle": "V(3,3) Uzawa (Chebyshev(3) x 3 velocity sweeps, omega 0.7, inverted PSPG diagonal), 100 coarse Uzawa steps",
+            "cycle": "V(3,3) Uzawa (Chebyshev(3) x 3 velocity sweeps, omega 0.7, inverted PSPG diagonal), 30 coarse Uzawa steps",
             "ms_per_cycle": sec * 1e3, "factors": [float(f) for f in hist[1:] / hist[:-1]], "dtype": "f64",
             "stored_velocity_matrices": True}
 
@@ -702,7 +702,7 @@ def config4_solve(H, rtol=1e-8, level=5, max_outer=60):
            "velocity_dofs": 3 * pm.packed_size(level + 1), "pressure_dofs": pm.packed_size(level), "rtol": rtol,
            "viscosity": "exp(2.99 (1 - r) / 0.45)", "rhs": "T r/|r|, T seeded uniform [0, 1]",
            "cycle": "V(3,3) Uzawa, Chebyshev(3) x 3 velocity sweeps, pressure update by the inverse lumped mass "
-                    "weighted by 1/eta, omega = 1/rho (estimated), 100 coarse Uzawa steps"}
+                    "weighted by 1/eta, omega = 1/rho (estimated), 30 coarse Uzawa steps"}
     runs = {}
     for mode in ("fp32_inner_fp64_outer", "fp64"):
         st = H.StokesUzawaMultigrid(ctx, pm, 0, level, viscosity=visc, blending="shell", pressure_scaling="lumped_mass")

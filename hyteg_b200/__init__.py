@@ -755,7 +755,7 @@ class StokesUzawaMultigrid:
     (2/3) eta div u div v, the three components coupled) with Chebyshev on the coupled block."""
 
     def __init__(self, ctx, storage, min_level, max_level, viscosity=None, blending=None, pre=3, post=3,
-                 velocity_sweeps=3, cheb_order=3, power_iterations=20, omega=0.7, coarse_sweeps=100,
+                 velocity_sweeps=3, cheb_order=3, power_iterations=20, omega=0.7, coarse_sweeps=30,
                  velocity_block="laplace", pressure_scaling="pspg"):
         if velocity_block not in ("laplace", "full_viscous"):
             raise ValueError("velocity_block must be 'laplace' or 'full_viscous'")

@@ -2926,7 +2926,7 @@ int hyb_stokes_params_default( hyb_stokes_params* p )
    p->cheb_order       = 3;
    p->power_iterations = 20;
    p->omega            = 0.7;
-   p->coarse_sweeps    = 100;
+   p->coarse_sweeps    = 30;
    p->velocity_block   = 0;
    p->pressure_scaling = 0;
    return HYB_OK;

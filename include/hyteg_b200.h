@@ -411,7 +411,7 @@ typedef struct hyb_stokes_params
    int    cheb_order;       /* Chebyshev order of the velocity smoother (ChebyshevSmoother) */
    int    power_iterations; /* spectral-radius estimate of D^-1 A per level */
    double omega;            /* Uzawa relaxation parameter (UzawaSmoother::setRelaxationParameter) */
-   int    coarse_sweeps;    /* Uzawa steps on the coarsest level (the coarse solve) */
+   int    coarse_sweeps;    /* Uzawa steps on the coarsest level (the coarse solve; default 30) */
    int    velocity_block;   /* 0: -div(eta grad) per component (block Laplace); 1: the full viscous block
                                P2ElementwiseBlendingFullViscousOperator, Chebyshev on the coupled block */
    int    pressure_scaling; /* scaling S^-1 of the pressure update p += omega S^-1 (b_p - div u):

@@ -1809,7 +1809,7 @@ class P2P1Stokes:
         p[mp] += omega * (self.sinv[L] * rp)[mp]
         return u, self.plev[L].sync(p)
 
-    def vcycle(self, u, p, bu, bp, L, radii, order=3, pre=3, post=3, sweeps=3, omega=0.7, coarse=100):
+    def vcycle(self, u, p, bu, bp, L, radii, order=3, pre=3, post=3, sweeps=3, omega=0.7, coarse=30):
         if L == self.minL:
             for _ in range(coarse):
                 u, p = self.uzawa(u, p, bu, bp, L, radii[L], order, sweeps, omega)

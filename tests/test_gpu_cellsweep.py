@@ -94,3 +94,21 @@ def test_zstream_low_precision(ctx, dtype, tol):
     bq = fb.download(L)
     ref = s.op.smooth_jac(np.zeros_like(xq), bq, xq, 0.6, L, O.INNER)
     assert relerr(fy.download(L), ref, mask) < tol
+
+
+def test_chebyshev_vcycle_factors_fp32(ctx):
+    """FP32 storage: the Chebyshev V-cycle on levels 0-6 (fused CHEB0 / CHEBI / CHEBL sweeps on levels 5
+    and 6 in FP32) follows the FP64 oracle's residual reduction within 1e-4 per cycle, and its iterate
+    within 1e-5."""
+    L = 6
+    s = Setup(ctx, "cube_6", 0, L, dtype="float32")
+    radii = {l: 2.0 + 0.03 * l for l in range(0, L + 1)}
+    ref_hist, ref_x, b = _gmg_history(s, L, "chebyshev", 3, radii=radii, pre=2, post=2, cheb_order=3)
+    fx, fb = s.fn(), s.fn()
+    fb.upload(L, b)
+    gmg = H.GeometricMultigridSolver(ctx, s.A, 0, L, preSmoothSteps=2, postSmoothSteps=2, smoother="chebyshev",
+                                     chebyshev_order=3)
+    gmg.set_radii([radii[l] for l in range(0, L + 1)])
+    hist = gmg.solve_cycles(fx, fb, L, 3)
+    np.testing.assert_allclose(hist[1:] / hist[:-1], ref_hist[1:] / ref_hist[:-1], rtol=0, atol=1e-4)
+    assert relerr(fx.download(L), ref_x, s.op.levels[L].owned_mask(O.ALL)) < 1e-5
