@@ -12,6 +12,7 @@
  *   P1toP1LinearRestriction / P1toP1LinearProlongation  gridtransferoperators/
  *   CGSolver(storage, minLevel, maxLevel, maxIter, relTol, absTol)  solvers/CGSolver.hpp:44-75
  *   GeometricMultigridSolver::solve(A, x, b, level)  solvers/GeometricMultigridSolver.hpp:180-305
+ *   VTKOutput(dir, filename, storage, writeFrequency)  dataexport/VTKOutput/VTKOutput.hpp:44-139
  *
  * Errors: the reference aborts the process (WALBERLA_ABORT / WALBERLA_CHECK); here every failing
  * call goes to one error handler, by default throwing hyteg::b200::Error with the library's message.
@@ -345,6 +346,41 @@ class GeometricMultigridSolver
 
  private:
    hyb_gmg* h_ = nullptr;
+};
+
+// VTKOutput (dataexport/VTKOutput/VTKOutput.hpp:44-139): add() functions, write( level, timestep )
+// writes <dir>/<filename>_VertexDoF_level<L>_ts<T>.vtu when timestep % writeFrequency == 0;
+// setParameter( "vtkDataFormat", "ASCII" | "BINARY" ).  Added functions must outlive the writer's
+// write() calls (they are downloaded at write time).
+class VTKOutput
+{
+ public:
+   VTKOutput( const std::string& dir, const std::string& filename, const PrimitiveStorage& storage, uint_fast32_t writeFrequency = 1 )
+   {
+      b200::check( hyb_vtk_create( storage.get(), dir.c_str(), filename.c_str(), int( writeFrequency ), &h_ ) );
+   }
+   ~VTKOutput() { if ( h_ ) hyb_vtk_destroy( h_ ); }
+   VTKOutput( const VTKOutput& )            = delete;
+   VTKOutput& operator=( const VTKOutput& ) = delete;
+
+   template < typename Function >
+   void add( const Function& function )
+   {
+      b200::check( hyb_vtk_add( h_, function.get(), function.getFunctionName().c_str() ) );
+   }
+   template < typename Function >
+   void remove( const Function& function )
+   {
+      b200::check( hyb_vtk_remove( h_, function.get() ) );
+   }
+   void setParameter( const std::string& key, const std::string& value )
+   {
+      b200::check( hyb_vtk_set_parameter( h_, key.c_str(), value.c_str() ) );
+   }
+   void write( uint_fast32_t level, uint_fast32_t timestep = 0 ) const { b200::check( hyb_vtk_write( h_, int( level ), int( timestep ) ) ); }
+
+ private:
+   hyb_vtk* h_ = nullptr;
 };
 
 }  // namespace hyteg

@@ -8,6 +8,7 @@
 //         y32.bin     the same apply with FP32 storage, converted to doubles
 //         x32.bin     its input as stored in FP32, converted to doubles
 //         hist.txt    residual norms ||r_0|| .. ||r_6|| of six V(2,2) cycles for b = f(x, y, z)
+//         gmg_VertexDoF_level<level>_ts0.vtu   x and y written by VTKOutput (binary)
 #include <cmath>
 #include <cstdio>
 #include <fstream>
@@ -46,6 +47,13 @@ int main( int argc, char** argv )
       x.interpolate( u, level, All );
       A.apply( x, y, level, Inner, Replace );
       write( dir + "/y.bin", y.download( level, packed ) );
+      {
+         VTKOutput vtk( dir, "gmg", storage );
+         vtk.add( x );
+         vtk.add( y );
+         vtk.setParameter( "vtkDataFormat", "BINARY" );
+         vtk.write( level );
+      }
 
       P1Function< float > x32( "x32", ctx, storage, 0, level ), y32( "y32", ctx, storage, 0, level );
       x32.copyFrom( x, level );

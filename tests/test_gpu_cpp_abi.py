@@ -93,3 +93,19 @@ def test_cpp_gmg_factors_match_oracle(cpp_run):
     ref = np.array(ref)
     np.testing.assert_allclose(hist[0], ref[0], rtol=1e-12)
     np.testing.assert_allclose(hist[1:] / hist[:-1], ref[1:] / ref[:-1], rtol=0, atol=1e-6)
+
+
+def test_cpp_vtk_output_holds_the_functions(cpp_run):
+    """The C++ VTKOutput adaptor wrote the level's file; its point data "y" is the macro-cells' arrays of
+    the downloaded apply result."""
+    from tests.test_dataexport import read_vtu, tet_size
+
+    npts, ncells, _, _, data = read_vtu(str(cpp_run / f"gmg_VertexDoF_level{LEVEL}_ts0.vtu"))
+    coords, tets = O.mesh_cuboid()
+    m = O.MacroMesh(coords, tets)
+    lev = O.Level(m, LEVEL)
+    ppc = tet_size((1 << LEVEL) + 1)
+    assert npts == m.nC * ppc and ncells == m.nC * 8 ** LEVEL and set(data) == {"x", "y"}
+    y = np.fromfile(cpp_run / "y.bin", dtype=np.float64)
+    want = np.concatenate([y[o:o + ppc] for o in lev.off_c])
+    assert np.array_equal(data["y"], want)
