@@ -112,6 +112,32 @@ def test_vtu_binary_equals_ascii(tmp_path):
 
 
 @pytest.mark.skipif(not R.shell_available(), reason="oracle/_ref shell library not built")
+def test_vtu_p2_shell_nodes_match_reference_map(tmp_path):
+    """P2 file on the blended shell: every node of the level+1 grid (vertex and edge nodes of the
+    quadratic tetrahedra) is the reference map's image of its affine position, so the edge nodes are
+    mapped midpoints, not midpoints of the mapped corners."""
+    pm = H.PrimitiveStorage.spherical_shell(3, 2, 0.55, 1.0)
+    nC = pm.counts()[3]
+    L = 1
+    N = 2 << L
+    pb, pa = str(tmp_path / "b.vtu"), str(tmp_path / "a.vtu")
+    H.write_vtu_packed(pm, pb, L, {}, order=2, blending="shell")
+    H.write_vtu_packed(pm, pa, L, {}, order=2)
+    _, nc, ptsb, cells, _ = read_vtu(pb)
+    _, _, ptsa, _, _ = read_vtu(pa)
+    assert nc == nC * 8 ** L and np.all(cells["types"] == 24)
+    coords = pm.vertex_coords()
+    tets = np.array([pm.primitive_vertices(3, c) for c in range(nC)], dtype=np.int32)
+    ppc = tet_size(N + 1)
+    for c in range(0, nC, 7):
+        F, _, _ = R.shell_map_eval(coords, tets, c, ptsa[c * ppc:(c + 1) * ppc])
+        assert np.abs(F - ptsb[c * ppc:(c + 1) * ppc]).max() < 1e-14
+    t = cells["connectivity"].reshape(-1, 10)
+    mid = 0.5 * (ptsb[t[:, 0]] + ptsb[t[:, 1]])
+    assert np.abs(ptsb[t[:, 4]] - mid).max() > 1e-4  # curved edges
+
+
+@pytest.mark.skipif(not R.shell_available(), reason="oracle/_ref shell library not built")
 def test_vtu_shell_points_match_reference_map(tmp_path):
     """Points under the shell blending: every macro-cell's micro-vertices equal the reference's
     IcosahedralShellMap::evalF at their affine positions (1e-14), and the blended micro-tetrahedra fill
