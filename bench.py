@@ -1101,7 +1101,8 @@ def run_ours(args, rank, world, local):
         rate, k, threads, el = cpu
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
                                 "sample": f"{k} applies of the 6 macro-cell interiors at level {L} in {el:.1f} s "
-                                          f"(reference's generated kernel, one macro-cell per thread)"}
+                                          f"(reference's generated kernel, one macro-cell per thread: {threads} of "
+                                          f"{os.cpu_count()} host cores, the reference parallelises applies over macro-cells)"}
     print(json.dumps(line))
 
 
