@@ -190,3 +190,38 @@ def test_vtu_and_checkpoint_arguments_are_checked(tmp_path):
     bad.write_bytes(b"not a checkpoint at all")
     with pytest.raises(H.HybError):
         H.CheckpointImporter(str(tmp_path), "bad").getFunctionDetails()
+
+
+def _fake_checkpoint(path, entries, counts=(8, 19, 18, 6), mesh_hash=0):
+    """A checkpoint file in the library's format written from Python: magic, version, primitive counts,
+    mesh hash, then per function name, kind, value type, level range and per level a packed vector."""
+    import struct
+
+    def s(x):
+        b = x.encode()
+        return struct.pack("<I", len(b)) + b
+
+    out = b"HYBCKPT1" + struct.pack("<I", 1) + struct.pack("<4i", *counts) + struct.pack("<Q", mesh_hash)
+    out += struct.pack("<I", len(entries))
+    for name, kind, vt, lo, hi in entries:
+        out += s(name) + s(kind) + s(vt) + struct.pack("<ii", lo, hi)
+        for lv in range(lo, hi + 1):
+            n = 3 + lv
+            out += struct.pack("<q", n) + np.arange(n, dtype=np.float64).tobytes()
+    path.write_bytes(out)
+
+
+def test_checkpoint_table_is_read_and_checked(tmp_path):
+    """getFunctionDetails reads the function table (skipping every level's data); a truncated file and a
+    wrong format version are refused."""
+    _fake_checkpoint(tmp_path / "ok.hybckpt", [("u", "P1Function", "double", 1, 3), ("w", "P2Function", "float", 0, 2)])
+    det = H.CheckpointImporter(str(tmp_path), "ok").getFunctionDetails()
+    assert det == [{"name": "u", "kind": "P1Function", "valueType": "double", "minLevel": 1, "maxLevel": 3},
+                   {"name": "w", "kind": "P2Function", "valueType": "float", "minLevel": 0, "maxLevel": 2}]
+    raw = (tmp_path / "ok.hybckpt").read_bytes()
+    (tmp_path / "cut.hybckpt").write_bytes(raw[:60])
+    with pytest.raises(H.HybError):
+        H.CheckpointImporter(str(tmp_path), "cut").getFunctionDetails()
+    (tmp_path / "v2.hybckpt").write_bytes(raw[:8] + (2).to_bytes(4, "little") + raw[12:])
+    with pytest.raises(H.HybError):
+        H.CheckpointImporter(str(tmp_path), "v2").getFunctionDetails()
